@@ -1,0 +1,94 @@
+/* Seeded initial conditions for the hydro / MHD step workloads.
+ *
+ * Header-only, valid C99 and C++, host-side, so that every party that sets up a
+ * mesh (the problem generators of this package, the CPU restatement of the
+ * step, and the problem generator compiled against the original Kratos
+ * sources) builds bit-identical initial states from the same cell coordinates.
+ * The noise is a counter-based generator (SplitMix64 of seed and global cell
+ * index), so it does not depend on how the mesh is split into blocks.
+ *
+ * Workloads (coordinates on [0,1)^3, periodic):
+ *   shock : rho = 1 | 0.125, p = 1 | 0.1 split at x = 0.5, v = 0,
+ *           rho *= 1 + 1e-3 U(-1,1)
+ *   ot    : Orszag-Tang-type vortex, rho = 25/(36 pi), p = 5/(12 pi),
+ *           v = (-sin 2 pi y, sin 2 pi x, 0) + 1e-3 U(-1,1) per component,
+ *           B = (-sin 2 pi y, sin 4 pi x, 0) / sqrt(4 pi) sampled at face
+ *           centres (exactly divergence free: B_x has no x dependence, B_y no
+ *           y dependence)
+ */
+#ifndef KR_PROBLEMS_H
+#define KR_PROBLEMS_H
+
+#include <math.h>
+#include <stdint.h>
+
+static inline uint64_t kr_splitmix64( uint64_t x )
+{
+    x += 0x9E3779B97F4A7C15ull;
+    x  = ( x ^ ( x >> 30 ) ) * 0xBF58476D1CE4E5B9ull;
+    x  = ( x ^ ( x >> 27 ) ) * 0x94D049BB133111EBull;
+    return x ^ ( x >> 31 );
+}
+
+/* Uniform in [-1, 1): 53 random bits of the hashed (seed, stream, cell) key. */
+static inline double kr_uniform_pm1( uint64_t seed, uint64_t stream, uint64_t cell )
+{
+    const uint64_t h = kr_splitmix64( kr_splitmix64( seed * 0x100000001B3ull + stream ) ^ cell );
+    return ( double )( h >> 11 ) * ( 2.0 / 9007199254740992.0 ) - 1.0;
+}
+
+/* Global linear cell index at a refinement level (x fastest). */
+static inline uint64_t kr_cell_key( int level, const int ig[ 3 ], const int n_glob[ 3 ] )
+{
+    const uint64_t nx = ( uint64_t ) n_glob[ 0 ] << level;
+    const uint64_t ny = ( uint64_t ) n_glob[ 1 ] << level;
+    return ( ( uint64_t ) level << 58 )
+         ^ ( ( uint64_t ) ig[ 0 ] + nx * ( ( uint64_t ) ig[ 1 ] + ny * ( uint64_t ) ig[ 2 ] ) );
+}
+
+#define KR_PI 3.14159265358979323846
+
+/* shock: conserved state of one cell.  u[0] rho, u[1] E, u[2..4] momentum. */
+static inline void kr_shock_cell( double * u, double x, double gamma,
+                                  uint64_t seed, uint64_t key )
+{
+    const int left = x < 0.5;
+    double rho = left ? 1.0 : 0.125;
+    const double pre = left ? 1.0 : 0.1;
+    rho *= 1.0 + 1e-3 * kr_uniform_pm1( seed, 0, key );
+    u[ 0 ] = rho;
+    u[ 1 ] = pre / ( gamma - 1.0 );
+    u[ 2 ] = u[ 3 ] = u[ 4 ] = 0.0;
+}
+
+/* ot: face fields and the conserved state of one cell. */
+static inline double kr_ot_bx( double y_cc ) { return -sin( 2 * KR_PI * y_cc ) / sqrt( 4 * KR_PI ); }
+static inline double kr_ot_by( double x_cc ) { return  sin( 4 * KR_PI * x_cc ) / sqrt( 4 * KR_PI ); }
+static inline double kr_ot_bz( void )        { return 0.0; }
+
+/* u[0] rho, u[1] E (incl. magnetic energy of the face-averaged field),
+ * u[2..4] momentum, u[5..7] cell-centred B.  b_cc: face-averaged B of the cell. */
+static inline void kr_ot_cell( double * u, const double x_cc[ 3 ], const double b_cc[ 3 ],
+                               double gamma, uint64_t seed, uint64_t key )
+{
+    const double rho = 25.0 / ( 36.0 * KR_PI );
+    const double pre =  5.0 / ( 12.0 * KR_PI );
+    double v[ 3 ], ek = 0, em = 0;
+    v[ 0 ] = -sin( 2 * KR_PI * x_cc[ 1 ] ) + 1e-3 * kr_uniform_pm1( seed, 0, key );
+    v[ 1 ] =  sin( 2 * KR_PI * x_cc[ 0 ] ) + 1e-3 * kr_uniform_pm1( seed, 1, key );
+    v[ 2 ] =                                 1e-3 * kr_uniform_pm1( seed, 2, key );
+    for( int a = 0; a < 3; ++ a )
+    {
+        ek += v[ a ] * v[ a ];
+        em += b_cc[ a ] * b_cc[ a ];
+    }
+    u[ 0 ] = rho;
+    u[ 1 ] = pre / ( gamma - 1.0 ) + 0.5 * rho * ek + 0.5 * em;
+    for( int a = 0; a < 3; ++ a )
+    {
+        u[ 2 + a ] = rho * v[ a ];
+        u[ 5 + a ] = b_cc[ a ];
+    }
+}
+
+#endif

@@ -1,0 +1,116 @@
+"""Reader and writer for Kratos binary snapshots.
+
+Format (reference: src/io/binary/binary_io_base.cpp:101-118 save_header,
+binary_io_types.h:58-78 b_info_t, utilities/data_transfer/serialize.h):
+    char   (is_little_endian | sizeof(size_t))
+    size_t header_size
+    size_t n_entries, then per entry:
+        size_t key_len, key bytes, size_t size, char unit_size, size_t offset
+    bulk: entry data at header_size + offset
+Entries are sorted by key (std::map order) and laid out in that order.
+"""
+import struct
+from typing import Dict, Tuple
+
+import numpy as np
+
+
+class Snapshot:
+    def __init__(self):
+        self.data: Dict[str, bytes] = {}
+        self.unit: Dict[str, int] = {}
+
+    # ------------------------------------------------------------------ read
+    @classmethod
+    def read(cls, path: str) -> "Snapshot":
+        snap = cls()
+        with open(path, "rb") as f:
+            raw = f.read()
+        sst = raw[0]
+        if not (sst & 1):
+            raise ValueError("big-endian snapshots are not supported")
+        if (sst & ~1) != 8:
+            raise ValueError("snapshot written with sizeof(size_t) != 8")
+        header_size, n = struct.unpack_from("<QQ", raw, 1)
+        pos = 17
+        for _ in range(n):
+            (klen,) = struct.unpack_from("<Q", raw, pos)
+            pos += 8
+            key = raw[pos:pos + klen].decode("ascii")
+            pos += klen
+            size, usize, off = struct.unpack_from("<QbQ", raw, pos)
+            pos += 17
+            snap.data[key] = raw[header_size + off: header_size + off + size]
+            snap.unit[key] = usize
+        if pos != header_size:
+            raise ValueError("inconsistent snapshot header")
+        return snap
+
+    # ----------------------------------------------------------------- write
+    def write(self, path: str) -> None:
+        keys = sorted(self.data)
+        hdr = bytearray(struct.pack("<Q", len(keys)))
+        off = 0
+        for k in keys:
+            kb = k.encode("ascii")
+            size = len(self.data[k])
+            hdr += struct.pack("<Q", len(kb)) + kb + struct.pack("<QbQ", size, self.unit[k], off)
+            off += size
+        header_size = 1 + 8 + len(hdr)
+        with open(path, "wb") as f:
+            f.write(bytes([1 | 8]))
+            f.write(struct.pack("<Q", header_size))
+            f.write(hdr)
+            for k in keys:
+                f.write(self.data[k])
+
+    # --------------------------------------------------------------- access
+    def keys(self):
+        return self.data.keys()
+
+    def array(self, key: str, kind: str = "f") -> np.ndarray:
+        return np.frombuffer(self.data[key], dtype="<%s%d" % (kind, self.unit[key]))
+
+    def put(self, key: str, arr, unit: int = None) -> None:
+        a = np.ascontiguousarray(arr)
+        self.data[key] = a.tobytes()
+        self.unit[key] = int(unit if unit is not None else a.dtype.itemsize)
+
+    def field(self, block: int, prefix: str) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """(data[n_step?, z, y, x, n_int], n_cell, n_gh) of a dat_3d_t entry
+        such as prefix='hydro_cons_' or 'field_bf_' (dat_3d.h:117-126)."""
+        base = "block_%d|%s" % (block, prefix)
+        n_int = int(self.array(base + "n_int", "i")[0])
+        n_cell = self.array(base + "n_cell", "i").astype(int)
+        n_gh = self.array(base + "n_gh", "i").astype(int)
+        f = self.array(base + "field", "f")
+        return f.reshape(n_cell[2], n_cell[1], n_cell[0], n_int), n_cell, n_gh
+
+
+def block_ids(snap: Snapshot):
+    """Block ids present in a snapshot, sorted."""
+    ids = set()
+    for k in snap.keys():
+        if k.startswith("block_"):
+            ids.add(int(k.split("|")[0][6:]))
+    return sorted(ids)
+
+
+def to_lex_arrays(snap: Snapshot, nb):
+    """Gather the per-block conserved field (and face field, if present) of a
+    single-level snapshot into arrays in lexicographic block order (x fastest):
+    u [nblk, n2, n1, n0, n_int], bf [nblk, n2+5, n1+5, n0+5, 3] or None.
+    Block positions come from the `i_logic` entry (block.cpp:18-39)."""
+    nblk = nb[0] * nb[1] * nb[2]
+    u_out, bf_out = [None] * nblk, [None] * nblk
+    for bid in block_ids(snap):
+        il = snap.array("block_%d|i_logic" % bid, "i")
+        lex = int(il[0] + nb[0] * (il[1] + nb[1] * il[2]))
+        u, _, _ = snap.field(bid, "hydro_cons_")
+        u_out[lex] = u
+        if ("block_%d|field_bf_field" % bid) in snap.data:
+            bf, _, _ = snap.field(bid, "field_bf_")
+            bf_out[lex] = bf
+    u = np.stack(u_out)
+    bf = np.stack(bf_out) if bf_out[0] is not None else None
+    return u, bf

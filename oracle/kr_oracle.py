@@ -1,0 +1,164 @@
+"""ctypes front end of the CPU restatement of the step (test infrastructure).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module, as the checker; the product never imports it.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "ref_cpu", "libkr_oracle.so")
+
+
+class _Cfg(ctypes.Structure):
+    _fields_ = [
+        ("mhd", ctypes.c_int),
+        ("nb", ctypes.c_int * 3),
+        ("n", ctypes.c_int * 3),
+        ("x_min", ctypes.c_double * 3),
+        ("x_max", ctypes.c_double * 3),
+        ("gamma", ctypes.c_double),
+        ("cfl", ctypes.c_double),
+        ("d_floor", ctypes.c_double),
+        ("t_floor", ctypes.c_double),
+        ("dt_expand", ctypes.c_double),
+        ("n_threads", ctypes.c_int),
+    ]
+
+
+_lib = None
+
+
+def build():
+    subprocess.check_call(["make", "-s", "-f", os.path.join(_HERE, "Makefile")])
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        dp = ctypes.POINTER(ctypes.c_double)
+        L.kro_create.restype = ctypes.c_void_p
+        L.kro_create.argtypes = [ctypes.POINTER(_Cfg)]
+        L.kro_destroy.argtypes = [ctypes.c_void_p]
+        L.kro_set_state.argtypes = [ctypes.c_void_p, dp, dp]
+        L.kro_get_state.argtypes = [ctypes.c_void_p, dp, dp]
+        L.kro_step.restype = ctypes.c_int
+        L.kro_step.argtypes = [ctypes.c_void_p, ctypes.c_int, dp, dp, dp]
+        for f in ("kro_x_cc", "kro_x_fc"):
+            getattr(L, f).restype = ctypes.c_double
+            getattr(L, f).argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.kro_dx.restype = ctypes.c_double
+        L.kro_dx.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+        L.kro_hllc.argtypes = [dp, dp, ctypes.c_int, ctypes.c_double, dp]
+        L.kro_hlld.argtypes = [dp, dp, ctypes.c_int, ctypes.c_double, dp]
+        L.kro_plm.argtypes = [dp, dp, dp]
+        L.kro_init_problem.restype = ctypes.c_int
+        L.kro_init_problem.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_ulonglong]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+FLT_MAX = float(np.finfo(np.float32).max)
+
+
+class OracleMesh:
+    """Uniform periodic mesh of nb blocks of n cells, state in lexicographic
+    block order (x fastest).  u: [nblk, n2, n1, n0, nw]; bf: [nblk, n2+5,
+    n1+5, n0+5, 3] (face lattice with 2 ghost layers)."""
+
+    def __init__(self, mhd, nb, n, gamma, cfl=0.3, x_min=(0, 0, 0), x_max=(1, 1, 1),
+                 d_floor=1e-9, t_floor=1e-9, dt_expand=2.0, dt_init=0.0, n_threads=0):
+        c = _Cfg()
+        c.mhd = int(mhd)
+        for a in range(3):
+            c.nb[a], c.n[a] = int(nb[a]), int(n[a])
+            c.x_min[a], c.x_max[a] = float(x_min[a]), float(x_max[a])
+        c.gamma, c.cfl, c.d_floor, c.t_floor = float(gamma), float(cfl), float(d_floor), float(t_floor)
+        c.dt_expand, c.n_threads = float(dt_expand), int(n_threads)
+        self.cfg = c
+        self.mhd = bool(mhd)
+        self.nb, self.n = tuple(nb), tuple(n)
+        self.nblk = nb[0] * nb[1] * nb[2]
+        self.nw = 8 if mhd else 5
+        self._h = lib().kro_create(ctypes.byref(c))
+        self.t = 0.0
+        # cycle.cpp:163-166: an unset dt_init starts the device dt at FLT_MAX / 10
+        self.dt_bound = dt_init if dt_init >= np.finfo(np.float32).tiny else FLT_MAX / 10
+        self.dt_last = 0.0
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().kro_destroy(self._h)
+            self._h = None
+
+    @property
+    def u_shape(self):
+        n = self.n
+        return (self.nblk, n[2], n[1], n[0], self.nw)
+
+    @property
+    def bf_shape(self):
+        n = self.n
+        return (self.nblk, n[2] + 5, n[1] + 5, n[0] + 5, 3)
+
+    def set_state(self, u, bf=None):
+        u = np.ascontiguousarray(u, dtype=np.float64).reshape(self.u_shape)
+        if self.mhd:
+            bf = np.ascontiguousarray(bf, dtype=np.float64).reshape(self.bf_shape)
+            lib().kro_set_state(self._h, _p(u), _p(bf))
+        else:
+            lib().kro_set_state(self._h, _p(u), None)
+
+    def get_state(self):
+        u = np.empty(self.u_shape)
+        if self.mhd:
+            bf = np.empty(self.bf_shape)
+            lib().kro_get_state(self._h, _p(u), _p(bf))
+            return u, bf
+        lib().kro_get_state(self._h, _p(u), None)
+        return u, None
+
+    def step(self, n_steps=1):
+        t = ctypes.c_double(self.t)
+        db = ctypes.c_double(self.dt_bound)
+        dl = ctypes.c_double(0.0)
+        rc = lib().kro_step(self._h, int(n_steps), ctypes.byref(t), ctypes.byref(db), ctypes.byref(dl))
+        if rc != 0:
+            raise FloatingPointError("oracle step produced a non-finite dt")
+        self.t, self.dt_bound, self.dt_last = t.value, db.value, dl.value
+
+    def init_problem(self, name, seed):
+        if lib().kro_init_problem(self._h, name.encode(), int(seed)) != 0:
+            raise ValueError("unknown problem %r for this mesh" % name)
+
+    def x_cc(self, block, axis, i):
+        return lib().kro_x_cc(self._h, block, axis, i)
+
+    def dx(self, block, axis):
+        return lib().kro_dx(self._h, block, axis)
+
+
+def hllc(ql, qr, axis, gamma):
+    ql = np.ascontiguousarray(ql, dtype=np.float64)
+    qr = np.ascontiguousarray(qr, dtype=np.float64)
+    f = np.empty(5)
+    lib().kro_hllc(_p(ql), _p(qr), int(axis), float(gamma), _p(f))
+    return f
+
+
+def hlld(ql, qr, axis, gamma):
+    ql = np.ascontiguousarray(ql, dtype=np.float64)
+    qr = np.ascontiguousarray(qr, dtype=np.float64)
+    f = np.empty(8)
+    lib().kro_hlld(_p(ql), _p(qr), int(axis), float(gamma), _p(f))
+    return f

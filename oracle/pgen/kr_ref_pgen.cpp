@@ -1,0 +1,125 @@
+// Problem generator compiled together with the original Kratos sources (test
+// infrastructure, built by oracle/Makefile.ref into oracle/_ref/).
+//
+// It enrols the reference's own dynamics modules (dynamics::hydro_t with its
+// default PLM + HLLC + RK2 policies, dynamics::mhd_t with PLM + HLLD + CT + RK2)
+// exactly as a user pgen does (usr_example/bow_shock/usr.cpp:20-40 of the
+// reference) and overrides only init_cond, so that the reference integrates the
+// same seeded initial states as this package (kratos_b200/csrc/problems.h).
+//
+// [problem] name = shock | ot ; [problem] seed = <int>
+#include <iostream>
+
+#include "device/general.h"
+#include "mesh/mesh_enroll.h"
+#include "utilities/mapping/loop.h"
+#include "user/probgen.h"
+#include "modules/dynamics/hydro/hydro.h"
+#include "modules/dynamics/mhd/mhd.h"
+
+#include "../../kratos_b200/csrc/problems.h"
+
+namespace
+{
+int          g_seed = 1;
+int          g_nglob[ 3 ] = { 1, 1, 1 };
+
+uint64_t cell_key( const mesh::block_t & b, const type::idx_t & i )
+{
+    int ig[ 3 ];
+    for( int a = 0; a < 3; ++ a )
+        ig[ a ] = b.reg[ a ] * b.geo.n_ceff[ a ] + i[ a ];
+    return kr_cell_key( b.reg.level, ig, g_nglob );
+}
+}   // namespace
+
+struct shock_hydro_t : dynamics::hydro_t
+{
+    // hydro_t::enroll_default enrols the block data and boundary keeper only;
+    // the default policy set (PLM + HLLC + RK2) is enrolled here, as a hydro
+    // pgen does.
+    void enroll_default(  ) override
+    {
+        dynamics::hydro_t::enroll_default(  );
+        if( ! integrate )
+            enroll<  >(  );
+    }
+    void init_cond( mesh::block::dual_t & d ) override
+    {
+        auto & b_h = dynamic_cast< dynamics::hydro::block_data_t & >( d.h(  ) );
+        const auto & blk = d.b_w.get(  );
+        const auto & geo = blk.geo;
+        for( auto i : utils::loop( geo.n_ceff ) )
+        {
+            auto * u = b_h.hyd.u.at( i );
+            double uu[ 5 ];
+            kr_shock_cell( uu, geo.x_cc( 0, i[ 0 ] ), p_eos->gamma,
+                                 g_seed, cell_key( blk, i ) );
+            for( int n = 0; n < 5; ++ n )
+                u[ n ] = uu[ n ];
+        }
+    }
+};
+
+struct ot_mhd_t : dynamics::mhd_t
+{
+    void init_cond( mesh::block::dual_t & d ) override
+    {
+        auto & b_h = dynamic_cast< dynamics::mhd::block_data_t & >( d.h(  ) );
+        const auto & blk = d.b_w.get(  );
+        const auto & geo = blk.geo;
+        auto n_face = geo.n_ceff;
+        for( auto & n_s : n_face.x )
+            n_s += ( n_s > 1 );
+        for( auto i : utils::loop( n_face ) )
+        {
+            auto * bf = b_h.fld.bf.at( i );
+            bf[ 0 ] = kr_ot_bx( geo.x_cc( 1, i[ 1 ] ) );
+            bf[ 1 ] = kr_ot_by( geo.x_cc( 0, i[ 0 ] ) );
+            bf[ 2 ] = kr_ot_bz(  );
+        }
+        for( auto i : utils::loop( geo.n_ceff ) )
+        {
+            double x[ 3 ], bc[ 3 ];
+            for( int a = 0; a < 3; ++ a )
+            {
+                x[ a ] = geo.x_cc( a, i[ a ] );
+                auto j = i;
+                ++ j[ a ];
+                bc[ a ] = ( b_h.fld.bf.at( i )[ a ] + b_h.fld.bf.at( j )[ a ] ) / 2;
+            }
+            double uu[ 8 ];
+            kr_ot_cell( uu, x, bc, p_eos->gamma, g_seed, cell_key( blk, i ) );
+            auto * u = b_h.hyd.u.at( i );
+            for( int n = 0; n < 8; ++ n )
+                u[ n ] = uu[ n ];
+        }
+    }
+};
+
+namespace prob
+{
+void run( int argc, char * argv[  ] )
+{
+    mesh::mesh_t mesh;
+    mesh.enroll_device< device_t >(  );
+    mesh.enroll_comm< comm::base_t >(  );
+    input args;
+    args.set_comm( mesh.p_com );
+    cmd( argc, argv, args );
+    const auto name = args.get< std::string >( "problem", "name" );
+    g_seed          = args.get< int >( "problem", "seed", 1 );
+    const auto ng   = args.get< type::idx_t >( "mesh", "n_cell_global" );
+    for( int a = 0; a < 3; ++ a )
+        g_nglob[ a ] = ng[ a ];
+
+    if( name == "shock" )
+        mesh.enroll_module< shock_hydro_t >(  );
+    else if( name == "ot" )
+        mesh.enroll_module< ot_mhd_t >(  );
+    else
+        throw std::runtime_error( "unknown [problem] name " + name );
+    mesh.init( args );
+    return mesh.evolve(  );
+}
+};  // namespace prob

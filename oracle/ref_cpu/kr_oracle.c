@@ -1,0 +1,1163 @@
+/* CPU restatement (FP64) of the Kratos hydro / ideal-MHD step.  TEST
+ * INFRASTRUCTURE ONLY -- see kr_oracle.h for scope, layout and conventions.
+ * Build: oracle/Makefile (gcc, no fused multiply-add). */
+#include "kr_oracle.h"
+#include "../../kratos_b200/csrc/problems.h"
+
+#include <float.h>
+#include <math.h>
+#include <pthread.h>
+#include <stdlib.h>
+#include <string.h>
+#include <unistd.h>
+
+enum { RHO = 0, ENE = 1, MOM = 2, BCC = 5 };       /* dynamics/indices.h:5-13 */
+
+struct kro_mesh
+{
+    kro_cfg c;
+    int     nw, nblk;
+    long    ncell;                       /* interior cells per block        */
+    int     gw[ 3 ];                     /* w extents with 2 ghosts         */
+    long    nw_cells;
+    int     gb[ 3 ];                     /* bf lattice extents (n+1+4)      */
+    long    nbf;
+    int     gf[ 3 ][ 3 ];                /* flux extents per axis, 1 ghost  */
+    long    nf[ 3 ];
+    int     ge[ 3 ];                     /* edge lattice extents (n+1+2)    */
+    long    nee;
+    /* per block geometry (meshgen.cpp:286-363) */
+    double *xf0, *dx0, *sfc0, *vol0;     /* [nblk*3], [nblk*3], [nblk*3], [nblk] */
+    double *u[ 2 ], *bf[ 2 ], *w, *f[ 3 ], *ee;
+    double *dtc;                         /* per block CFL minimum           */
+};
+
+/* ------------------------------------------------------------------ */
+/* indexing                                                             */
+
+static inline long iw( const kro_mesh * m, int i0, int i1, int i2 )
+{
+    return ( ( i0 + 2 ) + m->gw[ 0 ] * ( ( long )( i1 + 2 ) + m->gw[ 1 ] * ( long )( i2 + 2 ) ) )
+           * m->nw;
+}
+static inline long iu( const kro_mesh * m, int i0, int i1, int i2 )
+{
+    return ( i0 + m->c.n[ 0 ] * ( ( long ) i1 + m->c.n[ 1 ] * ( long ) i2 ) ) * m->nw;
+}
+static inline long ib( const kro_mesh * m, int i0, int i1, int i2 )
+{
+    return ( ( i0 + 2 ) + m->gb[ 0 ] * ( ( long )( i1 + 2 ) + m->gb[ 1 ] * ( long )( i2 + 2 ) ) ) * 3;
+}
+static inline long ifl( const kro_mesh * m, int a, int i0, int i1, int i2 )
+{
+    const int * g = m->gf[ a ];
+    return ( ( i0 + 1 ) + g[ 0 ] * ( ( long )( i1 + 1 ) + g[ 1 ] * ( long )( i2 + 1 ) ) ) * m->nw;
+}
+static inline long ie( const kro_mesh * m, int i0, int i1, int i2 )
+{
+    return ( ( i0 + 1 ) + m->ge[ 0 ] * ( ( long )( i1 + 1 ) + m->ge[ 1 ] * ( long )( i2 + 1 ) ) ) * 3;
+}
+static inline int mod3( int a ) { return a < 3 ? a : a - 3; }
+
+/* utilities/functions.h:51-64 (PRECISION == 2) */
+static inline double dmax( double a, double b ) { return a > b ? a : b; }
+static inline double dmin( double a, double b ) { return a < b ? a : b; }
+static inline double uabs( double a ) { return a > 0 ? a : -a; }   /* functions.h:32-36 */
+static inline int    sgn ( double a ) { return a > 0 ? 1 : ( a < 0 ? -1 : 0 ); }
+
+/* utilities/mapping/mapping.h idx_swap: cyclic rotation of a 3-vector */
+static inline void idx_swap( double * x, int axis )
+{
+    if( mod3( axis ) != 0 )
+    {
+        double s[ 3 ];
+        for( int i = 0; i < 3; ++ i )
+            s[ i ] = x[ mod3( i + axis ) ];
+        for( int i = 0; i < 3; ++ i )
+            x[ i ] = s[ i ];
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* thread helper: run fn(m, b, aux) for every block                      */
+
+typedef void ( * blk_fn )( kro_mesh *, int, void * );
+typedef struct { kro_mesh * m; blk_fn fn; void * aux; int next; pthread_mutex_t mx; } pf_t;
+
+static void * pf_worker( void * p )
+{
+    pf_t * pf = ( pf_t * ) p;
+    for( ;; )
+    {
+        pthread_mutex_lock( & pf->mx );
+        const int b = pf->next ++;
+        pthread_mutex_unlock( & pf->mx );
+        if( b >= pf->m->nblk )
+            break;
+        pf->fn( pf->m, b, pf->aux );
+    }
+    return NULL;
+}
+
+static void par_blocks( kro_mesh * m, blk_fn fn, void * aux )
+{
+    int nt = m->c.n_threads > 0 ? m->c.n_threads : ( int ) sysconf( _SC_NPROCESSORS_ONLN );
+    if( nt > m->nblk ) nt = m->nblk;
+    if( nt <= 1 )
+    {
+        for( int b = 0; b < m->nblk; ++ b )
+            fn( m, b, aux );
+        return;
+    }
+    pf_t pf = { m, fn, aux, 0 };
+    pthread_mutex_init( & pf.mx, NULL );
+    pthread_t th[ 256 ];
+    if( nt > 256 ) nt = 256;
+    for( int t = 0; t < nt; ++ t )
+        pthread_create( & th[ t ], NULL, pf_worker, & pf );
+    for( int t = 0; t < nt; ++ t )
+        pthread_join( th[ t ], NULL );
+    pthread_mutex_destroy( & pf.mx );
+}
+
+/* ------------------------------------------------------------------ */
+/* geometry (mesh/meshgen/meshgen.cpp:252-363, geometry/geometry.h:73-150) */
+
+static void set_geometry( kro_mesh * m )
+{
+    for( int b = 0; b < m->nblk; ++ b )
+    {
+        int reg[ 3 ] = { b % m->c.nb[ 0 ], ( b / m->c.nb[ 0 ] ) % m->c.nb[ 1 ],
+                         b / ( m->c.nb[ 0 ] * m->c.nb[ 1 ] ) };
+        for( int a = 0; a < 3; ++ a )
+        {
+            /* loc(i) = location( ( reg + i / n ) / ( i_logic_lim << level ) ) */
+            const double lim = ( double ) m->c.nb[ a ];
+            const double x0 = ( reg[ a ] + 0.0 / m->c.n[ a ] ) / lim;
+            const double x1 = ( reg[ a ] + 1.0 / m->c.n[ a ] ) / lim;
+            const double l0 = m->c.x_min[ a ] + x0 * ( m->c.x_max[ a ] - m->c.x_min[ a ] );
+            const double l1 = m->c.x_min[ a ] + x1 * ( m->c.x_max[ a ] - m->c.x_min[ a ] );
+            m->xf0[ b * 3 + a ] = l0;
+            m->dx0[ b * 3 + a ] = l1 - l0;
+        }
+        /* surface(): res = 1; res *= dx_f( (a+1)%3 ); res *= dx_f( (a+2)%3 ) */
+        double vol = 1.;
+        for( int a = 0; a < 3; ++ a )
+        {
+            double s = 1.;
+            s *= m->dx0[ b * 3 + ( a + 1 ) % 3 ];
+            s *= m->dx0[ b * 3 + ( a + 2 ) % 3 ];
+            m->sfc0[ b * 3 + a ] = s;
+            vol *= m->dx0[ b * 3 + a ];
+        }
+        m->vol0[ b ] = vol;
+    }
+}
+
+double kro_x_cc( const kro_mesh * m, int b, int a, int i )
+{
+    return m->xf0[ b * 3 + a ] + ( i + 0.5f ) * m->dx0[ b * 3 + a ];   /* geometry.h:73-79 */
+}
+double kro_x_fc( const kro_mesh * m, int b, int a, int i )
+{
+    return m->xf0[ b * 3 + a ] + i * m->dx0[ b * 3 + a ];              /* geometry.h:80-95 */
+}
+double kro_dx( const kro_mesh * m, int b, int a ) { return m->dx0[ b * 3 + a ]; }
+
+/* ------------------------------------------------------------------ */
+/* create / destroy / state                                             */
+
+kro_mesh * kro_create( const kro_cfg * cfg )
+{
+    kro_mesh * m = ( kro_mesh * ) calloc( 1, sizeof( kro_mesh ) );
+    m->c    = * cfg;
+    m->nw   = cfg->mhd ? 8 : 5;
+    m->nblk = cfg->nb[ 0 ] * cfg->nb[ 1 ] * cfg->nb[ 2 ];
+    m->ncell = ( long ) cfg->n[ 0 ] * cfg->n[ 1 ] * cfg->n[ 2 ];
+    m->nw_cells = 1; m->nbf = 3; m->nee = 3;
+    for( int a = 0; a < 3; ++ a )
+    {
+        m->gw[ a ] = cfg->n[ a ] + 4;
+        m->gb[ a ] = cfg->n[ a ] + 5;
+        m->ge[ a ] = cfg->n[ a ] + 3;
+        m->nw_cells *= m->gw[ a ];
+        m->nbf *= m->gb[ a ];
+        m->nee *= m->ge[ a ];
+    }
+    for( int a = 0; a < 3; ++ a )
+    {
+        m->nf[ a ] = m->nw;
+        for( int d = 0; d < 3; ++ d )
+        {
+            m->gf[ a ][ d ] = cfg->n[ d ] + ( d == a ) + 2;
+            m->nf[ a ] *= m->gf[ a ][ d ];
+        }
+    }
+    m->xf0  = ( double * ) calloc( m->nblk * 3, sizeof( double ) );
+    m->dx0  = ( double * ) calloc( m->nblk * 3, sizeof( double ) );
+    m->sfc0 = ( double * ) calloc( m->nblk * 3, sizeof( double ) );
+    m->vol0 = ( double * ) calloc( m->nblk, sizeof( double ) );
+    m->dtc  = ( double * ) calloc( m->nblk, sizeof( double ) );
+    for( int s = 0; s < 2; ++ s )
+    {
+        m->u [ s ] = ( double * ) calloc( ( size_t ) m->nblk * m->ncell * m->nw, sizeof( double ) );
+        m->bf[ s ] = ( double * ) calloc( ( size_t ) m->nblk * m->nbf, sizeof( double ) );
+    }
+    m->w = ( double * ) calloc( ( size_t ) m->nblk * m->nw_cells * m->nw, sizeof( double ) );
+    for( int a = 0; a < 3; ++ a )
+        m->f[ a ] = ( double * ) calloc( ( size_t ) m->nblk * m->nf[ a ], sizeof( double ) );
+    m->ee = ( double * ) calloc( ( size_t ) m->nblk * m->nee, sizeof( double ) );
+    set_geometry( m );
+    return m;
+}
+
+void kro_destroy( kro_mesh * m )
+{
+    if( ! m ) return;
+    free( m->xf0 ); free( m->dx0 ); free( m->sfc0 ); free( m->vol0 ); free( m->dtc );
+    for( int s = 0; s < 2; ++ s ) { free( m->u[ s ] ); free( m->bf[ s ] ); }
+    free( m->w );
+    for( int a = 0; a < 3; ++ a ) free( m->f[ a ] );
+    free( m->ee );
+    free( m );
+}
+
+int  kro_nw   ( const kro_mesh * m ) { return m->nw; }
+long kro_ncell( const kro_mesh * m ) { return m->ncell; }
+long kro_nface( const kro_mesh * m ) { return m->nbf / 3; }
+
+void kro_set_state( kro_mesh * m, const double * u, const double * bf )
+{
+    memcpy( m->u[ 0 ], u, sizeof( double ) * m->nblk * m->ncell * m->nw );
+    if( m->c.mhd && bf )
+        memcpy( m->bf[ 0 ], bf, sizeof( double ) * m->nblk * m->nbf );
+}
+void kro_get_state( const kro_mesh * m, double * u, double * bf )
+{
+    memcpy( u, m->u[ 0 ], sizeof( double ) * m->nblk * m->ncell * m->nw );
+    if( m->c.mhd && bf )
+        memcpy( bf, m->bf[ 0 ], sizeof( double ) * m->nblk * m->nbf );
+}
+
+/* ------------------------------------------------------------------ */
+/* EOS                                                                  */
+
+/* hydro/eos/adiabatic.h:62-76 et_cs: total energy and sound speed of a
+ * primitive state; returns cv_kb = 1 / ( gamma - 1 ). */
+static inline double et_cs( double gamma, double * e_tot, double * c_s, const double * w )
+{
+    const double pre = w[ ENE ], rho = w[ RHO ];
+    const double cv_kb = 1 / ( gamma - 1 );
+    double v2 = 0;
+    for( int a = 0; a < 3; ++ a )
+        v2 += w[ MOM + a ] * w[ MOM + a ];
+    * e_tot = pre * cv_kb + rho * v2 / 2;
+    * c_s   = sqrt( gamma * dmax( pre / rho, 0 ) );
+    return cv_kb;
+}
+
+/* hydro/eos/adiabatic.h:159-206 c2p (+ pre_cs2 77-85).  cons: the cell's
+ * conserved state (floor corrections are written back); prim: output.
+ * Returns the squared sound speed. */
+static double c2p( const kro_mesh * m, double * prim, double * cons )
+{
+    const double gamma = m->c.gamma;
+    double rho = cons[ RHO ];
+    if( isnan( rho ) || rho < m->c.d_floor )
+    {
+        rho = m->c.d_floor;
+        cons[ RHO ] = m->c.d_floor;
+    }
+    prim[ RHO ] = rho;
+    const double rho_inv = 1 / rho;
+    double e_k = 0.;
+    for( int n = MOM; n < MOM + 3; ++ n )
+    {
+        prim[ n ] = rho_inv * cons[ n ];
+        e_k += cons[ n ] * cons[ n ];
+    }
+    e_k *= rho_inv / 2;
+    const double e_g = cons[ ENE ] - e_k;
+    const double cv_kb = 1 / ( gamma - 1 );
+    prim[ ENE ] = e_g / cv_kb;
+    double cs2 = gamma * prim[ ENE ] / prim[ RHO ];
+    double pre = prim[ ENE ];
+    const double pre_floor = m->c.t_floor * prim[ RHO ];
+    if( isnan( pre ) || pre < pre_floor )
+    {
+        pre = pre_floor;
+        prim[ ENE ] = pre;
+        cons[ ENE ] = e_k + pre / ( gamma - 1 );
+        cs2 = gamma * pre / rho;
+    }
+    return cs2;
+}
+
+/* mhd/eos/adiabatic.h:84-98 fast magnetosonic speed along axis */
+static inline double c_fms( const double * w, const double * b_2, double gam, int axis )
+{
+    const double rho  = w[ RHO ];
+    const double cs_2 = w[ ENE ] * gam / rho;
+    const double v_ax2 = b_2[ axis ] / rho;
+    const double v_t2 = ( b_2[ mod3( axis + 1 ) ] + b_2[ mod3( axis + 2 ) ] ) / rho;
+    const double q_2 = v_ax2 + v_t2 + cs_2;
+    const double r_2 = v_ax2 + v_t2 - cs_2;
+    return sqrt( 0.5f * ( q_2 + sqrt( r_2 * r_2 + 4 * cs_2 * v_t2 ) ) );
+}
+
+/* Per-block cons -> prim over the interior, from RK slot `step`.
+ * hydro: hydro/eos/adiabatic.h:211-258; MHD: mhd/eos/adiabatic.h:127-234.
+ * Stage 0 also takes the per-cell CFL dt (adiabatic.h:146-157 /
+ * mhd/eos/adiabatic.h:105-122) into m->dtc[b]. */
+typedef struct { int step; } c2p_arg;
+
+static void c2p_block( kro_mesh * m, int b, void * aux )
+{
+    const int step = ( ( c2p_arg * ) aux )->step;
+    const int nw = m->nw;
+    const int * n = m->c.n;
+    double * u  = m->u[ step ] + ( size_t ) b * m->ncell * nw;
+    double * bf = m->c.mhd ? m->bf[ step ] + ( size_t ) b * m->nbf : NULL;
+    double * w  = m->w + ( size_t ) b * m->nw_cells * nw;
+    const double * dx = m->dx0 + b * 3;
+    double dt_min = FLT_MAX;
+    for( int i2 = 0; i2 < n[ 2 ]; ++ i2 )
+    for( int i1 = 0; i1 < n[ 1 ]; ++ i1 )
+    for( int i0 = 0; i0 < n[ 0 ]; ++ i0 )
+    {
+        double * c = u + iu( m, i0, i1, i2 );
+        double * p = w + iw( m, i0, i1, i2 );
+        double prim[ 8 ], cons[ 8 ];
+        double dt = FLT_MAX;
+        if( ! m->c.mhd )
+        {
+            for( int k = 0; k < 5; ++ k ) cons[ k ] = c[ k ];
+            const double cs2 = c2p( m, prim, cons );
+            c[ RHO ] = cons[ RHO ];
+            c[ ENE ] = cons[ ENE ];
+            for( int k = 0; k < 5; ++ k ) p[ k ] = prim[ k ];
+            if( step == 0 )
+            {
+                const double cs = sqrt( cs2 );
+                for( int a = 0; a < 3; ++ a )
+                    dt = dmin( dt, dx[ a ] / ( cs + fabs( prim[ MOM + a ] ) ) );
+                dt = dt * m->c.cfl;
+            }
+        }
+        else
+        {
+            const int ii[ 3 ] = { i0, i1, i2 };
+            double bc[ 3 ], bc_2[ 3 ], b_max[ 3 ];
+            double e_m = 0;
+            for( int a = 0; a < 3; ++ a )
+            {
+                int jj[ 3 ] = { ii[ 0 ], ii[ 1 ], ii[ 2 ] };
+                const double b_l = bf[ ib( m, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) + a ];
+                ++ jj[ a ];
+                const double b_r = bf[ ib( m, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) + a ];
+                const double bc_m = ( b_l + b_r ) / 2;
+                bc[ a ] = bc_m;
+                const double bcs2 = bc_m * bc_m;
+                e_m += bcs2;
+                bc_2 [ a ] = bcs2;
+                b_max[ a ] = dmax( fabs( b_l ), fabs( b_r ) );
+            }
+            e_m /= 2;
+            c[ ENE ] -= e_m;
+            for( int k = 0; k < 8; ++ k ) cons[ k ] = c[ k ];
+            ( void ) c2p( m, prim, cons );
+            c[ RHO ] = cons[ RHO ];
+            c[ ENE ] = cons[ ENE ];
+            c[ ENE ] += e_m;
+            for( int k = 0; k < 5; ++ k ) p[ k ] = prim[ k ];
+            for( int a = 0; a < 3; ++ a )
+            {
+                p[ BCC + a ] = bc[ a ];
+                c[ BCC + a ] = bc[ a ];
+            }
+            if( step == 0 )
+            {
+                double bm_2[ 3 ] = { bc_2[ 0 ], bc_2[ 1 ], bc_2[ 2 ] };
+                for( int a = 0; a < 3; ++ a )
+                {
+                    bm_2[ a ] = b_max[ a ] * b_max[ a ];
+                    const double cf = c_fms( prim, bm_2, m->c.gamma, a );
+                    dt = dmin( dt, dx[ a ] / ( cf + fabs( prim[ MOM + a ] ) ) );
+                    bm_2[ a ] = bc_2[ a ];
+                }
+                dt = dt * m->c.cfl;
+            }
+        }
+        if( step == 0 )
+            dt_min = dmin( dt_min, dt );
+    }
+    m->dtc[ b ] = dt_min;
+}
+
+/* ------------------------------------------------------------------ */
+/* ghost fill (same level, periodic): every ghost cell of w and every  */
+/* non-owned face slot of bf takes the value of the block that owns it */
+/* (hydro/boundary/comm_functions.h:306-327, 456-483; MHD              */
+/* mhd/boundary/comm_functions.h:433-465, 786-815).                   */
+
+static inline int wrap( int i, int n, int * shift )
+{
+    if( i < 0 )       { * shift = -1; return i + n; }
+    if( i >= n )      { * shift = +1; return i - n; }
+    * shift = 0; return i;
+}
+
+static inline int nbr_block( const kro_mesh * m, int b, const int sh[ 3 ] )
+{
+    int reg[ 3 ] = { b % m->c.nb[ 0 ], ( b / m->c.nb[ 0 ] ) % m->c.nb[ 1 ],
+                     b / ( m->c.nb[ 0 ] * m->c.nb[ 1 ] ) };
+    for( int a = 0; a < 3; ++ a )
+        reg[ a ] = ( reg[ a ] + sh[ a ] + m->c.nb[ a ] ) % m->c.nb[ a ];
+    return reg[ 0 ] + m->c.nb[ 0 ] * ( reg[ 1 ] + m->c.nb[ 1 ] * reg[ 2 ] );
+}
+
+typedef struct { int step; } ghost_arg;
+
+static void ghost_block( kro_mesh * m, int b, void * aux )
+{
+    const int step = ( ( ghost_arg * ) aux )->step;
+    const int nw = m->nw;
+    const int * n = m->c.n;
+    double * w = m->w + ( size_t ) b * m->nw_cells * nw;
+    for( int i2 = -2; i2 < n[ 2 ] + 2; ++ i2 )
+    for( int i1 = -2; i1 < n[ 1 ] + 2; ++ i1 )
+    for( int i0 = -2; i0 < n[ 0 ] + 2; ++ i0 )
+    {
+        int sh[ 3 ], j[ 3 ];
+        j[ 0 ] = wrap( i0, n[ 0 ], & sh[ 0 ] );
+        j[ 1 ] = wrap( i1, n[ 1 ], & sh[ 1 ] );
+        j[ 2 ] = wrap( i2, n[ 2 ], & sh[ 2 ] );
+        if( ! sh[ 0 ] && ! sh[ 1 ] && ! sh[ 2 ] )
+            continue;
+        const int s = nbr_block( m, b, sh );
+        const double * src = m->w + ( size_t ) s * m->nw_cells * nw + iw( m, j[ 0 ], j[ 1 ], j[ 2 ] );
+        memcpy( w + iw( m, i0, i1, i2 ), src, sizeof( double ) * nw );
+    }
+    if( ! m->c.mhd )
+        return;
+    double * bf = m->bf[ step ] + ( size_t ) b * m->nbf;
+    for( int c = 0; c < 3; ++ c )
+    for( int i2 = -2; i2 <= n[ 2 ] + 2; ++ i2 )
+    for( int i1 = -2; i1 <= n[ 1 ] + 2; ++ i1 )
+    for( int i0 = -2; i0 <= n[ 0 ] + 2; ++ i0 )
+    {
+        const int ii[ 3 ] = { i0, i1, i2 };
+        int own = 1, sh[ 3 ], j[ 3 ];
+        for( int a = 0; a < 3; ++ a )
+        {
+            const int hi = ( a == c ) ? n[ a ] : n[ a ] - 1;
+            own &= ii[ a ] >= 0 && ii[ a ] <= hi;
+        }
+        if( own )
+            continue;
+        int ok = 1;
+        for( int a = 0; a < 3; ++ a )
+        {
+            if( a == c )
+            {   /* face index: owned 0..n; wrap outside that range */
+                if( ii[ a ] < 0 )          { sh[ a ] = -1; j[ a ] = ii[ a ] + n[ a ]; }
+                else if( ii[ a ] > n[ a ] ) { sh[ a ] = +1; j[ a ] = ii[ a ] - n[ a ]; }
+                else                        { sh[ a ] = 0;  j[ a ] = ii[ a ]; }
+            }
+            else
+                j[ a ] = wrap( ii[ a ], n[ a ], & sh[ a ] );
+            ok &= j[ a ] >= -2 && j[ a ] <= n[ a ] + 2;
+        }
+        if( ! ok )
+            continue;
+        const int s = nbr_block( m, b, sh );
+        bf[ ib( m, i0, i1, i2 ) + c ]
+            = m->bf[ step ][ ( size_t ) s * m->nbf + ib( m, j[ 0 ], j[ 1 ], j[ 2 ] ) + c ];
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* PLM (hydro/reconstruct/plm.h:116-153, uniform mesh, FP64: norm = 1)  */
+
+static inline void plm_face( double q_ll, double q_l, double q_r, double q_rr,
+                             double * ql, double * qr )
+{
+    const double norm = 1;
+    const double dql = ( q_l  - q_ll );
+    const double dqc = ( q_r  - q_l  );
+    const double dqr = ( q_rr - q_r  );
+    const double dqr2  = norm * dqr * dqr;
+    const double dql2  = norm * dql * dql;
+    const double dqc2  = norm * dqc * dqc;
+    const double dq2_l = norm * dql * dqc;
+    const double dq2_r = norm * dqr * dqc;
+    const double ql_coef = dq2_l <= 0 ? 0 :  dq2_l / ( dql2 + dqc2 + dq2_l * 2 );
+    const double qr_coef = dq2_r <= 0 ? 0 : -dq2_r / ( dqr2 + dqc2 + dq2_r * 2 );
+    * ql = q_l + ( dq2_l <= 0 ? 0 : ql_coef * ( dql + dqc ) );
+    * qr = q_r + ( dq2_r <= 0 ? 0 : qr_coef * ( dqc + dqr ) );
+}
+
+void kro_plm( const double * q4, double * ql, double * qr )
+{
+    plm_face( q4[ 0 ], q4[ 1 ], q4[ 2 ], q4[ 3 ], ql, qr );
+}
+
+/* ------------------------------------------------------------------ */
+/* HLLC (hydro/riemann/hllc.h:239-250 f_lr_hyd, 262-379 eval), on the   */
+/* rotated states; wli / wri are overwritten (the reference reuses them */
+/* as flux scratch).                                                    */
+
+static inline void f_lr_hyd( double * f, const double * w, double v, double e )
+{
+    const double rho = w[ RHO ];
+    const double pre = w[ ENE ];
+    f[ RHO ] = rho * v;
+    f[ ENE ] = pre * w[ MOM ] + e * v;
+    for( int a = MOM; a < MOM + 3; ++ a )
+        f[ a ] = rho * w[ a ] * v;
+    f[ MOM ] += pre;
+}
+
+static void hllc_eval( double * flx, double * wli, double * wri, double gamma )
+{
+    double * fl = wli, * fr = wri, * wroe = flx;
+    double el, er, cl, cr;
+    const double gm1i_l = et_cs( gamma, & el, & cl, wli );
+    const double gm1i_r = et_cs( gamma, & er, & cr, wri );
+
+    const double sqrtdl  = sqrt( wli[ RHO ] );
+    const double sqrtdr  = sqrt( wri[ RHO ] );
+    const double isdlpdr = ( double ) 1 / ( sqrtdl + sqrtdr );
+    wroe[ RHO ] = sqrtdl * sqrtdr;
+    for( int n = MOM; n < MOM + 3; ++ n )
+        wroe[ n ] = ( sqrtdl * wli[ n ] + sqrtdr * wri[ n ] ) * isdlpdr;
+    const double hroe = isdlpdr *
+        ( ( el + wli[ ENE ] ) / sqrtdl + ( er + wri[ ENE ] ) / sqrtdr );
+    const double gam1_roe = ( double ) 1 /
+        ( isdlpdr * ( sqrtdl * gm1i_l + sqrtdr * gm1i_r ) );
+
+    const double v2roe = wroe[ MOM ] * wroe[ MOM ] + wroe[ MOM + 1 ] * wroe[ MOM + 1 ]
+                       + wroe[ MOM + 2 ] * wroe[ MOM + 2 ];
+    const double q = hroe - 0.5f * v2roe;
+    const double a = ( q <= 0 ) ? 0 : sqrt( gam1_roe * q );
+
+    const double al = dmin( wroe[ MOM ] - a, wli[ MOM ] - cl );
+    const double ar = dmax( wroe[ MOM ] + a, wri[ MOM ] + cr );
+    const double bp = ar > 0 ? ar : 0;
+    const double bm = al < 0 ? al : 0;
+
+    const double vxl = wli[ MOM ] - al;
+    const double vxr = wri[ MOM ] - ar;
+    const double tl  = wli[ ENE ] + vxl * wli[ RHO ] * wli[ MOM ];
+    const double tr  = wri[ ENE ] + vxr * wri[ RHO ] * wri[ MOM ];
+    const double ml  =  wli[ RHO ] * vxl;
+    const double mr  = -wri[ RHO ] * vxr;
+
+    double cp, am;
+    const double f_max = FLT_MAX / 1e1f;     /* float constants, as hllc.h:326-327 */
+    const double f_min = FLT_MIN * 1e1f;
+    if( fabs( ml + mr ) < f_min )
+    {
+        cp = 0;
+        am = 0;
+    }
+    else if( ( tr != 0 && fabs( ml ) > f_max / fabs( tr ) ) ||
+             ( tl != 0 && fabs( mr ) > f_max / fabs( tl ) ) )
+    {
+        const double mli = sgn( ml ) / dmax( fabs( ml ), f_min );
+        const double mri = sgn( mr ) / dmax( fabs( mr ), f_min );
+        am = ( tl - tr ) / ( ml + mr );
+        cp = dmax( ( mri * tr + mli * tl ) / ( mli + mri ), ( double ) 0 );
+    }
+    else
+    {
+        am = ( tl - tr ) / ( ml + mr );
+        cp = dmax( ( ml * tr + mr * tl ) / ( ml + mr ), ( double ) 0 );
+    }
+
+    const double d_am_bm = dmax( fabs( am - bm ), f_min ) * ( am > bm ? 1 : -1 );
+    const double d_am_bp = dmax( fabs( am - bp ), f_min ) * ( am > bp ? 1 : -1 );
+    const double sl = ( am >= 0 ? am / d_am_bm : 0 );
+    const double sr = ( am <  0 ? am / d_am_bp : 0 );
+    const double sm = ( am >  0 ? -bm / d_am_bm : -bp / d_am_bp );
+
+    f_lr_hyd( fl, wli, wli[ MOM ] - bm, el );
+    f_lr_hyd( fr, wri, wri[ MOM ] - bp, er );
+    for( int n = RHO; n < MOM + 3; ++ n )
+        flx[ n ] = sl * fl[ n ] + sr * fr[ n ];
+    flx[ MOM ] += sm * cp;
+    flx[ ENE ] += sm * cp * am;
+}
+
+/* hydro/riemann/hllc.h:218-229 calc: rotate, solve, rotate back */
+static void hllc_calc( double * flx, double * ql, double * qr, int axis, double gamma )
+{
+    idx_swap( ql + MOM, axis );
+    idx_swap( qr + MOM, axis );
+    hllc_eval( flx, ql, qr, gamma );
+    idx_swap( flx + MOM, 3 - axis );
+}
+
+void kro_hllc( const double * ql_in, const double * qr_in, int axis, double gamma, double * flx )
+{
+    double ql[ 5 ], qr[ 5 ];
+    memcpy( ql, ql_in, sizeof ql );
+    memcpy( qr, qr_in, sizeof qr );
+    hllc_calc( flx, ql, qr, axis, gamma );
+}
+
+/* ------------------------------------------------------------------ */
+/* HLLD (mhd/riemann/hlld.h:49-69 f_flux, 81-298 eval)                 */
+
+static inline void hlld_f_flux( double * flux, const double * u, const double * w,
+                                double p_tot, double b_x )
+{
+    const double bx_2 = b_x * b_x;
+    flux[ RHO ] = u[ MOM ];
+    flux[ ENE ] = w[ MOM ] * ( p_tot + u[ ENE ] - bx_2 ) - b_x
+                * ( w[ MOM + 1 ] * u[ BCC + 1 ] + w[ MOM + 2 ] * u[ BCC + 2 ] );
+    flux[ MOM ]     = p_tot - bx_2 + u[ MOM ] * w[ MOM ];
+    flux[ MOM + 1 ] = -b_x * u[ BCC + 1 ] + u[ MOM + 1 ] * w[ MOM ];
+    flux[ MOM + 2 ] = -b_x * u[ BCC + 2 ] + u[ MOM + 2 ] * w[ MOM ];
+    flux[ BCC + 1 ] = -b_x * w[ MOM + 1 ] + u[ BCC + 1 ] * w[ MOM ];
+    flux[ BCC + 2 ] = -b_x * w[ MOM + 2 ] + u[ BCC + 2 ] * w[ MOM ];
+}
+
+static inline double hlld_cons( double * u, const double * w, double bx_2, double b_x,
+                                double gamma, double * gam1 )
+{
+    double p_m = bx_2 / 2, cs;
+    for( int a = 1; a <= 2; ++ a )
+    {
+        const int n = BCC + a;
+        p_m += w[ n ] * w[ n ] / 2;
+        u[ n ] = w[ n ];
+    }
+    * gam1 = 1 / et_cs( gamma, & u[ ENE ], & cs, w );
+    for( int n = MOM; n < MOM + 3; ++ n )
+        u[ n ] = w[ RHO ] * w[ n ];
+    u[ RHO ] = w[ RHO ];
+    u[ ENE ] += p_m;
+    u[ BCC ] = b_x;
+    return p_m;
+}
+
+typedef struct { double b_x, bx_2, ptot_s, spd0; } hlld_ctx;
+
+static double hlld_star( const hlld_ctx * h, double * u_star, const double * u,
+                         const double * w, double rhos, double sd, double sdm,
+                         double p_tot, double f_tiny )
+{
+    const double b_x = h->b_x, bx_2 = h->bx_2;
+    u_star[ RHO ] = rhos;
+    u_star[ MOM ] = rhos * h->spd0;
+    u_star[ BCC ] = b_x;
+    const double denom = u[ RHO ] * sd * sdm - bx_2;
+    if( uabs( denom ) < f_tiny * h->ptot_s )
+        for( int a = 1; a <= 2; ++ a )
+        {
+            u_star[ MOM + a ] = rhos * w[ MOM + a ];
+            u_star[ BCC + a ] = u[ BCC + a ];
+        }
+    else
+    {
+        const double tmp_v = b_x * ( sd - sdm ) / denom;
+        const double tmp_b = ( u[ RHO ] * sd * sd - bx_2 ) / denom;
+        for( int a = 1; a <= 2; ++ a )
+        {
+            u_star[ MOM + a ] = rhos * ( w[ MOM + a ] - u[ BCC + a ] * tmp_v );
+            u_star[ BCC + a ] = u[ BCC + a ] * tmp_b;
+        }
+    }
+    double u_dot_b = 0, w_dot_b = 0;
+    for( int a = 0; a < 3; ++ a )
+    {
+        u_dot_b += u_star[ MOM + a ] * u_star[ BCC + a ];
+        w_dot_b += w[ MOM + a ] * u[ BCC + a ];
+    }
+    u_dot_b /= rhos;
+    u_star[ ENE ] = b_x * ( w_dot_b - u_dot_b )
+        - p_tot * w[ MOM ] + sd * u[ ENE ]
+        + h->ptot_s * h->spd0;
+    u_star[ ENE ] /= sdm;
+    return u_dot_b;
+}
+
+static void hlld_eval( double * flx, const double * wli, const double * wri, double gamma )
+{
+    flx[ BCC ] = 0;
+    double spd_m2, spd_m1, spd0, spd_p1, spd_p2;
+    double u_l[ 8 ], u_r[ 8 ];
+    const double b_x  = wli[ BCC ];
+    const double bx_2 = b_x * b_x;
+    double gam1_l, gam1_r;
+    const double pm_l = hlld_cons( u_l, wli, bx_2, b_x, gamma, & gam1_l );
+    const double pm_r = hlld_cons( u_r, wri, bx_2, b_x, gamma, & gam1_r );
+    const double ptot_l = wli[ ENE ] + pm_l;
+    const double ptot_r = wri[ ENE ] + pm_r;
+
+    double b2_eff_l[ 3 ] = { b_x, wli[ BCC + 1 ], wli[ BCC + 2 ] };
+    double b2_eff_r[ 3 ] = { b_x, wri[ BCC + 1 ], wri[ BCC + 2 ] };
+    for( int a = 0; a < 3; ++ a )
+    {
+        b2_eff_l[ a ] *= b2_eff_l[ a ];
+        b2_eff_r[ a ] *= b2_eff_r[ a ];
+    }
+    const double cfm_l = c_fms( wli, b2_eff_l, gam1_l + 1, 0 );
+    const double cfm_r = c_fms( wri, b2_eff_r, gam1_r + 1, 0 );
+
+    spd_m2 = dmin( wli[ MOM ] - cfm_l, wri[ MOM ] - cfm_r );
+    spd_p2 = dmax( wli[ MOM ] + cfm_l, wri[ MOM ] + cfm_r );
+
+    if( spd_m2 >= 0 || spd_p2 <= 0 )
+    {
+        const int is_left = spd_m2 >= 0;
+        hlld_f_flux( flx, is_left ? u_l : u_r, is_left ? wli : wri,
+                     is_left ? ptot_l : ptot_r, b_x );
+        return;
+    }
+
+    const double sd_l = spd_m2 - wli[ MOM ];
+    const double sd_r = spd_p2 - wri[ MOM ];
+    spd0 = ( sd_r * u_r[ MOM ] - ptot_r - sd_l * u_l[ MOM ] + ptot_l )
+         / ( sd_r * u_r[ RHO ] - sd_l * u_l[ RHO ] );
+
+    const double sdm_l  = spd_m2 - spd0;
+    const double sdm_r  = spd_p2 - spd0;
+    const double rhos_l = u_l[ RHO ] * sd_l / sdm_l;
+    const double rhos_r = u_r[ RHO ] * sd_r / sdm_r;
+    const double rhos_l_sqrt = sqrt( rhos_l );
+    const double rhos_r_sqrt = sqrt( rhos_r );
+    spd_m1 = spd0 - uabs( b_x ) / rhos_l_sqrt;
+    spd_p1 = spd0 + uabs( b_x ) / rhos_r_sqrt;
+
+    const double f_tiny = ( double )( 1.00e-4f );
+    const double ptot_s = ptot_l + u_l[ RHO ] * sd_l * ( sd_l - sdm_l );
+    const hlld_ctx h = { b_x, bx_2, ptot_s, spd0 };
+
+    double us_l[ 8 ], us_r[ 8 ];
+    const double u_dot_b_l = hlld_star( & h, us_l, u_l, wli, rhos_l, sd_l, sdm_l, ptot_l, f_tiny );
+    const double u_dot_b_r = hlld_star( & h, us_r, u_r, wri, rhos_r, sd_r, sdm_r, ptot_r, f_tiny );
+    if( spd_m1 >= 0 )
+    {
+        hlld_f_flux( flx, u_l, wli, ptot_l, b_x );
+        for( int n = 0; n < 8; ++ n )
+            flx[ n ] += spd_m2 * ( us_l[ n ] - u_l[ n ] );
+        return;
+    }
+    else if( spd_p1 <= 0 )
+    {
+        hlld_f_flux( flx, u_r, wri, ptot_r, b_x );
+        for( int n = 0; n < 8; ++ n )
+            flx[ n ] += spd_p2 * ( us_r[ n ] - u_r[ n ] );
+        return;
+    }
+
+    double uss_l[ 8 ], uss_r[ 8 ];
+    for( int n = 0; n < 8; ++ n )
+    {
+        uss_l[ n ] = us_l[ n ];
+        uss_r[ n ] = us_r[ n ];
+    }
+    if( bx_2 > ptot_s * f_tiny )
+    {
+        const int bx_sgn = b_x > 0 ? 1 : -1;
+        const double rhos_norm_inv = 1.f / ( rhos_l_sqrt + rhos_r_sqrt );
+        for( int a = 1; a <= 2; ++ a )
+        {
+            double tmp = rhos_norm_inv *
+                ( us_l[ MOM + a ] / rhos_l_sqrt
+                + us_r[ MOM + a ] / rhos_r_sqrt
+                + bx_sgn * ( us_r[ BCC + a ] - us_l[ BCC + a ] ) );
+            uss_l[ MOM + a ] = uss_l[ RHO ] * tmp;
+            uss_r[ MOM + a ] = uss_r[ RHO ] * tmp;
+
+            tmp = rhos_norm_inv *
+                ( rhos_l_sqrt * us_r[ BCC + a ]
+                + rhos_r_sqrt * us_l[ BCC + a ]
+                + bx_sgn * rhos_l_sqrt * rhos_r_sqrt
+                * ( us_r[ MOM + a ] / rhos_r - us_l[ MOM + a ] / rhos_l ) );
+            uss_l[ BCC + a ] = tmp;
+            uss_r[ BCC + a ] = tmp;
+        }
+        const double tmp = spd0 * b_x +
+            ( uss_l[ MOM + 1 ] * uss_l[ BCC + 1 ]
+            + uss_l[ MOM + 2 ] * uss_l[ BCC + 2 ] ) / uss_l[ RHO ];
+        uss_l[ ENE ] -= rhos_l_sqrt * bx_sgn * ( u_dot_b_l - tmp );
+        uss_r[ ENE ] += rhos_r_sqrt * bx_sgn * ( u_dot_b_r - tmp );
+    }
+    if( spd0 >= 0 )
+    {
+        hlld_f_flux( flx, u_l, wli, ptot_l, b_x );
+        const double d_v = spd_m1 - spd_m2;
+        for( int n = 0; n < 8; ++ n )
+            flx[ n ] += -spd_m2 * u_l[ n ] - d_v * us_l[ n ] + spd_m1 * uss_l[ n ];
+    }
+    else
+    {
+        hlld_f_flux( flx, u_r, wri, ptot_r, b_x );
+        const double d_v = spd_p1 - spd_p2;
+        for( int n = 0; n < 8; ++ n )
+            flx[ n ] += -spd_p2 * u_r[ n ] - d_v * us_r[ n ] + spd_p1 * uss_r[ n ];
+    }
+}
+
+/* mhd/riemann/hlld.h:29-47 calc: rotate momenta and B, solve, rotate the
+ * momentum flux back, remap the transverse B fluxes to edge EMFs. */
+static void hlld_calc( double * flx, double * ql, double * qr, int axis, double gamma )
+{
+    idx_swap( ql + MOM, axis );
+    idx_swap( qr + MOM, axis );
+    idx_swap( ql + BCC, axis );
+    idx_swap( qr + BCC, axis );
+    hlld_eval( flx, ql, qr, gamma );
+    idx_swap( flx + MOM, 3 - axis );
+    const double ef[ 2 ] = { flx[ BCC + 2 ], -flx[ BCC + 1 ] };
+    flx[ BCC + mod3( axis + 1 ) ] = ef[ 0 ];
+    flx[ BCC + mod3( axis + 2 ) ] = ef[ 1 ];
+    flx[ BCC + axis ] = 0;
+}
+
+void kro_hlld( const double * ql_in, const double * qr_in, int axis, double gamma, double * flx )
+{
+    double ql[ 8 ], qr[ 8 ];
+    memcpy( ql, ql_in, sizeof ql );
+    memcpy( qr, qr_in, sizeof qr );
+    hlld_calc( flx, ql, qr, axis, gamma );
+}
+
+/* ------------------------------------------------------------------ */
+/* Face fluxes along one axis for one block: PLM + Riemann on every    */
+/* face of every pencil (integrator.h:14-32 flux_kernel; pencil gather  */
+/* hydro/integrator/data.h:139-157, MHD mhd/integrator/data.h:146-194;  */
+/* MHD also covers the transverse ghost lines, mhd/integrator/         */
+/* integrator.h:138-168 and data.h:106-144).                           */
+
+typedef struct { int step; int axis; } flux_arg;
+
+static void flux_pencil( kro_mesh * m, int b, int axis, int step, int t1, int t2 )
+{
+    const int nw = m->nw;
+    const int a1 = mod3( axis + 1 ), a2 = mod3( axis + 2 );
+    const int nax = m->c.n[ axis ];
+    const double * w  = m->w + ( size_t ) b * m->nw_cells * nw;
+    const double * bf = m->c.mhd ? m->bf[ step ] + ( size_t ) b * m->nbf : NULL;
+    double * f = m->f[ axis ] + ( size_t ) b * m->nf[ axis ];
+    for( int fc = 0; fc <= nax; ++ fc )
+    {
+        double ql[ 8 ], qr[ 8 ], flx[ 8 ];
+        int ii[ 3 ];
+        ii[ a1 ] = t1;
+        ii[ a2 ] = t2;
+        for( int k = 0; k < nw; ++ k )
+        {
+            if( m->c.mhd && k == BCC + axis )
+            {
+                ii[ axis ] = fc;
+                ql[ k ] = qr[ k ] = bf[ ib( m, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) + axis ];
+                continue;
+            }
+            double q4[ 4 ];
+            for( int s = 0; s < 4; ++ s )
+            {
+                ii[ axis ] = fc - 2 + s;
+                q4[ s ] = w[ iw( m, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) + k ];
+            }
+            plm_face( q4[ 0 ], q4[ 1 ], q4[ 2 ], q4[ 3 ], & ql[ k ], & qr[ k ] );
+        }
+        if( m->c.mhd )
+            hlld_calc( flx, ql, qr, axis, m->c.gamma );
+        else
+            hllc_calc( flx, ql, qr, axis, m->c.gamma );
+        ii[ axis ] = fc;
+        memcpy( f + ifl( m, axis, ii[ 0 ], ii[ 1 ], ii[ 2 ] ), flx, sizeof( double ) * nw );
+    }
+}
+
+static void flux_block( kro_mesh * m, int b, void * aux )
+{
+    const flux_arg * fa = ( const flux_arg * ) aux;
+    const int axis = fa->axis;
+    const int a1 = mod3( axis + 1 ), a2 = mod3( axis + 2 );
+    const int n1 = m->c.n[ a1 ], n2 = m->c.n[ a2 ];
+    for( int t2 = 0; t2 < n2; ++ t2 )
+        for( int t1 = 0; t1 < n1; ++ t1 )
+            flux_pencil( m, b, axis, fa->step, t1, t2 );
+    if( ! m->c.mhd )
+        return;
+    for( int t2 = 0; t2 < n2; ++ t2 )
+    {
+        flux_pencil( m, b, axis, fa->step, -1, t2 );
+        flux_pencil( m, b, axis, fa->step, n1, t2 );
+    }
+    for( int t1 = 0; t1 < n1; ++ t1 )
+    {
+        flux_pencil( m, b, axis, fa->step, t1, -1 );
+        flux_pencil( m, b, axis, fa->step, t1, n2 );
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* Conserved update (hydro/integrator/integrator.h:58-67 flux_to_du,    */
+/* 156-182 load_flux_sfc, 241-265 add_flux; rk2.h:404-425 load).        */
+
+typedef struct { int step; double dt; } upd_arg;
+
+static void update_block( kro_mesh * m, int b, void * aux )
+{
+    const upd_arg * ua = ( const upd_arg * ) aux;
+    const int step = ua->step, nw = m->nw;
+    const int * n = m->c.n;
+    const double * us = m->u[ step ]     + ( size_t ) b * m->ncell * nw;
+    double       * ut = m->u[ 1 - step ] + ( size_t ) b * m->ncell * nw;
+    const double vol  = m->vol0[ b ];
+    const double dt_dv = ua->dt / vol;
+    double f_a[ 3 ];
+    for( int a = 0; a < 3; ++ a )
+        f_a[ a ] = m->sfc0[ b * 3 + a ] * dt_dv;
+    for( int i2 = 0; i2 < n[ 2 ]; ++ i2 )
+    for( int i1 = 0; i1 < n[ 1 ]; ++ i1 )
+    for( int i0 = 0; i0 < n[ 0 ]; ++ i0 )
+    {
+        const long c = iu( m, i0, i1, i2 );
+        double v[ 8 ];
+        for( int k = 0; k < nw; ++ k )
+            v[ k ] = step == 0 ? us[ c + k ] : ( us[ c + k ] + ut[ c + k ] ) * 0.5f;
+        for( int a = 0; a < 3; ++ a )
+        {
+            int ii[ 3 ] = { i0, i1, i2 };
+            const double * fl = m->f[ a ] + ( size_t ) b * m->nf[ a ]
+                              + ifl( m, a, ii[ 0 ], ii[ 1 ], ii[ 2 ] );
+            ++ ii[ a ];
+            const double * fr = m->f[ a ] + ( size_t ) b * m->nf[ a ]
+                              + ifl( m, a, ii[ 0 ], ii[ 1 ], ii[ 2 ] );
+            for( int k = 0; k < nw; ++ k )
+            {
+                double res = 0;
+                if( f_a[ a ] > 0 )
+                    res += f_a[ a ] * fl[ k ];
+                if( f_a[ a ] > 0 )
+                    res -= f_a[ a ] * fr[ k ];
+                v[ k ] += res;
+            }
+        }
+        for( int k = 0; k < nw; ++ k )
+            ut[ c + k ] = v[ k ];
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* CT: edge EMF (mhd/integrator/integrator.h:189-327 calc_field) and   */
+/* face update (385-462 intg_field; rk2.h:244-258 set_field).          */
+
+static inline double e_cell( const kro_mesh * m, const double * w, const int * j, int ax )
+{
+    /* ec = B x v, from the cell's primitives (mhd/eos/adiabatic.h:216-220;
+     * ghost cells: integrator.h:201-213) */
+    const double * p = w + iw( m, j[ 0 ], j[ 1 ], j[ 2 ] );
+    const int ax1 = mod3( ax + 1 ), ax2 = mod3( ax + 2 );
+    return p[ BCC + ax1 ] * p[ MOM + ax2 ] - p[ BCC + ax2 ] * p[ MOM + ax1 ];
+}
+
+static void emf_block( kro_mesh * m, int b, void * aux )
+{
+    ( void ) aux;
+    const int nw = m->nw;
+    const int * n = m->c.n;
+    const double * w = m->w + ( size_t ) b * m->nw_cells * nw;
+    const double * F[ 3 ];
+    for( int a = 0; a < 3; ++ a )
+        F[ a ] = m->f[ a ] + ( size_t ) b * m->nf[ a ];
+    double * ee = m->ee + ( size_t ) b * m->nee;
+    const double w_e = 0.25f;
+    for( int i2 = 0; i2 <= n[ 2 ]; ++ i2 )
+    for( int i1 = 0; i1 <= n[ 1 ]; ++ i1 )
+    for( int i0 = 0; i0 <= n[ 0 ]; ++ i0 )
+    {
+        int i[ 3 ] = { i0, i1, i2 };
+        for( int ax = 0; ax < 3; ++ ax )
+        {
+            if( i[ ax ] >= n[ ax ] )
+                continue;
+            const int ax1 = mod3( 1 + ax ), ax2 = mod3( 2 + ax );
+            double ec[ 2 ][ 2 ];
+            ec[ 1 ][ 1 ] = e_cell( m, w, i, ax );
+            -- i[ ax1 ];
+            ec[ 1 ][ 0 ] = e_cell( m, w, i, ax );
+            -- i[ ax2 ];
+            ec[ 0 ][ 0 ] = e_cell( m, w, i, ax );
+            ++ i[ ax1 ];
+            ec[ 0 ][ 1 ] = e_cell( m, w, i, ax );
+            ++ i[ ax2 ];
+            double e = 0;
+            for( int it = 0; it < 2; ++ it )
+            {
+                const int a_para = it == 0 ? ax1 : ax2;
+                const int a_perp = it == 0 ? ax2 : ax1;
+                -- i[ a_perp ];
+                const double ef_m = F[ a_para ][ ifl( m, a_para, i[ 0 ], i[ 1 ], i[ 2 ] ) + BCC + ax ];
+                ++ i[ a_perp ];
+                const double ef_p = F[ a_para ][ ifl( m, a_para, i[ 0 ], i[ 1 ], i[ 2 ] ) + BCC + ax ];
+                e += w_e * ( ef_m + ef_p );
+                const double frho_p = F[ a_perp ][ ifl( m, a_perp, i[ 0 ], i[ 1 ], i[ 2 ] ) + RHO ];
+                -- i[ a_para ];
+                const double frho_m = F[ a_perp ][ ifl( m, a_perp, i[ 0 ], i[ 1 ], i[ 2 ] ) + RHO ];
+                ++ i[ a_para ];
+                const double de_p = frho_p > 0 ?  ( ec[ 0 ][ 1 ] - ef_m ) :  ( ec[ 1 ][ 1 ] - ef_p );
+                const double de_m = frho_m > 0 ? -( ec[ 0 ][ 0 ] - ef_m ) : -( ec[ 1 ][ 0 ] - ef_p );
+                e += w_e * ( de_m - de_p );
+                if( it == 0 )
+                {
+                    const double swp = ec[ 0 ][ 1 ];
+                    ec[ 0 ][ 1 ] = ec[ 1 ][ 0 ];
+                    ec[ 1 ][ 0 ] = swp;
+                }
+            }
+            ee[ ie( m, i0, i1, i2 ) + ax ] = e;
+        }
+    }
+}
+
+typedef struct { int step; double dt; } ct_arg;
+
+static void ct_block( kro_mesh * m, int b, void * aux )
+{
+    const ct_arg * ca = ( const ct_arg * ) aux;
+    const int step = ca->step;
+    const int * n = m->c.n;
+    const double * ee = m->ee + ( size_t ) b * m->nee;
+    const double * bs = m->bf[ step ]     + ( size_t ) b * m->nbf;
+    double       * bt = m->bf[ 1 - step ] + ( size_t ) b * m->nbf;
+    const double * dx = m->dx0 + b * 3;
+    for( int i2 = 0; i2 <= n[ 2 ]; ++ i2 )
+    for( int i1 = 0; i1 <= n[ 1 ]; ++ i1 )
+    for( int i0 = 0; i0 <= n[ 0 ]; ++ i0 )
+    {
+        int i[ 3 ] = { i0, i1, i2 };
+        for( int a = 0; a < 3; ++ a )
+        {
+            const int ax1 = mod3( a + 1 ), ax2 = mod3( a + 2 );
+            if( i[ ax1 ] >= n[ ax1 ] || i[ ax2 ] >= n[ ax2 ] )
+                continue;
+            double db;
+            db  = ( ee[ ie( m, i[ 0 ], i[ 1 ], i[ 2 ] ) + ax1 ] * dx[ ax1 ] );
+            db -= ( ee[ ie( m, i[ 0 ], i[ 1 ], i[ 2 ] ) + ax2 ] * dx[ ax2 ] );
+            ++ i[ ax1 ];
+            db += ( ee[ ie( m, i[ 0 ], i[ 1 ], i[ 2 ] ) + ax2 ] * dx[ ax2 ] );
+            -- i[ ax1 ];
+            ++ i[ ax2 ];
+            db -= ( ee[ ie( m, i[ 0 ], i[ 1 ], i[ 2 ] ) + ax1 ] * dx[ ax1 ] );
+            -- i[ ax2 ];
+            const double sfc = m->sfc0[ b * 3 + a ];
+            db *= ( sfc > 0 ? ( -ca->dt / sfc ) : 0. );
+            const long k = ib( m, i[ 0 ], i[ 1 ], i[ 2 ] ) + a;
+            bt[ k ] = db + ( step == 0 ? bs[ k ] : ( bs[ k ] + bt[ k ] ) / 2 );
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* One Heun step (dynamics.h:74-114 integrate, dynamics.cpp:156-161    */
+/* step; cycle.cpp:77-115 dt reduction).                                */
+
+int kro_step( kro_mesh * m, int n_steps, double * t, double * dt_bound, double * dt_last )
+{
+    for( int s = 0; s < n_steps; ++ s )
+    {
+        double dt_use = 0;
+        for( int stage = 0; stage < 2; ++ stage )
+        {
+            c2p_arg ca = { stage };
+            par_blocks( m, c2p_block, & ca );
+            if( stage == 0 )
+            {
+                double d = * dt_bound;
+                for( int b = 0; b < m->nblk; ++ b )
+                    d = fmin( d, m->dtc[ b ] );
+                dt_use = d;
+                if( ! isfinite( dt_use ) || dt_use <= 0 )
+                    return -1;
+            }
+            ghost_arg ga = { stage };
+            par_blocks( m, ghost_block, & ga );
+            const double dt = dt_use * ( stage == 0 ? 1.0 : ( double ) 0.5f );
+            for( int axis = 2; axis >= 0; -- axis )
+            {
+                flux_arg fa = { stage, axis };
+                par_blocks( m, flux_block, & fa );
+            }
+            upd_arg ua = { stage, dt };
+            par_blocks( m, update_block, & ua );
+            if( m->c.mhd )
+            {
+                par_blocks( m, emf_block, NULL );
+                ct_arg cta = { stage, dt };
+                par_blocks( m, ct_block, & cta );
+            }
+        }
+        * t += dt_use;
+        * dt_bound = dt_use * m->c.dt_expand;
+        if( dt_last ) * dt_last = dt_use;
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* initial conditions (the pgen side: oracle/pgen/kr_ref_pgen.cpp)       */
+
+int kro_init_problem( kro_mesh * m, const char * name, unsigned long long seed )
+{
+    const int * n = m->c.n;
+    int nglob[ 3 ];
+    for( int a = 0; a < 3; ++ a )
+        nglob[ a ] = n[ a ] * m->c.nb[ a ];
+    const int is_shock = ! strcmp( name, "shock" ), is_ot = ! strcmp( name, "ot" );
+    if( ! is_shock && ! is_ot )
+        return -1;
+    if( is_ot != m->c.mhd )
+        return -1;
+    for( int b = 0; b < m->nblk; ++ b )
+    {
+        const int reg[ 3 ] = { b % m->c.nb[ 0 ], ( b / m->c.nb[ 0 ] ) % m->c.nb[ 1 ],
+                               b / ( m->c.nb[ 0 ] * m->c.nb[ 1 ] ) };
+        double * u  = m->u[ 0 ] + ( size_t ) b * m->ncell * m->nw;
+        double * bf = is_ot ? m->bf[ 0 ] + ( size_t ) b * m->nbf : NULL;
+        if( is_ot )
+            for( int i2 = 0; i2 <= n[ 2 ]; ++ i2 )
+            for( int i1 = 0; i1 <= n[ 1 ]; ++ i1 )
+            for( int i0 = 0; i0 <= n[ 0 ]; ++ i0 )
+            {
+                double * p = bf + ib( m, i0, i1, i2 );
+                p[ 0 ] = kr_ot_bx( kro_x_cc( m, b, 1, i1 ) );
+                p[ 1 ] = kr_ot_by( kro_x_cc( m, b, 0, i0 ) );
+                p[ 2 ] = kr_ot_bz(  );
+            }
+        for( int i2 = 0; i2 < n[ 2 ]; ++ i2 )
+        for( int i1 = 0; i1 < n[ 1 ]; ++ i1 )
+        for( int i0 = 0; i0 < n[ 0 ]; ++ i0 )
+        {
+            const int ii[ 3 ] = { i0, i1, i2 };
+            int ig[ 3 ];
+            for( int a = 0; a < 3; ++ a )
+                ig[ a ] = reg[ a ] * n[ a ] + ii[ a ];
+            const uint64_t key = kr_cell_key( 0, ig, nglob );
+            double * c = u + iu( m, i0, i1, i2 );
+            if( is_shock )
+                kr_shock_cell( c, kro_x_cc( m, b, 0, i0 ), m->c.gamma, seed, key );
+            else
+            {
+                double x[ 3 ], bc[ 3 ];
+                for( int a = 0; a < 3; ++ a )
+                {
+                    int jj[ 3 ] = { i0, i1, i2 };
+                    x[ a ] = kro_x_cc( m, b, a, ii[ a ] );
+                    const double bl = bf[ ib( m, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) + a ];
+                    ++ jj[ a ];
+                    bc[ a ] = ( bl + bf[ ib( m, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) + a ] ) / 2;
+                }
+                kr_ot_cell( c, x, bc, m->c.gamma, seed, key );
+            }
+        }
+    }
+    return 0;
+}

@@ -1,0 +1,115 @@
+"""Generate the golden fixtures of the hydro / MHD step from the original Kratos
+solver.
+
+The reference is compiled for the CPU from its own sources (its ARCH=HIPCPU
+path, PRECISION=2) by oracle/Makefile.ref into oracle/_ref/kratos_ref, with the
+problem generator oracle/pgen/kr_ref_pgen.cpp.  This script runs it on a few
+small seeded workloads, reads the snapshots it writes (initial and final) and
+stores them under tests/golden/ as compressed .npz files:
+
+    u0, u1      conserved state before / after the run, [nblk, n2, n1, n0, nw]
+                in lexicographic block order (x fastest)
+    bf0, bf1    MHD face field, owned lattice box [nblk, n2+1, n1+1, n0+1, 3]
+    meta        JSON: workload, mesh, physics, steps, final time and dt
+Large cases keep only checksums (per-component sum, sum of |.|, min, max).
+
+Usage:  make -f oracle/Makefile.ref REF=<kratos tree> -j8
+        python tests/golden/make_golden.py
+"""
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+from kratos_b200.snapshot import Snapshot, to_lex_arrays  # noqa: E402
+
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "kratos_ref")
+
+CASES = [
+    # name, problem, nb, n, steps, seed, gamma, extra dynamics keys, keep fields
+    # keep: "full" (initial and final fields), "final" (final fields) or "sums"
+    ("shock_16", "shock", (2, 2, 2), (8, 8, 8), 5, 1, 1.4, {}, "full"),
+    ("ot_16", "ot", (2, 2, 2), (8, 8, 8), 5, 2, 1.6666666666666667, {}, "full"),
+    ("ot_ragged", "ot", (3, 2, 1), (8, 8, 8), 4, 3, 1.6666666666666667, {}, "final"),
+    ("shock_floor", "shock", (2, 2, 2), (8, 8, 8), 3, 4, 1.4, {"tmp_floor": "1.0"}, "final"),
+    ("shock_c1", "shock", (2, 2, 2), (32, 32, 32), 20, 1, 1.4, {}, "sums"),
+    ("ot_64", "ot", (2, 2, 2), (32, 32, 32), 10, 2, 1.6666666666666667, {}, "sums"),
+]
+
+
+def par_text(problem, nb, n, steps, seed, gamma, extra, prefix):
+    ng = [nb[a] * n[a] for a in range(3)]
+    dyn = {"gamma": repr(gamma), "cfl": "0.3", "thread_limit": "1", "bnd_thread_limit": "1"}
+    dyn.update(extra)
+    lines = [
+        "[problem]", "name = %s" % problem, "seed = %d" % seed, "",
+        "[mesh]", "x_min = 0 0 0", "x_max = 1 1 1",
+        "n_cell_global = %d %d %d" % tuple(ng), "n_cell_block = %d %d %d" % tuple(n), "",
+        "[cycle]", "prefix_output = %s" % prefix, "n_cycle_lim = %d" % (steps - 1),
+        "final_output = 1", "n_display_freq = 1000000", "",
+        "[dynamics]"] + ["%s = %s" % kv for kv in dyn.items()] + [
+        "", "[boundary]", "kinds = per per per per per per", ""]
+    return "\n".join(lines)
+
+
+def checksums(a):
+    a = a.reshape(-1, a.shape[-1])
+    return np.stack([a.sum(0), np.abs(a).sum(0), a.min(0), a.max(0)])
+
+
+def owned_bf(bf, n):
+    return bf[:, 2:3 + n[2], 2:3 + n[1], 2:3 + n[0], :].copy()
+
+
+def run_case(name, problem, nb, n, steps, seed, gamma, extra, keep):
+    with tempfile.TemporaryDirectory() as tmp:
+        prefix = os.path.join(tmp, "snap")
+        par = os.path.join(tmp, "case.par")
+        with open(par, "w") as f:
+            f.write(par_text(problem, nb, n, steps, seed, gamma, extra, prefix))
+        subprocess.check_call([REF_BIN, par], cwd=tmp, stdout=subprocess.DEVNULL)
+        s0 = Snapshot.read(prefix + "_00000.bin")
+        s1 = Snapshot.read(prefix + "_00001.bin")
+    u0, bf0 = to_lex_arrays(s0, nb)
+    u1, bf1 = to_lex_arrays(s1, nb)
+    meta = {
+        "workload": problem, "seed": seed, "gamma": gamma, "nb": list(nb), "n": list(n),
+        "steps": steps, "cfl": 0.3, "dynamics": extra,
+        "t": float(s1.array("time")[0]), "dt": float(s1.array("dt")[0]),
+        "cycle": int(s1.array("cycle", "i")[0]),
+    }
+    out = {"meta": np.array(json.dumps(meta))}
+    if keep == "full":
+        out["u0"] = u0
+        if bf0 is not None:
+            out["bf0"] = owned_bf(bf0, n)
+    if keep in ("full", "final"):
+        out["u1"] = u1
+        if bf1 is not None:
+            out["bf1"] = owned_bf(bf1, n)
+    out["u0_sum"], out["u1_sum"] = checksums(u0), checksums(u1)
+    if bf0 is not None:
+        out["bf0_sum"] = checksums(owned_bf(bf0, n))
+        out["bf1_sum"] = checksums(owned_bf(bf1, n))
+    path = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(path, **out)
+    print("%-12s t=%.6e  %7.1f kB" % (name, meta["t"], os.path.getsize(path) / 1e3))
+
+
+def main():
+    if not os.path.exists(REF_BIN):
+        sys.exit("build the reference first: make -f oracle/Makefile.ref REF=<kratos tree>")
+    only = set(sys.argv[1:])
+    for c in CASES:
+        if not only or c[0] in only:
+            run_case(*c)
+
+
+if __name__ == "__main__":
+    main()

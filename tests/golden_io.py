@@ -1,0 +1,36 @@
+"""Loading of the golden fixtures made by tests/golden/make_golden.py."""
+import json
+import os
+
+import numpy as np
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+CASES = ["shock_16", "ot_16", "ot_ragged", "shock_floor", "shock_c1", "ot_64"]
+
+
+def load(name):
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    meta = json.loads(str(z["meta"]))
+    return meta, {k: z[k] for k in z.files if k != "meta"}
+
+
+def checksums(a):
+    a = a.reshape(-1, a.shape[-1])
+    return np.stack([a.sum(0), np.abs(a).sum(0), a.min(0), a.max(0)])
+
+
+def owned_bf(bf, n):
+    """Owned face-lattice box [nblk, n2+1, n1+1, n0+1, 3] of a full bf array
+    [nblk, n2+5, n1+5, n0+5, 3] (2 ghost layers)."""
+    return bf[:, 2:3 + n[2], 2:3 + n[1], 2:3 + n[0], :]
+
+
+def face_mask(n):
+    """Boolean mask over the owned box marking faces a block owns:
+    component c at index 0..n along c and 0..n-1 along the other axes."""
+    m = np.zeros((n[2] + 1, n[1] + 1, n[0] + 1, 3), bool)
+    for c in range(3):
+        sl = [slice(0, n[2]), slice(0, n[1]), slice(0, n[0])]
+        sl[2 - c] = slice(0, n[c] + 1)
+        m[tuple(sl) + (c,)] = True
+    return m

@@ -1,0 +1,112 @@
+"""The CPU restatement (oracle/) against the original Kratos solver.
+
+The golden fixtures were produced by the reference's own code compiled for the
+CPU (tests/golden/make_golden.py).  The restatement follows the reference
+expression by expression and is built without fused multiply-add, so the
+comparison is bit for bit: initial state, every conserved component (including
+the cell-centred B slots), every owned face of B, the final time and dt.
+"""
+import numpy as np
+import pytest
+
+from oracle.kr_oracle import OracleMesh
+import golden_io as G
+
+
+def _mesh(meta):
+    extra = meta.get("dynamics", {})
+    return OracleMesh(meta["workload"] == "ot", meta["nb"], meta["n"], meta["gamma"],
+                      cfl=meta["cfl"], t_floor=float(extra.get("tmp_floor", 1e-9)))
+
+
+@pytest.mark.parametrize("name", ["shock_16", "ot_16"])
+def test_initial_state_bit_exact(name):
+    meta, g = G.load(name)
+    m = _mesh(meta)
+    m.init_problem(meta["workload"], meta["seed"])
+    u, bf = m.get_state()
+    assert np.array_equal(u, g["u0"])
+    if m.mhd:
+        mask = G.face_mask(meta["n"])
+        own = G.owned_bf(bf, meta["n"])
+        assert np.array_equal(own[:, mask], g["bf0"][:, mask])
+
+
+@pytest.mark.parametrize("name", G.CASES)
+def test_step_bit_exact(name):
+    meta, g = G.load(name)
+    m = _mesh(meta)
+    m.init_problem(meta["workload"], meta["seed"])
+    u_init, bf_init = m.get_state()
+    assert np.array_equal(G.checksums(u_init), g["u0_sum"])
+    m.step(meta["steps"])
+    u, bf = m.get_state()
+    assert m.t == meta["t"]
+    assert m.dt_last == meta["dt"]
+    if "u1" in g:
+        assert np.array_equal(u, g["u1"])
+    assert np.array_equal(G.checksums(u), g["u1_sum"])
+    if m.mhd:
+        n = meta["n"]
+        own = G.owned_bf(bf, n)
+        if "bf1" in g:
+            mask = G.face_mask(n)
+            assert np.array_equal(own[:, mask], g["bf1"][:, mask])
+
+
+def test_floor_case_triggers_floor():
+    """The floor fixture must actually exercise the pressure floor: with
+    tmp_floor = 1 the low-pressure side (p = 0.1 < 1 * rho) is healed, which
+    changes the energy of the very first conversion."""
+    meta, g = G.load("shock_floor")
+    m = _mesh(meta)
+    m.init_problem("shock", meta["seed"])
+    u0, _ = m.get_state()
+    m.step(1)
+    u1, _ = m.get_state()
+    right = u0[..., 0] < 0.5                     # rho ~ 0.125 half
+    e_floor = u0[..., 0][right] * 1.0 / (meta["gamma"] - 1)
+    # after one step the right half's internal energy sits near the floor value
+    assert np.median(u1[..., 1][right] / e_floor) > 0.9
+
+
+def test_hllc_symmetry():
+    """Mirror symmetry of the restated HLLC: swapping left/right and flipping the
+    normal velocity negates the mass and energy fluxes."""
+    from oracle import kr_oracle as K
+    rng = np.random.default_rng(0)
+    for _ in range(50):
+        ql = np.array([rng.uniform(.1, 2), rng.uniform(.1, 2), *rng.uniform(-1, 1, 3)])
+        qr = np.array([rng.uniform(.1, 2), rng.uniform(.1, 2), *rng.uniform(-1, 1, 3)])
+        f = K.hllc(ql, qr, 0, 1.4)
+        ml, mr = qr.copy(), ql.copy()
+        ml[2] *= -1
+        mr[2] *= -1
+        g = K.hllc(ml, mr, 0, 1.4)
+        np.testing.assert_allclose(g[0], -f[0], rtol=1e-12, atol=1e-14)
+        np.testing.assert_allclose(g[1], -f[1], rtol=1e-12, atol=1e-14)
+        np.testing.assert_allclose(g[2], f[2], rtol=1e-12, atol=1e-14)
+
+
+def test_hlld_consistency():
+    """For identical left and right states the HLLD flux is the physical flux
+    (consistency), with the normal B flux zero and the transverse ones remapped
+    to the edge EMF E = -v x B."""
+    from oracle import kr_oracle as K
+    rng = np.random.default_rng(1)
+    gam = 5 / 3
+    for _ in range(50):
+        q = np.array([rng.uniform(.2, 2), rng.uniform(.2, 2), *rng.uniform(-1, 1, 3),
+                      *rng.uniform(-1, 1, 3)])
+        f = K.hlld(q, q, 0, gam)
+        rho, p, v, b = q[0], q[1], q[2:5], q[5:8]
+        pt = p + 0.5 * b @ b
+        e = p / (gam - 1) + 0.5 * rho * v @ v + 0.5 * b @ b
+        np.testing.assert_allclose(f[0], rho * v[0], rtol=1e-12, atol=1e-13)
+        np.testing.assert_allclose(f[1], (e + pt) * v[0] - b[0] * (v @ b), rtol=1e-12, atol=1e-13)
+        np.testing.assert_allclose(f[2], rho * v[0] ** 2 + pt - b[0] ** 2, rtol=1e-12, atol=1e-13)
+        ez = -(v[0] * b[1] - v[1] * b[0])
+        ey = -(v[2] * b[0] - v[0] * b[2])
+        assert f[5] == 0
+        np.testing.assert_allclose(f[6], ey, rtol=1e-12, atol=1e-13)
+        np.testing.assert_allclose(f[7], ez, rtol=1e-12, atol=1e-13)
