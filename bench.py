@@ -1,0 +1,295 @@
+"""Benchmark of the hydro / ideal-MHD step on B200.
+
+Workload (one GPU): 3-D ideal MHD on a 256^3 periodic mesh split into 64 blocks
+of 64^3, gamma = 5/3, PLM + HLLD + CT, Heun RK2, Orszag-Tang-type vortex with
+seeded 1e-3 velocity noise (synthetic, seeded; no dataset involved).  A "step" is
+one Heun step over the whole mesh.  The state (1.6 GB) is larger than L2, so no
+flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--modes fp64,mixed]
+
+Prints one JSON line (rank 0).  `value` is whole-job zone-cycles/s of the
+headline mode; every measured mode is listed under "modes".
+"""
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "zone-cycles/s, 256³ MHD: learned FP32/64 vs plain FP64 HLLD at stated L1 error"
+UNIT = "zone-cycles/s"
+NB, N = (4, 4, 4), (64, 64, 64)
+GAMMA = 5.0 / 3.0
+SEED = 2
+# algorithmic bytes: 8 FP64 state words (5 conserved + 3 face B) x 5 transfers
+BYTES_PER_ZONE_CYCLE = 320
+WORKLOAD = "ot 256^3 periodic MHD, 64 blocks of 64^3, PLM+HLLD+CT, Heun RK2"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--modes", default="fp64,mixed")
+    return p.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples SM clock and throttle reasons with NVML while running."""
+
+    def __init__(self, index):
+        self.index, self.samples, self.reasons = index, [], set()
+        self.max_mhz, self._stop = None, threading.Event()
+
+    def __enter__(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.nv = pynvml
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+        except Exception:
+            self.nv = None
+        return self
+
+    def _run(self):
+        nv = self.nv
+        names = {
+            getattr(nv, "nvmlClocksEventReasonHwSlowdown", 0x8): "hw_slowdown",
+            getattr(nv, "nvmlClocksEventReasonHwThermalSlowdown", 0x40): "hw_thermal_slowdown",
+            getattr(nv, "nvmlClocksEventReasonSwThermalSlowdown", 0x20): "sw_thermal_slowdown",
+            getattr(nv, "nvmlClocksEventReasonSwPowerCap", 0x4): "sw_power_cap",
+        }
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for bit, name in names.items():
+                    if r & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.05)
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self.nv is not None:
+            self.t.join(timeout=1)
+
+    def summary(self):
+        s = sorted(self.samples)
+        med = s[len(s) // 2] if s else None
+        return {"sm_mhz": med, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                "samples": len(s)}
+
+
+# --------------------------------------------------------------------------- CPU
+def run_reference_cpu(steps, nb=(2, 2, 2), n=(64, 64, 64), threads=None):
+    """Time the original Kratos solver (its CPU path, built from source into
+    oracle/_ref/kratos_ref) on an OT mesh; returns (zone-cycles/s, cores) from
+    its own `Speed = ... cell/s` line (cycle.cpp:184-190)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "kratos_ref")
+    if not os.path.exists(exe):
+        return None
+    threads = threads or os.cpu_count()
+    with tempfile.TemporaryDirectory() as tmp:
+        par = os.path.join(tmp, "b.par")
+        ng = [nb[a] * n[a] for a in range(3)]
+        with open(par, "w") as f:
+            f.write("\n".join([
+                "[problem]", "name = ot", "seed = %d" % SEED, "[mesh]", "x_min = 0 0 0", "x_max = 1 1 1",
+                "n_cell_global = %d %d %d" % tuple(ng), "n_cell_block = %d %d %d" % tuple(n),
+                "[cycle]", "prefix_output = %s/s" % tmp, "n_cycle_lim = %d" % (steps - 1),
+                "final_output = 0", "t_output_next = 1e99", "n_display_freq = 1000000",
+                "[dynamics]", "gamma = %r" % GAMMA, "thread_limit = 1", "bnd_thread_limit = 1",
+                "[boundary]", "kinds = per per per per per per", ""]))
+        env = dict(os.environ, KR_REF_THREADS=str(threads))
+        out = subprocess.run([exe, par], cwd=tmp, env=env, capture_output=True, text=True, timeout=1200)
+    m = re.search(r"Speed = ([0-9.eE+-]+) cell/s", out.stdout)
+    if not m:
+        return None
+    return float(m.group(1)), threads
+
+
+def run_oracle_cpu(steps, nb=(2, 2, 2), n=(64, 64, 64)):
+    from oracle.kr_oracle import OracleMesh
+    o = OracleMesh(True, nb, n, GAMMA)
+    o.init_problem("ot", SEED)
+    t0 = time.perf_counter()
+    o.step(steps)
+    dt = time.perf_counter() - t0
+    return nb[0] * nb[1] * nb[2] * n[0] * n[1] * n[2] * steps / dt, os.cpu_count()
+
+
+def cpu_baseline(steps=2):
+    r = run_reference_cpu(steps)
+    sample = "%d Heun steps of a 128^3 OT mesh (8 blocks of 64^3), PRECISION=2" % steps
+    if r is not None:
+        return {"value": r[0], "unit": UNIT, "cores": r[1], "kind": "reference",
+                "sample": sample + ", original Kratos CPU path (HIP-CPU mode) built from source"}
+    v, cores = run_oracle_cpu(steps)
+    return {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": sample + ", CPU restatement (oracle/)"}
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    steps = max(1, args.steps + args.warmup)
+    r = run_reference_cpu(steps)
+    if r is not None:
+        kind, v, cores = "reference", r[0], r[1]
+    else:
+        kind = "port"
+        v, cores = run_oracle_cpu(steps)
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD.replace("256^3", "128^3 sample of the"),
+                       "mesh_sample": "128^3 = 8 blocks of 64^3 (same block shape)"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
+                             "sample": "%d Heun steps of a 128^3 OT mesh (8 blocks of 64^3)" % steps},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------- GPU
+MODES = {"fp64": dict(precision=2, riemann=0), "mixed": dict(precision=1, riemann=0),
+         "hlle_mixed": dict(precision=1, riemann=1)}
+
+
+def time_mode(mode, args, local_rank, world, dist):
+    import torch
+    from kratos_b200 import Dynamics
+    d = Dynamics(True, NB, N, gamma=GAMMA, device=local_rank, **MODES[mode])
+    stream = torch.cuda.Stream(device=local_rank)
+    d.set_stream(stream.cuda_stream)
+    d.init_problem("ot", SEED)
+    d.step(args.warmup)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        t0.record(stream)
+        d.step(args.steps)
+        t1.record(stream)
+        torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    ms = t0.elapsed_time(t1)
+    if dist is not None:
+        x = torch.tensor([ms], device="cuda:%d" % local_rank)
+        dist.all_reduce(x, op=dist.ReduceOp.MAX)
+        ms = float(x.item())
+    if d.status() != 0:
+        raise RuntimeError("device status %d in mode %s" % (d.status(), mode))
+    zcs = d.n_cells * args.steps / (ms * 1e-3) * world
+    prof = d.profile_step()
+    out = {"value": zcs, "ms_per_step": ms / args.steps, "clocks": clk.summary(),
+           "kernels_ms_per_step": prof, "launches_per_step": d.launches_per_step()}
+    # end-to-end through the C ABI with host buffers: upload the state from pinned
+    # host memory, run the steps, read the state back, all inside the timed region
+    import numpy as np
+    u, bf = d.get_state()
+    hu = torch.from_numpy(u).pin_memory().numpy()
+    hb = torch.from_numpy(bf).pin_memory().numpy()
+    e2e_steps = args.steps
+    torch.cuda.synchronize()
+    w0 = time.perf_counter()
+    d.set_state(hu, hb)
+    d.step(e2e_steps)
+    d.get_state(hu, hb)
+    w1 = time.perf_counter()
+    out["e2e"] = {"value": d.n_cells * e2e_steps / (w1 - w0) * world, "unit": UNIT,
+                  "h2d_bytes_per_step": d.state_bytes() // e2e_steps,
+                  "d2h_bytes_per_step": d.state_bytes() // e2e_steps}
+    out["n_cells"] = d.n_cells
+    del np
+    d.close()
+    return out
+
+
+def main():
+    args = parse()
+    rank, world, local_rank = dist_env()
+    if args.impl == "reference":
+        return reference_arm(args, rank, world)
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as tdist
+        torch.cuda.set_device(local_rank)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    torch.cuda.set_device(local_rank)
+    results = {}
+    for mode in [m for m in args.modes.split(",") if m]:
+        results[mode] = time_mode(mode, args, local_rank, world, dist)
+    head = "mixed" if "mixed" in results else next(iter(results))
+    h = results[head]
+    peak, peak_kind = measured_peaks()
+    flux_ms = h["kernels_ms_per_step"]["flux_x"] + h["kernels_ms_per_step"]["flux_y"] + h["kernels_ms_per_step"]["flux_z"]
+    kernels = h["kernels_ms_per_step"]
+    top = max(kernels, key=kernels.get)
+    step_gbs = h["value"] / world * BYTES_PER_ZONE_CYCLE / 1e9
+    line = {
+        "metric": METRIC, "value": h["value"], "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": h["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32/f64" if head != "fp64" else "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "mode": head, "global_cells": h["n_cells"] * world,
+                   "parallelism": "replica per GPU" if world > 1 else "1 GPU",
+                   "l2": "state 1.6 GB > 126 MB L2; no flush needed"},
+        "modes": {m: {"value": r["value"], "ms_per_step": r["ms_per_step"],
+                      "kernels_ms_per_step": r["kernels_ms_per_step"]} for m, r in results.items()},
+        "roofline": {"bound": "hbm", "achieved": step_gbs, "peak": peak, "unit": "GB/s",
+                     "frac": step_gbs / peak, "traffic": None,
+                     "basis": "whole step: %d B/zone-cycle algorithmic (%s peak); top kernel %s"
+                              % (BYTES_PER_ZONE_CYCLE, peak_kind, top)},
+        "clocks": h["clocks"],
+        "e2e": h["e2e"],
+        "gpu_launches": h["launches_per_step"] * args.steps,
+    }
+    line["flux_ms_per_step"] = flux_ms
+    if rank == 0:
+        try:
+            line["cpu_baseline"] = cpu_baseline()
+        except Exception as e:  # the baseline is reported, never required
+            line["cpu_baseline"] = {"value": None, "error": str(e)}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,123 @@
+/* kratos_b200 -- C ABI of the B200 (sm_100a) hydro / ideal-MHD step.
+ *
+ * The library replaces the device side of Kratos's dynamics module: the
+ * per-stage `integrate` driver that dynamics::base_t::enroll builds
+ * (src/modules/dynamics/dynamics.h:65-117), run once per RK stage by
+ * dynamics::base_t::step (src/modules/dynamics/dynamics.cpp:156-161), together
+ * with the policy kernels it launches:
+ *   cons2prim + CFL dt       hydro/eos/adiabatic.h:211-258, mhd/eos/adiabatic.h:127-234
+ *   ghost fill (same level)  hydro/boundary/comm_functions.h:306-483,
+ *                            mhd/boundary/comm_functions.h:433-815
+ *   PLM + HLLC / HLLD flux   prototypes/integrator.h:107-125 flux_kernel,
+ *                            hydro/reconstruct/plm.h, hydro/riemann/hllc.h,
+ *                            mhd/riemann/hlld.h
+ *   RK2 conserved update     hydro/integrator/integrator.h:241-265, rk2.h:404-425
+ *   CT edge EMF + face B     mhd/integrator/integrator.h:189-462, mhd/integrator/rk2.h
+ *   dt reduction             mesh/cycle/cycle.cpp:77-115
+ * The host side (mesh, parameter files, snapshots, problem generators) calls
+ * it with plain pointers; no torch or CUDA types cross this boundary.
+ *
+ * Conventions
+ *   - Blocks: a uniform mesh of nb[0] x nb[1] x nb[2] blocks of n[0] x n[1] x
+ *     n[2] cells, numbered lexicographically (x fastest).
+ *   - Host state arrays use the reference's per-block layouts (dat_3d_t,
+ *     src/mesh/types/dat_3d.h:153-156, field index fastest):
+ *       u  : [block][n2][n1][n0][nw]   nw = 5 (hydro) or 8 (MHD), no ghosts
+ *       bf : [block][n2+5][n1+5][n0+5][3]  face B on the (n+1)^3 lattice with
+ *            2 ghost layers (as the snapshot's field_bf_field)
+ *   - Return codes: 0 success, negative on error; kr_last_error() describes
+ *     the last error of a context (or of kr_ctx_create when ctx is NULL).
+ *   - Threading: one host thread per context; one context per GPU.
+ */
+#ifndef KRATOS_B200_H
+#define KRATOS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KR_ABI_VERSION 1
+
+/* Riemann solver selection ([b200] riemann). */
+enum kr_riemann_t
+{
+    KR_RIEMANN_DEFAULT = 0,    /* HLLC (hydro) / HLLD (MHD), as the reference     */
+    KR_RIEMANN_HLLE    = 1,    /* two-wave HLLE everywhere (MHD only)            */
+    KR_RIEMANN_LEARNED = 2     /* MLP face selector: HLLE where predicted safe,  */
+                               /* HLLD elsewhere (MHD only)                      */
+};
+
+/* Step configuration.  Physics keys mirror the reference's [dynamics] and
+ * [cycle] parameters (prototypes/eos.h:43-56, cycle.cpp:30-65). */
+typedef struct
+{
+    int    abi_version;        /* KR_ABI_VERSION                                 */
+    int    mhd;                /* 0: hydro (PLM+HLLC), 1: ideal MHD (PLM+HLLD+CT) */
+    int    precision;          /* 2: FP64 throughout; 1: FP32 reconstruction and */
+                               /*    Riemann, FP64 state / CT update / dt / c2p  */
+    int    riemann;            /* enum kr_riemann_t                              */
+    int    nb[ 3 ];            /* blocks per axis                                */
+    int    n [ 3 ];            /* cells per block per axis (each >= 4)           */
+    double x_min[ 3 ], x_max[ 3 ];
+    double gamma, cfl, rho_floor, tmp_floor;
+    double dt_init;            /* [cycle] dt_init (0: unset)                     */
+    double dt_expand;          /* [cycle] dt_expand                              */
+    int    device;             /* CUDA device ordinal                            */
+    int    reserved[ 7 ];
+} kr_cfg;
+
+typedef struct kr_ctx kr_ctx;
+
+/* Fill a configuration with the reference's defaults: gamma 1.66667, cfl 0.3,
+ * floors 1e-9, dt_expand 2, FP64, default Riemann solver, unit cube. */
+void        kr_cfg_default( kr_cfg * cfg );
+
+kr_ctx *    kr_ctx_create ( const kr_cfg * cfg );
+void        kr_ctx_destroy( kr_ctx * ctx );
+const char* kr_last_error ( const kr_ctx * ctx );
+
+/* Optional: run on a caller-owned stream (a cudaStream_t passed as void*). */
+int kr_set_stream( kr_ctx * ctx, void * stream );
+
+/* Seeded workload initial state into the device state (host-built, uploaded):
+ * "shock" (hydro) or "ot" (MHD). */
+int kr_init_problem( kr_ctx * ctx, const char * name, uint64_t seed );
+
+/* Host <-> device state transfers (layouts above).  bf is ignored for hydro.
+ * kr_get_state writes the cell-centred face-averaged B into u's slots 5..7. */
+int kr_set_state( kr_ctx * ctx, const double * u, const double * bf );
+int kr_get_state( kr_ctx * ctx, double * u, double * bf );
+
+/* Advance n_steps Heun steps on the device (enqueued; returns without waiting).
+ * Time and dt stay on the device until kr_get_time. */
+int kr_step( kr_ctx * ctx, int n_steps );
+
+/* Wait for the context's stream; read time, last dt, next dt bound, steps. */
+int kr_get_time( kr_ctx * ctx, double * t, double * dt_last, double * dt_bound,
+                 long long * n_steps_done );
+/* Set time and the dt bound the next step starts from (restart). */
+int kr_set_time( kr_ctx * ctx, double t, double dt_bound );
+
+/* Sticky device status word: 0 ok; bit 0 non-finite or non-positive dt. */
+int kr_status( kr_ctx * ctx );
+
+/* Number of kernel launches kr_step enqueues per step (instrumentation). */
+int kr_launches_per_step( kr_ctx * ctx );
+
+/* Run one step eagerly (outside the captured graph) with CUDA events around
+ * every kernel and return the step's milliseconds per kernel kind in ms[0..6]:
+ * c2p, ghost, flux z, flux y, flux x, emf, update (both stages summed).
+ * The step advances the state like kr_step.  n_kinds must be >= 7. */
+int kr_profile_step( kr_ctx * ctx, int n_kinds, double * ms );
+
+/* Diagnostics on the device state: max |div B| over owned cells (MHD) and the
+ * domain totals of mass, momentum and energy (5 doubles). */
+int kr_diagnostics( kr_ctx * ctx, double * max_div_b, double * totals5 );
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,74 @@
+"""ctypes binding of the C ABI in include/kratos_b200.h (libkrb200.so)."""
+import ctypes
+import os
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libkrb200.so")
+
+KR_ABI_VERSION = 1
+KR_RIEMANN_DEFAULT, KR_RIEMANN_HLLE, KR_RIEMANN_LEARNED = 0, 1, 2
+
+
+class kr_cfg(ctypes.Structure):
+    _fields_ = [
+        ("abi_version", ctypes.c_int),
+        ("mhd", ctypes.c_int),
+        ("precision", ctypes.c_int),
+        ("riemann", ctypes.c_int),
+        ("nb", ctypes.c_int * 3),
+        ("n", ctypes.c_int * 3),
+        ("x_min", ctypes.c_double * 3),
+        ("x_max", ctypes.c_double * 3),
+        ("gamma", ctypes.c_double),
+        ("cfl", ctypes.c_double),
+        ("rho_floor", ctypes.c_double),
+        ("tmp_floor", ctypes.c_double),
+        ("dt_init", ctypes.c_double),
+        ("dt_expand", ctypes.c_double),
+        ("device", ctypes.c_int),
+        ("reserved", ctypes.c_int * 7),
+    ]
+
+
+# name -> (restype, argtypes); every symbol include/kratos_b200.h declares
+_dp = ctypes.POINTER(ctypes.c_double)
+_vp = ctypes.c_void_p
+SIGNATURES = {
+    "kr_cfg_default": (None, [ctypes.POINTER(kr_cfg)]),
+    "kr_ctx_create": (_vp, [ctypes.POINTER(kr_cfg)]),
+    "kr_ctx_destroy": (None, [_vp]),
+    "kr_last_error": (ctypes.c_char_p, [_vp]),
+    "kr_set_stream": (ctypes.c_int, [_vp, _vp]),
+    "kr_init_problem": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_uint64]),
+    "kr_set_state": (ctypes.c_int, [_vp, _vp, _vp]),
+    "kr_get_state": (ctypes.c_int, [_vp, _vp, _vp]),
+    "kr_step": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "kr_get_time": (ctypes.c_int, [_vp, _dp, _dp, _dp, ctypes.POINTER(ctypes.c_longlong)]),
+    "kr_set_time": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double]),
+    "kr_status": (ctypes.c_int, [_vp]),
+    "kr_launches_per_step": (ctypes.c_int, [_vp]),
+    "kr_profile_step": (ctypes.c_int, [_vp, ctypes.c_int, _dp]),
+    "kr_diagnostics": (ctypes.c_int, [_vp, _dp, _dp]),
+}
+
+_lib = None
+
+
+class EngineMissing(RuntimeError):
+    pass
+
+
+def lib():
+    """Load libkrb200.so.  There is no fallback: without the compiled engine
+    every entry point raises."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise EngineMissing("%s is missing; build it with `python -m kratos_b200.build`" % LIB_PATH)
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib

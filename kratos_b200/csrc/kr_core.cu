@@ -1,0 +1,1177 @@
+// kratos_b200 device engine: storage, kernels and the C ABI of
+// include/kratos_b200.h.
+//
+// HBM layout (one pool per array, blocks back to back, component-major within
+// a block, x fastest -- every kernel below maps consecutive threads to
+// consecutive x, so all global traffic is coalesced):
+//   U [slot][block][5][n2][n1][n0]           conserved rho, E, m0..2 (double)
+//   BF[slot][block][3][n2+5][n1+5][n0+5]     face B, 2 ghost layers (double)
+//   W [block][nw][n2+4][n1+4][n0+4]          primitives, 2 ghost layers (R)
+//   F [axis][block][nf][n2+3][n1+3][n0+3]    face fluxes, 1 ghost layer (R);
+//                                            nf = 5 hydro, 7 MHD (5 + edge E)
+//   EE[block][3][n2+3][n1+3][n0+3]           edge EMF (R)
+// R is double for the FP64 step and float for the mixed step.  One Heun step
+// is 2 x (c2p, ghost, flux z, flux y, flux x, [emf], update) plus two scalar
+// kernels, captured once into a CUDA graph and replayed.
+#include "../../include/kratos_b200.h"
+#include "kr_math.cuh"
+#include "problems.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace kr
+{
+////////////////////////////////////////////////////////////
+// Device-side scalars of the time loop (cycle.cpp:77-115 semantics)
+
+struct scal_t
+{
+    unsigned long long dt_bits;   // running CFL minimum (positive double bits)
+    double dt_bound;              // value a step's minimum starts from
+    double dt_last;               // dt of the last completed step
+    double t;
+    long long n_steps;
+    int status;                   // sticky error bits
+    int heal_count;               // floor corrections (diagnostic)
+};
+
+struct geo_t
+{
+    double dx[ 3 ], sfc[ 3 ], vol;
+};
+
+// Kernel parameters (by value).
+template< class R >
+struct args_t
+{
+    int n0, n1, n2, nblk;
+    long long nc, ngw, nbf, nfb;      // per-component sizes: U, W, BF, F/EE
+    int sw1, sw2, sb1, sb2, sf1, sf2; // strides of W, BF, F/EE boxes
+    double gamma, cfl, d_floor, t_floor, dt_expand;
+    double * u[ 2 ];
+    double * bf[ 2 ];
+    R * w;
+    R * f[ 3 ];
+    R * ee;
+    const geo_t * geo;
+    const int * nbr;                  // [block][27]
+    scal_t * s;
+};
+
+template< class R > __device__ __forceinline__
+long long iw( const args_t< R > & a, int b, int c, int nw, int i0, int i1, int i2 )
+{
+    return ( long long )( b * nw + c ) * a.ngw + ( i0 + 2 ) + a.sw1 * ( i1 + 2 ) + a.sw2 * ( i2 + 2 );
+}
+template< class R > __device__ __forceinline__
+long long iuc( const args_t< R > & a, int b, int c, int i0, int i1, int i2 )
+{
+    return ( long long )( b * 5 + c ) * a.nc + i0 + a.n0 * ( i1 + a.n1 * i2 );
+}
+template< class R > __device__ __forceinline__
+long long ibf( const args_t< R > & a, int b, int c, int i0, int i1, int i2 )
+{
+    return ( long long )( b * 3 + c ) * a.nbf + ( i0 + 2 ) + a.sb1 * ( i1 + 2 ) + a.sb2 * ( i2 + 2 );
+}
+template< class R > __device__ __forceinline__
+long long ifx( const args_t< R > & a, int b, int c, int nf, int i0, int i1, int i2 )
+{
+    return ( long long )( b * nf + c ) * a.nfb + ( i0 + 1 ) + a.sf1 * ( i1 + 1 ) + a.sf2 * ( i2 + 1 );
+}
+
+__device__ __forceinline__ double warp_min( double v )
+{
+    for( int o = 16; o > 0; o >>= 1 )
+        v = fmin( v, __shfl_xor_sync( 0xffffffffu, v, o ) );
+    return v;
+}
+
+////////////////////////////////////////////////////////////
+// Scalars: step begin / end (cycle.cpp:77-115)
+
+__global__ void k_step_begin( scal_t * s )
+{
+    s->dt_bits = __double_as_longlong( s->dt_bound );
+}
+
+__global__ void k_step_end( scal_t * s, double dt_expand )
+{
+    const double dt = __longlong_as_double( s->dt_bits );
+    if( ! ( dt > 0 ) || ! isfinite( dt ) )
+        s->status |= 1;
+    s->dt_last  = dt;
+    s->t       += dt;
+    s->dt_bound = dt * dt_expand;
+    s->n_steps += 1;
+}
+
+////////////////////////////////////////////////////////////
+// cons -> prim over the interior of every block, CFL dt at stage 0
+// (hydro/eos/adiabatic.h:211-258; mhd/eos/adiabatic.h:127-234).
+
+template< bool MHD, class R >
+__global__ void __launch_bounds__( 256 ) k_c2p( const args_t< R > a, int step )
+{
+    constexpr int NW = MHD ? 8 : 5;
+    const int b = blockIdx.y;
+    const long long c = ( long long ) blockIdx.x * blockDim.x + threadIdx.x;
+    double dt = FLT_MAX;
+    if( c < a.nc )
+    {
+        const int i0 = int( c % a.n0 );
+        const int i1 = int( ( c / a.n0 ) % a.n1 );
+        const int i2 = int( c / ( ( long long ) a.n0 * a.n1 ) );
+        double * U = a.u[ step ];
+        double cons[ 5 ], cout[ 5 ], prim[ 5 ];
+        for( int k = 0; k < 5; ++ k )
+            cons[ k ] = U[ iuc( a, b, k, i0, i1, i2 ) ];
+        double bc[ 3 ], bc_2[ 3 ], b_max[ 3 ], e_m = 0;
+        if( MHD )
+        {
+            const double * BF = a.bf[ step ];
+            const int ii[ 3 ] = { i0, i1, i2 };
+            for( int d = 0; d < 3; ++ d )
+            {
+                int jj[ 3 ] = { ii[ 0 ], ii[ 1 ], ii[ 2 ] };
+                const double b_l = BF[ ibf( a, b, d, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) ];
+                ++ jj[ d ];
+                const double b_r = BF[ ibf( a, b, d, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) ];
+                const double bc_m = ( b_l + b_r ) / 2;
+                bc[ d ] = bc_m;
+                bc_2[ d ] = bc_m * bc_m;
+                e_m += bc_2[ d ];
+                b_max[ d ] = fmax( fabs( b_l ), fabs( b_r ) );
+            }
+            e_m /= 2;
+            cons[ ENE ] -= e_m;
+        }
+        double cs2;
+        const int healed = c2p( cons, prim, cout, a.gamma, a.d_floor, a.t_floor, cs2 );
+        if( healed )
+        {
+            U[ iuc( a, b, RHO, i0, i1, i2 ) ] = cout[ RHO ];
+            U[ iuc( a, b, ENE, i0, i1, i2 ) ] = MHD ? cout[ ENE ] + e_m : cout[ ENE ];
+            atomicAdd( & a.s->heal_count, 1 );
+        }
+        for( int k = 0; k < 5; ++ k )
+            a.w[ iw( a, b, k, NW, i0, i1, i2 ) ] = R( prim[ k ] );
+        if( MHD )
+            for( int d = 0; d < 3; ++ d )
+                a.w[ iw( a, b, BCC + d, NW, i0, i1, i2 ) ] = R( bc[ d ] );
+        if( step == 0 )
+        {
+            const geo_t & g = a.geo[ b ];
+            if( ! MHD )
+            {
+                const double cs = sqrt( cs2 );
+                for( int d = 0; d < 3; ++ d )
+                    dt = fmin( dt, g.dx[ d ] / ( cs + fabs( prim[ MOM + d ] ) ) );
+            }
+            else
+            {
+                double bm_2[ 3 ] = { bc_2[ 0 ], bc_2[ 1 ], bc_2[ 2 ] };
+                for( int d = 0; d < 3; ++ d )
+                {
+                    bm_2[ d ] = b_max[ d ] * b_max[ d ];
+                    const double cf = c_fms< double >( prim, bm_2, a.gamma, d );
+                    dt = fmin( dt, g.dx[ d ] / ( cf + fabs( prim[ MOM + d ] ) ) );
+                    bm_2[ d ] = bc_2[ d ];
+                }
+            }
+            dt *= a.cfl;
+        }
+    }
+    if( step == 0 )
+    {
+        __shared__ double red[ 8 ];
+        dt = warp_min( dt );
+        if( ( threadIdx.x & 31 ) == 0 )
+            red[ threadIdx.x >> 5 ] = dt;
+        __syncthreads(  );
+        if( threadIdx.x < 32 )
+        {
+            dt = threadIdx.x < ( blockDim.x >> 5 ) ? red[ threadIdx.x ] : FLT_MAX;
+            dt = warp_min( dt );
+            if( threadIdx.x == 0 )
+                atomicMin( & a.s->dt_bits, ( unsigned long long ) __double_as_longlong( dt ) );
+        }
+    }
+}
+
+////////////////////////////////////////////////////////////
+// Ghost fill between same-level blocks: every ghost cell of W and every
+// non-owned slot of BF takes the value held by the block that owns it.
+
+__device__ __forceinline__ int wrap_axis( int i, int n, int & sh )
+{
+    if( i < 0 )  { sh = -1; return i + n; }
+    if( i >= n ) { sh = +1; return i - n; }
+    sh = 0;
+    return i;
+}
+
+template< bool MHD, class R >
+__global__ void __launch_bounds__( 256 ) k_ghost( const args_t< R > a, int step )
+{
+    constexpr int NW = MHD ? 8 : 5;
+    const int b = blockIdx.y;
+    const long long t = ( long long ) blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nbox_w = a.ngw;
+    if( t < nbox_w )
+    {
+        const int i0 = int( t % a.sw1 ) - 2;
+        const int i1 = int( ( t / a.sw1 ) % ( a.n1 + 4 ) ) - 2;
+        const int i2 = int( t / a.sw2 ) - 2;
+        int s0, s1, s2;
+        const int j0 = wrap_axis( i0, a.n0, s0 );
+        const int j1 = wrap_axis( i1, a.n1, s1 );
+        const int j2 = wrap_axis( i2, a.n2, s2 );
+        if( s0 | s1 | s2 )
+        {
+            const int src = a.nbr[ b * 27 + ( s0 + 1 ) + 3 * ( s1 + 1 ) + 9 * ( s2 + 1 ) ];
+            for( int k = 0; k < NW; ++ k )
+                a.w[ iw( a, b, k, NW, i0, i1, i2 ) ] = a.w[ iw( a, src, k, NW, j0, j1, j2 ) ];
+        }
+    }
+    if( ! MHD )
+        return;
+    if( t < a.nbf )
+    {
+        double * BF = a.bf[ step ];
+        const int i0 = int( t % a.sb1 ) - 2;
+        const int i1 = int( ( t / a.sb1 ) % ( a.n1 + 5 ) ) - 2;
+        const int i2 = int( t / a.sb2 ) - 2;
+        const int ii[ 3 ] = { i0, i1, i2 };
+        const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
+        for( int c = 0; c < 3; ++ c )
+        {
+            bool own = true;
+            int sh[ 3 ], jj[ 3 ];
+            for( int d = 0; d < 3; ++ d )
+            {
+                if( d == c )
+                {
+                    own = own && ii[ d ] >= 0 && ii[ d ] <= nn[ d ];
+                    if( ii[ d ] < 0 )           { sh[ d ] = -1; jj[ d ] = ii[ d ] + nn[ d ]; }
+                    else if( ii[ d ] > nn[ d ] ) { sh[ d ] = +1; jj[ d ] = ii[ d ] - nn[ d ]; }
+                    else                         { sh[ d ] = 0;  jj[ d ] = ii[ d ]; }
+                }
+                else
+                {
+                    own = own && ii[ d ] >= 0 && ii[ d ] < nn[ d ];
+                    jj[ d ] = wrap_axis( ii[ d ], nn[ d ], sh[ d ] );
+                }
+            }
+            if( own )
+                continue;
+            const int src = a.nbr[ b * 27 + ( sh[ 0 ] + 1 ) + 3 * ( sh[ 1 ] + 1 ) + 9 * ( sh[ 2 ] + 1 ) ];
+            BF[ ibf( a, b, c, i0, i1, i2 ) ] = BF[ ibf( a, src, c, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) ];
+        }
+    }
+}
+
+////////////////////////////////////////////////////////////
+// Face fluxes along one axis: PLM + HLLC / HLLD / HLLE per face.
+// One thread per face; consecutive threads take consecutive x.  MHD also covers
+// the transverse ghost lines that the corner EMF reads
+// (mhd/integrator/integrator.h:138-168, mhd/integrator/data.h:106-144).
+
+template< bool MHD, class R >
+__global__ void __launch_bounds__( 128 ) k_flux( const args_t< R > a, int axis, int step, int rsel )
+{
+    constexpr int NW = MHD ? 8 : 5;
+    constexpr int NF = MHD ? 7 : 5;
+    const int b = blockIdx.y;
+    const int lo = MHD ? -1 : 0;
+    const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
+    int ext[ 3 ];
+    for( int d = 0; d < 3; ++ d )
+        ext[ d ] = d == axis ? nn[ d ] + 1 : nn[ d ] - 2 * lo;
+    const long long t = ( long long ) blockIdx.x * blockDim.x + threadIdx.x;
+    if( t >= ( long long ) ext[ 0 ] * ext[ 1 ] * ext[ 2 ] )
+        return;
+    int ii[ 3 ];
+    ii[ 0 ] = int( t % ext[ 0 ] );
+    ii[ 1 ] = int( ( t / ext[ 0 ] ) % ext[ 1 ] );
+    ii[ 2 ] = int( t / ( ( long long ) ext[ 0 ] * ext[ 1 ] ) );
+    int outside = 0;
+    for( int d = 0; d < 3; ++ d )
+        if( d != axis )
+        {
+            ii[ d ] += lo;
+            outside += ( ii[ d ] < 0 || ii[ d ] >= nn[ d ] );
+        }
+    if( outside > 1 )
+        return;                                  // corner line: never read
+    const int st = axis == 0 ? 1 : ( axis == 1 ? a.sw1 : a.sw2 );
+    R ql[ 8 ], qr[ 8 ], flx[ 8 ];
+    for( int k = 0; k < NW; ++ k )
+    {
+        if( MHD && k == BCC + axis )
+        {
+            const R bn = R( a.bf[ step ][ ibf( a, b, axis, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] );
+            ql[ k ] = qr[ k ] = bn;
+            continue;
+        }
+        const R * p = a.w + iw( a, b, k, NW, ii[ 0 ], ii[ 1 ], ii[ 2 ] );
+        plm_face< R >( p[ -2 * st ], p[ -st ], p[ 0 ], p[ st ], ql[ k ], qr[ k ] );
+    }
+    const R gam = R( a.gamma );
+    idx_swap( ql + MOM, axis );
+    idx_swap( qr + MOM, axis );
+    if( ! MHD )
+        hllc_eval< R >( flx, ql, qr, gam );
+    else
+    {
+        idx_swap( ql + BCC, axis );
+        idx_swap( qr + BCC, axis );
+        if( rsel == KR_RIEMANN_HLLE )
+            hlle_eval< R >( flx, ql, qr, gam );
+        else
+            hlld_eval< R >( flx, ql, qr, gam );
+    }
+    idx_swap( flx + MOM, 3 - axis );
+    R * F = a.f[ axis ];
+    for( int k = 0; k < 5; ++ k )
+        F[ ifx( a, b, k, NF, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] = flx[ k ];
+    if( MHD )
+    {   // mhd/riemann/hlld.h:42-46: B flux -> edge EMF.  Slot 5 holds
+        // E_{(axis+1)%3}, slot 6 holds E_{(axis+2)%3}.
+        F[ ifx( a, b, 5, NF, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] =  flx[ BCC + 2 ];
+        F[ ifx( a, b, 6, NF, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] = -flx[ BCC + 1 ];
+    }
+}
+
+////////////////////////////////////////////////////////////
+// Edge EMF (mhd/integrator/integrator.h:189-327 calc_field): face EMF average
+// plus the upwinded corner terms chosen by the sign of the mass flux.
+
+template< class R > __device__ __forceinline__
+R e_cell( const args_t< R > & a, int b, const int * j, int ax )
+{
+    const int ax1 = mod3( ax + 1 ), ax2 = mod3( ax + 2 );
+    const R b1 = a.w[ iw( a, b, BCC + ax1, 8, j[ 0 ], j[ 1 ], j[ 2 ] ) ];
+    const R b2 = a.w[ iw( a, b, BCC + ax2, 8, j[ 0 ], j[ 1 ], j[ 2 ] ) ];
+    const R v1 = a.w[ iw( a, b, MOM + ax1, 8, j[ 0 ], j[ 1 ], j[ 2 ] ) ];
+    const R v2 = a.w[ iw( a, b, MOM + ax2, 8, j[ 0 ], j[ 1 ], j[ 2 ] ) ];
+    return b1 * v2 - b2 * v1;
+}
+
+template< class R > __device__ __forceinline__
+R face_emf( const args_t< R > & a, int b, int fa, int ax, const int * i )
+{   // E_ax held by the flux of axis fa
+    const int slot = ( ax == mod3( fa + 1 ) ) ? 5 : 6;
+    return a.f[ fa ][ ifx( a, b, slot, 7, i[ 0 ], i[ 1 ], i[ 2 ] ) ];
+}
+
+template< class R >
+__global__ void __launch_bounds__( 256 ) k_emf( const args_t< R > a )
+{
+    const int b = blockIdx.y;
+    const int e0 = a.n0 + 1, e1 = a.n1 + 1;
+    const long long t = ( long long ) blockIdx.x * blockDim.x + threadIdx.x;
+    if( t >= ( long long ) e0 * e1 * ( a.n2 + 1 ) )
+        return;
+    int i[ 3 ] = { int( t % e0 ), int( ( t / e0 ) % e1 ), int( t / ( ( long long ) e0 * e1 ) ) };
+    const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
+    const R w_e = R( 0.25f );
+    for( int ax = 0; ax < 3; ++ ax )
+    {
+        if( i[ ax ] >= nn[ ax ] )
+            continue;
+        const int ax1 = mod3( 1 + ax ), ax2 = mod3( 2 + ax );
+        R ec[ 2 ][ 2 ];
+        ec[ 1 ][ 1 ] = e_cell( a, b, i, ax );
+        -- i[ ax1 ];
+        ec[ 1 ][ 0 ] = e_cell( a, b, i, ax );
+        -- i[ ax2 ];
+        ec[ 0 ][ 0 ] = e_cell( a, b, i, ax );
+        ++ i[ ax1 ];
+        ec[ 0 ][ 1 ] = e_cell( a, b, i, ax );
+        ++ i[ ax2 ];
+        R e = 0;
+        for( int it = 0; it < 2; ++ it )
+        {
+            const int a_para = it == 0 ? ax1 : ax2;
+            const int a_perp = it == 0 ? ax2 : ax1;
+            -- i[ a_perp ];
+            const R ef_m = face_emf( a, b, a_para, ax, i );
+            ++ i[ a_perp ];
+            const R ef_p = face_emf( a, b, a_para, ax, i );
+            e += w_e * ( ef_m + ef_p );
+            const R frho_p = a.f[ a_perp ][ ifx( a, b, RHO, 7, i[ 0 ], i[ 1 ], i[ 2 ] ) ];
+            -- i[ a_para ];
+            const R frho_m = a.f[ a_perp ][ ifx( a, b, RHO, 7, i[ 0 ], i[ 1 ], i[ 2 ] ) ];
+            ++ i[ a_para ];
+            const R de_p = frho_p > 0 ?  ( ec[ 0 ][ 1 ] - ef_m ) :  ( ec[ 1 ][ 1 ] - ef_p );
+            const R de_m = frho_m > 0 ? -( ec[ 0 ][ 0 ] - ef_m ) : -( ec[ 1 ][ 0 ] - ef_p );
+            e += w_e * ( de_m - de_p );
+            if( it == 0 )
+            {
+                const R swp = ec[ 0 ][ 1 ];
+                ec[ 0 ][ 1 ] = ec[ 1 ][ 0 ];
+                ec[ 1 ][ 0 ] = swp;
+            }
+        }
+        a.ee[ ifx( a, b, ax, 3, i[ 0 ], i[ 1 ], i[ 2 ] ) ] = e;
+    }
+}
+
+////////////////////////////////////////////////////////////
+// Conserved update (hydro/integrator/integrator.h:241-265 add_flux with
+// rk2.h:404-425 load) and CT face update (mhd/integrator/integrator.h:385-462,
+// mhd/integrator/rk2.h:244-258 set_field).  One thread per lattice site.
+
+template< bool MHD, class R >
+__global__ void __launch_bounds__( 256 ) k_update( const args_t< R > a, int step )
+{
+    constexpr int NF = MHD ? 7 : 5;
+    const int b = blockIdx.y;
+    const int e0 = a.n0 + 1, e1 = a.n1 + 1;
+    const long long t = ( long long ) blockIdx.x * blockDim.x + threadIdx.x;
+    if( t >= ( long long ) e0 * e1 * ( a.n2 + 1 ) )
+        return;
+    int i[ 3 ] = { int( t % e0 ), int( ( t / e0 ) % e1 ), int( t / ( ( long long ) e0 * e1 ) ) };
+    const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
+    const double dt = __longlong_as_double( a.s->dt_bits ) * ( step == 0 ? 1.0 : double( 0.5f ) );
+    const geo_t & g = a.geo[ b ];
+    if( i[ 0 ] < nn[ 0 ] && i[ 1 ] < nn[ 1 ] && i[ 2 ] < nn[ 2 ] )
+    {
+        const double * us = a.u[ step ];
+        double * ut = a.u[ 1 - step ];
+        const double dt_dv = dt / g.vol;
+        for( int k = 0; k < 5; ++ k )
+        {
+            const long long c = iuc( a, b, k, i[ 0 ], i[ 1 ], i[ 2 ] );
+            double v = step == 0 ? us[ c ] : ( us[ c ] + ut[ c ] ) * 0.5f;
+            for( int d = 0; d < 3; ++ d )
+            {
+                const double f_a = g.sfc[ d ] * dt_dv;
+                int j[ 3 ] = { i[ 0 ], i[ 1 ], i[ 2 ] };
+                const double fl = double( a.f[ d ][ ifx( a, b, k, NF, j[ 0 ], j[ 1 ], j[ 2 ] ) ] );
+                ++ j[ d ];
+                const double fr = double( a.f[ d ][ ifx( a, b, k, NF, j[ 0 ], j[ 1 ], j[ 2 ] ) ] );
+                double res = 0;
+                res += f_a * fl;
+                res -= f_a * fr;
+                v += res;
+            }
+            ut[ c ] = v;
+        }
+    }
+    if( ! MHD )
+        return;
+    const double * bs = a.bf[ step ];
+    double * bt = a.bf[ 1 - step ];
+    for( int c = 0; c < 3; ++ c )
+    {
+        const int ax1 = mod3( c + 1 ), ax2 = mod3( c + 2 );
+        if( i[ ax1 ] >= nn[ ax1 ] || i[ ax2 ] >= nn[ ax2 ] )
+            continue;
+        double db;
+        db  = double( a.ee[ ifx( a, b, ax1, 3, i[ 0 ], i[ 1 ], i[ 2 ] ) ] ) * g.dx[ ax1 ];
+        db -= double( a.ee[ ifx( a, b, ax2, 3, i[ 0 ], i[ 1 ], i[ 2 ] ) ] ) * g.dx[ ax2 ];
+        ++ i[ ax1 ];
+        db += double( a.ee[ ifx( a, b, ax2, 3, i[ 0 ], i[ 1 ], i[ 2 ] ) ] ) * g.dx[ ax2 ];
+        -- i[ ax1 ];
+        ++ i[ ax2 ];
+        db -= double( a.ee[ ifx( a, b, ax1, 3, i[ 0 ], i[ 1 ], i[ 2 ] ) ] ) * g.dx[ ax1 ];
+        -- i[ ax2 ];
+        const double sfc = g.sfc[ c ];
+        db *= ( sfc > 0 ? ( -dt / sfc ) : 0. );
+        const long long k = ibf( a, b, c, i[ 0 ], i[ 1 ], i[ 2 ] );
+        bt[ k ] = db + ( step == 0 ? bs[ k ] : ( bs[ k ] + bt[ k ] ) / 2 );
+    }
+}
+
+////////////////////////////////////////////////////////////
+// Host layout <-> device layout (per-block AoS as in the snapshot).
+
+template< bool MHD, class R >
+__global__ void k_scatter( const args_t< R > a, const double * hu, const double * hbf )
+{
+    constexpr int NWR = MHD ? 8 : 5;
+    const int b = blockIdx.y;
+    const long long t = ( long long ) blockIdx.x * blockDim.x + threadIdx.x;
+    if( t < a.nc )
+        for( int k = 0; k < 5; ++ k )
+            a.u[ 0 ][ ( long long )( b * 5 + k ) * a.nc + t ] = hu[ ( ( long long ) b * a.nc + t ) * NWR + k ];
+    if( MHD && t < a.nbf )
+        for( int c = 0; c < 3; ++ c )
+            a.bf[ 0 ][ ( long long )( b * 3 + c ) * a.nbf + t ] = hbf[ ( ( long long ) b * a.nbf + t ) * 3 + c ];
+}
+
+template< bool MHD, class R >
+__global__ void k_gather( const args_t< R > a, double * hu, double * hbf )
+{
+    constexpr int NWR = MHD ? 8 : 5;
+    const int b = blockIdx.y;
+    const long long t = ( long long ) blockIdx.x * blockDim.x + threadIdx.x;
+    if( t < a.nc )
+    {
+        for( int k = 0; k < 5; ++ k )
+            hu[ ( ( long long ) b * a.nc + t ) * NWR + k ] = a.u[ 0 ][ ( long long )( b * 5 + k ) * a.nc + t ];
+        if( MHD )
+        {
+            const int i0 = int( t % a.n0 ), i1 = int( ( t / a.n0 ) % a.n1 ), i2 = int( t / ( ( long long ) a.n0 * a.n1 ) );
+            const int ii[ 3 ] = { i0, i1, i2 };
+            for( int d = 0; d < 3; ++ d )
+            {
+                int jj[ 3 ] = { ii[ 0 ], ii[ 1 ], ii[ 2 ] };
+                const double bl = a.bf[ 0 ][ ibf( a, b, d, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) ];
+                ++ jj[ d ];
+                const double br = a.bf[ 0 ][ ibf( a, b, d, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) ];
+                hu[ ( ( long long ) b * a.nc + t ) * NWR + BCC + d ] = ( bl + br ) / 2;
+            }
+        }
+    }
+    if( MHD && t < a.nbf )
+        for( int c = 0; c < 3; ++ c )
+            hbf[ ( ( long long ) b * a.nbf + t ) * 3 + c ] = a.bf[ 0 ][ ( long long )( b * 3 + c ) * a.nbf + t ];
+}
+
+////////////////////////////////////////////////////////////
+// Diagnostics: max |div B| (owned cells) and domain totals.
+
+template< bool MHD, class R >
+__global__ void k_diag( const args_t< R > a, double * out )
+{
+    const int b = blockIdx.y;
+    const long long t = ( long long ) blockIdx.x * blockDim.x + threadIdx.x;
+    if( t >= a.nc )
+        return;
+    const int i0 = int( t % a.n0 ), i1 = int( ( t / a.n0 ) % a.n1 ), i2 = int( t / ( ( long long ) a.n0 * a.n1 ) );
+    const geo_t & g = a.geo[ b ];
+    for( int k = 0; k < 5; ++ k )
+        atomicAdd( out + 1 + k, a.u[ 0 ][ iuc( a, b, k, i0, i1, i2 ) ] * g.vol );
+    if( MHD )
+    {
+        const int ii[ 3 ] = { i0, i1, i2 };
+        double div = 0;
+        for( int d = 0; d < 3; ++ d )
+        {
+            int jj[ 3 ] = { ii[ 0 ], ii[ 1 ], ii[ 2 ] };
+            const double bl = a.bf[ 0 ][ ibf( a, b, d, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) ];
+            ++ jj[ d ];
+            const double br = a.bf[ 0 ][ ibf( a, b, d, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) ];
+            div += ( br - bl ) * g.sfc[ d ];
+        }
+        div = fabs( div ) / g.vol;
+        atomicMax( ( unsigned long long * ) out, ( unsigned long long ) __double_as_longlong( div ) );
+    }
+}
+
+}   // namespace kr
+
+////////////////////////////////////////////////////////////
+// Context
+
+using namespace kr;
+
+struct kr_ctx
+{
+    kr_cfg cfg;
+    std::string err;
+    int nblk = 0, nw = 0, nf = 0;
+    long long nc = 0, ngw = 0, nbf = 0, nfb = 0;
+    size_t rsize = 8;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    // device memory
+    double * u[ 2 ] = { nullptr, nullptr };
+    double * bf[ 2 ] = { nullptr, nullptr };
+    void * w = nullptr;
+    void * f[ 3 ] = { nullptr, nullptr, nullptr };
+    void * ee = nullptr;
+    geo_t * geo = nullptr;
+    int * nbr = nullptr;
+    scal_t * s = nullptr;
+    double * stage = nullptr;          // host-layout staging buffer (device)
+    size_t stage_bytes = 0;
+    double * diag = nullptr;
+    // graph of one step
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    cudaStream_t graph_stream = nullptr;
+    std::vector< geo_t > geo_h;
+};
+
+static thread_local std::string g_create_error;
+
+static bool ck( kr_ctx * c, cudaError_t e, const char * what )
+{
+    if( e == cudaSuccess )
+        return true;
+    if( c )
+        c->err = std::string( what ) + ": " + cudaGetErrorString( e );
+    else
+        g_create_error = std::string( what ) + ": " + cudaGetErrorString( e );
+    return false;
+}
+
+template< class R >
+static args_t< R > make_args( kr_ctx * c )
+{
+    args_t< R > a;
+    const int * n = c->cfg.n;
+    a.n0 = n[ 0 ]; a.n1 = n[ 1 ]; a.n2 = n[ 2 ]; a.nblk = c->nblk;
+    a.nc = c->nc; a.ngw = c->ngw; a.nbf = c->nbf; a.nfb = c->nfb;
+    a.sw1 = n[ 0 ] + 4; a.sw2 = ( n[ 0 ] + 4 ) * ( n[ 1 ] + 4 );
+    a.sb1 = n[ 0 ] + 5; a.sb2 = ( n[ 0 ] + 5 ) * ( n[ 1 ] + 5 );
+    a.sf1 = n[ 0 ] + 3; a.sf2 = ( n[ 0 ] + 3 ) * ( n[ 1 ] + 3 );
+    a.gamma = c->cfg.gamma; a.cfl = c->cfg.cfl;
+    a.d_floor = c->cfg.rho_floor; a.t_floor = c->cfg.tmp_floor;
+    a.dt_expand = c->cfg.dt_expand;
+    for( int s = 0; s < 2; ++ s ) { a.u[ s ] = c->u[ s ]; a.bf[ s ] = c->bf[ s ]; }
+    a.w = ( R * ) c->w;
+    for( int d = 0; d < 3; ++ d ) a.f[ d ] = ( R * ) c->f[ d ];
+    a.ee = ( R * ) c->ee;
+    a.geo = c->geo; a.nbr = c->nbr; a.s = c->s;
+    return a;
+}
+
+static inline unsigned blocks_for( long long n, int th ) { return unsigned( ( n + th - 1 ) / th ); }
+
+// Enqueue one Heun step on stream st.
+template< bool MHD, class R >
+static void enqueue_step( kr_ctx * c, cudaStream_t st )
+{
+    const args_t< R > a = make_args< R >( c );
+    const int * n = c->cfg.n;
+    const unsigned nb = unsigned( c->nblk );
+    const long long nlat = ( long long )( n[ 0 ] + 1 ) * ( n[ 1 ] + 1 ) * ( n[ 2 ] + 1 );
+    const long long nghost = MHD ? std::max( c->ngw, c->nbf ) : c->ngw;
+    k_step_begin<<< 1, 1, 0, st >>>( c->s );
+    for( int stage = 0; stage < 2; ++ stage )
+    {
+        k_c2p< MHD, R ><<< dim3( blocks_for( c->nc, 256 ), nb ), 256, 0, st >>>( a, stage );
+        k_ghost< MHD, R ><<< dim3( blocks_for( nghost, 256 ), nb ), 256, 0, st >>>( a, stage );
+        for( int axis = 2; axis >= 0; -- axis )
+        {
+            long long nface = 1;
+            for( int d = 0; d < 3; ++ d )
+                nface *= ( d == axis ) ? n[ d ] + 1 : n[ d ] + ( MHD ? 2 : 0 );
+            k_flux< MHD, R ><<< dim3( blocks_for( nface, 128 ), nb ), 128, 0, st >>>( a, axis, stage, c->cfg.riemann );
+        }
+        if( MHD )
+            k_emf< R ><<< dim3( blocks_for( nlat, 256 ), nb ), 256, 0, st >>>( a );
+        k_update< MHD, R ><<< dim3( blocks_for( nlat, 256 ), nb ), 256, 0, st >>>( a, stage );
+    }
+    k_step_end<<< 1, 1, 0, st >>>( c->s, c->cfg.dt_expand );
+}
+
+// One step launched eagerly with CUDA events around every kernel; per kind
+// (0 c2p, 1 ghost, 2 flux z, 3 flux y, 4 flux x, 5 emf, 6 update) the summed
+// milliseconds of the step are added to ms[kind].
+template< bool MHD, class R >
+static bool profile_step( kr_ctx * c, double * ms )
+{
+    const args_t< R > a = make_args< R >( c );
+    const int * n = c->cfg.n;
+    const unsigned nb = unsigned( c->nblk );
+    const long long nlat = ( long long )( n[ 0 ] + 1 ) * ( n[ 1 ] + 1 ) * ( n[ 2 ] + 1 );
+    const long long nghost = MHD ? std::max( c->ngw, c->nbf ) : c->ngw;
+    cudaStream_t st = c->stream;
+    cudaEvent_t ev[ 2 ];
+    cudaEventCreate( & ev[ 0 ] );
+    cudaEventCreate( & ev[ 1 ] );
+    auto timed = [ & ]( int kind, auto && launch )
+    {
+        cudaEventRecord( ev[ 0 ], st );
+        launch(  );
+        cudaEventRecord( ev[ 1 ], st );
+        cudaEventSynchronize( ev[ 1 ] );
+        float t = 0;
+        cudaEventElapsedTime( & t, ev[ 0 ], ev[ 1 ] );
+        ms[ kind ] += t;
+    };
+    k_step_begin<<< 1, 1, 0, st >>>( c->s );
+    for( int stage = 0; stage < 2; ++ stage )
+    {
+        timed( 0, [ & ] { k_c2p< MHD, R ><<< dim3( blocks_for( c->nc, 256 ), nb ), 256, 0, st >>>( a, stage ); } );
+        timed( 1, [ & ] { k_ghost< MHD, R ><<< dim3( blocks_for( nghost, 256 ), nb ), 256, 0, st >>>( a, stage ); } );
+        for( int axis = 2; axis >= 0; -- axis )
+        {
+            long long nface = 1;
+            for( int d = 0; d < 3; ++ d )
+                nface *= ( d == axis ) ? n[ d ] + 1 : n[ d ] + ( MHD ? 2 : 0 );
+            timed( 4 - axis, [ & ] { k_flux< MHD, R ><<< dim3( blocks_for( nface, 128 ), nb ), 128, 0, st >>>( a, axis, stage, c->cfg.riemann ); } );
+        }
+        if( MHD )
+            timed( 5, [ & ] { k_emf< R ><<< dim3( blocks_for( nlat, 256 ), nb ), 256, 0, st >>>( a ); } );
+        timed( 6, [ & ] { k_update< MHD, R ><<< dim3( blocks_for( nlat, 256 ), nb ), 256, 0, st >>>( a, stage ); } );
+    }
+    k_step_end<<< 1, 1, 0, st >>>( c->s, c->cfg.dt_expand );
+    cudaEventDestroy( ev[ 0 ] );
+    cudaEventDestroy( ev[ 1 ] );
+    return ck( c, cudaStreamSynchronize( st ), "profile" );
+}
+
+static void enqueue_step_any( kr_ctx * c, cudaStream_t st )
+{
+    if( c->cfg.mhd )
+    {
+        if( c->cfg.precision == 1 ) enqueue_step< true, float >( c, st );
+        else                        enqueue_step< true, double >( c, st );
+    }
+    else
+    {
+        if( c->cfg.precision == 1 ) enqueue_step< false, float >( c, st );
+        else                        enqueue_step< false, double >( c, st );
+    }
+}
+
+static void drop_graph( kr_ctx * c )
+{
+    if( c->graph_exec ) cudaGraphExecDestroy( c->graph_exec );
+    if( c->graph ) cudaGraphDestroy( c->graph );
+    c->graph_exec = nullptr;
+    c->graph = nullptr;
+    c->graph_stream = nullptr;
+}
+
+static bool build_graph( kr_ctx * c )
+{
+    drop_graph( c );
+    if( ! ck( c, cudaStreamBeginCapture( c->stream, cudaStreamCaptureModeThreadLocal ), "capture begin" ) )
+        return false;
+    enqueue_step_any( c, c->stream );
+    if( ! ck( c, cudaStreamEndCapture( c->stream, & c->graph ), "capture end" ) )
+        return false;
+    if( ! ck( c, cudaGraphInstantiate( & c->graph_exec, c->graph, 0 ), "graph instantiate" ) )
+        return false;
+    c->graph_stream = c->stream;
+    return true;
+}
+
+// Geometry exactly as meshgen computes it (meshgen.cpp:252-363).
+static void set_geometry( kr_ctx * c )
+{
+    const kr_cfg & g = c->cfg;
+    c->geo_h.resize( c->nblk );
+    for( int b = 0; b < c->nblk; ++ b )
+    {
+        const int reg[ 3 ] = { b % g.nb[ 0 ], ( b / g.nb[ 0 ] ) % g.nb[ 1 ], b / ( g.nb[ 0 ] * g.nb[ 1 ] ) };
+        geo_t & o = c->geo_h[ b ];
+        for( int a = 0; a < 3; ++ a )
+        {
+            const double lim = double( g.nb[ a ] );
+            const double x0 = ( reg[ a ] + 0.0 / g.n[ a ] ) / lim;
+            const double x1 = ( reg[ a ] + 1.0 / g.n[ a ] ) / lim;
+            const double l0 = g.x_min[ a ] + x0 * ( g.x_max[ a ] - g.x_min[ a ] );
+            const double l1 = g.x_min[ a ] + x1 * ( g.x_max[ a ] - g.x_min[ a ] );
+            o.dx[ a ] = l1 - l0;
+        }
+        double vol = 1.;
+        for( int a = 0; a < 3; ++ a )
+        {
+            double s = 1.;
+            s *= o.dx[ ( a + 1 ) % 3 ];
+            s *= o.dx[ ( a + 2 ) % 3 ];
+            o.sfc[ a ] = s;
+            vol *= o.dx[ a ];
+        }
+        o.vol = vol;
+    }
+}
+
+static double x_cc( const kr_cfg & g, int b, int a, int i )
+{
+    const int reg[ 3 ] = { b % g.nb[ 0 ], ( b / g.nb[ 0 ] ) % g.nb[ 1 ], b / ( g.nb[ 0 ] * g.nb[ 1 ] ) };
+    const double lim = double( g.nb[ a ] );
+    const double x0 = ( reg[ a ] + 0.0 / g.n[ a ] ) / lim;
+    const double x1 = ( reg[ a ] + 1.0 / g.n[ a ] ) / lim;
+    const double l0 = g.x_min[ a ] + x0 * ( g.x_max[ a ] - g.x_min[ a ] );
+    const double l1 = g.x_min[ a ] + x1 * ( g.x_max[ a ] - g.x_min[ a ] );
+    return l0 + ( i + 0.5f ) * ( l1 - l0 );
+}
+
+extern "C" {
+
+void kr_cfg_default( kr_cfg * g )
+{
+    std::memset( g, 0, sizeof( * g ) );
+    g->abi_version = KR_ABI_VERSION;
+    g->precision = 2;
+    for( int a = 0; a < 3; ++ a ) { g->nb[ a ] = 1; g->n[ a ] = 16; g->x_max[ a ] = 1; }
+    g->gamma = 1.66667;
+    g->cfl = 0.3;
+    g->rho_floor = 1e-9;
+    g->tmp_floor = 1e-9;
+    g->dt_expand = 2;
+}
+
+const char * kr_last_error( const kr_ctx * c )
+{
+    return c ? c->err.c_str(  ) : g_create_error.c_str(  );
+}
+
+kr_ctx * kr_ctx_create( const kr_cfg * cfg )
+{
+    g_create_error.clear(  );
+    if( ! cfg || cfg->abi_version != KR_ABI_VERSION )
+    {
+        g_create_error = "kr_ctx_create: missing config or ABI version mismatch";
+        return nullptr;
+    }
+    for( int a = 0; a < 3; ++ a )
+        if( cfg->n[ a ] < 4 || cfg->nb[ a ] < 1 )
+        {
+            g_create_error = "kr_ctx_create: need n >= 4 cells and nb >= 1 blocks per axis";
+            return nullptr;
+        }
+    if( cfg->precision != 1 && cfg->precision != 2 )
+    {
+        g_create_error = "kr_ctx_create: precision must be 1 (mixed) or 2 (FP64)";
+        return nullptr;
+    }
+    if( cfg->riemann != KR_RIEMANN_DEFAULT && ! cfg->mhd )
+    {
+        g_create_error = "kr_ctx_create: HLLE / learned selection is MHD only";
+        return nullptr;
+    }
+    if( cfg->riemann == KR_RIEMANN_LEARNED )
+    {
+        g_create_error = "kr_ctx_create: the learned selector needs kr_selector_load";
+        return nullptr;
+    }
+    int ndev = 0;
+    if( ! ck( nullptr, cudaGetDeviceCount( & ndev ), "cudaGetDeviceCount" ) )
+        return nullptr;
+    if( cfg->device < 0 || cfg->device >= ndev )
+    {
+        g_create_error = "kr_ctx_create: no such CUDA device";
+        return nullptr;
+    }
+    if( ! ck( nullptr, cudaSetDevice( cfg->device ), "cudaSetDevice" ) )
+        return nullptr;
+
+    kr_ctx * c = new kr_ctx;
+    c->cfg = * cfg;
+    const int * n = cfg->n;
+    c->nblk = cfg->nb[ 0 ] * cfg->nb[ 1 ] * cfg->nb[ 2 ];
+    c->nw = cfg->mhd ? 8 : 5;
+    c->nf = cfg->mhd ? 7 : 5;
+    c->nc  = ( long long ) n[ 0 ] * n[ 1 ] * n[ 2 ];
+    c->ngw = ( long long )( n[ 0 ] + 4 ) * ( n[ 1 ] + 4 ) * ( n[ 2 ] + 4 );
+    c->nbf = ( long long )( n[ 0 ] + 5 ) * ( n[ 1 ] + 5 ) * ( n[ 2 ] + 5 );
+    c->nfb = ( long long )( n[ 0 ] + 3 ) * ( n[ 1 ] + 3 ) * ( n[ 2 ] + 3 );
+    c->rsize = cfg->precision == 1 ? 4 : 8;
+    const size_t nb = size_t( c->nblk );
+    bool ok = ck( c, cudaStreamCreateWithFlags( & c->stream, cudaStreamNonBlocking ), "stream" );
+    c->own_stream = ok;
+    for( int s = 0; s < 2 && ok; ++ s )
+    {
+        ok = ok && ck( c, cudaMalloc( & c->u[ s ], nb * 5 * c->nc * 8 ), "malloc u" );
+        if( cfg->mhd )
+            ok = ok && ck( c, cudaMalloc( & c->bf[ s ], nb * 3 * c->nbf * 8 ), "malloc bf" );
+    }
+    ok = ok && ck( c, cudaMalloc( & c->w, nb * c->nw * c->ngw * c->rsize ), "malloc w" );
+    for( int d = 0; d < 3 && ok; ++ d )
+        ok = ck( c, cudaMalloc( & c->f[ d ], nb * c->nf * c->nfb * c->rsize ), "malloc f" );
+    if( cfg->mhd && ok )
+        ok = ck( c, cudaMalloc( & c->ee, nb * 3 * c->nfb * c->rsize ), "malloc ee" );
+    ok = ok && ck( c, cudaMalloc( & c->geo, nb * sizeof( geo_t ) ), "malloc geo" );
+    ok = ok && ck( c, cudaMalloc( & c->nbr, nb * 27 * sizeof( int ) ), "malloc nbr" );
+    ok = ok && ck( c, cudaMalloc( & c->s, sizeof( scal_t ) ), "malloc scalars" );
+    ok = ok && ck( c, cudaMalloc( & c->diag, 8 * sizeof( double ) ), "malloc diag" );
+    c->stage_bytes = nb * ( size_t( c->nc ) * c->nw + ( cfg->mhd ? size_t( c->nbf ) * 3 : 0 ) ) * 8;
+    ok = ok && ck( c, cudaMalloc( & c->stage, c->stage_bytes ), "malloc staging" );
+    if( ! ok )
+    {
+        g_create_error = c->err;
+        kr_ctx_destroy( c );
+        return nullptr;
+    }
+    // zero everything that a kernel may read before writing it
+    for( int s = 0; s < 2; ++ s )
+    {
+        cudaMemsetAsync( c->u[ s ], 0, nb * 5 * c->nc * 8, c->stream );
+        if( cfg->mhd ) cudaMemsetAsync( c->bf[ s ], 0, nb * 3 * c->nbf * 8, c->stream );
+    }
+    cudaMemsetAsync( c->w, 0, nb * c->nw * c->ngw * c->rsize, c->stream );
+    for( int d = 0; d < 3; ++ d )
+        cudaMemsetAsync( c->f[ d ], 0, nb * c->nf * c->nfb * c->rsize, c->stream );
+    if( cfg->mhd ) cudaMemsetAsync( c->ee, 0, nb * 3 * c->nfb * c->rsize, c->stream );
+
+    set_geometry( c );
+    std::vector< int > nbr( nb * 27 );
+    for( int b = 0; b < c->nblk; ++ b )
+    {
+        const int reg[ 3 ] = { b % cfg->nb[ 0 ], ( b / cfg->nb[ 0 ] ) % cfg->nb[ 1 ],
+                               b / ( cfg->nb[ 0 ] * cfg->nb[ 1 ] ) };
+        for( int k = 0; k < 27; ++ k )
+        {
+            const int sh[ 3 ] = { k % 3 - 1, ( k / 3 ) % 3 - 1, k / 9 - 1 };
+            int r[ 3 ];
+            for( int a = 0; a < 3; ++ a )
+                r[ a ] = ( reg[ a ] + sh[ a ] + cfg->nb[ a ] ) % cfg->nb[ a ];
+            nbr[ b * 27 + k ] = r[ 0 ] + cfg->nb[ 0 ] * ( r[ 1 ] + cfg->nb[ 1 ] * r[ 2 ] );
+        }
+    }
+    scal_t s0{};
+    s0.dt_bound = cfg->dt_init >= FLT_MIN ? cfg->dt_init : FLT_MAX / 10;   // cycle.cpp:163-166
+    ok = ck( c, cudaMemcpyAsync( c->geo, c->geo_h.data(  ), nb * sizeof( geo_t ), cudaMemcpyHostToDevice, c->stream ), "upload geo" )
+      && ck( c, cudaMemcpyAsync( c->nbr, nbr.data(  ), nbr.size(  ) * sizeof( int ), cudaMemcpyHostToDevice, c->stream ), "upload nbr" )
+      && ck( c, cudaMemcpyAsync( c->s, & s0, sizeof( s0 ), cudaMemcpyHostToDevice, c->stream ), "upload scalars" )
+      && ck( c, cudaStreamSynchronize( c->stream ), "sync" );
+    if( ! ok )
+    {
+        g_create_error = c->err;
+        kr_ctx_destroy( c );
+        return nullptr;
+    }
+    return c;
+}
+
+void kr_ctx_destroy( kr_ctx * c )
+{
+    if( ! c ) return;
+    cudaSetDevice( c->cfg.device );
+    if( c->stream ) cudaStreamSynchronize( c->stream );
+    drop_graph( c );
+    for( int s = 0; s < 2; ++ s ) { cudaFree( c->u[ s ] ); cudaFree( c->bf[ s ] ); }
+    cudaFree( c->w );
+    for( int d = 0; d < 3; ++ d ) cudaFree( c->f[ d ] );
+    cudaFree( c->ee ); cudaFree( c->geo ); cudaFree( c->nbr ); cudaFree( c->s );
+    cudaFree( c->stage ); cudaFree( c->diag );
+    if( c->own_stream && c->stream ) cudaStreamDestroy( c->stream );
+    delete c;
+}
+
+int kr_set_stream( kr_ctx * c, void * stream )
+{
+    if( ! c ) return -1;
+    cudaStreamSynchronize( c->stream );
+    if( c->own_stream ) cudaStreamDestroy( c->stream );
+    c->own_stream = stream == nullptr;
+    if( stream ) c->stream = ( cudaStream_t ) stream;
+    else if( ! ck( c, cudaStreamCreateWithFlags( & c->stream, cudaStreamNonBlocking ), "stream" ) )
+        return -1;
+    drop_graph( c );
+    return 0;
+}
+
+}   // extern "C"
+
+template< bool MHD, class R >
+static void launch_scatter( kr_ctx * c )
+{
+    const args_t< R > a = make_args< R >( c );
+    const long long nmax = MHD ? std::max( c->nc, c->nbf ) : c->nc;
+    const double * hu = c->stage;
+    const double * hb = c->stage + size_t( c->nblk ) * c->nc * c->nw;
+    k_scatter< MHD, R ><<< dim3( blocks_for( nmax, 256 ), c->nblk ), 256, 0, c->stream >>>( a, hu, hb );
+}
+template< bool MHD, class R >
+static void launch_gather( kr_ctx * c )
+{
+    const args_t< R > a = make_args< R >( c );
+    const long long nmax = MHD ? std::max( c->nc, c->nbf ) : c->nc;
+    double * hu = c->stage;
+    double * hb = c->stage + size_t( c->nblk ) * c->nc * c->nw;
+    k_gather< MHD, R ><<< dim3( blocks_for( nmax, 256 ), c->nblk ), 256, 0, c->stream >>>( a, hu, hb );
+}
+
+extern "C" {
+
+int kr_set_state( kr_ctx * c, const double * u, const double * bf )
+{
+    if( ! c || ! u || ( c->cfg.mhd && ! bf ) ) { if( c ) c->err = "kr_set_state: null array"; return -1; }
+    cudaSetDevice( c->cfg.device );
+    const size_t su = size_t( c->nblk ) * c->nc * c->nw * 8;
+    const size_t sb = c->cfg.mhd ? size_t( c->nblk ) * c->nbf * 3 * 8 : 0;
+    if( ! ck( c, cudaMemcpyAsync( c->stage, u, su, cudaMemcpyHostToDevice, c->stream ), "upload u" ) )
+        return -1;
+    if( sb && ! ck( c, cudaMemcpyAsync( ( char * ) c->stage + su, bf, sb, cudaMemcpyHostToDevice, c->stream ), "upload bf" ) )
+        return -1;
+    if( c->cfg.mhd ) { if( c->cfg.precision == 1 ) launch_scatter< true, float >( c ); else launch_scatter< true, double >( c ); }
+    else             { if( c->cfg.precision == 1 ) launch_scatter< false, float >( c ); else launch_scatter< false, double >( c ); }
+    return ck( c, cudaGetLastError(  ), "scatter" ) && ck( c, cudaStreamSynchronize( c->stream ), "sync" ) ? 0 : -1;
+}
+
+int kr_get_state( kr_ctx * c, double * u, double * bf )
+{
+    if( ! c || ! u || ( c->cfg.mhd && ! bf ) ) { if( c ) c->err = "kr_get_state: null array"; return -1; }
+    cudaSetDevice( c->cfg.device );
+    const size_t su = size_t( c->nblk ) * c->nc * c->nw * 8;
+    const size_t sb = c->cfg.mhd ? size_t( c->nblk ) * c->nbf * 3 * 8 : 0;
+    if( c->cfg.mhd ) { if( c->cfg.precision == 1 ) launch_gather< true, float >( c ); else launch_gather< true, double >( c ); }
+    else             { if( c->cfg.precision == 1 ) launch_gather< false, float >( c ); else launch_gather< false, double >( c ); }
+    if( ! ck( c, cudaGetLastError(  ), "gather" ) ) return -1;
+    if( ! ck( c, cudaMemcpyAsync( u, c->stage, su, cudaMemcpyDeviceToHost, c->stream ), "download u" ) )
+        return -1;
+    if( sb && ! ck( c, cudaMemcpyAsync( bf, ( char * ) c->stage + su, sb, cudaMemcpyDeviceToHost, c->stream ), "download bf" ) )
+        return -1;
+    return ck( c, cudaStreamSynchronize( c->stream ), "sync" ) ? 0 : -1;
+}
+
+int kr_init_problem( kr_ctx * c, const char * name, uint64_t seed )
+{
+    if( ! c || ! name ) return -1;
+    const bool shock = ! std::strcmp( name, "shock" ), ot = ! std::strcmp( name, "ot" );
+    if( ( ! shock && ! ot ) || ( ot != bool( c->cfg.mhd ) ) )
+    {
+        c->err = std::string( "kr_init_problem: unknown workload '" ) + name + "' for this mesh";
+        return -1;
+    }
+    const kr_cfg & g = c->cfg;
+    const int * n = g.n;
+    const int nw = c->nw;
+    std::vector< double > hu( size_t( c->nblk ) * c->nc * nw, 0.0 );
+    std::vector< double > hb( ot ? size_t( c->nblk ) * c->nbf * 3 : 0, 0.0 );
+    int nglob[ 3 ];
+    for( int a = 0; a < 3; ++ a ) nglob[ a ] = n[ a ] * g.nb[ a ];
+    const long long sb1 = n[ 0 ] + 5, sb2 = ( long long )( n[ 0 ] + 5 ) * ( n[ 1 ] + 5 );
+    auto bidx = [ & ]( int b, int i0, int i1, int i2 )
+    {   return ( ( size_t ) b * c->nbf + ( i0 + 2 ) + sb1 * ( i1 + 2 ) + sb2 * ( i2 + 2 ) ) * 3; };
+    auto work = [ & ]( int b )
+    {
+        const int reg[ 3 ] = { b % g.nb[ 0 ], ( b / g.nb[ 0 ] ) % g.nb[ 1 ], b / ( g.nb[ 0 ] * g.nb[ 1 ] ) };
+        if( ot )
+            for( int i2 = 0; i2 <= n[ 2 ]; ++ i2 )
+            for( int i1 = 0; i1 <= n[ 1 ]; ++ i1 )
+            for( int i0 = 0; i0 <= n[ 0 ]; ++ i0 )
+            {
+                double * p = hb.data(  ) + bidx( b, i0, i1, i2 );
+                p[ 0 ] = kr_ot_bx( x_cc( g, b, 1, i1 ) );
+                p[ 1 ] = kr_ot_by( x_cc( g, b, 0, i0 ) );
+                p[ 2 ] = kr_ot_bz(  );
+            }
+        for( int i2 = 0; i2 < n[ 2 ]; ++ i2 )
+        for( int i1 = 0; i1 < n[ 1 ]; ++ i1 )
+        for( int i0 = 0; i0 < n[ 0 ]; ++ i0 )
+        {
+            const int ii[ 3 ] = { i0, i1, i2 };
+            int ig[ 3 ];
+            for( int a = 0; a < 3; ++ a ) ig[ a ] = reg[ a ] * n[ a ] + ii[ a ];
+            const uint64_t key = kr_cell_key( 0, ig, nglob );
+            double * u = hu.data(  ) + ( ( size_t ) b * c->nc + i0 + ( size_t ) n[ 0 ] * ( i1 + ( size_t ) n[ 1 ] * i2 ) ) * nw;
+            if( shock )
+                kr_shock_cell( u, x_cc( g, b, 0, i0 ), g.gamma, seed, key );
+            else
+            {
+                double x[ 3 ], bc[ 3 ];
+                for( int a = 0; a < 3; ++ a )
+                {
+                    int jj[ 3 ] = { i0, i1, i2 };
+                    x[ a ] = x_cc( g, b, a, ii[ a ] );
+                    const double bl = hb[ bidx( b, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) + a ];
+                    ++ jj[ a ];
+                    bc[ a ] = ( bl + hb[ bidx( b, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) + a ] ) / 2;
+                }
+                kr_ot_cell( u, x, bc, g.gamma, seed, key );
+            }
+        }
+    };
+    const int nt = std::max( 1, std::min( c->nblk, int( std::thread::hardware_concurrency(  ) ) ) );
+    std::vector< std::thread > th;
+    for( int t = 0; t < nt; ++ t )
+        th.emplace_back( [ & , t ] (  ) { for( int b = t; b < c->nblk; b += nt ) work( b ); } );
+    for( auto & x : th ) x.join(  );
+    return kr_set_state( c, hu.data(  ), ot ? hb.data(  ) : nullptr );
+}
+
+int kr_step( kr_ctx * c, int n_steps )
+{
+    if( ! c || n_steps < 0 ) return -1;
+    cudaSetDevice( c->cfg.device );
+    if( ! c->graph_exec || c->graph_stream != c->stream )
+        if( ! build_graph( c ) )
+            return -1;
+    for( int s = 0; s < n_steps; ++ s )
+        if( ! ck( c, cudaGraphLaunch( c->graph_exec, c->stream ), "graph launch" ) )
+            return -1;
+    return 0;
+}
+
+int kr_get_time( kr_ctx * c, double * t, double * dt_last, double * dt_bound, long long * n )
+{
+    if( ! c ) return -1;
+    scal_t s;
+    if( ! ck( c, cudaMemcpyAsync( & s, c->s, sizeof( s ), cudaMemcpyDeviceToHost, c->stream ), "read scalars" )
+        || ! ck( c, cudaStreamSynchronize( c->stream ), "sync" ) )
+        return -1;
+    if( t ) * t = s.t;
+    if( dt_last ) * dt_last = s.dt_last;
+    if( dt_bound ) * dt_bound = s.dt_bound;
+    if( n ) * n = s.n_steps;
+    return 0;
+}
+
+int kr_set_time( kr_ctx * c, double t, double dt_bound )
+{
+    if( ! c ) return -1;
+    scal_t s;
+    if( ! ck( c, cudaMemcpyAsync( & s, c->s, sizeof( s ), cudaMemcpyDeviceToHost, c->stream ), "read scalars" )
+        || ! ck( c, cudaStreamSynchronize( c->stream ), "sync" ) )
+        return -1;
+    s.t = t;
+    s.dt_bound = dt_bound;
+    return ck( c, cudaMemcpyAsync( c->s, & s, sizeof( s ), cudaMemcpyHostToDevice, c->stream ), "write scalars" )
+        && ck( c, cudaStreamSynchronize( c->stream ), "sync" ) ? 0 : -1;
+}
+
+int kr_status( kr_ctx * c )
+{
+    if( ! c ) return -1;
+    scal_t s;
+    if( ! ck( c, cudaMemcpyAsync( & s, c->s, sizeof( s ), cudaMemcpyDeviceToHost, c->stream ), "read scalars" )
+        || ! ck( c, cudaStreamSynchronize( c->stream ), "sync" ) )
+        return -1;
+    const cudaError_t e = cudaGetLastError(  );
+    if( e != cudaSuccess ) { ck( c, e, "device" ); return -1; }
+    return s.status;
+}
+
+int kr_profile_step( kr_ctx * c, int n_kinds, double * ms )
+{
+    if( ! c || ! ms || n_kinds < 7 ) { if( c ) c->err = "kr_profile_step: need 7 slots"; return -1; }
+    cudaSetDevice( c->cfg.device );
+    for( int k = 0; k < n_kinds; ++ k ) ms[ k ] = 0;
+    bool ok;
+    if( c->cfg.mhd ) ok = c->cfg.precision == 1 ? profile_step< true, float >( c, ms ) : profile_step< true, double >( c, ms );
+    else             ok = c->cfg.precision == 1 ? profile_step< false, float >( c, ms ) : profile_step< false, double >( c, ms );
+    return ok ? 0 : -1;
+}
+
+int kr_launches_per_step( kr_ctx * c )
+{
+    if( ! c ) return -1;
+    return 2 + 2 * ( c->cfg.mhd ? 7 : 6 );
+}
+
+int kr_diagnostics( kr_ctx * c, double * max_div_b, double * totals5 )
+{
+    if( ! c ) return -1;
+    cudaSetDevice( c->cfg.device );
+    cudaMemsetAsync( c->diag, 0, 8 * sizeof( double ), c->stream );
+    const long long nmax = c->nc;
+    if( c->cfg.mhd )
+    {
+        if( c->cfg.precision == 1 ) k_diag< true, float ><<< dim3( blocks_for( nmax, 256 ), c->nblk ), 256, 0, c->stream >>>( make_args< float >( c ), c->diag );
+        else                        k_diag< true, double ><<< dim3( blocks_for( nmax, 256 ), c->nblk ), 256, 0, c->stream >>>( make_args< double >( c ), c->diag );
+    }
+    else
+    {
+        if( c->cfg.precision == 1 ) k_diag< false, float ><<< dim3( blocks_for( nmax, 256 ), c->nblk ), 256, 0, c->stream >>>( make_args< float >( c ), c->diag );
+        else                        k_diag< false, double ><<< dim3( blocks_for( nmax, 256 ), c->nblk ), 256, 0, c->stream >>>( make_args< double >( c ), c->diag );
+    }
+    double h[ 8 ];
+    if( ! ck( c, cudaMemcpyAsync( h, c->diag, sizeof( h ), cudaMemcpyDeviceToHost, c->stream ), "diag" )
+        || ! ck( c, cudaStreamSynchronize( c->stream ), "sync" ) )
+        return -1;
+    if( max_div_b ) * max_div_b = h[ 0 ];
+    if( totals5 ) for( int k = 0; k < 5; ++ k ) totals5[ k ] = h[ 1 + k ];
+    return 0;
+}
+
+}   // extern "C"

@@ -1,0 +1,137 @@
+"""Python handle on the device engine (tests, bench and scripting).
+
+A `Dynamics` object owns one kr_ctx: the device state of a uniform block mesh
+and the captured step.  Arrays exchanged with it use the reference's per-block
+layouts in lexicographic block order (see include/kratos_b200.h).
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib as L
+
+FLT_MAX = float(np.finfo(np.float32).max)
+
+
+class KratosError(RuntimeError):
+    pass
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class Dynamics:
+    def __init__(self, mhd, nb, n, gamma=1.66667, cfl=0.3, precision=2, riemann=0,
+                 x_min=(0, 0, 0), x_max=(1, 1, 1), rho_floor=1e-9, tmp_floor=1e-9,
+                 dt_init=0.0, dt_expand=2.0, device=0):
+        lib = L.lib()
+        c = L.kr_cfg()
+        lib.kr_cfg_default(ctypes.byref(c))
+        c.mhd, c.precision, c.riemann = int(mhd), int(precision), int(riemann)
+        for a in range(3):
+            c.nb[a], c.n[a] = int(nb[a]), int(n[a])
+            c.x_min[a], c.x_max[a] = float(x_min[a]), float(x_max[a])
+        c.gamma, c.cfl = float(gamma), float(cfl)
+        c.rho_floor, c.tmp_floor = float(rho_floor), float(tmp_floor)
+        c.dt_init, c.dt_expand, c.device = float(dt_init), float(dt_expand), int(device)
+        self.cfg = c
+        self._h = lib.kr_ctx_create(ctypes.byref(c))
+        if not self._h:
+            raise KratosError(lib.kr_last_error(None).decode())
+        self.mhd = bool(mhd)
+        self.nb, self.n = tuple(int(x) for x in nb), tuple(int(x) for x in n)
+        self.nblk = self.nb[0] * self.nb[1] * self.nb[2]
+        self.nw = 8 if mhd else 5
+
+    # ------------------------------------------------------------------ admin
+    def close(self):
+        if getattr(self, "_h", None):
+            L.lib().kr_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise KratosError("%s: %s" % (what, L.lib().kr_last_error(self._h).decode()))
+
+    @property
+    def u_shape(self):
+        n = self.n
+        return (self.nblk, n[2], n[1], n[0], self.nw)
+
+    @property
+    def bf_shape(self):
+        n = self.n
+        return (self.nblk, n[2] + 5, n[1] + 5, n[0] + 5, 3)
+
+    @property
+    def n_cells(self):
+        return self.nblk * self.n[0] * self.n[1] * self.n[2]
+
+    # ------------------------------------------------------------------ state
+    def set_stream(self, stream_handle):
+        self._check(L.lib().kr_set_stream(self._h, ctypes.c_void_p(stream_handle)), "kr_set_stream")
+
+    def init_problem(self, name, seed):
+        self._check(L.lib().kr_init_problem(self._h, name.encode(), int(seed)), "kr_init_problem")
+
+    def set_state(self, u, bf=None):
+        u = np.ascontiguousarray(u, dtype=np.float64).reshape(self.u_shape)
+        if self.mhd:
+            bf = np.ascontiguousarray(bf, dtype=np.float64).reshape(self.bf_shape)
+        self._check(L.lib().kr_set_state(self._h, _ptr(u), _ptr(bf) if self.mhd else None),
+                    "kr_set_state")
+
+    def get_state(self, u=None, bf=None):
+        u = np.empty(self.u_shape) if u is None else u
+        if self.mhd:
+            bf = np.empty(self.bf_shape) if bf is None else bf
+        self._check(L.lib().kr_get_state(self._h, _ptr(u), _ptr(bf) if self.mhd else None),
+                    "kr_get_state")
+        return u, (bf if self.mhd else None)
+
+    def state_bytes(self):
+        b = self.nblk * self.n[0] * self.n[1] * self.n[2] * self.nw * 8
+        if self.mhd:
+            b += self.nblk * (self.n[0] + 5) * (self.n[1] + 5) * (self.n[2] + 5) * 3 * 8
+        return b
+
+    # ------------------------------------------------------------------- time
+    def step(self, n_steps=1):
+        self._check(L.lib().kr_step(self._h, int(n_steps)), "kr_step")
+
+    def time(self):
+        t, dl, db = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        ns = ctypes.c_longlong()
+        self._check(L.lib().kr_get_time(self._h, ctypes.byref(t), ctypes.byref(dl),
+                                        ctypes.byref(db), ctypes.byref(ns)), "kr_get_time")
+        return {"t": t.value, "dt_last": dl.value, "dt_bound": db.value, "n_steps": ns.value}
+
+    def set_time(self, t, dt_bound):
+        self._check(L.lib().kr_set_time(self._h, float(t), float(dt_bound)), "kr_set_time")
+
+    def status(self):
+        s = L.lib().kr_status(self._h)
+        if s < 0:
+            raise KratosError("kr_status: " + L.lib().kr_last_error(self._h).decode())
+        return s
+
+    def launches_per_step(self):
+        return L.lib().kr_launches_per_step(self._h)
+
+    KERNEL_KINDS = ("c2p", "ghost", "flux_z", "flux_y", "flux_x", "emf", "update")
+
+    def profile_step(self):
+        """One eager step with CUDA events per kernel: {kind: ms}."""
+        ms = (ctypes.c_double * 7)()
+        self._check(L.lib().kr_profile_step(self._h, 7, ms), "kr_profile_step")
+        return dict(zip(self.KERNEL_KINDS, ms[:]))
+
+    def diagnostics(self):
+        dv = ctypes.c_double()
+        tot = (ctypes.c_double * 5)()
+        self._check(L.lib().kr_diagnostics(self._h, ctypes.byref(dv), tot), "kr_diagnostics")
+        return dv.value, np.array(tot[:])

@@ -1,0 +1,148 @@
+"""CUDA step against the original Kratos solver (golden fixtures) and the CPU
+restatement of it, through the C ABI.
+
+Tolerances (FP64 step): the device arithmetic follows the reference expression
+by expression but fuses multiply-adds, so agreement is to rounding, not to the
+bit.  Stated bound: relative L1 per conserved field <= 1e-11 and per face-B
+component <= 1e-11 after the fixture's steps; initial states are bit-exact
+(host-built from the same header).  Mixed step (FP32 reconstruction / Riemann,
+FP64 state): relative L1 density error vs the FP64 oracle <= 1e-4 (the
+north-star bound); |div B| <= 1e-12 in both modes.
+"""
+import numpy as np
+import pytest
+
+import golden_io as G
+
+pytestmark = pytest.mark.gpu
+
+TOL_FP64 = 1e-11
+
+
+def _dyn(meta, precision=2, riemann=0):
+    from kratos_b200 import Dynamics
+    extra = meta.get("dynamics", {})
+    return Dynamics(meta["workload"] == "ot", meta["nb"], meta["n"], gamma=meta["gamma"],
+                    cfl=meta["cfl"], tmp_floor=float(extra.get("tmp_floor", 1e-9)),
+                    precision=precision, riemann=riemann)
+
+
+def rel_l1(a, b):
+    den = np.abs(b).sum()
+    return np.abs(a - b).sum() / (den if den > 0 else 1.0)
+
+
+@pytest.mark.parametrize("name", ["shock_16", "ot_16"])
+def test_initial_state_bit_exact(name):
+    meta, g = G.load(name)
+    d = _dyn(meta)
+    d.init_problem(meta["workload"], meta["seed"])
+    u, bf = d.get_state()
+    assert np.array_equal(u[..., :5], g["u0"][..., :5])
+    if d.mhd:
+        mask = G.face_mask(meta["n"])
+        assert np.array_equal(G.owned_bf(bf, meta["n"])[:, mask], g["bf0"][:, mask])
+        # u slots 5..7 hold the face-averaged B, which is what the reference
+        # pgen writes there initially
+        np.testing.assert_array_equal(u[..., 5:], g["u0"][..., 5:])
+
+
+@pytest.mark.parametrize("name", ["shock_16", "ot_16", "ot_ragged", "shock_floor"])
+def test_fp64_step_matches_reference(name):
+    meta, g = G.load(name)
+    d = _dyn(meta)
+    d.init_problem(meta["workload"], meta["seed"])
+    d.step(meta["steps"])
+    u, bf = d.get_state()
+    tm = d.time()
+    assert d.status() == 0
+    assert abs(tm["t"] - meta["t"]) <= 1e-12 * meta["t"]
+    assert abs(tm["dt_last"] - meta["dt"]) <= 1e-12 * meta["dt"]
+    for k in range(5):
+        e = rel_l1(u[..., k], g["u1"][..., k])
+        assert e <= TOL_FP64, "field %d rel L1 %.3e" % (k, e)
+    if d.mhd:
+        own = G.owned_bf(bf, meta["n"])
+        mask = G.face_mask(meta["n"])
+        for c in range(3):
+            m = mask[..., c]
+            e = rel_l1(own[..., c][:, m], g["bf1"][..., c][:, m])
+            assert e <= TOL_FP64, "bf %d rel L1 %.3e" % (c, e)
+
+
+@pytest.mark.parametrize("name", ["shock_c1", "ot_64"])
+def test_fp64_full_size_checksums(name):
+    """Configs at full block size: checksum-of-fields against the reference."""
+    meta, g = G.load(name)
+    d = _dyn(meta)
+    d.init_problem(meta["workload"], meta["seed"])
+    u0, _ = d.get_state()
+    assert np.array_equal(G.checksums(u0[..., :5]), g["u0_sum"][:, :5])
+    d.step(meta["steps"])
+    u, bf = d.get_state()
+    s = G.checksums(u[..., :5])
+    ref = g["u1_sum"][:, :5]
+    # sums of |u| and extrema to 1e-11 relative; signed sums (momenta ~ 0) absolute
+    np.testing.assert_allclose(s[1:], ref[1:], rtol=TOL_FP64, atol=0)
+    scale = ref[1]
+    assert np.all(np.abs(s[0] - ref[0]) <= TOL_FP64 * scale)
+    assert abs(d.time()["t"] - meta["t"]) <= 1e-12 * meta["t"]
+
+
+def test_fp64_against_oracle_c1_shape():
+    """C1's mesh (64^3 in 8 blocks of 32^3), 20 steps, field by field."""
+    from oracle.kr_oracle import OracleMesh
+    meta, _ = G.load("shock_c1")
+    d = _dyn(meta)
+    d.init_problem("shock", meta["seed"])
+    d.step(meta["steps"])
+    u, _ = d.get_state()
+    o = OracleMesh(False, meta["nb"], meta["n"], meta["gamma"])
+    o.init_problem("shock", meta["seed"])
+    o.step(meta["steps"])
+    uo, _ = o.get_state()
+    for k in range(5):
+        assert rel_l1(u[..., k], uo[..., k]) <= TOL_FP64
+
+
+def test_mhd_invariants_fp64():
+    """div B at roundoff and conservation of mass, momentum and energy."""
+    from kratos_b200 import Dynamics
+    d = Dynamics(True, (2, 2, 2), (16, 16, 16), gamma=5 / 3)
+    d.init_problem("ot", 7)
+    div0, tot0 = d.diagnostics()
+    d.step(10)
+    div1, tot1 = d.diagnostics()
+    assert div0 <= 1e-12 and div1 <= 1e-12, (div0, div1)
+    assert abs(tot1[0] - tot0[0]) <= 1e-13 * abs(tot0[0])
+    assert abs(tot1[1] - tot0[1]) <= 1e-13 * abs(tot0[1])
+    assert np.all(np.abs(tot1[2:] - tot0[2:]) <= 1e-13 * abs(tot0[1]))
+
+
+def test_mixed_precision_error_bound():
+    """FP32 reconstruction + Riemann with FP64 state: density within 1e-4
+    relative L1 of the FP64 oracle; div B at FP64 roundoff."""
+    from oracle.kr_oracle import OracleMesh
+    meta, _ = G.load("ot_64")
+    d = _dyn(meta, precision=1)
+    d.init_problem("ot", meta["seed"])
+    d.step(meta["steps"])
+    u, _ = d.get_state()
+    div, _ = d.diagnostics()
+    o = OracleMesh(True, meta["nb"], meta["n"], meta["gamma"])
+    o.init_problem("ot", meta["seed"])
+    o.step(meta["steps"])
+    uo, _ = o.get_state()
+    e = rel_l1(u[..., 0], uo[..., 0])
+    assert e <= 1e-4, e
+    assert div <= 1e-12
+
+
+def test_status_word_starts_clean_and_steps_counted():
+    from kratos_b200 import Dynamics
+    d = Dynamics(False, (1, 1, 1), (8, 8, 8), gamma=1.4)
+    d.init_problem("shock", 1)
+    d.step(3)
+    tm = d.time()
+    assert tm["n_steps"] == 3 and d.status() == 0
+    assert d.launches_per_step() == 14
