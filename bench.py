@@ -42,7 +42,13 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--modes", default="fp64,mixed")
-    return p.parse_args()
+    p.add_argument("--mesh", type=int, default=256, choices=[128, 256],
+                   help="global cells per axis (128: profiling-sized sample, 8 blocks of 64^3)")
+    p.add_argument("--cpu-baseline", type=int, default=1, help="0: skip the CPU baseline leg")
+    args = p.parse_args()
+    global NB
+    NB = (args.mesh // 64,) * 3
+    return args
 
 
 def dist_env():
@@ -172,7 +178,7 @@ def reference_arm(args, rank, world):
     line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD.replace("256^3", "128^3 sample of the"),
+            "config": {"workload": WORKLOAD,
                        "mesh_sample": "128^3 = 8 blocks of 64^3 (same block shape)"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
                              "sample": "%d Heun steps of a 128^3 OT mesh (8 blocks of 64^3)" % steps},
@@ -281,11 +287,15 @@ def main():
         "gpu_launches": h["launches_per_step"] * args.steps,
     }
     line["flux_ms_per_step"] = flux_ms
+    if args.mesh != 256:
+        line["config"]["workload"] = WORKLOAD.replace("256^3", "%d^3" % args.mesh).replace(
+            "64 blocks", "%d blocks" % (NB[0] * NB[1] * NB[2]))
     if rank == 0:
-        try:
-            line["cpu_baseline"] = cpu_baseline()
-        except Exception as e:  # the baseline is reported, never required
-            line["cpu_baseline"] = {"value": None, "error": str(e)}
+        if args.cpu_baseline:
+            try:
+                line["cpu_baseline"] = cpu_baseline()
+            except Exception as e:  # the baseline is reported, never required
+                line["cpu_baseline"] = {"value": None, "error": str(e)}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
