@@ -117,6 +117,30 @@ int kr_profile_step( kr_ctx * ctx, int n_kinds, double * ms );
  * domain totals of mass, momentum and energy (5 doubles). */
 int kr_diagnostics( kr_ctx * ctx, double * max_div_b, double * totals5 );
 
+/* Allocation-free cons -> prim and CFL dt for ONE block, on device pointers.
+ * No counterpart in the reference: it exists for callers that cannot allocate
+ * device memory (code that runs under another framework's memory pool, or
+ * where cudaMalloc is not allowed), so the one kernel it launches keeps its
+ * scratch (per-CTA dt minima and a completion counter) in a fixed array inside
+ * the library instead of asking for memory.  Limit: blocks of at most
+ * 4,194,304 cells (16384 CTAs of 256 threads, 128 KiB of scratch, held by every
+ * GPU that loads the library until the process exits); larger blocks return -2
+ * with the reason in kr_last_error(NULL).  The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress) -- make that first call
+ * before any stream capture.  All calls share the array: calls that overlap on
+ * the GPU race and must be serialised by the caller.
+ *   cfg   : mhd, n[3], x_min/x_max (one block covering the box), gamma, cfl,
+ *           rho_floor, tmp_floor; nb and precision are ignored
+ *   u     : device, conserved state [5][n2][n1][n0] (rho, E, m0..2)
+ *   bf    : device, face B [3][n2+5][n1+5][n0+5] (MHD only, else may be NULL)
+ *   w     : device output, primitives [nw][n2+4][n1+4][n0+4], interior written
+ *           (nw = 8 MHD: rho, p, v0..2, B_cc0..2; 5 hydro)
+ *   dt_out: device output, one double: cfl * min over cells of dx / signal speed
+ *   stream: cudaStream_t (NULL: legacy default stream)
+ * Returns 0, or a negative code (enqueued work is asynchronous on `stream`). */
+int kr_c2p_dt_noalloc( const kr_cfg * cfg, const double * u, const double * bf,
+                       double * w, double * dt_out, void * stream );
+
 #ifdef __cplusplus
 }
 #endif

@@ -48,6 +48,7 @@ SIGNATURES = {
     "kr_status": (ctypes.c_int, [_vp]),
     "kr_launches_per_step": (ctypes.c_int, [_vp]),
     "kr_profile_step": (ctypes.c_int, [_vp, ctypes.c_int, _dp]),
+    "kr_c2p_dt_noalloc": (ctypes.c_int, [ctypes.POINTER(kr_cfg), _vp, _vp, _vp, _vp, _vp]),
     "kr_diagnostics": (ctypes.c_int, [_vp, _dp, _dp]),
 }
 

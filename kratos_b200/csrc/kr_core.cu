@@ -23,6 +23,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -1175,3 +1176,207 @@ int kr_diagnostics( kr_ctx * c, double * max_div_b, double * totals5 )
 }
 
 }   // extern "C"
+
+////////////////////////////////////////////////////////////
+// Allocation-free cons -> prim + CFL dt for one block.
+//
+// For callers that cannot allocate device memory themselves: code that runs
+// under another framework's memory pool or inside a region where cudaMalloc is
+// not allowed (a real-time loop, a plugin whose host forbids allocation).  The
+// caller passes device inputs (u, bf) and outputs (w, dt); the only scratch the
+// kernel needs -- the per-CTA partial minima of the CFL dt and a completion
+// counter -- lives in the file-scope array below, which every GPU that loads
+// the library holds until the process exits.
+//
+// The array is shared by every call: calls that overlap on the GPU (two
+// streams, or two host threads) race on it and give wrong results; serialise
+// them.  The counter is cleared on the caller's stream at the start of every
+// call, and the partials need no clearing (each CTA writes its own slot before
+// the last CTA reads them all).
+
+namespace kr
+{
+constexpr int NOALLOC_THREADS   = 256;
+constexpr int NOALLOC_MAX_CTAS  = 16384;
+constexpr long long NOALLOC_MAX_CELLS = ( long long ) NOALLOC_THREADS * NOALLOC_MAX_CTAS;
+
+// [0]: completion counter; [32 ..]: one partial minimum per CTA (bit patterns)
+static __device__ __align__( 256 ) unsigned long long g_noalloc_scratch[ 32 + NOALLOC_MAX_CTAS ];
+
+template< bool MHD >
+__global__ void __launch_bounds__( NOALLOC_THREADS )
+k_c2p_dt_noalloc( const double * u, const double * bf, double * w, double * dt_out,
+                  unsigned long long * scratch, int n0, int n1, int n2,
+                  double gamma, double cfl, double d_floor, double t_floor,
+                  double dx0, double dx1, double dx2 )
+{
+    constexpr int NW = MHD ? 8 : 5;
+    const long long nc = ( long long ) n0 * n1 * n2;
+    const long long c = ( long long ) blockIdx.x * blockDim.x + threadIdx.x;
+    const long long ngw = ( long long )( n0 + 4 ) * ( n1 + 4 ) * ( n2 + 4 );
+    const long long nbf = ( long long )( n0 + 5 ) * ( n1 + 5 ) * ( n2 + 5 );
+    const double dx[ 3 ] = { dx0, dx1, dx2 };
+    double dt = FLT_MAX;
+    if( c < nc )
+    {
+        const int i0 = int( c % n0 ), i1 = int( ( c / n0 ) % n1 ), i2 = int( c / ( ( long long ) n0 * n1 ) );
+        double cons[ 5 ], cout[ 5 ], prim[ 5 ];
+        for( int k = 0; k < 5; ++ k )
+            cons[ k ] = u[ k * nc + c ];
+        double bc[ 3 ] = { 0, 0, 0 }, bc_2[ 3 ] = { 0, 0, 0 }, b_max[ 3 ] = { 0, 0, 0 }, e_m = 0;
+        if( MHD )
+        {
+            const int ii[ 3 ] = { i0, i1, i2 };
+            for( int d = 0; d < 3; ++ d )
+            {
+                int jj[ 3 ] = { ii[ 0 ], ii[ 1 ], ii[ 2 ] };
+                auto at = [ & ]( const int * j )
+                {   return bf[ d * nbf + ( j[ 0 ] + 2 ) + ( long long )( n0 + 5 ) * ( ( j[ 1 ] + 2 ) + ( long long )( n1 + 5 ) * ( j[ 2 ] + 2 ) ) ]; };
+                const double b_l = at( jj );
+                ++ jj[ d ];
+                const double b_r = at( jj );
+                bc[ d ] = ( b_l + b_r ) / 2;
+                bc_2[ d ] = bc[ d ] * bc[ d ];
+                e_m += bc_2[ d ];
+                b_max[ d ] = fmax( fabs( b_l ), fabs( b_r ) );
+            }
+            e_m /= 2;
+            cons[ ENE ] -= e_m;
+        }
+        double cs2;
+        c2p( cons, prim, cout, gamma, d_floor, t_floor, cs2 );
+        const long long iw0 = ( i0 + 2 ) + ( long long )( n0 + 4 ) * ( ( i1 + 2 ) + ( long long )( n1 + 4 ) * ( i2 + 2 ) );
+        for( int k = 0; k < 5; ++ k )
+            w[ k * ngw + iw0 ] = prim[ k ];
+        if( MHD )
+            for( int d = 0; d < 3; ++ d )
+                w[ ( BCC + d ) * ngw + iw0 ] = bc[ d ];
+        if( ! MHD )
+        {
+            const double cs = sqrt( cs2 );
+            for( int d = 0; d < 3; ++ d )
+                dt = fmin( dt, dx[ d ] / ( cs + fabs( prim[ MOM + d ] ) ) );
+        }
+        else
+        {
+            double bm_2[ 3 ] = { bc_2[ 0 ], bc_2[ 1 ], bc_2[ 2 ] };
+            for( int d = 0; d < 3; ++ d )
+            {
+                bm_2[ d ] = b_max[ d ] * b_max[ d ];
+                const double cf = c_fms< double >( prim, bm_2, gamma, d );
+                dt = fmin( dt, dx[ d ] / ( cf + fabs( prim[ MOM + d ] ) ) );
+                bm_2[ d ] = bc_2[ d ];
+            }
+        }
+        dt *= cfl;
+        ( void ) NW;
+    }
+    // CTA minimum -> this CTA's scratch slot; the last CTA to finish reduces
+    // all slots into dt_out and re-arms the counter.
+    __shared__ double red[ NOALLOC_THREADS / 32 ];
+    __shared__ bool last;
+    dt = warp_min( dt );
+    if( ( threadIdx.x & 31 ) == 0 )
+        red[ threadIdx.x >> 5 ] = dt;
+    __syncthreads(  );
+    if( threadIdx.x == 0 )
+    {
+        double m = red[ 0 ];
+        for( int k = 1; k < NOALLOC_THREADS / 32; ++ k )
+            m = fmin( m, red[ k ] );
+        scratch[ 32 + blockIdx.x ] = ( unsigned long long ) __double_as_longlong( m );
+        __threadfence(  );
+        const unsigned long long done = atomicAdd( & scratch[ 0 ], 1ull );
+        last = ( done == gridDim.x - 1 );
+    }
+    __syncthreads(  );
+    if( ! last )
+        return;
+    __threadfence(  );
+    double m = FLT_MAX;
+    for( unsigned k = threadIdx.x; k < gridDim.x; k += blockDim.x )
+        m = fmin( m, __longlong_as_double( ( long long ) ( ( volatile unsigned long long * ) scratch )[ 32 + k ] ) );
+    m = warp_min( m );
+    if( ( threadIdx.x & 31 ) == 0 )
+        red[ threadIdx.x >> 5 ] = m;
+    __syncthreads(  );
+    if( threadIdx.x == 0 )
+    {
+        for( int k = 1; k < NOALLOC_THREADS / 32; ++ k )
+            red[ 0 ] = fmin( red[ 0 ], red[ k ] );
+        * dt_out = red[ 0 ];
+        scratch[ 0 ] = 0;
+    }
+}
+
+// Per-device address of the scratch array, looked up once per device.
+static unsigned long long * g_noalloc_ptr[ 64 ] = { nullptr };
+static std::mutex g_noalloc_mx;
+}   // namespace kr
+
+extern "C" int kr_c2p_dt_noalloc( const kr_cfg * cfg, const double * u, const double * bf,
+                                  double * w, double * dt_out, void * stream )
+{
+    using namespace kr;
+    g_create_error.clear(  );
+    if( ! cfg || ! u || ! w || ! dt_out || ( cfg->mhd && ! bf ) )
+    {
+        g_create_error = "kr_c2p_dt_noalloc: null argument";
+        return -1;
+    }
+    for( int a = 0; a < 3; ++ a )
+        if( cfg->n[ a ] < 1 )
+        {
+            g_create_error = "kr_c2p_dt_noalloc: block size must be positive";
+            return -1;
+        }
+    const long long nc = ( long long ) cfg->n[ 0 ] * cfg->n[ 1 ] * cfg->n[ 2 ];
+    if( nc > NOALLOC_MAX_CELLS )
+    {
+        g_create_error = "kr_c2p_dt_noalloc: block of " + std::to_string( nc ) + " cells exceeds the "
+                         "scratch limit of " + std::to_string( NOALLOC_MAX_CELLS ) + " cells "
+                         "(16384 CTAs of 256 threads)";
+        return -2;
+    }
+    int dev = 0;
+    if( ! ck( nullptr, cudaGetDevice( & dev ), "cudaGetDevice" ) )
+        return -1;
+    if( dev < 0 || dev >= 64 )
+    {
+        g_create_error = "kr_c2p_dt_noalloc: device ordinal out of range";
+        return -1;
+    }
+    unsigned long long * scratch;
+    {
+        std::lock_guard< std::mutex > lk( g_noalloc_mx );
+        if( ! g_noalloc_ptr[ dev ] )
+        {   // first call on this device: resolve the array's device address
+            void * p = nullptr;
+            if( ! ck( nullptr, cudaGetSymbolAddress( & p, g_noalloc_scratch ), "cudaGetSymbolAddress" ) )
+                return -1;
+            g_noalloc_ptr[ dev ] = ( unsigned long long * ) p;
+        }
+        scratch = g_noalloc_ptr[ dev ];
+    }
+    cudaStream_t st = ( cudaStream_t ) stream;
+    if( ! ck( nullptr, cudaMemsetAsync( scratch, 0, sizeof( unsigned long long ), st ), "clear counter" ) )
+        return -1;
+    // uniform block geometry as meshgen computes it for a single-block mesh
+    double dx[ 3 ];
+    for( int a = 0; a < 3; ++ a )
+    {
+        const double l0 = cfg->x_min[ a ] + ( 0 + 0.0 / cfg->n[ a ] ) / 1.0 * ( cfg->x_max[ a ] - cfg->x_min[ a ] );
+        const double l1 = cfg->x_min[ a ] + ( 0 + 1.0 / cfg->n[ a ] ) / 1.0 * ( cfg->x_max[ a ] - cfg->x_min[ a ] );
+        dx[ a ] = l1 - l0;
+    }
+    const unsigned grid = unsigned( ( nc + NOALLOC_THREADS - 1 ) / NOALLOC_THREADS );
+    if( cfg->mhd )
+        k_c2p_dt_noalloc< true ><<< grid, NOALLOC_THREADS, 0, st >>>( u, bf, w, dt_out, scratch,
+            cfg->n[ 0 ], cfg->n[ 1 ], cfg->n[ 2 ], cfg->gamma, cfg->cfl, cfg->rho_floor, cfg->tmp_floor,
+            dx[ 0 ], dx[ 1 ], dx[ 2 ] );
+    else
+        k_c2p_dt_noalloc< false ><<< grid, NOALLOC_THREADS, 0, st >>>( u, bf, w, dt_out, scratch,
+            cfg->n[ 0 ], cfg->n[ 1 ], cfg->n[ 2 ], cfg->gamma, cfg->cfl, cfg->rho_floor, cfg->tmp_floor,
+            dx[ 0 ], dx[ 1 ], dx[ 2 ] );
+    return ck( nullptr, cudaGetLastError(  ), "kr_c2p_dt_noalloc launch" ) ? 0 : -1;
+}
