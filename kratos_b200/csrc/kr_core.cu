@@ -14,7 +14,7 @@
 // is 2 x (c2p, ghost, flux z, flux y, flux x, [emf], update) plus two scalar
 // kernels, captured once into a CUDA graph and replayed.
 #include "../../include/kratos_b200.h"
-#include "kr_math.cuh"
+#include "kr_fast.cuh"
 #include "problems.h"
 
 #include <cuda_runtime.h>
@@ -57,6 +57,7 @@ struct args_t
     long long nc, ngw, nbf, nfb;      // per-component sizes: U, W, BF, F/EE
     int sw1, sw2, sb1, sb2, sf1, sf2; // strides of W, BF, F/EE boxes
     double gamma, cfl, d_floor, t_floor, dt_expand;
+    double gm1, cv;                   // gamma - 1 and 1 / (gamma - 1)
     double * u[ 2 ];
     double * bf[ 2 ];
     R * w;
@@ -219,63 +220,112 @@ __device__ __forceinline__ int wrap_axis( int i, int n, int & sh )
     return i;
 }
 
+// Site t of the ghost shell [-g, n+g)^3 \ [0, n)^3, enumerated as z slabs, then
+// y slabs (interior z), then x slabs (interior y, z).
+__device__ __forceinline__ void shell_site( long long t, int n0, int n1, int n2, int g,
+                                            int & i0, int & i1, int & i2 )
+{
+    const int e0 = n0 + 2 * g, e1 = n1 + 2 * g, l2 = 2 * g;
+    const long long zs = ( long long ) l2 * e0 * e1;
+    if( t < zs )
+    {
+        i0 = int( t % e0 ) - g;
+        i1 = int( ( t / e0 ) % e1 ) - g;
+        const int l = int( t / ( ( long long ) e0 * e1 ) );
+        i2 = l < g ? l - g : n2 + l - g;
+        return;
+    }
+    t -= zs;
+    const long long ys = ( long long ) l2 * e0 * n2;
+    if( t < ys )
+    {
+        i0 = int( t % e0 ) - g;
+        const int l = int( ( t / e0 ) % l2 );
+        i2 = int( t / ( ( long long ) e0 * l2 ) );
+        i1 = l < g ? l - g : n1 + l - g;
+        return;
+    }
+    t -= ys;
+    const int l = int( t % l2 );
+    i1 = int( ( t / l2 ) % n1 );
+    i2 = int( t / ( ( long long ) l2 * n1 ) );
+    i0 = l < g ? l - g : n0 + l - g;
+}
+
+__host__ __device__ __forceinline__ long long shell_count( int n0, int n1, int n2, int g )
+{
+    return ( long long ) 2 * g * ( ( long long )( n0 + 2 * g ) * ( n1 + 2 * g )
+                                 + ( long long )( n0 + 2 * g ) * n2 + ( long long ) n1 * n2 );
+}
+
+// Face-B ghost slots the flux sweeps read: component c on its own faces
+// (0..n_c) at the first transverse ghost line (-1 or n) of one transverse axis.
+__host__ __device__ __forceinline__ long long bf_strip_count( int n0, int n1, int n2 )
+{
+    const int nn[ 3 ] = { n0, n1, n2 };
+    long long s = 0;
+    for( int c = 0; c < 3; ++ c )
+        s += 2LL * ( nn[ c ] + 1 ) * ( nn[ ( c + 1 ) % 3 ] + nn[ ( c + 2 ) % 3 ] );
+    return s;
+}
+
 template< bool MHD, class R >
 __global__ void __launch_bounds__( 256 ) k_ghost( const args_t< R > a, int step )
 {
     constexpr int NW = MHD ? 8 : 5;
     const int b = blockIdx.y;
-    const long long t = ( long long ) blockIdx.x * blockDim.x + threadIdx.x;
-    const long long nbox_w = a.ngw;
-    if( t < nbox_w )
+    long long t = ( long long ) blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nsh = shell_count( a.n0, a.n1, a.n2, 2 );
+    if( t < nsh )
     {
-        const int i0 = int( t % a.sw1 ) - 2;
-        const int i1 = int( ( t / a.sw1 ) % ( a.n1 + 4 ) ) - 2;
-        const int i2 = int( t / a.sw2 ) - 2;
-        int s0, s1, s2;
+        int i0, i1, i2, s0, s1, s2;
+        shell_site( t, a.n0, a.n1, a.n2, 2, i0, i1, i2 );
         const int j0 = wrap_axis( i0, a.n0, s0 );
         const int j1 = wrap_axis( i1, a.n1, s1 );
         const int j2 = wrap_axis( i2, a.n2, s2 );
-        if( s0 | s1 | s2 )
-        {
-            const int src = a.nbr[ b * 27 + ( s0 + 1 ) + 3 * ( s1 + 1 ) + 9 * ( s2 + 1 ) ];
-            for( int k = 0; k < NW; ++ k )
-                a.w[ iw( a, b, k, NW, i0, i1, i2 ) ] = a.w[ iw( a, src, k, NW, j0, j1, j2 ) ];
-        }
+        const int src = a.nbr[ b * 27 + ( s0 + 1 ) + 3 * ( s1 + 1 ) + 9 * ( s2 + 1 ) ];
+        for( int k = 0; k < NW; ++ k )
+            a.w[ iw( a, b, k, NW, i0, i1, i2 ) ] = a.w[ iw( a, src, k, NW, j0, j1, j2 ) ];
+        return;
     }
     if( ! MHD )
         return;
-    if( t < a.nbf )
+    t -= nsh;
+    const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
+    for( int c = 0; c < 3; ++ c )
     {
-        double * BF = a.bf[ step ];
-        const int i0 = int( t % a.sb1 ) - 2;
-        const int i1 = int( ( t / a.sb1 ) % ( a.n1 + 5 ) ) - 2;
-        const int i2 = int( t / a.sb2 ) - 2;
-        const int ii[ 3 ] = { i0, i1, i2 };
-        const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
-        for( int c = 0; c < 3; ++ c )
+        const int a1 = ( c + 1 ) % 3, a2 = ( c + 2 ) % 3;
+        const long long cnt = 2LL * ( nn[ c ] + 1 ) * ( nn[ a1 ] + nn[ a2 ] );
+        if( t >= cnt )
         {
-            bool own = true;
-            int sh[ 3 ], jj[ 3 ];
-            for( int d = 0; d < 3; ++ d )
-            {
-                if( d == c )
-                {
-                    own = own && ii[ d ] >= 0 && ii[ d ] <= nn[ d ];
-                    if( ii[ d ] < 0 )           { sh[ d ] = -1; jj[ d ] = ii[ d ] + nn[ d ]; }
-                    else if( ii[ d ] > nn[ d ] ) { sh[ d ] = +1; jj[ d ] = ii[ d ] - nn[ d ]; }
-                    else                         { sh[ d ] = 0;  jj[ d ] = ii[ d ]; }
-                }
-                else
-                {
-                    own = own && ii[ d ] >= 0 && ii[ d ] < nn[ d ];
-                    jj[ d ] = wrap_axis( ii[ d ], nn[ d ], sh[ d ] );
-                }
-            }
-            if( own )
-                continue;
-            const int src = a.nbr[ b * 27 + ( sh[ 0 ] + 1 ) + 3 * ( sh[ 1 ] + 1 ) + 9 * ( sh[ 2 ] + 1 ) ];
-            BF[ ibf( a, b, c, i0, i1, i2 ) ] = BF[ ibf( a, src, c, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) ];
+            t -= cnt;
+            continue;
         }
+        // t -> (face index along c, side, transverse position along the other axis)
+        const int fc = int( t % ( nn[ c ] + 1 ) );
+        long long r = t / ( nn[ c ] + 1 );
+        const int side = int( r % 2 );
+        r /= 2;
+        int ii[ 3 ];
+        ii[ c ] = fc;
+        if( r < nn[ a2 ] )
+        {   // ghost line along a1
+            ii[ a1 ] = side ? nn[ a1 ] : -1;
+            ii[ a2 ] = int( r );
+        }
+        else
+        {
+            ii[ a2 ] = side ? nn[ a2 ] : -1;
+            ii[ a1 ] = int( r - nn[ a2 ] );
+        }
+        int sh[ 3 ] = { 0, 0, 0 }, jj[ 3 ] = { ii[ 0 ], ii[ 1 ], ii[ 2 ] };
+        for( int d = 0; d < 3; ++ d )
+            if( d != c )
+                jj[ d ] = wrap_axis( ii[ d ], nn[ d ], sh[ d ] );
+        const int src = a.nbr[ b * 27 + ( sh[ 0 ] + 1 ) + 3 * ( sh[ 1 ] + 1 ) + 9 * ( sh[ 2 ] + 1 ) ];
+        double * BF = a.bf[ step ];
+        BF[ ibf( a, b, c, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] = BF[ ibf( a, src, c, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) ];
+        return;
     }
 }
 
@@ -286,7 +336,7 @@ __global__ void __launch_bounds__( 256 ) k_ghost( const args_t< R > a, int step 
 // (mhd/integrator/integrator.h:138-168, mhd/integrator/data.h:106-144).
 
 template< bool MHD, class R >
-__global__ void __launch_bounds__( 128 ) k_flux( const args_t< R > a, int axis, int step, int rsel )
+__global__ void __launch_bounds__( 128, 4 ) k_flux( const args_t< R > a, int axis, int step, int rsel )
 {
     constexpr int NW = MHD ? 8 : 5;
     constexpr int NF = MHD ? 7 : 5;
@@ -323,21 +373,21 @@ __global__ void __launch_bounds__( 128 ) k_flux( const args_t< R > a, int axis, 
             continue;
         }
         const R * p = a.w + iw( a, b, k, NW, ii[ 0 ], ii[ 1 ], ii[ 2 ] );
-        plm_face< R >( p[ -2 * st ], p[ -st ], p[ 0 ], p[ st ], ql[ k ], qr[ k ] );
+        plm_face_fast< R >( p[ -2 * st ], p[ -st ], p[ 0 ], p[ st ], ql[ k ], qr[ k ] );
     }
-    const R gam = R( a.gamma );
+    const eos_c< R > e = { R( a.gamma ), R( a.gm1 ), R( a.cv ) };
     idx_swap( ql + MOM, axis );
     idx_swap( qr + MOM, axis );
     if( ! MHD )
-        hllc_eval< R >( flx, ql, qr, gam );
+        hllc_fast< R >( flx, ql, qr, e );
     else
     {
         idx_swap( ql + BCC, axis );
         idx_swap( qr + BCC, axis );
         if( rsel == KR_RIEMANN_HLLE )
-            hlle_eval< R >( flx, ql, qr, gam );
+            hlle_fast< R >( flx, ql, qr, e );
         else
-            hlld_eval< R >( flx, ql, qr, gam );
+            hlld_fast< R >( flx, ql, qr, e );
     }
     idx_swap( flx + MOM, 3 - axis );
     R * F = a.f[ axis ];
@@ -629,6 +679,7 @@ static args_t< R > make_args( kr_ctx * c )
     a.sb1 = n[ 0 ] + 5; a.sb2 = ( n[ 0 ] + 5 ) * ( n[ 1 ] + 5 );
     a.sf1 = n[ 0 ] + 3; a.sf2 = ( n[ 0 ] + 3 ) * ( n[ 1 ] + 3 );
     a.gamma = c->cfg.gamma; a.cfl = c->cfg.cfl;
+    a.gm1 = c->cfg.gamma - 1; a.cv = 1 / ( c->cfg.gamma - 1 );
     a.d_floor = c->cfg.rho_floor; a.t_floor = c->cfg.tmp_floor;
     a.dt_expand = c->cfg.dt_expand;
     for( int s = 0; s < 2; ++ s ) { a.u[ s ] = c->u[ s ]; a.bf[ s ] = c->bf[ s ]; }
@@ -649,7 +700,8 @@ static void enqueue_step( kr_ctx * c, cudaStream_t st )
     const int * n = c->cfg.n;
     const unsigned nb = unsigned( c->nblk );
     const long long nlat = ( long long )( n[ 0 ] + 1 ) * ( n[ 1 ] + 1 ) * ( n[ 2 ] + 1 );
-    const long long nghost = MHD ? std::max( c->ngw, c->nbf ) : c->ngw;
+    const long long nghost = shell_count( n[ 0 ], n[ 1 ], n[ 2 ], 2 )
+                           + ( MHD ? bf_strip_count( n[ 0 ], n[ 1 ], n[ 2 ] ) : 0 );
     k_step_begin<<< 1, 1, 0, st >>>( c->s );
     for( int stage = 0; stage < 2; ++ stage )
     {
@@ -679,7 +731,8 @@ static bool profile_step( kr_ctx * c, double * ms )
     const int * n = c->cfg.n;
     const unsigned nb = unsigned( c->nblk );
     const long long nlat = ( long long )( n[ 0 ] + 1 ) * ( n[ 1 ] + 1 ) * ( n[ 2 ] + 1 );
-    const long long nghost = MHD ? std::max( c->ngw, c->nbf ) : c->ngw;
+    const long long nghost = shell_count( n[ 0 ], n[ 1 ], n[ 2 ], 2 )
+                           + ( MHD ? bf_strip_count( n[ 0 ], n[ 1 ], n[ 2 ] ) : 0 );
     cudaStream_t st = c->stream;
     cudaEvent_t ev[ 2 ];
     cudaEventCreate( & ev[ 0 ] );
