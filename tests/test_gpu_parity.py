@@ -3,8 +3,9 @@ restatement of it, through the C ABI.
 
 Tolerances (FP64 step): the device arithmetic follows the reference expression
 by expression but fuses multiply-adds, so agreement is to rounding, not to the
-bit.  Stated bound: relative L1 per conserved field <= 1e-11 and per face-B
-component <= 1e-11 after the fixture's steps; initial states are bit-exact
+bit.  Stated bound: relative L1 per conserved field and per face-B component
+<= 1e-11 after the fixtures' 3-10 steps, <= 1e-10 after config 1's 20 shock
+steps (limiter switches amplify rounding there); initial states are bit-exact
 (host-built from the same header).  Mixed step (FP32 reconstruction / Riemann,
 FP64 state): relative L1 density error vs the FP64 oracle <= 1e-4 (the
 north-star bound); |div B| <= 1e-12 in both modes.
@@ -17,6 +18,7 @@ import golden_io as G
 pytestmark = pytest.mark.gpu
 
 TOL_FP64 = 1e-11
+TOL_FP64_LONG = 1e-10
 
 
 def _dyn(meta, precision=2, riemann=0):
@@ -102,7 +104,7 @@ def test_fp64_against_oracle_c1_shape():
     o.step(meta["steps"])
     uo, _ = o.get_state()
     for k in range(5):
-        assert rel_l1(u[..., k], uo[..., k]) <= TOL_FP64
+        assert rel_l1(u[..., k], uo[..., k]) <= TOL_FP64_LONG
 
 
 def test_mhd_invariants_fp64():
