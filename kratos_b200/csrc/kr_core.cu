@@ -122,7 +122,7 @@ __global__ void k_step_end( scal_t * s, double dt_expand )
 template< bool MHD, class R >
 __global__ void __launch_bounds__( 256 ) k_c2p( const args_t< R > a, int step )
 {
-    constexpr int NW = MHD ? 8 : 5;
+    constexpr int NW = MHD ? 11 : 5;   // stored W words: prim (8) + cell E (3)
     const int b = blockIdx.y;
     const long long c = ( long long ) blockIdx.x * blockDim.x + threadIdx.x;
     double dt = FLT_MAX;
@@ -167,7 +167,13 @@ __global__ void __launch_bounds__( 256 ) k_c2p( const args_t< R > a, int step )
             a.w[ iw( a, b, k, NW, i0, i1, i2 ) ] = R( prim[ k ] );
         if( MHD )
             for( int d = 0; d < 3; ++ d )
+            {   // cell-centred E = B x v (mhd/eos/adiabatic.h:216-220), from the
+                // stored (R-rounded) primitives so ghost copies agree bit for bit
+                const int d1 = mod3( d + 1 ), d2 = mod3( d + 2 );
                 a.w[ iw( a, b, BCC + d, NW, i0, i1, i2 ) ] = R( bc[ d ] );
+                a.w[ iw( a, b, 8 + d, NW, i0, i1, i2 ) ] =
+                    R( bc[ d1 ] ) * R( prim[ MOM + d2 ] ) - R( bc[ d2 ] ) * R( prim[ MOM + d1 ] );
+            }
         if( step == 0 )
         {
             const geo_t & g = a.geo[ b ];
@@ -272,7 +278,7 @@ __host__ __device__ __forceinline__ long long bf_strip_count( int n0, int n1, in
 template< bool MHD, class R >
 __global__ void __launch_bounds__( 256 ) k_ghost( const args_t< R > a, int step )
 {
-    constexpr int NW = MHD ? 8 : 5;
+    constexpr int NW = MHD ? 11 : 5;   // stored W words: prim (8) + cell E (3)
     const int b = blockIdx.y;
     long long t = ( long long ) blockIdx.x * blockDim.x + threadIdx.x;
     const long long nsh = shell_count( a.n0, a.n1, a.n2, 2 );
@@ -338,7 +344,7 @@ __global__ void __launch_bounds__( 256 ) k_ghost( const args_t< R > a, int step 
 template< bool MHD, class R >
 __global__ void __launch_bounds__( 128, 4 ) k_flux( const args_t< R > a, int axis, int step, int rsel )
 {
-    constexpr int NW = MHD ? 8 : 5;
+    constexpr int NW = MHD ? 11 : 5;   // stored W words: prim (8) + cell E (3)
     constexpr int NF = MHD ? 7 : 5;
     const int b = blockIdx.y;
     const int lo = MHD ? -1 : 0;
@@ -408,12 +414,7 @@ __global__ void __launch_bounds__( 128, 4 ) k_flux( const args_t< R > a, int axi
 template< class R > __device__ __forceinline__
 R e_cell( const args_t< R > & a, int b, const int * j, int ax )
 {
-    const int ax1 = mod3( ax + 1 ), ax2 = mod3( ax + 2 );
-    const R b1 = a.w[ iw( a, b, BCC + ax1, 8, j[ 0 ], j[ 1 ], j[ 2 ] ) ];
-    const R b2 = a.w[ iw( a, b, BCC + ax2, 8, j[ 0 ], j[ 1 ], j[ 2 ] ) ];
-    const R v1 = a.w[ iw( a, b, MOM + ax1, 8, j[ 0 ], j[ 1 ], j[ 2 ] ) ];
-    const R v2 = a.w[ iw( a, b, MOM + ax2, 8, j[ 0 ], j[ 1 ], j[ 2 ] ) ];
-    return b1 * v2 - b2 * v1;
+    return a.w[ iw( a, b, 8 + ax, 11, j[ 0 ], j[ 1 ], j[ 2 ] ) ];   // cell E, stored by k_c2p
 }
 
 template< class R > __device__ __forceinline__
@@ -631,7 +632,7 @@ struct kr_ctx
 {
     kr_cfg cfg;
     std::string err;
-    int nblk = 0, nw = 0, nf = 0;
+    int nblk = 0, nw = 0, nws = 0, nf = 0;   // nw: host words / cell; nws: stored W words
     long long nc = 0, ngw = 0, nbf = 0, nfb = 0;
     size_t rsize = 8;
     cudaStream_t stream = nullptr;
@@ -913,6 +914,7 @@ kr_ctx * kr_ctx_create( const kr_cfg * cfg )
     const int * n = cfg->n;
     c->nblk = cfg->nb[ 0 ] * cfg->nb[ 1 ] * cfg->nb[ 2 ];
     c->nw = cfg->mhd ? 8 : 5;
+    c->nws = cfg->mhd ? 11 : 5;
     c->nf = cfg->mhd ? 7 : 5;
     c->nc  = ( long long ) n[ 0 ] * n[ 1 ] * n[ 2 ];
     c->ngw = ( long long )( n[ 0 ] + 4 ) * ( n[ 1 ] + 4 ) * ( n[ 2 ] + 4 );
@@ -928,7 +930,7 @@ kr_ctx * kr_ctx_create( const kr_cfg * cfg )
         if( cfg->mhd )
             ok = ok && ck( c, cudaMalloc( & c->bf[ s ], nb * 3 * c->nbf * 8 ), "malloc bf" );
     }
-    ok = ok && ck( c, cudaMalloc( & c->w, nb * c->nw * c->ngw * c->rsize ), "malloc w" );
+    ok = ok && ck( c, cudaMalloc( & c->w, nb * c->nws * c->ngw * c->rsize ), "malloc w" );
     for( int d = 0; d < 3 && ok; ++ d )
         ok = ck( c, cudaMalloc( & c->f[ d ], nb * c->nf * c->nfb * c->rsize ), "malloc f" );
     if( cfg->mhd && ok )
@@ -951,7 +953,7 @@ kr_ctx * kr_ctx_create( const kr_cfg * cfg )
         cudaMemsetAsync( c->u[ s ], 0, nb * 5 * c->nc * 8, c->stream );
         if( cfg->mhd ) cudaMemsetAsync( c->bf[ s ], 0, nb * 3 * c->nbf * 8, c->stream );
     }
-    cudaMemsetAsync( c->w, 0, nb * c->nw * c->ngw * c->rsize, c->stream );
+    cudaMemsetAsync( c->w, 0, nb * c->nws * c->ngw * c->rsize, c->stream );
     for( int d = 0; d < 3; ++ d )
         cudaMemsetAsync( c->f[ d ], 0, nb * c->nf * c->nfb * c->rsize, c->stream );
     if( cfg->mhd ) cudaMemsetAsync( c->ee, 0, nb * 3 * c->nfb * c->rsize, c->stream );
