@@ -117,6 +117,44 @@ int kr_profile_step( kr_ctx * ctx, int n_kinds, double * ms );
  * domain totals of mass, momentum and energy (5 doubles). */
 int kr_diagnostics( kr_ctx * ctx, double * max_div_b, double * totals5 );
 
+/* ---- Learned HLLE/HLLD face selector (MHD).  No reference counterpart: the
+ * reference always solves HLLD (mhd/riemann/hlld.h).  A 16 -> 32 -> 32 -> 1 MLP
+ * (ReLU) predicts per face whether the cheap HLLE flux is within tolerance of
+ * HLLD; with riemann = KR_RIEMANN_LEARNED the flux sweep evaluates it with BF16
+ * tensor-core MMAs (FP32 accumulate) and uses HLLE where logit > threshold,
+ * HLLD elsewhere.  Parameters: 1633 floats, W1[16][32], b1[32], W2[32][32],
+ * b2[32], W3[32], b3, row-major [in][out]. */
+
+/* Upload selector parameters and the logit threshold to a context. */
+int kr_set_selector( kr_ctx * ctx, const float * params, float threshold );
+
+/* Faces evaluated and faces given HLLE since the last reset (learned mode). */
+int kr_selector_stats( kr_ctx * ctx, long long * faces, long long * cheap, int reset );
+
+/* Run n_steps ordinary steps while logging about one face in `stride` (per
+ * axis, stage and step; seeded) as a training sample: out[k*17 + 0..15] the
+ * selector features, out[k*17 + 16] the face's HLLE-HLLD flux gap in units of
+ * its flux scales.  At most max_samples are kept; *n_out receives the count. */
+int kr_selector_collect( kr_ctx * ctx, int n_steps, unsigned stride, uint64_t seed,
+                         long long max_samples, float * out, long long * n_out );
+
+/* Selector network on the GPU, with the project's own kernels.  X: [n][16]
+ * features, Y: [n] labels (1 = HLLE safe).  Loss: class-weighted binary
+ * cross-entropy on the logit, weight 1 for y = 1 and wneg for y = 0.
+ * kr_mlp_init: He-initialised parameters; kr_mlp_grad: mean loss and mean
+ * gradient (one forward / backward pass); kr_mlp_train: Adam over mini-batches
+ * of consecutive samples, params in/out; kr_mlp_infer: logits through the BF16
+ * tensor-core path of the flux sweep.  Errors: kr_learn_last_error(). */
+int         kr_mlp_param_count( void );
+void        kr_mlp_init ( float * params, uint64_t seed );
+int         kr_mlp_grad ( const float * X, const float * Y, long long n, const float * params,
+                          float wneg, float * grad, double * loss, int device );
+int         kr_mlp_train( const float * X, const float * Y, long long n, float * params,
+                          int epochs, int batch, float lr, float wneg, double * loss, int device );
+int         kr_mlp_infer( const float * X, long long n, const float * params, float * logits,
+                          int device );
+const char* kr_learn_last_error( void );
+
 /* Allocation-free cons -> prim and CFL dt for ONE block, on device pointers.
  * No counterpart in the reference: it exists for callers that cannot allocate
  * device memory (code that runs under another framework's memory pool, or

@@ -49,6 +49,20 @@ SIGNATURES = {
     "kr_launches_per_step": (ctypes.c_int, [_vp]),
     "kr_profile_step": (ctypes.c_int, [_vp, ctypes.c_int, _dp]),
     "kr_c2p_dt_noalloc": (ctypes.c_int, [ctypes.POINTER(kr_cfg), _vp, _vp, _vp, _vp, _vp]),
+    "kr_set_selector": (ctypes.c_int, [_vp, _vp, ctypes.c_float]),
+    "kr_selector_stats": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong),
+                                         ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]),
+    "kr_selector_collect": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_uint, ctypes.c_uint64,
+                                           ctypes.c_longlong, _vp, ctypes.POINTER(ctypes.c_longlong)]),
+    "kr_mlp_param_count": (ctypes.c_int, []),
+    "kr_mlp_init": (None, [_vp, ctypes.c_uint64]),
+    "kr_mlp_grad": (ctypes.c_int, [_vp, _vp, ctypes.c_longlong, _vp, ctypes.c_float, _vp,
+                                   ctypes.POINTER(ctypes.c_double), ctypes.c_int]),
+    "kr_mlp_train": (ctypes.c_int, [_vp, _vp, ctypes.c_longlong, _vp, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_float, ctypes.c_float, ctypes.POINTER(ctypes.c_double),
+                                    ctypes.c_int]),
+    "kr_mlp_infer": (ctypes.c_int, [_vp, ctypes.c_longlong, _vp, _vp, ctypes.c_int]),
+    "kr_learn_last_error": (ctypes.c_char_p, []),
     "kr_diagnostics": (ctypes.c_int, [_vp, _dp, _dp]),
 }
 

@@ -15,6 +15,7 @@
 // kernels, captured once into a CUDA graph and replayed.
 #include "../../include/kratos_b200.h"
 #include "kr_fast.cuh"
+#include "kr_mlp.cuh"
 #include "problems.h"
 
 #include <cuda_runtime.h>
@@ -64,6 +65,16 @@ struct args_t
     R * f[ 3 ];
     R * ee;
     const geo_t * geo;
+    // learned face selector (riemann == KR_RIEMANN_LEARNED)
+    const unsigned * sel_w;           // [32 lanes][MLP_BFRAG] bf16 pairs
+    const float * sel_b;              // b1, b2, b3
+    float sel_thr;                    // logit threshold for HLLE
+    unsigned long long * sel_cnt;     // [0] faces, [1] faces given HLLE
+    // face sampling for selector training (collect steps only)
+    float * smp;                      // [max][17]: 16 features + flux gap
+    unsigned long long * smp_n;
+    long long smp_max;
+    unsigned smp_stride, smp_seed;
     const int * nbr;                  // [block][27]
     scal_t * s;
 };
@@ -341,11 +352,12 @@ __global__ void __launch_bounds__( 256 ) k_ghost( const args_t< R > a, int step 
 // the transverse ghost lines that the corner EMF reads
 // (mhd/integrator/integrator.h:138-168, mhd/integrator/data.h:106-144).
 
-template< bool MHD, class R >
+template< bool MHD, class R, bool SAMPLE >
 __global__ void __launch_bounds__( 128, 4 ) k_flux( const args_t< R > a, int axis, int step, int rsel )
 {
     constexpr int NW = MHD ? 11 : 5;   // stored W words: prim (8) + cell E (3)
     constexpr int NF = MHD ? 7 : 5;
+    constexpr int NP = MHD ? 8 : 5;    // primitive words reconstructed
     const int b = blockIdx.y;
     const int lo = MHD ? -1 : 0;
     const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
@@ -353,8 +365,6 @@ __global__ void __launch_bounds__( 128, 4 ) k_flux( const args_t< R > a, int axi
     for( int d = 0; d < 3; ++ d )
         ext[ d ] = d == axis ? nn[ d ] + 1 : nn[ d ] - 2 * lo;
     const long long t = ( long long ) blockIdx.x * blockDim.x + threadIdx.x;
-    if( t >= ( long long ) ext[ 0 ] * ext[ 1 ] * ext[ 2 ] )
-        return;
     int ii[ 3 ];
     ii[ 0 ] = int( t % ext[ 0 ] );
     ii[ 1 ] = int( ( t / ext[ 0 ] ) % ext[ 1 ] );
@@ -366,21 +376,29 @@ __global__ void __launch_bounds__( 128, 4 ) k_flux( const args_t< R > a, int axi
             ii[ d ] += lo;
             outside += ( ii[ d ] < 0 || ii[ d ] >= nn[ d ] );
         }
-    if( outside > 1 )
-        return;                                  // corner line: never read
+    // corner lines are never read; lanes past the end idle.  Lanes stay alive
+    // until the (warp-collective) selector has run.
+    const bool valid = t < ( long long ) ext[ 0 ] * ext[ 1 ] * ext[ 2 ] && outside <= 1;
+    const bool learned = MHD && rsel == KR_RIEMANN_LEARNED;
+    if( ! valid && ! learned )
+        return;
     const int st = axis == 0 ? 1 : ( axis == 1 ? a.sw1 : a.sw2 );
     R ql[ 8 ], qr[ 8 ], flx[ 8 ];
-    for( int k = 0; k < NW; ++ k )
-    {
-        if( MHD && k == BCC + axis )
+    if( valid )
+        for( int k = 0; k < NP; ++ k )
         {
-            const R bn = R( a.bf[ step ][ ibf( a, b, axis, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] );
-            ql[ k ] = qr[ k ] = bn;
-            continue;
+            if( MHD && k == BCC + axis )
+            {
+                const R bn = R( a.bf[ step ][ ibf( a, b, axis, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] );
+                ql[ k ] = qr[ k ] = bn;
+                continue;
+            }
+            const R * p = a.w + iw( a, b, k, NW, ii[ 0 ], ii[ 1 ], ii[ 2 ] );
+            plm_face_fast< R >( p[ -2 * st ], p[ -st ], p[ 0 ], p[ st ], ql[ k ], qr[ k ] );
         }
-        const R * p = a.w + iw( a, b, k, NW, ii[ 0 ], ii[ 1 ], ii[ 2 ] );
-        plm_face_fast< R >( p[ -2 * st ], p[ -st ], p[ 0 ], p[ st ], ql[ k ], qr[ k ] );
-    }
+    else
+        for( int k = 0; k < 8; ++ k )
+            ql[ k ] = qr[ k ] = ( k == RHO || k == ENE ) ? R( 1 ) : R( 0 );
     const eos_c< R > e = { R( a.gamma ), R( a.gm1 ), R( a.cv ) };
     idx_swap( ql + MOM, axis );
     idx_swap( qr + MOM, axis );
@@ -390,10 +408,51 @@ __global__ void __launch_bounds__( 128, 4 ) k_flux( const args_t< R > a, int axi
     {
         idx_swap( ql + BCC, axis );
         idx_swap( qr + BCC, axis );
-        if( rsel == KR_RIEMANN_HLLE )
+        if( learned )
+        {
+            __shared__ __nv_bfloat16 xs[ 4 ][ 32 * MLP_IN ];
+            float f[ MLP_IN ];
+            face_features< R >( ql, qr, e.gamma, f );
+            const float z = mlp_logit( f, a.sel_w, a.sel_b, xs[ threadIdx.x >> 5 ] );
+            const bool cheap = valid && z > a.sel_thr;
+            const unsigned nv = __popc( __ballot_sync( 0xffffffffu, valid ) );
+            const unsigned nc = __popc( __ballot_sync( 0xffffffffu, cheap ) );
+            if( ( threadIdx.x & 31 ) == 0 && nv )
+            {
+                atomicAdd( a.sel_cnt, ( unsigned long long ) nv );
+                atomicAdd( a.sel_cnt + 1, ( unsigned long long ) nc );
+            }
+            if( ! valid )
+                return;
+            if( cheap )
+                hlle_fast< R >( flx, ql, qr, e );
+            else
+                hlld_fast< R >( flx, ql, qr, e );
+        }
+        else if( rsel == KR_RIEMANN_HLLE )
             hlle_fast< R >( flx, ql, qr, e );
         else
             hlld_fast< R >( flx, ql, qr, e );
+        if( SAMPLE )
+        {   // training sample: features, and the HLLE-HLLD gap of this face
+            const unsigned long long key = ( ( unsigned long long ) b * 3 + axis ) * 0x9E3779B97F4A7C15ull
+                                         + ( unsigned long long ) t * 0xBF58476D1CE4E5B9ull + a.smp_seed;
+            if( ( unsigned )( ( key ^ ( key >> 29 ) ) % a.smp_stride ) == 0 )
+            {
+                R fe[ 8 ], fd[ 8 ];
+                hlle_fast< R >( fe, ql, qr, e );
+                hlld_fast< R >( fd, ql, qr, e );
+                const unsigned long long slot = atomicAdd( a.smp_n, 1ull );
+                if( ( long long ) slot < a.smp_max )
+                {
+                    float f[ MLP_IN ];
+                    face_features< R >( ql, qr, e.gamma, f );
+                    float * o = a.smp + slot * ( MLP_IN + 1 );
+                    for( int k = 0; k < MLP_IN; ++ k ) o[ k ] = f[ k ];
+                    o[ MLP_IN ] = flux_gap< R >( fe, fd, ql, qr, e.gamma );
+                }
+            }
+        }
     }
     idx_swap( flx + MOM, 3 - axis );
     R * F = a.f[ axis ];
@@ -649,6 +708,17 @@ struct kr_ctx
     double * stage = nullptr;          // host-layout staging buffer (device)
     size_t stage_bytes = 0;
     double * diag = nullptr;
+    // learned selector
+    unsigned * sel_w = nullptr;
+    float * sel_b = nullptr;
+    unsigned long long * sel_cnt = nullptr;
+    float sel_thr = 0.f;
+    bool sel_ready = false;
+    // selector training samples (only during kr_selector_collect)
+    float * smp = nullptr;
+    unsigned long long * smp_n = nullptr;
+    long long smp_max = 0;
+    unsigned smp_stride = 1, smp_seed = 0;
     // graph of one step
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
@@ -657,6 +727,9 @@ struct kr_ctx
 };
 
 static thread_local std::string g_create_error;
+
+// FP32 selector parameters -> per-lane bf16 fragment words + biases (kr_learn.cu)
+void kr_mlp_pack( const float * w, std::vector< unsigned > & words, std::vector< float > & bias );
 
 static bool ck( kr_ctx * c, cudaError_t e, const char * what )
 {
@@ -688,13 +761,16 @@ static args_t< R > make_args( kr_ctx * c )
     for( int d = 0; d < 3; ++ d ) a.f[ d ] = ( R * ) c->f[ d ];
     a.ee = ( R * ) c->ee;
     a.geo = c->geo; a.nbr = c->nbr; a.s = c->s;
+    a.sel_w = c->sel_w; a.sel_b = c->sel_b; a.sel_thr = c->sel_thr; a.sel_cnt = c->sel_cnt;
+    a.smp = c->smp; a.smp_n = c->smp_n; a.smp_max = c->smp_max;
+    a.smp_stride = c->smp_stride; a.smp_seed = c->smp_seed;
     return a;
 }
 
 static inline unsigned blocks_for( long long n, int th ) { return unsigned( ( n + th - 1 ) / th ); }
 
-// Enqueue one Heun step on stream st.
-template< bool MHD, class R >
+// Enqueue one Heun step on stream st (SAMPLE: also log selector training samples).
+template< bool MHD, class R, bool SAMPLE = false >
 static void enqueue_step( kr_ctx * c, cudaStream_t st )
 {
     const args_t< R > a = make_args< R >( c );
@@ -713,7 +789,7 @@ static void enqueue_step( kr_ctx * c, cudaStream_t st )
             long long nface = 1;
             for( int d = 0; d < 3; ++ d )
                 nface *= ( d == axis ) ? n[ d ] + 1 : n[ d ] + ( MHD ? 2 : 0 );
-            k_flux< MHD, R ><<< dim3( blocks_for( nface, 128 ), nb ), 128, 0, st >>>( a, axis, stage, c->cfg.riemann );
+            k_flux< MHD, R, SAMPLE ><<< dim3( blocks_for( nface, 128 ), nb ), 128, 0, st >>>( a, axis, stage, c->cfg.riemann );
         }
         if( MHD )
             k_emf< R ><<< dim3( blocks_for( nlat, 256 ), nb ), 256, 0, st >>>( a );
@@ -758,7 +834,7 @@ static bool profile_step( kr_ctx * c, double * ms )
             long long nface = 1;
             for( int d = 0; d < 3; ++ d )
                 nface *= ( d == axis ) ? n[ d ] + 1 : n[ d ] + ( MHD ? 2 : 0 );
-            timed( 4 - axis, [ & ] { k_flux< MHD, R ><<< dim3( blocks_for( nface, 128 ), nb ), 128, 0, st >>>( a, axis, stage, c->cfg.riemann ); } );
+            timed( 4 - axis, [ & ] { k_flux< MHD, R, false ><<< dim3( blocks_for( nface, 128 ), nb ), 128, 0, st >>>( a, axis, stage, c->cfg.riemann ); } );
         }
         if( MHD )
             timed( 5, [ & ] { k_emf< R ><<< dim3( blocks_for( nlat, 256 ), nb ), 256, 0, st >>>( a ); } );
@@ -893,11 +969,6 @@ kr_ctx * kr_ctx_create( const kr_cfg * cfg )
         g_create_error = "kr_ctx_create: HLLE / learned selection is MHD only";
         return nullptr;
     }
-    if( cfg->riemann == KR_RIEMANN_LEARNED )
-    {
-        g_create_error = "kr_ctx_create: the learned selector needs kr_selector_load";
-        return nullptr;
-    }
     int ndev = 0;
     if( ! ck( nullptr, cudaGetDeviceCount( & ndev ), "cudaGetDeviceCount" ) )
         return nullptr;
@@ -939,6 +1010,11 @@ kr_ctx * kr_ctx_create( const kr_cfg * cfg )
     ok = ok && ck( c, cudaMalloc( & c->nbr, nb * 27 * sizeof( int ) ), "malloc nbr" );
     ok = ok && ck( c, cudaMalloc( & c->s, sizeof( scal_t ) ), "malloc scalars" );
     ok = ok && ck( c, cudaMalloc( & c->diag, 8 * sizeof( double ) ), "malloc diag" );
+    if( cfg->mhd )
+        ok = ok && ck( c, cudaMalloc( & c->sel_w, 32 * MLP_BFRAG * sizeof( unsigned ) ), "malloc selector" )
+                && ck( c, cudaMalloc( & c->sel_b, ( 2 * MLP_H + 1 ) * sizeof( float ) ), "malloc selector" )
+                && ck( c, cudaMalloc( & c->sel_cnt, 2 * sizeof( unsigned long long ) ), "malloc selector" )
+                && ck( c, cudaMemset( c->sel_cnt, 0, 2 * sizeof( unsigned long long ) ), "memset selector" );
     c->stage_bytes = nb * ( size_t( c->nc ) * c->nw + ( cfg->mhd ? size_t( c->nbf ) * 3 : 0 ) ) * 8;
     ok = ok && ck( c, cudaMalloc( & c->stage, c->stage_bytes ), "malloc staging" );
     if( ! ok )
@@ -999,6 +1075,7 @@ void kr_ctx_destroy( kr_ctx * c )
     for( int d = 0; d < 3; ++ d ) cudaFree( c->f[ d ] );
     cudaFree( c->ee ); cudaFree( c->geo ); cudaFree( c->nbr ); cudaFree( c->s );
     cudaFree( c->stage ); cudaFree( c->diag );
+    cudaFree( c->sel_w ); cudaFree( c->sel_b ); cudaFree( c->sel_cnt );
     if( c->own_stream && c->stream ) cudaStreamDestroy( c->stream );
     delete c;
 }
@@ -1139,6 +1216,11 @@ int kr_init_problem( kr_ctx * c, const char * name, uint64_t seed )
 int kr_step( kr_ctx * c, int n_steps )
 {
     if( ! c || n_steps < 0 ) return -1;
+    if( c->cfg.riemann == KR_RIEMANN_LEARNED && ! c->sel_ready )
+    {
+        c->err = "kr_step: learned face selector configured but no weights set (kr_set_selector)";
+        return -1;
+    }
     cudaSetDevice( c->cfg.device );
     if( ! c->graph_exec || c->graph_stream != c->stream )
         if( ! build_graph( c ) )
@@ -1186,6 +1268,74 @@ int kr_status( kr_ctx * c )
     const cudaError_t e = cudaGetLastError(  );
     if( e != cudaSuccess ) { ck( c, e, "device" ); return -1; }
     return s.status;
+}
+
+int kr_set_selector( kr_ctx * c, const float * w, float threshold )
+{
+    if( ! c || ! w ) return -1;
+    if( ! c->cfg.mhd ) { c->err = "kr_set_selector: MHD only"; return -1; }
+    cudaSetDevice( c->cfg.device );
+    std::vector< unsigned > words;
+    std::vector< float > bias;
+    kr_mlp_pack( w, words, bias );
+    if( ! ck( c, cudaMemcpyAsync( c->sel_w, words.data(  ), words.size(  ) * 4, cudaMemcpyHostToDevice, c->stream ), "upload selector" )
+        || ! ck( c, cudaMemcpyAsync( c->sel_b, bias.data(  ), bias.size(  ) * 4, cudaMemcpyHostToDevice, c->stream ), "upload selector" )
+        || ! ck( c, cudaStreamSynchronize( c->stream ), "sync" ) )
+        return -1;
+    if( c->sel_thr != threshold )
+        drop_graph( c );                 // the threshold is a kernel argument
+    c->sel_thr = threshold;
+    c->sel_ready = true;
+    return 0;
+}
+
+int kr_selector_stats( kr_ctx * c, long long * faces, long long * cheap, int reset )
+{
+    if( ! c || ! c->sel_cnt ) return -1;
+    unsigned long long h[ 2 ];
+    if( ! ck( c, cudaMemcpyAsync( h, c->sel_cnt, sizeof( h ), cudaMemcpyDeviceToHost, c->stream ), "read counters" )
+        || ! ck( c, cudaStreamSynchronize( c->stream ), "sync" ) )
+        return -1;
+    if( faces ) * faces = ( long long ) h[ 0 ];
+    if( cheap ) * cheap = ( long long ) h[ 1 ];
+    if( reset && ! ck( c, cudaMemsetAsync( c->sel_cnt, 0, sizeof( h ), c->stream ), "reset counters" ) )
+        return -1;
+    return 0;
+}
+
+int kr_selector_collect( kr_ctx * c, int n_steps, unsigned stride, uint64_t seed,
+                         long long max_samples, float * out, long long * n_out )
+{
+    if( ! c || ! out || max_samples <= 0 || stride == 0 || n_steps < 0 ) return -1;
+    if( ! c->cfg.mhd ) { c->err = "kr_selector_collect: MHD only"; return -1; }
+    cudaSetDevice( c->cfg.device );
+    const size_t bytes = size_t( max_samples ) * ( MLP_IN + 1 ) * sizeof( float );
+    if( ! ck( c, cudaMalloc( & c->smp, bytes ), "malloc samples" )
+        || ! ck( c, cudaMalloc( & c->smp_n, sizeof( unsigned long long ) ), "malloc samples" )
+        || ! ck( c, cudaMemsetAsync( c->smp_n, 0, sizeof( unsigned long long ), c->stream ), "memset" ) )
+        return -1;
+    c->smp_max = max_samples;
+    c->smp_stride = stride;
+    bool ok = true;
+    for( int k = 0; k < n_steps && ok; ++ k )
+    {
+        c->smp_seed = unsigned( seed * 0x9E3779B9u + k );
+        if( c->cfg.precision == 1 ) enqueue_step< true, float, true >( c, c->stream );
+        else                        enqueue_step< true, double, true >( c, c->stream );
+        ok = ck( c, cudaGetLastError(  ), "collect step" );
+    }
+    unsigned long long n = 0;
+    ok = ok && ck( c, cudaMemcpyAsync( & n, c->smp_n, sizeof( n ), cudaMemcpyDeviceToHost, c->stream ), "read count" )
+            && ck( c, cudaStreamSynchronize( c->stream ), "sync" );
+    const long long got = std::min( ( long long ) n, max_samples );
+    ok = ok && ck( c, cudaMemcpy( out, c->smp, size_t( got ) * ( MLP_IN + 1 ) * sizeof( float ), cudaMemcpyDeviceToHost ), "download samples" );
+    cudaFree( c->smp );
+    cudaFree( c->smp_n );
+    c->smp = nullptr;
+    c->smp_n = nullptr;
+    c->smp_max = 0;
+    if( n_out ) * n_out = got;
+    return ok ? 0 : -1;
 }
 
 int kr_profile_step( kr_ctx * c, int n_kinds, double * ms )

@@ -130,6 +130,18 @@ class Dynamics:
         self._check(L.lib().kr_profile_step(self._h, 7, ms), "kr_profile_step")
         return dict(zip(self.KERNEL_KINDS, ms[:]))
 
+    def set_selector(self, params, threshold=0.0):
+        import numpy as _np
+        w = _np.ascontiguousarray(params, _np.float32)
+        self._check(L.lib().kr_set_selector(self._h, ctypes.c_void_p(w.ctypes.data), float(threshold)),
+                    "kr_set_selector")
+
+    def selector_stats(self, reset=False):
+        f, c = ctypes.c_longlong(), ctypes.c_longlong()
+        self._check(L.lib().kr_selector_stats(self._h, ctypes.byref(f), ctypes.byref(c), int(reset)),
+                    "kr_selector_stats")
+        return f.value, c.value
+
     def diagnostics(self):
         dv = ctypes.c_double()
         tot = (ctypes.c_double * 5)()

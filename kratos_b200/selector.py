@@ -1,0 +1,99 @@
+"""Learned HLLE/HLLD face selector: sample collection, GPU training, install.
+
+The network and its training kernels live in the engine (kr_learn.cu); this
+module only moves arrays across the C ABI:
+
+    X, gap = collect(dyn, steps, stride)     # faces logged from ordinary steps
+    y = (gap < tol).astype(float32)          # 1 = HLLE within tolerance
+    w = train(X, y)                           # Adam on the GPU, project kernels
+    dyn.set_selector(w, threshold)            # used when riemann = LEARNED
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib as L
+
+N_IN = 16
+N_PARAM = 16 * 32 + 32 + 32 * 32 + 32 + 32 + 1
+
+
+def _p(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def _err():
+    return L.lib().kr_learn_last_error().decode()
+
+
+def init_params(seed=0):
+    w = np.empty(N_PARAM, np.float32)
+    L.lib().kr_mlp_init(_p(w), int(seed))
+    return w
+
+
+def grad(X, y, w, wneg=1.0, device=0):
+    X = np.ascontiguousarray(X, np.float32)
+    y = np.ascontiguousarray(y, np.float32)
+    w = np.ascontiguousarray(w, np.float32)
+    g = np.empty(N_PARAM, np.float32)
+    loss = ctypes.c_double()
+    rc = L.lib().kr_mlp_grad(_p(X), _p(y), len(y), _p(w), float(wneg), _p(g), ctypes.byref(loss), device)
+    if rc:
+        raise RuntimeError(_err())
+    return loss.value, g
+
+
+def train(X, y, w=None, epochs=20, batch=4096, lr=3e-3, wneg=4.0, seed=0, device=0):
+    X = np.ascontiguousarray(X, np.float32)
+    y = np.ascontiguousarray(y, np.float32)
+    w = init_params(seed) if w is None else np.array(w, np.float32)
+    loss = ctypes.c_double()
+    rc = L.lib().kr_mlp_train(_p(X), _p(y), len(y), _p(w), int(epochs), int(batch), float(lr),
+                              float(wneg), ctypes.byref(loss), device)
+    if rc:
+        raise RuntimeError(_err())
+    return w, loss.value
+
+
+def infer(X, w, device=0):
+    X = np.ascontiguousarray(X, np.float32)
+    w = np.ascontiguousarray(w, np.float32)
+    out = np.empty(len(X), np.float32)
+    if L.lib().kr_mlp_infer(_p(X), len(X), _p(w), _p(out), device):
+        raise RuntimeError(_err())
+    return out
+
+
+def collect(dyn, steps, stride=64, seed=0, max_samples=1 << 21):
+    out = np.empty((max_samples, N_IN + 1), np.float32)
+    n = ctypes.c_longlong()
+    rc = L.lib().kr_selector_collect(dyn._h, int(steps), int(stride), int(seed), int(max_samples),
+                                     _p(out), ctypes.byref(n))
+    dyn._check(rc, "kr_selector_collect")
+    out = out[:n.value]
+    return out[:, :N_IN].copy(), out[:, N_IN].copy()
+
+
+def shuffle(X, y, seed=0):
+    idx = np.random.default_rng(seed).permutation(len(y))
+    return X[idx], y[idx]
+
+
+def build_selector(dyn_factory, steps=4, stride=16, tol=1e-3, epochs=30, seed=0, device=0):
+    """Collect faces from runs of the given workloads, label them with the gap
+    tolerance and train.  dyn_factory: iterable of callables returning a
+    Dynamics object with its initial state set.  Returns (params, info)."""
+    Xs, gs = [], []
+    for make in dyn_factory:
+        d = make()
+        X, g = collect(d, steps, stride, seed)
+        Xs.append(X)
+        gs.append(g)
+        d.close()
+    X = np.concatenate(Xs)
+    gap = np.concatenate(gs)
+    y = (gap < tol).astype(np.float32)
+    X, y = shuffle(X, y, seed)
+    w, loss = train(X, y, epochs=epochs, seed=seed, device=device)
+    return w, {"samples": int(len(y)), "safe_fraction": float(y.mean()), "loss": loss, "tol": tol}

@@ -1,0 +1,103 @@
+"""Learned HLLE/HLLD face selector on the GPU.
+
+* the hand-written FP32 training kernels' loss and gradient against the float64
+  CPU restatement (oracle/kr_mlp_ref.py): relative error <= 1e-4;
+* the BF16 tensor-core inference path against the same network with bf16
+  roundings restated on the CPU;
+* training on faces logged from the method's own runs separates safe from
+  unsafe faces;
+* the learned mixed step stays within 1e-4 relative L1 density of the FP64
+  oracle with div B at roundoff, and its gain over the method without it: it
+  sends a share of faces to HLLE while its error stays far below the all-HLLE
+  step's.
+"""
+import numpy as np
+import pytest
+
+from oracle import kr_mlp_ref as M
+
+pytestmark = pytest.mark.gpu
+
+
+def _data(n=3000, seed=0):
+    rng = np.random.default_rng(seed)
+    X = rng.normal(size=(n, 16)).astype(np.float32)
+    y = (X[:, 0] * 0.7 - X[:, 3] + 0.2 * X[:, 9] ** 2 > 0.1).astype(np.float32)
+    return X, y
+
+
+def test_training_gradient_matches_cpu_oracle():
+    from kratos_b200 import selector as S
+    X, y = _data()
+    w = S.init_params(3) * 1.0
+    loss, g = S.grad(X, y, w, wneg=2.5)
+    lo, go = M.loss_grad(X, y, w, wneg=2.5)
+    assert abs(loss - lo) <= 1e-5 * abs(lo)
+    scale = np.abs(go).max()
+    np.testing.assert_allclose(g, go, rtol=1e-3, atol=1e-4 * scale)
+    assert np.abs(g - go).max() <= 1e-4 * scale
+
+
+def test_bf16_inference_matches_restated_rounding():
+    from kratos_b200 import selector as S
+    X, y = _data(1000, 1)
+    w, _ = S.train(X, y, epochs=5, batch=256, lr=3e-3, wneg=1.0)
+    z = S.infer(X, w)
+    zo = M.forward_bf16(X, w)
+    zf, _ = M.forward(X, w)
+    # bf16 roundings of inputs, weights and activations: agreement to ~1e-2
+    assert np.abs(z - zo).max() <= 2e-2 * (1 + np.abs(zo).max())
+    assert np.corrcoef(z, zf)[0, 1] > 0.999
+
+
+def test_training_separates_synthetic_classes():
+    from kratos_b200 import selector as S
+    X, y = _data(20000, 2)
+    w, loss = S.train(X, y, epochs=30, batch=1024, lr=3e-3, wneg=1.0)
+    z = S.infer(X, w)
+    acc = ((z > 0) == (y > 0.5)).mean()
+    assert acc > 0.95, acc
+    assert loss < 0.2
+
+
+def _ot(nb=(2, 2, 2), n=(32, 32, 32), **kw):
+    from kratos_b200 import Dynamics
+    d = Dynamics(True, nb, n, gamma=5 / 3, **kw)
+    d.init_problem("ot", 2)
+    return d
+
+
+def test_learned_step_error_and_gain():
+    from kratos_b200 import selector as S
+    from oracle.kr_oracle import OracleMesh
+    # training data: faces logged from the method's own mixed steps
+    w, info = S.build_selector([lambda: _ot(n=(16, 16, 16), precision=1),
+                                lambda: _ot(precision=1)], steps=4, stride=4, tol=1e-3, epochs=25)
+    assert info["samples"] > 10000
+    steps = 10
+    o = OracleMesh(True, (2, 2, 2), (32, 32, 32), 5 / 3)
+    o.init_problem("ot", 2)
+    o.step(steps)
+    ref, _ = o.get_state()
+
+    def run(riemann, thr=None):
+        d = _ot(precision=1, riemann=riemann)
+        if thr is not None:
+            d.set_selector(w, thr)
+        d.step(steps)
+        u, _ = d.get_state()
+        div, _ = d.diagnostics()
+        stats = d.selector_stats() if thr is not None else None
+        e = np.abs(u[..., 0] - ref[..., 0]).sum() / np.abs(ref[..., 0]).sum()
+        return e, div, stats
+
+    e_hlld, _, _ = run(0)
+    e_hlle, _, _ = run(1)
+    e_learn, div, (faces, cheap) = run(2, thr=2.0)
+    frac = cheap / faces
+    print("rel L1 density: hlld %.2e  hlle %.2e  learned %.2e (HLLE on %.1f%% of faces)"
+          % (e_hlld, e_hlle, e_learn, 100 * frac))
+    assert e_learn <= 1e-4
+    assert div <= 1e-12
+    assert frac > 0.05                     # the network routes faces to HLLE ...
+    assert e_learn < 0.5 * e_hlle          # ... at a fraction of the all-HLLE error
