@@ -41,7 +41,7 @@ def parse():
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--modes", default="fp64,mixed")
+    p.add_argument("--modes", default="fp64,mixed,learned")
     p.add_argument("--mesh", type=int, default=256, choices=[128, 256],
                    help="global cells per axis (128: profiling-sized sample, 8 blocks of 64^3)")
     p.add_argument("--cpu-baseline", type=int, default=1, help="0: skip the CPU baseline leg")
@@ -188,13 +188,36 @@ def reference_arm(args, rank, world):
 
 # --------------------------------------------------------------------------- GPU
 MODES = {"fp64": dict(precision=2, riemann=0), "mixed": dict(precision=1, riemann=0),
-         "hlle_mixed": dict(precision=1, riemann=1)}
+         "hlle_mixed": dict(precision=1, riemann=1), "learned": dict(precision=1, riemann=2)}
+
+
+def train_selector(local_rank):
+    """Selector for the learned mode, trained on the GPU from faces logged on
+    a 128^3 OT run (mixed step) and a 64^3 one: ~2 M samples, 20 epochs."""
+    from kratos_b200 import Dynamics, selector as S
+
+    def make(nb):
+        def f():
+            d = Dynamics(True, nb, N, gamma=GAMMA, precision=1, device=local_rank)
+            d.init_problem("ot", SEED + 1)
+            return d
+        return f
+    t0 = time.perf_counter()
+    w, info = S.build_selector([make((1, 1, 1)), make((2, 2, 2))], steps=4, stride=8,
+                               epochs=20, device=local_rank)
+    info["train_s"] = time.perf_counter() - t0
+    info["threshold"] = S.DEFAULT_THRESHOLD
+    return w, info
 
 
 def time_mode(mode, args, local_rank, world, dist):
     import torch
     from kratos_b200 import Dynamics
     d = Dynamics(True, NB, N, gamma=GAMMA, device=local_rank, **MODES[mode])
+    sel_info = None
+    if mode == "learned":
+        w, sel_info = train_selector(local_rank)
+        d.set_selector(w, sel_info["threshold"])
     stream = torch.cuda.Stream(device=local_rank)
     d.set_stream(stream.cuda_stream)
     d.init_problem("ot", SEED)
@@ -239,6 +262,10 @@ def time_mode(mode, args, local_rank, world, dist):
                   "h2d_bytes_per_step": d.state_bytes() // e2e_steps,
                   "d2h_bytes_per_step": d.state_bytes() // e2e_steps}
     out["n_cells"] = d.n_cells
+    if sel_info is not None:
+        faces, cheap = d.selector_stats()
+        sel_info["hlle_fraction"] = cheap / max(faces, 1)
+        out["selector"] = sel_info
     del np
     d.close()
     return out
@@ -261,7 +288,7 @@ def main():
     results = {}
     for mode in [m for m in args.modes.split(",") if m]:
         results[mode] = time_mode(mode, args, local_rank, world, dist)
-    head = "mixed" if "mixed" in results else next(iter(results))
+    head = next((m for m in ("learned", "mixed", "fp64") if m in results), next(iter(results)))
     h = results[head]
     peak, peak_kind = measured_peaks()
     flux_ms = h["kernels_ms_per_step"]["flux_x"] + h["kernels_ms_per_step"]["flux_y"] + h["kernels_ms_per_step"]["flux_z"]
@@ -276,8 +303,10 @@ def main():
         "config": {"workload": WORKLOAD, "mode": head, "global_cells": h["n_cells"] * world,
                    "parallelism": "replica per GPU" if world > 1 else "1 GPU",
                    "l2": "state 1.6 GB > 126 MB L2; no flush needed"},
-        "modes": {m: {"value": r["value"], "ms_per_step": r["ms_per_step"],
-                      "kernels_ms_per_step": r["kernels_ms_per_step"]} for m, r in results.items()},
+        "modes": {m: dict({"value": r["value"], "ms_per_step": r["ms_per_step"],
+                           "kernels_ms_per_step": r["kernels_ms_per_step"]},
+                          **({"selector": r["selector"]} if "selector" in r else {}))
+                  for m, r in results.items()},
         "roofline": {"bound": "hbm", "achieved": step_gbs, "peak": peak, "unit": "GB/s",
                      "frac": step_gbs / peak, "traffic": None,
                      "basis": "whole step: %d B/zone-cycle algorithmic (%s peak); top kernel %s"

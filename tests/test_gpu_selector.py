@@ -72,7 +72,7 @@ def test_learned_step_error_and_gain():
     from oracle.kr_oracle import OracleMesh
     # training data: faces logged from the method's own mixed steps
     w, info = S.build_selector([lambda: _ot(n=(16, 16, 16), precision=1),
-                                lambda: _ot(precision=1)], steps=4, stride=4, tol=1e-3, epochs=25)
+                                lambda: _ot(precision=1)], steps=4, stride=4, tol=3e-4, epochs=25)
     assert info["samples"] > 10000
     steps = 10
     o = OracleMesh(True, (2, 2, 2), (32, 32, 32), 5 / 3)
@@ -99,5 +99,5 @@ def test_learned_step_error_and_gain():
           % (e_hlld, e_hlle, e_learn, 100 * frac))
     assert e_learn <= 1e-4
     assert div <= 1e-12
-    assert frac > 0.05                     # the network routes faces to HLLE ...
+    assert frac > 0.3                      # the network routes faces to HLLE ...
     assert e_learn < 0.5 * e_hlle          # ... at a fraction of the all-HLLE error
