@@ -352,9 +352,16 @@ __global__ void __launch_bounds__( 256 ) k_ghost( const args_t< R > a, int step 
 // the transverse ghost lines that the corner EMF reads
 // (mhd/integrator/integrator.h:138-168, mhd/integrator/data.h:106-144).
 
-template< bool MHD, class R, bool SAMPLE >
-__global__ void __launch_bounds__( 128, 4 ) k_flux( const args_t< R > a, int axis, int step, int rsel )
+// MODE: KR_RIEMANN_DEFAULT, KR_RIEMANN_HLLE, KR_RIEMANN_LEARNED, or FLUX_SAMPLE
+// (HLLD step that also logs selector training samples).  Compile-time, so the
+// plain step carries none of the selector's registers.
+constexpr int FLUX_SAMPLE = 3;
+
+template< bool MHD, class R, int MODE >
+__global__ void __launch_bounds__( 128, 4 ) k_flux( const args_t< R > a, int axis, int step )
 {
+    constexpr bool SAMPLE = MODE == FLUX_SAMPLE;
+    constexpr int rsel = MODE == FLUX_SAMPLE ? KR_RIEMANN_DEFAULT : MODE;
     constexpr int NW = MHD ? 11 : 5;   // stored W words: prim (8) + cell E (3)
     constexpr int NF = MHD ? 7 : 5;
     constexpr int NP = MHD ? 8 : 5;    // primitive words reconstructed
@@ -379,7 +386,7 @@ __global__ void __launch_bounds__( 128, 4 ) k_flux( const args_t< R > a, int axi
     // corner lines are never read; lanes past the end idle.  Lanes stay alive
     // until the (warp-collective) selector has run.
     const bool valid = t < ( long long ) ext[ 0 ] * ext[ 1 ] * ext[ 2 ] && outside <= 1;
-    const bool learned = MHD && rsel == KR_RIEMANN_LEARNED;
+    constexpr bool learned = MHD && rsel == KR_RIEMANN_LEARNED;
     if( ! valid && ! learned )
         return;
     const int st = axis == 0 ? 1 : ( axis == 1 ? a.sw1 : a.sw2 );
@@ -414,13 +421,16 @@ __global__ void __launch_bounds__( 128, 4 ) k_flux( const args_t< R > a, int axi
             float f[ MLP_IN ];
             face_features< R >( ql, qr, e.gamma, f );
             const float z = mlp_logit( f, a.sel_w, a.sel_b, xs[ threadIdx.x >> 5 ] );
-            const bool cheap = valid && z > a.sel_thr;
-            const unsigned nv = __popc( __ballot_sync( 0xffffffffu, valid ) );
-            const unsigned nc = __popc( __ballot_sync( 0xffffffffu, cheap ) );
-            if( ( threadIdx.x & 31 ) == 0 && nv )
+            // Warp-uniform choice: the warp takes HLLE only when every valid
+            // face of it is predicted safe, so no warp pays for both solvers.
+            const unsigned vmask = __ballot_sync( 0xffffffffu, valid );
+            const unsigned cmask = __ballot_sync( 0xffffffffu, valid && z > a.sel_thr );
+            const bool cheap = vmask != 0 && cmask == vmask;
+            if( ( threadIdx.x & 31 ) == 0 && vmask )
             {
-                atomicAdd( a.sel_cnt, ( unsigned long long ) nv );
-                atomicAdd( a.sel_cnt + 1, ( unsigned long long ) nc );
+                atomicAdd( a.sel_cnt, ( unsigned long long ) __popc( vmask ) );
+                if( cheap )
+                    atomicAdd( a.sel_cnt + 1, ( unsigned long long ) __popc( vmask ) );
             }
             if( ! valid )
                 return;
@@ -789,7 +799,15 @@ static void enqueue_step( kr_ctx * c, cudaStream_t st )
             long long nface = 1;
             for( int d = 0; d < 3; ++ d )
                 nface *= ( d == axis ) ? n[ d ] + 1 : n[ d ] + ( MHD ? 2 : 0 );
-            k_flux< MHD, R, SAMPLE ><<< dim3( blocks_for( nface, 128 ), nb ), 128, 0, st >>>( a, axis, stage, c->cfg.riemann );
+            const dim3 g( blocks_for( nface, 128 ), nb );
+            if( SAMPLE )
+                k_flux< MHD, R, FLUX_SAMPLE ><<< g, 128, 0, st >>>( a, axis, stage );
+            else if( c->cfg.riemann == KR_RIEMANN_LEARNED )
+                k_flux< MHD, R, KR_RIEMANN_LEARNED ><<< g, 128, 0, st >>>( a, axis, stage );
+            else if( c->cfg.riemann == KR_RIEMANN_HLLE )
+                k_flux< MHD, R, KR_RIEMANN_HLLE ><<< g, 128, 0, st >>>( a, axis, stage );
+            else
+                k_flux< MHD, R, KR_RIEMANN_DEFAULT ><<< g, 128, 0, st >>>( a, axis, stage );
         }
         if( MHD )
             k_emf< R ><<< dim3( blocks_for( nlat, 256 ), nb ), 256, 0, st >>>( a );
@@ -834,7 +852,14 @@ static bool profile_step( kr_ctx * c, double * ms )
             long long nface = 1;
             for( int d = 0; d < 3; ++ d )
                 nface *= ( d == axis ) ? n[ d ] + 1 : n[ d ] + ( MHD ? 2 : 0 );
-            timed( 4 - axis, [ & ] { k_flux< MHD, R, false ><<< dim3( blocks_for( nface, 128 ), nb ), 128, 0, st >>>( a, axis, stage, c->cfg.riemann ); } );
+            const dim3 g( blocks_for( nface, 128 ), nb );
+            timed( 4 - axis, [ & ] {
+                if( c->cfg.riemann == KR_RIEMANN_LEARNED )
+                    k_flux< MHD, R, KR_RIEMANN_LEARNED ><<< g, 128, 0, st >>>( a, axis, stage );
+                else if( c->cfg.riemann == KR_RIEMANN_HLLE )
+                    k_flux< MHD, R, KR_RIEMANN_HLLE ><<< g, 128, 0, st >>>( a, axis, stage );
+                else
+                    k_flux< MHD, R, KR_RIEMANN_DEFAULT ><<< g, 128, 0, st >>>( a, axis, stage ); } );
         }
         if( MHD )
             timed( 5, [ & ] { k_emf< R ><<< dim3( blocks_for( nlat, 256 ), nb ), 256, 0, st >>>( a ); } );
