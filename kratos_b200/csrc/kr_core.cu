@@ -421,16 +421,18 @@ __global__ void __launch_bounds__( 128, 4 ) k_flux( const args_t< R > a, int axi
             float f[ MLP_IN ];
             face_features< R >( ql, qr, e.gamma, f );
             const float z = mlp_logit( f, a.sel_w, a.sel_b, xs[ threadIdx.x >> 5 ] );
-            // Warp-uniform choice: the warp takes HLLE only when every valid
-            // face of it is predicted safe, so no warp pays for both solvers.
+            // Per-face choice: HLLE where the network predicts the face safe,
+            // HLLD for every flagged face.  (A warp-uniform choice -- HLLE only
+            // when all 32 faces of a warp are safe -- avoids running both
+            // solvers in one warp but left HLLE on under 1% of the faces of
+            // the 64^3 OT run, so it is not used.)
+            const bool cheap = valid && z > a.sel_thr;
             const unsigned vmask = __ballot_sync( 0xffffffffu, valid );
-            const unsigned cmask = __ballot_sync( 0xffffffffu, valid && z > a.sel_thr );
-            const bool cheap = vmask != 0 && cmask == vmask;
+            const unsigned cmask = __ballot_sync( 0xffffffffu, cheap );
             if( ( threadIdx.x & 31 ) == 0 && vmask )
             {
                 atomicAdd( a.sel_cnt, ( unsigned long long ) __popc( vmask ) );
-                if( cheap )
-                    atomicAdd( a.sel_cnt + 1, ( unsigned long long ) __popc( vmask ) );
+                atomicAdd( a.sel_cnt + 1, ( unsigned long long ) __popc( cmask ) );
             }
             if( ! valid )
                 return;
