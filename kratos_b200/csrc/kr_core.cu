@@ -357,70 +357,41 @@ __global__ void __launch_bounds__( 256 ) k_ghost( const args_t< R > a, int step 
 // plain step carries none of the selector's registers.
 constexpr int FLUX_SAMPLE = 3;
 
-template< bool MHD, class R, int MODE >
-__global__ void __launch_bounds__( 128, 4 ) k_flux( const args_t< R > a, int axis, int step )
+// Riemann solve of one face from its reconstructed states and store of the
+// flux (and, for MHD, the two edge EMFs: hlld.h:42-46 -- slot 5 holds
+// E_{(axis+1)%3}, slot 6 E_{(axis+2)%3}).  Every lane of the warp must call it
+// in the learned mode (the selector is warp-collective); invalid lanes only
+// take part in that.
+template< bool MHD, class R, int MODE > __device__ __forceinline__
+void solve_store( const args_t< R > & a, int b, int axis, const int * ii, bool valid,
+                  R * ql, R * qr, int warp, unsigned long long key )
 {
     constexpr bool SAMPLE = MODE == FLUX_SAMPLE;
     constexpr int rsel = MODE == FLUX_SAMPLE ? KR_RIEMANN_DEFAULT : MODE;
-    constexpr int NW = MHD ? 11 : 5;   // stored W words: prim (8) + cell E (3)
     constexpr int NF = MHD ? 7 : 5;
-    constexpr int NP = MHD ? 8 : 5;    // primitive words reconstructed
-    const int b = blockIdx.y;
-    const int lo = MHD ? -1 : 0;
-    const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
-    int ext[ 3 ];
-    for( int d = 0; d < 3; ++ d )
-        ext[ d ] = d == axis ? nn[ d ] + 1 : nn[ d ] - 2 * lo;
-    const long long t = ( long long ) blockIdx.x * blockDim.x + threadIdx.x;
-    int ii[ 3 ];
-    ii[ 0 ] = int( t % ext[ 0 ] );
-    ii[ 1 ] = int( ( t / ext[ 0 ] ) % ext[ 1 ] );
-    ii[ 2 ] = int( t / ( ( long long ) ext[ 0 ] * ext[ 1 ] ) );
-    int outside = 0;
-    for( int d = 0; d < 3; ++ d )
-        if( d != axis )
-        {
-            ii[ d ] += lo;
-            outside += ( ii[ d ] < 0 || ii[ d ] >= nn[ d ] );
-        }
-    // corner lines are never read; lanes past the end idle.  Lanes stay alive
-    // until the (warp-collective) selector has run.
-    const bool valid = t < ( long long ) ext[ 0 ] * ext[ 1 ] * ext[ 2 ] && outside <= 1;
     constexpr bool learned = MHD && rsel == KR_RIEMANN_LEARNED;
-    if( ! valid && ! learned )
-        return;
-    const int st = axis == 0 ? 1 : ( axis == 1 ? a.sw1 : a.sw2 );
-    R ql[ 8 ], qr[ 8 ], flx[ 8 ];
-    if( valid )
-        for( int k = 0; k < NP; ++ k )
-        {
-            if( MHD && k == BCC + axis )
-            {
-                const R bn = R( a.bf[ step ][ ibf( a, b, axis, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] );
-                ql[ k ] = qr[ k ] = bn;
-                continue;
-            }
-            const R * p = a.w + iw( a, b, k, NW, ii[ 0 ], ii[ 1 ], ii[ 2 ] );
-            plm_face_fast< R >( p[ -2 * st ], p[ -st ], p[ 0 ], p[ st ], ql[ k ], qr[ k ] );
-        }
-    else
+    R flx[ 8 ];
+    const eos_c< R > e = { R( a.gamma ), R( a.gm1 ), R( a.cv ) };
+    if( ! valid )
         for( int k = 0; k < 8; ++ k )
             ql[ k ] = qr[ k ] = ( k == RHO || k == ENE ) ? R( 1 ) : R( 0 );
-    const eos_c< R > e = { R( a.gamma ), R( a.gm1 ), R( a.cv ) };
     idx_swap( ql + MOM, axis );
     idx_swap( qr + MOM, axis );
     if( ! MHD )
+    {
+        if( ! valid ) return;
         hllc_fast< R >( flx, ql, qr, e );
+    }
     else
     {
         idx_swap( ql + BCC, axis );
         idx_swap( qr + BCC, axis );
-        if( learned )
+        if constexpr( learned )
         {
-            __shared__ __nv_bfloat16 xs[ 4 ][ 32 * MLP_IN ];
+            __shared__ __nv_bfloat16 xs[ 8 ][ 32 * MLP_IN ];
             float f[ MLP_IN ];
             face_features< R >( ql, qr, e.gamma, f );
-            const float z = mlp_logit( f, a.sel_w, a.sel_b, xs[ threadIdx.x >> 5 ] );
+            const float z = mlp_logit( f, a.sel_w, a.sel_b, xs[ warp ] );
             // Per-face choice: HLLE where the network predicts the face safe,
             // HLLD for every flagged face.  (A warp-uniform choice -- HLLE only
             // when all 32 faces of a warp are safe -- avoids running both
@@ -441,14 +412,17 @@ __global__ void __launch_bounds__( 128, 4 ) k_flux( const args_t< R > a, int axi
             else
                 hlld_fast< R >( flx, ql, qr, e );
         }
-        else if( rsel == KR_RIEMANN_HLLE )
-            hlle_fast< R >( flx, ql, qr, e );
         else
-            hlld_fast< R >( flx, ql, qr, e );
-        if( SAMPLE )
+        {
+            if( ! valid ) return;
+            if( rsel == KR_RIEMANN_HLLE )
+                hlle_fast< R >( flx, ql, qr, e );
+            else
+                hlld_fast< R >( flx, ql, qr, e );
+        }
+        if constexpr( SAMPLE )
         {   // training sample: features, and the HLLE-HLLD gap of this face
-            const unsigned long long key = ( ( unsigned long long ) b * 3 + axis ) * 0x9E3779B97F4A7C15ull
-                                         + ( unsigned long long ) t * 0xBF58476D1CE4E5B9ull + a.smp_seed;
+            key = ( key + a.smp_seed ) * 0xBF58476D1CE4E5B9ull;
             if( ( unsigned )( ( key ^ ( key >> 29 ) ) % a.smp_stride ) == 0 )
             {
                 R fe[ 8 ], fd[ 8 ];
@@ -471,10 +445,187 @@ __global__ void __launch_bounds__( 128, 4 ) k_flux( const args_t< R > a, int axi
     for( int k = 0; k < 5; ++ k )
         F[ ifx( a, b, k, NF, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] = flx[ k ];
     if( MHD )
-    {   // mhd/riemann/hlld.h:42-46: B flux -> edge EMF.  Slot 5 holds
-        // E_{(axis+1)%3}, slot 6 holds E_{(axis+2)%3}.
+    {
         F[ ifx( a, b, 5, NF, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] =  flx[ BCC + 2 ];
         F[ ifx( a, b, 6, NF, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] = -flx[ BCC + 1 ];
+    }
+}
+
+// One thread per face.  lines == 0: every face of the sweep (the MHD transverse
+// ghost lines included, mhd/integrator/integrator.h:138-168); lines != 0: only
+// those ghost lines (the tiled kernel below does the rest).
+template< bool MHD, class R, int MODE >
+__global__ void __launch_bounds__( 128, 4 ) k_flux( const args_t< R > a, int axis, int step, int lines )
+{
+    constexpr int NW = MHD ? 11 : 5;   // stored W words: prim (8) + cell E (3)
+    constexpr int NP = MHD ? 8 : 5;    // primitive words reconstructed
+    constexpr bool learned = MHD && MODE == KR_RIEMANN_LEARNED;
+    const int b = blockIdx.y;
+    const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
+    const long long t = ( long long ) blockIdx.x * blockDim.x + threadIdx.x;
+    int ii[ 3 ];
+    int outside = 0;
+    long long total;
+    if( ! lines )
+    {
+        const int lo = MHD ? -1 : 0;
+        int ext[ 3 ];
+        for( int d = 0; d < 3; ++ d )
+            ext[ d ] = d == axis ? nn[ d ] + 1 : nn[ d ] - 2 * lo;
+        total = ( long long ) ext[ 0 ] * ext[ 1 ] * ext[ 2 ];
+        ii[ 0 ] = int( t % ext[ 0 ] );
+        ii[ 1 ] = int( ( t / ext[ 0 ] ) % ext[ 1 ] );
+        ii[ 2 ] = int( t / ( ( long long ) ext[ 0 ] * ext[ 1 ] ) );
+        for( int d = 0; d < 3; ++ d )
+            if( d != axis )
+            {
+                ii[ d ] += lo;
+                outside += ( ii[ d ] < 0 || ii[ d ] >= nn[ d ] );
+            }
+    }
+    else
+    {
+        const int a1 = mod3( axis + 1 ), a2 = mod3( axis + 2 );
+        const int nf = nn[ axis ] + 1;
+        total = ( long long ) nf * ( 2LL * nn[ a2 ] + 2LL * nn[ a1 ] );
+        ii[ axis ] = int( t % nf );
+        long long l = t / nf;
+        if( l < 2LL * nn[ a2 ] )
+        {
+            ii[ a1 ] = ( l & 1 ) ? nn[ a1 ] : -1;
+            ii[ a2 ] = int( l >> 1 );
+        }
+        else
+        {
+            l -= 2LL * nn[ a2 ];
+            ii[ a2 ] = ( l & 1 ) ? nn[ a2 ] : -1;
+            ii[ a1 ] = int( l >> 1 );
+        }
+        outside = 1;
+    }
+    // corner lines are never read; lanes past the end idle.  Lanes stay alive
+    // until the (warp-collective) selector has run.
+    const bool valid = t < total && outside <= 1;
+    if( ! valid && ! learned )
+        return;
+    const int st = axis == 0 ? 1 : ( axis == 1 ? a.sw1 : a.sw2 );
+    R ql[ 8 ], qr[ 8 ];
+    if( valid )
+        for( int k = 0; k < NP; ++ k )
+        {
+            if( MHD && k == BCC + axis )
+            {
+                const R bn = R( a.bf[ step ][ ibf( a, b, axis, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] );
+                ql[ k ] = qr[ k ] = bn;
+                continue;
+            }
+            const R * p = a.w + iw( a, b, k, NW, ii[ 0 ], ii[ 1 ], ii[ 2 ] );
+            plm_face_fast< R >( p[ -2 * st ], p[ -st ], p[ 0 ], p[ st ], ql[ k ], qr[ k ] );
+        }
+    const unsigned long long key = ( ( unsigned long long ) b * 3 + axis ) * 0x9E3779B97F4A7C15ull
+                                 + ( unsigned long long ) ( lines ? t + ( 1ll << 40 ) : t );
+    solve_store< MHD, R, MODE >( a, b, axis, ii, valid, ql, qr, threadIdx.x >> 5, key );
+}
+
+// Shared-memory tiled sweep over the faces whose transverse position lies in
+// the block interior.  A CTA of 32 x 4 threads loads the primitives of its tile
+// once (coalesced, halo of 2 + 1 cells along the sweep) and reconstructs from
+// shared memory.  AX = 1, 2: 32 lanes along x, TS faces along the sweep, one
+// position along the third axis.  AX = 0: TS faces along x, 4 rows along y.
+// Tile t of T covers faces [t*nf/T, (t+1)*nf/T) of the nf = n+1 along the sweep.
+template< bool MHD, class R, int MODE, int AX >
+__global__ void __launch_bounds__( 128, 4 ) k_flux_tile( const args_t< R > a, int step, int T, int TSmax )
+{
+    constexpr int NW = MHD ? 11 : 5;
+    constexpr int NP = MHD ? 8 : 5;
+    extern __shared__ __align__( 16 ) unsigned char smem_raw[  ];
+    R * q = reinterpret_cast< R * >( smem_raw );
+    const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
+    const int b = blockIdx.z;
+    const int nf = nn[ AX ] + 1;
+    const int tid = threadIdx.x + 32 * threadIdx.y;
+    const int warp = threadIdx.y;
+    int tile, f0, f1, base[ 3 ];
+    if( AX != 0 )
+    {   // blockIdx.x = x-tile * T + face tile; blockIdx.y = third-axis position
+        const int A2 = AX == 1 ? 2 : 1;
+        tile = blockIdx.x % T;
+        base[ 0 ] = 32 * ( blockIdx.x / T );
+        base[ A2 ] = blockIdx.y;
+        base[ AX ] = 0;
+    }
+    else
+    {   // blockIdx.x = row group * T + face tile; rows along y; blockIdx.y = z
+        tile = blockIdx.x % T;
+        base[ 1 ] = 4 * ( blockIdx.x / T );
+        base[ 2 ] = blockIdx.y;
+        base[ 0 ] = 0;
+    }
+    f0 = int( ( long long ) tile * nf / T );
+    f1 = int( ( long long )( tile + 1 ) * nf / T );
+    const int ts = f1 - f0;                        // faces in this tile
+    const int ncell = ts + 3;                      // cells f0-2 .. f1
+    // load: q[k][r][c] with (r, c) = (sweep cell, lane) for AX != 0 and
+    // (row, sweep cell) for AX == 0; cells f0-2+s
+    if( AX != 0 )
+    {
+        const int NR = TSmax + 3;
+        for( int idx = tid; idx < NP * ncell * 32; idx += 128 )
+        {
+            const int c = idx & 31, r = ( idx >> 5 ) % ncell, k = ( idx >> 5 ) / ncell;
+            if( MHD && k == BCC + AX )
+                continue;
+            int jj[ 3 ] = { base[ 0 ] + c, base[ 1 ], base[ 2 ] };
+            jj[ AX ] = f0 - 2 + r;
+            q[ ( k * NR + r ) * 32 + c ] = a.w[ iw( a, b, k, NW, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) ];
+        }
+    }
+    else
+    {
+        const int NC = TSmax + 3;
+        for( int idx = tid; idx < NP * 4 * ncell; idx += 128 )
+        {
+            const int c = idx % ncell, r = ( idx / ncell ) % 4, k = idx / ( ncell * 4 );
+            if( MHD && k == BCC )
+                continue;
+            q[ ( k * 4 + r ) * NC + c ] = a.w[ iw( a, b, k, NW, f0 - 2 + c, base[ 1 ] + r, base[ 2 ] ) ];
+        }
+    }
+    __syncthreads(  );
+    // compute: AX != 0 -> face j = threadIdx.y + 4 m, lane c = threadIdx.x;
+    //          AX == 0 -> face j = threadIdx.x + 32 m, row = threadIdx.y
+    const int nloop = AX != 0 ? ( TSmax + 3 ) / 4 : ( TSmax + 31 ) / 32;
+    for( int m = 0; m < nloop; ++ m )
+    {
+        const int j = AX != 0 ? int( threadIdx.y ) + 4 * m : int( threadIdx.x ) + 32 * m;
+        if( AX != 0 && j >= TSmax )
+            break;                                 // j is uniform per warp here
+        const bool valid = j < ts;
+        int ii[ 3 ] = { base[ 0 ], base[ 1 ], base[ 2 ] };
+        if( AX != 0 ) { ii[ 0 ] += threadIdx.x; ii[ AX ] = f0 + j; }
+        else          { ii[ 0 ] = f0 + j; ii[ 1 ] += threadIdx.y; }
+        R ql[ 8 ], qr[ 8 ];
+        if( valid )
+            for( int k = 0; k < NP; ++ k )
+            {
+                if( MHD && k == BCC + AX )
+                {
+                    const R bn = R( a.bf[ step ][ ibf( a, b, AX, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] );
+                    ql[ k ] = qr[ k ] = bn;
+                    continue;
+                }
+                R v[ 4 ];
+                if( AX != 0 )
+                    for( int s = 0; s < 4; ++ s )
+                        v[ s ] = q[ ( k * ( TSmax + 3 ) + j + s ) * 32 + threadIdx.x ];
+                else
+                    for( int s = 0; s < 4; ++ s )
+                        v[ s ] = q[ ( k * 4 + threadIdx.y ) * ( TSmax + 3 ) + j + s ];
+                plm_face_fast< R >( v[ 0 ], v[ 1 ], v[ 2 ], v[ 3 ], ql[ k ], qr[ k ] );
+            }
+        const unsigned long long key = ( ( unsigned long long ) b * 3 + AX ) * 0x9E3779B97F4A7C15ull
+            + ( unsigned long long )( ii[ 0 ] + 1 + ( nn[ 0 ] + 3 ) * ( ( long long )( ii[ 1 ] + 1 ) + ( nn[ 1 ] + 3 ) * ( long long )( ii[ 2 ] + 1 ) ) );
+        solve_store< MHD, R, MODE >( a, b, AX, ii, valid, ql, qr, warp, key );
     }
 }
 
@@ -736,6 +887,7 @@ struct kr_ctx
     cudaGraphExec_t graph_exec = nullptr;
     cudaStream_t graph_stream = nullptr;
     std::vector< geo_t > geo_h;
+    bool no_tiles = false;             // force the per-face flux kernel (testing)
 };
 
 static thread_local std::string g_create_error;
@@ -781,6 +933,79 @@ static args_t< R > make_args( kr_ctx * c )
 
 static inline unsigned blocks_for( long long n, int th ) { return unsigned( ( n + th - 1 ) / th ); }
 
+// Flux sweep along `axis`: the shared-memory tiled kernel over the interior
+// transverse positions plus, for MHD, the per-face kernel over the transverse
+// ghost lines; the per-face kernel alone where the tile shape does not fit.
+struct flux_tiling { int T, TSmax; size_t smem; bool ok; };
+
+template< class R >
+static flux_tiling tiling_for( const kr_ctx * c, int axis, int np )
+{
+    const int * n = c->cfg.n;
+    flux_tiling t;
+    const int nf = n[ axis ] + 1;
+    // about 32 faces per tile in FP32, 16 in FP64 (shared memory per CTA)
+    t.T = std::max( 1, nf / ( sizeof( R ) == 4 ? 32 : 16 ) );
+    t.TSmax = ( nf + t.T - 1 ) / t.T;
+    t.smem = axis != 0 ? size_t( np ) * ( t.TSmax + 3 ) * 32 * sizeof( R )
+                       : size_t( np ) * 4 * ( t.TSmax + 3 ) * sizeof( R );
+    t.ok = n[ 0 ] % 32 == 0 && n[ 1 ] % 4 == 0 && t.smem <= 96 * 1024;
+    return t;
+}
+
+template< bool MHD, class R, int MODE, int AX >
+static void launch_tile( kr_ctx * c, cudaStream_t st, const args_t< R > & a, int stage,
+                         const flux_tiling & t )
+{
+    const int * n = c->cfg.n;
+    dim3 grid;
+    if( AX == 0 ) grid = dim3( t.T * ( n[ 1 ] / 4 ), n[ 2 ], c->nblk );
+    else          grid = dim3( t.T * ( n[ 0 ] / 32 ), AX == 1 ? n[ 2 ] : n[ 1 ], c->nblk );
+    static bool attr_set = false;
+    if( ! attr_set && t.smem > 48 * 1024 )
+    {
+        cudaFuncSetAttribute( k_flux_tile< MHD, R, MODE, AX >,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024 );
+        attr_set = true;
+    }
+    k_flux_tile< MHD, R, MODE, AX ><<< grid, dim3( 32, 4 ), t.smem, st >>>( a, stage, t.T, t.TSmax );
+}
+
+template< bool MHD, class R, int MODE >
+static void launch_flux( kr_ctx * c, cudaStream_t st, const args_t< R > & a, int axis, int stage )
+{
+    const int * n = c->cfg.n;
+    constexpr int NP = MHD ? 8 : 5;
+    const flux_tiling t = tiling_for< R >( c, axis, NP );
+    if( ! t.ok || c->no_tiles )
+    {
+        long long nface = 1;
+        for( int d = 0; d < 3; ++ d )
+            nface *= ( d == axis ) ? n[ d ] + 1 : n[ d ] + ( MHD ? 2 : 0 );
+        k_flux< MHD, R, MODE ><<< dim3( blocks_for( nface, 128 ), c->nblk ), 128, 0, st >>>( a, axis, stage, 0 );
+        return;
+    }
+    if( axis == 0 )      launch_tile< MHD, R, MODE, 0 >( c, st, a, stage, t );
+    else if( axis == 1 ) launch_tile< MHD, R, MODE, 1 >( c, st, a, stage, t );
+    else                 launch_tile< MHD, R, MODE, 2 >( c, st, a, stage, t );
+    if( MHD )
+    {
+        const int a1 = ( axis + 1 ) % 3, a2 = ( axis + 2 ) % 3;
+        const long long nline = ( long long )( n[ axis ] + 1 ) * ( 2LL * n[ a1 ] + 2LL * n[ a2 ] );
+        k_flux< MHD, R, MODE ><<< dim3( blocks_for( nline, 128 ), c->nblk ), 128, 0, st >>>( a, axis, stage, 1 );
+    }
+}
+
+template< bool MHD, class R >
+static void launch_flux_mode( kr_ctx * c, cudaStream_t st, const args_t< R > & a, int axis,
+                              int stage, int mode )
+{
+    if( mode == FLUX_SAMPLE )                   launch_flux< MHD, R, FLUX_SAMPLE >( c, st, a, axis, stage );
+    else if( mode == KR_RIEMANN_LEARNED && MHD ) launch_flux< MHD, R, KR_RIEMANN_LEARNED >( c, st, a, axis, stage );
+    else if( mode == KR_RIEMANN_HLLE && MHD )    launch_flux< MHD, R, KR_RIEMANN_HLLE >( c, st, a, axis, stage );
+    else                                          launch_flux< MHD, R, KR_RIEMANN_DEFAULT >( c, st, a, axis, stage );
+}
+
 // Enqueue one Heun step on stream st (SAMPLE: also log selector training samples).
 template< bool MHD, class R, bool SAMPLE = false >
 static void enqueue_step( kr_ctx * c, cudaStream_t st )
@@ -798,18 +1023,7 @@ static void enqueue_step( kr_ctx * c, cudaStream_t st )
         k_ghost< MHD, R ><<< dim3( blocks_for( nghost, 256 ), nb ), 256, 0, st >>>( a, stage );
         for( int axis = 2; axis >= 0; -- axis )
         {
-            long long nface = 1;
-            for( int d = 0; d < 3; ++ d )
-                nface *= ( d == axis ) ? n[ d ] + 1 : n[ d ] + ( MHD ? 2 : 0 );
-            const dim3 g( blocks_for( nface, 128 ), nb );
-            if( SAMPLE )
-                k_flux< MHD, R, FLUX_SAMPLE ><<< g, 128, 0, st >>>( a, axis, stage );
-            else if( c->cfg.riemann == KR_RIEMANN_LEARNED )
-                k_flux< MHD, R, KR_RIEMANN_LEARNED ><<< g, 128, 0, st >>>( a, axis, stage );
-            else if( c->cfg.riemann == KR_RIEMANN_HLLE )
-                k_flux< MHD, R, KR_RIEMANN_HLLE ><<< g, 128, 0, st >>>( a, axis, stage );
-            else
-                k_flux< MHD, R, KR_RIEMANN_DEFAULT ><<< g, 128, 0, st >>>( a, axis, stage );
+            launch_flux_mode< MHD, R >( c, st, a, axis, stage, SAMPLE ? FLUX_SAMPLE : c->cfg.riemann );
         }
         if( MHD )
             k_emf< R ><<< dim3( blocks_for( nlat, 256 ), nb ), 256, 0, st >>>( a );
@@ -851,17 +1065,7 @@ static bool profile_step( kr_ctx * c, double * ms )
         timed( 1, [ & ] { k_ghost< MHD, R ><<< dim3( blocks_for( nghost, 256 ), nb ), 256, 0, st >>>( a, stage ); } );
         for( int axis = 2; axis >= 0; -- axis )
         {
-            long long nface = 1;
-            for( int d = 0; d < 3; ++ d )
-                nface *= ( d == axis ) ? n[ d ] + 1 : n[ d ] + ( MHD ? 2 : 0 );
-            const dim3 g( blocks_for( nface, 128 ), nb );
-            timed( 4 - axis, [ & ] {
-                if( c->cfg.riemann == KR_RIEMANN_LEARNED )
-                    k_flux< MHD, R, KR_RIEMANN_LEARNED ><<< g, 128, 0, st >>>( a, axis, stage );
-                else if( c->cfg.riemann == KR_RIEMANN_HLLE )
-                    k_flux< MHD, R, KR_RIEMANN_HLLE ><<< g, 128, 0, st >>>( a, axis, stage );
-                else
-                    k_flux< MHD, R, KR_RIEMANN_DEFAULT ><<< g, 128, 0, st >>>( a, axis, stage ); } );
+            timed( 4 - axis, [ & ] { launch_flux_mode< MHD, R >( c, st, a, axis, stage, c->cfg.riemann ); } );
         }
         if( MHD )
             timed( 5, [ & ] { k_emf< R ><<< dim3( blocks_for( nlat, 256 ), nb ), 256, 0, st >>>( a ); } );
@@ -1009,6 +1213,7 @@ kr_ctx * kr_ctx_create( const kr_cfg * cfg )
 
     kr_ctx * c = new kr_ctx;
     c->cfg = * cfg;
+    c->no_tiles = ( cfg->reserved[ 0 ] & 1 ) != 0;
     const int * n = cfg->n;
     c->nblk = cfg->nb[ 0 ] * cfg->nb[ 1 ] * cfg->nb[ 2 ];
     c->nw = cfg->mhd ? 8 : 5;
@@ -1379,7 +1584,14 @@ int kr_profile_step( kr_ctx * c, int n_kinds, double * ms )
 int kr_launches_per_step( kr_ctx * c )
 {
     if( ! c ) return -1;
-    return 2 + 2 * ( c->cfg.mhd ? 7 : 6 );
+    int flux = 0;
+    for( int axis = 0; axis < 3; ++ axis )
+    {
+        const flux_tiling t = c->cfg.precision == 1 ? tiling_for< float >( c, axis, c->cfg.mhd ? 8 : 5 )
+                                                    : tiling_for< double >( c, axis, c->cfg.mhd ? 8 : 5 );
+        flux += ( t.ok && ! c->no_tiles && c->cfg.mhd ) ? 2 : 1;
+    }
+    return 2 + 2 * ( ( c->cfg.mhd ? 4 : 3 ) + flux );
 }
 
 int kr_diagnostics( kr_ctx * c, double * max_div_b, double * totals5 )

@@ -24,7 +24,7 @@ def _ptr(a):
 class Dynamics:
     def __init__(self, mhd, nb, n, gamma=1.66667, cfl=0.3, precision=2, riemann=0,
                  x_min=(0, 0, 0), x_max=(1, 1, 1), rho_floor=1e-9, tmp_floor=1e-9,
-                 dt_init=0.0, dt_expand=2.0, device=0):
+                 dt_init=0.0, dt_expand=2.0, device=0, flags=0):
         lib = L.lib()
         c = L.kr_cfg()
         lib.kr_cfg_default(ctypes.byref(c))
@@ -35,6 +35,7 @@ class Dynamics:
         c.gamma, c.cfl = float(gamma), float(cfl)
         c.rho_floor, c.tmp_floor = float(rho_floor), float(tmp_floor)
         c.dt_init, c.dt_expand, c.device = float(dt_init), float(dt_expand), int(device)
+        c.reserved[0] = int(flags)           # bit 0: per-face flux kernel only
         self.cfg = c
         self._h = lib.kr_ctx_create(ctypes.byref(c))
         if not self._h:
