@@ -66,8 +66,8 @@ typedef struct
     double dt_init;            /* [cycle] dt_init (0: unset)                     */
     double dt_expand;          /* [cycle] dt_expand                              */
     int    device;             /* CUDA device ordinal                            */
-    int    reserved[ 7 ];      /* reserved[0] bit 0: use the per-face flux kernel */
-                               /* for every sweep (no shared-memory tiles); test */
+    int    reserved[ 7 ];      /* reserved[0] bit 0: shared-memory tiled flux    */
+                               /* sweeps (opt-in; default per-face kernel)       */
 } kr_cfg;
 
 typedef struct kr_ctx kr_ctx;

@@ -20,10 +20,15 @@ template< class R > struct eos_c
     R gamma, gm1, cv;        // gamma, gamma - 1, 1 / (gamma - 1)
 };
 
+// FP64: correctly rounded reciprocal / IEEE square root.  FP32 (the mixed
+// step, whose error budget is 1e-4 in density): the SFU approximations, one
+// MUFU instruction each instead of an IEEE refinement sequence.
 __device__ __forceinline__ double rcp( double x ) { return __drcp_rn( x ); }
-__device__ __forceinline__ float  rcp( float x )  { return __frcp_rn( x ); }
+__device__ __forceinline__ float  rcp( float x )  { return __fdividef( 1.0f, x ); }
 __device__ __forceinline__ double rsq( double x ) { return rsqrt( x ); }
 __device__ __forceinline__ float  rsq( float x )  { return rsqrtf( x ); }
+__device__ __forceinline__ double fsqrt( double x ) { return sqrt( x ); }
+__device__ __forceinline__ float  fsqrt( float x )  { return x > 0.f ? x * rsqrtf( x ) : 0.f; }
 
 // PLM on one face from the four cells around it (plm.h:116-153 mathematics).
 template< class R > __device__ __forceinline__
@@ -60,7 +65,7 @@ R c_fms_fast( R pre, R inv_rho, R bn2, R bt2, R gam )
     const R v_t2  = bt2 * inv_rho;
     const R q_2   = v_ax2 + v_t2 + cs_2;
     const R r_2   = v_ax2 + v_t2 - cs_2;
-    return sqrt( R( 0.5f ) * ( q_2 + sqrt( r_2 * r_2 + R( 4 ) * cs_2 * v_t2 ) ) );
+    return fsqrt( R( 0.5f ) * ( q_2 + fsqrt( r_2 * r_2 + R( 4 ) * cs_2 * v_t2 ) ) );
 }
 
 ////////////////////////////////////////////////////////////
@@ -74,8 +79,8 @@ void hllc_fast( R * flx, const R * wl, const R * wr, const eos_c< R > & e )
     R v2r = wr[ MOM ] * wr[ MOM ] + wr[ MOM + 1 ] * wr[ MOM + 1 ] + wr[ MOM + 2 ] * wr[ MOM + 2 ];
     const R el = wl[ ENE ] * e.cv + wl[ RHO ] * v2l * R( 0.5f );
     const R er = wr[ ENE ] * e.cv + wr[ RHO ] * v2r * R( 0.5f );
-    const R cl = sqrt( e.gamma * rmax( wl[ ENE ] * irl, R( 0 ) ) );
-    const R cr = sqrt( e.gamma * rmax( wr[ ENE ] * irr, R( 0 ) ) );
+    const R cl = fsqrt( e.gamma * rmax( wl[ ENE ] * irl, R( 0 ) ) );
+    const R cr = fsqrt( e.gamma * rmax( wr[ ENE ] * irr, R( 0 ) ) );
     const R rsl = rsq( wl[ RHO ] ), rsr = rsq( wr[ RHO ] );
     const R sqrtdl = wl[ RHO ] * rsl, sqrtdr = wr[ RHO ] * rsr;
     const R isdlpdr = rcp( sqrtdl + sqrtdr );
@@ -87,7 +92,7 @@ void hllc_fast( R * flx, const R * wl, const R * wr, const eos_c< R > & e )
     const R v2roe = wroe[ MOM ] * wroe[ MOM ] + wroe[ MOM + 1 ] * wroe[ MOM + 1 ]
                   + wroe[ MOM + 2 ] * wroe[ MOM + 2 ];
     const R q = hroe - R( 0.5f ) * v2roe;
-    const R a = ( q <= 0 ) ? R( 0 ) : sqrt( gam1_roe * q );
+    const R a = ( q <= 0 ) ? R( 0 ) : fsqrt( gam1_roe * q );
     const R al = rmin( wroe[ MOM ] - a, wl[ MOM ] - cl );
     const R ar = rmax( wroe[ MOM ] + a, wr[ MOM ] + cr );
     const R bp = ar > 0 ? ar : R( 0 );

@@ -35,7 +35,7 @@ class Dynamics:
         c.gamma, c.cfl = float(gamma), float(cfl)
         c.rho_floor, c.tmp_floor = float(rho_floor), float(tmp_floor)
         c.dt_init, c.dt_expand, c.device = float(dt_init), float(dt_expand), int(device)
-        c.reserved[0] = int(flags)           # bit 0: per-face flux kernel only
+        c.reserved[0] = int(flags)           # bit 0: shared-memory tiled flux sweeps
         self.cfg = c
         self._h = lib.kr_ctx_create(ctypes.byref(c))
         if not self._h:
