@@ -39,7 +39,18 @@
 extern "C" {
 #endif
 
-#define KR_ABI_VERSION 1
+#define KR_ABI_VERSION 2
+
+/* [boundary] kinds per side (hydro/boundary/phys_functors.h:11-91): an axis is
+ * periodic only when both its sides are KR_BC_PER. */
+enum kr_bc_t
+{
+    KR_BC_PER  = 0,            /* periodic                                       */
+    KR_BC_OUT  = 1,            /* outflow: zero gradient, inflow velocity clamped */
+    KR_BC_REF  = 2,            /* reflect: mirror, normal velocity negated        */
+    KR_BC_FRE  = 3,            /* free: zero gradient                             */
+    KR_BC_FIXD = 4             /* fixed: ghosts = w_fix (the [init] medium)       */
+};
 
 /* Riemann solver selection ([b200] riemann). */
 enum kr_riemann_t
@@ -66,6 +77,9 @@ typedef struct
     double dt_init;            /* [cycle] dt_init (0: unset)                     */
     double dt_expand;          /* [cycle] dt_expand                              */
     int    device;             /* CUDA device ordinal                            */
+    int    bc[ 6 ];            /* enum kr_bc_t for x-, x+, y-, y+, z-, z+;       */
+                               /* non-periodic sides: hydro only                 */
+    double w_fix[ 5 ];         /* KR_BC_FIXD primitive state: rho, p, v0..2       */
     int    reserved[ 7 ];      /* reserved[0] bit 0: shared-memory tiled flux    */
                                /* sweeps (opt-in; default per-face kernel)       */
 } kr_cfg;

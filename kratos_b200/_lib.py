@@ -5,7 +5,8 @@ import os
 _PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_PKG, "libkrb200.so")
 
-KR_ABI_VERSION = 1
+KR_ABI_VERSION = 2
+BC_KINDS = {"per": 0, "out": 1, "ref": 2, "fre": 3, "fixd": 4}
 KR_RIEMANN_DEFAULT, KR_RIEMANN_HLLE, KR_RIEMANN_LEARNED = 0, 1, 2
 
 
@@ -26,6 +27,8 @@ class kr_cfg(ctypes.Structure):
         ("dt_init", ctypes.c_double),
         ("dt_expand", ctypes.c_double),
         ("device", ctypes.c_int),
+        ("bc", ctypes.c_int * 6),
+        ("w_fix", ctypes.c_double * 5),
         ("reserved", ctypes.c_int * 7),
     ]
 

@@ -75,7 +75,10 @@ struct args_t
     unsigned long long * smp_n;
     long long smp_max;
     unsigned smp_stride, smp_seed;
-    const int * nbr;                  // [block][27]
+    const int * nbr;                  // [block][27], -1 past a physical boundary
+    int nbk[ 3 ];                     // blocks per axis
+    int bc[ 6 ];                      // kr_bc_t per side
+    double w_fix[ 5 ];
     scal_t * s;
 };
 
@@ -301,6 +304,8 @@ __global__ void __launch_bounds__( 256 ) k_ghost( const args_t< R > a, int step 
         const int j1 = wrap_axis( i1, a.n1, s1 );
         const int j2 = wrap_axis( i2, a.n2, s2 );
         const int src = a.nbr[ b * 27 + ( s0 + 1 ) + 3 * ( s1 + 1 ) + 9 * ( s2 + 1 ) ];
+        if( src < 0 )
+            return;                              // physical boundary: k_phys
         for( int k = 0; k < NW; ++ k )
             a.w[ iw( a, b, k, NW, i0, i1, i2 ) ] = a.w[ iw( a, src, k, NW, j0, j1, j2 ) ];
         return;
@@ -340,9 +345,61 @@ __global__ void __launch_bounds__( 256 ) k_ghost( const args_t< R > a, int step 
             if( d != c )
                 jj[ d ] = wrap_axis( ii[ d ], nn[ d ], sh[ d ] );
         const int src = a.nbr[ b * 27 + ( sh[ 0 ] + 1 ) + 3 * ( sh[ 1 ] + 1 ) + 9 * ( sh[ 2 ] + 1 ) ];
+        if( src < 0 )
+            return;
         double * BF = a.bf[ step ];
         BF[ ibf( a, b, c, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] = BF[ ibf( a, src, c, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) ];
         return;
+    }
+}
+
+////////////////////////////////////////////////////////////
+// Physical boundaries on the primitives (hydro/boundary/phys.h:95-139,
+// phys_functors.h:11-91).  One thread per transverse interior position of a
+// domain-edge side of a block: the two cells next to the boundary (index 0 =
+// adjacent) feed the two ghost cells.  Hydro only.
+
+template< class R >
+__global__ void __launch_bounds__( 128 ) k_phys( const args_t< R > a )
+{
+    const int b = blockIdx.z, side = blockIdx.y;
+    const int axis = side >> 1, right = side & 1;
+    const int kind = a.bc[ side ];
+    if( kind == KR_BC_PER )
+        return;
+    const int reg[ 3 ] = { b % a.nbk[ 0 ], ( b / a.nbk[ 0 ] ) % a.nbk[ 1 ], b / ( a.nbk[ 0 ] * a.nbk[ 1 ] ) };
+    if( reg[ axis ] != ( right ? a.nbk[ axis ] - 1 : 0 ) )
+        return;
+    const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
+    const int a1 = mod3( axis + 1 ), a2 = mod3( axis + 2 );
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if( t >= nn[ a1 ] * nn[ a2 ] )
+        return;
+    int ii[ 3 ];
+    ii[ a1 ] = t % nn[ a1 ];
+    ii[ a2 ] = t / nn[ a1 ];
+    const int i_mom = MOM + axis;
+    R c0[ 5 ], c1[ 5 ];
+    ii[ axis ] = right ? nn[ axis ] - 1 : 0;
+    for( int k = 0; k < 5; ++ k ) c0[ k ] = a.w[ iw( a, b, k, 5, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ];
+    ii[ axis ] = right ? nn[ axis ] - 2 : 1;
+    for( int k = 0; k < 5; ++ k ) c1[ k ] = a.w[ iw( a, b, k, 5, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ];
+    if( kind == KR_BC_OUT && c0[ i_mom ] * R( right ? -1 : 1 ) > 0 )
+        c0[ i_mom ] = 0;                     // no inflow through an outflow side
+    for( int g = 1; g <= 2; ++ g )           // ghost g: -g (left) or n - 1 + g (right)
+    {
+        ii[ axis ] = right ? nn[ axis ] - 1 + g : -g;
+        for( int k = 0; k < 5; ++ k )
+        {
+            R v;
+            if( kind == KR_BC_REF )
+                v = ( g == 1 ? c0[ k ] : c1[ k ] ) * R( k == i_mom ? -1 : 1 );
+            else if( kind == KR_BC_FIXD )
+                v = R( a.w_fix[ k ] );
+            else
+                v = c0[ k ];                 // outflow, free: zero gradient
+            a.w[ iw( a, b, k, 5, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] = v;
+        }
     }
 }
 
@@ -925,6 +982,9 @@ static args_t< R > make_args( kr_ctx * c )
     for( int d = 0; d < 3; ++ d ) a.f[ d ] = ( R * ) c->f[ d ];
     a.ee = ( R * ) c->ee;
     a.geo = c->geo; a.nbr = c->nbr; a.s = c->s;
+    for( int d = 0; d < 3; ++ d ) a.nbk[ d ] = c->cfg.nb[ d ];
+    for( int k = 0; k < 6; ++ k ) a.bc[ k ] = c->cfg.bc[ k ];
+    for( int k = 0; k < 5; ++ k ) a.w_fix[ k ] = c->cfg.w_fix[ k ];
     a.sel_w = c->sel_w; a.sel_b = c->sel_b; a.sel_thr = c->sel_thr; a.sel_cnt = c->sel_cnt;
     a.smp = c->smp; a.smp_n = c->smp_n; a.smp_max = c->smp_max;
     a.smp_stride = c->smp_stride; a.smp_seed = c->smp_seed;
@@ -932,6 +992,20 @@ static args_t< R > make_args( kr_ctx * c )
 }
 
 static inline unsigned blocks_for( long long n, int th ) { return unsigned( ( n + th - 1 ) / th ); }
+
+static bool has_phys( const kr_ctx * c )
+{
+    for( int k = 0; k < 6; ++ k )
+        if( c->cfg.bc[ k ] != KR_BC_PER )
+            return true;
+    return false;
+}
+
+static long long phys_sites( const kr_ctx * c )
+{   // largest transverse face count of a side
+    const int * n = c->cfg.n;
+    return std::max( { ( long long ) n[ 1 ] * n[ 2 ], ( long long ) n[ 0 ] * n[ 2 ], ( long long ) n[ 0 ] * n[ 1 ] } );
+}
 
 // Flux sweep along `axis`: the shared-memory tiled kernel over the interior
 // transverse positions plus, for MHD, the per-face kernel over the transverse
@@ -1021,6 +1095,8 @@ static void enqueue_step( kr_ctx * c, cudaStream_t st )
     {
         k_c2p< MHD, R ><<< dim3( blocks_for( c->nc, 256 ), nb ), 256, 0, st >>>( a, stage );
         k_ghost< MHD, R ><<< dim3( blocks_for( nghost, 256 ), nb ), 256, 0, st >>>( a, stage );
+        if( ! MHD && has_phys( c ) )
+            k_phys< R ><<< dim3( blocks_for( phys_sites( c ), 128 ), 6, nb ), 128, 0, st >>>( a );
         for( int axis = 2; axis >= 0; -- axis )
         {
             launch_flux_mode< MHD, R >( c, st, a, axis, stage, SAMPLE ? FLUX_SAMPLE : c->cfg.riemann );
@@ -1062,7 +1138,10 @@ static bool profile_step( kr_ctx * c, double * ms )
     for( int stage = 0; stage < 2; ++ stage )
     {
         timed( 0, [ & ] { k_c2p< MHD, R ><<< dim3( blocks_for( c->nc, 256 ), nb ), 256, 0, st >>>( a, stage ); } );
-        timed( 1, [ & ] { k_ghost< MHD, R ><<< dim3( blocks_for( nghost, 256 ), nb ), 256, 0, st >>>( a, stage ); } );
+        timed( 1, [ & ] {
+            k_ghost< MHD, R ><<< dim3( blocks_for( nghost, 256 ), nb ), 256, 0, st >>>( a, stage );
+            if( ! MHD && has_phys( c ) )
+                k_phys< R ><<< dim3( blocks_for( phys_sites( c ), 128 ), 6, nb ), 128, 0, st >>>( a ); } );
         for( int axis = 2; axis >= 0; -- axis )
         {
             timed( 4 - axis, [ & ] { launch_flux_mode< MHD, R >( c, st, a, axis, stage, c->cfg.riemann ); } );
@@ -1195,6 +1274,19 @@ kr_ctx * kr_ctx_create( const kr_cfg * cfg )
         g_create_error = "kr_ctx_create: precision must be 1 (mixed) or 2 (FP64)";
         return nullptr;
     }
+    for( int k = 0; k < 6; ++ k )
+        if( cfg->bc[ k ] < KR_BC_PER || cfg->bc[ k ] > KR_BC_FIXD
+            || ( cfg->mhd && cfg->bc[ k ] != KR_BC_PER ) )
+        {
+            g_create_error = "kr_ctx_create: boundary kinds must be kr_bc_t; non-periodic sides are hydro only";
+            return nullptr;
+        }
+    for( int a = 0; a < 3; ++ a )
+        if( ( cfg->bc[ 2 * a ] == KR_BC_PER ) != ( cfg->bc[ 2 * a + 1 ] == KR_BC_PER ) )
+        {
+            g_create_error = "kr_ctx_create: a periodic axis needs both sides periodic";
+            return nullptr;
+        }
     if( cfg->riemann != KR_RIEMANN_DEFAULT && ! cfg->mhd )
     {
         g_create_error = "kr_ctx_create: HLLE / learned selection is MHD only";
@@ -1279,9 +1371,16 @@ kr_ctx * kr_ctx_create( const kr_cfg * cfg )
         {
             const int sh[ 3 ] = { k % 3 - 1, ( k / 3 ) % 3 - 1, k / 9 - 1 };
             int r[ 3 ];
+            bool exists = true;
             for( int a = 0; a < 3; ++ a )
-                r[ a ] = ( reg[ a ] + sh[ a ] + cfg->nb[ a ] ) % cfg->nb[ a ];
-            nbr[ b * 27 + k ] = r[ 0 ] + cfg->nb[ 0 ] * ( r[ 1 ] + cfg->nb[ 1 ] * r[ 2 ] );
+            {
+                r[ a ] = reg[ a ] + sh[ a ];
+                const bool periodic = cfg->bc[ 2 * a ] == KR_BC_PER && cfg->bc[ 2 * a + 1 ] == KR_BC_PER;
+                if( ( r[ a ] < 0 || r[ a ] >= cfg->nb[ a ] ) && ! periodic )
+                    exists = false;          // past a physical boundary: no neighbour
+                r[ a ] = ( r[ a ] + cfg->nb[ a ] ) % cfg->nb[ a ];
+            }
+            nbr[ b * 27 + k ] = exists ? r[ 0 ] + cfg->nb[ 0 ] * ( r[ 1 ] + cfg->nb[ 1 ] * r[ 2 ] ) : -1;
         }
     }
     scal_t s0{};
@@ -1594,7 +1693,7 @@ int kr_launches_per_step( kr_ctx * c )
                                                     : tiling_for< double >( c, axis, c->cfg.mhd ? 8 : 5 );
         flux += ( t.ok && ! c->no_tiles && c->cfg.mhd ) ? 2 : 1;
     }
-    return 2 + 2 * ( ( c->cfg.mhd ? 4 : 3 ) + flux );
+    return 2 + 2 * ( ( c->cfg.mhd ? 4 : 3 ) + flux + ( ! c->cfg.mhd && has_phys( c ) ? 1 : 0 ) );
 }
 
 int kr_diagnostics( kr_ctx * c, double * max_div_b, double * totals5 )

@@ -24,7 +24,8 @@ def _ptr(a):
 class Dynamics:
     def __init__(self, mhd, nb, n, gamma=1.66667, cfl=0.3, precision=2, riemann=0,
                  x_min=(0, 0, 0), x_max=(1, 1, 1), rho_floor=1e-9, tmp_floor=1e-9,
-                 dt_init=0.0, dt_expand=2.0, device=0, flags=0):
+                 dt_init=0.0, dt_expand=2.0, device=0, flags=0,
+                 kinds=("per",) * 6, w_fix=(0, 0, 0, 0, 0)):
         lib = L.lib()
         c = L.kr_cfg()
         lib.kr_cfg_default(ctypes.byref(c))
@@ -36,6 +37,10 @@ class Dynamics:
         c.rho_floor, c.tmp_floor = float(rho_floor), float(tmp_floor)
         c.dt_init, c.dt_expand, c.device = float(dt_init), float(dt_expand), int(device)
         c.reserved[0] = int(flags)           # bit 0: shared-memory tiled flux sweeps
+        for k in range(6):
+            c.bc[k] = L.BC_KINDS[kinds[k]]
+        for k in range(5):
+            c.w_fix[k] = float(w_fix[k])
         self.cfg = c
         self._h = lib.kr_ctx_create(ctypes.byref(c))
         if not self._h:

@@ -26,7 +26,12 @@ class _Cfg(ctypes.Structure):
         ("t_floor", ctypes.c_double),
         ("dt_expand", ctypes.c_double),
         ("n_threads", ctypes.c_int),
+        ("bc", ctypes.c_int * 6),
+        ("w_fix", ctypes.c_double * 5),
     ]
+
+
+BC_KINDS = {"per": 0, "out": 1, "ref": 2, "fre": 3, "fixd": 4}
 
 
 _lib = None
@@ -77,7 +82,8 @@ class OracleMesh:
     n1+5, n0+5, 3] (face lattice with 2 ghost layers)."""
 
     def __init__(self, mhd, nb, n, gamma, cfl=0.3, x_min=(0, 0, 0), x_max=(1, 1, 1),
-                 d_floor=1e-9, t_floor=1e-9, dt_expand=2.0, dt_init=0.0, n_threads=0):
+                 d_floor=1e-9, t_floor=1e-9, dt_expand=2.0, dt_init=0.0, n_threads=0,
+                 kinds=("per",) * 6, w_fix=(0, 0, 0, 0, 0)):
         c = _Cfg()
         c.mhd = int(mhd)
         for a in range(3):
@@ -85,12 +91,18 @@ class OracleMesh:
             c.x_min[a], c.x_max[a] = float(x_min[a]), float(x_max[a])
         c.gamma, c.cfl, c.d_floor, c.t_floor = float(gamma), float(cfl), float(d_floor), float(t_floor)
         c.dt_expand, c.n_threads = float(dt_expand), int(n_threads)
+        for k in range(6):
+            c.bc[k] = BC_KINDS[kinds[k]]
+        for k in range(5):
+            c.w_fix[k] = float(w_fix[k])
         self.cfg = c
         self.mhd = bool(mhd)
         self.nb, self.n = tuple(nb), tuple(n)
         self.nblk = nb[0] * nb[1] * nb[2]
         self.nw = 8 if mhd else 5
         self._h = lib().kro_create(ctypes.byref(c))
+        if not self._h:
+            raise ValueError("oracle: non-periodic boundaries are restated for hydro only")
         self.t = 0.0
         # cycle.cpp:163-166: an unset dt_init starts the device dt at FLT_MAX / 10
         self.dt_bound = dt_init if dt_init >= np.finfo(np.float32).tiny else FLT_MAX / 10

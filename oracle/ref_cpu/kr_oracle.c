@@ -169,6 +169,10 @@ double kro_dx( const kro_mesh * m, int b, int a ) { return m->dx0[ b * 3 + a ]; 
 
 kro_mesh * kro_create( const kro_cfg * cfg )
 {
+    if( cfg->mhd )
+        for( int s = 0; s < 6; ++ s )
+            if( cfg->bc[ s ] != KRO_PER )
+                return NULL;                 /* non-periodic MHD: not restated */
     kro_mesh * m = ( kro_mesh * ) calloc( 1, sizeof( kro_mesh ) );
     m->c    = * cfg;
     m->nw   = cfg->mhd ? 8 : 5;
@@ -407,12 +411,27 @@ static inline int wrap( int i, int n, int * shift )
     * shift = 0; return i;
 }
 
+static inline int periodic_axis( const kro_mesh * m, int a )
+{   /* meshgen.cpp:51-55: an axis is periodic when its kinds say "per" */
+    return m->c.bc[ 2 * a ] == KRO_PER && m->c.bc[ 2 * a + 1 ] == KRO_PER;
+}
+
+/* Neighbour block in direction sh, or -1 past a non-periodic domain edge
+ * (no tree neighbour there: tree.cpp neighbour search). */
 static inline int nbr_block( const kro_mesh * m, int b, const int sh[ 3 ] )
 {
     int reg[ 3 ] = { b % m->c.nb[ 0 ], ( b / m->c.nb[ 0 ] ) % m->c.nb[ 1 ],
                      b / ( m->c.nb[ 0 ] * m->c.nb[ 1 ] ) };
     for( int a = 0; a < 3; ++ a )
-        reg[ a ] = ( reg[ a ] + sh[ a ] + m->c.nb[ a ] ) % m->c.nb[ a ];
+    {
+        reg[ a ] += sh[ a ];
+        if( reg[ a ] < 0 || reg[ a ] >= m->c.nb[ a ] )
+        {
+            if( ! periodic_axis( m, a ) )
+                return -1;
+            reg[ a ] = ( reg[ a ] + m->c.nb[ a ] ) % m->c.nb[ a ];
+        }
+    }
     return reg[ 0 ] + m->c.nb[ 0 ] * ( reg[ 1 ] + m->c.nb[ 1 ] * reg[ 2 ] );
 }
 
@@ -435,6 +454,8 @@ static void ghost_block( kro_mesh * m, int b, void * aux )
         if( ! sh[ 0 ] && ! sh[ 1 ] && ! sh[ 2 ] )
             continue;
         const int s = nbr_block( m, b, sh );
+        if( s < 0 )
+            continue;                        /* physical boundary: bc_block */
         const double * src = m->w + ( size_t ) s * m->nw_cells * nw + iw( m, j[ 0 ], j[ 1 ], j[ 2 ] );
         memcpy( w + iw( m, i0, i1, i2 ), src, sizeof( double ) * nw );
     }
@@ -473,6 +494,70 @@ static void ghost_block( kro_mesh * m, int b, void * aux )
         const int s = nbr_block( m, b, sh );
         bf[ ib( m, i0, i1, i2 ) + c ]
             = m->bf[ step ][ ( size_t ) s * m->nbf + ib( m, j[ 0 ], j[ 1 ], j[ 2 ] ) + c ];
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* Physical boundaries on the primitives (hydro/boundary/phys.h:95-139,  */
+/* phys_functors.h:11-91): for every transverse interior position of a   */
+/* domain-edge side, the n_gh cells next to the boundary are copied to a */
+/* buffer (index 0 = adjacent cell), the functor fills the ghost part of */
+/* the buffer, and the ghosts are written back.                          */
+
+static void bc_block( kro_mesh * m, int b, void * aux )
+{
+    ( void ) aux;
+    const int nw = m->nw;
+    const int * n = m->c.n;
+    const int reg[ 3 ] = { b % m->c.nb[ 0 ], ( b / m->c.nb[ 0 ] ) % m->c.nb[ 1 ],
+                           b / ( m->c.nb[ 0 ] * m->c.nb[ 1 ] ) };
+    double * w = m->w + ( size_t ) b * m->nw_cells * nw;
+    for( int side = 0; side < 6; ++ side )
+    {
+        const int axis = side / 2, right = side & 1;
+        const int kind = m->c.bc[ side ];
+        if( kind == KRO_PER )
+            continue;
+        if( reg[ axis ] != ( right ? m->c.nb[ axis ] - 1 : 0 ) )
+            continue;                        /* not on this domain edge */
+        const int a1 = mod3( axis + 1 ), a2 = mod3( axis + 2 );
+        const int i_mom = MOM + axis;
+        for( int t2 = 0; t2 < n[ a2 ]; ++ t2 )
+        for( int t1 = 0; t1 < n[ a1 ]; ++ t1 )
+        {
+            double buf[ 4 ][ 8 ];            /* rows -2, -1, 0, 1 */
+            int ii[ 3 ];
+            ii[ a1 ] = t1;
+            ii[ a2 ] = t2;
+            for( int i = 0; i < 2; ++ i )
+            {
+                ii[ axis ] = right ? n[ axis ] - i - 1 : i;
+                memcpy( buf[ 2 + i ], w + iw( m, ii[ 0 ], ii[ 1 ], ii[ 2 ] ), sizeof( double ) * nw );
+            }
+            if( kind == KRO_OUT )
+            {
+                if( buf[ 2 ][ i_mom ] * ( right ? -1 : 1 ) > 0 )
+                    buf[ 2 ][ i_mom ] = 0;
+                for( int i = -2; i < 0; ++ i )
+                    memcpy( buf[ 2 + i ], buf[ 2 ], sizeof( double ) * nw );
+            }
+            else if( kind == KRO_FRE )
+                for( int i = -2; i < 0; ++ i )
+                    memcpy( buf[ 2 + i ], buf[ 2 ], sizeof( double ) * nw );
+            else if( kind == KRO_REF )
+                for( int i = -2; i < 0; ++ i )
+                    for( int k = 0; k < nw; ++ k )
+                        buf[ 2 + i ][ k ] = buf[ 2 - i - 1 ][ k ] * ( k == i_mom ? -1 : 1 );
+            else if( kind == KRO_FIXD )
+                for( int i = -2; i < 0; ++ i )
+                    for( int k = 0; k < nw; ++ k )
+                        buf[ 2 + i ][ k ] = m->c.w_fix[ k ];
+            for( int i = -2; i < 0; ++ i )
+            {
+                ii[ axis ] = right ? n[ axis ] - i - 1 : i;
+                memcpy( w + iw( m, ii[ 0 ], ii[ 1 ], ii[ 2 ] ), buf[ 2 + i ], sizeof( double ) * nw );
+            }
+        }
     }
 }
 
@@ -1080,6 +1165,7 @@ int kro_step( kro_mesh * m, int n_steps, double * t, double * dt_bound, double *
             }
             ghost_arg ga = { stage };
             par_blocks( m, ghost_block, & ga );
+            par_blocks( m, bc_block, NULL );
             const double dt = dt_use * ( stage == 0 ? 1.0 : ( double ) 0.5f );
             for( int axis = 2; axis >= 0; -- axis )
             {

@@ -27,6 +27,8 @@
 extern "C" {
 #endif
 
+enum { KRO_PER = 0, KRO_OUT = 1, KRO_REF = 2, KRO_FRE = 3, KRO_FIXD = 4 };
+
 typedef struct
 {
     int    mhd;              /* 0: hydro (PLM + HLLC), 1: MHD (PLM + HLLD + CT) */
@@ -36,6 +38,12 @@ typedef struct
     double gamma, cfl, d_floor, t_floor;
     double dt_expand;        /* [cycle] dt_expand                               */
     int    n_threads;        /* host threads used (<= 0: all)                   */
+    /* [boundary] kinds per side (x-, x+, y-, y+, z-, z+): KRO_PER, KRO_OUT,
+     * KRO_REF, KRO_FRE, KRO_FIXD (hydro/boundary/phys_functors.h); an axis is
+     * periodic only if both its sides are KRO_PER.  Non-periodic sides are
+     * hydro only here. */
+    int    bc[ 6 ];
+    double w_fix[ 5 ];       /* [init] rho0, pre0, vel0 for KRO_FIXD            */
 } kro_cfg;
 
 typedef struct kro_mesh kro_mesh;

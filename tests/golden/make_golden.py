@@ -40,12 +40,22 @@ CASES = [
     ("shock_floor", "shock", (2, 2, 2), (8, 8, 8), 3, 4, 1.4, {"tmp_floor": "1.0"}, "final"),
     ("shock_c1", "shock", (2, 2, 2), (32, 32, 32), 20, 1, 1.4, {}, "sums"),
     ("ot_64", "ot", (2, 2, 2), (32, 32, 32), 10, 2, 1.6666666666666667, {}, "sums"),
+    # physical boundaries (hydro/boundary/phys_functors.h): reflect, outflow, free,
+    # fixed (Dirichlet inflow from [init]); "kinds" lists x-, x+, y-, y+, z-, z+
+    ("shock_bc", "shock", (2, 2, 2), (8, 8, 8), 5, 5, 1.4,
+     {"kinds": "ref out fre out per per"}, "final"),
+    ("shock_fixd", "shock", (2, 2, 1), (8, 8, 8), 4, 6, 1.4,
+     {"kinds": "fixd out ref ref per per", "init": {"rho0": "1.0", "pre0": "1.0", "vel0": "0.5 0 0"}},
+     "final"),
 ]
 
 
 def par_text(problem, nb, n, steps, seed, gamma, extra, prefix):
     ng = [nb[a] * n[a] for a in range(3)]
     dyn = {"gamma": repr(gamma), "cfl": "0.3", "thread_limit": "1", "bnd_thread_limit": "1"}
+    extra = dict(extra)
+    kinds = extra.pop("kinds", "per per per per per per")
+    init = extra.pop("init", {})
     dyn.update(extra)
     lines = [
         "[problem]", "name = %s" % problem, "seed = %d" % seed, "",
@@ -54,7 +64,9 @@ def par_text(problem, nb, n, steps, seed, gamma, extra, prefix):
         "[cycle]", "prefix_output = %s" % prefix, "n_cycle_lim = %d" % (steps - 1),
         "final_output = 1", "n_display_freq = 1000000", "",
         "[dynamics]"] + ["%s = %s" % kv for kv in dyn.items()] + [
-        "", "[boundary]", "kinds = per per per per per per", ""]
+        "", "[boundary]", "kinds = %s" % kinds, ""]
+    if init:
+        lines += ["[init]"] + ["%s = %s" % kv for kv in init.items()] + [""]
     return "\n".join(lines)
 
 

@@ -5,7 +5,18 @@ import os
 import numpy as np
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-CASES = ["shock_16", "ot_16", "ot_ragged", "shock_floor", "shock_c1", "ot_64"]
+CASES = ["shock_16", "ot_16", "ot_ragged", "shock_floor", "shock_c1", "ot_64",
+         "shock_bc", "shock_fixd"]
+
+
+def boundary(meta):
+    """(kinds per side, fixed state) of a fixture; periodic when unset."""
+    extra = meta.get("dynamics", {})
+    kinds = extra.get("kinds", "per per per per per per").split()
+    init = extra.get("init", {})
+    w_fix = [float(init.get("rho0", 0)), float(init.get("pre0", 0))] + \
+        [float(x) for x in init.get("vel0", "0 0 0").split()]
+    return kinds, w_fix
 
 
 def load(name):

@@ -24,9 +24,10 @@ TOL_FP64_LONG = 1e-10
 def _dyn(meta, precision=2, riemann=0):
     from kratos_b200 import Dynamics
     extra = meta.get("dynamics", {})
+    kinds, w_fix = G.boundary(meta)
     return Dynamics(meta["workload"] == "ot", meta["nb"], meta["n"], gamma=meta["gamma"],
                     cfl=meta["cfl"], tmp_floor=float(extra.get("tmp_floor", 1e-9)),
-                    precision=precision, riemann=riemann)
+                    precision=precision, riemann=riemann, kinds=kinds, w_fix=w_fix)
 
 
 def rel_l1(a, b):
@@ -49,7 +50,8 @@ def test_initial_state_bit_exact(name):
         np.testing.assert_array_equal(u[..., 5:], g["u0"][..., 5:])
 
 
-@pytest.mark.parametrize("name", ["shock_16", "ot_16", "ot_ragged", "shock_floor"])
+@pytest.mark.parametrize("name", ["shock_16", "ot_16", "ot_ragged", "shock_floor",
+                                  "shock_bc", "shock_fixd"])
 def test_fp64_step_matches_reference(name):
     meta, g = G.load(name)
     d = _dyn(meta)

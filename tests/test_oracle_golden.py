@@ -15,8 +15,10 @@ import golden_io as G
 
 def _mesh(meta):
     extra = meta.get("dynamics", {})
+    kinds, w_fix = G.boundary(meta)
     return OracleMesh(meta["workload"] == "ot", meta["nb"], meta["n"], meta["gamma"],
-                      cfl=meta["cfl"], t_floor=float(extra.get("tmp_floor", 1e-9)))
+                      cfl=meta["cfl"], t_floor=float(extra.get("tmp_floor", 1e-9)),
+                      kinds=kinds, w_fix=w_fix)
 
 
 @pytest.mark.parametrize("name", ["shock_16", "ot_16"])
