@@ -20,8 +20,10 @@
  * Conventions
  *   - Blocks: a uniform mesh of nb[0] x nb[1] x nb[2] blocks of n[0] x n[1] x
  *     n[2] cells, numbered lexicographically (x fastest).
+ *     A sharded context (n_ranks > 1, below) holds a subset of them.
  *   - Host state arrays use the reference's per-block layouts (dat_3d_t,
- *     src/mesh/types/dat_3d.h:153-156, field index fastest):
+ *     src/mesh/types/dat_3d.h:153-156, field index fastest), blocks in
+ *     ascending global id:
  *       u  : [block][n2][n1][n0][nw]   nw = 5 (hydro) or 8 (MHD), no ghosts
  *       bf : [block][n2+5][n1+5][n0+5][3]  face B on the (n+1)^3 lattice with
  *            2 ghost layers (as the snapshot's field_bf_field)
@@ -39,7 +41,7 @@
 extern "C" {
 #endif
 
-#define KR_ABI_VERSION 2
+#define KR_ABI_VERSION 3
 
 /* [boundary] kinds per side (hydro/boundary/phys_functors.h:11-91): an axis is
  * periodic only when both its sides are KR_BC_PER. */
@@ -80,9 +82,18 @@ typedef struct
     int    bc[ 6 ];            /* enum kr_bc_t for x-, x+, y-, y+, z-, z+;       */
                                /* non-periodic sides: hydro only                 */
     double w_fix[ 5 ];         /* KR_BC_FIXD primitive state: rho, p, v0..2       */
-    int    reserved[ 7 ];      /* reserved[0] bit 0: shared-memory tiled flux    */
-                               /* sweeps (opt-in; default per-face kernel)       */
+    int    flags;              /* KR_FLAG_* bits                                 */
+    int    n_ranks;            /* ranks sharing the mesh (0 or 1: not sharded)   */
+    int    rank;               /* this context's rank, 0 <= rank < n_ranks       */
+    int    reserved[ 4 ];
 } kr_cfg;
+
+/* kr_cfg.flags */
+#define KR_FLAG_TILED    1     /* shared-memory tiled flux sweeps (opt-in; the   */
+                               /* per-face kernel is the default)                */
+#define KR_FLAG_HALO_ALL 2     /* route every neighbour copy, same-rank ones     */
+                               /* included, through the halo exchange            */
+                               /* (verification of the pack / exchange / unpack) */
 
 typedef struct kr_ctx kr_ctx;
 
@@ -193,6 +204,51 @@ const char* kr_learn_last_error( void );
  * Returns 0, or a negative code (enqueued work is asynchronous on `stream`). */
 int kr_c2p_dt_noalloc( const kr_cfg * cfg, const double * u, const double * bf,
                        double * w, double * dt_out, void * stream );
+
+/* ---- Sharding over ranks: one context per GPU.
+ * The reference distributes blocks over MPI ranks (mesh/meshgen/meshgen.cpp:
+ * 166-247), fills ghosts from other ranks' blocks through MPI messages
+ * (hydro/boundary/keeper.cpp:86-185, mhd/boundary/keeper.h:189-324) and
+ * reduces dt over ranks (cycle.cpp:77-95).  Here, with cfg.n_ranks > 1, the
+ * nb[0] x nb[1] x nb[2] global blocks are split into n_ranks boxes of whole
+ * blocks by recursive coordinate bisection (largest extent first, ties to the
+ * outer axis); a context holds the blocks of cfg.rank in ascending global
+ * (lexicographic) id, and kr_set_state / kr_get_state / kr_init_problem /
+ * kr_diagnostics work on those blocks only.  Per stage the ghost values a
+ * block needs from another rank's block -- the 2-layer primitive box of each
+ * of the 26 directions and, for MHD, the face-B strips of the 6 face
+ * directions -- are packed into one send buffer grouped by peer, exchanged
+ * with grouped NCCL send / receive inside the step's CUDA graph, and unpacked
+ * into the ghost zones; after stage 0's CFL reduction an NCCL all-reduce(min)
+ * makes dt global.  NCCL is loaded at run time (libnccl.so.2).
+ *
+ * kr_shard_owner : host only (no device needed).  owner[g] = rank of global
+ *                  block g for every block; returns the number of blocks of
+ *                  cfg->rank, or < 0 (kr_last_error(NULL)) if the mesh has
+ *                  fewer blocks than ranks along the bisection.
+ * kr_halo_counts : host only.  Words exchanged per stage with every peer p:
+ *                  send[2p] primitive words (the step's arithmetic type),
+ *                  send[2p+1] face-B words (double); recv likewise.  Arrays of
+ *                  2 * n_ranks entries.  Peer p = rank: same-rank copies, only
+ *                  with KR_FLAG_HALO_ALL.
+ * kr_shard_blocks: global ids of the context's blocks (gid may be NULL);
+ *                  returns their number.
+ * kr_comm_unique_id / kr_comm_init: ncclGetUniqueId on one rank, the 128
+ *                  bytes shared by the caller (e.g. a torch.distributed
+ *                  broadcast), then ncclCommInitRank(n_ranks, rank) on every
+ *                  rank's context (collective; call before the first step).
+ *                  kr_step on a sharded context without a communicator fails.
+ * kr_group_step  : all n_ranks contexts of one mesh driven from one process
+ *                  (ctxs[r] of rank r, same device): the exchange becomes
+ *                  device copies between the contexts and the dt minimum a
+ *                  kernel over their scalars, all on ctxs[0]'s stream
+ *                  (synchronous).  For running a sharded mesh on one GPU. */
+int kr_shard_owner   ( const kr_cfg * cfg, int * owner );
+int kr_halo_counts   ( const kr_cfg * cfg, long long * send, long long * recv );
+int kr_shard_blocks  ( kr_ctx * ctx, int * gid );
+int kr_comm_unique_id( unsigned char id[ 128 ] );
+int kr_comm_init     ( kr_ctx * ctx, const unsigned char id[ 128 ] );
+int kr_group_step    ( kr_ctx * const * ctxs, int n, int n_steps );
 
 #ifdef __cplusplus
 }

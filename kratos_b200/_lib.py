@@ -5,7 +5,8 @@ import os
 _PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_PKG, "libkrb200.so")
 
-KR_ABI_VERSION = 2
+KR_ABI_VERSION = 3
+KR_FLAG_TILED, KR_FLAG_HALO_ALL = 1, 2
 BC_KINDS = {"per": 0, "out": 1, "ref": 2, "fre": 3, "fixd": 4}
 KR_RIEMANN_DEFAULT, KR_RIEMANN_HLLE, KR_RIEMANN_LEARNED = 0, 1, 2
 
@@ -29,7 +30,10 @@ class kr_cfg(ctypes.Structure):
         ("device", ctypes.c_int),
         ("bc", ctypes.c_int * 6),
         ("w_fix", ctypes.c_double * 5),
-        ("reserved", ctypes.c_int * 7),
+        ("flags", ctypes.c_int),
+        ("n_ranks", ctypes.c_int),
+        ("rank", ctypes.c_int),
+        ("reserved", ctypes.c_int * 4),
     ]
 
 
@@ -67,6 +71,12 @@ SIGNATURES = {
     "kr_mlp_infer": (ctypes.c_int, [_vp, ctypes.c_longlong, _vp, _vp, ctypes.c_int]),
     "kr_learn_last_error": (ctypes.c_char_p, []),
     "kr_diagnostics": (ctypes.c_int, [_vp, _dp, _dp]),
+    "kr_shard_owner": (ctypes.c_int, [ctypes.POINTER(kr_cfg), _vp]),
+    "kr_halo_counts": (ctypes.c_int, [ctypes.POINTER(kr_cfg), _vp, _vp]),
+    "kr_shard_blocks": (ctypes.c_int, [_vp, _vp]),
+    "kr_comm_unique_id": (ctypes.c_int, [_vp]),
+    "kr_comm_init": (ctypes.c_int, [_vp, _vp]),
+    "kr_group_step": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
 }
 
 _lib = None

@@ -19,14 +19,18 @@
 #include "problems.h"
 
 #include <cuda_runtime.h>
+#include <dlfcn.h>
+#include <nccl.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 namespace kr
@@ -75,8 +79,10 @@ struct args_t
     unsigned long long * smp_n;
     long long smp_max;
     unsigned smp_stride, smp_seed;
-    const int * nbr;                  // [block][27], -1 past a physical boundary
-    int nbk[ 3 ];                     // blocks per axis
+    const int * nbr;                  // [block][27]: local block, -1 past a physical
+                                      // boundary, -2 filled by the halo exchange
+    const int * gid;                  // [block] global (lexicographic) block id
+    int nbk[ 3 ];                     // blocks per axis (global mesh)
     int bc[ 6 ];                      // kr_bc_t per side
     double w_fix[ 5 ];
     scal_t * s;
@@ -367,7 +373,8 @@ __global__ void __launch_bounds__( 128 ) k_phys( const args_t< R > a )
     const int kind = a.bc[ side ];
     if( kind == KR_BC_PER )
         return;
-    const int reg[ 3 ] = { b % a.nbk[ 0 ], ( b / a.nbk[ 0 ] ) % a.nbk[ 1 ], b / ( a.nbk[ 0 ] * a.nbk[ 1 ] ) };
+    const int g = a.gid[ b ];
+    const int reg[ 3 ] = { g % a.nbk[ 0 ], ( g / a.nbk[ 0 ] ) % a.nbk[ 1 ], g / ( a.nbk[ 0 ] * a.nbk[ 1 ] ) };
     if( reg[ axis ] != ( right ? a.nbk[ axis ] - 1 : 0 ) )
         return;
     const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
@@ -900,12 +907,303 @@ __global__ void k_diag( const args_t< R > a, double * out )
     }
 }
 
+////////////////////////////////////////////////////////////
+// Halo exchange between ranks: pack / unpack of the ghost values one block
+// takes from a neighbour in direction `dir` (k_ghost's sources, per item).
+// Item layout in the buffers: primitive words component-major over the
+// destination's ghost box (x fastest), then for a face direction along d the
+// face-B strips of components (d+1)%3 and (d+2)%3.  PACK runs on the rank
+// owning the source block (blk = source, coordinates shifted by -dir * n),
+// !PACK on the rank owning the destination block (blk = destination).
+
+struct halo_item_t
+{
+    int blk, dir;
+    long long woff, boff;
+};
+
+template< bool MHD, class R, bool PACK >
+__global__ void __launch_bounds__( 256 ) k_halo( const args_t< R > a, const halo_item_t * items,
+                                                 R * wbuf, double * bbuf, int step )
+{
+    constexpr int NW = MHD ? 11 : 5;
+    const halo_item_t m = items[ blockIdx.y ];
+    const int s[ 3 ] = { m.dir % 3 - 1, ( m.dir / 3 ) % 3 - 1, m.dir / 9 - 1 };
+    const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
+    int org[ 3 ], ext[ 3 ];
+    for( int d = 0; d < 3; ++ d )
+    {
+        ext[ d ] = s[ d ] ? 2 : nn[ d ];
+        org[ d ] = s[ d ] < 0 ? -2 : ( s[ d ] > 0 ? nn[ d ] : 0 );
+    }
+    const int sh[ 3 ] = { PACK ? s[ 0 ] * nn[ 0 ] : 0, PACK ? s[ 1 ] * nn[ 1 ] : 0, PACK ? s[ 2 ] * nn[ 2 ] : 0 };
+    const long long cells = ( long long ) ext[ 0 ] * ext[ 1 ] * ext[ 2 ];
+    const long long stride = ( long long ) gridDim.x * blockDim.x;
+    const long long t0 = ( long long ) blockIdx.x * blockDim.x + threadIdx.x;
+    for( long long t = t0; t < cells; t += stride )
+    {
+        const int i0 = org[ 0 ] + int( t % ext[ 0 ] ) - sh[ 0 ];
+        const int i1 = org[ 1 ] + int( ( t / ext[ 0 ] ) % ext[ 1 ] ) - sh[ 1 ];
+        const int i2 = org[ 2 ] + int( t / ( ( long long ) ext[ 0 ] * ext[ 1 ] ) ) - sh[ 2 ];
+        for( int k = 0; k < NW; ++ k )
+        {
+            R * p = wbuf + m.woff + k * cells + t;
+            R * q = a.w + iw( a, m.blk, k, NW, i0, i1, i2 );
+            if( PACK ) * p = * q;
+            else       * q = * p;
+        }
+    }
+    if( ! MHD || abs( s[ 0 ] ) + abs( s[ 1 ] ) + abs( s[ 2 ] ) != 1 )
+        return;
+    const int d = s[ 0 ] ? 0 : ( s[ 1 ] ? 1 : 2 );
+    double * BF = a.bf[ step ];
+    long long off = m.boff;
+    for( int h = 0; h < 2; ++ h )
+    {
+        const int c = ( d + 1 + h ) % 3, o = 3 - d - c;
+        const long long cnt = ( long long )( nn[ c ] + 1 ) * nn[ o ];
+        for( long long t = t0; t < cnt; t += stride )
+        {
+            int ii[ 3 ];
+            ii[ c ] = int( t % ( nn[ c ] + 1 ) );
+            ii[ o ] = int( t / ( nn[ c ] + 1 ) );
+            ii[ d ] = ( s[ d ] < 0 ? -1 : nn[ d ] ) - sh[ d ];
+            double * p = bbuf + off + t;
+            double * q = BF + ibf( a, m.blk, c, ii[ 0 ], ii[ 1 ], ii[ 2 ] );
+            if( PACK ) * p = * q;
+            else       * q = * p;
+        }
+        off += cnt;
+    }
+}
+
+// dt of a mesh split over several contexts in one process: the minimum of
+// their stage-0 CFL minima, written back to each.
+constexpr int KR_GROUP_MAX = 64;
+struct group_scal_t { scal_t * s[ KR_GROUP_MAX ]; int n; };
+
+__global__ void k_group_dt_min( group_scal_t g )
+{
+    unsigned long long m = ~0ull;
+    for( int r = 0; r < g.n; ++ r )
+    {
+        const unsigned long long v = g.s[ r ]->dt_bits;
+        m = v < m ? v : m;
+    }
+    for( int r = 0; r < g.n; ++ r )
+        g.s[ r ]->dt_bits = m;
+}
+
 }   // namespace kr
 
 ////////////////////////////////////////////////////////////
 // Context
 
 using namespace kr;
+
+////////////////////////////////////////////////////////////
+// Sharding plan (host): block owners, neighbour ids, halo items
+
+static int ranks_of( const kr_cfg & g ) { return g.n_ranks > 1 ? g.n_ranks : 1; }
+
+// owner[g] for every global block: recursive coordinate bisection of the
+// block grid into n_ranks boxes (largest extent first, ties to the outer axis;
+// the lower part gets floor(ranks / 2) ranks and a proportional share).
+static bool shard_owner( const kr_cfg & g, std::vector< int > & owner, std::string & err )
+{
+    const int R = ranks_of( g );
+    const int nb0 = g.nb[ 0 ], nb1 = g.nb[ 1 ], nb2 = g.nb[ 2 ];
+    owner.assign( size_t( nb0 ) * nb1 * nb2, 0 );
+    struct box_t { int lo[ 3 ], hi[ 3 ], r0, r1; };
+    std::vector< box_t > todo{ { { 0, 0, 0 }, { nb0, nb1, nb2 }, 0, R } };
+    while( ! todo.empty(  ) )
+    {
+        const box_t b = todo.back(  );
+        todo.pop_back(  );
+        const int nr = b.r1 - b.r0;
+        long long nblk = 1;
+        for( int a = 0; a < 3; ++ a ) nblk *= b.hi[ a ] - b.lo[ a ];
+        if( nblk < nr )
+        {
+            err = "kr_shard_owner: fewer blocks than ranks in a bisection box";
+            return false;
+        }
+        if( nr == 1 )
+        {
+            for( int k = b.lo[ 2 ]; k < b.hi[ 2 ]; ++ k )
+            for( int j = b.lo[ 1 ]; j < b.hi[ 1 ]; ++ j )
+            for( int i = b.lo[ 0 ]; i < b.hi[ 0 ]; ++ i )
+                owner[ i + size_t( nb0 ) * ( j + size_t( nb1 ) * k ) ] = b.r0;
+            continue;
+        }
+        int ax = 2;
+        for( int a = 1; a >= 0; -- a )
+            if( b.hi[ a ] - b.lo[ a ] > b.hi[ ax ] - b.lo[ ax ] ) ax = a;
+        const int ext = b.hi[ ax ] - b.lo[ ax ];
+        const int k = nr / 2;
+        int cut = b.lo[ ax ] + int( ( ( long long ) ext * k + nr / 2 ) / nr );
+        cut = std::min( std::max( cut, b.lo[ ax ] + 1 ), b.hi[ ax ] - 1 );
+        box_t lo = b, hi = b;
+        lo.hi[ ax ] = cut; lo.r1 = b.r0 + k;
+        hi.lo[ ax ] = cut; hi.r0 = b.r0 + k;
+        todo.push_back( hi );
+        todo.push_back( lo );
+    }
+    return true;
+}
+
+// Global neighbour of global block gb in direction k (0..26, x fastest), or
+// -1 past a non-periodic side.
+static int nbr_global( const kr_cfg & g, int gb, int k )
+{
+    const int reg[ 3 ] = { gb % g.nb[ 0 ], ( gb / g.nb[ 0 ] ) % g.nb[ 1 ], gb / ( g.nb[ 0 ] * g.nb[ 1 ] ) };
+    const int sh[ 3 ] = { k % 3 - 1, ( k / 3 ) % 3 - 1, k / 9 - 1 };
+    int r[ 3 ];
+    for( int a = 0; a < 3; ++ a )
+    {
+        r[ a ] = reg[ a ] + sh[ a ];
+        const bool periodic = g.bc[ 2 * a ] == KR_BC_PER && g.bc[ 2 * a + 1 ] == KR_BC_PER;
+        if( ( r[ a ] < 0 || r[ a ] >= g.nb[ a ] ) && ! periodic )
+            return -1;
+        r[ a ] = ( r[ a ] + g.nb[ a ] ) % g.nb[ a ];
+    }
+    return r[ 0 ] + g.nb[ 0 ] * ( r[ 1 ] + g.nb[ 1 ] * r[ 2 ] );
+}
+
+// Words of one halo item: primitives over the ghost box of direction k, and
+// for MHD face directions the two face-B strips.
+static long long halo_w_words( const kr_cfg & g, int k )
+{
+    const int sh[ 3 ] = { k % 3 - 1, ( k / 3 ) % 3 - 1, k / 9 - 1 };
+    long long cells = 1;
+    for( int a = 0; a < 3; ++ a ) cells *= sh[ a ] ? 2 : g.n[ a ];
+    return cells * ( g.mhd ? 11 : 5 );
+}
+static long long halo_b_words( const kr_cfg & g, int k )
+{
+    const int sh[ 3 ] = { k % 3 - 1, ( k / 3 ) % 3 - 1, k / 9 - 1 };
+    if( ! g.mhd || std::abs( sh[ 0 ] ) + std::abs( sh[ 1 ] ) + std::abs( sh[ 2 ] ) != 1 )
+        return 0;
+    const int d = sh[ 0 ] ? 0 : ( sh[ 1 ] ? 1 : 2 );
+    const int c1 = ( d + 1 ) % 3, c2 = ( d + 2 ) % 3;
+    return ( long long )( g.n[ c1 ] + 1 ) * g.n[ c2 ] + ( long long )( g.n[ c2 ] + 1 ) * g.n[ c1 ];
+}
+
+// One side (send or receive) of a rank's exchange: items grouped by peer in
+// the order both ends enumerate them -- destination blocks by ascending global
+// id, directions 0..26.
+struct halo_side_t
+{
+    std::vector< halo_item_t > items;
+    std::vector< long long > w_off, w_cnt, b_off, b_cnt;   // per peer, words
+    long long w_tot = 0, b_tot = 0;
+};
+
+static void halo_plan( const kr_cfg & g, const std::vector< int > & owner, const std::vector< int > & local,
+                       bool all, halo_side_t & snd, halo_side_t & rcv )
+{
+    const int R = ranks_of( g ), me = ranks_of( g ) > 1 ? g.rank : 0;
+    const int nglob = int( owner.size(  ) );
+    for( halo_side_t * h : { & snd, & rcv } )
+    {
+        h->items.clear(  );
+        h->w_off.assign( R, 0 ); h->w_cnt.assign( R, 0 );
+        h->b_off.assign( R, 0 ); h->b_cnt.assign( R, 0 );
+        h->w_tot = h->b_tot = 0;
+    }
+    for( int q = 0; q < R; ++ q )
+    {
+        if( q == me && ! all )
+            continue;
+        snd.w_off[ q ] = snd.w_tot; snd.b_off[ q ] = snd.b_tot;
+        rcv.w_off[ q ] = rcv.w_tot; rcv.b_off[ q ] = rcv.b_tot;
+        for( int gb = 0; gb < nglob; ++ gb )
+        {
+            const bool to_q = owner[ gb ] == q, mine = owner[ gb ] == me;
+            if( ! to_q && ! mine )
+                continue;
+            for( int k = 0; k < 27; ++ k )
+            {
+                const int src = k == 13 ? -1 : nbr_global( g, gb, k );
+                if( src < 0 )
+                    continue;
+                const long long wn = halo_w_words( g, k ), bn = halo_b_words( g, k );
+                if( to_q && owner[ src ] == me )      // q's block gb reads my block src
+                {
+                    snd.items.push_back( { local[ src ], k, snd.w_tot, snd.b_tot } );
+                    snd.w_tot += wn; snd.b_tot += bn;
+                }
+                if( mine && owner[ src ] == q )       // my block gb reads q's block src
+                {
+                    rcv.items.push_back( { local[ gb ], k, rcv.w_tot, rcv.b_tot } );
+                    rcv.w_tot += wn; rcv.b_tot += bn;
+                }
+            }
+        }
+        snd.w_cnt[ q ] = snd.w_tot - snd.w_off[ q ]; snd.b_cnt[ q ] = snd.b_tot - snd.b_off[ q ];
+        rcv.w_cnt[ q ] = rcv.w_tot - rcv.w_off[ q ]; rcv.b_cnt[ q ] = rcv.b_tot - rcv.b_off[ q ];
+    }
+}
+
+////////////////////////////////////////////////////////////
+// NCCL, loaded at run time: the library has no link dependency on it.  A copy
+// of libnccl.so.2 already in the process (e.g. the one torch links) is used;
+// else the file named by $KRATOS_B200_NCCL; else the one the dynamic linker
+// finds.  Opened with local symbol scope.  A process holds one libnccl.so.2
+// (one soname): a framework loaded later that links a newer NCCL than the one
+// opened here fails to load, so name that framework's copy in the variable.
+
+struct nccl_api_t
+{
+    bool ok = false;
+    std::string err;
+    decltype( & ncclGetUniqueId ) GetUniqueId = nullptr;
+    decltype( & ncclCommInitRank ) CommInitRank = nullptr;
+    decltype( & ncclCommDestroy ) CommDestroy = nullptr;
+    decltype( & ncclGroupStart ) GroupStart = nullptr;
+    decltype( & ncclGroupEnd ) GroupEnd = nullptr;
+    decltype( & ncclSend ) Send = nullptr;
+    decltype( & ncclRecv ) Recv = nullptr;
+    decltype( & ncclAllReduce ) AllReduce = nullptr;
+    decltype( & ncclGetErrorString ) GetErrorString = nullptr;
+};
+
+static nccl_api_t & nccl(  )
+{
+    static nccl_api_t api;
+    static std::once_flag once;
+    std::call_once( once, [](  )
+    {
+        void * h = dlopen( "libnccl.so.2", RTLD_NOW | RTLD_NOLOAD );
+        const char * path = std::getenv( "KRATOS_B200_NCCL" );
+        if( ! h && path && * path )
+            h = dlopen( path, RTLD_NOW | RTLD_LOCAL );
+        if( ! h )
+            h = dlopen( "libnccl.so.2", RTLD_NOW | RTLD_LOCAL );
+        if( ! h )
+        {
+            api.err = std::string( "dlopen libnccl.so.2: " ) + dlerror(  );
+            return;
+        }
+        bool ok = true;
+        auto sym = [ & ]( auto & fn, const char * name )
+        {
+            fn = reinterpret_cast< std::remove_reference_t< decltype( fn ) > >( dlsym( h, name ) );
+            if( ! fn ) { ok = false; api.err = std::string( "libnccl.so.2 lacks " ) + name; }
+        };
+        sym( api.GetUniqueId, "ncclGetUniqueId" );
+        sym( api.CommInitRank, "ncclCommInitRank" );
+        sym( api.CommDestroy, "ncclCommDestroy" );
+        sym( api.GroupStart, "ncclGroupStart" );
+        sym( api.GroupEnd, "ncclGroupEnd" );
+        sym( api.Send, "ncclSend" );
+        sym( api.Recv, "ncclRecv" );
+        sym( api.AllReduce, "ncclAllReduce" );
+        sym( api.GetErrorString, "ncclGetErrorString" );
+        api.ok = ok;
+    } );
+    return api;
+}
 
 struct kr_ctx
 {
@@ -945,6 +1243,19 @@ struct kr_ctx
     cudaStream_t graph_stream = nullptr;
     std::vector< geo_t > geo_h;
     bool no_tiles = false;             // force the per-face flux kernel (testing)
+    // sharding: this rank's blocks and the halo exchange with the others
+    int nranks = 1, rank = 0;
+    std::vector< int > gid_h;          // global id of each local block
+    int * gid = nullptr;
+    halo_side_t hsend, hrecv;
+    halo_item_t * send_items = nullptr;
+    halo_item_t * recv_items = nullptr;
+    void * send_w = nullptr;           // R words
+    void * recv_w = nullptr;
+    double * send_b = nullptr;
+    double * recv_b = nullptr;
+    int halo_grid = 1;                 // CTAs per item of k_halo
+    ncclComm_t comm = nullptr;
 };
 
 static thread_local std::string g_create_error;
@@ -981,7 +1292,7 @@ static args_t< R > make_args( kr_ctx * c )
     a.w = ( R * ) c->w;
     for( int d = 0; d < 3; ++ d ) a.f[ d ] = ( R * ) c->f[ d ];
     a.ee = ( R * ) c->ee;
-    a.geo = c->geo; a.nbr = c->nbr; a.s = c->s;
+    a.geo = c->geo; a.nbr = c->nbr; a.gid = c->gid; a.s = c->s;
     for( int d = 0; d < 3; ++ d ) a.nbk[ d ] = c->cfg.nb[ d ];
     for( int k = 0; k < 6; ++ k ) a.bc[ k ] = c->cfg.bc[ k ];
     for( int k = 0; k < 5; ++ k ) a.w_fix[ k ] = c->cfg.w_fix[ k ];
@@ -1080,46 +1391,123 @@ static void launch_flux_mode( kr_ctx * c, cudaStream_t st, const args_t< R > & a
     else                                          launch_flux< MHD, R, KR_RIEMANN_DEFAULT >( c, st, a, axis, stage );
 }
 
-// Enqueue one Heun step on stream st (SAMPLE: also log selector training samples).
-template< bool MHD, class R, bool SAMPLE = false >
-static void enqueue_step( kr_ctx * c, cudaStream_t st )
+// One stage is front (cons -> prim, CFL dt at stage 0, pack of the halo other
+// ranks read), exchange (NCCL send / receive by peer; at stage 0 the dt
+// all-reduce), back (unpack, same-rank ghosts, physical sides, flux sweeps,
+// EMF, update).  `timed( kind, launch )` wraps each piece (profiling: kinds
+// 0 c2p, 1 ghost and halo, 2..4 flux z, y, x, 5 emf, 6 update).
+struct untimed_t { template< class F > void operator(  )( int, F && f ) const { f(  ); } };
+
+template< bool MHD, class R, class T >
+static void enqueue_front( kr_ctx * c, cudaStream_t st, const args_t< R > & a, int stage, T && timed )
 {
-    const args_t< R > a = make_args< R >( c );
+    const unsigned nb = unsigned( c->nblk );
+    timed( 0, [ & ] { k_c2p< MHD, R ><<< dim3( blocks_for( c->nc, 256 ), nb ), 256, 0, st >>>( a, stage ); } );
+    if( ! c->hsend.items.empty(  ) )
+        timed( 1, [ & ] {
+            k_halo< MHD, R, true ><<< dim3( c->halo_grid, unsigned( c->hsend.items.size(  ) ) ), 256, 0, st >>>(
+                a, c->send_items, ( R * ) c->send_w, c->send_b, stage ); } );
+}
+
+template< bool MHD, class R, class T >
+static void enqueue_back( kr_ctx * c, cudaStream_t st, const args_t< R > & a, int stage, int mode, T && timed )
+{
     const int * n = c->cfg.n;
     const unsigned nb = unsigned( c->nblk );
     const long long nlat = ( long long )( n[ 0 ] + 1 ) * ( n[ 1 ] + 1 ) * ( n[ 2 ] + 1 );
     const long long nghost = shell_count( n[ 0 ], n[ 1 ], n[ 2 ], 2 )
                            + ( MHD ? bf_strip_count( n[ 0 ], n[ 1 ], n[ 2 ] ) : 0 );
+    timed( 1, [ & ] {
+        if( ! c->hrecv.items.empty(  ) )
+            k_halo< MHD, R, false ><<< dim3( c->halo_grid, unsigned( c->hrecv.items.size(  ) ) ), 256, 0, st >>>(
+                a, c->recv_items, ( R * ) c->recv_w, c->recv_b, stage );
+        k_ghost< MHD, R ><<< dim3( blocks_for( nghost, 256 ), nb ), 256, 0, st >>>( a, stage );
+        if( ! MHD && has_phys( c ) )
+            k_phys< R ><<< dim3( blocks_for( phys_sites( c ), 128 ), 6, nb ), 128, 0, st >>>( a ); } );
+    for( int axis = 2; axis >= 0; -- axis )
+        timed( 4 - axis, [ & ] { launch_flux_mode< MHD, R >( c, st, a, axis, stage, mode ); } );
+    if( MHD )
+        timed( 5, [ & ] { k_emf< R ><<< dim3( blocks_for( nlat, 256 ), nb ), 256, 0, st >>>( a ); } );
+    timed( 6, [ & ] { k_update< MHD, R ><<< dim3( blocks_for( nlat, 256 ), nb ), 256, 0, st >>>( a, stage ); } );
+}
+
+// Halo transfer of one stage between this rank and its peers, and at stage 0
+// the global dt minimum.  Same-rank items without a communicator (the
+// KR_FLAG_HALO_ALL check of one unsharded context) are device copies.
+static bool enqueue_exchange( kr_ctx * c, cudaStream_t st, int stage )
+{
+    const size_t rs = c->rsize;
+    if( ! c->comm && c->hsend.items.empty(  ) && c->hrecv.items.empty(  ) )
+        return true;                     // nothing to move; NCCL never loaded
+    nccl_api_t * api = c->comm ? & nccl(  ) : nullptr;
+    bool grouped = false;
+    ncclResult_t r = ncclSuccess;
+    for( int q = 0; q < c->nranks; ++ q )
+    {
+        const long long sw = c->hsend.w_cnt[ q ], sb = c->hsend.b_cnt[ q ];
+        const long long rw = c->hrecv.w_cnt[ q ], rb = c->hrecv.b_cnt[ q ];
+        if( ! ( sw || sb || rw || rb ) )
+            continue;
+        char * sW = ( char * ) c->send_w + c->hsend.w_off[ q ] * rs;
+        char * rW = ( char * ) c->recv_w + c->hrecv.w_off[ q ] * rs;
+        double * sB = c->send_b + c->hsend.b_off[ q ];
+        double * rB = c->recv_b + c->hrecv.b_off[ q ];
+        if( q == c->rank && ! c->comm )
+        {   // send and receive lists to oneself coincide item by item
+            if( sw && ! ck( c, cudaMemcpyAsync( rW, sW, sw * rs, cudaMemcpyDeviceToDevice, st ), "halo copy" ) ) return false;
+            if( sb && ! ck( c, cudaMemcpyAsync( rB, sB, sb * 8, cudaMemcpyDeviceToDevice, st ), "halo copy" ) ) return false;
+            continue;
+        }
+        if( ! c->comm )
+        {
+            c->err = "sharded context without a communicator (call kr_comm_init)";
+            return false;
+        }
+        if( ! grouped ) { r = api->GroupStart(  ); grouped = true; }
+        const ncclDataType_t tw = rs == 4 ? ncclFloat32 : ncclFloat64;
+        if( sw && r == ncclSuccess ) r = api->Send( sW, size_t( sw ), tw, q, c->comm, st );
+        if( sb && r == ncclSuccess ) r = api->Send( sB, size_t( sb ), ncclFloat64, q, c->comm, st );
+        if( rw && r == ncclSuccess ) r = api->Recv( rW, size_t( rw ), tw, q, c->comm, st );
+        if( rb && r == ncclSuccess ) r = api->Recv( rB, size_t( rb ), ncclFloat64, q, c->comm, st );
+    }
+    if( grouped )
+    {
+        const ncclResult_t e = api->GroupEnd(  );
+        if( r == ncclSuccess ) r = e;
+    }
+    if( stage == 0 && c->comm && r == ncclSuccess )   // cycle.cpp:77-95 reduce_all(min)
+        r = api->AllReduce( & c->s->dt_bits, & c->s->dt_bits, 1, ncclUint64, ncclMin, c->comm, st );
+    if( r != ncclSuccess )
+    {
+        c->err = std::string( "NCCL: " ) + api->GetErrorString( r );
+        return false;
+    }
+    return true;
+}
+
+// Enqueue one Heun step on stream st (SAMPLE: also log selector training samples).
+template< bool MHD, class R, bool SAMPLE = false >
+static bool enqueue_step( kr_ctx * c, cudaStream_t st )
+{
+    const args_t< R > a = make_args< R >( c );
     k_step_begin<<< 1, 1, 0, st >>>( c->s );
     for( int stage = 0; stage < 2; ++ stage )
     {
-        k_c2p< MHD, R ><<< dim3( blocks_for( c->nc, 256 ), nb ), 256, 0, st >>>( a, stage );
-        k_ghost< MHD, R ><<< dim3( blocks_for( nghost, 256 ), nb ), 256, 0, st >>>( a, stage );
-        if( ! MHD && has_phys( c ) )
-            k_phys< R ><<< dim3( blocks_for( phys_sites( c ), 128 ), 6, nb ), 128, 0, st >>>( a );
-        for( int axis = 2; axis >= 0; -- axis )
-        {
-            launch_flux_mode< MHD, R >( c, st, a, axis, stage, SAMPLE ? FLUX_SAMPLE : c->cfg.riemann );
-        }
-        if( MHD )
-            k_emf< R ><<< dim3( blocks_for( nlat, 256 ), nb ), 256, 0, st >>>( a );
-        k_update< MHD, R ><<< dim3( blocks_for( nlat, 256 ), nb ), 256, 0, st >>>( a, stage );
+        enqueue_front< MHD, R >( c, st, a, stage, untimed_t(  ) );
+        if( ! enqueue_exchange( c, st, stage ) )
+            return false;
+        enqueue_back< MHD, R >( c, st, a, stage, SAMPLE ? FLUX_SAMPLE : c->cfg.riemann, untimed_t(  ) );
     }
     k_step_end<<< 1, 1, 0, st >>>( c->s, c->cfg.dt_expand );
+    return true;
 }
 
 // One step launched eagerly with CUDA events around every kernel; per kind
-// (0 c2p, 1 ghost, 2 flux z, 3 flux y, 4 flux x, 5 emf, 6 update) the summed
-// milliseconds of the step are added to ms[kind].
+// the summed milliseconds of the step are added to ms[kind].
 template< bool MHD, class R >
 static bool profile_step( kr_ctx * c, double * ms )
 {
     const args_t< R > a = make_args< R >( c );
-    const int * n = c->cfg.n;
-    const unsigned nb = unsigned( c->nblk );
-    const long long nlat = ( long long )( n[ 0 ] + 1 ) * ( n[ 1 ] + 1 ) * ( n[ 2 ] + 1 );
-    const long long nghost = shell_count( n[ 0 ], n[ 1 ], n[ 2 ], 2 )
-                           + ( MHD ? bf_strip_count( n[ 0 ], n[ 1 ], n[ 2 ] ) : 0 );
     cudaStream_t st = c->stream;
     cudaEvent_t ev[ 2 ];
     cudaEventCreate( & ev[ 0 ] );
@@ -1134,40 +1522,26 @@ static bool profile_step( kr_ctx * c, double * ms )
         cudaEventElapsedTime( & t, ev[ 0 ], ev[ 1 ] );
         ms[ kind ] += t;
     };
+    bool ok = true;
     k_step_begin<<< 1, 1, 0, st >>>( c->s );
-    for( int stage = 0; stage < 2; ++ stage )
+    for( int stage = 0; stage < 2 && ok; ++ stage )
     {
-        timed( 0, [ & ] { k_c2p< MHD, R ><<< dim3( blocks_for( c->nc, 256 ), nb ), 256, 0, st >>>( a, stage ); } );
-        timed( 1, [ & ] {
-            k_ghost< MHD, R ><<< dim3( blocks_for( nghost, 256 ), nb ), 256, 0, st >>>( a, stage );
-            if( ! MHD && has_phys( c ) )
-                k_phys< R ><<< dim3( blocks_for( phys_sites( c ), 128 ), 6, nb ), 128, 0, st >>>( a ); } );
-        for( int axis = 2; axis >= 0; -- axis )
-        {
-            timed( 4 - axis, [ & ] { launch_flux_mode< MHD, R >( c, st, a, axis, stage, c->cfg.riemann ); } );
-        }
-        if( MHD )
-            timed( 5, [ & ] { k_emf< R ><<< dim3( blocks_for( nlat, 256 ), nb ), 256, 0, st >>>( a ); } );
-        timed( 6, [ & ] { k_update< MHD, R ><<< dim3( blocks_for( nlat, 256 ), nb ), 256, 0, st >>>( a, stage ); } );
+        enqueue_front< MHD, R >( c, st, a, stage, timed );
+        timed( 1, [ & ] { ok = enqueue_exchange( c, st, stage ); } );
+        if( ok )
+            enqueue_back< MHD, R >( c, st, a, stage, c->cfg.riemann, timed );
     }
     k_step_end<<< 1, 1, 0, st >>>( c->s, c->cfg.dt_expand );
     cudaEventDestroy( ev[ 0 ] );
     cudaEventDestroy( ev[ 1 ] );
-    return ck( c, cudaStreamSynchronize( st ), "profile" );
+    return ck( c, cudaStreamSynchronize( st ), "profile" ) && ok;
 }
 
-static void enqueue_step_any( kr_ctx * c, cudaStream_t st )
+static bool enqueue_step_any( kr_ctx * c, cudaStream_t st )
 {
     if( c->cfg.mhd )
-    {
-        if( c->cfg.precision == 1 ) enqueue_step< true, float >( c, st );
-        else                        enqueue_step< true, double >( c, st );
-    }
-    else
-    {
-        if( c->cfg.precision == 1 ) enqueue_step< false, float >( c, st );
-        else                        enqueue_step< false, double >( c, st );
-    }
+        return c->cfg.precision == 1 ? enqueue_step< true, float >( c, st ) : enqueue_step< true, double >( c, st );
+    return c->cfg.precision == 1 ? enqueue_step< false, float >( c, st ) : enqueue_step< false, double >( c, st );
 }
 
 static void drop_graph( kr_ctx * c )
@@ -1184,9 +1558,15 @@ static bool build_graph( kr_ctx * c )
     drop_graph( c );
     if( ! ck( c, cudaStreamBeginCapture( c->stream, cudaStreamCaptureModeThreadLocal ), "capture begin" ) )
         return false;
-    enqueue_step_any( c, c->stream );
-    if( ! ck( c, cudaStreamEndCapture( c->stream, & c->graph ), "capture end" ) )
+    const bool ok = enqueue_step_any( c, c->stream );
+    const bool ended = ck( c, cudaStreamEndCapture( c->stream, & c->graph ), "capture end" );
+    if( ! ok || ! ended )
+    {
+        const std::string e = c->err;
+        drop_graph( c );
+        c->err = e;
         return false;
+    }
     if( ! ck( c, cudaGraphInstantiate( & c->graph_exec, c->graph, 0 ), "graph instantiate" ) )
         return false;
     c->graph_stream = c->stream;
@@ -1200,7 +1580,8 @@ static void set_geometry( kr_ctx * c )
     c->geo_h.resize( c->nblk );
     for( int b = 0; b < c->nblk; ++ b )
     {
-        const int reg[ 3 ] = { b % g.nb[ 0 ], ( b / g.nb[ 0 ] ) % g.nb[ 1 ], b / ( g.nb[ 0 ] * g.nb[ 1 ] ) };
+        const int gb = c->gid_h[ b ];
+        const int reg[ 3 ] = { gb % g.nb[ 0 ], ( gb / g.nb[ 0 ] ) % g.nb[ 1 ], gb / ( g.nb[ 0 ] * g.nb[ 1 ] ) };
         geo_t & o = c->geo_h[ b ];
         for( int a = 0; a < 3; ++ a )
         {
@@ -1224,9 +1605,10 @@ static void set_geometry( kr_ctx * c )
     }
 }
 
-static double x_cc( const kr_cfg & g, int b, int a, int i )
+// Cell centre of cell i along axis a of global block gb.
+static double x_cc( const kr_cfg & g, int gb, int a, int i )
 {
-    const int reg[ 3 ] = { b % g.nb[ 0 ], ( b / g.nb[ 0 ] ) % g.nb[ 1 ], b / ( g.nb[ 0 ] * g.nb[ 1 ] ) };
+    const int reg[ 3 ] = { gb % g.nb[ 0 ], ( gb / g.nb[ 0 ] ) % g.nb[ 1 ], gb / ( g.nb[ 0 ] * g.nb[ 1 ] ) };
     const double lim = double( g.nb[ a ] );
     const double x0 = ( reg[ a ] + 0.0 / g.n[ a ] ) / lim;
     const double x1 = ( reg[ a ] + 1.0 / g.n[ a ] ) / lim;
@@ -1292,6 +1674,14 @@ kr_ctx * kr_ctx_create( const kr_cfg * cfg )
         g_create_error = "kr_ctx_create: HLLE / learned selection is MHD only";
         return nullptr;
     }
+    if( cfg->n_ranks < 0 || cfg->n_ranks > 65536 || ( cfg->n_ranks > 1 && ( cfg->rank < 0 || cfg->rank >= cfg->n_ranks ) ) )
+    {
+        g_create_error = "kr_ctx_create: need 0 <= rank < n_ranks";
+        return nullptr;
+    }
+    std::vector< int > owner;
+    if( ! shard_owner( * cfg, owner, g_create_error ) )
+        return nullptr;
     int ndev = 0;
     if( ! ck( nullptr, cudaGetDeviceCount( & ndev ), "cudaGetDeviceCount" ) )
         return nullptr;
@@ -1308,9 +1698,26 @@ kr_ctx * kr_ctx_create( const kr_cfg * cfg )
     // The shared-memory tiled sweep is opt-in: on the 256^3 OT step it measured
     // slower than the per-face kernel (more registers per thread, long per-thread
     // face loops, a tail of partial CTAs), so the per-face kernel is the default.
-    c->no_tiles = ( cfg->reserved[ 0 ] & 1 ) == 0;
+    c->no_tiles = ( cfg->flags & KR_FLAG_TILED ) == 0;
     const int * n = cfg->n;
-    c->nblk = cfg->nb[ 0 ] * cfg->nb[ 1 ] * cfg->nb[ 2 ];
+    c->nranks = ranks_of( * cfg );
+    c->rank = c->nranks > 1 ? cfg->rank : 0;
+    std::vector< int > local( owner.size(  ), -1 );
+    for( int gb = 0; gb < int( owner.size(  ) ); ++ gb )
+        if( owner[ gb ] == c->rank )
+        {
+            local[ gb ] = int( c->gid_h.size(  ) );
+            c->gid_h.push_back( gb );
+        }
+    c->nblk = int( c->gid_h.size(  ) );
+    const bool halo_all = ( cfg->flags & KR_FLAG_HALO_ALL ) != 0;
+    halo_plan( * cfg, owner, local, halo_all, c->hsend, c->hrecv );
+    if( c->hsend.items.size(  ) > 65535 || c->hrecv.items.size(  ) > 65535 )
+    {   // one grid row per item
+        g_create_error = "kr_ctx_create: more than 65535 halo items on one rank";
+        delete c;
+        return nullptr;
+    }
     c->nw = cfg->mhd ? 8 : 5;
     c->nws = cfg->mhd ? 11 : 5;
     c->nf = cfg->mhd ? 7 : 5;
@@ -1335,6 +1742,27 @@ kr_ctx * kr_ctx_create( const kr_cfg * cfg )
         ok = ck( c, cudaMalloc( & c->ee, nb * 3 * c->nfb * c->rsize ), "malloc ee" );
     ok = ok && ck( c, cudaMalloc( & c->geo, nb * sizeof( geo_t ) ), "malloc geo" );
     ok = ok && ck( c, cudaMalloc( & c->nbr, nb * 27 * sizeof( int ) ), "malloc nbr" );
+    ok = ok && ck( c, cudaMalloc( & c->gid, nb * sizeof( int ) ), "malloc gid" );
+    // halo exchange: item lists and buffers (1-word minimum keeps pointers valid)
+    {
+        const halo_side_t * hs[ 2 ] = { & c->hsend, & c->hrecv };
+        halo_item_t ** di[ 2 ] = { & c->send_items, & c->recv_items };
+        void ** wb[ 2 ] = { & c->send_w, & c->recv_w };
+        double ** bb[ 2 ] = { & c->send_b, & c->recv_b };
+        for( int k = 0; k < 2 && ok; ++ k )
+        {
+            ok = ck( c, cudaMalloc( di[ k ], std::max< size_t >( 1, hs[ k ]->items.size(  ) ) * sizeof( halo_item_t ) ), "malloc halo items" )
+              && ck( c, cudaMalloc( wb[ k ], std::max< long long >( 1, hs[ k ]->w_tot ) * c->rsize ), "malloc halo buffer" )
+              && ck( c, cudaMalloc( bb[ k ], std::max< long long >( 1, hs[ k ]->b_tot ) * sizeof( double ) ), "malloc halo buffer" );
+            if( ok && ! hs[ k ]->items.empty(  ) )
+                ok = ck( c, cudaMemcpyAsync( * di[ k ], hs[ k ]->items.data(  ), hs[ k ]->items.size(  ) * sizeof( halo_item_t ),
+                                             cudaMemcpyHostToDevice, c->stream ), "upload halo items" );
+        }
+        long long mx = 0;
+        for( int a = 0; a < 3; ++ a )
+            mx = std::max( mx, 2LL * n[ ( a + 1 ) % 3 ] * n[ ( a + 2 ) % 3 ] );
+        c->halo_grid = int( std::min< long long >( 64, blocks_for( mx, 256 ) ) );
+    }
     ok = ok && ck( c, cudaMalloc( & c->s, sizeof( scal_t ) ), "malloc scalars" );
     ok = ok && ck( c, cudaMalloc( & c->diag, 8 * sizeof( double ) ), "malloc diag" );
     if( cfg->mhd )
@@ -1362,31 +1790,20 @@ kr_ctx * kr_ctx_create( const kr_cfg * cfg )
     if( cfg->mhd ) cudaMemsetAsync( c->ee, 0, nb * 3 * c->nfb * c->rsize, c->stream );
 
     set_geometry( c );
+    // neighbour table of the local blocks: local index of a same-rank
+    // neighbour, -1 past a physical side, -2 where the halo exchange fills
     std::vector< int > nbr( nb * 27 );
     for( int b = 0; b < c->nblk; ++ b )
-    {
-        const int reg[ 3 ] = { b % cfg->nb[ 0 ], ( b / cfg->nb[ 0 ] ) % cfg->nb[ 1 ],
-                               b / ( cfg->nb[ 0 ] * cfg->nb[ 1 ] ) };
         for( int k = 0; k < 27; ++ k )
         {
-            const int sh[ 3 ] = { k % 3 - 1, ( k / 3 ) % 3 - 1, k / 9 - 1 };
-            int r[ 3 ];
-            bool exists = true;
-            for( int a = 0; a < 3; ++ a )
-            {
-                r[ a ] = reg[ a ] + sh[ a ];
-                const bool periodic = cfg->bc[ 2 * a ] == KR_BC_PER && cfg->bc[ 2 * a + 1 ] == KR_BC_PER;
-                if( ( r[ a ] < 0 || r[ a ] >= cfg->nb[ a ] ) && ! periodic )
-                    exists = false;          // past a physical boundary: no neighbour
-                r[ a ] = ( r[ a ] + cfg->nb[ a ] ) % cfg->nb[ a ];
-            }
-            nbr[ b * 27 + k ] = exists ? r[ 0 ] + cfg->nb[ 0 ] * ( r[ 1 ] + cfg->nb[ 1 ] * r[ 2 ] ) : -1;
+            const int src = nbr_global( * cfg, c->gid_h[ b ], k );
+            nbr[ b * 27 + k ] = src < 0 ? -1 : ( owner[ src ] == c->rank && ! ( halo_all && k != 13 ) ? local[ src ] : -2 );
         }
-    }
     scal_t s0{};
     s0.dt_bound = cfg->dt_init >= FLT_MIN ? cfg->dt_init : FLT_MAX / 10;   // cycle.cpp:163-166
     ok = ck( c, cudaMemcpyAsync( c->geo, c->geo_h.data(  ), nb * sizeof( geo_t ), cudaMemcpyHostToDevice, c->stream ), "upload geo" )
       && ck( c, cudaMemcpyAsync( c->nbr, nbr.data(  ), nbr.size(  ) * sizeof( int ), cudaMemcpyHostToDevice, c->stream ), "upload nbr" )
+      && ck( c, cudaMemcpyAsync( c->gid, c->gid_h.data(  ), nb * sizeof( int ), cudaMemcpyHostToDevice, c->stream ), "upload gid" )
       && ck( c, cudaMemcpyAsync( c->s, & s0, sizeof( s0 ), cudaMemcpyHostToDevice, c->stream ), "upload scalars" )
       && ck( c, cudaStreamSynchronize( c->stream ), "sync" );
     if( ! ok )
@@ -1403,7 +1820,11 @@ void kr_ctx_destroy( kr_ctx * c )
     if( ! c ) return;
     cudaSetDevice( c->cfg.device );
     if( c->stream ) cudaStreamSynchronize( c->stream );
-    drop_graph( c );
+    drop_graph( c );                   // before the communicator its graph uses
+    if( c->comm ) nccl(  ).CommDestroy( c->comm );
+    cudaFree( c->gid );
+    cudaFree( c->send_items ); cudaFree( c->recv_items );
+    cudaFree( c->send_w ); cudaFree( c->recv_w ); cudaFree( c->send_b ); cudaFree( c->recv_b );
     for( int s = 0; s < 2; ++ s ) { cudaFree( c->u[ s ] ); cudaFree( c->bf[ s ] ); }
     cudaFree( c->w );
     for( int d = 0; d < 3; ++ d ) cudaFree( c->f[ d ] );
@@ -1502,15 +1923,16 @@ int kr_init_problem( kr_ctx * c, const char * name, uint64_t seed )
     {   return ( ( size_t ) b * c->nbf + ( i0 + 2 ) + sb1 * ( i1 + 2 ) + sb2 * ( i2 + 2 ) ) * 3; };
     auto work = [ & ]( int b )
     {
-        const int reg[ 3 ] = { b % g.nb[ 0 ], ( b / g.nb[ 0 ] ) % g.nb[ 1 ], b / ( g.nb[ 0 ] * g.nb[ 1 ] ) };
+        const int gb = c->gid_h[ b ];
+        const int reg[ 3 ] = { gb % g.nb[ 0 ], ( gb / g.nb[ 0 ] ) % g.nb[ 1 ], gb / ( g.nb[ 0 ] * g.nb[ 1 ] ) };
         if( ot )
             for( int i2 = 0; i2 <= n[ 2 ]; ++ i2 )
             for( int i1 = 0; i1 <= n[ 1 ]; ++ i1 )
             for( int i0 = 0; i0 <= n[ 0 ]; ++ i0 )
             {
                 double * p = hb.data(  ) + bidx( b, i0, i1, i2 );
-                p[ 0 ] = kr_ot_bx( x_cc( g, b, 1, i1 ) );
-                p[ 1 ] = kr_ot_by( x_cc( g, b, 0, i0 ) );
+                p[ 0 ] = kr_ot_bx( x_cc( g, gb, 1, i1 ) );
+                p[ 1 ] = kr_ot_by( x_cc( g, gb, 0, i0 ) );
                 p[ 2 ] = kr_ot_bz(  );
             }
         for( int i2 = 0; i2 < n[ 2 ]; ++ i2 )
@@ -1523,14 +1945,14 @@ int kr_init_problem( kr_ctx * c, const char * name, uint64_t seed )
             const uint64_t key = kr_cell_key( 0, ig, nglob );
             double * u = hu.data(  ) + ( ( size_t ) b * c->nc + i0 + ( size_t ) n[ 0 ] * ( i1 + ( size_t ) n[ 1 ] * i2 ) ) * nw;
             if( shock )
-                kr_shock_cell( u, x_cc( g, b, 0, i0 ), g.gamma, seed, key );
+                kr_shock_cell( u, x_cc( g, gb, 0, i0 ), g.gamma, seed, key );
             else
             {
                 double x[ 3 ], bc[ 3 ];
                 for( int a = 0; a < 3; ++ a )
                 {
                     int jj[ 3 ] = { i0, i1, i2 };
-                    x[ a ] = x_cc( g, b, a, ii[ a ] );
+                    x[ a ] = x_cc( g, gb, a, ii[ a ] );
                     const double bl = hb[ bidx( b, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) + a ];
                     ++ jj[ a ];
                     bc[ a ] = ( bl + hb[ bidx( b, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) + a ] ) / 2;
@@ -1553,6 +1975,11 @@ int kr_step( kr_ctx * c, int n_steps )
     if( c->cfg.riemann == KR_RIEMANN_LEARNED && ! c->sel_ready )
     {
         c->err = "kr_step: learned face selector configured but no weights set (kr_set_selector)";
+        return -1;
+    }
+    if( c->nranks > 1 && ! c->comm )
+    {
+        c->err = "kr_step: sharded context without a communicator (kr_comm_init, or kr_group_step)";
         return -1;
     }
     cudaSetDevice( c->cfg.device );
@@ -1654,9 +2081,9 @@ int kr_selector_collect( kr_ctx * c, int n_steps, unsigned stride, uint64_t seed
     for( int k = 0; k < n_steps && ok; ++ k )
     {
         c->smp_seed = unsigned( seed * 0x9E3779B9u + k );
-        if( c->cfg.precision == 1 ) enqueue_step< true, float, true >( c, c->stream );
-        else                        enqueue_step< true, double, true >( c, c->stream );
-        ok = ck( c, cudaGetLastError(  ), "collect step" );
+        ok = c->cfg.precision == 1 ? enqueue_step< true, float, true >( c, c->stream )
+                                   : enqueue_step< true, double, true >( c, c->stream );
+        ok = ok && ck( c, cudaGetLastError(  ), "collect step" );
     }
     unsigned long long n = 0;
     ok = ok && ck( c, cudaMemcpyAsync( & n, c->smp_n, sizeof( n ), cudaMemcpyDeviceToHost, c->stream ), "read count" )
@@ -1693,7 +2120,8 @@ int kr_launches_per_step( kr_ctx * c )
                                                     : tiling_for< double >( c, axis, c->cfg.mhd ? 8 : 5 );
         flux += ( t.ok && ! c->no_tiles && c->cfg.mhd ) ? 2 : 1;
     }
-    return 2 + 2 * ( ( c->cfg.mhd ? 4 : 3 ) + flux + ( ! c->cfg.mhd && has_phys( c ) ? 1 : 0 ) );
+    const int halo = ( c->hsend.items.empty(  ) ? 0 : 1 ) + ( c->hrecv.items.empty(  ) ? 0 : 1 );
+    return 2 + 2 * ( ( c->cfg.mhd ? 4 : 3 ) + flux + ( ! c->cfg.mhd && has_phys( c ) ? 1 : 0 ) + halo );
 }
 
 int kr_diagnostics( kr_ctx * c, double * max_div_b, double * totals5 )
@@ -1718,6 +2146,181 @@ int kr_diagnostics( kr_ctx * c, double * max_div_b, double * totals5 )
         return -1;
     if( max_div_b ) * max_div_b = h[ 0 ];
     if( totals5 ) for( int k = 0; k < 5; ++ k ) totals5[ k ] = h[ 1 + k ];
+    return 0;
+}
+
+////////////////////////////////////////////////////////////
+// Sharding
+
+int kr_shard_owner( const kr_cfg * cfg, int * owner )
+{
+    g_create_error.clear(  );
+    if( ! cfg || cfg->nb[ 0 ] < 1 || cfg->nb[ 1 ] < 1 || cfg->nb[ 2 ] < 1
+        || cfg->n_ranks < 0 || ( cfg->n_ranks > 1 && ( cfg->rank < 0 || cfg->rank >= cfg->n_ranks ) ) )
+    {
+        g_create_error = "kr_shard_owner: need nb >= 1 and 0 <= rank < n_ranks";
+        return -1;
+    }
+    std::vector< int > o;
+    if( ! shard_owner( * cfg, o, g_create_error ) )
+        return -1;
+    const int me = ranks_of( * cfg ) > 1 ? cfg->rank : 0;
+    if( owner )
+        std::copy( o.begin(  ), o.end(  ), owner );
+    return int( std::count( o.begin(  ), o.end(  ), me ) );
+}
+
+int kr_halo_counts( const kr_cfg * cfg, long long * send, long long * recv )
+{
+    if( kr_shard_owner( cfg, nullptr ) < 0 || ! send || ! recv )
+        return -1;
+    std::vector< int > owner;
+    shard_owner( * cfg, owner, g_create_error );
+    const int me = ranks_of( * cfg ) > 1 ? cfg->rank : 0;
+    std::vector< int > local( owner.size(  ), -1 );
+    int nl = 0;
+    for( size_t gb = 0; gb < owner.size(  ); ++ gb )
+        if( owner[ gb ] == me ) local[ gb ] = nl ++;
+    halo_side_t hs, hr;
+    halo_plan( * cfg, owner, local, ( cfg->flags & KR_FLAG_HALO_ALL ) != 0, hs, hr );
+    for( int q = 0; q < ranks_of( * cfg ); ++ q )
+    {
+        send[ 2 * q ] = hs.w_cnt[ q ]; send[ 2 * q + 1 ] = hs.b_cnt[ q ];
+        recv[ 2 * q ] = hr.w_cnt[ q ]; recv[ 2 * q + 1 ] = hr.b_cnt[ q ];
+    }
+    return 0;
+}
+
+int kr_shard_blocks( kr_ctx * c, int * gid )
+{
+    if( ! c ) return -1;
+    if( gid ) std::copy( c->gid_h.begin(  ), c->gid_h.end(  ), gid );
+    return c->nblk;
+}
+
+int kr_comm_unique_id( unsigned char id[ 128 ] )
+{
+    static_assert( sizeof( ncclUniqueId ) == 128, "NCCL unique id size" );
+    nccl_api_t & api = nccl(  );
+    if( ! api.ok ) { g_create_error = api.err; return -1; }
+    ncclUniqueId uid;
+    const ncclResult_t r = api.GetUniqueId( & uid );
+    if( r != ncclSuccess ) { g_create_error = std::string( "ncclGetUniqueId: " ) + api.GetErrorString( r ); return -1; }
+    std::memcpy( id, & uid, sizeof( uid ) );
+    return 0;
+}
+
+int kr_comm_init( kr_ctx * c, const unsigned char id[ 128 ] )
+{
+    if( ! c || ! id ) return -1;
+    nccl_api_t & api = nccl(  );
+    if( ! api.ok ) { c->err = api.err; return -1; }
+    if( c->comm ) { c->err = "kr_comm_init: communicator already set"; return -1; }
+    cudaSetDevice( c->cfg.device );
+    ncclUniqueId uid;
+    std::memcpy( & uid, id, sizeof( uid ) );
+    const ncclResult_t r = api.CommInitRank( & c->comm, c->nranks, uid, c->rank );
+    if( r != ncclSuccess )
+    {
+        c->comm = nullptr;
+        c->err = std::string( "ncclCommInitRank: " ) + api.GetErrorString( r );
+        return -1;
+    }
+    drop_graph( c );                   // the next step captures the exchange
+    return 0;
+}
+
+}   // extern "C"
+
+template< bool MHD, class R >
+static void group_front( kr_ctx * c, cudaStream_t st, int stage )
+{
+    enqueue_front< MHD, R >( c, st, make_args< R >( c ), stage, untimed_t(  ) );
+}
+template< bool MHD, class R >
+static void group_back( kr_ctx * c, cudaStream_t st, int stage )
+{
+    enqueue_back< MHD, R >( c, st, make_args< R >( c ), stage, c->cfg.riemann, untimed_t(  ) );
+}
+
+extern "C" {
+
+int kr_group_step( kr_ctx * const * ctxs, int n, int n_steps )
+{
+    g_create_error.clear(  );
+    if( ! ctxs || n < 1 || n > KR_GROUP_MAX || n_steps < 0 || ! ctxs[ 0 ] )
+    {
+        g_create_error = "kr_group_step: need 1..64 contexts and n_steps >= 0";
+        return -1;
+    }
+    const kr_cfg & g0 = ctxs[ 0 ]->cfg;
+    std::vector< kr_ctx * > by( n, nullptr );
+    for( int k = 0; k < n; ++ k )
+    {
+        kr_ctx * c = ctxs[ k ];
+        if( ! c || c->nranks != n || by[ c->rank ] || c->cfg.device != g0.device || c->cfg.mhd != g0.mhd
+            || c->cfg.precision != g0.precision || ( c->cfg.riemann == KR_RIEMANN_LEARNED && ! c->sel_ready ) )
+        {
+            g_create_error = "kr_group_step: need the n_ranks contexts of one mesh, one per rank, on one device";
+            return -1;
+        }
+        by[ c->rank ] = c;
+    }
+    for( int p = 0; p < n; ++ p )
+        for( int q = 0; q < n; ++ q )
+            if( by[ p ]->hsend.w_cnt[ q ] != by[ q ]->hrecv.w_cnt[ p ]
+                || by[ p ]->hsend.b_cnt[ q ] != by[ q ]->hrecv.b_cnt[ p ] )
+            {
+                g_create_error = "kr_group_step: halo plans of the contexts disagree (different meshes?)";
+                return -1;
+            }
+    cudaSetDevice( g0.device );
+    cudaStream_t st = ctxs[ 0 ]->stream;
+    for( kr_ctx * c : by )
+        cudaStreamSynchronize( c->stream );
+    group_scal_t gs;
+    gs.n = n;
+    for( int r = 0; r < n; ++ r ) gs.s[ r ] = by[ r ]->s;
+    const size_t rs = by[ 0 ]->rsize;
+    const bool mhd = g0.mhd, fp32 = g0.precision == 1;
+    for( int step = 0; step < n_steps; ++ step )
+    {
+        for( kr_ctx * c : by ) k_step_begin<<< 1, 1, 0, st >>>( c->s );
+        for( int stage = 0; stage < 2; ++ stage )
+        {
+            for( kr_ctx * c : by )
+            {
+                if( mhd ) fp32 ? group_front< true, float >( c, st, stage ) : group_front< true, double >( c, st, stage );
+                else      fp32 ? group_front< false, float >( c, st, stage ) : group_front< false, double >( c, st, stage );
+            }
+            for( int p = 0; p < n; ++ p )
+                for( int q = 0; q < n; ++ q )
+                {
+                    const kr_ctx * P = by[ p ];
+                    const kr_ctx * Q = by[ q ];
+                    const long long w = P->hsend.w_cnt[ q ], b = P->hsend.b_cnt[ q ];
+                    if( w ) cudaMemcpyAsync( ( char * ) Q->recv_w + Q->hrecv.w_off[ p ] * rs,
+                                             ( char * ) P->send_w + P->hsend.w_off[ q ] * rs, w * rs, cudaMemcpyDeviceToDevice, st );
+                    if( b ) cudaMemcpyAsync( Q->recv_b + Q->hrecv.b_off[ p ], P->send_b + P->hsend.b_off[ q ],
+                                             b * sizeof( double ), cudaMemcpyDeviceToDevice, st );
+                }
+            if( stage == 0 )
+                k_group_dt_min<<< 1, 1, 0, st >>>( gs );
+            for( kr_ctx * c : by )
+            {
+                if( mhd ) fp32 ? group_back< true, float >( c, st, stage ) : group_back< true, double >( c, st, stage );
+                else      fp32 ? group_back< false, float >( c, st, stage ) : group_back< false, double >( c, st, stage );
+            }
+        }
+        for( kr_ctx * c : by ) k_step_end<<< 1, 1, 0, st >>>( c->s, c->cfg.dt_expand );
+    }
+    const cudaError_t e = cudaStreamSynchronize( st );
+    const cudaError_t l = cudaGetLastError(  );
+    if( e != cudaSuccess || l != cudaSuccess )
+    {
+        g_create_error = std::string( "kr_group_step: " ) + cudaGetErrorString( e != cudaSuccess ? e : l );
+        return -1;
+    }
     return 0;
 }
 

@@ -21,34 +21,110 @@ def _ptr(a):
     return ctypes.c_void_p(a.ctypes.data)
 
 
+def make_cfg(mhd, nb, n, gamma=1.66667, cfl=0.3, precision=2, riemann=0,
+             x_min=(0, 0, 0), x_max=(1, 1, 1), rho_floor=1e-9, tmp_floor=1e-9,
+             dt_init=0.0, dt_expand=2.0, device=0, flags=0,
+             kinds=("per",) * 6, w_fix=(0, 0, 0, 0, 0), n_ranks=1, rank=0):
+    """A kr_cfg (include/kratos_b200.h) from keyword arguments."""
+    lib = L.lib()
+    c = L.kr_cfg()
+    lib.kr_cfg_default(ctypes.byref(c))
+    c.mhd, c.precision, c.riemann = int(mhd), int(precision), int(riemann)
+    for a in range(3):
+        c.nb[a], c.n[a] = int(nb[a]), int(n[a])
+        c.x_min[a], c.x_max[a] = float(x_min[a]), float(x_max[a])
+    c.gamma, c.cfl = float(gamma), float(cfl)
+    c.rho_floor, c.tmp_floor = float(rho_floor), float(tmp_floor)
+    c.dt_init, c.dt_expand, c.device = float(dt_init), float(dt_expand), int(device)
+    c.flags = int(flags)              # KR_FLAG_TILED, KR_FLAG_HALO_ALL
+    c.n_ranks, c.rank = int(n_ranks), int(rank)
+    for k in range(6):
+        c.bc[k] = L.BC_KINDS[kinds[k]]
+    for k in range(5):
+        c.w_fix[k] = float(w_fix[k])
+    return c
+
+
+def shard_owner(cfg):
+    """Owner rank of every global block, and the number of cfg.rank's blocks."""
+    nglob = cfg.nb[0] * cfg.nb[1] * cfg.nb[2]
+    owner = np.empty(nglob, np.int32)
+    k = L.lib().kr_shard_owner(ctypes.byref(cfg), _ptr(owner))
+    if k < 0:
+        raise KratosError(L.lib().kr_last_error(None).decode())
+    return owner, k
+
+
+def halo_counts(cfg):
+    """Per-stage halo words of cfg.rank with every peer: (send, recv), each
+    [n_ranks, 2] = (primitive words, face-B words)."""
+    r = max(1, cfg.n_ranks)
+    snd, rcv = np.zeros((r, 2), np.int64), np.zeros((r, 2), np.int64)
+    if L.lib().kr_halo_counts(ctypes.byref(cfg), _ptr(snd), _ptr(rcv)) != 0:
+        raise KratosError(L.lib().kr_last_error(None).decode())
+    return snd, rcv
+
+
+def _nccl_host():
+    """Point the engine at the libnccl.so.2 that torch links (the nvidia-nccl
+    wheel), without importing torch: a process holds one NCCL, and torch
+    needs its own version's symbols when it is imported later."""
+    import importlib.util
+    import os
+    if os.environ.get("KRATOS_B200_NCCL"):
+        return
+    try:
+        spec = importlib.util.find_spec("nvidia.nccl")
+    except (ImportError, ValueError):
+        spec = None
+    for d in (spec.submodule_search_locations if spec else []) or []:
+        cand = os.path.join(d, "lib", "libnccl.so.2")
+        if os.path.exists(cand):
+            os.environ["KRATOS_B200_NCCL"] = cand
+            return
+
+
+def comm_unique_id():
+    """128-byte NCCL unique id (ncclGetUniqueId), to be shared with every rank."""
+    _nccl_host()
+    buf = (ctypes.c_ubyte * 128)()
+    if L.lib().kr_comm_unique_id(buf) != 0:
+        raise KratosError(L.lib().kr_last_error(None).decode())
+    return bytes(buf)
+
+
+def group_step(dyns, n_steps=1):
+    """Step the n_ranks shard contexts of one mesh together from this process
+    (one device; the exchange is device copies, synchronous)."""
+    arr = (ctypes.c_void_p * len(dyns))(*[d._h for d in dyns])
+    if L.lib().kr_group_step(arr, len(dyns), int(n_steps)) != 0:
+        raise KratosError(L.lib().kr_last_error(None).decode())
+
+
 class Dynamics:
-    def __init__(self, mhd, nb, n, gamma=1.66667, cfl=0.3, precision=2, riemann=0,
-                 x_min=(0, 0, 0), x_max=(1, 1, 1), rho_floor=1e-9, tmp_floor=1e-9,
-                 dt_init=0.0, dt_expand=2.0, device=0, flags=0,
-                 kinds=("per",) * 6, w_fix=(0, 0, 0, 0, 0)):
+    """One engine context.  With n_ranks > 1 it holds rank `rank`'s share of
+    the nb[0] x nb[1] x nb[2] blocks (`gid`, ascending global ids) and needs a
+    communicator (`comm_init`) or `group_step` to advance."""
+
+    def __init__(self, mhd, nb, n, **kw):
         lib = L.lib()
-        c = L.kr_cfg()
-        lib.kr_cfg_default(ctypes.byref(c))
-        c.mhd, c.precision, c.riemann = int(mhd), int(precision), int(riemann)
-        for a in range(3):
-            c.nb[a], c.n[a] = int(nb[a]), int(n[a])
-            c.x_min[a], c.x_max[a] = float(x_min[a]), float(x_max[a])
-        c.gamma, c.cfl = float(gamma), float(cfl)
-        c.rho_floor, c.tmp_floor = float(rho_floor), float(tmp_floor)
-        c.dt_init, c.dt_expand, c.device = float(dt_init), float(dt_expand), int(device)
-        c.reserved[0] = int(flags)           # bit 0: shared-memory tiled flux sweeps
-        for k in range(6):
-            c.bc[k] = L.BC_KINDS[kinds[k]]
-        for k in range(5):
-            c.w_fix[k] = float(w_fix[k])
+        c = make_cfg(mhd, nb, n, **kw)
         self.cfg = c
         self._h = lib.kr_ctx_create(ctypes.byref(c))
         if not self._h:
             raise KratosError(lib.kr_last_error(None).decode())
         self.mhd = bool(mhd)
         self.nb, self.n = tuple(int(x) for x in nb), tuple(int(x) for x in n)
-        self.nblk = self.nb[0] * self.nb[1] * self.nb[2]
+        self.nblk = lib.kr_shard_blocks(self._h, None)
+        gid = np.empty(self.nblk, np.int32)
+        lib.kr_shard_blocks(self._h, _ptr(gid))
+        self.gid = gid
         self.nw = 8 if mhd else 5
+
+    def comm_init(self, uid):
+        _nccl_host()
+        buf = (ctypes.c_ubyte * 128).from_buffer_copy(uid)
+        self._check(L.lib().kr_comm_init(self._h, buf), "kr_comm_init")
 
     # ------------------------------------------------------------------ admin
     def close(self):
