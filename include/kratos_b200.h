@@ -41,7 +41,7 @@
 extern "C" {
 #endif
 
-#define KR_ABI_VERSION 3
+#define KR_ABI_VERSION 4
 
 /* [boundary] kinds per side (hydro/boundary/phys_functors.h:11-91): an axis is
  * periodic only when both its sides are KR_BC_PER. */
@@ -79,9 +79,9 @@ typedef struct
     double dt_init;            /* [cycle] dt_init (0: unset)                     */
     double dt_expand;          /* [cycle] dt_expand                              */
     int    device;             /* CUDA device ordinal                            */
-    int    bc[ 6 ];            /* enum kr_bc_t for x-, x+, y-, y+, z-, z+;       */
-                               /* non-periodic sides: hydro only                 */
+    int    bc[ 6 ];            /* enum kr_bc_t for x-, x+, y-, y+, z-, z+       */
     double w_fix[ 5 ];         /* KR_BC_FIXD primitive state: rho, p, v0..2       */
+    double b_fix[ 3 ];         /* KR_BC_FIXD magnetic field (MHD): [init] b0      */
     int    flags;              /* KR_FLAG_* bits                                 */
     int    n_ranks;            /* ranks sharing the mesh (0 or 1: not sharded)   */
     int    rank;               /* this context's rank, 0 <= rank < n_ranks       */

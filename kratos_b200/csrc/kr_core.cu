@@ -85,6 +85,8 @@ struct args_t
     int nbk[ 3 ];                     // blocks per axis (global mesh)
     int bc[ 6 ];                      // kr_bc_t per side
     double w_fix[ 5 ];
+    double b_fix[ 3 ];
+    int emf_out;                      // bit a: high side of axis a is out / fre (MHD)
     scal_t * s;
 };
 
@@ -406,6 +408,127 @@ __global__ void __launch_bounds__( 128 ) k_phys( const args_t< R > a )
             else
                 v = c0[ k ];                 // outflow, free: zero gradient
             a.w[ iw( a, b, k, 5, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] = v;
+        }
+    }
+}
+
+////////////////////////////////////////////////////////////
+// MHD physical boundaries (mhd/boundary/phys.h:118-250, phys_functors.h:9-132).
+// One launch per non-periodic side (sides in order, so cells shared by two
+// sides take the later side's values); one thread per transverse row of the
+// ghost shell, ghost rows included.  The source row is clamped into the
+// interior only along transverse axes that end at a physical side there; the
+// three cells (primitives, cell-centred B) and faces (normal B on the face
+// lattice, tangential B on the cell lattice) next to the boundary go through
+// the functor into the two ghost layers.  The ghost cells' E = B x v is
+// stored with them, as the edge EMF reads it (integrator.h:201-213).  Runs
+// after the same-level fill: the reference also runs it once before, with
+// face B, but those values from not-yet-filled rows land only in ghost-shell
+// corner slots that no stencil reads.
+
+template< class R >
+__global__ void __launch_bounds__( 128 ) k_phys_mhd( const args_t< R > a, int side, int step )
+{
+    const int b = blockIdx.y;
+    const int axis = side >> 1, right = side & 1;
+    const int kind = a.bc[ side ];
+    const int g = a.gid[ b ];
+    const int reg[ 3 ] = { g % a.nbk[ 0 ], ( g / a.nbk[ 0 ] ) % a.nbk[ 1 ], g / ( a.nbk[ 0 ] * a.nbk[ 1 ] ) };
+    if( reg[ axis ] != ( right ? a.nbk[ axis ] - 1 : 0 ) )
+        return;
+    const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
+    const int a1 = mod3( axis + 1 ), a2 = mod3( axis + 2 );
+    const int e1 = nn[ a1 ] + 4;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if( t >= e1 * ( nn[ a2 ] + 4 ) )
+        return;
+    int i_tgt[ 3 ], i_src[ 3 ], i_sfc[ 3 ];
+    i_tgt[ a1 ] = t % e1 - 2;
+    i_tgt[ a2 ] = t / e1 - 2;
+    for( int h = 0; h < 2; ++ h )
+    {
+        const int d = h ? a2 : a1;
+        int r = i_tgt[ d ], f = i_tgt[ d ];
+        if( a.bc[ 2 * d ] != KR_BC_PER && reg[ d ] == 0 )
+        {   r = max( r, 0 ); f = max( f, 0 ); }
+        if( a.bc[ 2 * d + 1 ] != KR_BC_PER && reg[ d ] == a.nbk[ d ] - 1 )
+        {   r = min( r, nn[ d ] - 1 ); f = min( f, nn[ d ] ); }
+        i_src[ d ] = r;
+        i_sfc[ d ] = f;
+    }
+    const int n = nn[ axis ];
+    const double * BF = a.bf[ step ];
+    R hyd[ 5 ][ 8 ], bc[ 5 ][ 3 ];          // index i + 2, i = -2..2
+    double bfb[ 5 ][ 3 ];
+    for( int i = 0; i <= 2; ++ i )
+    {
+        i_src[ axis ] = right ? n - i - 1 : i;
+        i_sfc[ axis ] = right ? n - i : i;
+        for( int k = 0; k < 8; ++ k )
+            hyd[ 2 + i ][ k ] = a.w[ iw( a, b, k, 11, i_src[ 0 ], i_src[ 1 ], i_src[ 2 ] ) ];
+        for( int q = 0; q < 3; ++ q )
+        {
+            bc[ 2 + i ][ q ] = hyd[ 2 + i ][ BCC + q ];
+            bfb[ 2 + i ][ q ] = q == axis ? BF[ ibf( a, b, q, i_sfc[ 0 ], i_sfc[ 1 ], i_sfc[ 2 ] ) ]
+                                          : BF[ ibf( a, b, q, i_src[ 0 ], i_src[ 1 ], i_src[ 2 ] ) ];
+        }
+    }
+    const int i_mom = MOM + axis;
+    if( kind == KR_BC_OUT && hyd[ 2 ][ i_mom ] * R( right ? -1 : 1 ) > 0 )
+        hyd[ 2 ][ i_mom ] = 0;                   // no inflow through an outflow side
+    for( int i = -2; i < 0; ++ i )
+    {
+        for( int k = 0; k < 8; ++ k )
+        {
+            if( kind == KR_BC_REF )
+                hyd[ 2 + i ][ k ] = hyd[ 2 - i - 1 ][ k ] * R( k == i_mom ? -1 : 1 );
+            else if( kind == KR_BC_FIXD )
+                hyd[ 2 + i ][ k ] = R( k < 5 ? a.w_fix[ k ] : a.b_fix[ k - 5 ] );
+            else
+                hyd[ 2 + i ][ k ] = hyd[ 2 ][ k ];
+        }
+        for( int q = 0; q < 3; ++ q )
+        {
+            if( kind == KR_BC_REF )
+            {   // faces mirror at -i, cells at -i-1; tangential components flip
+                bfb[ 2 + i ][ q ] = ( q != axis ? -1. : 1. ) * bfb[ 2 - i ][ q ];
+                bc [ 2 + i ][ q ] = R( q != axis ? -1 : 1 ) * bc[ 2 - i - 1 ][ q ];
+            }
+            else if( kind == KR_BC_FIXD )
+            {
+                bfb[ 2 + i ][ q ] = a.b_fix[ q ];
+                bc [ 2 + i ][ q ] = R( a.b_fix[ q ] );
+            }
+            else
+            {
+                bfb[ 2 + i ][ q ] = bfb[ 2 ][ q ];
+                bc [ 2 + i ][ q ] = bc [ 2 ][ q ];
+            }
+        }
+    }
+    double * BFw = a.bf[ step ];
+    for( int i = -2; i < 0; ++ i )
+    {
+        i_tgt[ axis ] = right ? n - i - 1 : i;
+        int i_fbc[ 3 ] = { i_tgt[ 0 ], i_tgt[ 1 ], i_tgt[ 2 ] };
+        i_fbc[ axis ] = right ? n - i : i;
+        R * p = hyd[ 2 + i ];
+        for( int q = 0; q < 3; ++ q )
+            p[ BCC + q ] = bc[ 2 + i ][ q ];
+        for( int k = 0; k < 8; ++ k )
+            a.w[ iw( a, b, k, 11, i_tgt[ 0 ], i_tgt[ 1 ], i_tgt[ 2 ] ) ] = p[ k ];
+        for( int d = 0; d < 3; ++ d )
+        {
+            const int d1 = mod3( d + 1 ), d2 = mod3( d + 2 );
+            a.w[ iw( a, b, 8 + d, 11, i_tgt[ 0 ], i_tgt[ 1 ], i_tgt[ 2 ] ) ] =
+                p[ BCC + d1 ] * p[ MOM + d2 ] - p[ BCC + d2 ] * p[ MOM + d1 ];
+        }
+        for( int q = 0; q < 3; ++ q )
+        {
+            if( q == axis )
+                BFw[ ibf( a, b, q, i_fbc[ 0 ], i_fbc[ 1 ], i_fbc[ 2 ] ) ] = bfb[ 2 + i ][ q ];
+            else
+                BFw[ ibf( a, b, q, i_tgt[ 0 ], i_tgt[ 1 ], i_tgt[ 2 ] ) ] = bfb[ 2 + i ][ q ];
         }
     }
 }
@@ -760,6 +883,30 @@ __global__ void __launch_bounds__( 256 ) k_emf( const args_t< R > a )
             }
         }
         a.ee[ ifx( a, b, ax, 3, i[ 0 ], i[ 1 ], i[ 2 ] ) ] = e;
+    }
+    if( ! a.emf_out )
+        return;
+    // boundary-plane edges of a high out / fre side: the interior cell's
+    // advective E, with the reference's velocity scaling (w holds v, which it
+    // multiplies by 1 / rho once more) -- integrator.h:329-382
+    const int g = a.gid[ b ];
+    const int reg[ 3 ] = { g % a.nbk[ 0 ], ( g / a.nbk[ 0 ] ) % a.nbk[ 1 ], g / ( a.nbk[ 0 ] * a.nbk[ 1 ] ) };
+    for( int d = 0; d < 3; ++ d )
+    {
+        if( ! ( a.emf_out >> d & 1 ) || i[ d ] != nn[ d ] || nn[ d ] < 2 || reg[ d ] != a.nbk[ d ] - 1 )
+            continue;
+        int jc[ 3 ] = { i[ 0 ], i[ 1 ], i[ 2 ] };
+        -- jc[ d ];
+        const R irho = R( 1 ) / fmax( a.w[ iw( a, b, RHO, 11, jc[ 0 ], jc[ 1 ], jc[ 2 ] ) ], R( 1e-30 ) );
+        R v_c[ 3 ], b_c[ 3 ];
+        for( int q = 0; q < 3; ++ q )
+        {
+            v_c[ q ] = a.w[ iw( a, b, MOM + q, 11, jc[ 0 ], jc[ 1 ], jc[ 2 ] ) ] * irho;
+            b_c[ q ] = a.w[ iw( a, b, BCC + q, 11, jc[ 0 ], jc[ 1 ], jc[ 2 ] ) ];
+        }
+        const int d1 = mod3( d + 1 ), d2 = mod3( d + 2 );
+        a.ee[ ifx( a, b, d1, 3, i[ 0 ], i[ 1 ], i[ 2 ] ) ] = v_c[ d ] * b_c[ d2 ] - v_c[ d2 ] * b_c[ d ];
+        a.ee[ ifx( a, b, d2, 3, i[ 0 ], i[ 1 ], i[ 2 ] ) ] = v_c[ d1 ] * b_c[ d ] - v_c[ d ] * b_c[ d1 ];
     }
 }
 
@@ -1296,6 +1443,11 @@ static args_t< R > make_args( kr_ctx * c )
     for( int d = 0; d < 3; ++ d ) a.nbk[ d ] = c->cfg.nb[ d ];
     for( int k = 0; k < 6; ++ k ) a.bc[ k ] = c->cfg.bc[ k ];
     for( int k = 0; k < 5; ++ k ) a.w_fix[ k ] = c->cfg.w_fix[ k ];
+    for( int k = 0; k < 3; ++ k ) a.b_fix[ k ] = c->cfg.b_fix[ k ];
+    a.emf_out = 0;
+    for( int d = 0; d < 3; ++ d )
+        if( c->cfg.bc[ 2 * d + 1 ] == KR_BC_OUT || c->cfg.bc[ 2 * d + 1 ] == KR_BC_FRE )
+            a.emf_out |= 1 << d;
     a.sel_w = c->sel_w; a.sel_b = c->sel_b; a.sel_thr = c->sel_thr; a.sel_cnt = c->sel_cnt;
     a.smp = c->smp; a.smp_n = c->smp_n; a.smp_max = c->smp_max;
     a.smp_stride = c->smp_stride; a.smp_seed = c->smp_seed;
@@ -1423,7 +1575,15 @@ static void enqueue_back( kr_ctx * c, cudaStream_t st, const args_t< R > & a, in
                 a, c->recv_items, ( R * ) c->recv_w, c->recv_b, stage );
         k_ghost< MHD, R ><<< dim3( blocks_for( nghost, 256 ), nb ), 256, 0, st >>>( a, stage );
         if( ! MHD && has_phys( c ) )
-            k_phys< R ><<< dim3( blocks_for( phys_sites( c ), 128 ), 6, nb ), 128, 0, st >>>( a ); } );
+            k_phys< R ><<< dim3( blocks_for( phys_sites( c ), 128 ), 6, nb ), 128, 0, st >>>( a );
+        if( MHD )
+            for( int side = 0; side < 6; ++ side )
+                if( c->cfg.bc[ side ] != KR_BC_PER )
+                {
+                    const int ax = side / 2;
+                    const long long rows = ( long long )( n[ ( ax + 1 ) % 3 ] + 4 ) * ( n[ ( ax + 2 ) % 3 ] + 4 );
+                    k_phys_mhd< R ><<< dim3( blocks_for( rows, 128 ), nb ), 128, 0, st >>>( a, side, stage );
+                } } );
     for( int axis = 2; axis >= 0; -- axis )
         timed( 4 - axis, [ & ] { launch_flux_mode< MHD, R >( c, st, a, axis, stage, mode ); } );
     if( MHD )
@@ -1657,10 +1817,9 @@ kr_ctx * kr_ctx_create( const kr_cfg * cfg )
         return nullptr;
     }
     for( int k = 0; k < 6; ++ k )
-        if( cfg->bc[ k ] < KR_BC_PER || cfg->bc[ k ] > KR_BC_FIXD
-            || ( cfg->mhd && cfg->bc[ k ] != KR_BC_PER ) )
+        if( cfg->bc[ k ] < KR_BC_PER || cfg->bc[ k ] > KR_BC_FIXD )
         {
-            g_create_error = "kr_ctx_create: boundary kinds must be kr_bc_t; non-periodic sides are hydro only";
+            g_create_error = "kr_ctx_create: boundary kinds must be kr_bc_t";
             return nullptr;
         }
     for( int a = 0; a < 3; ++ a )
@@ -2121,7 +2280,11 @@ int kr_launches_per_step( kr_ctx * c )
         flux += ( t.ok && ! c->no_tiles && c->cfg.mhd ) ? 2 : 1;
     }
     const int halo = ( c->hsend.items.empty(  ) ? 0 : 1 ) + ( c->hrecv.items.empty(  ) ? 0 : 1 );
-    return 2 + 2 * ( ( c->cfg.mhd ? 4 : 3 ) + flux + ( ! c->cfg.mhd && has_phys( c ) ? 1 : 0 ) + halo );
+    int phys = ! c->cfg.mhd && has_phys( c ) ? 1 : 0;
+    if( c->cfg.mhd )
+        for( int s = 0; s < 6; ++ s )
+            phys += c->cfg.bc[ s ] != KR_BC_PER;
+    return 2 + 2 * ( ( c->cfg.mhd ? 4 : 3 ) + flux + phys + halo );
 }
 
 int kr_diagnostics( kr_ctx * c, double * max_div_b, double * totals5 )

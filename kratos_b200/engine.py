@@ -24,7 +24,7 @@ def _ptr(a):
 def make_cfg(mhd, nb, n, gamma=1.66667, cfl=0.3, precision=2, riemann=0,
              x_min=(0, 0, 0), x_max=(1, 1, 1), rho_floor=1e-9, tmp_floor=1e-9,
              dt_init=0.0, dt_expand=2.0, device=0, flags=0,
-             kinds=("per",) * 6, w_fix=(0, 0, 0, 0, 0), n_ranks=1, rank=0):
+             kinds=("per",) * 6, w_fix=(0, 0, 0, 0, 0), b_fix=(0, 0, 0), n_ranks=1, rank=0):
     """A kr_cfg (include/kratos_b200.h) from keyword arguments."""
     lib = L.lib()
     c = L.kr_cfg()
@@ -42,6 +42,8 @@ def make_cfg(mhd, nb, n, gamma=1.66667, cfl=0.3, precision=2, riemann=0,
         c.bc[k] = L.BC_KINDS[kinds[k]]
     for k in range(5):
         c.w_fix[k] = float(w_fix[k])
+    for k in range(3):
+        c.b_fix[k] = float(b_fix[k])
     return c
 
 

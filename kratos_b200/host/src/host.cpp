@@ -404,6 +404,8 @@ void mesh_t::init( const input & args )
     c.w_fix[ 1 ] = args.get< double >( "init", "pre0", 0 );
     const auto v0 = args.get< type::coord2_t >( "init", "vel0", 0 );
     for( int a = 0; a < 3; ++ a ) c.w_fix[ 2 + a ] = v0[ a ];
+    const auto b0 = args.get< type::coord2_t >( "init", "b0", 0 );
+    for( int a = 0; a < 3; ++ a ) c.b_fix[ a ] = b0[ a ];
     ctx_ = kr_ctx_create( & c );
     if( ! ctx_ )
         throw std::runtime_error( std::string( "kratos_b200: " ) + kr_last_error( nullptr ) );

@@ -28,6 +28,7 @@ class _Cfg(ctypes.Structure):
         ("n_threads", ctypes.c_int),
         ("bc", ctypes.c_int * 6),
         ("w_fix", ctypes.c_double * 5),
+        ("b_fix", ctypes.c_double * 3),
     ]
 
 
@@ -83,7 +84,7 @@ class OracleMesh:
 
     def __init__(self, mhd, nb, n, gamma, cfl=0.3, x_min=(0, 0, 0), x_max=(1, 1, 1),
                  d_floor=1e-9, t_floor=1e-9, dt_expand=2.0, dt_init=0.0, n_threads=0,
-                 kinds=("per",) * 6, w_fix=(0, 0, 0, 0, 0)):
+                 kinds=("per",) * 6, w_fix=(0, 0, 0, 0, 0), b_fix=(0, 0, 0)):
         c = _Cfg()
         c.mhd = int(mhd)
         for a in range(3):
@@ -95,6 +96,8 @@ class OracleMesh:
             c.bc[k] = BC_KINDS[kinds[k]]
         for k in range(5):
             c.w_fix[k] = float(w_fix[k])
+        for k in range(3):
+            c.b_fix[k] = float(b_fix[k])
         self.cfg = c
         self.mhd = bool(mhd)
         self.nb, self.n = tuple(nb), tuple(n)
@@ -102,7 +105,7 @@ class OracleMesh:
         self.nw = 8 if mhd else 5
         self._h = lib().kro_create(ctypes.byref(c))
         if not self._h:
-            raise ValueError("oracle: non-periodic boundaries are restated for hydro only")
+            raise ValueError("oracle: kro_create failed")
         self.t = 0.0
         # cycle.cpp:163-166: an unset dt_init starts the device dt at FLT_MAX / 10
         self.dt_bound = dt_init if dt_init >= np.finfo(np.float32).tiny else FLT_MAX / 10

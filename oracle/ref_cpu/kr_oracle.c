@@ -169,10 +169,6 @@ double kro_dx( const kro_mesh * m, int b, int a ) { return m->dx0[ b * 3 + a ]; 
 
 kro_mesh * kro_create( const kro_cfg * cfg )
 {
-    if( cfg->mhd )
-        for( int s = 0; s < 6; ++ s )
-            if( cfg->bc[ s ] != KRO_PER )
-                return NULL;                 /* non-periodic MHD: not restated */
     kro_mesh * m = ( kro_mesh * ) calloc( 1, sizeof( kro_mesh ) );
     m->c    = * cfg;
     m->nw   = cfg->mhd ? 8 : 5;
@@ -556,6 +552,129 @@ static void bc_block( kro_mesh * m, int b, void * aux )
             {
                 ii[ axis ] = right ? n[ axis ] - i - 1 : i;
                 memcpy( w + iw( m, ii[ 0 ], ii[ 1 ], ii[ 2 ] ), buf[ 2 + i ], sizeof( double ) * nw );
+            }
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* MHD physical boundaries (mhd/boundary/phys.h:118-250 operator(),      */
+/* phys_functors.h:9-132 free / fixed / outflow / reflect).  Per side on  */
+/* the domain edge, every transverse row of the ghost shell (ghost rows   */
+/* included) takes its source row clamped into the interior only along    */
+/* transverse axes that end at a physical side there; the n_gh + 1 cells  */
+/* (primitives, cell-centred B) and faces (normal B on the face lattice,  */
+/* tangential B on the cell lattice) next to the boundary go through the  */
+/* functor into the ghost slots.  Sides in order x-, x+, y-, y+, z-, z+.  */
+/* The reference runs this once before and once after the same-level     */
+/* exchange (keeper_t::act_bnd, face B only in the first pass); this      */
+/* restatement runs it once after the exchange: the first pass's face-B   */
+/* values from not-yet-exchanged rows land only in ghost-shell corner     */
+/* slots, which no later stencil reads.                                   */
+
+static void bc_block_mhd( kro_mesh * m, int b, void * aux )
+{
+    const int step = ( ( ghost_arg * ) aux )->step;
+    const int * n = m->c.n;
+    const int nw = m->nw;
+    const int reg[ 3 ] = { b % m->c.nb[ 0 ], ( b / m->c.nb[ 0 ] ) % m->c.nb[ 1 ],
+                           b / ( m->c.nb[ 0 ] * m->c.nb[ 1 ] ) };
+    double * w = m->w + ( size_t ) b * m->nw_cells * nw;
+    double * bf = m->bf[ step ] + ( size_t ) b * m->nbf;
+    int phy[ 3 ][ 2 ];                       /* geo.phybnd_flag */
+    for( int a = 0; a < 3; ++ a )
+    {
+        phy[ a ][ 0 ] = m->c.bc[ 2 * a ] != KRO_PER && reg[ a ] == 0;
+        phy[ a ][ 1 ] = m->c.bc[ 2 * a + 1 ] != KRO_PER && reg[ a ] == m->c.nb[ a ] - 1;
+    }
+    for( int side = 0; side < 6; ++ side )
+    {
+        const int axis = side / 2, right = side & 1;
+        const int kind = m->c.bc[ side ];
+        if( kind == KRO_PER || ! phy[ axis ][ right ] )
+            continue;
+        const int a1 = mod3( axis + 1 ), a2 = mod3( axis + 2 );
+        const int i_mom = MOM + axis;
+        const int nn = n[ axis ];
+        for( int t2 = -2; t2 < n[ a2 ] + 2; ++ t2 )
+        for( int t1 = -2; t1 < n[ a1 ] + 2; ++ t1 )
+        {
+            int i_tgt[ 3 ], i_src[ 3 ], i_sfc[ 3 ];
+            i_tgt[ a1 ] = t1;
+            i_tgt[ a2 ] = t2;
+            for( int h = 0; h < 2; ++ h )
+            {
+                const int a = h ? a2 : a1;
+                int r = i_tgt[ a ], f = i_tgt[ a ];
+                if( phy[ a ][ 0 ] ) { r = r < 0 ? 0 : r; f = f < 0 ? 0 : f; }
+                if( phy[ a ][ 1 ] ) { r = r > n[ a ] - 1 ? n[ a ] - 1 : r; f = f > n[ a ] ? n[ a ] : f; }
+                i_src[ a ] = r;
+                i_sfc[ a ] = f;
+            }
+            double hyd[ 5 ][ 8 ], bc[ 5 ][ 3 ], bfb[ 5 ][ 3 ];   /* index i + 2, i = -2..2 */
+            for( int i = 0; i <= 2; ++ i )
+            {
+                i_src[ axis ] = right ? nn - i - 1 : i;
+                i_sfc[ axis ] = right ? nn - i : i;
+                const double * hs = w + iw( m, i_src[ 0 ], i_src[ 1 ], i_src[ 2 ] );
+                for( int k = 0; k < 8; ++ k )
+                    hyd[ 2 + i ][ k ] = hs[ k ];
+                for( int q = 0; q < 3; ++ q )
+                {
+                    bc[ 2 + i ][ q ] = hs[ BCC + q ];
+                    bfb[ 2 + i ][ q ] = q == axis ? bf[ ib( m, i_sfc[ 0 ], i_sfc[ 1 ], i_sfc[ 2 ] ) + q ]
+                                                  : bf[ ib( m, i_src[ 0 ], i_src[ 1 ], i_src[ 2 ] ) + q ];
+                }
+            }
+            /* hydro part of the functor (n_int = 8: the B_cc slots ride along and
+             * are replaced by the field part below) */
+            if( kind == KRO_OUT && hyd[ 2 ][ i_mom ] * ( right ? -1 : 1 ) > 0 )
+                hyd[ 2 ][ i_mom ] = 0;
+            for( int i = -2; i < 0; ++ i )
+                for( int k = 0; k < 8; ++ k )
+                {
+                    if( kind == KRO_REF )
+                        hyd[ 2 + i ][ k ] = hyd[ 2 - i - 1 ][ k ] * ( k == i_mom ? -1 : 1 );
+                    else if( kind == KRO_FIXD )
+                        hyd[ 2 + i ][ k ] = k < 5 ? m->c.w_fix[ k ] : m->c.b_fix[ k - 5 ];
+                    else
+                        hyd[ 2 + i ][ k ] = hyd[ 2 ][ k ];
+                }
+            /* field part */
+            for( int i = -2; i < 0; ++ i )
+                for( int q = 0; q < 3; ++ q )
+                {
+                    if( kind == KRO_REF )
+                    {   /* faces mirror at -i, cells at -i-1; tangential components
+                         * flip sign (phys_functors.h:120-131) */
+                        const double sg = q != axis ? -1 : 1;
+                        bfb[ 2 + i ][ q ] = sg * bfb[ 2 - i ][ q ];
+                        bc [ 2 + i ][ q ] = sg * bc [ 2 - i - 1 ][ q ];
+                    }
+                    else if( kind == KRO_FIXD )
+                        bfb[ 2 + i ][ q ] = bc[ 2 + i ][ q ] = m->c.b_fix[ q ];
+                    else
+                    {
+                        bc [ 2 + i ][ q ] = bc [ 2 ][ q ];
+                        bfb[ 2 + i ][ q ] = bfb[ 2 ][ q ];
+                    }
+                }
+            for( int i = -2; i < 0; ++ i )
+            {
+                i_tgt[ axis ] = right ? nn - i - 1 : i;
+                int i_fbc[ 3 ] = { i_tgt[ 0 ], i_tgt[ 1 ], i_tgt[ 2 ] };
+                i_fbc[ axis ] = right ? nn - i : i;
+                double * ht = w + iw( m, i_tgt[ 0 ], i_tgt[ 1 ], i_tgt[ 2 ] );
+                for( int k = 0; k < 8; ++ k )
+                    ht[ k ] = hyd[ 2 + i ][ k ];
+                for( int q = 0; q < 3; ++ q )
+                {
+                    ht[ BCC + q ] = bc[ 2 + i ][ q ];
+                    if( q == axis )
+                        bf[ ib( m, i_fbc[ 0 ], i_fbc[ 1 ], i_fbc[ 2 ] ) + q ] = bfb[ 2 + i ][ q ];
+                    else
+                        bf[ ib( m, i_tgt[ 0 ], i_tgt[ 1 ], i_tgt[ 2 ] ) + q ] = bfb[ 2 + i ][ q ];
+                }
             }
         }
     }
@@ -1100,6 +1219,32 @@ static void emf_block( kro_mesh * m, int b, void * aux )
             }
             ee[ ie( m, i0, i1, i2 ) + ax ] = e;
         }
+        /* boundary-plane edges of a high out / fre side: the interior cell's
+         * advective E, with the reference's velocity scaling (w holds v, which
+         * it multiplies by 1 / rho once more) -- integrator.h:329-382 */
+        for( int a = 0; a < 3; ++ a )
+        {
+            if( i[ a ] != n[ a ] || n[ a ] < 2 )
+                continue;
+            const int kind = m->c.bc[ 2 * a + 1 ];
+            const int reg_a = a == 0 ? b % m->c.nb[ 0 ]
+                            : a == 1 ? ( b / m->c.nb[ 0 ] ) % m->c.nb[ 1 ] : b / ( m->c.nb[ 0 ] * m->c.nb[ 1 ] );
+            if( kind == KRO_PER || reg_a != m->c.nb[ a ] - 1 || ( kind != KRO_OUT && kind != KRO_FRE ) )
+                continue;
+            int jc[ 3 ] = { i[ 0 ], i[ 1 ], i[ 2 ] };
+            -- jc[ a ];
+            const double * p = w + iw( m, jc[ 0 ], jc[ 1 ], jc[ 2 ] );
+            const double irho = 1.0 / fmax( p[ RHO ], 1e-30 );
+            double v_c[ 3 ], b_c[ 3 ];
+            for( int q = 0; q < 3; ++ q )
+            {
+                v_c[ q ] = p[ MOM + q ] * irho;
+                b_c[ q ] = p[ BCC + q ];
+            }
+            const int a1 = mod3( a + 1 ), a2 = mod3( a + 2 );
+            ee[ ie( m, i0, i1, i2 ) + a1 ] = v_c[ a ] * b_c[ a2 ] - v_c[ a2 ] * b_c[ a ];
+            ee[ ie( m, i0, i1, i2 ) + a2 ] = v_c[ a1 ] * b_c[ a ] - v_c[ a ] * b_c[ a1 ];
+        }
     }
 }
 
@@ -1165,7 +1310,7 @@ int kro_step( kro_mesh * m, int n_steps, double * t, double * dt_bound, double *
             }
             ghost_arg ga = { stage };
             par_blocks( m, ghost_block, & ga );
-            par_blocks( m, bc_block, NULL );
+            par_blocks( m, m->c.mhd ? bc_block_mhd : bc_block, & ga );
             const double dt = dt_use * ( stage == 0 ? 1.0 : ( double ) 0.5f );
             for( int axis = 2; axis >= 0; -- axis )
             {

@@ -40,10 +40,10 @@ typedef struct
     int    n_threads;        /* host threads used (<= 0: all)                   */
     /* [boundary] kinds per side (x-, x+, y-, y+, z-, z+): KRO_PER, KRO_OUT,
      * KRO_REF, KRO_FRE, KRO_FIXD (hydro/boundary/phys_functors.h); an axis is
-     * periodic only if both its sides are KRO_PER.  Non-periodic sides are
-     * hydro only here. */
+     * periodic only if both its sides are KRO_PER. */
     int    bc[ 6 ];
     double w_fix[ 5 ];       /* [init] rho0, pre0, vel0 for KRO_FIXD            */
+    double b_fix[ 3 ];       /* [init] b0 for KRO_FIXD (MHD)                    */
 } kro_cfg;
 
 typedef struct kro_mesh kro_mesh;

@@ -24,10 +24,10 @@ TOL_FP64_LONG = 1e-10
 def _dyn(meta, precision=2, riemann=0):
     from kratos_b200 import Dynamics
     extra = meta.get("dynamics", {})
-    kinds, w_fix = G.boundary(meta)
+    kinds, w_fix, b_fix = G.boundary(meta)
     return Dynamics(meta["workload"] == "ot", meta["nb"], meta["n"], gamma=meta["gamma"],
                     cfl=meta["cfl"], tmp_floor=float(extra.get("tmp_floor", 1e-9)),
-                    precision=precision, riemann=riemann, kinds=kinds, w_fix=w_fix)
+                    precision=precision, riemann=riemann, kinds=kinds, w_fix=w_fix, b_fix=b_fix)
 
 
 def rel_l1(a, b):
@@ -51,7 +51,7 @@ def test_initial_state_bit_exact(name):
 
 
 @pytest.mark.parametrize("name", ["shock_16", "ot_16", "ot_ragged", "shock_floor",
-                                  "shock_bc", "shock_fixd"])
+                                  "shock_bc", "shock_fixd", "ot_bc_out", "ot_bc_fre"])
 def test_fp64_step_matches_reference(name):
     meta, g = G.load(name)
     d = _dyn(meta)
@@ -72,6 +72,66 @@ def test_fp64_step_matches_reference(name):
             m = mask[..., c]
             e = rel_l1(own[..., c][:, m], g["bf1"][..., c][:, m])
             assert e <= TOL_FP64, "bf %d rel L1 %.3e" % (c, e)
+
+
+# Reflecting MHD sides put mirror-image states on the two sides of the wall
+# face, where HLLD's branch choices (contact speed sign, the f_tiny switches)
+# sit at their thresholds; rounding decides them.  Two builds of the oracle
+# that differ only in fused multiply-add already differ by up to 6e-2 relative
+# L1 (face B_z, 4 steps) on this fixture, so the device step -- which fuses --
+# is held to that spread, and to the invariants exactly.
+TOL_ILL_POSED = 1e-1
+
+
+def test_mhd_reflecting_sides():
+    meta, g = G.load("ot_bc_ref")
+    d = _dyn(meta)
+    d.init_problem("ot", meta["seed"])
+    div0, tot0 = d.diagnostics()
+    d.step(meta["steps"])
+    u, bf = d.get_state()
+    div1, tot1 = d.diagnostics()
+    assert abs(d.time()["t"] - meta["t"]) <= 1e-5 * meta["t"]
+    for k in range(5):
+        assert rel_l1(u[..., k], g["u1"][..., k]) <= TOL_ILL_POSED
+    n, mask = meta["n"], G.face_mask(meta["n"])
+    own = G.owned_bf(bf, n)
+    for c in range(3):
+        m = mask[..., c]
+        assert rel_l1(own[..., c][:, m], g["bf1"][..., c][:, m]) <= TOL_ILL_POSED
+    assert div1 <= 1e-12
+    assert abs(tot1[0] - tot0[0]) <= 1e-12 * abs(tot0[0])    # walls pass no mass
+
+
+def test_mhd_fixed_sides_against_oracle_and_reference():
+    """Fixed MHD sides: the reference's own result varies run to run, so the
+    device step is held to the oracle and to the reference fixture within that
+    spread.  Against the oracle the step stays at rounding level except where
+    an HLLD switch (f_tiny) at the wall face flips under the device's
+    rounding (seen from the first step on this fixture).  Vector fields are
+    measured against the scale of the whole vector (m_z and B_z start near
+    zero in this workload)."""
+    from oracle.kr_oracle import OracleMesh
+    meta, g = G.load("ot_bc_fix")
+    d = _dyn(meta)
+    d.init_problem("ot", meta["seed"])
+    d.step(meta["steps"])
+    u, bf = d.get_state()
+    kinds, w_fix, b_fix = G.boundary(meta)
+    o = OracleMesh(True, meta["nb"], meta["n"], meta["gamma"], kinds=kinds, w_fix=w_fix, b_fix=b_fix)
+    o.init_problem("ot", meta["seed"])
+    o.step(meta["steps"])
+    uo, bfo = o.get_state()
+    n, mask = meta["n"], G.face_mask(meta["n"])
+
+    def err(a, b, ks):
+        return max(np.abs(a[..., k] - b[..., k]).sum() for k in ks) / max(np.abs(b[..., k]).sum() for k in ks)
+    for ks in ((0,), (1,), (2, 3, 4)):
+        assert err(u, uo, ks) <= 1e-4, ks
+        assert err(u, g["u1"], ks) <= G.SPREAD_CASES["ot_bc_fix"], ks
+    own, owo = G.owned_bf(bf, n) * mask, G.owned_bf(bfo, n) * mask
+    assert err(own, owo, (0, 1, 2)) <= 1e-3         # measured 3.7e-4: the flip sits at the wall
+    assert err(own, g["bf1"] * mask, (0, 1, 2)) <= G.SPREAD_CASES["ot_bc_fix"]
 
 
 @pytest.mark.parametrize("name", ["shock_c1", "ot_64"])

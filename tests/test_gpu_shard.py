@@ -55,10 +55,13 @@ def _assemble(shards, ref):
     (True, (2, 2, 2), 8, ("per",) * 6),          # every block alone on its rank
     (False, (4, 2, 2), 4, SHOCK_BC),
     (False, (3, 2, 1), 2, ("fixd", "out", "ref", "ref", "per", "per")),
+    (True, (2, 2, 2), 4, ("out", "fre", "per", "per", "ref", "fixd")),
 ])
 def test_group_step_equals_unsharded(mhd, nb, ranks, kinds, precision):
     n = (8, 8, 8)
     extra = {"w_fix": (1.0, 1.0, 0.5, 0.0, 0.0)} if "fixd" in kinds else {}
+    if "fixd" in kinds and mhd:
+        extra["b_fix"] = (0.1, 0.05, 0.2)
     ref, shards = _pair(mhd, nb, n, 3, "ot" if mhd else "shock", 5, ranks, precision, kinds, **extra)
     u_ref, bf_ref = ref.get_state()
     u, bf = _assemble(shards, ref)
