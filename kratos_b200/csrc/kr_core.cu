@@ -641,8 +641,17 @@ void solve_store( const args_t< R > & a, int b, int axis, const int * ii, bool v
 // One thread per face.  lines == 0: every face of the sweep (the MHD transverse
 // ghost lines included, mhd/integrator/integrator.h:138-168); lines != 0: only
 // those ghost lines (the tiled kernel below does the rest).
+// Resident CTAs per SM the per-face sweep is compiled for: register budgets
+// that ptxas meets without spilling (FP32 default / HLLE: 64 registers, 8 CTAs;
+// learned: 6; FP64: 4).
+template< class R, int MODE > constexpr int flux_min_ctas(  )
+{
+    return sizeof( R ) == 4 ? ( MODE <= KR_RIEMANN_HLLE ? 8 : ( MODE == KR_RIEMANN_LEARNED ? 6 : 4 ) )
+                            : ( MODE == KR_RIEMANN_HLLE ? 5 : 4 );
+}
+
 template< bool MHD, class R, int MODE >
-__global__ void __launch_bounds__( 128, 4 ) k_flux( const args_t< R > a, int axis, int step, int lines )
+__global__ void __launch_bounds__( 128, ( flux_min_ctas< R, MODE >(  ) ) ) k_flux( const args_t< R > a, int axis, int step, int lines )
 {
     constexpr int NW = MHD ? 11 : 5;   // stored W words: prim (8) + cell E (3)
     constexpr int NP = MHD ? 8 : 5;    // primitive words reconstructed
