@@ -937,47 +937,61 @@ __global__ void __launch_bounds__( 256 ) k_update( const args_t< R > a, int step
     const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
     const double dt = __longlong_as_double( a.s->dt_bits ) * ( step == 0 ? 1.0 : double( 0.5f ) );
     const geo_t & g = a.geo[ b ];
+    // The arrays never overlap: restrict lets the loads of later components
+    // issue ahead of the stores of earlier ones.
+    const R * __restrict__ F[ 3 ] = { a.f[ 0 ], a.f[ 1 ], a.f[ 2 ] };
+    const R * __restrict__ EE = a.ee;
     if( i[ 0 ] < nn[ 0 ] && i[ 1 ] < nn[ 1 ] && i[ 2 ] < nn[ 2 ] )
     {
-        const double * us = a.u[ step ];
-        double * ut = a.u[ 1 - step ];
+        const double * __restrict__ us = a.u[ step ];
+        double * __restrict__ ut = a.u[ 1 - step ];
         const double dt_dv = dt / g.vol;
+        // all loads first (30 flux words, 5 or 10 state words), then the sums
+        R fl[ 3 ][ 5 ], fr[ 3 ][ 5 ];
+        for( int d = 0; d < 3; ++ d )
+        {
+            const long long o = ifx( a, b, 0, NF, i[ 0 ], i[ 1 ], i[ 2 ] );
+            const long long s1 = d == 0 ? 1 : ( d == 1 ? a.sf1 : a.sf2 );
+            for( int k = 0; k < 5; ++ k )
+            {
+                fl[ d ][ k ] = F[ d ][ o + k * a.nfb ];
+                fr[ d ][ k ] = F[ d ][ o + k * a.nfb + s1 ];
+            }
+        }
+        const long long c0 = iuc( a, b, 0, i[ 0 ], i[ 1 ], i[ 2 ] );
+        double v[ 5 ];
+        for( int k = 0; k < 5; ++ k )
+            v[ k ] = step == 0 ? us[ c0 + k * a.nc ] : ( us[ c0 + k * a.nc ] + ut[ c0 + k * a.nc ] ) * 0.5f;
         for( int k = 0; k < 5; ++ k )
         {
-            const long long c = iuc( a, b, k, i[ 0 ], i[ 1 ], i[ 2 ] );
-            double v = step == 0 ? us[ c ] : ( us[ c ] + ut[ c ] ) * 0.5f;
             for( int d = 0; d < 3; ++ d )
             {
                 const double f_a = g.sfc[ d ] * dt_dv;
-                int j[ 3 ] = { i[ 0 ], i[ 1 ], i[ 2 ] };
-                const double fl = double( a.f[ d ][ ifx( a, b, k, NF, j[ 0 ], j[ 1 ], j[ 2 ] ) ] );
-                ++ j[ d ];
-                const double fr = double( a.f[ d ][ ifx( a, b, k, NF, j[ 0 ], j[ 1 ], j[ 2 ] ) ] );
                 double res = 0;
-                res += f_a * fl;
-                res -= f_a * fr;
-                v += res;
+                res += f_a * double( fl[ d ][ k ] );
+                res -= f_a * double( fr[ d ][ k ] );
+                v[ k ] += res;
             }
-            ut[ c ] = v;
+            ut[ c0 + k * a.nc ] = v[ k ];
         }
     }
     if( ! MHD )
         return;
-    const double * bs = a.bf[ step ];
-    double * bt = a.bf[ 1 - step ];
+    const double * __restrict__ bs = a.bf[ step ];
+    double * __restrict__ bt = a.bf[ 1 - step ];
     for( int c = 0; c < 3; ++ c )
     {
         const int ax1 = mod3( c + 1 ), ax2 = mod3( c + 2 );
         if( i[ ax1 ] >= nn[ ax1 ] || i[ ax2 ] >= nn[ ax2 ] )
             continue;
         double db;
-        db  = double( a.ee[ ifx( a, b, ax1, 3, i[ 0 ], i[ 1 ], i[ 2 ] ) ] ) * g.dx[ ax1 ];
-        db -= double( a.ee[ ifx( a, b, ax2, 3, i[ 0 ], i[ 1 ], i[ 2 ] ) ] ) * g.dx[ ax2 ];
+        db  = double( EE[ ifx( a, b, ax1, 3, i[ 0 ], i[ 1 ], i[ 2 ] ) ] ) * g.dx[ ax1 ];
+        db -= double( EE[ ifx( a, b, ax2, 3, i[ 0 ], i[ 1 ], i[ 2 ] ) ] ) * g.dx[ ax2 ];
         ++ i[ ax1 ];
-        db += double( a.ee[ ifx( a, b, ax2, 3, i[ 0 ], i[ 1 ], i[ 2 ] ) ] ) * g.dx[ ax2 ];
+        db += double( EE[ ifx( a, b, ax2, 3, i[ 0 ], i[ 1 ], i[ 2 ] ) ] ) * g.dx[ ax2 ];
         -- i[ ax1 ];
         ++ i[ ax2 ];
-        db -= double( a.ee[ ifx( a, b, ax1, 3, i[ 0 ], i[ 1 ], i[ 2 ] ) ] ) * g.dx[ ax1 ];
+        db -= double( EE[ ifx( a, b, ax1, 3, i[ 0 ], i[ 1 ], i[ 2 ] ) ] ) * g.dx[ ax1 ];
         -- i[ ax2 ];
         const double sfc = g.sfc[ c ];
         db *= ( sfc > 0 ? ( -dt / sfc ) : 0. );
