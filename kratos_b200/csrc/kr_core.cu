@@ -111,6 +111,16 @@ long long ifx( const args_t< R > & a, int b, int c, int nf, int i0, int i1, int 
     return ( long long )( b * nf + c ) * a.nfb + ( i0 + 1 ) + a.sf1 * ( i1 + 1 ) + a.sf2 * ( i2 + 1 );
 }
 
+// Quotient of a non-negative n by a fixed d >= 2 with one multiply-high:
+// q = umulhi( n, ceil( 2^32 / d ) ), exact while n * d < 2^32 (the rounding
+// error of the multiplier, below d, times n stays under 2^32).
+struct udiv_t { unsigned d, m; };
+static inline udiv_t make_udiv( unsigned d )
+{
+    return { d, unsigned( ( ( 1ull << 32 ) + d - 1 ) / d ) };
+}
+__device__ __forceinline__ unsigned udiv_q( unsigned n, const udiv_t & v ) { return __umulhi( n, v.m ); }
+
 __device__ __forceinline__ double warp_min( double v )
 {
     for( int o = 16; o > 0; o >>= 1 )
@@ -142,17 +152,19 @@ __global__ void k_step_end( scal_t * s, double dt_expand )
 // (hydro/eos/adiabatic.h:211-258; mhd/eos/adiabatic.h:127-234).
 
 template< bool MHD, class R >
-__global__ void __launch_bounds__( 256 ) k_c2p( const args_t< R > a, int step )
+__global__ void __launch_bounds__( 256 ) k_c2p( const args_t< R > a, int step, udiv_t dv )
 {
+    // grid: x over the cells of one (x, y) plane, y over z, z over blocks
     constexpr int NW = MHD ? 11 : 5;   // stored W words: prim (8) + cell E (3)
-    const int b = blockIdx.y;
-    const long long c = ( long long ) blockIdx.x * blockDim.x + threadIdx.x;
+    const int b = blockIdx.z;
+    const unsigned c = blockIdx.x * blockDim.x + threadIdx.x;
     double dt = FLT_MAX;
-    if( c < a.nc )
+    if( c < unsigned( a.n0 * a.n1 ) )
     {
-        const int i0 = int( c % a.n0 );
-        const int i1 = int( ( c / a.n0 ) % a.n1 );
-        const int i2 = int( c / ( ( long long ) a.n0 * a.n1 ) );
+        const unsigned q = udiv_q( c, dv );
+        const int i0 = int( c - q * unsigned( a.n0 ) );
+        const int i1 = int( q );
+        const int i2 = int( blockIdx.y );
         double * U = a.u[ step ];
         double cons[ 5 ], cout[ 5 ], prim[ 5 ];
         for( int k = 0; k < 5; ++ k )
@@ -628,13 +640,16 @@ void solve_store( const args_t< R > & a, int b, int axis, const int * ii, bool v
         }
     }
     idx_swap( flx + MOM, 3 - axis );
-    R * F = a.f[ axis ];
+    // block base once in 64 bits, offsets inside the block in 32
+    R * F = a.f[ axis ] + ( size_t ) b * NF * a.nfb;
+    const int off = ( ii[ 0 ] + 1 ) + a.sf1 * ( ii[ 1 ] + 1 ) + a.sf2 * ( ii[ 2 ] + 1 );
+    const int nfb = int( a.nfb );
     for( int k = 0; k < 5; ++ k )
-        F[ ifx( a, b, k, NF, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] = flx[ k ];
+        F[ k * nfb + off ] = flx[ k ];
     if( MHD )
     {
-        F[ ifx( a, b, 5, NF, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] =  flx[ BCC + 2 ];
-        F[ ifx( a, b, 6, NF, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] = -flx[ BCC + 1 ];
+        F[ 5 * nfb + off ] =  flx[ BCC + 2 ];
+        F[ 6 * nfb + off ] = -flx[ BCC + 1 ];
     }
 }
 
@@ -651,27 +666,32 @@ template< class R, int MODE > constexpr int flux_min_ctas(  )
 }
 
 template< bool MHD, class R, int MODE >
-__global__ void __launch_bounds__( 128, ( flux_min_ctas< R, MODE >(  ) ) ) k_flux( const args_t< R > a, int axis, int step, int lines )
+__global__ void __launch_bounds__( 128, ( flux_min_ctas< R, MODE >(  ) ) ) k_flux( const args_t< R > a, int axis, int step, int lines, udiv_t dv )
 {
     constexpr int NW = MHD ? 11 : 5;   // stored W words: prim (8) + cell E (3)
     constexpr int NP = MHD ? 8 : 5;    // primitive words reconstructed
     constexpr bool learned = MHD && MODE == KR_RIEMANN_LEARNED;
-    const int b = blockIdx.y;
+    // grid: x over the faces of one (x, y) plane (lines: over all line
+    // faces), y over z planes, z over blocks; dv divides by the row length
+    const int b = blockIdx.z;
     const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
-    const long long t = ( long long ) blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
     int ii[ 3 ];
     int outside = 0;
-    long long total;
+    unsigned total;
+    long long t_lin;                  // face number within the sweep (sampling keys)
     if( ! lines )
     {
         const int lo = MHD ? -1 : 0;
         int ext[ 3 ];
         for( int d = 0; d < 3; ++ d )
             ext[ d ] = d == axis ? nn[ d ] + 1 : nn[ d ] - 2 * lo;
-        total = ( long long ) ext[ 0 ] * ext[ 1 ] * ext[ 2 ];
-        ii[ 0 ] = int( t % ext[ 0 ] );
-        ii[ 1 ] = int( ( t / ext[ 0 ] ) % ext[ 1 ] );
-        ii[ 2 ] = int( t / ( ( long long ) ext[ 0 ] * ext[ 1 ] ) );
+        total = unsigned( ext[ 0 ] * ext[ 1 ] );
+        const unsigned q = udiv_q( t, dv );
+        ii[ 0 ] = int( t - q * unsigned( ext[ 0 ] ) );
+        ii[ 1 ] = int( q );
+        ii[ 2 ] = int( blockIdx.y );
+        t_lin = ( long long ) t + ( long long ) total * blockIdx.y;
         for( int d = 0; d < 3; ++ d )
             if( d != axis )
             {
@@ -683,9 +703,11 @@ __global__ void __launch_bounds__( 128, ( flux_min_ctas< R, MODE >(  ) ) ) k_flu
     {
         const int a1 = mod3( axis + 1 ), a2 = mod3( axis + 2 );
         const int nf = nn[ axis ] + 1;
-        total = ( long long ) nf * ( 2LL * nn[ a2 ] + 2LL * nn[ a1 ] );
-        ii[ axis ] = int( t % nf );
-        long long l = t / nf;
+        total = unsigned( nf * ( 2 * nn[ a2 ] + 2 * nn[ a1 ] ) );
+        const unsigned q = udiv_q( t, dv );
+        ii[ axis ] = int( t - q * unsigned( nf ) );
+        long long l = q;
+        t_lin = t;
         if( l < 2LL * nn[ a2 ] )
         {
             ii[ a1 ] = ( l & 1 ) ? nn[ a1 ] : -1;
@@ -707,6 +729,10 @@ __global__ void __launch_bounds__( 128, ( flux_min_ctas< R, MODE >(  ) ) ) k_flu
     const int st = axis == 0 ? 1 : ( axis == 1 ? a.sw1 : a.sw2 );
     R ql[ 8 ], qr[ 8 ];
     if( valid )
+    {
+        const R * wb = a.w + ( size_t ) b * NW * a.ngw
+                     + ( ( ii[ 0 ] + 2 ) + a.sw1 * ( ii[ 1 ] + 2 ) + a.sw2 * ( ii[ 2 ] + 2 ) );
+        const int ngw = int( a.ngw );
         for( int k = 0; k < NP; ++ k )
         {
             if( MHD && k == BCC + axis )
@@ -715,11 +741,12 @@ __global__ void __launch_bounds__( 128, ( flux_min_ctas< R, MODE >(  ) ) ) k_flu
                 ql[ k ] = qr[ k ] = bn;
                 continue;
             }
-            const R * p = a.w + iw( a, b, k, NW, ii[ 0 ], ii[ 1 ], ii[ 2 ] );
+            const R * p = wb + k * ngw;
             plm_face_fast< R >( p[ -2 * st ], p[ -st ], p[ 0 ], p[ st ], ql[ k ], qr[ k ] );
         }
+    }
     const unsigned long long key = ( ( unsigned long long ) b * 3 + axis ) * 0x9E3779B97F4A7C15ull
-                                 + ( unsigned long long ) ( lines ? t + ( 1ll << 40 ) : t );
+                                 + ( unsigned long long ) ( lines ? t_lin + ( 1ll << 40 ) : t_lin );
     solve_store< MHD, R, MODE >( a, b, axis, ii, valid, ql, qr, threadIdx.x >> 5, key );
 }
 
@@ -843,14 +870,16 @@ R face_emf( const args_t< R > & a, int b, int fa, int ax, const int * i )
 }
 
 template< class R >
-__global__ void __launch_bounds__( 256 ) k_emf( const args_t< R > a )
+__global__ void __launch_bounds__( 256 ) k_emf( const args_t< R > a, udiv_t dv )
 {
-    const int b = blockIdx.y;
+    // grid: x over the edges of one (x, y) plane, y over z, z over blocks
+    const int b = blockIdx.z;
     const int e0 = a.n0 + 1, e1 = a.n1 + 1;
-    const long long t = ( long long ) blockIdx.x * blockDim.x + threadIdx.x;
-    if( t >= ( long long ) e0 * e1 * ( a.n2 + 1 ) )
+    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+    if( t >= unsigned( e0 * e1 ) )
         return;
-    int i[ 3 ] = { int( t % e0 ), int( ( t / e0 ) % e1 ), int( t / ( ( long long ) e0 * e1 ) ) };
+    const unsigned q = udiv_q( t, dv );
+    int i[ 3 ] = { int( t - q * unsigned( e0 ) ), int( q ), int( blockIdx.y ) };
     const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
     const R w_e = R( 0.25f );
     for( int ax = 0; ax < 3; ++ ax )
@@ -925,15 +954,17 @@ __global__ void __launch_bounds__( 256 ) k_emf( const args_t< R > a )
 // mhd/integrator/rk2.h:244-258 set_field).  One thread per lattice site.
 
 template< bool MHD, class R >
-__global__ void __launch_bounds__( 256 ) k_update( const args_t< R > a, int step )
+__global__ void __launch_bounds__( 256 ) k_update( const args_t< R > a, int step, udiv_t dv )
 {
+    // grid: x over the lattice sites of one (x, y) plane, y over z, z over blocks
     constexpr int NF = MHD ? 7 : 5;
-    const int b = blockIdx.y;
+    const int b = blockIdx.z;
     const int e0 = a.n0 + 1, e1 = a.n1 + 1;
-    const long long t = ( long long ) blockIdx.x * blockDim.x + threadIdx.x;
-    if( t >= ( long long ) e0 * e1 * ( a.n2 + 1 ) )
+    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+    if( t >= unsigned( e0 * e1 ) )
         return;
-    int i[ 3 ] = { int( t % e0 ), int( ( t / e0 ) % e1 ), int( t / ( ( long long ) e0 * e1 ) ) };
+    const unsigned q = udiv_q( t, dv );
+    int i[ 3 ] = { int( t - q * unsigned( e0 ) ), int( q ), int( blockIdx.y ) };
     const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
     const double dt = __longlong_as_double( a.s->dt_bits ) * ( step == 0 ? 1.0 : double( 0.5f ) );
     const geo_t & g = a.geo[ b ];
@@ -946,34 +977,49 @@ __global__ void __launch_bounds__( 256 ) k_update( const args_t< R > a, int step
         const double * __restrict__ us = a.u[ step ];
         double * __restrict__ ut = a.u[ 1 - step ];
         const double dt_dv = dt / g.vol;
-        // all loads first (30 flux words, 5 or 10 state words), then the sums
-        R fl[ 3 ][ 5 ], fr[ 3 ][ 5 ];
-        for( int d = 0; d < 3; ++ d )
-        {
-            const long long o = ifx( a, b, 0, NF, i[ 0 ], i[ 1 ], i[ 2 ] );
-            const long long s1 = d == 0 ? 1 : ( d == 1 ? a.sf1 : a.sf2 );
+        const long long o = ifx( a, b, 0, NF, i[ 0 ], i[ 1 ], i[ 2 ] );
+        const long long c0 = iuc( a, b, 0, i[ 0 ], i[ 1 ], i[ 2 ] );
+        const long long s1[ 3 ] = { 1, a.sf1, a.sf2 };
+        if constexpr( sizeof( R ) == 4 )
+        {   // all loads first (30 flux words, 5 or 10 state words), then the sums
+            R fl[ 3 ][ 5 ], fr[ 3 ][ 5 ];
+            for( int d = 0; d < 3; ++ d )
+                for( int k = 0; k < 5; ++ k )
+                {
+                    fl[ d ][ k ] = F[ d ][ o + k * a.nfb ];
+                    fr[ d ][ k ] = F[ d ][ o + k * a.nfb + s1[ d ] ];
+                }
+            double v[ 5 ];
+            for( int k = 0; k < 5; ++ k )
+                v[ k ] = step == 0 ? us[ c0 + k * a.nc ] : ( us[ c0 + k * a.nc ] + ut[ c0 + k * a.nc ] ) * 0.5f;
             for( int k = 0; k < 5; ++ k )
             {
-                fl[ d ][ k ] = F[ d ][ o + k * a.nfb ];
-                fr[ d ][ k ] = F[ d ][ o + k * a.nfb + s1 ];
+                for( int d = 0; d < 3; ++ d )
+                {
+                    const double f_a = g.sfc[ d ] * dt_dv;
+                    double res = 0;
+                    res += f_a * double( fl[ d ][ k ] );
+                    res -= f_a * double( fr[ d ][ k ] );
+                    v[ k ] += res;
+                }
+                ut[ c0 + k * a.nc ] = v[ k ];
             }
         }
-        const long long c0 = iuc( a, b, 0, i[ 0 ], i[ 1 ], i[ 2 ] );
-        double v[ 5 ];
-        for( int k = 0; k < 5; ++ k )
-            v[ k ] = step == 0 ? us[ c0 + k * a.nc ] : ( us[ c0 + k * a.nc ] + ut[ c0 + k * a.nc ] ) * 0.5f;
-        for( int k = 0; k < 5; ++ k )
-        {
-            for( int d = 0; d < 3; ++ d )
-            {
-                const double f_a = g.sfc[ d ] * dt_dv;
-                double res = 0;
-                res += f_a * double( fl[ d ][ k ] );
-                res -= f_a * double( fr[ d ][ k ] );
-                v[ k ] += res;
+        else
+            for( int k = 0; k < 5; ++ k )
+            {   // FP64 fluxes: one component at a time keeps the registers low
+                const long long c = c0 + k * a.nc;
+                double v = step == 0 ? us[ c ] : ( us[ c ] + ut[ c ] ) * 0.5f;
+                for( int d = 0; d < 3; ++ d )
+                {
+                    const double f_a = g.sfc[ d ] * dt_dv;
+                    double res = 0;
+                    res += f_a * double( F[ d ][ o + k * a.nfb ] );
+                    res -= f_a * double( F[ d ][ o + k * a.nfb + s1[ d ] ] );
+                    v += res;
+                }
+                ut[ c ] = v;
             }
-            ut[ c0 + k * a.nc ] = v[ k ];
-        }
     }
     if( ! MHD )
         return;
@@ -1539,10 +1585,11 @@ static void launch_flux( kr_ctx * c, cudaStream_t st, const args_t< R > & a, int
     const flux_tiling t = tiling_for< R >( c, axis, NP );
     if( ! t.ok || c->no_tiles )
     {
-        long long nface = 1;
+        int ext[ 3 ];
         for( int d = 0; d < 3; ++ d )
-            nface *= ( d == axis ) ? n[ d ] + 1 : n[ d ] + ( MHD ? 2 : 0 );
-        k_flux< MHD, R, MODE ><<< dim3( blocks_for( nface, 128 ), c->nblk ), 128, 0, st >>>( a, axis, stage, 0 );
+            ext[ d ] = ( d == axis ) ? n[ d ] + 1 : n[ d ] + ( MHD ? 2 : 0 );
+        k_flux< MHD, R, MODE ><<< dim3( blocks_for( ( long long ) ext[ 0 ] * ext[ 1 ], 128 ), ext[ 2 ], c->nblk ), 128, 0, st >>>(
+            a, axis, stage, 0, make_udiv( unsigned( ext[ 0 ] ) ) );
         return;
     }
     if( axis == 0 )      launch_tile< MHD, R, MODE, 0 >( c, st, a, stage, t );
@@ -1552,7 +1599,8 @@ static void launch_flux( kr_ctx * c, cudaStream_t st, const args_t< R > & a, int
     {
         const int a1 = ( axis + 1 ) % 3, a2 = ( axis + 2 ) % 3;
         const long long nline = ( long long )( n[ axis ] + 1 ) * ( 2LL * n[ a1 ] + 2LL * n[ a2 ] );
-        k_flux< MHD, R, MODE ><<< dim3( blocks_for( nline, 128 ), c->nblk ), 128, 0, st >>>( a, axis, stage, 1 );
+        k_flux< MHD, R, MODE ><<< dim3( blocks_for( nline, 128 ), 1, c->nblk ), 128, 0, st >>>(
+            a, axis, stage, 1, make_udiv( unsigned( n[ axis ] + 1 ) ) );
     }
 }
 
@@ -1577,7 +1625,9 @@ template< bool MHD, class R, class T >
 static void enqueue_front( kr_ctx * c, cudaStream_t st, const args_t< R > & a, int stage, T && timed )
 {
     const unsigned nb = unsigned( c->nblk );
-    timed( 0, [ & ] { k_c2p< MHD, R ><<< dim3( blocks_for( c->nc, 256 ), nb ), 256, 0, st >>>( a, stage ); } );
+    const int * n = c->cfg.n;
+    timed( 0, [ & ] { k_c2p< MHD, R ><<< dim3( blocks_for( ( long long ) n[ 0 ] * n[ 1 ], 256 ), n[ 2 ], nb ), 256, 0, st >>>(
+        a, stage, make_udiv( unsigned( n[ 0 ] ) ) ); } );
     if( ! c->hsend.items.empty(  ) )
         timed( 1, [ & ] {
             k_halo< MHD, R, true ><<< dim3( c->halo_grid, unsigned( c->hsend.items.size(  ) ) ), 256, 0, st >>>(
@@ -1610,8 +1660,9 @@ static void enqueue_back( kr_ctx * c, cudaStream_t st, const args_t< R > & a, in
     for( int axis = 2; axis >= 0; -- axis )
         timed( 4 - axis, [ & ] { launch_flux_mode< MHD, R >( c, st, a, axis, stage, mode ); } );
     if( MHD )
-        timed( 5, [ & ] { k_emf< R ><<< dim3( blocks_for( nlat, 256 ), nb ), 256, 0, st >>>( a ); } );
-    timed( 6, [ & ] { k_update< MHD, R ><<< dim3( blocks_for( nlat, 256 ), nb ), 256, 0, st >>>( a, stage ); } );
+        timed( 5, [ & ] { k_emf< R ><<< dim3( blocks_for( ( long long )( n[ 0 ] + 1 ) * ( n[ 1 ] + 1 ), 256 ), n[ 2 ] + 1, nb ), 256, 0, st >>>(
+            a, make_udiv( unsigned( n[ 0 ] + 1 ) ) ); } );
+    timed( 6, [ & ] { k_update< MHD, R ><<< dim3( blocks_for( ( long long )( n[ 0 ] + 1 ) * ( n[ 1 ] + 1 ), 256 ), n[ 2 ] + 1, nb ), 256, 0, st >>>( a, stage, make_udiv( unsigned( n[ 0 ] + 1 ) ) ); } );
 }
 
 // Halo transfer of one stage between this rank and its peers, and at stage 0
