@@ -188,7 +188,8 @@ def reference_arm(args, rank, world):
 
 # --------------------------------------------------------------------------- GPU
 MODES = {"fp64": dict(precision=2, riemann=0), "mixed": dict(precision=1, riemann=0),
-         "hlle_mixed": dict(precision=1, riemann=1), "learned": dict(precision=1, riemann=2)}
+         "hlle_mixed": dict(precision=1, riemann=1), "learned": dict(precision=1, riemann=2, sel_period=4),
+         "learned_p1": dict(precision=1, riemann=2, sel_period=1)}
 
 
 def train_selector(local_rank):
@@ -236,7 +237,7 @@ def time_mode(mode, args, local_rank, world, dist):
     else:
         d = Dynamics(True, NB, N, gamma=GAMMA, device=local_rank, **MODES[mode])
     sel_info = None
-    if mode == "learned":
+    if mode.startswith("learned"):
         # one selector for every rank: faces shared by two blocks must get the
         # same solver on both sides
         got = [None]

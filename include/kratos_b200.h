@@ -41,7 +41,7 @@
 extern "C" {
 #endif
 
-#define KR_ABI_VERSION 4
+#define KR_ABI_VERSION 5
 
 /* [boundary] kinds per side (hydro/boundary/phys_functors.h:11-91): an axis is
  * periodic only when both its sides are KR_BC_PER. */
@@ -85,7 +85,10 @@ typedef struct
     int    flags;              /* KR_FLAG_* bits                                 */
     int    n_ranks;            /* ranks sharing the mesh (0 or 1: not sharded)   */
     int    rank;               /* this context's rank, 0 <= rank < n_ranks       */
-    int    reserved[ 4 ];
+    int    sel_period;         /* learned mode: the network runs at stage 0 of   */
+                               /* every sel_period-th step; the other stages    */
+                               /* reuse its per-face choices (0 or 1: every step)*/
+    int    reserved[ 3 ];
 } kr_cfg;
 
 /* kr_cfg.flags */

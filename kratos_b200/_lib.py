@@ -5,7 +5,7 @@ import os
 _PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_PKG, "libkrb200.so")
 
-KR_ABI_VERSION = 4
+KR_ABI_VERSION = 5
 KR_FLAG_TILED, KR_FLAG_HALO_ALL = 1, 2
 BC_KINDS = {"per": 0, "out": 1, "ref": 2, "fre": 3, "fixd": 4}
 KR_RIEMANN_DEFAULT, KR_RIEMANN_HLLE, KR_RIEMANN_LEARNED = 0, 1, 2
@@ -34,7 +34,8 @@ class kr_cfg(ctypes.Structure):
         ("flags", ctypes.c_int),
         ("n_ranks", ctypes.c_int),
         ("rank", ctypes.c_int),
-        ("reserved", ctypes.c_int * 4),
+        ("sel_period", ctypes.c_int),
+        ("reserved", ctypes.c_int * 3),
     ]
 
 

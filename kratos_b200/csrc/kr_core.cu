@@ -74,6 +74,9 @@ struct args_t
     const float * sel_b;              // b1, b2, b3
     float sel_thr;                    // logit threshold for HLLE
     unsigned long long * sel_cnt;     // [0] faces, [1] faces given HLLE
+    unsigned * sel_mask;              // per-warp choice words, reused between evaluations
+    long long sel_stride;             // words per (axis, block, lines) region
+    int sel_period;                   // steps between evaluations of the network
     // face sampling for selector training (collect steps only)
     float * smp;                      // [max][17]: 16 features + flux gap
     unsigned long long * smp_n;
@@ -558,9 +561,8 @@ constexpr int FLUX_SAMPLE = 3;
 
 // Riemann solve of one face from its reconstructed states and store of the
 // flux (and, for MHD, the two edge EMFs: hlld.h:42-46 -- slot 5 holds
-// E_{(axis+1)%3}, slot 6 E_{(axis+2)%3}).  Every lane of the warp must call it
-// in the learned mode (the selector is warp-collective); invalid lanes only
-// take part in that.
+// E_{(axis+1)%3}, slot 6 E_{(axis+2)%3}).  (The learned mode goes through
+// learned_solve below.)
 template< bool MHD, class R, int MODE > __device__ __forceinline__
 void solve_store( const args_t< R > & a, int b, int axis, const int * ii, bool valid,
                   R * ql, R * qr, int warp, unsigned long long key )
@@ -568,7 +570,6 @@ void solve_store( const args_t< R > & a, int b, int axis, const int * ii, bool v
     constexpr bool SAMPLE = MODE == FLUX_SAMPLE;
     constexpr int rsel = MODE == FLUX_SAMPLE ? KR_RIEMANN_DEFAULT : MODE;
     constexpr int NF = MHD ? 7 : 5;
-    constexpr bool learned = MHD && rsel == KR_RIEMANN_LEARNED;
     R flx[ 8 ];
     const eos_c< R > e = { R( a.gamma ), R( a.gm1 ), R( a.cv ) };
     if( ! valid )
@@ -585,40 +586,11 @@ void solve_store( const args_t< R > & a, int b, int axis, const int * ii, bool v
     {
         idx_swap( ql + BCC, axis );
         idx_swap( qr + BCC, axis );
-        if constexpr( learned )
-        {
-            __shared__ __nv_bfloat16 xs[ 8 ][ 32 * MLP_IN ];
-            float f[ MLP_IN ];
-            face_features< R >( ql, qr, e.gamma, f );
-            const float z = mlp_logit( f, a.sel_w, a.sel_b, xs[ warp ] );
-            // Per-face choice: HLLE where the network predicts the face safe,
-            // HLLD for every flagged face.  (A warp-uniform choice -- HLLE only
-            // when all 32 faces of a warp are safe -- avoids running both
-            // solvers in one warp but left HLLE on under 1% of the faces of
-            // the 64^3 OT run, so it is not used.)
-            const bool cheap = valid && z > a.sel_thr;
-            const unsigned vmask = __ballot_sync( 0xffffffffu, valid );
-            const unsigned cmask = __ballot_sync( 0xffffffffu, cheap );
-            if( ( threadIdx.x & 31 ) == 0 && vmask )
-            {
-                atomicAdd( a.sel_cnt, ( unsigned long long ) __popc( vmask ) );
-                atomicAdd( a.sel_cnt + 1, ( unsigned long long ) __popc( cmask ) );
-            }
-            if( ! valid )
-                return;
-            if( cheap )
-                hlle_fast< R >( flx, ql, qr, e );
-            else
-                hlld_fast< R >( flx, ql, qr, e );
-        }
+        if( ! valid ) return;
+        if( rsel == KR_RIEMANN_HLLE )
+            hlle_fast< R >( flx, ql, qr, e );
         else
-        {
-            if( ! valid ) return;
-            if( rsel == KR_RIEMANN_HLLE )
-                hlle_fast< R >( flx, ql, qr, e );
-            else
-                hlld_fast< R >( flx, ql, qr, e );
-        }
+            hlld_fast< R >( flx, ql, qr, e );
         if constexpr( SAMPLE )
         {   // training sample: features, and the HLLE-HLLD gap of this face
             key = ( key + a.smp_seed ) * 0xBF58476D1CE4E5B9ull;
@@ -656,6 +628,91 @@ void solve_store( const args_t< R > & a, int b, int axis, const int * ii, bool v
 // One thread per face.  lines == 0: every face of the sweep (the MHD transverse
 // ghost lines included, mhd/integrator/integrator.h:138-168); lines != 0: only
 // those ghost lines (the tiled kernel below does the rest).
+// Learned mode (no reference counterpart).  The network runs at stage 0 of
+// every sel_period-th step; its per-face choices are kept as one ballot word
+// per warp and reused by the other stages and steps.  The CTA then sorts its
+// 128 faces into one run of HLLD faces and one run of HLLE faces (through
+// shared memory, original order kept within each run), so that each warp
+// executes one solver -- a per-face choice inside a warp would make the warp
+// pay for both.
+template< bool MHD, class R > __device__ __forceinline__
+void learned_solve( const args_t< R > & a, int b, int axis, const int * ii, bool valid,
+                    R * ql, R * qr, int step, long long word )
+{
+    constexpr int NF = 7;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const eos_c< R > e = { R( a.gamma ), R( a.gm1 ), R( a.cv ) };
+    if( ! valid )
+        for( int k = 0; k < 8; ++ k )
+            ql[ k ] = qr[ k ] = ( k == RHO || k == ENE ) ? R( 1 ) : R( 0 );
+    idx_swap( ql + MOM, axis ); idx_swap( qr + MOM, axis );
+    idx_swap( ql + BCC, axis ); idx_swap( qr + BCC, axis );
+    __shared__ __nv_bfloat16 xs[ 4 ][ 32 * MLP_IN ];
+    __shared__ R sq[ 128 ][ 17 ];                // rotated left / right states (+1 pad)
+    __shared__ int sid[ 128 ];                   // face position, packed
+    __shared__ int cnt[ 4 ][ 2 ];
+    bool cheap;
+    if( step == 0 && a.s->n_steps % a.sel_period == 0 )
+    {   // grid-uniform branch: every lane of the warp takes part in the MMAs
+        float f[ MLP_IN ];
+        face_features< R >( ql, qr, e.gamma, f );
+        const float z = mlp_logit( f, a.sel_w, a.sel_b, xs[ warp ] );
+        cheap = valid && z > a.sel_thr;
+        const unsigned m = __ballot_sync( 0xffffffffu, cheap );
+        if( lane == 0 )
+            a.sel_mask[ word ] = m;
+    }
+    else
+        cheap = valid && ( ( a.sel_mask[ word ] >> lane ) & 1u );
+    const unsigned mh = __ballot_sync( 0xffffffffu, valid && ! cheap );
+    const unsigned mc = __ballot_sync( 0xffffffffu, cheap );
+    if( lane == 0 )
+    {
+        cnt[ warp ][ 0 ] = __popc( mh );
+        cnt[ warp ][ 1 ] = __popc( mc );
+        if( mh | mc )
+        {
+            atomicAdd( a.sel_cnt, ( unsigned long long ) __popc( mh | mc ) );
+            atomicAdd( a.sel_cnt + 1, ( unsigned long long ) __popc( mc ) );
+        }
+    }
+    __syncthreads(  );
+    int nh = 0, nh_before = 0, nc_before = 0, nall = 0;
+    for( int w = 0; w < 4; ++ w )
+    {
+        nh += cnt[ w ][ 0 ];
+        nall += cnt[ w ][ 0 ] + cnt[ w ][ 1 ];
+        if( w < warp ) { nh_before += cnt[ w ][ 0 ]; nc_before += cnt[ w ][ 1 ]; }
+    }
+    const unsigned below = ( 1u << lane ) - 1u;
+    int slot = -1;
+    if( valid && ! cheap ) slot = nh_before + __popc( mh & below );
+    else if( cheap )       slot = nh + nc_before + __popc( mc & below );
+    if( slot >= 0 )
+    {
+        for( int k = 0; k < 8; ++ k ) { sq[ slot ][ k ] = ql[ k ]; sq[ slot ][ 8 + k ] = qr[ k ]; }
+        sid[ slot ] = ( ii[ 0 ] + 2 ) | ( ( ii[ 1 ] + 2 ) << 10 ) | ( ( ii[ 2 ] + 2 ) << 20 );
+    }
+    __syncthreads(  );
+    const int j = threadIdx.x;
+    if( j >= nall )
+        return;
+    R l[ 8 ], r[ 8 ], flx[ 8 ];
+    for( int k = 0; k < 8; ++ k ) { l[ k ] = sq[ j ][ k ]; r[ k ] = sq[ j ][ 8 + k ]; }
+    const int pk = sid[ j ];
+    const int f0 = ( pk & 1023 ) - 2, f1 = ( ( pk >> 10 ) & 1023 ) - 2, f2 = ( pk >> 20 ) - 2;
+    if( j < nh ) hlld_fast< R >( flx, l, r, e );
+    else         hlle_fast< R >( flx, l, r, e );
+    idx_swap( flx + MOM, 3 - axis );
+    R * F = a.f[ axis ] + ( size_t ) b * NF * a.nfb;
+    const int off = ( f0 + 1 ) + a.sf1 * ( f1 + 1 ) + a.sf2 * ( f2 + 1 );
+    const int nfb = int( a.nfb );
+    for( int k = 0; k < 5; ++ k )
+        F[ k * nfb + off ] = flx[ k ];
+    F[ 5 * nfb + off ] =  flx[ BCC + 2 ];
+    F[ 6 * nfb + off ] = -flx[ BCC + 1 ];
+}
+
 // Resident CTAs per SM the per-face sweep is compiled for: register budgets
 // that ptxas meets without spilling (FP32 default / HLLE: 64 registers, 8 CTAs;
 // learned: 6; FP64: 4).
@@ -744,6 +801,13 @@ __global__ void __launch_bounds__( 128, ( flux_min_ctas< R, MODE >(  ) ) ) k_flu
             const R * p = wb + k * ngw;
             plm_face_fast< R >( p[ -2 * st ], p[ -st ], p[ 0 ], p[ st ], ql[ k ], qr[ k ] );
         }
+    }
+    if constexpr( learned )
+    {   // the per-face kernel covers every face of the sweep here (lines == 0)
+        const long long word = ( ( long long ) axis * a.nblk + b ) * a.sel_stride
+                             + ( ( long long ) blockIdx.y * gridDim.x + blockIdx.x ) * 4 + ( threadIdx.x >> 5 );
+        learned_solve< MHD, R >( a, b, axis, ii, valid, ql, qr, step, word );
+        return;
     }
     const unsigned long long key = ( ( unsigned long long ) b * 3 + axis ) * 0x9E3779B97F4A7C15ull
                                  + ( unsigned long long ) ( lines ? t_lin + ( 1ll << 40 ) : t_lin );
@@ -1448,6 +1512,8 @@ struct kr_ctx
     unsigned long long * sel_cnt = nullptr;
     float sel_thr = 0.f;
     bool sel_ready = false;
+    unsigned * sel_mask = nullptr;     // learned mode: choice words of the last evaluation
+    long long sel_stride = 0;
     // selector training samples (only during kr_selector_collect)
     float * smp = nullptr;
     unsigned long long * smp_n = nullptr;
@@ -1518,6 +1584,8 @@ static args_t< R > make_args( kr_ctx * c )
         if( c->cfg.bc[ 2 * d + 1 ] == KR_BC_OUT || c->cfg.bc[ 2 * d + 1 ] == KR_BC_FRE )
             a.emf_out |= 1 << d;
     a.sel_w = c->sel_w; a.sel_b = c->sel_b; a.sel_thr = c->sel_thr; a.sel_cnt = c->sel_cnt;
+    a.sel_mask = c->sel_mask; a.sel_stride = c->sel_stride;
+    a.sel_period = c->cfg.sel_period > 1 ? c->cfg.sel_period : 1;
     a.smp = c->smp; a.smp_n = c->smp_n; a.smp_max = c->smp_max;
     a.smp_stride = c->smp_stride; a.smp_seed = c->smp_seed;
     return a;
@@ -1583,7 +1651,7 @@ static void launch_flux( kr_ctx * c, cudaStream_t st, const args_t< R > & a, int
     const int * n = c->cfg.n;
     constexpr int NP = MHD ? 8 : 5;
     const flux_tiling t = tiling_for< R >( c, axis, NP );
-    if( ! t.ok || c->no_tiles )
+    if( ! t.ok || c->no_tiles || MODE == KR_RIEMANN_LEARNED )
     {
         int ext[ 3 ];
         for( int d = 0; d < 3; ++ d )
@@ -1639,7 +1707,6 @@ static void enqueue_back( kr_ctx * c, cudaStream_t st, const args_t< R > & a, in
 {
     const int * n = c->cfg.n;
     const unsigned nb = unsigned( c->nblk );
-    const long long nlat = ( long long )( n[ 0 ] + 1 ) * ( n[ 1 ] + 1 ) * ( n[ 2 ] + 1 );
     const long long nghost = shell_count( n[ 0 ], n[ 1 ], n[ 2 ], 2 )
                            + ( MHD ? bf_strip_count( n[ 0 ], n[ 1 ], n[ 2 ] ) : 0 );
     timed( 1, [ & ] {
@@ -2003,6 +2070,20 @@ kr_ctx * kr_ctx_create( const kr_cfg * cfg )
                 && ck( c, cudaMalloc( & c->sel_b, ( 2 * MLP_H + 1 ) * sizeof( float ) ), "malloc selector" )
                 && ck( c, cudaMalloc( & c->sel_cnt, 2 * sizeof( unsigned long long ) ), "malloc selector" )
                 && ck( c, cudaMemset( c->sel_cnt, 0, 2 * sizeof( unsigned long long ) ), "memset selector" );
+    if( cfg->mhd && cfg->riemann == KR_RIEMANN_LEARNED && ok )
+    {   // one choice word per warp of the per-face sweep, per (axis, block)
+        for( int ax = 0; ax < 3; ++ ax )
+        {
+            int ext[ 3 ];
+            for( int d = 0; d < 3; ++ d )
+                ext[ d ] = d == ax ? n[ d ] + 1 : n[ d ] + 2;
+            c->sel_stride = std::max( c->sel_stride,
+                                      ( long long ) blocks_for( ( long long ) ext[ 0 ] * ext[ 1 ], 128 ) * ext[ 2 ] * 4 );
+        }
+        const size_t words = size_t( 3 ) * nb * c->sel_stride;
+        ok = ck( c, cudaMalloc( & c->sel_mask, words * sizeof( unsigned ) ), "malloc selector mask" )
+          && ck( c, cudaMemset( c->sel_mask, 0, words * sizeof( unsigned ) ), "memset selector mask" );
+    }
     c->stage_bytes = nb * ( size_t( c->nc ) * c->nw + ( cfg->mhd ? size_t( c->nbf ) * 3 : 0 ) ) * 8;
     ok = ok && ck( c, cudaMalloc( & c->stage, c->stage_bytes ), "malloc staging" );
     if( ! ok )
@@ -2063,7 +2144,7 @@ void kr_ctx_destroy( kr_ctx * c )
     for( int d = 0; d < 3; ++ d ) cudaFree( c->f[ d ] );
     cudaFree( c->ee ); cudaFree( c->geo ); cudaFree( c->nbr ); cudaFree( c->s );
     cudaFree( c->stage ); cudaFree( c->diag );
-    cudaFree( c->sel_w ); cudaFree( c->sel_b ); cudaFree( c->sel_cnt );
+    cudaFree( c->sel_w ); cudaFree( c->sel_b ); cudaFree( c->sel_cnt ); cudaFree( c->sel_mask );
     if( c->own_stream && c->stream ) cudaStreamDestroy( c->stream );
     delete c;
 }

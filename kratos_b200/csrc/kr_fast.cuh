@@ -35,17 +35,19 @@ template< class R > __device__ __forceinline__
 void plm_face_fast( R q_ll, R q_l, R q_r, R q_rr, R & ql, R & qr )
 {
     R dql = q_l - q_ll, dqc = q_r - q_l, dqr = q_rr - q_r;
-    R scale = R( 1 );
     if constexpr( sizeof( R ) == 4 )
-    {   // as the reference's FP32 path: bring the differences to O(1) first
-        const R m = rmax( rmax( uabs( dql ), uabs( dqr ) ), uabs( dqc ) );
-        if( m > R( 1e-24f ) )
-        {
-            scale = m;
-            const R s = rcp( m );
-            dql *= s; dqc *= s; dqr *= s;
-        }
+    {   // Scale-free form of the same limiter: dl dr / ( dl + dr ) =
+        // dl * ( dr / ( dl + dr ) ), whose quotient lies in ( 0, 1 ) when dl
+        // and dr share a sign, so no product of two differences is formed --
+        // no FP32 underflow for tiny or overflow for huge differences (the
+        // reference's FP32 path rescales by max |d| for the same purpose).
+        const bool lpos = fminf( dql, dqc ) > 0 || fmaxf( dql, dqc ) < 0;
+        const bool rpos = fminf( dqr, dqc ) > 0 || fmaxf( dqr, dqc ) < 0;
+        ql = lpos ? q_l + dql * ( dqc * rcp( dql + dqc ) ) : q_l;
+        qr = rpos ? q_r - dqr * ( dqc * rcp( dqc + dqr ) ) : q_r;
+        return;
     }
+    const R scale = R( 1 );
     const R dq2_l = dql * dqc;
     const R dq2_r = dqr * dqc;
     const bool lpos = dq2_l > 0, rpos = dq2_r > 0;

@@ -80,8 +80,8 @@ def test_learned_step_error_and_gain():
     o.step(steps)
     ref, _ = o.get_state()
 
-    def run(riemann, thr=None):
-        d = _ot(precision=1, riemann=riemann)
+    def run(riemann, thr=None, **kw):
+        d = _ot(precision=1, riemann=riemann, **kw)
         if thr is not None:
             d.set_selector(w, thr)
         d.step(steps)
@@ -101,3 +101,8 @@ def test_learned_step_error_and_gain():
     assert div <= 1e-12
     assert frac > 0.3                      # the network routes faces to HLLE ...
     assert e_learn < 0.5 * e_hlle          # ... at a fraction of the all-HLLE error
+    # choices kept for 4 steps between evaluations of the network
+    e_p4, div4, (faces4, cheap4) = run(2, thr=2.0, sel_period=4)
+    print("sel_period 4: rel L1 density %.2e (HLLE on %.1f%% of faces)" % (e_p4, 100 * cheap4 / faces4))
+    assert e_p4 <= 1e-4 and div4 <= 1e-12
+    assert cheap4 / faces4 > 0.3
