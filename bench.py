@@ -32,6 +32,16 @@ GAMMA = 5.0 / 3.0
 SEED = 2
 # algorithmic bytes: 8 FP64 state words (5 conserved + 3 face B) x 5 transfers
 BYTES_PER_ZONE_CYCLE = 320
+# The flux sweep (the kernel with the largest share of the step): per face it
+# reads the 8 primitive words of one cell (neighbouring faces share the rest of
+# the stencil through L1) and the face's normal B (FP64), and writes 7 flux
+# words -- 68 B in the FP32 modes, 128 B in FP64.  Faces per launch include
+# the transverse ghost lines the edge EMF reads: (n+1) ((n+2)^2 - 4) per block.
+FLUX_BYTES_PER_FACE = {4: 8 * 4 + 8 + 7 * 4, 8: 8 * 8 + 8 + 7 * 8}
+# DRAM bytes per face of one FP32 flux launch, ncu dram__bytes_read.sum +
+# dram__bytes_write.sum on the 128^3 sample (8 blocks of 64^3) divided by its
+# 2.26 M faces; traffic scales with the faces (same block shape)
+FLUX_DRAM_BYTES_PER_FACE = 54.9
 WORKLOAD = "ot 256^3 periodic MHD, 64 blocks of 64^3, PLM+HLLD+CT, Heun RK2"
 
 
@@ -310,6 +320,24 @@ def time_mode(mode, args, local_rank, world, dist):
     return out
 
 
+def flux_roofline(h, head, world, peak, peak_kind):
+    """Roofline line of the flux sweep: algorithmic bytes per launch over the
+    mean launch duration (CUDA events around each launch, kr_profile_step)."""
+    rsize = 8 if head == "fp64" else 4
+    nblk = NB[0] * NB[1] * NB[2]
+    faces = nblk * (N[0] + 1) * ((N[1] + 2) * (N[2] + 2) - 4)
+    k = h["kernels_ms_per_step"]
+    launch_ms = (k["flux_x"] + k["flux_y"] + k["flux_z"]) / 6.0      # 3 sweeps x 2 stages
+    gbs = faces * FLUX_BYTES_PER_FACE[rsize] / (launch_ms * 1e-3) / 1e9
+    return {"bound": "hbm", "kernel": "k_flux (one sweep, %s mode)" % head, "achieved": gbs, "peak": peak,
+            "unit": "GB/s", "frac": gbs / peak,
+            "traffic": FLUX_DRAM_BYTES_PER_FACE * faces if rsize == 4 else None,
+            "algorithmic_bytes_per_launch": faces * FLUX_BYTES_PER_FACE[rsize],
+            "launch_ms": launch_ms,
+            "basis": "%d B/face x %d faces per launch (%s peak); the sweep is bound by instruction "
+                     "issue and latency (FP32 PLM + HLLD), not by HBM" % (FLUX_BYTES_PER_FACE[rsize], faces, peak_kind)}
+
+
 def main():
     args = parse()
     rank, world, local_rank = dist_env()
@@ -348,10 +376,11 @@ def main():
                            "kernels_ms_per_step": r["kernels_ms_per_step"]},
                           **({"selector": r["selector"]} if "selector" in r else {}))
                   for m, r in results.items()},
-        "roofline": {"bound": "hbm", "achieved": step_gbs, "peak": peak, "unit": "GB/s",
-                     "frac": step_gbs / peak, "traffic": None,
-                     "basis": "whole step: %d B/zone-cycle algorithmic (%s peak); top kernel %s"
-                              % (BYTES_PER_ZONE_CYCLE, peak_kind, top)},
+        "roofline": flux_roofline(h, head, world, peak, peak_kind),
+        "step_roofline": {"bound": "hbm", "achieved": step_gbs, "peak": peak, "unit": "GB/s",
+                          "frac": step_gbs / peak,
+                          "basis": "whole step: %d B/zone-cycle algorithmic (%s peak); longest kernel kind %s"
+                                   % (BYTES_PER_ZONE_CYCLE, peak_kind, top)},
         "clocks": h["clocks"],
         "e2e": h["e2e"],
         "gpu_launches": h["launches_per_step"] * args.steps,

@@ -312,56 +312,99 @@ __host__ __device__ __forceinline__ long long bf_strip_count( int n0, int n1, in
     return s;
 }
 
+// Divisors of the shell and strip enumerations (multiply-high quotients).
+struct ghost_div_t { udiv_t e0, e1, n1, f[ 3 ]; };
+
+static ghost_div_t make_ghost_div( const int * n )
+{
+    ghost_div_t g;
+    g.e0 = make_udiv( unsigned( n[ 0 ] + 4 ) );
+    g.e1 = make_udiv( unsigned( n[ 1 ] + 4 ) );
+    g.n1 = make_udiv( unsigned( n[ 1 ] ) );
+    for( int c = 0; c < 3; ++ c )
+        g.f[ c ] = make_udiv( unsigned( n[ c ] + 1 ) );
+    return g;
+}
+
 template< bool MHD, class R >
-__global__ void __launch_bounds__( 256 ) k_ghost( const args_t< R > a, int step )
+__global__ void __launch_bounds__( 256 ) k_ghost( const args_t< R > a, int step, ghost_div_t gd )
 {
     constexpr int NW = MHD ? 11 : 5;   // stored W words: prim (8) + cell E (3)
     const int b = blockIdx.y;
-    long long t = ( long long ) blockIdx.x * blockDim.x + threadIdx.x;
-    const long long nsh = shell_count( a.n0, a.n1, a.n2, 2 );
-    if( t < nsh )
-    {
-        int i0, i1, i2, s0, s1, s2;
-        shell_site( t, a.n0, a.n1, a.n2, 2, i0, i1, i2 );
+    unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int e0 = a.n0 + 4, e1 = a.n1 + 4;
+    const unsigned zs = 4u * e0 * e1, ys = 4u * e0 * a.n2, xs = 4u * a.n1 * a.n2;
+    if( t < zs + ys + xs )
+    {   // shell [-2, n+2)^3 \ [0, n)^3: z slabs, y slabs (interior z), x slabs
+        int i0, i1, i2;
+        if( t < zs )
+        {
+            const unsigned q = udiv_q( t, gd.e0 ), q2 = udiv_q( q, gd.e1 );
+            i0 = int( t - q * e0 ) - 2;
+            i1 = int( q - q2 * e1 ) - 2;
+            i2 = q2 < 2 ? int( q2 ) - 2 : a.n2 + int( q2 ) - 2;
+        }
+        else if( ( t -= zs ) < ys )
+        {
+            const unsigned q = udiv_q( t, gd.e0 ), l = q & 3u;
+            i0 = int( t - q * e0 ) - 2;
+            i2 = int( q >> 2 );
+            i1 = l < 2 ? int( l ) - 2 : a.n1 + int( l ) - 2;
+        }
+        else
+        {
+            t -= ys;
+            const unsigned l = t & 3u, q = t >> 2, q2 = udiv_q( q, gd.n1 );
+            i1 = int( q - q2 * a.n1 );
+            i2 = int( q2 );
+            i0 = l < 2 ? int( l ) - 2 : a.n0 + int( l ) - 2;
+        }
+        int s0, s1, s2;
         const int j0 = wrap_axis( i0, a.n0, s0 );
         const int j1 = wrap_axis( i1, a.n1, s1 );
         const int j2 = wrap_axis( i2, a.n2, s2 );
         const int src = a.nbr[ b * 27 + ( s0 + 1 ) + 3 * ( s1 + 1 ) + 9 * ( s2 + 1 ) ];
         if( src < 0 )
-            return;                              // physical boundary: k_phys
+            return;                              // physical side or another rank
+        const int ngw = int( a.ngw );
+        R * dst = a.w + ( size_t ) b * NW * a.ngw + ( ( i0 + 2 ) + a.sw1 * ( i1 + 2 ) + a.sw2 * ( i2 + 2 ) );
+        const R * srcp = a.w + ( size_t ) src * NW * a.ngw + ( ( j0 + 2 ) + a.sw1 * ( j1 + 2 ) + a.sw2 * ( j2 + 2 ) );
+        R v[ NW ];
         for( int k = 0; k < NW; ++ k )
-            a.w[ iw( a, b, k, NW, i0, i1, i2 ) ] = a.w[ iw( a, src, k, NW, j0, j1, j2 ) ];
+            v[ k ] = srcp[ k * ngw ];
+        for( int k = 0; k < NW; ++ k )
+            dst[ k * ngw ] = v[ k ];
         return;
     }
     if( ! MHD )
         return;
-    t -= nsh;
+    t -= zs + ys + xs;
     const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
     for( int c = 0; c < 3; ++ c )
     {
         const int a1 = ( c + 1 ) % 3, a2 = ( c + 2 ) % 3;
-        const long long cnt = 2LL * ( nn[ c ] + 1 ) * ( nn[ a1 ] + nn[ a2 ] );
+        const unsigned cnt = 2u * ( nn[ c ] + 1 ) * ( nn[ a1 ] + nn[ a2 ] );
         if( t >= cnt )
         {
             t -= cnt;
             continue;
         }
         // t -> (face index along c, side, transverse position along the other axis)
-        const int fc = int( t % ( nn[ c ] + 1 ) );
-        long long r = t / ( nn[ c ] + 1 );
-        const int side = int( r % 2 );
-        r /= 2;
+        const unsigned q = udiv_q( t, gd.f[ c ] );
+        const int fc = int( t - q * unsigned( nn[ c ] + 1 ) );
+        const int side = int( q & 1u );
+        const int r = int( q >> 1 );
         int ii[ 3 ];
         ii[ c ] = fc;
         if( r < nn[ a2 ] )
         {   // ghost line along a1
             ii[ a1 ] = side ? nn[ a1 ] : -1;
-            ii[ a2 ] = int( r );
+            ii[ a2 ] = r;
         }
         else
         {
             ii[ a2 ] = side ? nn[ a2 ] : -1;
-            ii[ a1 ] = int( r - nn[ a2 ] );
+            ii[ a1 ] = r - nn[ a2 ];
         }
         int sh[ 3 ] = { 0, 0, 0 }, jj[ 3 ] = { ii[ 0 ], ii[ 1 ], ii[ 2 ] };
         for( int d = 0; d < 3; ++ d )
@@ -1713,7 +1756,7 @@ static void enqueue_back( kr_ctx * c, cudaStream_t st, const args_t< R > & a, in
         if( ! c->hrecv.items.empty(  ) )
             k_halo< MHD, R, false ><<< dim3( c->halo_grid, unsigned( c->hrecv.items.size(  ) ) ), 256, 0, st >>>(
                 a, c->recv_items, ( R * ) c->recv_w, c->recv_b, stage );
-        k_ghost< MHD, R ><<< dim3( blocks_for( nghost, 256 ), nb ), 256, 0, st >>>( a, stage );
+        k_ghost< MHD, R ><<< dim3( blocks_for( nghost, 256 ), nb ), 256, 0, st >>>( a, stage, make_ghost_div( n ) );
         if( ! MHD && has_phys( c ) )
             k_phys< R ><<< dim3( blocks_for( phys_sites( c ), 128 ), 6, nb ), 128, 0, st >>>( a );
         if( MHD )
