@@ -24,6 +24,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -46,6 +47,7 @@ struct scal_t
     double t;
     long long n_steps;
     int status;                   // sticky error bits
+    int sel_force;                // learned mode: run the network at the next step
     int heal_count;               // floor corrections (diagnostic)
 };
 
@@ -74,8 +76,10 @@ struct args_t
     const float * sel_b;              // b1, b2, b3
     float sel_thr;                    // logit threshold for HLLE
     unsigned long long * sel_cnt;     // [0] faces, [1] faces given HLLE
-    unsigned * sel_mask;              // per-warp choice words, reused between evaluations
-    long long sel_stride;             // words per (axis, block, lines) region
+    unsigned * sel_list;              // per (axis, block): HLLD faces from the front,
+                                      // HLLE faces from the back (packed positions)
+    unsigned * sel_count;             // per (axis, block): [HLLD, HLLE] list lengths
+    long long sel_cap;                // list capacity per (axis, block)
     int sel_period;                   // steps between evaluations of the network
     // face sampling for selector training (collect steps only)
     float * smp;                      // [max][17]: 16 features + flux gap
@@ -134,9 +138,17 @@ __device__ __forceinline__ double warp_min( double v )
 ////////////////////////////////////////////////////////////
 // Scalars: step begin / end (cycle.cpp:77-115)
 
-__global__ void k_step_begin( scal_t * s )
+__device__ __forceinline__ bool sel_eval_step( const scal_t * s, int period )
+{   // learned mode: the network runs at stage 0 of this step
+    return s->sel_force || s->n_steps % period == 0;
+}
+
+__global__ void k_step_begin( scal_t * s, unsigned * sel_count, int n_count, int period )
 {
     s->dt_bits = __double_as_longlong( s->dt_bound );
+    if( sel_count && sel_eval_step( s, period ) )
+        for( int k = 0; k < n_count; ++ k )
+            sel_count[ k ] = 0;
 }
 
 __global__ void k_step_end( scal_t * s, double dt_expand )
@@ -148,6 +160,7 @@ __global__ void k_step_end( scal_t * s, double dt_expand )
     s->t       += dt;
     s->dt_bound = dt * dt_expand;
     s->n_steps += 1;
+    s->sel_force = 0;
 }
 
 ////////////////////////////////////////////////////////////
@@ -672,15 +685,15 @@ void solve_store( const args_t< R > & a, int b, int axis, const int * ii, bool v
 // ghost lines included, mhd/integrator/integrator.h:138-168); lines != 0: only
 // those ghost lines (the tiled kernel below does the rest).
 // Learned mode (no reference counterpart).  The network runs at stage 0 of
-// every sel_period-th step; its per-face choices are kept as one ballot word
-// per warp and reused by the other stages and steps.  The CTA then sorts its
-// 128 faces into one run of HLLD faces and one run of HLLE faces (through
-// shared memory, original order kept within each run), so that each warp
-// executes one solver -- a per-face choice inside a warp would make the warp
-// pay for both.
+// every sel_period-th step (and the step after new weights): this sweep
+// evaluates it for every face, appends each face to its (axis, block) HLLD or
+// HLLE list, sorts the CTA's 128 faces into one run of HLLD faces and one run
+// of HLLE faces through shared memory (so that each warp executes one solver:
+// a per-face choice inside a warp makes the warp pay for both) and solves
+// them.  Every other sweep runs k_flux_list over the two lists.
 template< bool MHD, class R > __device__ __forceinline__
 void learned_solve( const args_t< R > & a, int b, int axis, const int * ii, bool valid,
-                    R * ql, R * qr, int step, long long word )
+                    R * ql, R * qr )
 {
     constexpr int NF = 7;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -694,31 +707,35 @@ void learned_solve( const args_t< R > & a, int b, int axis, const int * ii, bool
     __shared__ R sq[ 128 ][ 17 ];                // rotated left / right states (+1 pad)
     __shared__ int sid[ 128 ];                   // face position, packed
     __shared__ int cnt[ 4 ][ 2 ];
-    bool cheap;
-    if( step == 0 && a.s->n_steps % a.sel_period == 0 )
-    {   // grid-uniform branch: every lane of the warp takes part in the MMAs
-        float f[ MLP_IN ];
-        face_features< R >( ql, qr, e.gamma, f );
-        const float z = mlp_logit( f, a.sel_w, a.sel_b, xs[ warp ] );
-        cheap = valid && z > a.sel_thr;
-        const unsigned m = __ballot_sync( 0xffffffffu, cheap );
-        if( lane == 0 )
-            a.sel_mask[ word ] = m;
-    }
-    else
-        cheap = valid && ( ( a.sel_mask[ word ] >> lane ) & 1u );
+    // the network: every lane of the warp takes part in the MMAs
+    float f[ MLP_IN ];
+    face_features< R >( ql, qr, e.gamma, f );
+    const float z = mlp_logit( f, a.sel_w, a.sel_b, xs[ warp ] );
+    const bool cheap = valid && z > a.sel_thr;
     const unsigned mh = __ballot_sync( 0xffffffffu, valid && ! cheap );
     const unsigned mc = __ballot_sync( 0xffffffffu, cheap );
+    const unsigned below = ( 1u << lane ) - 1u;
+    // append this warp's faces to the (axis, block) lists the other sweeps use
+    unsigned * cntg = a.sel_count + ( ( size_t ) axis * a.nblk + b ) * 2;
+    unsigned * list = a.sel_list + ( ( size_t ) axis * a.nblk + b ) * a.sel_cap;
+    unsigned bh = 0, bc = 0;
     if( lane == 0 )
     {
         cnt[ warp ][ 0 ] = __popc( mh );
         cnt[ warp ][ 1 ] = __popc( mc );
+        if( mh ) bh = atomicAdd( cntg, ( unsigned ) __popc( mh ) );
+        if( mc ) bc = atomicAdd( cntg + 1, ( unsigned ) __popc( mc ) );
         if( mh | mc )
         {
             atomicAdd( a.sel_cnt, ( unsigned long long ) __popc( mh | mc ) );
             atomicAdd( a.sel_cnt + 1, ( unsigned long long ) __popc( mc ) );
         }
     }
+    bh = __shfl_sync( 0xffffffffu, bh, 0 );
+    bc = __shfl_sync( 0xffffffffu, bc, 0 );
+    const unsigned packed = unsigned( ( ii[ 0 ] + 2 ) | ( ( ii[ 1 ] + 2 ) << 10 ) | ( ( ii[ 2 ] + 2 ) << 20 ) );
+    if( valid && ! cheap ) list[ bh + __popc( mh & below ) ] = packed;
+    else if( cheap )       list[ a.sel_cap - 1 - ( bc + __popc( mc & below ) ) ] = packed;
     __syncthreads(  );
     int nh = 0, nh_before = 0, nc_before = 0, nall = 0;
     for( int w = 0; w < 4; ++ w )
@@ -727,14 +744,13 @@ void learned_solve( const args_t< R > & a, int b, int axis, const int * ii, bool
         nall += cnt[ w ][ 0 ] + cnt[ w ][ 1 ];
         if( w < warp ) { nh_before += cnt[ w ][ 0 ]; nc_before += cnt[ w ][ 1 ]; }
     }
-    const unsigned below = ( 1u << lane ) - 1u;
     int slot = -1;
     if( valid && ! cheap ) slot = nh_before + __popc( mh & below );
     else if( cheap )       slot = nh + nc_before + __popc( mc & below );
     if( slot >= 0 )
     {
         for( int k = 0; k < 8; ++ k ) { sq[ slot ][ k ] = ql[ k ]; sq[ slot ][ 8 + k ] = qr[ k ]; }
-        sid[ slot ] = ( ii[ 0 ] + 2 ) | ( ( ii[ 1 ] + 2 ) << 10 ) | ( ( ii[ 2 ] + 2 ) << 20 );
+        sid[ slot ] = int( packed );
     }
     __syncthreads(  );
     const int j = threadIdx.x;
@@ -773,6 +789,9 @@ __global__ void __launch_bounds__( 128, ( flux_min_ctas< R, MODE >(  ) ) ) k_flu
     constexpr bool learned = MHD && MODE == KR_RIEMANN_LEARNED;
     // grid: x over the faces of one (x, y) plane (lines: over all line
     // faces), y over z planes, z over blocks; dv divides by the row length
+    if constexpr( learned )
+        if( step != 0 || ! sel_eval_step( a.s, a.sel_period ) )
+            return;                   // k_flux_list solves this sweep
     const int b = blockIdx.z;
     const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
     const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -847,14 +866,58 @@ __global__ void __launch_bounds__( 128, ( flux_min_ctas< R, MODE >(  ) ) ) k_flu
     }
     if constexpr( learned )
     {   // the per-face kernel covers every face of the sweep here (lines == 0)
-        const long long word = ( ( long long ) axis * a.nblk + b ) * a.sel_stride
-                             + ( ( long long ) blockIdx.y * gridDim.x + blockIdx.x ) * 4 + ( threadIdx.x >> 5 );
-        learned_solve< MHD, R >( a, b, axis, ii, valid, ql, qr, step, word );
+        learned_solve< MHD, R >( a, b, axis, ii, valid, ql, qr );
         return;
     }
     const unsigned long long key = ( ( unsigned long long ) b * 3 + axis ) * 0x9E3779B97F4A7C15ull
                                  + ( unsigned long long ) ( lines ? t_lin + ( 1ll << 40 ) : t_lin );
     solve_store< MHD, R, MODE >( a, b, axis, ii, valid, ql, qr, threadIdx.x >> 5, key );
+}
+
+// Learned mode, sweeps without the network: one thread per entry of the
+// (axis, block) HLLD list (CHEAP = false) or HLLE list (CHEAP = true) built by
+// the last evaluation.  Warps run one solver; entries of a warp come from
+// one or two producer warps, so loads and stores stay nearly coalesced.
+template< bool MHD, class R, bool CHEAP >
+__global__ void __launch_bounds__( 128, ( flux_min_ctas< R, KR_RIEMANN_DEFAULT >(  ) ) )
+k_flux_list( const args_t< R > a, int axis, int step )
+{
+    constexpr int NW = MHD ? 11 : 5;
+    constexpr int NP = MHD ? 8 : 5;
+    if( step == 0 && sel_eval_step( a.s, a.sel_period ) )
+        return;                       // the network's sweep (k_flux) solves this one
+    const int b = blockIdx.z;
+    const size_t r = ( size_t ) axis * a.nblk + b;
+    const unsigned n = a.sel_count[ r * 2 + ( CHEAP ? 1 : 0 ) ];
+    const unsigned * list = a.sel_list + r * a.sel_cap;
+    // a fixed grid strides over the list (its length is known only on the device);
+    // the next entry is fetched before this face's work
+    const unsigned stride = gridDim.x * blockDim.x;
+    unsigned j = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned pk_next = j < n ? ( CHEAP ? list[ a.sel_cap - 1 - j ] : list[ j ] ) : 0u;
+    for( ; j < n; j += stride )
+    {
+    const unsigned pk = pk_next;
+    if( j + stride < n )
+        pk_next = CHEAP ? list[ a.sel_cap - 1 - ( j + stride ) ] : list[ j + stride ];
+    int ii[ 3 ] = { int( pk & 1023u ) - 2, int( ( pk >> 10 ) & 1023u ) - 2, int( pk >> 20 ) - 2 };
+    const int st = axis == 0 ? 1 : ( axis == 1 ? a.sw1 : a.sw2 );
+    R ql[ 8 ], qr[ 8 ];
+    const R * wb = a.w + ( size_t ) b * NW * a.ngw
+                 + ( ( ii[ 0 ] + 2 ) + a.sw1 * ( ii[ 1 ] + 2 ) + a.sw2 * ( ii[ 2 ] + 2 ) );
+    const int ngw = int( a.ngw );
+    for( int k = 0; k < NP; ++ k )
+    {
+        if( MHD && k == BCC + axis )
+        {
+            ql[ k ] = qr[ k ] = R( a.bf[ step ][ ibf( a, b, axis, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] );
+            continue;
+        }
+        const R * p = wb + k * ngw;
+        plm_face_fast< R >( p[ -2 * st ], p[ -st ], p[ 0 ], p[ st ], ql[ k ], qr[ k ] );
+    }
+    solve_store< MHD, R, CHEAP ? KR_RIEMANN_HLLE : KR_RIEMANN_DEFAULT >( a, b, axis, ii, true, ql, qr, 0, 0ull );
+    }
 }
 
 // Shared-memory tiled sweep over the faces whose transverse position lies in
@@ -1555,8 +1618,9 @@ struct kr_ctx
     unsigned long long * sel_cnt = nullptr;
     float sel_thr = 0.f;
     bool sel_ready = false;
-    unsigned * sel_mask = nullptr;     // learned mode: choice words of the last evaluation
-    long long sel_stride = 0;
+    unsigned * sel_list = nullptr;     // learned mode: face lists of the last evaluation
+    unsigned * sel_count = nullptr;
+    long long sel_cap = 0;
     // selector training samples (only during kr_selector_collect)
     float * smp = nullptr;
     unsigned long long * smp_n = nullptr;
@@ -1568,6 +1632,7 @@ struct kr_ctx
     cudaStream_t graph_stream = nullptr;
     std::vector< geo_t > geo_h;
     bool no_tiles = false;             // force the per-face flux kernel (testing)
+    int n_sm = 148;                    // multiprocessors of the device
     // sharding: this rank's blocks and the halo exchange with the others
     int nranks = 1, rank = 0;
     std::vector< int > gid_h;          // global id of each local block
@@ -1627,7 +1692,7 @@ static args_t< R > make_args( kr_ctx * c )
         if( c->cfg.bc[ 2 * d + 1 ] == KR_BC_OUT || c->cfg.bc[ 2 * d + 1 ] == KR_BC_FRE )
             a.emf_out |= 1 << d;
     a.sel_w = c->sel_w; a.sel_b = c->sel_b; a.sel_thr = c->sel_thr; a.sel_cnt = c->sel_cnt;
-    a.sel_mask = c->sel_mask; a.sel_stride = c->sel_stride;
+    a.sel_list = c->sel_list; a.sel_count = c->sel_count; a.sel_cap = c->sel_cap;
     a.sel_period = c->cfg.sel_period > 1 ? c->cfg.sel_period : 1;
     a.smp = c->smp; a.smp_n = c->smp_n; a.smp_max = c->smp_max;
     a.smp_stride = c->smp_stride; a.smp_seed = c->smp_seed;
@@ -1701,6 +1766,15 @@ static void launch_flux( kr_ctx * c, cudaStream_t st, const args_t< R > & a, int
             ext[ d ] = ( d == axis ) ? n[ d ] + 1 : n[ d ] + ( MHD ? 2 : 0 );
         k_flux< MHD, R, MODE ><<< dim3( blocks_for( ( long long ) ext[ 0 ] * ext[ 1 ], 128 ), ext[ 2 ], c->nblk ), 128, 0, st >>>(
             a, axis, stage, 0, make_udiv( unsigned( ext[ 0 ] ) ) );
+        if constexpr( MODE == KR_RIEMANN_LEARNED && MHD )
+        {   // sweeps without the network: the two face lists (each kernel exits
+            // at once on the network's sweep; CTAs past a list's length exit)
+            // about two waves of CTAs over all blocks, striding over the lists
+            const unsigned gx = unsigned( std::max< long long >( 1, std::min< long long >(
+                blocks_for( ( long long ) ext[ 0 ] * ext[ 1 ] * ext[ 2 ], 128 ), ( 2LL * c->n_sm * 8 ) / c->nblk ) ) );
+            k_flux_list< MHD, R, false ><<< dim3( gx, 1, c->nblk ), 128, 0, st >>>( a, axis, stage );
+            k_flux_list< MHD, R, true ><<< dim3( gx, 1, c->nblk ), 128, 0, st >>>( a, axis, stage );
+        }
         return;
     }
     if( axis == 0 )      launch_tile< MHD, R, MODE, 0 >( c, st, a, stage, t );
@@ -1834,7 +1908,7 @@ template< bool MHD, class R, bool SAMPLE = false >
 static bool enqueue_step( kr_ctx * c, cudaStream_t st )
 {
     const args_t< R > a = make_args< R >( c );
-    k_step_begin<<< 1, 1, 0, st >>>( c->s );
+    k_step_begin<<< 1, 1, 0, st >>>( c->s, c->sel_count, 6 * c->nblk, c->cfg.sel_period > 1 ? c->cfg.sel_period : 1 );
     for( int stage = 0; stage < 2; ++ stage )
     {
         enqueue_front< MHD, R >( c, st, a, stage, untimed_t(  ) );
@@ -1867,7 +1941,7 @@ static bool profile_step( kr_ctx * c, double * ms )
         ms[ kind ] += t;
     };
     bool ok = true;
-    k_step_begin<<< 1, 1, 0, st >>>( c->s );
+    k_step_begin<<< 1, 1, 0, st >>>( c->s, c->sel_count, 6 * c->nblk, c->cfg.sel_period > 1 ? c->cfg.sel_period : 1 );
     for( int stage = 0; stage < 2 && ok; ++ stage )
     {
         enqueue_front< MHD, R >( c, st, a, stage, timed );
@@ -2035,9 +2109,12 @@ kr_ctx * kr_ctx_create( const kr_cfg * cfg )
     }
     if( ! ck( nullptr, cudaSetDevice( cfg->device ), "cudaSetDevice" ) )
         return nullptr;
+    int n_sm = 148;
+    cudaDeviceGetAttribute( & n_sm, cudaDevAttrMultiProcessorCount, cfg->device );
 
     kr_ctx * c = new kr_ctx;
     c->cfg = * cfg;
+    c->n_sm = n_sm;
     // The shared-memory tiled sweep is opt-in: on the 256^3 OT step it measured
     // slower than the per-face kernel (more registers per thread, long per-thread
     // face loops, a tail of partial CTAs), so the per-face kernel is the default.
@@ -2114,18 +2191,18 @@ kr_ctx * kr_ctx_create( const kr_cfg * cfg )
                 && ck( c, cudaMalloc( & c->sel_cnt, 2 * sizeof( unsigned long long ) ), "malloc selector" )
                 && ck( c, cudaMemset( c->sel_cnt, 0, 2 * sizeof( unsigned long long ) ), "memset selector" );
     if( cfg->mhd && cfg->riemann == KR_RIEMANN_LEARNED && ok )
-    {   // one choice word per warp of the per-face sweep, per (axis, block)
+    {   // per (axis, block): a list with room for every face of the sweep
         for( int ax = 0; ax < 3; ++ ax )
         {
-            int ext[ 3 ];
+            long long f = 1;
             for( int d = 0; d < 3; ++ d )
-                ext[ d ] = d == ax ? n[ d ] + 1 : n[ d ] + 2;
-            c->sel_stride = std::max( c->sel_stride,
-                                      ( long long ) blocks_for( ( long long ) ext[ 0 ] * ext[ 1 ], 128 ) * ext[ 2 ] * 4 );
+                f *= d == ax ? n[ d ] + 1 : n[ d ] + 2;
+            c->sel_cap = std::max( c->sel_cap, f );
         }
-        const size_t words = size_t( 3 ) * nb * c->sel_stride;
-        ok = ck( c, cudaMalloc( & c->sel_mask, words * sizeof( unsigned ) ), "malloc selector mask" )
-          && ck( c, cudaMemset( c->sel_mask, 0, words * sizeof( unsigned ) ), "memset selector mask" );
+        const size_t words = size_t( 3 ) * nb * c->sel_cap;
+        ok = ck( c, cudaMalloc( & c->sel_list, words * sizeof( unsigned ) ), "malloc selector lists" )
+          && ck( c, cudaMalloc( & c->sel_count, 6 * nb * sizeof( unsigned ) ), "malloc selector counts" )
+          && ck( c, cudaMemset( c->sel_count, 0, 6 * nb * sizeof( unsigned ) ), "memset selector counts" );
     }
     c->stage_bytes = nb * ( size_t( c->nc ) * c->nw + ( cfg->mhd ? size_t( c->nbf ) * 3 : 0 ) ) * 8;
     ok = ok && ck( c, cudaMalloc( & c->stage, c->stage_bytes ), "malloc staging" );
@@ -2187,7 +2264,7 @@ void kr_ctx_destroy( kr_ctx * c )
     for( int d = 0; d < 3; ++ d ) cudaFree( c->f[ d ] );
     cudaFree( c->ee ); cudaFree( c->geo ); cudaFree( c->nbr ); cudaFree( c->s );
     cudaFree( c->stage ); cudaFree( c->diag );
-    cudaFree( c->sel_w ); cudaFree( c->sel_b ); cudaFree( c->sel_cnt ); cudaFree( c->sel_mask );
+    cudaFree( c->sel_w ); cudaFree( c->sel_b ); cudaFree( c->sel_cnt ); cudaFree( c->sel_list ); cudaFree( c->sel_count );
     if( c->own_stream && c->stream ) cudaStreamDestroy( c->stream );
     delete c;
 }
@@ -2404,6 +2481,11 @@ int kr_set_selector( kr_ctx * c, const float * w, float threshold )
         drop_graph( c );                 // the threshold is a kernel argument
     c->sel_thr = threshold;
     c->sel_ready = true;
+    const int one = 1;                   // face lists are rebuilt at the next step
+    if( ! ck( c, cudaMemcpyAsync( ( char * ) c->s + offsetof( scal_t, sel_force ), & one, sizeof( one ),
+                                  cudaMemcpyHostToDevice, c->stream ), "selector force" )
+        || ! ck( c, cudaStreamSynchronize( c->stream ), "sync" ) )
+        return -1;
     return 0;
 }
 
@@ -2477,6 +2559,8 @@ int kr_launches_per_step( kr_ctx * c )
                                                     : tiling_for< double >( c, axis, c->cfg.mhd ? 8 : 5 );
         flux += ( t.ok && ! c->no_tiles && c->cfg.mhd ) ? 2 : 1;
     }
+    if( c->cfg.mhd && c->cfg.riemann == KR_RIEMANN_LEARNED )
+        flux = 9;                     // per sweep: the network's kernel and the two list kernels
     const int halo = ( c->hsend.items.empty(  ) ? 0 : 1 ) + ( c->hrecv.items.empty(  ) ? 0 : 1 );
     int phys = ! c->cfg.mhd && has_phys( c ) ? 1 : 0;
     if( c->cfg.mhd )
@@ -2646,7 +2730,7 @@ int kr_group_step( kr_ctx * const * ctxs, int n, int n_steps )
     const bool mhd = g0.mhd, fp32 = g0.precision == 1;
     for( int step = 0; step < n_steps; ++ step )
     {
-        for( kr_ctx * c : by ) k_step_begin<<< 1, 1, 0, st >>>( c->s );
+        for( kr_ctx * c : by ) k_step_begin<<< 1, 1, 0, st >>>( c->s, c->sel_count, 6 * c->nblk, c->cfg.sel_period > 1 ? c->cfg.sel_period : 1 );
         for( int stage = 0; stage < 2; ++ stage )
         {
             for( kr_ctx * c : by )
