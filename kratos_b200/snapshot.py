@@ -114,3 +114,23 @@ def to_lex_arrays(snap: Snapshot, nb):
     u = np.stack(u_out)
     bf = np.stack(bf_out) if bf_out[0] is not None else None
     return u, bf
+
+
+def to_tree_arrays(snap: Snapshot):
+    """Gather a (possibly refined) snapshot's blocks in tree order: level by
+    level, lexicographic (x fastest) inside a level, from each block's `level`
+    and `i_logic` entries.  Returns (level [nblk], reg [nblk, 3], u, bf or None)
+    with u and bf shaped as in to_lex_arrays."""
+    rows = []
+    for bid in block_ids(snap):
+        lv = int(snap.array("block_%d|level" % bid, "i")[0])
+        il = snap.array("block_%d|i_logic" % bid, "i").astype(int)
+        rows.append(((lv, int(il[2]), int(il[1]), int(il[0])), bid))
+    rows.sort()
+    level = np.array([r[0][0] for r in rows], dtype=np.int32)
+    reg = np.array([[r[0][3], r[0][2], r[0][1]] for r in rows], dtype=np.int32).reshape(-1, 3)
+    u = np.stack([snap.field(bid, "hydro_cons_")[0] for _, bid in rows])
+    bf = None
+    if rows and ("block_%d|field_bf_field" % rows[0][1]) in snap.data:
+        bf = np.stack([snap.field(bid, "field_bf_")[0] for _, bid in rows])
+    return level, reg, u, bf

@@ -32,6 +32,14 @@ class _Cfg(ctypes.Structure):
     ]
 
 
+class _Region(ctypes.Structure):
+    _fields_ = [
+        ("level", ctypes.c_int),
+        ("x_min", ctypes.c_double * 3),
+        ("x_max", ctypes.c_double * 3),
+    ]
+
+
 BC_KINDS = {"per": 0, "out": 1, "ref": 2, "fre": 3, "fixd": 4}
 
 
@@ -51,6 +59,12 @@ def lib():
         dp = ctypes.POINTER(ctypes.c_double)
         L.kro_create.restype = ctypes.c_void_p
         L.kro_create.argtypes = [ctypes.POINTER(_Cfg)]
+        L.kro_create_tree.restype = ctypes.c_void_p
+        L.kro_create_tree.argtypes = [ctypes.POINTER(_Cfg), ctypes.c_int, ctypes.POINTER(_Region)]
+        L.kro_nblk.restype = ctypes.c_int
+        L.kro_nblk.argtypes = [ctypes.c_void_p]
+        ip = ctypes.POINTER(ctypes.c_int)
+        L.kro_block_info.argtypes = [ctypes.c_void_p, ip, ip]
         L.kro_destroy.argtypes = [ctypes.c_void_p]
         L.kro_set_state.argtypes = [ctypes.c_void_p, dp, dp]
         L.kro_get_state.argtypes = [ctypes.c_void_p, dp, dp]
@@ -78,13 +92,15 @@ FLT_MAX = float(np.finfo(np.float32).max)
 
 
 class OracleMesh:
-    """Uniform periodic mesh of nb blocks of n cells, state in lexicographic
-    block order (x fastest).  u: [nblk, n2, n1, n0, nw]; bf: [nblk, n2+5,
-    n1+5, n0+5, 3] (face lattice with 2 ghost layers)."""
+    """Mesh of nb root blocks of n cells, state in block order: level by level,
+    lexicographic (x fastest) inside a level (a uniform mesh is one level).
+    u: [nblk, n2, n1, n0, nw]; bf: [nblk, n2+5, n1+5, n0+5, 3] (face lattice
+    with 2 ghost layers).  `regions`: static refinement, a list of
+    (level, x_min, x_max) as the [refine_region*] sections give them."""
 
     def __init__(self, mhd, nb, n, gamma, cfl=0.3, x_min=(0, 0, 0), x_max=(1, 1, 1),
                  d_floor=1e-9, t_floor=1e-9, dt_expand=2.0, dt_init=0.0, n_threads=0,
-                 kinds=("per",) * 6, w_fix=(0, 0, 0, 0, 0), b_fix=(0, 0, 0)):
+                 kinds=("per",) * 6, w_fix=(0, 0, 0, 0, 0), b_fix=(0, 0, 0), regions=()):
         c = _Cfg()
         c.mhd = int(mhd)
         for a in range(3):
@@ -101,11 +117,20 @@ class OracleMesh:
         self.cfg = c
         self.mhd = bool(mhd)
         self.nb, self.n = tuple(nb), tuple(n)
-        self.nblk = nb[0] * nb[1] * nb[2]
         self.nw = 8 if mhd else 5
-        self._h = lib().kro_create(ctypes.byref(c))
+        rg = (_Region * max(1, len(regions)))()
+        for k, (lvl, lo, hi) in enumerate(regions):
+            rg[k].level = int(lvl)
+            for a in range(3):
+                rg[k].x_min[a], rg[k].x_max[a] = float(lo[a]), float(hi[a])
+        self._h = lib().kro_create_tree(ctypes.byref(c), len(regions), rg)
         if not self._h:
-            raise ValueError("oracle: kro_create failed")
+            raise ValueError("oracle: kro_create_tree failed")
+        self.nblk = lib().kro_nblk(self._h)
+        self.level = np.zeros(self.nblk, dtype=np.int32)
+        self.reg = np.zeros((self.nblk, 3), dtype=np.int32)
+        ip = ctypes.POINTER(ctypes.c_int)
+        lib().kro_block_info(self._h, self.level.ctypes.data_as(ip), self.reg.ctypes.data_as(ip))
         self.t = 0.0
         # cycle.cpp:163-166: an unset dt_init starts the device dt at FLT_MAX / 10
         self.dt_bound = dt_init if dt_init >= np.finfo(np.float32).tiny else FLT_MAX / 10

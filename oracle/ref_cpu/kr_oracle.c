@@ -3,6 +3,7 @@
  * Build: oracle/Makefile (gcc, no fused multiply-add). */
 #include "kr_oracle.h"
 #include "../../kratos_b200/csrc/problems.h"
+#include "../../kratos_b200/csrc/smr_tree.h"
 
 #include <float.h>
 #include <math.h>
@@ -30,7 +31,13 @@ struct kro_mesh
     double *xf0, *dx0, *sfc0, *vol0;     /* [nblk*3], [nblk*3], [nblk*3], [nblk] */
     double *u[ 2 ], *bf[ 2 ], *w, *f[ 3 ], *ee;
     double *dtc;                         /* per block CFL minimum           */
+    kr_tree tree;                        /* blocks: levels, positions, faces */
+    int     smr;                         /* more than one level             */
 };
+
+/* logical position and per-axis block count of block b's level */
+static inline const int * blk_reg( const kro_mesh * m, int b ) { return m->tree.reg + 3 * b; }
+static inline int blk_lim( const kro_mesh * m, int b, int a ) { return m->c.nb[ a ] << m->tree.level[ b ]; }
 
 /* ------------------------------------------------------------------ */
 /* indexing                                                             */
@@ -127,12 +134,11 @@ static void set_geometry( kro_mesh * m )
 {
     for( int b = 0; b < m->nblk; ++ b )
     {
-        int reg[ 3 ] = { b % m->c.nb[ 0 ], ( b / m->c.nb[ 0 ] ) % m->c.nb[ 1 ],
-                         b / ( m->c.nb[ 0 ] * m->c.nb[ 1 ] ) };
+        const int * reg = blk_reg( m, b );
         for( int a = 0; a < 3; ++ a )
         {
             /* loc(i) = location( ( reg + i / n ) / ( i_logic_lim << level ) ) */
-            const double lim = ( double ) m->c.nb[ a ];
+            const double lim = ( double ) blk_lim( m, b, a );
             const double x0 = ( reg[ a ] + 0.0 / m->c.n[ a ] ) / lim;
             const double x1 = ( reg[ a ] + 1.0 / m->c.n[ a ] ) / lim;
             const double l0 = m->c.x_min[ a ] + x0 * ( m->c.x_max[ a ] - m->c.x_min[ a ] );
@@ -169,10 +175,40 @@ double kro_dx( const kro_mesh * m, int b, int a ) { return m->dx0[ b * 3 + a ]; 
 
 kro_mesh * kro_create( const kro_cfg * cfg )
 {
+    return kro_create_tree( cfg, 0, NULL );
+}
+
+kro_mesh * kro_create_tree( const kro_cfg * cfg, int n_regions, const kro_region * regions )
+{
     kro_mesh * m = ( kro_mesh * ) calloc( 1, sizeof( kro_mesh ) );
     m->c    = * cfg;
     m->nw   = cfg->mhd ? 8 : 5;
-    m->nblk = cfg->nb[ 0 ] * cfg->nb[ 1 ] * cfg->nb[ 2 ];
+    {   /* meshgen.cpp:51-55: an axis is periodic when its kinds say "per" */
+        int per[ 3 ];
+        kr_tree_region * rg = ( kr_tree_region * ) calloc( n_regions > 0 ? n_regions : 1, sizeof( * rg ) );
+        for( int a = 0; a < 3; ++ a )
+            per[ a ] = cfg->bc[ 2 * a ] == KRO_PER && cfg->bc[ 2 * a + 1 ] == KRO_PER;
+        for( int k = 0; k < n_regions; ++ k )
+        {
+            rg[ k ].level = regions[ k ].level;
+            for( int a = 0; a < 3; ++ a )
+            {
+                rg[ k ].x_min[ a ] = regions[ k ].x_min[ a ];
+                rg[ k ].x_max[ a ] = regions[ k ].x_max[ a ];
+            }
+        }
+        const int r = kr_tree_build( & m->tree, cfg->nb, per, cfg->x_min, cfg->x_max,
+                                     n_regions, rg, NULL, 0 );
+        free( rg );
+        if( r != 0 || ( m->tree.max_level > 0 && cfg->mhd ) )
+        {
+            kr_tree_free( & m->tree );
+            free( m );
+            return NULL;
+        }
+    }
+    m->smr  = m->tree.max_level > 0;
+    m->nblk = m->tree.nblk;
     m->ncell = ( long ) cfg->n[ 0 ] * cfg->n[ 1 ] * cfg->n[ 2 ];
     m->nw_cells = 1; m->nbf = 3; m->nee = 3;
     for( int a = 0; a < 3; ++ a )
@@ -211,9 +247,23 @@ kro_mesh * kro_create( const kro_cfg * cfg )
     return m;
 }
 
+int kro_nblk( const kro_mesh * m ) { return m->nblk; }
+
+void kro_block_info( const kro_mesh * m, int * level, int * reg )
+{
+    for( int b = 0; b < m->nblk; ++ b )
+    {
+        if( level ) level[ b ] = m->tree.level[ b ];
+        if( reg )
+            for( int a = 0; a < 3; ++ a )
+                reg[ 3 * b + a ] = m->tree.reg[ 3 * b + a ];
+    }
+}
+
 void kro_destroy( kro_mesh * m )
 {
     if( ! m ) return;
+    kr_tree_free( & m->tree );
     free( m->xf0 ); free( m->dx0 ); free( m->sfc0 ); free( m->vol0 ); free( m->dtc );
     for( int s = 0; s < 2; ++ s ) { free( m->u[ s ] ); free( m->bf[ s ] ); }
     free( m->w );
@@ -505,8 +555,7 @@ static void bc_block( kro_mesh * m, int b, void * aux )
     ( void ) aux;
     const int nw = m->nw;
     const int * n = m->c.n;
-    const int reg[ 3 ] = { b % m->c.nb[ 0 ], ( b / m->c.nb[ 0 ] ) % m->c.nb[ 1 ],
-                           b / ( m->c.nb[ 0 ] * m->c.nb[ 1 ] ) };
+    const int * reg = blk_reg( m, b );
     double * w = m->w + ( size_t ) b * m->nw_cells * nw;
     for( int side = 0; side < 6; ++ side )
     {
@@ -514,7 +563,7 @@ static void bc_block( kro_mesh * m, int b, void * aux )
         const int kind = m->c.bc[ side ];
         if( kind == KRO_PER )
             continue;
-        if( reg[ axis ] != ( right ? m->c.nb[ axis ] - 1 : 0 ) )
+        if( reg[ axis ] != ( right ? blk_lim( m, b, axis ) - 1 : 0 ) )
             continue;                        /* not on this domain edge */
         const int a1 = mod3( axis + 1 ), a2 = mod3( axis + 2 );
         const int i_mom = MOM + axis;
@@ -552,6 +601,212 @@ static void bc_block( kro_mesh * m, int b, void * aux )
             {
                 ii[ axis ] = right ? n[ axis ] - i - 1 : i;
                 memcpy( w + iw( m, ii[ 0 ], ii[ 1 ], ii[ 2 ] ), buf[ 2 + i ], sizeof( double ) * nw );
+            }
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* Static refinement, hydro: the ghost cells of a face whose neighbour   */
+/* is on another level (hydro/boundary/comm_functions.h:268-380         */
+/* to_same / to_coarser / to_finer; face neighbours only,               */
+/* keeper.cpp:86-89 desired_mode).  keeper.cpp:148-160 act_bnd runs the  */
+/* restrictions (finer -> coarser ghosts), the physical sides, the       */
+/* same-level copies and then the prolongations (coarser -> finer        */
+/* ghosts), which read the coarse block's ghosts filled before.          */
+
+static void smr_same_block( kro_mesh * m, int b, void * aux )
+{
+    ( void ) aux;
+    const int nw = m->nw;
+    const int * n = m->c.n;
+    double * w = m->w + ( size_t ) b * m->nw_cells * nw;
+    for( int f = 0; f < 6; ++ f )
+    {
+        if( m->tree.face[ 6 * b + f ] != KR_FACE_SAME )
+            continue;
+        const int a = f / 2, s = f & 1, a1 = mod3( a + 1 ), a2 = mod3( a + 2 );
+        const int src = m->tree.fnb[ ( 6 * b + f ) * 4 ];
+        const double * ws = m->w + ( size_t ) src * m->nw_cells * nw;
+        for( int g = 0; g < 2; ++ g )
+        for( int t2 = 0; t2 < n[ a2 ]; ++ t2 )
+        for( int t1 = 0; t1 < n[ a1 ]; ++ t1 )
+        {
+            int ii[ 3 ], jj[ 3 ];
+            ii[ a1 ] = jj[ a1 ] = t1;
+            ii[ a2 ] = jj[ a2 ] = t2;
+            ii[ a ] = s ? n[ a ] + g : g - 2;
+            jj[ a ] = s ? g : n[ a ] - 2 + g;
+            memcpy( w + iw( m, ii[ 0 ], ii[ 1 ], ii[ 2 ] ), ws + iw( m, jj[ 0 ], jj[ 1 ], jj[ 2 ] ),
+                    sizeof( double ) * nw );
+        }
+    }
+}
+
+/* comm_functions.h:329-380 to_coarser: a coarse ghost cell is the volume
+ * average of the 8 fine cells it covers, accumulated fine layer by fine
+ * layer in increasing index, (d1, d2) with d1 outer in each layer. */
+static void smr_restrict_block( kro_mesh * m, int b, void * aux )
+{
+    ( void ) aux;
+    const int nw = m->nw;
+    const int * n = m->c.n;
+    double * w = m->w + ( size_t ) b * m->nw_cells * nw;
+    for( int f = 0; f < 6; ++ f )
+    {
+        if( m->tree.face[ 6 * b + f ] != KR_FACE_FINE )
+            continue;
+        const int a = f / 2, s = f & 1, a1 = mod3( a + 1 ), a2 = mod3( a + 2 );
+        const int h1 = n[ a1 ] / 2, h2 = n[ a2 ] / 2;
+        for( int d1 = 0; d1 < 2; ++ d1 )
+        for( int d2 = 0; d2 < 2; ++ d2 )
+        {
+            const int fb = m->tree.fnb[ ( 6 * b + f ) * 4 + d1 * 2 + d2 ];
+            const double * wf = m->w + ( size_t ) fb * m->nw_cells * nw;
+            const double dv = m->vol0[ fb ];
+            for( int gl = 0; gl < 2; ++ gl )
+            for( int t2 = 0; t2 < h2; ++ t2 )
+            for( int t1 = 0; t1 < h1; ++ t1 )
+            {
+                double p[ 8 ] = { 0 }, norm = 0;
+                for( int kk = 0; kk < 2; ++ kk )
+                {
+                    const int k = 2 * gl + kk;       /* fine layer from offset_s */
+                    for( int e1 = 0; e1 < 2; ++ e1 )
+                    for( int e2 = 0; e2 < 2; ++ e2 )
+                    {
+                        int jj[ 3 ];
+                        jj[ a ] = s ? k : n[ a ] - 4 + k;
+                        jj[ a1 ] = 2 * t1 + e1;
+                        jj[ a2 ] = 2 * t2 + e2;
+                        const double * q = wf + iw( m, jj[ 0 ], jj[ 1 ], jj[ 2 ] );
+                        for( int c = 0; c < nw; ++ c )
+                            p[ c ] += q[ c ] * dv;
+                        norm += dv;
+                    }
+                }
+                int ii[ 3 ];
+                ii[ a ] = s ? n[ a ] + gl : gl - 2;
+                ii[ a1 ] = d1 * h1 + t1;
+                ii[ a2 ] = d2 * h2 + t2;
+                double * o = w + iw( m, ii[ 0 ], ii[ 1 ], ii[ 2 ] );
+                for( int c = 0; c < nw; ++ c )
+                    o[ c ] = p[ c ] / norm;
+            }
+        }
+    }
+}
+
+static inline double minmod( double a, double b )
+{   /* utilities/functions.h:159-170 */
+    return ( ( a < 0 ) ^ ( b < 0 ) ) ? 0 : ( fabs( a ) < fabs( b ) ? a : b );
+}
+
+/* comm_functions.h:382-447 to_finer: each coarse cell next to the face
+ * gives its 2 x 2 x 2 fine ghost cells q_c + sum over axes of
+ * +-minmod(q_r - q_c, q_c - q_l) / 4 (normal axis first, then (a+1)%3,
+ * (a+2)%3).  Blocks of one level per call (aux: the level), coarser
+ * levels first, since a coarse block's own ghosts feed its slopes. */
+typedef struct { int level; } prol_arg;
+
+static void smr_prolong_block( kro_mesh * m, int b, void * aux )
+{
+    if( m->tree.level[ b ] != ( ( const prol_arg * ) aux )->level )
+        return;
+    const int nw = m->nw;
+    const int * n = m->c.n;
+    double * w = m->w + ( size_t ) b * m->nw_cells * nw;
+    const int * rf = blk_reg( m, b );
+    for( int f = 0; f < 6; ++ f )
+    {
+        if( m->tree.face[ 6 * b + f ] != KR_FACE_COARSE )
+            continue;
+        const int a = f / 2, s = f & 1, a1 = mod3( a + 1 ), a2 = mod3( a + 2 );
+        const int h1 = n[ a1 ] / 2, h2 = n[ a2 ] / 2;
+        const int cb = m->tree.fnb[ ( 6 * b + f ) * 4 ];
+        const double * wc = m->w + ( size_t ) cb * m->nw_cells * nw;
+        const int o1 = ( rf[ a1 ] & 1 ) * h1, o2 = ( rf[ a2 ] & 1 ) * h2;
+        for( int t2 = 0; t2 < h2; ++ t2 )
+        for( int t1 = 0; t1 < h1; ++ t1 )
+        {
+            int jc[ 3 ];
+            jc[ a ] = s ? 0 : n[ a ] - 1;
+            jc[ a1 ] = o1 + t1;
+            jc[ a2 ] = o2 + t2;
+            const double * qc = wc + iw( m, jc[ 0 ], jc[ 1 ], jc[ 2 ] );
+            double dq[ 3 ][ 8 ];
+            for( int d = 0; d < 3; ++ d )
+            {
+                int jr[ 3 ] = { jc[ 0 ], jc[ 1 ], jc[ 2 ] }, jl[ 3 ] = { jc[ 0 ], jc[ 1 ], jc[ 2 ] };
+                ++ jr[ d ];
+                -- jl[ d ];
+                const double * qr = wc + iw( m, jr[ 0 ], jr[ 1 ], jr[ 2 ] );
+                const double * ql = wc + iw( m, jl[ 0 ], jl[ 1 ], jl[ 2 ] );
+                for( int c = 0; c < nw; ++ c )
+                    dq[ d ][ c ] = minmod( qr[ c ] - qc[ c ], qc[ c ] - ql[ c ] ) * 0.25f;
+            }
+            for( int k = 0; k < 2; ++ k )
+            for( int e1 = 0; e1 < 2; ++ e1 )
+            for( int e2 = 0; e2 < 2; ++ e2 )
+            {
+                int ii[ 3 ];
+                ii[ a ] = s ? n[ a ] + k : k - 2;
+                ii[ a1 ] = 2 * t1 + e1;
+                ii[ a2 ] = 2 * t2 + e2;
+                double * o = w + iw( m, ii[ 0 ], ii[ 1 ], ii[ 2 ] );
+                for( int c = 0; c < nw; ++ c )
+                    o[ c ] = qc[ c ] + dq[ a ][ c ] * ( 2 * ( k & 1 ) - 1 )
+                           + dq[ a1 ][ c ] * ( 2 * e1 - 1 )
+                           + dq[ a2 ][ c ] * ( 2 * e2 - 1 );
+            }
+        }
+    }
+}
+
+/* comm_functions.h:469-505 flux_to_buf / flux_from_buf: the coarse face
+ * flux over a refined face becomes the area average of the 4 fine face
+ * fluxes it covers ((d1, d2), d1 outer). */
+static void smr_flux_block( kro_mesh * m, int b, void * aux )
+{
+    ( void ) aux;
+    const int nw = m->nw;
+    const int * n = m->c.n;
+    for( int f = 0; f < 6; ++ f )
+    {
+        if( m->tree.face[ 6 * b + f ] != KR_FACE_FINE )
+            continue;
+        const int a = f / 2, s = f & 1, a1 = mod3( a + 1 ), a2 = mod3( a + 2 );
+        const int h1 = n[ a1 ] / 2, h2 = n[ a2 ] / 2;
+        double * fc = m->f[ a ] + ( size_t ) b * m->nf[ a ];
+        for( int d1 = 0; d1 < 2; ++ d1 )
+        for( int d2 = 0; d2 < 2; ++ d2 )
+        {
+            const int fb = m->tree.fnb[ ( 6 * b + f ) * 4 + d1 * 2 + d2 ];
+            const double * ff = m->f[ a ] + ( size_t ) fb * m->nf[ a ];
+            const double ds = m->sfc0[ fb * 3 + a ];
+            for( int t2 = 0; t2 < h2; ++ t2 )
+            for( int t1 = 0; t1 < h1; ++ t1 )
+            {
+                double acc[ 8 ] = { 0 }, norm = 0;
+                for( int e1 = 0; e1 < 2; ++ e1 )
+                for( int e2 = 0; e2 < 2; ++ e2 )
+                {
+                    int jj[ 3 ];
+                    jj[ a ] = s ? 0 : n[ a ];
+                    jj[ a1 ] = 2 * t1 + e1;
+                    jj[ a2 ] = 2 * t2 + e2;
+                    const double * fm = ff + ifl( m, a, jj[ 0 ], jj[ 1 ], jj[ 2 ] );
+                    for( int c = 0; c < nw; ++ c )
+                        acc[ c ] += fm[ c ] * ds;
+                    norm += ds;
+                }
+                int ii[ 3 ];
+                ii[ a ] = s ? n[ a ] : 0;
+                ii[ a1 ] = d1 * h1 + t1;
+                ii[ a2 ] = d2 * h2 + t2;
+                double * o = fc + ifl( m, a, ii[ 0 ], ii[ 1 ], ii[ 2 ] );
+                for( int c = 0; c < nw; ++ c )
+                    o[ c ] = acc[ c ] / norm;
             }
         }
     }
@@ -1119,6 +1374,9 @@ static void update_block( kro_mesh * m, int b, void * aux )
     double f_a[ 3 ];
     for( int a = 0; a < 3; ++ a )
         f_a[ a ] = m->sfc0[ b * 3 + a ] * dt_dv;
+    int fine[ 6 ];                       /* geometry.h refine_flag per side */
+    for( int k = 0; k < 6; ++ k )
+        fine[ k ] = m->smr && m->tree.face[ 6 * b + k ] == KR_FACE_FINE;
     for( int i2 = 0; i2 < n[ 2 ]; ++ i2 )
     for( int i1 = 0; i1 < n[ 1 ]; ++ i1 )
     for( int i0 = 0; i0 < n[ 0 ]; ++ i0 )
@@ -1135,16 +1393,40 @@ static void update_block( kro_mesh * m, int b, void * aux )
             ++ ii[ a ];
             const double * fr = m->f[ a ] + ( size_t ) b * m->nf[ a ]
                               + ifl( m, a, ii[ 0 ], ii[ 1 ], ii[ 2 ] );
+            /* load_flux_sfc: f_a = -1 (skipped) on a refined side's face */
+            const int i_a = a == 0 ? i0 : ( a == 1 ? i1 : i2 );
+            const int null_l = fine[ 2 * a ] && i_a == 0;
+            const int null_r = fine[ 2 * a + 1 ] && i_a == n[ a ] - 1;
             for( int k = 0; k < nw; ++ k )
             {
                 double res = 0;
-                if( f_a[ a ] > 0 )
+                if( f_a[ a ] > 0 && ! null_l )
                     res += f_a[ a ] * fl[ k ];
-                if( f_a[ a ] > 0 )
+                if( f_a[ a ] > 0 && ! null_r )
                     res -= f_a[ a ] * fr[ k ];
                 v[ k ] += res;
             }
         }
+        /* hydro/integrator/integrator.h:343-382 intg_flx / add_flux, after
+         * the update: the cells next to a refined side take the averaged
+         * fine flux, sides in the order z, y, x and low before high:
+         * u += ( dt * ds / ( +-vol ) ) * f */
+        for( int ax = 2; ax >= 0; -- ax )
+            for( int side = 0; side <= 1; ++ side )
+            {
+                const int i_ax = ax == 0 ? i0 : ( ax == 1 ? i1 : i2 );
+                if( ! fine[ 2 * ax + side ] || i_ax != ( side ? n[ ax ] - 1 : 0 ) )
+                    continue;
+                int jj[ 3 ] = { i0, i1, i2 };
+                jj[ ax ] = side * n[ ax ];
+                const double * fx = m->f[ ax ] + ( size_t ) b * m->nf[ ax ]
+                                  + ifl( m, ax, jj[ 0 ], jj[ 1 ], jj[ 2 ] );
+                const double ds = m->sfc0[ b * 3 + ax ];
+                const double dv = vol * ( side ? -1 : 1 );
+                const double conv = ua->dt * ds / dv;
+                for( int k = 0; k < nw; ++ k )
+                    v[ k ] += conv * fx[ k ];
+            }
         for( int k = 0; k < nw; ++ k )
             ut[ c + k ] = v[ k ];
     }
@@ -1309,14 +1591,30 @@ int kro_step( kro_mesh * m, int n_steps, double * t, double * dt_bound, double *
                     return -1;
             }
             ghost_arg ga = { stage };
-            par_blocks( m, ghost_block, & ga );
-            par_blocks( m, m->c.mhd ? bc_block_mhd : bc_block, & ga );
+            if( m->smr )
+            {   /* keeper.cpp:148-160 act_bnd */
+                par_blocks( m, smr_restrict_block, NULL );
+                par_blocks( m, bc_block, & ga );
+                par_blocks( m, smr_same_block, NULL );
+                for( int l = 1; l <= m->tree.max_level; ++ l )
+                {
+                    prol_arg pa = { l };
+                    par_blocks( m, smr_prolong_block, & pa );
+                }
+            }
+            else
+            {
+                par_blocks( m, ghost_block, & ga );
+                par_blocks( m, m->c.mhd ? bc_block_mhd : bc_block, & ga );
+            }
             const double dt = dt_use * ( stage == 0 ? 1.0 : ( double ) 0.5f );
             for( int axis = 2; axis >= 0; -- axis )
             {
                 flux_arg fa = { stage, axis };
                 par_blocks( m, flux_block, & fa );
             }
+            if( m->smr )                 /* keeper.cpp:162-166 act_flx */
+                par_blocks( m, smr_flux_block, NULL );
             upd_arg ua = { stage, dt };
             par_blocks( m, update_block, & ua );
             if( m->c.mhd )
@@ -1349,8 +1647,7 @@ int kro_init_problem( kro_mesh * m, const char * name, unsigned long long seed )
         return -1;
     for( int b = 0; b < m->nblk; ++ b )
     {
-        const int reg[ 3 ] = { b % m->c.nb[ 0 ], ( b / m->c.nb[ 0 ] ) % m->c.nb[ 1 ],
-                               b / ( m->c.nb[ 0 ] * m->c.nb[ 1 ] ) };
+        const int * reg = blk_reg( m, b );
         double * u  = m->u[ 0 ] + ( size_t ) b * m->ncell * m->nw;
         double * bf = is_ot ? m->bf[ 0 ] + ( size_t ) b * m->nbf : NULL;
         if( is_ot )
@@ -1371,7 +1668,7 @@ int kro_init_problem( kro_mesh * m, const char * name, unsigned long long seed )
             int ig[ 3 ];
             for( int a = 0; a < 3; ++ a )
                 ig[ a ] = reg[ a ] * n[ a ] + ii[ a ];
-            const uint64_t key = kr_cell_key( 0, ig, nglob );
+            const uint64_t key = kr_cell_key( m->tree.level[ b ], ig, nglob );
             double * c = u + iu( m, i0, i1, i2 );
             if( is_shock )
                 kr_shock_cell( c, kro_x_cc( m, b, 0, i0 ), m->c.gamma, seed, key );

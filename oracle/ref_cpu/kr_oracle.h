@@ -3,8 +3,10 @@
  * TEST INFRASTRUCTURE ONLY.  This is the oracle that the CUDA implementation of
  * the package is checked against; nothing in the product links or calls it.
  *
- * Scope: a uniform Cartesian mesh of nb[0] x nb[1] x nb[2] equal blocks, fully
- * periodic, two ghost layers (PLM), Heun RK2 (two stages per step).
+ * Scope: a Cartesian mesh of nb[0] x nb[1] x nb[2] root blocks, optionally
+ * statically refined (hydro: restriction / prolongation of the ghost cells
+ * across a level jump and the flux correction of the coarse side), two ghost
+ * layers (PLM), Heun RK2 (two stages per step).
  *   hydro : adiabatic EOS, PLM (van Leer harmonic limiter), HLLC.
  *   mhd   : adiabatic EOS with face-centred B, PLM, HLLD, Gardiner-Stone
  *           upwinded edge EMF (constrained transport), CT face update.
@@ -18,7 +20,8 @@
  *   u  : n0*n1*n2 cells x nw            (nw = 5 hydro, 8 MHD), no ghosts
  *   bf : (n0+5)(n1+5)(n2+5) x 3         face field on the (n+1)^3 lattice with
  *                                       2 ghost layers, as the snapshot stores it
- * Blocks are numbered lexicographically, x fastest.
+ * Blocks are numbered level by level, lexicographically (x fastest) inside a
+ * level; a uniform mesh is one level.
  */
 #ifndef KR_ORACLE_H
 #define KR_ORACLE_H
@@ -48,7 +51,24 @@ typedef struct
 
 typedef struct kro_mesh kro_mesh;
 
+/* A static refinement region ([refine_region*] section: level, x_min, x_max). */
+typedef struct
+{
+    int    level;
+    double x_min[ 3 ], x_max[ 3 ];
+} kro_region;
+
 kro_mesh * kro_create ( const kro_cfg * cfg );
+/* A mesh with static refinement (hydro only): the leaves of the block tree
+ * that the regions build (meshgen.cpp:111-160, tree.cpp:139-232), numbered
+ * level by level, lexicographically inside a level.  With no region (or only
+ * level-0 regions) this is kro_create's uniform mesh.  NULL for an MHD mesh
+ * with refinement or a region outside the domain. */
+kro_mesh * kro_create_tree( const kro_cfg * cfg, int n_regions, const kro_region * regions );
+int        kro_nblk   ( const kro_mesh * m );
+/* Level and logical position (at that level) of every block: level[nblk],
+ * reg[nblk][3]. */
+void       kro_block_info( const kro_mesh * m, int * level, int * reg );
 void       kro_destroy( kro_mesh * m );
 int        kro_nw     ( const kro_mesh * m );
 long       kro_ncell  ( const kro_mesh * m );   /* cells per block          */

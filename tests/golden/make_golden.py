@@ -8,7 +8,9 @@ small seeded workloads, reads the snapshots it writes (initial and final) and
 stores them under tests/golden/ as compressed .npz files:
 
     u0, u1      conserved state before / after the run, [nblk, n2, n1, n0, nw]
-                in lexicographic block order (x fastest)
+                in lexicographic block order (x fastest); refined meshes in
+                tree order (level, then lexicographic) with
+    level, reg  each block's level and logical position at that level
     bf0, bf1    MHD face field, owned lattice box [nblk, n2+1, n1+1, n0+1, 3]
     meta        JSON: workload, mesh, physics, steps, final time and dt
 Large cases keep only checksums (per-component sum, sum of |.|, min, max).
@@ -27,7 +29,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
-from kratos_b200.snapshot import Snapshot, to_lex_arrays  # noqa: E402
+from kratos_b200.snapshot import Snapshot, to_lex_arrays, to_tree_arrays  # noqa: E402
 
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "kratos_ref")
 
@@ -64,6 +66,19 @@ CASES = [
     ("ot_bc_fix", "ot", (2, 1, 2), (8, 8, 8), 4, 9, 1.6666666666666667,
      {"kinds": "per per per per fixd fixd", "bnd_thread_limit": "4",
       "init": {"rho0": "0.2", "pre0": "0.15", "vel0": "0 0 0", "b0": "0.1 0.05 0.2"}}, "final"),
+    # static mesh refinement, hydro ([refine_region*] sections: level, x_min,
+    # x_max); blocks are stored in tree order (level, then z, y, x) with their
+    # levels and logical positions
+    ("smr_shock", "shock", (2, 2, 2), (8, 8, 8), 5, 3, 1.4,
+     {"regions": [(1, (0.3, 0.1, 0.1), (0.45, 0.4, 0.4))]}, "full"),
+    # refined blocks on physical sides, ragged blocks, two regions
+    ("smr_bc", "shock", (3, 2, 1), (8, 16, 8), 4, 11, 1.4,
+     {"kinds": "ref out fre out per per",
+      "regions": [(1, (0.05, 0.05, 0.2), (0.2, 0.3, 0.6)), (1, (0.7, 0.8, 0.1), (0.9, 0.95, 0.2))]},
+     "final"),
+    # three levels (a level-2 region inside a level-1 one)
+    ("smr_3lvl", "shock", (1, 1, 1), (8, 8, 8), 4, 12, 1.4,
+     {"regions": [(2, (0.3, 0.3, 0.3), (0.3, 0.3, 0.3))]}, "final"),
 ]
 
 
@@ -73,6 +88,7 @@ def par_text(problem, nb, n, steps, seed, gamma, extra, prefix):
     extra = dict(extra)
     kinds = extra.pop("kinds", "per per per per per per")
     init = extra.pop("init", {})
+    regions = extra.pop("regions", [])
     dyn.update(extra)
     lines = [
         "[problem]", "name = %s" % problem, "seed = %d" % seed, "",
@@ -84,6 +100,9 @@ def par_text(problem, nb, n, steps, seed, gamma, extra, prefix):
         "", "[boundary]", "kinds = %s" % kinds, ""]
     if init:
         lines += ["[init]"] + ["%s = %s" % kv for kv in init.items()] + [""]
+    for k, (level, lo, hi) in enumerate(regions):
+        lines += ["[refine_region_%c]" % "abcdefghij"[k], "level = %d" % level,
+                  "x_min = %r %r %r" % tuple(lo), "x_max = %r %r %r" % tuple(hi), ""]
     return "\n".join(lines)
 
 
@@ -105,8 +124,13 @@ def run_case(name, problem, nb, n, steps, seed, gamma, extra, keep):
         subprocess.check_call([REF_BIN, par], cwd=tmp, stdout=subprocess.DEVNULL)
         s0 = Snapshot.read(prefix + "_00000.bin")
         s1 = Snapshot.read(prefix + "_00001.bin")
-    u0, bf0 = to_lex_arrays(s0, nb)
-    u1, bf1 = to_lex_arrays(s1, nb)
+    if extra.get("regions"):
+        level, reg, u0, bf0 = to_tree_arrays(s0)
+        level1, reg1, u1, bf1 = to_tree_arrays(s1)
+        assert np.array_equal(level, level1) and np.array_equal(reg, reg1)
+    else:
+        u0, bf0 = to_lex_arrays(s0, nb)
+        u1, bf1 = to_lex_arrays(s1, nb)
     if int(s1.array("cycle", "i")[0]) != steps - 1 or not float(s1.array("time")[0]) > 0:
         raise RuntimeError("%s: the reference run stopped early" % name)
     meta = {
@@ -116,6 +140,8 @@ def run_case(name, problem, nb, n, steps, seed, gamma, extra, keep):
         "cycle": int(s1.array("cycle", "i")[0]),
     }
     out = {"meta": np.array(json.dumps(meta))}
+    if extra.get("regions"):
+        out["level"], out["reg"] = level, reg
     if keep == "full":
         out["u0"] = u0
         if bf0 is not None:

@@ -6,7 +6,10 @@ import numpy as np
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 CASES = ["shock_16", "ot_16", "ot_ragged", "shock_floor", "shock_c1", "ot_64",
-         "shock_bc", "shock_fixd", "ot_bc_out", "ot_bc_ref", "ot_bc_fre"]
+         "shock_bc", "shock_fixd", "ot_bc_out", "ot_bc_ref", "ot_bc_fre",
+         "smr_shock", "smr_bc", "smr_3lvl"]
+# statically refined fixtures (blocks in tree order, with level / reg arrays)
+SMR_CASES = ["smr_shock", "smr_bc", "smr_3lvl"]
 # fixtures compared within a tolerance, not bit for bit: name -> relative L1
 # bound per conserved field.  ot_bc_fix: the reference's MHD fixed sides give
 # results that vary between identical runs (relative L1 ~1.1e-3 after 4 steps)
@@ -23,6 +26,11 @@ def boundary(meta):
         [float(x) for x in init.get("vel0", "0 0 0").split()]
     b_fix = [float(x) for x in init.get("b0", "0 0 0").split()]
     return kinds, w_fix, b_fix
+
+
+def regions(meta):
+    """Static refinement regions of a fixture: [(level, x_min, x_max)]."""
+    return [(int(l), tuple(lo), tuple(hi)) for l, lo, hi in meta.get("dynamics", {}).get("regions", [])]
 
 
 def load(name):

@@ -18,10 +18,10 @@ def _mesh(meta):
     kinds, w_fix, b_fix = G.boundary(meta)
     return OracleMesh(meta["workload"] == "ot", meta["nb"], meta["n"], meta["gamma"],
                       cfl=meta["cfl"], t_floor=float(extra.get("tmp_floor", 1e-9)),
-                      kinds=kinds, w_fix=w_fix, b_fix=b_fix)
+                      kinds=kinds, w_fix=w_fix, b_fix=b_fix, regions=G.regions(meta))
 
 
-@pytest.mark.parametrize("name", ["shock_16", "ot_16"])
+@pytest.mark.parametrize("name", ["shock_16", "ot_16", "smr_shock"])
 def test_initial_state_bit_exact(name):
     meta, g = G.load(name)
     m = _mesh(meta)
@@ -75,7 +75,6 @@ def test_floor_case_triggers_floor():
 def test_hllc_symmetry():
     """Mirror symmetry of the restated HLLC: swapping left/right and flipping the
     normal velocity negates the mass and energy fluxes."""
-    from oracle import kr_oracle as K
     rng = np.random.default_rng(0)
     for _ in range(50):
         ql = np.array([rng.uniform(.1, 2), rng.uniform(.1, 2), *rng.uniform(-1, 1, 3)])
@@ -94,7 +93,6 @@ def test_hlld_consistency():
     """For identical left and right states the HLLD flux is the physical flux
     (consistency), with the normal B flux zero and the transverse ones remapped
     to the edge EMF E = -v x B."""
-    from oracle import kr_oracle as K
     rng = np.random.default_rng(1)
     gam = 5 / 3
     for _ in range(50):
@@ -126,3 +124,32 @@ def test_step_within_reference_spread(name):
     for k in range(u.shape[-1]):
         e = np.abs(u[..., k] - g["u1"][..., k]).sum() / np.abs(g["u1"][..., k]).sum()
         assert e <= G.SPREAD_CASES[name], (k, e)
+
+
+@pytest.mark.parametrize("name", G.SMR_CASES)
+def test_refined_tree_matches_reference(name):
+    """The block tree that the refinement regions build (leaves, their levels
+    and logical positions) is the reference's, block for block."""
+    meta, g = G.load(name)
+    m = _mesh(meta)
+    assert np.array_equal(m.level, g["level"])
+    assert np.array_equal(m.reg, g["reg"])
+    assert m.level.max() >= 1
+
+
+def test_refined_fixtures_exercise_every_level_jump():
+    """The refined fixtures hold coarse / fine faces on every axis, across a
+    physical side's neighbour and between levels 1 and 2."""
+    seen = set()
+    for name in G.SMR_CASES:
+        meta, g = G.load(name)
+        lv = g["level"]
+        seen.add(("levels", int(lv.max())))
+        for b in range(len(lv)):
+            for c in range(len(lv)):
+                d = g["reg"][c] - (g["reg"][b] << (lv[c] - lv[b])) if lv[c] >= lv[b] else None
+                if d is not None and lv[c] == lv[b] + 1:
+                    for a in range(3):
+                        if d[a] in (-1, 2) and all(0 <= d[x] <= 1 for x in range(3) if x != a):
+                            seen.add(("fine", a))
+    assert {("fine", 0), ("fine", 1), ("fine", 2), ("levels", 2)} <= seen
