@@ -75,6 +75,7 @@ def test_floor_case_triggers_floor():
 def test_hllc_symmetry():
     """Mirror symmetry of the restated HLLC: swapping left/right and flipping the
     normal velocity negates the mass and energy fluxes."""
+    from oracle import kr_oracle as K
     rng = np.random.default_rng(0)
     for _ in range(50):
         ql = np.array([rng.uniform(.1, 2), rng.uniform(.1, 2), *rng.uniform(-1, 1, 3)])
@@ -93,6 +94,7 @@ def test_hlld_consistency():
     """For identical left and right states the HLLD flux is the physical flux
     (consistency), with the normal B flux zero and the transverse ones remapped
     to the edge EMF E = -v x B."""
+    from oracle import kr_oracle as K
     rng = np.random.default_rng(1)
     gam = 5 / 3
     for _ in range(50):
