@@ -8,6 +8,8 @@
  *   cons2prim + CFL dt       hydro/eos/adiabatic.h:211-258, mhd/eos/adiabatic.h:127-234
  *   ghost fill (same level)  hydro/boundary/comm_functions.h:306-483,
  *                            mhd/boundary/comm_functions.h:433-815
+ *   level jumps (hydro SMR)  hydro/boundary/comm_functions.h:329-505,
+ *                            hydro/integrator/integrator.h:343-382
  *   PLM + HLLC / HLLD flux   prototypes/integrator.h:107-125 flux_kernel,
  *                            hydro/reconstruct/plm.h, hydro/riemann/hllc.h,
  *                            mhd/riemann/hlld.h
@@ -19,7 +21,8 @@
  *
  * Conventions
  *   - Blocks: a uniform mesh of nb[0] x nb[1] x nb[2] blocks of n[0] x n[1] x
- *     n[2] cells, numbered lexicographically (x fastest).
+ *     n[2] cells, numbered lexicographically (x fastest); a statically refined
+ *     mesh (kr_ctx_create_refined) numbers its blocks level by level.
  *     A sharded context (n_ranks > 1, below) holds a subset of them.
  *   - Host state arrays use the reference's per-block layouts (dat_3d_t,
  *     src/mesh/types/dat_3d.h:153-156, field index fastest), blocks in
@@ -107,6 +110,31 @@ void        kr_cfg_default( kr_cfg * cfg );
 kr_ctx *    kr_ctx_create ( const kr_cfg * cfg );
 void        kr_ctx_destroy( kr_ctx * ctx );
 const char* kr_last_error ( const kr_ctx * ctx );
+
+/* Static mesh refinement (hydro, one rank) -------------------------------
+ * A region is one [refine_region*] section of the parameter file
+ * (meshgen.cpp:111-160 load_refinement): every level-`level` block holding a
+ * point of the box x_min..x_max is created, together with its ancestors and
+ * their neighbours, so adjacent blocks differ by at most one level
+ * (tree.cpp:139-232 insert).  The context's blocks are the tree's leaves,
+ * numbered level by level and lexicographically (x fastest) inside a level;
+ * every block has n cells, a level-L block a cell size 2^-L of the root's.
+ * Each stage fills the ghosts across a level jump (restriction of the fine
+ * side, prolongation with minmod slopes of the coarse side,
+ * hydro/boundary/comm_functions.h:329-447) and corrects the coarse cells
+ * next to a refined side with the area-averaged fine flux
+ * (comm_functions.h:469-505, hydro/integrator/integrator.h:343-382).
+ * With no region of level >= 1 this is kr_ctx_create.  Host state arrays hold
+ * the blocks in this order; kr_block_info gives each block's level and
+ * logical position (reg[3 b + a], at its level) and returns the count. */
+typedef struct
+{
+    int    level;
+    double x_min[ 3 ], x_max[ 3 ];
+} kr_region;
+
+kr_ctx *    kr_ctx_create_refined( const kr_cfg * cfg, int n_regions, const kr_region * regions );
+int         kr_block_info        ( kr_ctx * ctx, int * level, int * reg );
 
 /* Optional: run on a caller-owned stream (a cudaStream_t passed as void*). */
 int kr_set_stream( kr_ctx * ctx, void * stream );

@@ -39,6 +39,14 @@ class kr_cfg(ctypes.Structure):
     ]
 
 
+class kr_region(ctypes.Structure):
+    _fields_ = [
+        ("level", ctypes.c_int),
+        ("x_min", ctypes.c_double * 3),
+        ("x_max", ctypes.c_double * 3),
+    ]
+
+
 # name -> (restype, argtypes); every symbol include/kratos_b200.h declares
 _dp = ctypes.POINTER(ctypes.c_double)
 _vp = ctypes.c_void_p
@@ -46,6 +54,8 @@ SIGNATURES = {
     "kr_cfg_default": (None, [ctypes.POINTER(kr_cfg)]),
     "kr_ctx_create": (_vp, [ctypes.POINTER(kr_cfg)]),
     "kr_ctx_destroy": (None, [_vp]),
+    "kr_ctx_create_refined": (_vp, [ctypes.POINTER(kr_cfg), ctypes.c_int, ctypes.POINTER(kr_region)]),
+    "kr_block_info": (ctypes.c_int, [_vp, _vp, _vp]),
     "kr_last_error": (ctypes.c_char_p, [_vp]),
     "kr_set_stream": (ctypes.c_int, [_vp, _vp]),
     "kr_init_problem": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_uint64]),

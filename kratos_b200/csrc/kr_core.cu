@@ -17,6 +17,7 @@
 #include "kr_fast.cuh"
 #include "kr_mlp.cuh"
 #include "problems.h"
+#include "smr_tree.h"
 
 #include <cuda_runtime.h>
 #include <dlfcn.h>
@@ -54,6 +55,18 @@ struct scal_t
 struct geo_t
 {
     double dx[ 3 ], sfc[ 3 ], vol;
+    int phys;                     // bit 2a+s: side (a, s) is a non-periodic domain side
+    int fine;                     // bit 2a+s: the neighbours across side (a, s) are finer
+    int fitem[ 6 ];               // refined side: first of its 4 flux-average items
+};
+
+// Static refinement: one (block, face) pair across a level jump.  dst / src:
+// the block written / read; face: the written block's side 2a+s; o1, o2: the
+// cell offsets (along (a+1)%3, (a+2)%3) of the fine block's half inside the
+// coarse block.
+struct smr_item_t
+{
+    int dst, src, face, o1, o2;
 };
 
 // Kernel parameters (by value).
@@ -94,6 +107,8 @@ struct args_t
     double w_fix[ 5 ];
     double b_fix[ 3 ];
     int emf_out;                      // bit a: high side of axis a is out / fre (MHD)
+    double * favg;                    // refined mesh: averaged fine face fluxes,
+    int favg_n;                       //   [item][5][favg_n] (FP64 in both precisions)
     scal_t * s;
 };
 
@@ -444,12 +459,8 @@ __global__ void __launch_bounds__( 128 ) k_phys( const args_t< R > a )
     const int b = blockIdx.z, side = blockIdx.y;
     const int axis = side >> 1, right = side & 1;
     const int kind = a.bc[ side ];
-    if( kind == KR_BC_PER )
-        return;
-    const int g = a.gid[ b ];
-    const int reg[ 3 ] = { g % a.nbk[ 0 ], ( g / a.nbk[ 0 ] ) % a.nbk[ 1 ], g / ( a.nbk[ 0 ] * a.nbk[ 1 ] ) };
-    if( reg[ axis ] != ( right ? a.nbk[ axis ] - 1 : 0 ) )
-        return;
+    if( ! ( ( a.geo[ b ].phys >> side ) & 1 ) )
+        return;                              // periodic, or not on this domain side
     const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
     const int a1 = mod3( axis + 1 ), a2 = mod3( axis + 2 );
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -481,6 +492,142 @@ __global__ void __launch_bounds__( 128 ) k_phys( const args_t< R > a )
             a.w[ iw( a, b, k, 5, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] = v;
         }
     }
+}
+
+////////////////////////////////////////////////////////////
+// Static refinement, hydro (hydro/boundary/comm_functions.h:329-505,
+// keeper.cpp:148-166): ghost cells across a level jump and the coarse side's
+// face flux.  Arithmetic in FP64 from the stored words, in the reference's
+// order; one item per (coarse block, face, fine child) or (fine block, face).
+
+__device__ __forceinline__ void smr_axes( int face, int & ax, int & a1, int & a2, int & s )
+{
+    ax = face >> 1; s = face & 1; a1 = mod3( ax + 1 ); a2 = mod3( ax + 2 );
+}
+
+// to_coarser: each of the 2 ghost layers x (n1/2) x (n2/2) coarse cells that a
+// fine child covers is the volume average of its 8 fine cells, accumulated
+// fine layer by layer, (d1, d2) with d1 outer.
+template< class R >
+__global__ void __launch_bounds__( 128 ) k_restrict( const args_t< R > a, const smr_item_t * items )
+{
+    const smr_item_t it = items[ blockIdx.y ];
+    int ax, a1, a2, s;
+    smr_axes( it.face, ax, a1, a2, s );
+    const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
+    const int h1 = nn[ a1 ] >> 1, h2 = nn[ a2 ] >> 1;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if( t >= 2 * h1 * h2 )
+        return;
+    const int t1 = t % h1, t2 = ( t / h1 ) % h2, gl = t / ( h1 * h2 );
+    const double dv = a.geo[ it.src ].vol;
+    double p[ 5 ] = { 0, 0, 0, 0, 0 }, norm = 0;
+    for( int kk = 0; kk < 2; ++ kk )
+        for( int e1 = 0; e1 < 2; ++ e1 )
+            for( int e2 = 0; e2 < 2; ++ e2 )
+            {
+                const int k = 2 * gl + kk;
+                int jj[ 3 ];
+                jj[ ax ] = s ? k : nn[ ax ] - 4 + k;
+                jj[ a1 ] = 2 * t1 + e1;
+                jj[ a2 ] = 2 * t2 + e2;
+                for( int c = 0; c < 5; ++ c )
+                    p[ c ] += double( a.w[ iw( a, it.src, c, 5, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) ] ) * dv;
+                norm += dv;
+            }
+    int ii[ 3 ];
+    ii[ ax ] = s ? nn[ ax ] + gl : gl - 2;
+    ii[ a1 ] = it.o1 + t1;
+    ii[ a2 ] = it.o2 + t2;
+    for( int c = 0; c < 5; ++ c )
+        a.w[ iw( a, it.dst, c, 5, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] = R( p[ c ] / norm );
+}
+
+__device__ __forceinline__ double minmod( double x, double y )
+{   // utilities/functions.h:159-170
+    return ( ( x < 0 ) ^ ( y < 0 ) ) ? 0. : ( fabs( x ) < fabs( y ) ? x : y );
+}
+
+// to_finer: every coarse cell next to the face gives its 2 x 2 x 2 fine ghost
+// cells q_c + sum over the axes (normal, (a+1)%3, (a+2)%3) of
+// +-minmod(q_r - q_c, q_c - q_l) / 4.  Reads the coarse block's ghosts, so it
+// runs after the restriction, the same-level fill and the physical sides.
+template< class R >
+__global__ void __launch_bounds__( 128 ) k_prolong( const args_t< R > a, const smr_item_t * items )
+{
+    const smr_item_t it = items[ blockIdx.y ];
+    int ax, a1, a2, s;
+    smr_axes( it.face, ax, a1, a2, s );
+    const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
+    const int h1 = nn[ a1 ] >> 1, h2 = nn[ a2 ] >> 1;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if( t >= h1 * h2 )
+        return;
+    const int t1 = t % h1, t2 = t / h1;
+    int jc[ 3 ];
+    jc[ ax ] = s ? 0 : nn[ ax ] - 1;
+    jc[ a1 ] = it.o1 + t1;
+    jc[ a2 ] = it.o2 + t2;
+    for( int c = 0; c < 5; ++ c )
+    {
+        const double qc = double( a.w[ iw( a, it.src, c, 5, jc[ 0 ], jc[ 1 ], jc[ 2 ] ) ] );
+        double dq[ 3 ];
+        for( int d = 0; d < 3; ++ d )
+        {
+            int jr[ 3 ] = { jc[ 0 ], jc[ 1 ], jc[ 2 ] }, jl[ 3 ] = { jc[ 0 ], jc[ 1 ], jc[ 2 ] };
+            ++ jr[ d ];
+            -- jl[ d ];
+            const double qr = double( a.w[ iw( a, it.src, c, 5, jr[ 0 ], jr[ 1 ], jr[ 2 ] ) ] );
+            const double ql = double( a.w[ iw( a, it.src, c, 5, jl[ 0 ], jl[ 1 ], jl[ 2 ] ) ] );
+            dq[ d ] = minmod( qr - qc, qc - ql ) * 0.25;
+        }
+        for( int k = 0; k < 2; ++ k )
+            for( int e1 = 0; e1 < 2; ++ e1 )
+                for( int e2 = 0; e2 < 2; ++ e2 )
+                {
+                    int ii[ 3 ];
+                    ii[ ax ] = s ? nn[ ax ] + k : k - 2;
+                    ii[ a1 ] = 2 * t1 + e1;
+                    ii[ a2 ] = 2 * t2 + e2;
+                    const double q = qc + dq[ ax ] * double( 2 * ( k & 1 ) - 1 )
+                                   + dq[ a1 ] * double( 2 * e1 - 1 )
+                                   + dq[ a2 ] * double( 2 * e2 - 1 );
+                    a.w[ iw( a, it.dst, c, 5, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] = R( q );
+                }
+    }
+}
+
+// flux_to_buf / flux_from_buf: the coarse face flux over a refined side is the
+// area average of the 4 fine face fluxes it covers ((d1, d2), d1 outer).  Kept
+// in FP64 (a.favg) in both precisions, so the coarse correction carries the
+// fine fluxes without a rounding to the flux word type.
+template< class R >
+__global__ void __launch_bounds__( 128 ) k_flux_avg( const args_t< R > a, const smr_item_t * items )
+{
+    const smr_item_t it = items[ blockIdx.y ];
+    int ax, a1, a2, s;
+    smr_axes( it.face, ax, a1, a2, s );
+    const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
+    const int h1 = nn[ a1 ] >> 1, h2 = nn[ a2 ] >> 1;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if( t >= h1 * h2 )
+        return;
+    const int t1 = t % h1, t2 = t / h1;
+    const double ds = a.geo[ it.src ].sfc[ ax ];
+    double acc[ 5 ] = { 0, 0, 0, 0, 0 }, norm = 0;
+    for( int e1 = 0; e1 < 2; ++ e1 )
+        for( int e2 = 0; e2 < 2; ++ e2 )
+        {
+            int jj[ 3 ];
+            jj[ ax ] = s ? 0 : nn[ ax ];
+            jj[ a1 ] = 2 * t1 + e1;
+            jj[ a2 ] = 2 * t2 + e2;
+            for( int c = 0; c < 5; ++ c )
+                acc[ c ] += double( a.f[ ax ][ ifx( a, it.src, c, 5, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) ] ) * ds;
+            norm += ds;
+        }
+    for( int c = 0; c < 5; ++ c )
+        a.favg[ ( ( size_t ) blockIdx.y * 5 + c ) * a.favg_n + t ] = acc[ c ] / norm;
 }
 
 ////////////////////////////////////////////////////////////
@@ -1123,7 +1270,31 @@ __global__ void __launch_bounds__( 256 ) k_emf( const args_t< R > a, udiv_t dv )
 // rk2.h:404-425 load) and CT face update (mhd/integrator/integrator.h:385-462,
 // mhd/integrator/rk2.h:244-258 set_field).  One thread per lattice site.
 
-template< bool MHD, class R >
+// Static refinement (SMR): the face of a refined side is left out of the
+// update (load_flux_sfc, f_a = -1), and afterwards the cell takes the
+// averaged fine flux of that face, sides z, y, x and low before high
+// (hydro/integrator/integrator.h:343-382 intg_flx / add_flux):
+// u += ( dt * ds / ( +-vol ) ) * f.
+template< class R > __device__ __forceinline__
+double smr_correct( const args_t< R > & a, const geo_t & g, int b, const int * i, const int * nn,
+                    int k, double dt, double v )
+{
+    for( int ax = 2; ax >= 0; -- ax )
+        for( int side = 0; side <= 1; ++ side )
+            if( ( ( g.fine >> ( 2 * ax + side ) ) & 1 ) && i[ ax ] == ( side ? nn[ ax ] - 1 : 0 ) )
+            {
+                const int a1 = mod3( ax + 1 ), a2 = mod3( ax + 2 );
+                const int h1 = nn[ a1 ] >> 1, h2 = nn[ a2 ] >> 1;
+                const int d1 = i[ a1 ] >= h1, d2 = i[ a2 ] >= h2;
+                const int item = g.fitem[ 2 * ax + side ] + 2 * d1 + d2;
+                const int t = ( i[ a2 ] - d2 * h2 ) * h1 + ( i[ a1 ] - d1 * h1 );
+                const double conv = dt * g.sfc[ ax ] / ( g.vol * ( side ? -1 : 1 ) );
+                v += conv * a.favg[ ( ( size_t ) item * 5 + k ) * a.favg_n + t ];
+            }
+    return v;
+}
+
+template< bool MHD, class R, bool SMR = false >
 __global__ void __launch_bounds__( 256 ) k_update( const args_t< R > a, int step, udiv_t dv )
 {
     // grid: x over the lattice sites of one (x, y) plane, y over z, z over blocks
@@ -1168,10 +1339,14 @@ __global__ void __launch_bounds__( 256 ) k_update( const args_t< R > a, int step
                 {
                     const double f_a = g.sfc[ d ] * dt_dv;
                     double res = 0;
-                    res += f_a * double( fl[ d ][ k ] );
-                    res -= f_a * double( fr[ d ][ k ] );
+                    if( ! SMR || ! ( ( ( g.fine >> ( 2 * d ) ) & 1 ) && i[ d ] == 0 ) )
+                        res += f_a * double( fl[ d ][ k ] );
+                    if( ! SMR || ! ( ( ( g.fine >> ( 2 * d + 1 ) ) & 1 ) && i[ d ] == nn[ d ] - 1 ) )
+                        res -= f_a * double( fr[ d ][ k ] );
                     v[ k ] += res;
                 }
+                if constexpr( SMR )
+                    v[ k ] = smr_correct( a, g, b, i, nn, k, dt, v[ k ] );
                 ut[ c0 + k * a.nc ] = v[ k ];
             }
         }
@@ -1184,10 +1359,14 @@ __global__ void __launch_bounds__( 256 ) k_update( const args_t< R > a, int step
                 {
                     const double f_a = g.sfc[ d ] * dt_dv;
                     double res = 0;
-                    res += f_a * double( F[ d ][ o + k * a.nfb ] );
-                    res -= f_a * double( F[ d ][ o + k * a.nfb + s1[ d ] ] );
+                    if( ! SMR || ! ( ( ( g.fine >> ( 2 * d ) ) & 1 ) && i[ d ] == 0 ) )
+                        res += f_a * double( F[ d ][ o + k * a.nfb ] );
+                    if( ! SMR || ! ( ( ( g.fine >> ( 2 * d + 1 ) ) & 1 ) && i[ d ] == nn[ d ] - 1 ) )
+                        res -= f_a * double( F[ d ][ o + k * a.nfb + s1[ d ] ] );
                     v += res;
                 }
+                if constexpr( SMR )
+                    v = smr_correct( a, g, b, i, nn, k, dt, v );
                 ut[ c ] = v;
             }
     }
@@ -1646,6 +1825,14 @@ struct kr_ctx
     double * recv_b = nullptr;
     int halo_grid = 1;                 // CTAs per item of k_halo
     ncclComm_t comm = nullptr;
+    // static refinement (hydro, one rank): blocks are the tree's leaves
+    bool smr = false;
+    int max_level = 0;
+    std::vector< int > lvl_h, reg_h;   // per block: level, logical position (3)
+    smr_item_t * smr_items = nullptr;  // [restriction / flux-average items | prolongation items by level]
+    double * favg = nullptr;           // averaged fine fluxes of the flux-average items
+    int n_restrict = 0;
+    std::vector< int > prolong_off;    // prolongation items of level l: [prolong_off[l - 1], prolong_off[l])
 };
 
 static thread_local std::string g_create_error;
@@ -1662,6 +1849,13 @@ static bool ck( kr_ctx * c, cudaError_t e, const char * what )
     else
         g_create_error = std::string( what ) + ": " + cudaGetErrorString( e );
     return false;
+}
+
+static long long smr_half_sites( const kr_ctx * c )
+{   // largest (n1 / 2) x (n2 / 2) over the three face orientations
+    const int * n = c->cfg.n;
+    return std::max( { ( long long )( n[ 1 ] / 2 ) * ( n[ 2 ] / 2 ), ( long long )( n[ 0 ] / 2 ) * ( n[ 2 ] / 2 ),
+                       ( long long )( n[ 0 ] / 2 ) * ( n[ 1 ] / 2 ) } );
 }
 
 template< class R >
@@ -1683,6 +1877,7 @@ static args_t< R > make_args( kr_ctx * c )
     for( int d = 0; d < 3; ++ d ) a.f[ d ] = ( R * ) c->f[ d ];
     a.ee = ( R * ) c->ee;
     a.geo = c->geo; a.nbr = c->nbr; a.gid = c->gid; a.s = c->s;
+    a.favg = c->favg; a.favg_n = int( smr_half_sites( c ) );
     for( int d = 0; d < 3; ++ d ) a.nbk[ d ] = c->cfg.nb[ d ];
     for( int k = 0; k < 6; ++ k ) a.bc[ k ] = c->cfg.bc[ k ];
     for( int k = 0; k < 5; ++ k ) a.w_fix[ k ] = c->cfg.w_fix[ k ];
@@ -1831,8 +2026,16 @@ static void enqueue_back( kr_ctx * c, cudaStream_t st, const args_t< R > & a, in
             k_halo< MHD, R, false ><<< dim3( c->halo_grid, unsigned( c->hrecv.items.size(  ) ) ), 256, 0, st >>>(
                 a, c->recv_items, ( R * ) c->recv_w, c->recv_b, stage );
         k_ghost< MHD, R ><<< dim3( blocks_for( nghost, 256 ), nb ), 256, 0, st >>>( a, stage, make_ghost_div( n ) );
+        if( c->n_restrict )            // finer -> coarser ghosts
+            k_restrict< R ><<< dim3( blocks_for( 2 * smr_half_sites( c ), 128 ), c->n_restrict ), 128, 0, st >>>( a, c->smr_items );
         if( ! MHD && has_phys( c ) )
             k_phys< R ><<< dim3( blocks_for( phys_sites( c ), 128 ), 6, nb ), 128, 0, st >>>( a );
+        for( int l = 1; l <= c->max_level; ++ l )
+        {   // coarser -> finer ghosts, coarser levels first
+            const int i0 = c->prolong_off[ l - 1 ], cnt = c->prolong_off[ l ] - i0;
+            if( cnt )
+                k_prolong< R ><<< dim3( blocks_for( smr_half_sites( c ), 128 ), cnt ), 128, 0, st >>>( a, c->smr_items + i0 );
+        }
         if( MHD )
             for( int side = 0; side < 6; ++ side )
                 if( c->cfg.bc[ side ] != KR_BC_PER )
@@ -1846,7 +2049,17 @@ static void enqueue_back( kr_ctx * c, cudaStream_t st, const args_t< R > & a, in
     if( MHD )
         timed( 5, [ & ] { k_emf< R ><<< dim3( blocks_for( ( long long )( n[ 0 ] + 1 ) * ( n[ 1 ] + 1 ), 256 ), n[ 2 ] + 1, nb ), 256, 0, st >>>(
             a, make_udiv( unsigned( n[ 0 ] + 1 ) ) ); } );
-    timed( 6, [ & ] { k_update< MHD, R ><<< dim3( blocks_for( ( long long )( n[ 0 ] + 1 ) * ( n[ 1 ] + 1 ), 256 ), n[ 2 ] + 1, nb ), 256, 0, st >>>( a, stage, make_udiv( unsigned( n[ 0 ] + 1 ) ) ); } );
+    const dim3 ug( blocks_for( ( long long )( n[ 0 ] + 1 ) * ( n[ 1 ] + 1 ), 256 ), n[ 2 ] + 1, nb );
+    if constexpr( ! MHD )
+        if( c->smr )
+        {
+            timed( 6, [ & ] {
+                if( c->n_restrict )      // coarse face flux over a refined side
+                    k_flux_avg< R ><<< dim3( blocks_for( smr_half_sites( c ), 128 ), c->n_restrict ), 128, 0, st >>>( a, c->smr_items );
+                k_update< MHD, R, true ><<< ug, 256, 0, st >>>( a, stage, make_udiv( unsigned( n[ 0 ] + 1 ) ) ); } );
+            return;
+        }
+    timed( 6, [ & ] { k_update< MHD, R ><<< ug, 256, 0, st >>>( a, stage, make_udiv( unsigned( n[ 0 ] + 1 ) ) ); } );
 }
 
 // Halo transfer of one stage between this rank and its peers, and at stage 0
@@ -1998,12 +2211,17 @@ static void set_geometry( kr_ctx * c )
     c->geo_h.resize( c->nblk );
     for( int b = 0; b < c->nblk; ++ b )
     {
-        const int gb = c->gid_h[ b ];
-        const int reg[ 3 ] = { gb % g.nb[ 0 ], ( gb / g.nb[ 0 ] ) % g.nb[ 1 ], gb / ( g.nb[ 0 ] * g.nb[ 1 ] ) };
+        const int * reg = & c->reg_h[ 3 * b ];
+        const int lvl = c->lvl_h[ b ];
         geo_t & o = c->geo_h[ b ];
+        o.phys = o.fine = 0;
+        for( int f = 0; f < 6; ++ f ) o.fitem[ f ] = -1;
+        for( int side = 0; side < 6; ++ side )
+            if( g.bc[ side ] != KR_BC_PER && reg[ side / 2 ] == ( side & 1 ? ( g.nb[ side / 2 ] << lvl ) - 1 : 0 ) )
+                o.phys |= 1 << side;
         for( int a = 0; a < 3; ++ a )
-        {
-            const double lim = double( g.nb[ a ] );
+        {   // loc(i) = location( ( reg + i / n ) / ( i_logic_lim << level ) )
+            const double lim = double( g.nb[ a ] << lvl );
             const double x0 = ( reg[ a ] + 0.0 / g.n[ a ] ) / lim;
             const double x1 = ( reg[ a ] + 1.0 / g.n[ a ] ) / lim;
             const double l0 = g.x_min[ a ] + x0 * ( g.x_max[ a ] - g.x_min[ a ] );
@@ -2023,11 +2241,10 @@ static void set_geometry( kr_ctx * c )
     }
 }
 
-// Cell centre of cell i along axis a of global block gb.
-static double x_cc( const kr_cfg & g, int gb, int a, int i )
+// Cell centre of cell i along axis a of a block at `reg` on level lvl.
+static double x_cc( const kr_cfg & g, const int * reg, int lvl, int a, int i )
 {
-    const int reg[ 3 ] = { gb % g.nb[ 0 ], ( gb / g.nb[ 0 ] ) % g.nb[ 1 ], gb / ( g.nb[ 0 ] * g.nb[ 1 ] ) };
-    const double lim = double( g.nb[ a ] );
+    const double lim = double( g.nb[ a ] << lvl );
     const double x0 = ( reg[ a ] + 0.0 / g.n[ a ] ) / lim;
     const double x1 = ( reg[ a ] + 1.0 / g.n[ a ] ) / lim;
     const double l0 = g.x_min[ a ] + x0 * ( g.x_max[ a ] - g.x_min[ a ] );
@@ -2055,7 +2272,85 @@ const char * kr_last_error( const kr_ctx * c )
     return c ? c->err.c_str(  ) : g_create_error.c_str(  );
 }
 
-kr_ctx * kr_ctx_create( const kr_cfg * cfg )
+}   // extern "C"
+
+// The tree of a refined mesh (meshgen.cpp:111-160 load_refinement /
+// generate_tree); false with g_create_error set on a bad region or setup.
+static bool build_tree( const kr_cfg * cfg, int n_regions, const kr_region * regions, kr_tree & tree )
+{
+    int per[ 3 ];
+    for( int a = 0; a < 3; ++ a )
+        per[ a ] = cfg->bc[ 2 * a ] == KR_BC_PER && cfg->bc[ 2 * a + 1 ] == KR_BC_PER;
+    std::vector< kr_tree_region > rg( std::max( 1, n_regions ) );
+    for( int k = 0; k < n_regions; ++ k )
+    {
+        rg[ k ].level = regions[ k ].level;
+        for( int a = 0; a < 3; ++ a )
+        {
+            rg[ k ].x_min[ a ] = regions[ k ].x_min[ a ];
+            rg[ k ].x_max[ a ] = regions[ k ].x_max[ a ];
+        }
+    }
+    char err[ 128 ] = { 0 };
+    if( kr_tree_build( & tree, cfg->nb, per, cfg->x_min, cfg->x_max, n_regions, rg.data(  ), err, sizeof( err ) - 1 ) != 0 )
+    {
+        g_create_error = std::string( "kr_ctx_create_refined: " ) + err;
+        return false;
+    }
+    if( tree.max_level == 0 )
+        return true;
+    const char * why = nullptr;
+    if( cfg->mhd )
+        why = "static refinement is hydro only";
+    else if( ranks_of( * cfg ) > 1 || ( cfg->flags & KR_FLAG_HALO_ALL ) )
+        why = "static refinement runs on one rank, without KR_FLAG_HALO_ALL";
+    else if( cfg->n[ 0 ] % 2 || cfg->n[ 1 ] % 2 || cfg->n[ 2 ] % 2 )
+        why = "static refinement needs an even number of cells per block along every axis";
+    if( why )
+    {
+        g_create_error = std::string( "kr_ctx_create_refined: " ) + why;
+        kr_tree_free( & tree );
+        return false;
+    }
+    return true;
+}
+
+// Restriction / flux-average items (coarse block, side, child) and the
+// prolongation items (fine block, side) of each level, from the tree.
+static void smr_plan( const kr_tree & t, const int * n, std::vector< smr_item_t > & items, int & n_restrict,
+                      std::vector< int > & prolong_off )
+{
+    items.clear(  );
+    for( int b = 0; b < t.nblk; ++ b )
+        for( int f = 0; f < 6; ++ f )
+            if( t.face[ 6 * b + f ] == KR_FACE_FINE )
+            {
+                const int a = f / 2, h1 = n[ ( a + 1 ) % 3 ] / 2, h2 = n[ ( a + 2 ) % 3 ] / 2;
+                for( int d = 0; d < 4; ++ d )
+                    items.push_back( { b, t.fnb[ ( 6 * b + f ) * 4 + d ], f, ( d >> 1 ) * h1, ( d & 1 ) * h2 } );
+            }
+    n_restrict = int( items.size(  ) );
+    prolong_off.assign( 1, n_restrict );
+    for( int l = 1; l <= t.max_level; ++ l )
+    {
+        for( int b = 0; b < t.nblk; ++ b )
+        {
+            if( t.level[ b ] != l )
+                continue;
+            for( int f = 0; f < 6; ++ f )
+                if( t.face[ 6 * b + f ] == KR_FACE_COARSE )
+                {
+                    const int a = f / 2, a1 = ( a + 1 ) % 3, a2 = ( a + 2 ) % 3;
+                    const int * r = t.reg + 3 * b;
+                    items.push_back( { b, t.fnb[ ( 6 * b + f ) * 4 ], f, ( r[ a1 ] & 1 ) * ( n[ a1 ] / 2 ),
+                                       ( r[ a2 ] & 1 ) * ( n[ a2 ] / 2 ) } );
+                }
+        }
+        prolong_off.push_back( int( items.size(  ) ) );
+    }
+}
+
+static kr_ctx * create_ctx( const kr_cfg * cfg, int n_regions, const kr_region * regions )
 {
     g_create_error.clear(  );
     if( ! cfg || cfg->abi_version != KR_ABI_VERSION )
@@ -2096,8 +2391,19 @@ kr_ctx * kr_ctx_create( const kr_cfg * cfg )
         g_create_error = "kr_ctx_create: need 0 <= rank < n_ranks";
         return nullptr;
     }
+    if( n_regions < 0 || ( n_regions > 0 && ! regions ) )
+    {
+        g_create_error = "kr_ctx_create_refined: bad region list";
+        return nullptr;
+    }
+    kr_tree tree;
+    std::memset( & tree, 0, sizeof( tree ) );
+    if( n_regions > 0 && ! build_tree( cfg, n_regions, regions, tree ) )
+        return nullptr;
+    struct tree_guard { kr_tree & t; ~tree_guard(  ) { kr_tree_free( & t ); } } guard{ tree };
+    const bool smr = tree.max_level > 0;
     std::vector< int > owner;
-    if( ! shard_owner( * cfg, owner, g_create_error ) )
+    if( ! smr && ! shard_owner( * cfg, owner, g_create_error ) )
         return nullptr;
     int ndev = 0;
     if( ! ck( nullptr, cudaGetDeviceCount( & ndev ), "cudaGetDeviceCount" ) )
@@ -2129,9 +2435,44 @@ kr_ctx * kr_ctx_create( const kr_cfg * cfg )
             local[ gb ] = int( c->gid_h.size(  ) );
             c->gid_h.push_back( gb );
         }
-    c->nblk = int( c->gid_h.size(  ) );
     const bool halo_all = ( cfg->flags & KR_FLAG_HALO_ALL ) != 0;
-    halo_plan( * cfg, owner, local, halo_all, c->hsend, c->hrecv );
+    std::vector< smr_item_t > smr_items;
+    if( smr )
+    {   // the tree's leaves, one rank, no halo exchange
+        c->smr = true;
+        c->max_level = tree.max_level;
+        for( int b = 0; b < tree.nblk; ++ b )
+        {
+            c->gid_h.push_back( b );
+            c->lvl_h.push_back( tree.level[ b ] );
+            for( int a = 0; a < 3; ++ a )
+                c->reg_h.push_back( tree.reg[ 3 * b + a ] );
+        }
+        for( halo_side_t * h : { & c->hsend, & c->hrecv } )
+        {
+            h->w_off.assign( 1, 0 ); h->w_cnt.assign( 1, 0 );
+            h->b_off.assign( 1, 0 ); h->b_cnt.assign( 1, 0 );
+        }
+        smr_plan( tree, cfg->n, smr_items, c->n_restrict, c->prolong_off );
+        if( smr_items.size(  ) > 65535 )
+        {   // one grid row per item
+            g_create_error = "kr_ctx_create_refined: more than 65535 level-jump items";
+            delete c;
+            return nullptr;
+        }
+    }
+    else
+    {
+        for( int gb : c->gid_h )
+        {
+            c->lvl_h.push_back( 0 );
+            c->reg_h.push_back( gb % cfg->nb[ 0 ] );
+            c->reg_h.push_back( ( gb / cfg->nb[ 0 ] ) % cfg->nb[ 1 ] );
+            c->reg_h.push_back( gb / ( cfg->nb[ 0 ] * cfg->nb[ 1 ] ) );
+        }
+        halo_plan( * cfg, owner, local, halo_all, c->hsend, c->hrecv );
+    }
+    c->nblk = int( c->gid_h.size(  ) );
     if( c->hsend.items.size(  ) > 65535 || c->hrecv.items.size(  ) > 65535 )
     {   // one grid row per item
         g_create_error = "kr_ctx_create: more than 65535 halo items on one rank";
@@ -2163,6 +2504,11 @@ kr_ctx * kr_ctx_create( const kr_cfg * cfg )
     ok = ok && ck( c, cudaMalloc( & c->geo, nb * sizeof( geo_t ) ), "malloc geo" );
     ok = ok && ck( c, cudaMalloc( & c->nbr, nb * 27 * sizeof( int ) ), "malloc nbr" );
     ok = ok && ck( c, cudaMalloc( & c->gid, nb * sizeof( int ) ), "malloc gid" );
+    if( ok && ! smr_items.empty(  ) )
+        ok = ck( c, cudaMalloc( & c->favg, std::max( 1, c->n_restrict ) * 5 * smr_half_sites( c ) * sizeof( double ) ), "malloc refinement fluxes" )
+          && ck( c, cudaMalloc( & c->smr_items, smr_items.size(  ) * sizeof( smr_item_t ) ), "malloc refinement items" )
+          && ck( c, cudaMemcpyAsync( c->smr_items, smr_items.data(  ), smr_items.size(  ) * sizeof( smr_item_t ),
+                                     cudaMemcpyHostToDevice, c->stream ), "upload refinement items" );
     // halo exchange: item lists and buffers (1-word minimum keeps pointers valid)
     {
         const halo_side_t * hs[ 2 ] = { & c->hsend, & c->hrecv };
@@ -2225,11 +2571,34 @@ kr_ctx * kr_ctx_create( const kr_cfg * cfg )
 
     set_geometry( c );
     // neighbour table of the local blocks: local index of a same-rank
-    // neighbour, -1 past a physical side, -2 where the halo exchange fills
+    // neighbour, -1 past a physical side, -2 where the halo exchange fills,
+    // -3 across a level jump (refined mesh: only face neighbours of the same
+    // level are copied; hydro reads no edge or corner ghost)
     std::vector< int > nbr( nb * 27 );
     for( int b = 0; b < c->nblk; ++ b )
         for( int k = 0; k < 27; ++ k )
         {
+            if( smr )
+            {
+                const int sh[ 3 ] = { k % 3 - 1, ( k / 3 ) % 3 - 1, k / 9 - 1 };
+                const int nz = ( sh[ 0 ] != 0 ) + ( sh[ 1 ] != 0 ) + ( sh[ 2 ] != 0 );
+                int v = k == 13 ? b : -3;
+                if( nz == 1 )
+                {
+                    const int a = sh[ 0 ] ? 0 : ( sh[ 1 ] ? 1 : 2 );
+                    const int f = 2 * a + ( sh[ a ] > 0 );
+                    const int kind = tree.face[ 6 * b + f ];
+                    v = kind == KR_FACE_SAME ? tree.fnb[ ( 6 * b + f ) * 4 ] : ( kind == KR_FACE_PHYS ? -1 : -3 );
+                    if( kind == KR_FACE_FINE )
+                        c->geo_h[ b ].fine |= 1 << f;
+                    if( kind == KR_FACE_FINE )
+                        for( int it = 0; it < c->n_restrict; it += 4 )
+                            if( smr_items[ it ].dst == b && smr_items[ it ].face == f )
+                                c->geo_h[ b ].fitem[ f ] = it;
+                }
+                nbr[ b * 27 + k ] = v;
+                continue;
+            }
             const int src = nbr_global( * cfg, c->gid_h[ b ], k );
             nbr[ b * 27 + k ] = src < 0 ? -1 : ( owner[ src ] == c->rank && ! ( halo_all && k != 13 ) ? local[ src ] : -2 );
         }
@@ -2249,6 +2618,26 @@ kr_ctx * kr_ctx_create( const kr_cfg * cfg )
     return c;
 }
 
+extern "C" {
+
+kr_ctx * kr_ctx_create( const kr_cfg * cfg )
+{
+    return create_ctx( cfg, 0, nullptr );
+}
+
+kr_ctx * kr_ctx_create_refined( const kr_cfg * cfg, int n_regions, const kr_region * regions )
+{
+    return create_ctx( cfg, n_regions, regions );
+}
+
+int kr_block_info( kr_ctx * c, int * level, int * reg )
+{
+    if( ! c ) return -1;
+    if( level ) std::copy( c->lvl_h.begin(  ), c->lvl_h.end(  ), level );
+    if( reg ) std::copy( c->reg_h.begin(  ), c->reg_h.end(  ), reg );
+    return c->nblk;
+}
+
 void kr_ctx_destroy( kr_ctx * c )
 {
     if( ! c ) return;
@@ -2256,7 +2645,7 @@ void kr_ctx_destroy( kr_ctx * c )
     if( c->stream ) cudaStreamSynchronize( c->stream );
     drop_graph( c );                   // before the communicator its graph uses
     if( c->comm ) nccl(  ).CommDestroy( c->comm );
-    cudaFree( c->gid );
+    cudaFree( c->gid ); cudaFree( c->smr_items ); cudaFree( c->favg );
     cudaFree( c->send_items ); cudaFree( c->recv_items );
     cudaFree( c->send_w ); cudaFree( c->recv_w ); cudaFree( c->send_b ); cudaFree( c->recv_b );
     for( int s = 0; s < 2; ++ s ) { cudaFree( c->u[ s ] ); cudaFree( c->bf[ s ] ); }
@@ -2357,16 +2746,16 @@ int kr_init_problem( kr_ctx * c, const char * name, uint64_t seed )
     {   return ( ( size_t ) b * c->nbf + ( i0 + 2 ) + sb1 * ( i1 + 2 ) + sb2 * ( i2 + 2 ) ) * 3; };
     auto work = [ & ]( int b )
     {
-        const int gb = c->gid_h[ b ];
-        const int reg[ 3 ] = { gb % g.nb[ 0 ], ( gb / g.nb[ 0 ] ) % g.nb[ 1 ], gb / ( g.nb[ 0 ] * g.nb[ 1 ] ) };
+        const int * reg = & c->reg_h[ 3 * b ];
+        const int lvl = c->lvl_h[ b ];
         if( ot )
             for( int i2 = 0; i2 <= n[ 2 ]; ++ i2 )
             for( int i1 = 0; i1 <= n[ 1 ]; ++ i1 )
             for( int i0 = 0; i0 <= n[ 0 ]; ++ i0 )
             {
                 double * p = hb.data(  ) + bidx( b, i0, i1, i2 );
-                p[ 0 ] = kr_ot_bx( x_cc( g, gb, 1, i1 ) );
-                p[ 1 ] = kr_ot_by( x_cc( g, gb, 0, i0 ) );
+                p[ 0 ] = kr_ot_bx( x_cc( g, reg, lvl, 1, i1 ) );
+                p[ 1 ] = kr_ot_by( x_cc( g, reg, lvl, 0, i0 ) );
                 p[ 2 ] = kr_ot_bz(  );
             }
         for( int i2 = 0; i2 < n[ 2 ]; ++ i2 )
@@ -2376,17 +2765,17 @@ int kr_init_problem( kr_ctx * c, const char * name, uint64_t seed )
             const int ii[ 3 ] = { i0, i1, i2 };
             int ig[ 3 ];
             for( int a = 0; a < 3; ++ a ) ig[ a ] = reg[ a ] * n[ a ] + ii[ a ];
-            const uint64_t key = kr_cell_key( 0, ig, nglob );
+            const uint64_t key = kr_cell_key( lvl, ig, nglob );
             double * u = hu.data(  ) + ( ( size_t ) b * c->nc + i0 + ( size_t ) n[ 0 ] * ( i1 + ( size_t ) n[ 1 ] * i2 ) ) * nw;
             if( shock )
-                kr_shock_cell( u, x_cc( g, gb, 0, i0 ), g.gamma, seed, key );
+                kr_shock_cell( u, x_cc( g, reg, lvl, 0, i0 ), g.gamma, seed, key );
             else
             {
                 double x[ 3 ], bc[ 3 ];
                 for( int a = 0; a < 3; ++ a )
                 {
                     int jj[ 3 ] = { i0, i1, i2 };
-                    x[ a ] = x_cc( g, gb, a, ii[ a ] );
+                    x[ a ] = x_cc( g, reg, lvl, a, ii[ a ] );
                     const double bl = hb[ bidx( b, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) + a ];
                     ++ jj[ a ];
                     bc[ a ] = ( bl + hb[ bidx( b, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) + a ] ) / 2;
@@ -2566,7 +2955,14 @@ int kr_launches_per_step( kr_ctx * c )
     if( c->cfg.mhd )
         for( int s = 0; s < 6; ++ s )
             phys += c->cfg.bc[ s ] != KR_BC_PER;
-    return 2 + 2 * ( ( c->cfg.mhd ? 4 : 3 ) + flux + phys + halo );
+    int smr = 0;
+    if( c->smr )
+    {
+        smr = c->n_restrict ? 2 : 0;     // restriction, flux average
+        for( int l = 1; l <= c->max_level; ++ l )
+            smr += c->prolong_off[ l ] > c->prolong_off[ l - 1 ];
+    }
+    return 2 + 2 * ( ( c->cfg.mhd ? 4 : 3 ) + flux + phys + halo + smr );
 }
 
 int kr_diagnostics( kr_ctx * c, double * max_div_b, double * totals5 )
@@ -2661,6 +3057,7 @@ int kr_comm_init( kr_ctx * c, const unsigned char id[ 128 ] )
     nccl_api_t & api = nccl(  );
     if( ! api.ok ) { c->err = api.err; return -1; }
     if( c->comm ) { c->err = "kr_comm_init: communicator already set"; return -1; }
+    if( c->smr ) { c->err = "kr_comm_init: a refined mesh runs on one rank"; return -1; }
     cudaSetDevice( c->cfg.device );
     ncclUniqueId uid;
     std::memcpy( & uid, id, sizeof( uid ) );

@@ -41,8 +41,12 @@ void plm_face_fast( R q_ll, R q_l, R q_r, R q_rr, R & ql, R & qr )
         // and dr share a sign, so no product of two differences is formed --
         // no FP32 underflow for tiny or overflow for huge differences (the
         // reference's FP32 path rescales by max |d| for the same purpose).
-        const bool lpos = fminf( dql, dqc ) > 0 || fmaxf( dql, dqc ) < 0;
-        const bool rpos = fminf( dqr, dqc ) > 0 || fmaxf( dqr, dqc ) < 0;
+        // Differences below FLT_MIN give no slope: the SFU reciprocal of a
+        // subnormal sum is 1 / 0 = inf (a slope that small is below the FP32
+        // resolution of any state it would change).
+        const R tiny = R( FLT_MIN );
+        const bool lpos = fminf( dql, dqc ) > tiny || fmaxf( dql, dqc ) < -tiny;
+        const bool rpos = fminf( dqr, dqc ) > tiny || fmaxf( dqr, dqc ) < -tiny;
         ql = lpos ? q_l + dql * ( dqc * rcp( dql + dqc ) ) : q_l;
         qr = rpos ? q_r - dqr * ( dqc * rcp( dqc + dqr ) ) : q_r;
         return;

@@ -108,13 +108,24 @@ def group_step(dyns, n_steps=1):
 class Dynamics:
     """One engine context.  With n_ranks > 1 it holds rank `rank`'s share of
     the nb[0] x nb[1] x nb[2] blocks (`gid`, ascending global ids) and needs a
-    communicator (`comm_init`) or `group_step` to advance."""
+    communicator (`comm_init`) or `group_step` to advance.  `regions`, a list of
+    (level, x_min, x_max) as [refine_region*] sections give them, makes a
+    statically refined hydro mesh: its blocks are the tree's leaves, level by
+    level (`level`, `reg`: each block's level and logical position)."""
 
-    def __init__(self, mhd, nb, n, **kw):
+    def __init__(self, mhd, nb, n, regions=(), **kw):
         lib = L.lib()
         c = make_cfg(mhd, nb, n, **kw)
         self.cfg = c
-        self._h = lib.kr_ctx_create(ctypes.byref(c))
+        if regions:
+            rg = (L.kr_region * len(regions))()
+            for k, (lvl, lo, hi) in enumerate(regions):
+                rg[k].level = int(lvl)
+                for a in range(3):
+                    rg[k].x_min[a], rg[k].x_max[a] = float(lo[a]), float(hi[a])
+            self._h = lib.kr_ctx_create_refined(ctypes.byref(c), len(regions), rg)
+        else:
+            self._h = lib.kr_ctx_create(ctypes.byref(c))
         if not self._h:
             raise KratosError(lib.kr_last_error(None).decode())
         self.mhd = bool(mhd)
@@ -123,6 +134,9 @@ class Dynamics:
         gid = np.empty(self.nblk, np.int32)
         lib.kr_shard_blocks(self._h, _ptr(gid))
         self.gid = gid
+        self.level = np.empty(self.nblk, np.int32)
+        self.reg = np.empty((self.nblk, 3), np.int32)
+        lib.kr_block_info(self._h, _ptr(self.level), _ptr(self.reg))
         self.nw = 8 if mhd else 5
 
     def comm_init(self, uid):
