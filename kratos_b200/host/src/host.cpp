@@ -1,6 +1,7 @@
 // kratos_b200 host layer: parameter files, problem-generator entry, the
 // default initial conditions of the dynamics modules, the mesh / time loop on
 // top of the B200 engine, and the binary snapshot writer.
+#include <array>
 #include <cfloat>
 #include <chrono>
 #include <cmath>
@@ -272,22 +273,76 @@ void mesh_t::init( const input & args )
         n_[ a ] = nbl[ a ];
         nb_[ a ] = ng[ a ] / nbl[ a ];
     }
-    // blocks and their geometry (meshgen.cpp:252-363)
-    const int nblk = nb_[ 0 ] * nb_[ 1 ] * nb_[ 2 ];
+    // engine configuration
+    kr_cfg c;
+    kr_cfg_default( & c );
+    c.mhd = mhd_;
+    c.precision = args.get< int >( "b200", "precision", 2 );
+    c.riemann = args.get< int >( "b200", "riemann", 0 );
+    for( int a = 0; a < 3; ++ a )
+    {
+        c.nb[ a ] = nb_[ a ];
+        c.n[ a ] = n_[ a ];
+        c.x_min[ a ] = x_lo[ a ];
+        c.x_max[ a ] = x_hi[ a ];
+    }
+    c.gamma = mod.p_eos->gamma;
+    c.cfl = mod.p_eos->cfl;
+    c.rho_floor = mod.p_eos->d_floor;
+    c.tmp_floor = mod.p_eos->t_floor;
+    c.dt_init = args.get< double >( "cycle", "dt_init", 0.0 );
+    c.dt_expand = args.get< double >( "cycle", "dt_expand", 2.0 );
+    c.device = args.get< int >( "device", "idx_device", 0 );
+    std::vector< std::string > kinds;
+    args( "boundary", "kinds", kinds );
+    for( int s = 0; s < 6; ++ s )
+        c.bc[ s ] = s < int( kinds.size(  ) ) ? bc_kind( kinds[ s ] ) : KR_BC_PER;
+    c.w_fix[ 0 ] = args.get< double >( "init", "rho0", 0 );
+    c.w_fix[ 1 ] = args.get< double >( "init", "pre0", 0 );
+    const auto v0 = args.get< type::coord2_t >( "init", "vel0", 0 );
+    for( int a = 0; a < 3; ++ a ) c.w_fix[ 2 + a ] = v0[ a ];
+    const auto b0 = args.get< type::coord2_t >( "init", "b0", 0 );
+    for( int a = 0; a < 3; ++ a ) c.b_fix[ a ] = b0[ a ];
+    // static refinement: every [refine_region*] section (meshgen.cpp:111-137
+    // load_refinement: level, loc / x_min, x_max defaulting to x_min)
+    std::vector< kr_region > regions;
+    for( const auto & p : args.get_prefixes(  ) )
+    {
+        if( p.find( "refine_region" ) == std::string::npos )
+            continue;
+        kr_region r;
+        r.level = args.get< int >( p, "level", 0 );
+        type::coord2_t lo( 0 ), hi;
+        args( p, "loc", lo );
+        args( p, "x_min", lo );
+        hi = lo;
+        args( p, "x_max", hi );
+        for( int a = 0; a < 3; ++ a ) { r.x_min[ a ] = lo[ a ]; r.x_max[ a ] = hi[ a ]; }
+        regions.push_back( r );
+    }
+    ctx_ = kr_ctx_create_refined( & c, int( regions.size(  ) ), regions.data(  ) );
+    if( ! ctx_ )
+        throw std::runtime_error( std::string( "kratos_b200: " ) + kr_last_error( nullptr ) );
+    // blocks (the engine's: the tree's leaves, level by level) and their
+    // geometry (meshgen.cpp:252-363: loc(i) = ( reg + i / n ) / ( nb << level ))
+    const int nblk = kr_block_info( ctx_, nullptr, nullptr );
+    std::vector< int > lvl( nblk ), regs( 3 * size_t( nblk ) );
+    kr_block_info( ctx_, lvl.data(  ), regs.data(  ) );
     blocks_.assign( nblk, block_t(  ) );
     for( int b = 0; b < nblk; ++ b )
     {
         block_t & blk = blocks_[ b ];
         blk.id_g = blk.id_l = b;
-        const int reg[ 3 ] = { b % nb_[ 0 ], ( b / nb_[ 0 ] ) % nb_[ 1 ], b / ( nb_[ 0 ] * nb_[ 1 ] ) };
+        blk.reg.level = lvl[ b ];
         double vol = 1.;
         for( int a = 0; a < 3; ++ a )
         {
-            blk.reg[ a ] = reg[ a ];
+            const int reg = regs[ 3 * b + a ];
+            blk.reg[ a ] = reg;
             blk.geo.n_ceff[ a ] = n_[ a ];
-            const double lim = double( nb_[ a ] );
-            const double l0 = x_lo[ a ] + ( reg[ a ] + 0.0 / n_[ a ] ) / lim * ( x_hi[ a ] - x_lo[ a ] );
-            const double l1 = x_lo[ a ] + ( reg[ a ] + 1.0 / n_[ a ] ) / lim * ( x_hi[ a ] - x_lo[ a ] );
+            const double lim = double( nb_[ a ] << lvl[ b ] );
+            const double l0 = x_lo[ a ] + ( reg + 0.0 / n_[ a ] ) / lim * ( x_hi[ a ] - x_lo[ a ] );
+            const double l1 = x_lo[ a ] + ( reg + 1.0 / n_[ a ] ) / lim * ( x_hi[ a ] - x_lo[ a ] );
             blk.geo.xf0[ a ] = l0;
             blk.geo.dx0[ a ] = l1 - l0;
         }
@@ -309,12 +364,15 @@ void mesh_t::init( const input & args )
         if( ! snap->load( args.get< std::string >( "file", "binary" ) ) )
             throw std::runtime_error( "restart: unreadable snapshot" );
     }
-    // Stored blocks are matched by their logical position (i_logic): the
+    // Stored blocks are matched by level and logical position (i_logic): the
     // reference numbers blocks along a Hilbert curve (meshgen.cpp:188-243),
-    // this layer lexicographically.
+    // this layer level by level, lexicographically.
     std::vector< std::string > snap_block( nblk );
     if( snap )
     {
+        std::map< std::array< int, 4 >, int > where;
+        for( int b = 0; b < nblk; ++ b )
+            where[ { lvl[ b ], regs[ 3 * b ], regs[ 3 * b + 1 ], regs[ 3 * b + 2 ] } ] = b;
         const std::string suffix = "|i_logic";
         for( const auto & kv : snap->e )
         {
@@ -322,16 +380,14 @@ void mesh_t::init( const input & args )
             if( tag.compare( 0, 6, "block_" ) || tag.size(  ) < suffix.size(  ) ||
                 tag.compare( tag.size(  ) - suffix.size(  ), suffix.size(  ), suffix ) )
                 continue;
-            int il[ 3 ], lvl = 0;
+            int il[ 3 ], lv = 0;
             const std::string pre = tag.substr( 0, tag.size(  ) - suffix.size(  ) + 1 );
             snap->get( tag, il, 3 );
-            snap->get( pre + "level", & lvl, 1 );
-            if( lvl != 0 )
-                throw std::runtime_error( "restart: refined blocks are not supported" );
-            for( int a = 0; a < 3; ++ a )
-                if( il[ a ] < 0 || il[ a ] >= nb_[ a ] )
-                    throw std::runtime_error( "restart: block outside the mesh" );
-            snap_block[ il[ 0 ] + nb_[ 0 ] * ( il[ 1 ] + nb_[ 1 ] * il[ 2 ] ) ] = pre;
+            snap->get( pre + "level", & lv, 1 );
+            const auto it = where.find( { lv, il[ 0 ], il[ 1 ], il[ 2 ] } );
+            if( it == where.end(  ) )
+                throw std::runtime_error( "restart: the snapshot's blocks are not this mesh's" );
+            snap_block[ it->second ] = pre;
         }
         for( const auto & p : snap_block )
             if( p.empty(  ) )
@@ -376,39 +432,6 @@ void mesh_t::init( const input & args )
         }
         data_.push_back( p );
     }
-    // engine configuration
-    kr_cfg c;
-    kr_cfg_default( & c );
-    c.mhd = mhd_;
-    c.precision = args.get< int >( "b200", "precision", 2 );
-    c.riemann = args.get< int >( "b200", "riemann", 0 );
-    for( int a = 0; a < 3; ++ a )
-    {
-        c.nb[ a ] = nb_[ a ];
-        c.n[ a ] = n_[ a ];
-        c.x_min[ a ] = x_lo[ a ];
-        c.x_max[ a ] = x_hi[ a ];
-    }
-    c.gamma = mod.p_eos->gamma;
-    c.cfl = mod.p_eos->cfl;
-    c.rho_floor = mod.p_eos->d_floor;
-    c.tmp_floor = mod.p_eos->t_floor;
-    c.dt_init = args.get< double >( "cycle", "dt_init", 0.0 );
-    c.dt_expand = args.get< double >( "cycle", "dt_expand", 2.0 );
-    c.device = args.get< int >( "device", "idx_device", 0 );
-    std::vector< std::string > kinds;
-    args( "boundary", "kinds", kinds );
-    for( int s = 0; s < 6; ++ s )
-        c.bc[ s ] = s < int( kinds.size(  ) ) ? bc_kind( kinds[ s ] ) : KR_BC_PER;
-    c.w_fix[ 0 ] = args.get< double >( "init", "rho0", 0 );
-    c.w_fix[ 1 ] = args.get< double >( "init", "pre0", 0 );
-    const auto v0 = args.get< type::coord2_t >( "init", "vel0", 0 );
-    for( int a = 0; a < 3; ++ a ) c.w_fix[ 2 + a ] = v0[ a ];
-    const auto b0 = args.get< type::coord2_t >( "init", "b0", 0 );
-    for( int a = 0; a < 3; ++ a ) c.b_fix[ a ] = b0[ a ];
-    ctx_ = kr_ctx_create( & c );
-    if( ! ctx_ )
-        throw std::runtime_error( std::string( "kratos_b200: " ) + kr_last_error( nullptr ) );
     std::vector< double > u, bf;
     gather( u, bf );
     if( kr_set_state( ctx_, u.data(  ), mhd_ ? bf.data(  ) : nullptr ) )

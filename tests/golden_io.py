@@ -33,6 +33,19 @@ def regions(meta):
     return [(int(l), tuple(lo), tuple(hi)) for l, lo, hi in meta.get("dynamics", {}).get("regions", [])]
 
 
+def field_errors(u, ref):
+    """Relative L1 error per conserved field (0..4); the momentum components
+    against the L1 norm of the whole momentum vector (a transverse component
+    that only seeded noise drives is near zero, and its own norm would turn
+    rounding into a large relative number)."""
+    mom = np.abs(ref[..., 2:5]).sum()
+    out = []
+    for k in range(5):
+        den = mom if k >= 2 else np.abs(ref[..., k]).sum()
+        out.append(np.abs(u[..., k] - ref[..., k]).sum() / den)
+    return out
+
+
 def load(name):
     z = np.load(os.path.join(GOLDEN, name + ".npz"))
     meta = json.loads(str(z["meta"]))

@@ -28,19 +28,6 @@ def rel_l1(a, b):
     return np.abs(a - b).sum() / (den if den > 0 else 1.0)
 
 
-def field_errors(u, ref):
-    """Relative L1 error per conserved field; the momentum components against
-    the L1 norm of the whole momentum vector (a transverse component that
-    only the seeded noise drives is near zero, and its own norm would turn
-    rounding into a large relative number)."""
-    mom = np.abs(ref[..., 2:5]).sum()
-    out = []
-    for k in range(5):
-        den = mom if k >= 2 else np.abs(ref[..., k]).sum()
-        out.append(np.abs(u[..., k] - ref[..., k]).sum() / den)
-    return out
-
-
 def _dyn(meta, precision=2, **kw):
     from kratos_b200 import Dynamics
     kinds, w_fix, b_fix = G.boundary(meta)
@@ -63,7 +50,7 @@ def test_refined_step_matches_reference(name):
     assert d.status() == 0
     assert abs(tm["t"] - meta["t"]) <= 1e-12 * meta["t"]
     assert abs(tm["dt_last"] - meta["dt"]) <= 1e-12 * meta["dt"]
-    for k, e in enumerate(field_errors(u, g["u1"])):
+    for k, e in enumerate(G.field_errors(u, g["u1"])):
         assert e <= TOL_FP64, "field %d rel L1 %.3e" % (k, e)
 
 
@@ -87,7 +74,7 @@ def test_refined_step_matches_oracle(kinds):
     u_ref, _ = m.get_state()
     u, _ = d.get_state()
     assert d.time()["t"] == pytest.approx(m.t, rel=1e-12)
-    for k, e in enumerate(field_errors(u, u_ref)):
+    for k, e in enumerate(G.field_errors(u, u_ref)):
         assert e <= TOL_FP64_LONG, "field %d rel L1 %.3e" % (k, e)
 
 
