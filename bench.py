@@ -55,6 +55,8 @@ def parse():
     p.add_argument("--mesh", type=int, default=256, choices=[128, 256],
                    help="global cells per axis (128: profiling-sized sample, 8 blocks of 64^3)")
     p.add_argument("--cpu-baseline", type=int, default=1, help="0: skip the CPU baseline leg")
+    p.add_argument("--smr", type=int, default=1,
+                   help="1: also time the statically refined hydro mesh (1 GPU only)")
     args = p.parse_args()
     global NB
     NB = (args.mesh // 64,) * 3
@@ -320,6 +322,46 @@ def time_mode(mode, args, local_rank, world, dist):
     return out
 
 
+# Statically refined hydro mesh: root 128^3 in 512 blocks of 16^3, the shock
+# plane x = 0.5 covered by a level-1 slab (x in [0.4, 0.6]) and a level-2 slab
+# (x in [0.45, 0.55]) over the whole y-z extent.
+SMR_NB, SMR_N = (8, 8, 8), (16, 16, 16)
+SMR_REGIONS = [(1, (0.4, 0.0, 0.0), (0.6, 1.0, 1.0)), (2, (0.45, 0.0, 0.0), (0.55, 1.0, 1.0))]
+
+
+def time_smr(args, local_rank):
+    """Zone-cycles/s of the refined hydro step (every block of every level in
+    one captured graph per step), FP64 and mixed."""
+    import torch
+    from kratos_b200 import Dynamics
+    out = {"workload": "shock, root 128^3 (512 blocks of 16^3), level-1 slab x in [0.4, 0.6] and "
+                       "level-2 slab x in [0.45, 0.55], periodic, PLM + HLLC, Heun RK2"}
+    for mode, prec in (("fp64", 2), ("mixed", 1)):
+        d = Dynamics(False, SMR_NB, SMR_N, gamma=1.4, precision=prec, device=local_rank,
+                     regions=SMR_REGIONS)
+        stream = torch.cuda.Stream(device=local_rank)
+        d.set_stream(stream.cuda_stream)
+        d.init_problem("shock", SEED)
+        d.step(args.warmup)
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        d.step(args.steps)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        ms = t0.elapsed_time(t1)
+        if d.status() != 0:
+            raise RuntimeError("device status %d in the refined %s step" % (d.status(), mode))
+        out[mode] = {"value": d.n_cells * args.steps / (ms * 1e-3), "unit": UNIT,
+                     "ms_per_step": ms / args.steps, "kernels_ms_per_step": d.profile_step(),
+                     "launches_per_step": d.launches_per_step()}
+        out["blocks_per_level"] = [int((d.level == l).sum()) for l in range(int(d.level.max()) + 1)]
+        out["cells"] = d.n_cells
+        d.close()
+    return out
+
+
 def flux_roofline(h, head, world, peak, peak_kind):
     """Roofline line of the flux sweep: algorithmic bytes per launch over the
     mean launch duration (CUDA events around each launch, kr_profile_step)."""
@@ -394,6 +436,8 @@ def main():
     if args.mesh != 256:
         line["config"]["workload"] = WORKLOAD.replace("256^3", "%d^3" % args.mesh).replace(
             "64 blocks", "%d blocks" % (NB[0] * NB[1] * NB[2]))
+    if rank == 0 and world == 1 and args.smr:
+        line["smr"] = time_smr(args, local_rank)
     if rank == 0:
         if args.cpu_baseline:
             try:

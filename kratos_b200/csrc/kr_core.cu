@@ -1294,6 +1294,31 @@ double smr_correct( const args_t< R > & a, const geo_t & g, int b, const int * i
     return v;
 }
 
+// The same for all five components (sides outer, components inner: each
+// component still takes its sides in the order above).
+template< class R > __device__ __forceinline__
+void smr_correct5( const args_t< R > & a, const geo_t & g, int b, const int * i, const int * nn,
+                   double dt, double * v )
+{
+#pragma unroll
+    for( int ax = 2; ax >= 0; -- ax )
+#pragma unroll
+        for( int side = 0; side <= 1; ++ side )
+            if( ( ( g.fine >> ( 2 * ax + side ) ) & 1 ) && i[ ax ] == ( side ? nn[ ax ] - 1 : 0 ) )
+            {
+                const int a1 = mod3( ax + 1 ), a2 = mod3( ax + 2 );
+                const int h1 = nn[ a1 ] >> 1, h2 = nn[ a2 ] >> 1;
+                const int d1 = i[ a1 ] >= h1, d2 = i[ a2 ] >= h2;
+                const int item = g.fitem[ 2 * ax + side ] + 2 * d1 + d2;
+                const int t = ( i[ a2 ] - d2 * h2 ) * h1 + ( i[ a1 ] - d1 * h1 );
+                const double conv = dt * g.sfc[ ax ] / ( g.vol * ( side ? -1 : 1 ) );
+                const double * f = a.favg + ( size_t ) item * 5 * a.favg_n + t;
+#pragma unroll
+                for( int k = 0; k < 5; ++ k )
+                    v[ k ] += conv * f[ ( size_t ) k * a.favg_n ];
+            }
+}
+
 template< bool MHD, class R, bool SMR = false >
 __global__ void __launch_bounds__( 256 ) k_update( const args_t< R > a, int step, udiv_t dv )
 {
@@ -1333,21 +1358,45 @@ __global__ void __launch_bounds__( 256 ) k_update( const args_t< R > a, int step
             double v[ 5 ];
             for( int k = 0; k < 5; ++ k )
                 v[ k ] = step == 0 ? us[ c0 + k * a.nc ] : ( us[ c0 + k * a.nc ] + ut[ c0 + k * a.nc ] ) * 0.5f;
-            for( int k = 0; k < 5; ++ k )
+            if constexpr( ! SMR )
+                for( int k = 0; k < 5; ++ k )
+                {
+                    for( int d = 0; d < 3; ++ d )
+                    {
+                        const double f_a = g.sfc[ d ] * dt_dv;
+                        double res = 0;
+                        res += f_a * double( fl[ d ][ k ] );
+                        res -= f_a * double( fr[ d ][ k ] );
+                        v[ k ] += res;
+                    }
+                    ut[ c0 + k * a.nc ] = v[ k ];
+                }
+            else
             {
+                bool nl[ 3 ], nr[ 3 ];
                 for( int d = 0; d < 3; ++ d )
                 {
-                    const double f_a = g.sfc[ d ] * dt_dv;
-                    double res = 0;
-                    if( ! SMR || ! ( ( ( g.fine >> ( 2 * d ) ) & 1 ) && i[ d ] == 0 ) )
-                        res += f_a * double( fl[ d ][ k ] );
-                    if( ! SMR || ! ( ( ( g.fine >> ( 2 * d + 1 ) ) & 1 ) && i[ d ] == nn[ d ] - 1 ) )
-                        res -= f_a * double( fr[ d ][ k ] );
-                    v[ k ] += res;
+                    nl[ d ] = ( ( g.fine >> ( 2 * d ) ) & 1 ) && i[ d ] == 0;
+                    nr[ d ] = ( ( g.fine >> ( 2 * d + 1 ) ) & 1 ) && i[ d ] == nn[ d ] - 1;
                 }
-                if constexpr( SMR )
-                    v[ k ] = smr_correct( a, g, b, i, nn, k, dt, v[ k ] );
-                ut[ c0 + k * a.nc ] = v[ k ];
+#pragma unroll
+                for( int k = 0; k < 5; ++ k )
+#pragma unroll
+                    for( int d = 0; d < 3; ++ d )
+                    {
+                        const double f_a = g.sfc[ d ] * dt_dv;
+                        double res = 0;
+                        if( ! nl[ d ] )
+                            res += f_a * double( fl[ d ][ k ] );
+                        if( ! nr[ d ] )
+                            res -= f_a * double( fr[ d ][ k ] );
+                        v[ k ] += res;
+                    }
+                if( g.fine )
+                    smr_correct5( a, g, b, i, nn, dt, v );
+#pragma unroll
+                for( int k = 0; k < 5; ++ k )
+                    ut[ c0 + k * a.nc ] = v[ k ];
             }
         }
         else
