@@ -228,16 +228,50 @@ __global__ void __launch_bounds__( 256 ) k_c2p( const args_t< R > a, int step, u
             U[ iuc( a, b, ENE, i0, i1, i2 ) ] = MHD ? cout[ ENE ] + e_m : cout[ ENE ];
             atomicAdd( & a.s->heal_count, 1 );
         }
+        R wv[ NW ];
         for( int k = 0; k < 5; ++ k )
-            a.w[ iw( a, b, k, NW, i0, i1, i2 ) ] = R( prim[ k ] );
+            wv[ k ] = R( prim[ k ] );
         if( MHD )
             for( int d = 0; d < 3; ++ d )
             {   // cell-centred E = B x v (mhd/eos/adiabatic.h:216-220), from the
                 // stored (R-rounded) primitives so ghost copies agree bit for bit
                 const int d1 = mod3( d + 1 ), d2 = mod3( d + 2 );
-                a.w[ iw( a, b, BCC + d, NW, i0, i1, i2 ) ] = R( bc[ d ] );
-                a.w[ iw( a, b, 8 + d, NW, i0, i1, i2 ) ] =
-                    R( bc[ d1 ] ) * R( prim[ MOM + d2 ] ) - R( bc[ d2 ] ) * R( prim[ MOM + d1 ] );
+                wv[ BCC + d ] = R( bc[ d ] );
+                wv[ 8 + d ] = R( bc[ d1 ] ) * R( prim[ MOM + d2 ] ) - R( bc[ d2 ] ) * R( prim[ MOM + d1 ] );
+            }
+        {
+            R * o = a.w + iw( a, b, 0, NW, i0, i1, i2 );
+            const int ngw = int( a.ngw );
+#pragma unroll
+            for( int k = 0; k < NW; ++ k )
+                o[ k * ngw ] = wv[ k ];
+        }
+        // Same-level ghost fill by push: a cell within two cells of a side is a
+        // ghost cell of the block across it (faces, edges, corners).  The block
+        // that holds this cell's position at i + sh n in its ghost shell is the
+        // neighbour in direction -sh, the one whose k_ghost pull in direction sh
+        // reads this cell; past a physical side (-1), on another rank (-2, the
+        // halo exchange) or across a level jump (-3) nothing is written here.
+        // Per axis the shift is +1 within two cells of the low side, -1 of the
+        // high side (n >= 4: never both); the targets are the nonempty subsets.
+        const int sx = i0 < 2 ? 1 : ( i0 >= a.n0 - 2 ? -1 : 0 );
+        const int sy = i1 < 2 ? 1 : ( i1 >= a.n1 - 2 ? -1 : 0 );
+        const int sz = i2 < 2 ? 1 : ( i2 >= a.n2 - 2 ? -1 : 0 );
+        const int mask = ( sx != 0 ) | ( sy != 0 ) << 1 | ( sz != 0 ) << 2;
+        if( mask )
+            for( int m = 1; m < 8; ++ m )
+            {
+                if( m & ~mask )
+                    continue;
+                const int dx = m & 1 ? sx : 0, dy = m & 2 ? sy : 0, dz = m & 4 ? sz : 0;
+                const int dst = a.nbr[ b * 27 + ( 1 - dx ) + 3 * ( 1 - dy ) + 9 * ( 1 - dz ) ];
+                if( dst < 0 )
+                    continue;
+                R * o = a.w + iw( a, dst, 0, NW, i0 + dx * a.n0, i1 + dy * a.n1, i2 + dz * a.n2 );
+                const int ngw = int( a.ngw );
+#pragma unroll
+                for( int k = 0; k < NW; ++ k )
+                    o[ k * ngw ] = wv[ k ];
             }
         if( step == 0 )
         {
@@ -1440,7 +1474,24 @@ __global__ void __launch_bounds__( 256 ) k_update( const args_t< R > a, int step
         const double sfc = g.sfc[ c ];
         db *= ( sfc > 0 ? ( -dt / sfc ) : 0. );
         const long long k = ibf( a, b, c, i[ 0 ], i[ 1 ], i[ 2 ] );
-        bt[ k ] = db + ( step == 0 ? bs[ k ] : ( bs[ k ] + bt[ k ] ) / 2 );
+        const double nb = db + ( step == 0 ? bs[ k ] : ( bs[ k ] + bt[ k ] ) / 2 );
+        bt[ k ] = nb;
+        // Same-level face-B ghost strips by push, for the next stage: a face
+        // next to a transverse side is a ghost face of the block across it
+        // (the one whose pull along that axis reads it); -1 / -2 as for W.
+        for( int l = 0; l < 2; ++ l )
+        {
+            const int t = l ? ax2 : ax1;
+            if( i[ t ] != 0 && i[ t ] != nn[ t ] - 1 )
+                continue;
+            const int s = i[ t ] == 0 ? -1 : 1;
+            const int dst = a.nbr[ b * 27 + 13 + s * ( t == 0 ? 1 : ( t == 1 ? 3 : 9 ) ) ];
+            if( dst < 0 )
+                continue;
+            int j[ 3 ] = { i[ 0 ], i[ 1 ], i[ 2 ] };
+            j[ t ] = s < 0 ? nn[ t ] : -1;
+            bt[ ibf( a, dst, c, j[ 0 ], j[ 1 ], j[ 2 ] ) ] = nb;
+        }
     }
 }
 
@@ -2068,13 +2119,11 @@ static void enqueue_back( kr_ctx * c, cudaStream_t st, const args_t< R > & a, in
 {
     const int * n = c->cfg.n;
     const unsigned nb = unsigned( c->nblk );
-    const long long nghost = shell_count( n[ 0 ], n[ 1 ], n[ 2 ], 2 )
-                           + ( MHD ? bf_strip_count( n[ 0 ], n[ 1 ], n[ 2 ] ) : 0 );
     timed( 1, [ & ] {
         if( ! c->hrecv.items.empty(  ) )
             k_halo< MHD, R, false ><<< dim3( c->halo_grid, unsigned( c->hrecv.items.size(  ) ) ), 256, 0, st >>>(
                 a, c->recv_items, ( R * ) c->recv_w, c->recv_b, stage );
-        k_ghost< MHD, R ><<< dim3( blocks_for( nghost, 256 ), nb ), 256, 0, st >>>( a, stage, make_ghost_div( n ) );
+        // (the same-level ghost fill happens in k_c2p and k_update: push)
         if( c->n_restrict )            // finer -> coarser ghosts
             k_restrict< R ><<< dim3( blocks_for( 2 * smr_half_sites( c ), 128 ), c->n_restrict ), 128, 0, st >>>( a, c->smr_items );
         if( ! MHD && has_phys( c ) )
@@ -2730,6 +2779,13 @@ static void launch_scatter( kr_ctx * c )
     const double * hu = c->stage;
     const double * hb = c->stage + size_t( c->nblk ) * c->nc * c->nw;
     k_scatter< MHD, R ><<< dim3( blocks_for( nmax, 256 ), c->nblk ), 256, 0, c->stream >>>( a, hu, hb );
+    if( MHD )
+    {   // the face-B ghost strips of slot 0 for the first stage (later stages
+        // get them pushed by the face update)
+        const int * n = c->cfg.n;
+        const long long nghost = shell_count( n[ 0 ], n[ 1 ], n[ 2 ], 2 ) + bf_strip_count( n[ 0 ], n[ 1 ], n[ 2 ] );
+        k_ghost< MHD, R ><<< dim3( blocks_for( nghost, 256 ), c->nblk ), 256, 0, c->stream >>>( a, 0, make_ghost_div( n ) );
+    }
 }
 template< bool MHD, class R >
 static void launch_gather( kr_ctx * c )
@@ -3011,7 +3067,7 @@ int kr_launches_per_step( kr_ctx * c )
         for( int l = 1; l <= c->max_level; ++ l )
             smr += c->prolong_off[ l ] > c->prolong_off[ l - 1 ];
     }
-    return 2 + 2 * ( ( c->cfg.mhd ? 4 : 3 ) + flux + phys + halo + smr );
+    return 2 + 2 * ( ( c->cfg.mhd ? 3 : 2 ) + flux + phys + halo + smr );
 }
 
 int kr_diagnostics( kr_ctx * c, double * max_div_b, double * totals5 )

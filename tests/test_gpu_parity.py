@@ -227,4 +227,4 @@ def test_status_word_starts_clean_and_steps_counted():
     d.step(3)
     tm = d.time()
     assert tm["n_steps"] == 3 and d.status() == 0
-    assert d.launches_per_step() == 14
+    assert d.launches_per_step() == 12      # 2 x (c2p, 3 flux sweeps, update) + begin, end
