@@ -183,7 +183,7 @@ __global__ void k_step_end( scal_t * s, double dt_expand )
 // (hydro/eos/adiabatic.h:211-258; mhd/eos/adiabatic.h:127-234).
 
 template< bool MHD, class R >
-__global__ void __launch_bounds__( 256 ) k_c2p( const args_t< R > a, int step, udiv_t dv )
+__global__ void __launch_bounds__( 256, 4 ) k_c2p( const args_t< R > a, int step, udiv_t dv )
 {
     // grid: x over the cells of one (x, y) plane, y over z, z over blocks
     constexpr int NW = MHD ? 11 : 5;   // stored W words: prim (8) + cell E (3)
@@ -1354,7 +1354,7 @@ void smr_correct5( const args_t< R > & a, const geo_t & g, int b, const int * i,
 }
 
 template< bool MHD, class R, bool SMR = false >
-__global__ void __launch_bounds__( 256 ) k_update( const args_t< R > a, int step, udiv_t dv )
+__global__ void __launch_bounds__( 256, ( SMR && sizeof( R ) == 4 ) ? 3 : 4 ) k_update( const args_t< R > a, int step, udiv_t dv )
 {
     // grid: x over the lattice sites of one (x, y) plane, y over z, z over blocks
     constexpr int NF = MHD ? 7 : 5;
