@@ -200,8 +200,9 @@ def reference_arm(args, rank, world):
 
 # --------------------------------------------------------------------------- GPU
 MODES = {"fp64": dict(precision=2, riemann=0), "mixed": dict(precision=1, riemann=0),
-         "hlle_mixed": dict(precision=1, riemann=1), "learned": dict(precision=1, riemann=2, sel_period=4),
-         "learned_p1": dict(precision=1, riemann=2, sel_period=1)}
+         "hlle_mixed": dict(precision=1, riemann=1), "learned": dict(precision=1, riemann=2, sel_period=16),
+         "learned_p1": dict(precision=1, riemann=2, sel_period=1),
+         "learned_p4": dict(precision=1, riemann=2, sel_period=4)}
 
 
 def train_selector(local_rank):
@@ -309,6 +310,9 @@ def time_mode(mode, args, local_rank, world, dist):
         x = torch.tensor([wall], device="cuda:%d" % local_rank)
         dist.all_reduce(x, op=dist.ReduceOp.MAX)
         wall = float(x.item())
+    # final density (every mode runs warm-up + timed + end-to-end steps from the
+    # same initial state) for the error of the FP32 modes against the FP64 one
+    out["rho"] = np.array(hu[..., 0])
     out["e2e"] = {"value": n_all * e2e_steps / wall, "unit": UNIT,
                   "h2d_bytes_per_step": d.state_bytes() // e2e_steps,
                   "d2h_bytes_per_step": d.state_bytes() // e2e_steps}
@@ -397,6 +401,13 @@ def main():
     results = {}
     for mode in [m for m in args.modes.split(",") if m]:
         results[mode] = time_mode(mode, args, local_rank, world, dist)
+    if "fp64" in results:
+        import numpy as np
+        ref = results["fp64"]["rho"]
+        den = np.abs(ref).sum()
+        for m, r in results.items():
+            if m != "fp64":
+                r["l1_density_vs_fp64"] = float(np.abs(r["rho"] - ref).sum() / den)
     head = next((m for m in ("learned", "mixed", "fp64") if m in results), next(iter(results)))
     h = results[head]
     peak, peak_kind = measured_peaks()
@@ -416,7 +427,10 @@ def main():
                    "l2": "state 1.6 GB > 126 MB L2; no flush needed"},
         "modes": {m: dict({"value": r["value"], "ms_per_step": r["ms_per_step"],
                            "kernels_ms_per_step": r["kernels_ms_per_step"]},
-                          **({"selector": r["selector"]} if "selector" in r else {}))
+                          **({"selector": r["selector"]} if "selector" in r else {}),
+                          **({"l1_density_vs_fp64": r["l1_density_vs_fp64"],
+                              "steps_compared": args.warmup + 2 * args.steps}
+                             if "l1_density_vs_fp64" in r else {}))
                   for m, r in results.items()},
         "roofline": flux_roofline(h, head, world, peak, peak_kind),
         "step_roofline": {"bound": "hbm", "achieved": step_gbs, "peak": peak, "unit": "GB/s",

@@ -962,20 +962,18 @@ template< class R, int MODE > constexpr int flux_min_ctas(  )
                             : ( MODE == KR_RIEMANN_HLLE ? 5 : 4 );
 }
 
-template< bool MHD, class R, int MODE >
-__global__ void __launch_bounds__( 128, ( flux_min_ctas< R, MODE >(  ) ) ) k_flux( const args_t< R > a, int axis, int step, int lines, udiv_t dv )
+// One CTA's 128 faces of a sweep: bx = CTA along the faces of one (x, y)
+// plane (lines: along all line faces), by = z plane, blockIdx.z = block; dv
+// divides by the row length.
+template< bool MHD, class R, int MODE > __device__ __forceinline__
+void flux_faces( const args_t< R > & a, int axis, int step, int lines, udiv_t dv, unsigned bx, unsigned by )
 {
     constexpr int NW = MHD ? 11 : 5;   // stored W words: prim (8) + cell E (3)
     constexpr int NP = MHD ? 8 : 5;    // primitive words reconstructed
     constexpr bool learned = MHD && MODE == KR_RIEMANN_LEARNED;
-    // grid: x over the faces of one (x, y) plane (lines: over all line
-    // faces), y over z planes, z over blocks; dv divides by the row length
-    if constexpr( learned )
-        if( step != 0 || ! sel_eval_step( a.s, a.sel_period ) )
-            return;                   // k_flux_list solves this sweep
     const int b = blockIdx.z;
     const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
-    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned t = bx * blockDim.x + threadIdx.x;
     int ii[ 3 ];
     int outside = 0;
     unsigned total;
@@ -990,8 +988,8 @@ __global__ void __launch_bounds__( 128, ( flux_min_ctas< R, MODE >(  ) ) ) k_flu
         const unsigned q = udiv_q( t, dv );
         ii[ 0 ] = int( t - q * unsigned( ext[ 0 ] ) );
         ii[ 1 ] = int( q );
-        ii[ 2 ] = int( blockIdx.y );
-        t_lin = ( long long ) t + ( long long ) total * blockIdx.y;
+        ii[ 2 ] = int( by );
+        t_lin = ( long long ) t + ( long long ) total * by;
         for( int d = 0; d < 3; ++ d )
             if( d != axis )
             {
@@ -1055,32 +1053,56 @@ __global__ void __launch_bounds__( 128, ( flux_min_ctas< R, MODE >(  ) ) ) k_flu
     solve_store< MHD, R, MODE >( a, b, axis, ii, valid, ql, qr, threadIdx.x >> 5, key );
 }
 
+template< bool MHD, class R, int MODE >
+__global__ void __launch_bounds__( 128, ( flux_min_ctas< R, MODE >(  ) ) ) k_flux( const args_t< R > a, int axis, int step, int lines, udiv_t dv )
+{
+    flux_faces< MHD, R, MODE >( a, axis, step, lines, dv, blockIdx.x, blockIdx.y );
+}
+
+// Learned mode, the network's sweep: a fixed grid strides over the 128-face
+// chunks (cpp per z plane, nz planes), so on the stages where the network does
+// not run (k_flux_list solves them) only this small grid launches and exits.
+// The chunk loop is uniform over a CTA, as learned_solve's barriers need.
+template< bool MHD, class R >
+__global__ void __launch_bounds__( 128, ( flux_min_ctas< R, KR_RIEMANN_LEARNED >(  ) ) )
+k_flux_eval( const args_t< R > a, int axis, int step, udiv_t dv, unsigned cpp, unsigned nz )
+{
+    if( step != 0 || ! sel_eval_step( a.s, a.sel_period ) )
+        return;
+    for( unsigned ch = blockIdx.x; ch < cpp * nz; ch += gridDim.x )
+        flux_faces< MHD, R, KR_RIEMANN_LEARNED >( a, axis, step, 0, dv, ch % cpp, ch / cpp );
+}
+
 // Learned mode, sweeps without the network: one thread per entry of the
-// (axis, block) HLLD list (CHEAP = false) or HLLE list (CHEAP = true) built by
-// the last evaluation.  Warps run one solver; entries of a warp come from
-// one or two producer warps, so loads and stores stay nearly coalesced.
-template< bool MHD, class R, bool CHEAP >
+// (axis, block) HLLD and HLLE lists built by the last evaluation.  Warps run
+// one solver; entries of a warp come from one or two producer warps, so loads
+// and stores stay nearly coalesced.
+template< bool MHD, class R >
 __global__ void __launch_bounds__( 128, ( flux_min_ctas< R, KR_RIEMANN_DEFAULT >(  ) ) )
 k_flux_list( const args_t< R > a, int axis, int step )
 {
     constexpr int NW = MHD ? 11 : 5;
     constexpr int NP = MHD ? 8 : 5;
     if( step == 0 && sel_eval_step( a.s, a.sel_period ) )
-        return;                       // the network's sweep (k_flux) solves this one
+        return;                       // the network's sweep (k_flux_eval) solves this one
     const int b = blockIdx.z;
     const size_t r = ( size_t ) axis * a.nblk + b;
-    const unsigned n = a.sel_count[ r * 2 + ( CHEAP ? 1 : 0 ) ];
+    const unsigned nh = a.sel_count[ r * 2 ], n = nh + a.sel_count[ r * 2 + 1 ];
     const unsigned * list = a.sel_list + r * a.sel_cap;
-    // a fixed grid strides over the list (its length is known only on the device);
-    // the next entry is fetched before this face's work
+    // a fixed grid strides over both lists as one index space, the HLLD entries
+    // [0, nh) (front of the list) then the HLLE ones (back); only the warp that
+    // straddles nh mixes the two solvers.  The next entry is fetched before this
+    // face's work.
     const unsigned stride = gridDim.x * blockDim.x;
     unsigned j = blockIdx.x * blockDim.x + threadIdx.x;
-    unsigned pk_next = j < n ? ( CHEAP ? list[ a.sel_cap - 1 - j ] : list[ j ] ) : 0u;
+    auto entry = [ & ]( unsigned k ) { return k < nh ? list[ k ] : list[ a.sel_cap - 1 - ( k - nh ) ]; };
+    unsigned pk_next = j < n ? entry( j ) : 0u;
     for( ; j < n; j += stride )
     {
     const unsigned pk = pk_next;
+    const bool cheap = j >= nh;
     if( j + stride < n )
-        pk_next = CHEAP ? list[ a.sel_cap - 1 - ( j + stride ) ] : list[ j + stride ];
+        pk_next = entry( j + stride );
     int ii[ 3 ] = { int( pk & 1023u ) - 2, int( ( pk >> 10 ) & 1023u ) - 2, int( pk >> 20 ) - 2 };
     const int st = axis == 0 ? 1 : ( axis == 1 ? a.sw1 : a.sw2 );
     R ql[ 8 ], qr[ 8 ];
@@ -1097,7 +1119,10 @@ k_flux_list( const args_t< R > a, int axis, int step )
         const R * p = wb + k * ngw;
         plm_face_fast< R >( p[ -2 * st ], p[ -st ], p[ 0 ], p[ st ], ql[ k ], qr[ k ] );
     }
-    solve_store< MHD, R, CHEAP ? KR_RIEMANN_HLLE : KR_RIEMANN_DEFAULT >( a, b, axis, ii, true, ql, qr, 0, 0ull );
+    if( cheap )
+        solve_store< MHD, R, KR_RIEMANN_HLLE >( a, b, axis, ii, true, ql, qr, 0, 0ull );
+    else
+        solve_store< MHD, R, KR_RIEMANN_DEFAULT >( a, b, axis, ii, true, ql, qr, 0, 0ull );
     }
 }
 
@@ -2059,16 +2084,24 @@ static void launch_flux( kr_ctx * c, cudaStream_t st, const args_t< R > & a, int
         int ext[ 3 ];
         for( int d = 0; d < 3; ++ d )
             ext[ d ] = ( d == axis ) ? n[ d ] + 1 : n[ d ] + ( MHD ? 2 : 0 );
-        k_flux< MHD, R, MODE ><<< dim3( blocks_for( ( long long ) ext[ 0 ] * ext[ 1 ], 128 ), ext[ 2 ], c->nblk ), 128, 0, st >>>(
-            a, axis, stage, 0, make_udiv( unsigned( ext[ 0 ] ) ) );
         if constexpr( MODE == KR_RIEMANN_LEARNED && MHD )
-        {   // sweeps without the network: the two face lists (each kernel exits
-            // at once on the network's sweep; CTAs past a list's length exit)
-            // about two waves of CTAs over all blocks, striding over the lists
+        {
+            const unsigned cpp = blocks_for( ( long long ) ext[ 0 ] * ext[ 1 ], 128 );
+            const unsigned ge = unsigned( std::max< long long >( 1, std::min< long long >(
+                ( long long ) cpp * ext[ 2 ], ( 2LL * c->n_sm * flux_min_ctas< R, KR_RIEMANN_LEARNED >(  ) ) / c->nblk ) ) );
+            k_flux_eval< MHD, R ><<< dim3( ge, 1, c->nblk ), 128, 0, st >>>(
+                a, axis, stage, make_udiv( unsigned( ext[ 0 ] ) ), cpp, unsigned( ext[ 2 ] ) );
+        }
+        else
+            k_flux< MHD, R, MODE ><<< dim3( blocks_for( ( long long ) ext[ 0 ] * ext[ 1 ], 128 ), ext[ 2 ], c->nblk ), 128, 0, st >>>(
+                a, axis, stage, 0, make_udiv( unsigned( ext[ 0 ] ) ) );
+        if constexpr( MODE == KR_RIEMANN_LEARNED && MHD )
+        {   // sweeps without the network: the face lists (exits at once on the
+            // network's sweep; CTAs past the lists' length exit); about two
+            // waves of CTAs over all blocks, striding over the lists
             const unsigned gx = unsigned( std::max< long long >( 1, std::min< long long >(
                 blocks_for( ( long long ) ext[ 0 ] * ext[ 1 ] * ext[ 2 ], 128 ), ( 2LL * c->n_sm * 8 ) / c->nblk ) ) );
-            k_flux_list< MHD, R, false ><<< dim3( gx, 1, c->nblk ), 128, 0, st >>>( a, axis, stage );
-            k_flux_list< MHD, R, true ><<< dim3( gx, 1, c->nblk ), 128, 0, st >>>( a, axis, stage );
+            k_flux_list< MHD, R ><<< dim3( gx, 1, c->nblk ), 128, 0, st >>>( a, axis, stage );
         }
         return;
     }
@@ -3054,7 +3087,7 @@ int kr_launches_per_step( kr_ctx * c )
         flux += ( t.ok && ! c->no_tiles && c->cfg.mhd ) ? 2 : 1;
     }
     if( c->cfg.mhd && c->cfg.riemann == KR_RIEMANN_LEARNED )
-        flux = 9;                     // per sweep: the network's kernel and the two list kernels
+        flux = 6;                     // per sweep: the network's kernel and the list kernel
     const int halo = ( c->hsend.items.empty(  ) ? 0 : 1 ) + ( c->hrecv.items.empty(  ) ? 0 : 1 );
     int phys = ! c->cfg.mhd && has_phys( c ) ? 1 : 0;
     if( c->cfg.mhd )
