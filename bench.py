@@ -42,6 +42,9 @@ FLUX_BYTES_PER_FACE = {4: 8 * 4 + 8 + 7 * 4, 8: 8 * 8 + 8 + 7 * 8}
 # dram__bytes_write.sum on the 128^3 sample (8 blocks of 64^3) divided by its
 # 2.26 M faces; traffic scales with the faces (same block shape)
 FLUX_DRAM_BYTES_PER_FACE = 54.9
+# the same for the learned mode's list sweep (k_flux_list): 146.4 MB per launch
+# averaged over four captured launches on the 128^3 sample, 2.26 M faces
+FLUX_LIST_DRAM_BYTES_PER_FACE = 64.7
 WORKLOAD = "ot 256^3 periodic MHD, 64 blocks of 64^3, PLM+HLLD+CT, Heun RK2"
 
 
@@ -375,9 +378,11 @@ def flux_roofline(h, head, world, peak, peak_kind):
     k = h["kernels_ms_per_step"]
     launch_ms = (k["flux_x"] + k["flux_y"] + k["flux_z"]) / 6.0      # 3 sweeps x 2 stages
     gbs = faces * FLUX_BYTES_PER_FACE[rsize] / (launch_ms * 1e-3) / 1e9
-    return {"bound": "hbm", "kernel": "k_flux (one sweep, %s mode)" % head, "achieved": gbs, "peak": peak,
-            "unit": "GB/s", "frac": gbs / peak,
-            "traffic": FLUX_DRAM_BYTES_PER_FACE * faces if rsize == 4 else None,
+    learned = head.startswith("learned")
+    per_face = FLUX_LIST_DRAM_BYTES_PER_FACE if learned else FLUX_DRAM_BYTES_PER_FACE
+    return {"bound": "hbm", "kernel": "%s (one sweep, %s mode)" % ("k_flux_list" if learned else "k_flux", head),
+            "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+            "traffic": per_face * faces if rsize == 4 else None,
             "algorithmic_bytes_per_launch": faces * FLUX_BYTES_PER_FACE[rsize],
             "launch_ms": launch_ms,
             "basis": "%d B/face x %d faces per launch (%s peak); the sweep is bound by instruction "
