@@ -55,6 +55,7 @@ struct scal_t
 struct geo_t
 {
     double dx[ 3 ], sfc[ 3 ], vol;
+    double idx[ 3 ];              // 1 / dx
     int phys;                     // bit 2a+s: side (a, s) is a non-periodic domain side
     int fine;                     // bit 2a+s: the neighbours across side (a, s) are finer
     int fitem[ 6 ];               // refined side: first of its 4 flux-average items
@@ -274,26 +275,30 @@ __global__ void __launch_bounds__( 256, 4 ) k_c2p( const args_t< R > a, int step
                     o[ k * ngw ] = wv[ k ];
             }
         if( step == 0 )
-        {
+        {   // cfl * min_a dx_a / s_a as cfl / max_a ( s_a / dx_a ): one division
+            // (the reference divides per axis; rounding differs only); like
+            // fmin, fmax drops a NaN candidate
             const geo_t & g = a.geo[ b ];
+            double smax = 0;
             if( ! MHD )
             {
                 const double cs = sqrt( cs2 );
                 for( int d = 0; d < 3; ++ d )
-                    dt = fmin( dt, g.dx[ d ] / ( cs + fabs( prim[ MOM + d ] ) ) );
+                    smax = fmax( smax, ( cs + fabs( prim[ MOM + d ] ) ) * g.idx[ d ] );
             }
             else
             {
+                const double rho_inv = 1 / prim[ RHO ];
                 double bm_2[ 3 ] = { bc_2[ 0 ], bc_2[ 1 ], bc_2[ 2 ] };
                 for( int d = 0; d < 3; ++ d )
                 {
                     bm_2[ d ] = b_max[ d ] * b_max[ d ];
-                    const double cf = c_fms< double >( prim, bm_2, a.gamma, d );
-                    dt = fmin( dt, g.dx[ d ] / ( cf + fabs( prim[ MOM + d ] ) ) );
+                    const double cf = c_fms_ri< double >( prim, bm_2, a.gamma, d, rho_inv );
+                    smax = fmax( smax, ( cf + fabs( prim[ MOM + d ] ) ) * g.idx[ d ] );
                     bm_2[ d ] = bc_2[ d ];
                 }
             }
-            dt *= a.cfl;
+            dt = smax > 0 ? a.cfl / smax : FLT_MAX;
         }
     }
     if( step == 0 )
@@ -2358,6 +2363,7 @@ static void set_geometry( kr_ctx * c )
             const double l0 = g.x_min[ a ] + x0 * ( g.x_max[ a ] - g.x_min[ a ] );
             const double l1 = g.x_min[ a ] + x1 * ( g.x_max[ a ] - g.x_min[ a ] );
             o.dx[ a ] = l1 - l0;
+            o.idx[ a ] = 1 / o.dx[ a ];
         }
         double vol = 1.;
         for( int a = 0; a < 3; ++ a )

@@ -62,6 +62,19 @@ R c_fms( const R * w, const R * b_2, R gam, int axis )
     return sqrt( R( 0.5f ) * ( q_2 + sqrt( r_2 * r_2 + R( 4 ) * cs_2 * v_t2 ) ) );
 }
 
+// Fast magnetosonic speed along `axis` with 1 / rho given (c_fms with its three
+// divisions by rho replaced by products).
+template< class R > __device__ __forceinline__
+R c_fms_ri( const R * w, const R * b_2, R gam, int axis, R rho_inv )
+{
+    const R cs_2  = w[ ENE ] * gam * rho_inv;
+    const R v_ax2 = b_2[ axis ] * rho_inv;
+    const R v_t2  = ( b_2[ mod3( axis + 1 ) ] + b_2[ mod3( axis + 2 ) ] ) * rho_inv;
+    const R q_2   = v_ax2 + v_t2 + cs_2;
+    const R r_2   = v_ax2 + v_t2 - cs_2;
+    return sqrt( R( 0.5f ) * ( q_2 + sqrt( r_2 * r_2 + R( 4 ) * cs_2 * v_t2 ) ) );
+}
+
 // Conserved -> primitive with density / pressure floors (always FP64).
 // cons[0..4] in; prim[0..4] out; floor corrections are written back to cons
 // and flagged in the return's low bits (1: rho floored, 2: energy healed).
@@ -90,9 +103,10 @@ int c2p( const double * cons_in, double * prim, double * cons_out, double gamma,
     }
     e_k *= rho_inv / 2;
     const double e_g   = cons_in[ ENE ] - e_k;
-    const double cv_kb = 1 / ( gamma - 1 );
-    prim[ ENE ] = e_g / cv_kb;
-    cs2 = gamma * prim[ ENE ] / prim[ RHO ];
+    // the reference divides by cv = 1 / (gamma - 1) and by rho; multiplying by
+    // gamma - 1 and 1 / rho differs in rounding only
+    prim[ ENE ] = e_g * ( gamma - 1 );
+    cs2 = gamma * prim[ ENE ] * rho_inv;
     const double pre_floor = t_floor * prim[ RHO ];
     if( isnan( prim[ ENE ] ) || prim[ ENE ] < pre_floor )
     {
