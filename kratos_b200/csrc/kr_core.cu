@@ -1383,7 +1383,9 @@ void smr_correct5( const args_t< R > & a, const geo_t & g, int b, const int * i,
             }
 }
 
-template< bool MHD, class R, bool SMR = false >
+// PART 0: cells and faces in one launch; 1: the conserved update only; 2: the
+// CT face update only (MHD: two launches, each with fewer registers).
+template< bool MHD, class R, bool SMR = false, int PART = 0 >
 __global__ void __launch_bounds__( 256, ( SMR && sizeof( R ) == 4 ) ? 3 : 4 ) k_update( const args_t< R > a, int step, udiv_t dv )
 {
     // grid: x over the lattice sites of one (x, y) plane, y over z, z over blocks
@@ -1402,7 +1404,7 @@ __global__ void __launch_bounds__( 256, ( SMR && sizeof( R ) == 4 ) ? 3 : 4 ) k_
     // issue ahead of the stores of earlier ones.
     const R * __restrict__ F[ 3 ] = { a.f[ 0 ], a.f[ 1 ], a.f[ 2 ] };
     const R * __restrict__ EE = a.ee;
-    if( i[ 0 ] < nn[ 0 ] && i[ 1 ] < nn[ 1 ] && i[ 2 ] < nn[ 2 ] )
+    if( PART != 2 && i[ 0 ] < nn[ 0 ] && i[ 1 ] < nn[ 1 ] && i[ 2 ] < nn[ 2 ] )
     {
         const double * __restrict__ us = a.u[ step ];
         double * __restrict__ ut = a.u[ 1 - step ];
@@ -1483,7 +1485,7 @@ __global__ void __launch_bounds__( 256, ( SMR && sizeof( R ) == 4 ) ? 3 : 4 ) k_
                 ut[ c ] = v;
             }
     }
-    if( ! MHD )
+    if( ! MHD || PART == 1 )
         return;
     const double * __restrict__ bs = a.bf[ step ];
     double * __restrict__ bt = a.bf[ 1 - step ];
@@ -2195,7 +2197,14 @@ static void enqueue_back( kr_ctx * c, cudaStream_t st, const args_t< R > & a, in
                 k_update< MHD, R, true ><<< ug, 256, 0, st >>>( a, stage, make_udiv( unsigned( n[ 0 ] + 1 ) ) ); } );
             return;
         }
-    timed( 6, [ & ] { k_update< MHD, R ><<< ug, 256, 0, st >>>( a, stage, make_udiv( unsigned( n[ 0 ] + 1 ) ) ); } );
+    timed( 6, [ & ] {
+        if( MHD )
+        {
+            k_update< MHD, R, false, 1 ><<< ug, 256, 0, st >>>( a, stage, make_udiv( unsigned( n[ 0 ] + 1 ) ) );
+            k_update< MHD, R, false, 2 ><<< ug, 256, 0, st >>>( a, stage, make_udiv( unsigned( n[ 0 ] + 1 ) ) );
+        }
+        else
+            k_update< MHD, R ><<< ug, 256, 0, st >>>( a, stage, make_udiv( unsigned( n[ 0 ] + 1 ) ) ); } );
 }
 
 // Halo transfer of one stage between this rank and its peers, and at stage 0
@@ -3106,7 +3115,7 @@ int kr_launches_per_step( kr_ctx * c )
         for( int l = 1; l <= c->max_level; ++ l )
             smr += c->prolong_off[ l ] > c->prolong_off[ l - 1 ];
     }
-    return 2 + 2 * ( ( c->cfg.mhd ? 3 : 2 ) + flux + phys + halo + smr );
+    return 2 + 2 * ( ( c->cfg.mhd ? 4 : 2 ) + flux + phys + halo + smr );
 }
 
 int kr_diagnostics( kr_ctx * c, double * max_div_b, double * totals5 )
