@@ -183,8 +183,10 @@ __global__ void k_step_end( scal_t * s, double dt_expand )
 // cons -> prim over the interior of every block, CFL dt at stage 0
 // (hydro/eos/adiabatic.h:211-258; mhd/eos/adiabatic.h:127-234).
 
-template< bool MHD, class R >
-__global__ void __launch_bounds__( 256, 4 ) k_c2p( const args_t< R > a, int step, udiv_t dv )
+// DT: stage 0's launch, which also reduces the CFL dt; stage 1's launch has none
+// of that code (fewer registers).
+template< bool MHD, class R, bool DT >
+__global__ void __launch_bounds__( 256, ( MHD && DT ) ? 3 : 4 ) k_c2p( const args_t< R > a, int step, udiv_t dv )
 {
     // grid: x over the cells of one (x, y) plane, y over z, z over blocks
     constexpr int NW = MHD ? 11 : 5;   // stored W words: prim (8) + cell E (3)
@@ -274,7 +276,7 @@ __global__ void __launch_bounds__( 256, 4 ) k_c2p( const args_t< R > a, int step
                 for( int k = 0; k < NW; ++ k )
                     o[ k * ngw ] = wv[ k ];
             }
-        if( step == 0 )
+        if( DT )
         {   // cfl * min_a dx_a / s_a as cfl / max_a ( s_a / dx_a ): one division
             // (the reference divides per axis; rounding differs only); like
             // fmin, fmax drops a NaN candidate
@@ -301,7 +303,7 @@ __global__ void __launch_bounds__( 256, 4 ) k_c2p( const args_t< R > a, int step
             dt = smax > 0 ? a.cfl / smax : FLT_MAX;
         }
     }
-    if( step == 0 )
+    if( DT )
     {
         __shared__ double red[ 8 ];
         dt = warp_min( dt );
@@ -1386,7 +1388,7 @@ void smr_correct5( const args_t< R > & a, const geo_t & g, int b, const int * i,
 // PART 0: cells and faces in one launch; 1: the conserved update only; 2: the
 // CT face update only (MHD: two launches, each with fewer registers).
 template< bool MHD, class R, bool SMR = false, int PART = 0 >
-__global__ void __launch_bounds__( 256, ( SMR && sizeof( R ) == 4 ) ? 3 : 4 ) k_update( const args_t< R > a, int step, udiv_t dv )
+__global__ void __launch_bounds__( 256, ( SMR && sizeof( R ) == 4 ) ? 3 : ( PART == 2 ? 6 : 4 ) ) k_update( const args_t< R > a, int step, udiv_t dv )
 {
     // grid: x over the lattice sites of one (x, y) plane, y over z, z over blocks
     constexpr int NF = MHD ? 7 : 5;
@@ -2146,7 +2148,7 @@ static void enqueue_front( kr_ctx * c, cudaStream_t st, const args_t< R > & a, i
 {
     const unsigned nb = unsigned( c->nblk );
     const int * n = c->cfg.n;
-    timed( 0, [ & ] { k_c2p< MHD, R ><<< dim3( blocks_for( ( long long ) n[ 0 ] * n[ 1 ], 256 ), n[ 2 ], nb ), 256, 0, st >>>(
+    timed( 0, [ & ] { ( stage == 0 ? k_c2p< MHD, R, true > : k_c2p< MHD, R, false > )<<< dim3( blocks_for( ( long long ) n[ 0 ] * n[ 1 ], 256 ), n[ 2 ], nb ), 256, 0, st >>>(
         a, stage, make_udiv( unsigned( n[ 0 ] ) ) ); } );
     if( ! c->hsend.items.empty(  ) )
         timed( 1, [ & ] {
