@@ -56,6 +56,7 @@ struct geo_t
 {
     double dx[ 3 ], sfc[ 3 ], vol;
     double idx[ 3 ];              // 1 / dx
+    double isfc[ 3 ];             // 1 / sfc (0 for an empty face)
     int phys;                     // bit 2a+s: side (a, s) is a non-periodic domain side
     int fine;                     // bit 2a+s: the neighbours across side (a, s) are finer
     int fitem[ 6 ];               // refined side: first of its 4 flux-average items
@@ -1265,34 +1266,36 @@ __global__ void __launch_bounds__( 256 ) k_emf( const args_t< R > a, udiv_t dv )
     int i[ 3 ] = { int( t - q * unsigned( e0 ) ), int( q ), int( blockIdx.y ) };
     const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
     const R w_e = R( 0.25f );
+    // one base offset per site (cell E in W, the fluxes, the edge EMF); the
+    // neighbours by constant strides
+    const long long oW = iw( a, b, 8, 11, i[ 0 ], i[ 1 ], i[ 2 ] );
+    const long long oF = ifx( a, b, 0, 7, i[ 0 ], i[ 1 ], i[ 2 ] );
+    const long long oE = ifx( a, b, 0, 3, i[ 0 ], i[ 1 ], i[ 2 ] );
+    const int sw[ 3 ] = { 1, a.sw1, a.sw2 }, sf[ 3 ] = { 1, a.sf1, a.sf2 };
     for( int ax = 0; ax < 3; ++ ax )
     {
         if( i[ ax ] >= nn[ ax ] )
             continue;
         const int ax1 = mod3( 1 + ax ), ax2 = mod3( 2 + ax );
+        const R * we = a.w + oW + ( long long ) ax * a.ngw;   // cell E_ax, stored by k_c2p
         R ec[ 2 ][ 2 ];
-        ec[ 1 ][ 1 ] = e_cell( a, b, i, ax );
-        -- i[ ax1 ];
-        ec[ 1 ][ 0 ] = e_cell( a, b, i, ax );
-        -- i[ ax2 ];
-        ec[ 0 ][ 0 ] = e_cell( a, b, i, ax );
-        ++ i[ ax1 ];
-        ec[ 0 ][ 1 ] = e_cell( a, b, i, ax );
-        ++ i[ ax2 ];
+        ec[ 1 ][ 1 ] = we[ 0 ];
+        ec[ 1 ][ 0 ] = we[ -sw[ ax1 ] ];
+        ec[ 0 ][ 0 ] = we[ -sw[ ax1 ] - sw[ ax2 ] ];
+        ec[ 0 ][ 1 ] = we[ -sw[ ax2 ] ];
         R e = 0;
         for( int it = 0; it < 2; ++ it )
         {
             const int a_para = it == 0 ? ax1 : ax2;
             const int a_perp = it == 0 ? ax2 : ax1;
-            -- i[ a_perp ];
-            const R ef_m = face_emf( a, b, a_para, ax, i );
-            ++ i[ a_perp ];
-            const R ef_p = face_emf( a, b, a_para, ax, i );
+            // E_ax held by the flux of axis a_para (face_emf's slot)
+            const R * fe = a.f[ a_para ] + oF + ( long long )( ( ax == mod3( a_para + 1 ) ) ? 5 : 6 ) * a.nfb;
+            const R ef_m = fe[ -sf[ a_perp ] ];
+            const R ef_p = fe[ 0 ];
             e += w_e * ( ef_m + ef_p );
-            const R frho_p = a.f[ a_perp ][ ifx( a, b, RHO, 7, i[ 0 ], i[ 1 ], i[ 2 ] ) ];
-            -- i[ a_para ];
-            const R frho_m = a.f[ a_perp ][ ifx( a, b, RHO, 7, i[ 0 ], i[ 1 ], i[ 2 ] ) ];
-            ++ i[ a_para ];
+            const R * fr = a.f[ a_perp ] + oF;                   // mass flux (RHO = 0)
+            const R frho_p = fr[ 0 ];
+            const R frho_m = fr[ -sf[ a_para ] ];
             const R de_p = frho_p > 0 ?  ( ec[ 0 ][ 1 ] - ef_m ) :  ( ec[ 1 ][ 1 ] - ef_p );
             const R de_m = frho_m > 0 ? -( ec[ 0 ][ 0 ] - ef_m ) : -( ec[ 1 ][ 0 ] - ef_p );
             e += w_e * ( de_m - de_p );
@@ -1303,7 +1306,7 @@ __global__ void __launch_bounds__( 256 ) k_emf( const args_t< R > a, udiv_t dv )
                 ec[ 1 ][ 0 ] = swp;
             }
         }
-        a.ee[ ifx( a, b, ax, 3, i[ 0 ], i[ 1 ], i[ 2 ] ) ] = e;
+        a.ee[ oE + ( long long ) ax * a.nfb ] = e;
     }
     if( ! a.emf_out )
         return;
@@ -1491,23 +1494,26 @@ __global__ void __launch_bounds__( 256, ( SMR && sizeof( R ) == 4 ) ? 3 : ( PART
         return;
     const double * __restrict__ bs = a.bf[ step ];
     double * __restrict__ bt = a.bf[ 1 - step ];
+    // one base offset per site; components and neighbours by constant strides
+    const long long oe = ifx( a, b, 0, 3, i[ 0 ], i[ 1 ], i[ 2 ] );
+    const long long ob = ibf( a, b, 0, i[ 0 ], i[ 1 ], i[ 2 ] );
+    const int se[ 3 ] = { 1, a.sf1, a.sf2 };
+    const int sb[ 3 ] = { 1, a.sb1, a.sb2 };
     for( int c = 0; c < 3; ++ c )
     {
         const int ax1 = mod3( c + 1 ), ax2 = mod3( c + 2 );
         if( i[ ax1 ] >= nn[ ax1 ] || i[ ax2 ] >= nn[ ax2 ] )
             continue;
+        const R * e1 = EE + oe + ( long long ) ax1 * a.nfb;
+        const R * e2 = EE + oe + ( long long ) ax2 * a.nfb;
         double db;
-        db  = double( EE[ ifx( a, b, ax1, 3, i[ 0 ], i[ 1 ], i[ 2 ] ) ] ) * g.dx[ ax1 ];
-        db -= double( EE[ ifx( a, b, ax2, 3, i[ 0 ], i[ 1 ], i[ 2 ] ) ] ) * g.dx[ ax2 ];
-        ++ i[ ax1 ];
-        db += double( EE[ ifx( a, b, ax2, 3, i[ 0 ], i[ 1 ], i[ 2 ] ) ] ) * g.dx[ ax2 ];
-        -- i[ ax1 ];
-        ++ i[ ax2 ];
-        db -= double( EE[ ifx( a, b, ax1, 3, i[ 0 ], i[ 1 ], i[ 2 ] ) ] ) * g.dx[ ax1 ];
-        -- i[ ax2 ];
-        const double sfc = g.sfc[ c ];
-        db *= ( sfc > 0 ? ( -dt / sfc ) : 0. );
-        const long long k = ibf( a, b, c, i[ 0 ], i[ 1 ], i[ 2 ] );
+        db  = double( e1[ 0 ] ) * g.dx[ ax1 ];
+        db -= double( e2[ 0 ] ) * g.dx[ ax2 ];
+        db += double( e2[ se[ ax1 ] ] ) * g.dx[ ax2 ];
+        db -= double( e1[ se[ ax2 ] ] ) * g.dx[ ax1 ];
+        // the reference scales by -dt / sfc; -dt * (1 / sfc) differs in rounding only
+        db *= -dt * g.isfc[ c ];
+        const long long k = ob + ( long long ) c * a.nbf;
         const double nb = db + ( step == 0 ? bs[ k ] : ( bs[ k ] + bt[ k ] ) / 2 );
         bt[ k ] = nb;
         // Same-level face-B ghost strips by push, for the next stage: a face
@@ -1522,9 +1528,8 @@ __global__ void __launch_bounds__( 256, ( SMR && sizeof( R ) == 4 ) ? 3 : ( PART
             const int dst = a.nbr[ b * 27 + 13 + s * ( t == 0 ? 1 : ( t == 1 ? 3 : 9 ) ) ];
             if( dst < 0 )
                 continue;
-            int j[ 3 ] = { i[ 0 ], i[ 1 ], i[ 2 ] };
-            j[ t ] = s < 0 ? nn[ t ] : -1;
-            bt[ ibf( a, dst, c, j[ 0 ], j[ 1 ], j[ 2 ] ) ] = nb;
+            const int dj = ( s < 0 ? nn[ t ] : -1 ) - i[ t ];
+            bt[ k + ( long long )( dst - b ) * 3 * a.nbf + ( long long ) dj * sb[ t ] ] = nb;
         }
     }
 }
@@ -2383,6 +2388,7 @@ static void set_geometry( kr_ctx * c )
             s *= o.dx[ ( a + 1 ) % 3 ];
             s *= o.dx[ ( a + 2 ) % 3 ];
             o.sfc[ a ] = s;
+            o.isfc[ a ] = s > 0 ? 1 / s : 0.;
             vol *= o.dx[ a ];
         }
         o.vol = vol;
