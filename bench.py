@@ -210,7 +210,9 @@ MODES = {"fp64": dict(precision=2, riemann=0), "mixed": dict(precision=1, rieman
 
 def train_selector(local_rank):
     """Selector for the learned mode, trained on the GPU from faces logged on
-    a 128^3 OT run (mixed step) and a 64^3 one: ~2 M samples, 20 epochs."""
+    a 128^3 OT run (mixed step) and a 64^3 one: ~1.9 M samples (one face in 32,
+    under the collection cap, so the training data do not depend on the order
+    in which device threads log them), 20 epochs."""
     from kratos_b200 import Dynamics, selector as S
 
     def make(nb):
@@ -220,7 +222,7 @@ def train_selector(local_rank):
             return d
         return f
     t0 = time.perf_counter()
-    w, info = S.build_selector([make((1, 1, 1)), make((2, 2, 2))], steps=4, stride=8,
+    w, info = S.build_selector([make((1, 1, 1)), make((2, 2, 2))], steps=4, stride=32,
                                epochs=20, device=local_rank)
     info["train_s"] = time.perf_counter() - t0
     info["threshold"] = S.DEFAULT_THRESHOLD

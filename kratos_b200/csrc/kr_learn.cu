@@ -25,10 +25,13 @@ constexpr int GRAD_SAMPLES = 64;     // samples per CTA in the gradient kernel
 constexpr int GRAD_THREADS = 256;
 
 // One CTA: forward / backward of GRAD_SAMPLES samples, then their summed
-// contribution to every parameter gradient (one atomicAdd per parameter per CTA).
+// contribution to every parameter gradient, written to the CTA's row of
+// `partial` ([gridDim.x][MLP_NPARAM]); k_grad_sum adds the rows in a fixed
+// order, so a gradient (and the training run) does not depend on the order
+// in which CTAs finish.
 __global__ void __launch_bounds__( GRAD_THREADS )
 k_mlp_grad( const float * X, const float * Y, long long n0, long long n,
-            const float * w, float wneg, float * grad, double * loss )
+            const float * w, float wneg, float * partial, double * loss )
 {
     __shared__ float sw[ MLP_NPARAM ];
     __shared__ float sx[ GRAD_SAMPLES ][ MLP_IN ];
@@ -113,7 +116,7 @@ k_mlp_grad( const float * X, const float * Y, long long n0, long long n,
         }
         else
             for( int s = 0; s < GRAD_SAMPLES; ++ s ) acc += dz[ s ];
-        atomicAdd( grad + k, acc );
+        partial[ ( size_t ) blockIdx.x * MLP_NPARAM + k ] = acc;
     }
     if( threadIdx.x == 0 )
     {
@@ -121,6 +124,17 @@ k_mlp_grad( const float * X, const float * Y, long long n0, long long n,
         for( int s = 0; s < GRAD_SAMPLES; ++ s ) l += sloss[ s ];
         atomicAdd( loss, l );
     }
+}
+
+__global__ void k_grad_sum( const float * partial, int rows, float * grad )
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if( k >= MLP_NPARAM )
+        return;
+    float g = 0;
+    for( int r = 0; r < rows; ++ r )
+        g += partial[ ( size_t ) r * MLP_NPARAM + k ];
+    grad[ k ] = g;
 }
 
 __global__ void k_adam( float * w, const float * grad, float * m, float * v, int t,
@@ -208,19 +222,20 @@ int kr_mlp_grad( const float * X, const float * Y, long long n, const float * w,
     g_learn_error.clear(  );
     if( ! X || ! Y || ! w || ! grad_out || n <= 0 ) { g_learn_error = "kr_mlp_grad: bad arguments"; return -1; }
     if( ! lk( cudaSetDevice( device ), "cudaSetDevice" ) ) return -1;
-    float * dX = nullptr, * dY = nullptr, * dw = nullptr, * dg = nullptr;
+    float * dX = nullptr, * dY = nullptr, * dw = nullptr, * dg = nullptr, * dp = nullptr;
     double * dl = nullptr;
+    const unsigned nb = unsigned( ( n + GRAD_SAMPLES - 1 ) / GRAD_SAMPLES );
     bool ok = lk( cudaMalloc( & dX, n * MLP_IN * 4 ), "malloc" ) && lk( cudaMalloc( & dY, n * 4 ), "malloc" )
            && lk( cudaMalloc( & dw, MLP_NPARAM * 4 ), "malloc" ) && lk( cudaMalloc( & dg, MLP_NPARAM * 4 ), "malloc" )
-           && lk( cudaMalloc( & dl, 8 ), "malloc" );
+           && lk( cudaMalloc( & dp, size_t( nb ) * MLP_NPARAM * 4 ), "malloc" ) && lk( cudaMalloc( & dl, 8 ), "malloc" );
     ok = ok && lk( cudaMemcpy( dX, X, n * MLP_IN * 4, cudaMemcpyHostToDevice ), "upload" )
             && lk( cudaMemcpy( dY, Y, n * 4, cudaMemcpyHostToDevice ), "upload" )
             && lk( cudaMemcpy( dw, w, MLP_NPARAM * 4, cudaMemcpyHostToDevice ), "upload" )
             && lk( cudaMemset( dg, 0, MLP_NPARAM * 4 ), "memset" ) && lk( cudaMemset( dl, 0, 8 ), "memset" );
     if( ok )
     {
-        const unsigned nb = unsigned( ( n + GRAD_SAMPLES - 1 ) / GRAD_SAMPLES );
-        k_mlp_grad<<< nb, GRAD_THREADS >>>( dX, dY, 0, n, dw, wneg, dg, dl );
+        k_mlp_grad<<< nb, GRAD_THREADS >>>( dX, dY, 0, n, dw, wneg, dp, dl );
+        k_grad_sum<<< ( MLP_NPARAM + 255 ) / 256, 256 >>>( dp, int( nb ), dg );
         ok = lk( cudaGetLastError(  ), "k_mlp_grad" ) && lk( cudaDeviceSynchronize(  ), "sync" );
     }
     double l = 0;
@@ -231,7 +246,7 @@ int kr_mlp_grad( const float * X, const float * Y, long long n, const float * w,
         for( int k = 0; k < MLP_NPARAM; ++ k ) grad_out[ k ] /= float( n );
         if( loss_out ) * loss_out = l / double( n );
     }
-    cudaFree( dX ); cudaFree( dY ); cudaFree( dw ); cudaFree( dg ); cudaFree( dl );
+    cudaFree( dX ); cudaFree( dY ); cudaFree( dw ); cudaFree( dg ); cudaFree( dp ); cudaFree( dl );
     return ok ? 0 : -1;
 }
 
@@ -248,11 +263,13 @@ int kr_mlp_train( const float * X, const float * Y, long long n, float * w, int 
     }
     if( ! lk( cudaSetDevice( device ), "cudaSetDevice" ) ) return -1;
     float * dX = nullptr, * dY = nullptr, * dw = nullptr, * dg = nullptr, * dm = nullptr, * dv = nullptr;
+    float * dp = nullptr;
     double * dl = nullptr;
+    const long long rows = ( std::min( n, ( long long ) batch ) + GRAD_SAMPLES - 1 ) / GRAD_SAMPLES;
     bool ok = lk( cudaMalloc( & dX, n * MLP_IN * 4 ), "malloc" ) && lk( cudaMalloc( & dY, n * 4 ), "malloc" )
            && lk( cudaMalloc( & dw, MLP_NPARAM * 4 ), "malloc" ) && lk( cudaMalloc( & dg, MLP_NPARAM * 4 ), "malloc" )
            && lk( cudaMalloc( & dm, MLP_NPARAM * 4 ), "malloc" ) && lk( cudaMalloc( & dv, MLP_NPARAM * 4 ), "malloc" )
-           && lk( cudaMalloc( & dl, 8 ), "malloc" );
+           && lk( cudaMalloc( & dp, size_t( rows ) * MLP_NPARAM * 4 ), "malloc" ) && lk( cudaMalloc( & dl, 8 ), "malloc" );
     ok = ok && lk( cudaMemcpy( dX, X, n * MLP_IN * 4, cudaMemcpyHostToDevice ), "upload" )
             && lk( cudaMemcpy( dY, Y, n * 4, cudaMemcpyHostToDevice ), "upload" )
             && lk( cudaMemcpy( dw, w, MLP_NPARAM * 4, cudaMemcpyHostToDevice ), "upload" )
@@ -265,9 +282,9 @@ int kr_mlp_train( const float * X, const float * Y, long long n, float * w, int 
         for( long long b0 = 0; b0 < n && ok; b0 += batch )
         {
             const long long b1 = std::min( n, b0 + ( long long ) batch );
-            cudaMemsetAsync( dg, 0, MLP_NPARAM * 4 );
             const unsigned nb = unsigned( ( b1 - b0 + GRAD_SAMPLES - 1 ) / GRAD_SAMPLES );
-            k_mlp_grad<<< nb, GRAD_THREADS >>>( dX, dY, b0, b1, dw, wneg, dg, dl );
+            k_mlp_grad<<< nb, GRAD_THREADS >>>( dX, dY, b0, b1, dw, wneg, dp, dl );
+            k_grad_sum<<< ( MLP_NPARAM + 255 ) / 256, 256 >>>( dp, int( nb ), dg );
             k_adam<<< ( MLP_NPARAM + 255 ) / 256, 256 >>>( dw, dg, dm, dv, ++ t, lr, 1.f / float( b1 - b0 ) );
             ok = lk( cudaGetLastError(  ), "train kernels" );
         }
@@ -277,7 +294,8 @@ int kr_mlp_train( const float * X, const float * Y, long long n, float * w, int 
     }
     ok = ok && lk( cudaMemcpy( w, dw, MLP_NPARAM * 4, cudaMemcpyDeviceToHost ), "download" );
     if( ok && loss_out ) * loss_out = last;
-    cudaFree( dX ); cudaFree( dY ); cudaFree( dw ); cudaFree( dg ); cudaFree( dm ); cudaFree( dv ); cudaFree( dl );
+    cudaFree( dX ); cudaFree( dY ); cudaFree( dw ); cudaFree( dg ); cudaFree( dm ); cudaFree( dv );
+    cudaFree( dp ); cudaFree( dl );
     return ok ? 0 : -1;
 }
 

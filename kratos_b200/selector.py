@@ -66,12 +66,26 @@ def infer(X, w, device=0):
 
 
 def collect(dyn, steps, stride=64, seed=0, max_samples=1 << 21):
+    """Faces sampled from `steps` ordinary steps (a hash of the face picks one
+    in `stride`).  The device appends them in whatever order its threads get
+    there; they come back in a canonical order (sorted by a hash of their
+    bytes), so the same run gives the same training data.  Raises if the
+    samples would overflow `max_samples`: which ones were kept would then
+    depend on that order too."""
     out = np.empty((max_samples, N_IN + 1), np.float32)
     n = ctypes.c_longlong()
     rc = L.lib().kr_selector_collect(dyn._h, int(steps), int(stride), int(seed), int(max_samples),
                                      _p(out), ctypes.byref(n))
     dyn._check(rc, "kr_selector_collect")
+    if n.value >= max_samples:
+        raise ValueError("selector sampling reached %d samples; use a larger stride" % max_samples)
     out = out[:n.value]
+    words = out.view(np.uint32).astype(np.uint64)
+    h = np.zeros(len(out), np.uint64)
+    with np.errstate(over="ignore"):
+        for j in range(words.shape[1]):
+            h = (h ^ words[:, j]) * np.uint64(0x100000001B3)
+    out = out[np.argsort(h, kind="stable")]
     return out[:, :N_IN].copy(), out[:, N_IN].copy()
 
 
