@@ -106,3 +106,19 @@ def test_learned_step_error_and_gain():
     print("sel_period 4: rel L1 density %.2e (HLLE on %.1f%% of faces)" % (e_p4, 100 * cheap4 / faces4))
     assert e_p4 <= 1e-4 and div4 <= 1e-12
     assert cheap4 / faces4 > 0.3
+
+
+def test_gradient_and_training_are_reproducible():
+    """The gradient kernel writes one row of partial sums per CTA, added in a
+    fixed order: the mean gradient and a training run give the same bits every
+    time (float atomics would not)."""
+    from kratos_b200 import selector as S
+    X, y = _data(30000, seed=7)
+    w0 = S.init_params(3)
+    l1, g1 = S.grad(X, y, w0, wneg=4.0)
+    l2, g2 = S.grad(X, y, w0, wneg=4.0)
+    assert np.array_equal(g1, g2)
+    wa, _ = S.train(X, y, w=w0, epochs=3, batch=4096)
+    wb, _ = S.train(X, y, w=w0, epochs=3, batch=4096)
+    assert np.array_equal(wa, wb)
+    assert not np.array_equal(wa, w0)
