@@ -122,3 +122,15 @@ def test_uniform_state_stays_uniform_across_levels():
     d.step(5)
     out, _ = d.get_state()
     np.testing.assert_allclose(out, u, rtol=1e-13, atol=1e-13)
+
+
+def test_refined_mixed_precision_with_sides_against_reference():
+    """The mixed step on the refined fixture with reflecting / outflow / free
+    sides and ragged blocks, against the reference's FP64 run."""
+    meta, g = G.load("smr_bc")
+    d = _dyn(meta, precision=1)
+    d.init_problem("shock", meta["seed"])
+    d.step(meta["steps"])
+    u, _ = d.get_state()
+    assert d.status() == 0
+    assert rel_l1(u[..., 0], g["u1"][..., 0]) <= TOL_MIXED
