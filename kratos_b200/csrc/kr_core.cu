@@ -970,6 +970,49 @@ template< class R, int MODE > constexpr int flux_min_ctas(  )
                             : ( MODE == KR_RIEMANN_HLLE ? 5 : 4 );
 }
 
+// PLM of the NP primitive words of one face from the four cells around it
+// (wb: the right cell's first word, st: stride along the sweep, ngw: word
+// stride); the normal B of an MHD face comes from the face lattice instead.
+// FP32: words k and k + NP / 2 in pairs (plm_face_fast2).
+template< bool MHD, class R > __device__ __forceinline__
+void plm_stencil( const args_t< R > & a, int b, int axis, int step, const int * ii, const R * wb,
+                  int st, R * ql, R * qr )
+{
+    constexpr int NP = MHD ? 8 : 5;
+    const int ngw = int( a.ngw );
+    if constexpr( sizeof( R ) == 4 )
+    {
+        constexpr int H = NP / 2;
+        for( int k = 0; k < H; ++ k )
+        {
+            const R * p = wb + k * ngw, * p2 = wb + ( k + H ) * ngw;
+            float2 l2, r2;
+            plm_face_fast2( make_float2( p[ -2 * st ], p2[ -2 * st ] ), make_float2( p[ -st ], p2[ -st ] ),
+                            make_float2( p[ 0 ], p2[ 0 ] ), make_float2( p[ st ], p2[ st ] ), l2, r2 );
+            ql[ k ] = l2.x; ql[ k + H ] = l2.y;
+            qr[ k ] = r2.x; qr[ k + H ] = r2.y;
+        }
+        if constexpr( NP % 2 )
+        {
+            const R * p = wb + ( NP - 1 ) * ngw;
+            plm_face_fast< R >( p[ -2 * st ], p[ -st ], p[ 0 ], p[ st ], ql[ NP - 1 ], qr[ NP - 1 ] );
+        }
+        if constexpr( MHD )
+            ql[ BCC + axis ] = qr[ BCC + axis ] = R( a.bf[ step ][ ibf( a, b, axis, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] );
+    }
+    else
+        for( int k = 0; k < NP; ++ k )
+        {
+            if( MHD && k == BCC + axis )
+            {
+                ql[ k ] = qr[ k ] = R( a.bf[ step ][ ibf( a, b, axis, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] );
+                continue;
+            }
+            const R * p = wb + k * ngw;
+            plm_face_fast< R >( p[ -2 * st ], p[ -st ], p[ 0 ], p[ st ], ql[ k ], qr[ k ] );
+        }
+}
+
 // One CTA's 128 faces of a sweep: bx = CTA along the faces of one (x, y)
 // plane (lines: along all line faces), by = z plane, blockIdx.z = block; dv
 // divides by the row length.
@@ -977,7 +1020,6 @@ template< bool MHD, class R, int MODE > __device__ __forceinline__
 void flux_faces( const args_t< R > & a, int axis, int step, int lines, udiv_t dv, unsigned bx, unsigned by )
 {
     constexpr int NW = MHD ? 11 : 5;   // stored W words: prim (8) + cell E (3)
-    constexpr int NP = MHD ? 8 : 5;    // primitive words reconstructed
     constexpr bool learned = MHD && MODE == KR_RIEMANN_LEARNED;
     const int b = blockIdx.z;
     const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
@@ -1038,18 +1080,7 @@ void flux_faces( const args_t< R > & a, int axis, int step, int lines, udiv_t dv
     {
         const R * wb = a.w + ( size_t ) b * NW * a.ngw
                      + ( ( ii[ 0 ] + 2 ) + a.sw1 * ( ii[ 1 ] + 2 ) + a.sw2 * ( ii[ 2 ] + 2 ) );
-        const int ngw = int( a.ngw );
-        for( int k = 0; k < NP; ++ k )
-        {
-            if( MHD && k == BCC + axis )
-            {
-                const R bn = R( a.bf[ step ][ ibf( a, b, axis, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] );
-                ql[ k ] = qr[ k ] = bn;
-                continue;
-            }
-            const R * p = wb + k * ngw;
-            plm_face_fast< R >( p[ -2 * st ], p[ -st ], p[ 0 ], p[ st ], ql[ k ], qr[ k ] );
-        }
+        plm_stencil< MHD, R >( a, b, axis, step, ii, wb, st, ql, qr );
     }
     if constexpr( learned )
     {   // the per-face kernel covers every face of the sweep here (lines == 0)
@@ -1090,7 +1121,6 @@ __global__ void __launch_bounds__( 128, ( flux_min_ctas< R, KR_RIEMANN_DEFAULT >
 k_flux_list( const args_t< R > a, int axis, int step )
 {
     constexpr int NW = MHD ? 11 : 5;
-    constexpr int NP = MHD ? 8 : 5;
     if( step == 0 && sel_eval_step( a.s, a.sel_period ) )
         return;                       // the network's sweep (k_flux_eval) solves this one
     const int b = blockIdx.z;
@@ -1116,17 +1146,7 @@ k_flux_list( const args_t< R > a, int axis, int step )
     R ql[ 8 ], qr[ 8 ];
     const R * wb = a.w + ( size_t ) b * NW * a.ngw
                  + ( ( ii[ 0 ] + 2 ) + a.sw1 * ( ii[ 1 ] + 2 ) + a.sw2 * ( ii[ 2 ] + 2 ) );
-    const int ngw = int( a.ngw );
-    for( int k = 0; k < NP; ++ k )
-    {
-        if( MHD && k == BCC + axis )
-        {
-            ql[ k ] = qr[ k ] = R( a.bf[ step ][ ibf( a, b, axis, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] );
-            continue;
-        }
-        const R * p = wb + k * ngw;
-        plm_face_fast< R >( p[ -2 * st ], p[ -st ], p[ 0 ], p[ st ], ql[ k ], qr[ k ] );
-    }
+    plm_stencil< MHD, R >( a, b, axis, step, ii, wb, st, ql, qr );
     if( cheap )
         solve_store< MHD, R, KR_RIEMANN_HLLE >( a, b, axis, ii, true, ql, qr, 0, 0ull );
     else

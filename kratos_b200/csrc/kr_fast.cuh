@@ -62,6 +62,32 @@ void plm_face_fast( R q_ll, R q_l, R q_r, R q_rr, R & ql, R & qr )
     qr = rpos ? q_r - dq2_r * sl * inv * scale : q_r;
 }
 
+// The FP32 limiter of plm_face_fast on two variables at once (.x, .y): the
+// differences, sums and products as paired FP32 instructions (sm_100's
+// FADD2 / FMUL2 / FFMA2), the sign tests and reciprocals per element.  Same
+// operations per element as the scalar form.
+__device__ __forceinline__
+void plm_face_fast2( float2 q_ll, float2 q_l, float2 q_r, float2 q_rr, float2 & ql, float2 & qr )
+{
+    const float2 m1 = make_float2( -1.f, -1.f );
+    const float2 dql = __ffma2_rn( q_ll, m1, q_l );      // q_l - q_ll, exact
+    const float2 dqc = __ffma2_rn( q_l, m1, q_r );
+    const float2 dqr = __ffma2_rn( q_r, m1, q_rr );
+    const float tiny = FLT_MIN;
+    const bool lx = fminf( dql.x, dqc.x ) > tiny || fmaxf( dql.x, dqc.x ) < -tiny;
+    const bool ly = fminf( dql.y, dqc.y ) > tiny || fmaxf( dql.y, dqc.y ) < -tiny;
+    const bool rx = fminf( dqr.x, dqc.x ) > tiny || fmaxf( dqr.x, dqc.x ) < -tiny;
+    const bool ry = fminf( dqr.y, dqc.y ) > tiny || fmaxf( dqr.y, dqc.y ) < -tiny;
+    const float2 sl = __fadd2_rn( dql, dqc ), sr = __fadd2_rn( dqc, dqr );
+    const float2 il = make_float2( rcp( sl.x ), rcp( sl.y ) ), ir = make_float2( rcp( sr.x ), rcp( sr.y ) );
+    const float2 tl = __fmul2_rn( dqc, il );
+    const float2 tr = __fmul2_rn( __fmul2_rn( dqc, ir ), m1 );
+    const float2 cl = __ffma2_rn( dql, tl, q_l );        // q_l + dql ( dqc / ( dql + dqc ) )
+    const float2 cr = __ffma2_rn( dqr, tr, q_r );        // q_r - dqr ( dqc / ( dqc + dqr ) )
+    ql = make_float2( lx ? cl.x : q_l.x, ly ? cl.y : q_l.y );
+    qr = make_float2( rx ? cr.x : q_r.x, ry ? cr.y : q_r.y );
+}
+
 // Fast magnetosonic speed from squared field components and 1 / rho.
 template< class R > __device__ __forceinline__
 R c_fms_fast( R pre, R inv_rho, R bn2, R bt2, R gam )
