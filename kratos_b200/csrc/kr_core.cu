@@ -1116,8 +1116,10 @@ k_flux_eval( const args_t< R > a, int axis, int step, udiv_t dv, unsigned cpp, u
 // (axis, block) HLLD and HLLE lists built by the last evaluation.  Warps run
 // one solver; entries of a warp come from one or two producer warps, so loads
 // and stores stay nearly coalesced.
+// (both solvers in one kernel: 72 registers, 7 CTAs / SM, no spills; capped at
+// 64 for 8 CTAs it spilled and ran 1.5% slower)
 template< bool MHD, class R >
-__global__ void __launch_bounds__( 128, ( flux_min_ctas< R, KR_RIEMANN_DEFAULT >(  ) ) )
+__global__ void __launch_bounds__( 128, 7 )
 k_flux_list( const args_t< R > a, int axis, int step )
 {
     constexpr int NW = MHD ? 11 : 5;
