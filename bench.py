@@ -40,11 +40,12 @@ BYTES_PER_ZONE_CYCLE = 320
 FLUX_BYTES_PER_FACE = {4: 8 * 4 + 8 + 7 * 4, 8: 8 * 8 + 8 + 7 * 8}
 # DRAM bytes per face of one FP32 flux launch, ncu dram__bytes_read.sum +
 # dram__bytes_write.sum on the 128^3 sample (8 blocks of 64^3) divided by its
-# 2.26 M faces; traffic scales with the faces (same block shape)
-FLUX_DRAM_BYTES_PER_FACE = 54.9
-# the same for the learned mode's list sweep (k_flux_list): 146.4 MB per launch
+# 2.26 M faces (two captured launches, 135.9 MB on average); traffic scales with
+# the faces (same block shape)
+FLUX_DRAM_BYTES_PER_FACE = 60.0
+# the same for the learned mode's list sweep (k_flux_list): 153.5 MB per launch
 # averaged over four captured launches on the 128^3 sample, 2.26 M faces
-FLUX_LIST_DRAM_BYTES_PER_FACE = 64.7
+FLUX_LIST_DRAM_BYTES_PER_FACE = 67.8
 WORKLOAD = "ot 256^3 periodic MHD, 64 blocks of 64^3, PLM+HLLD+CT, Heun RK2"
 
 
