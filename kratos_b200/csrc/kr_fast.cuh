@@ -38,15 +38,17 @@ void plm_face_fast( R q_ll, R q_l, R q_r, R q_rr, R & ql, R & qr )
     if constexpr( sizeof( R ) == 4 )
     {   // Scale-free form of the same limiter: dl dr / ( dl + dr ) =
         // dl * ( dr / ( dl + dr ) ), whose quotient lies in ( 0, 1 ) when dl
-        // and dr share a sign, so no product of two differences is formed --
-        // no FP32 underflow for tiny or overflow for huge differences (the
+        // and dr share a sign, so the slope never forms the product of two
+        // differences -- no FP32 overflow for huge differences (the
         // reference's FP32 path rescales by max |d| for the same purpose).
-        // Differences below FLT_MIN give no slope: the SFU reciprocal of a
-        // subnormal sum is 1 / 0 = inf (a slope that small is below the FP32
-        // resolution of any state it would change).
-        const R tiny = R( FLT_MIN );
-        const bool lpos = fminf( dql, dqc ) > tiny || fmaxf( dql, dqc ) < -tiny;
-        const bool rpos = fminf( dqr, dqc ) > tiny || fmaxf( dqr, dqc ) < -tiny;
+        // Same sign is a positive product of the two differences (the limited
+        // slope itself is formed scale-free below).  A positive product needs
+        // one difference of normal size, so the sum is normal and its SFU
+        // reciprocal finite (a subnormal sum would give 1 / 0 = inf); two
+        // differences whose product underflows (both below ~1e-23) give no
+        // slope.  plm_face_fast2 makes the same test on pairs.
+        const bool lpos = dql * dqc > R( 0 );
+        const bool rpos = dqr * dqc > R( 0 );
         ql = lpos ? q_l + dql * ( dqc * rcp( dql + dqc ) ) : q_l;
         qr = rpos ? q_r - dqr * ( dqc * rcp( dqc + dqr ) ) : q_r;
         return;
@@ -73,11 +75,12 @@ void plm_face_fast2( float2 q_ll, float2 q_l, float2 q_r, float2 q_rr, float2 & 
     const float2 dql = __ffma2_rn( q_ll, m1, q_l );      // q_l - q_ll, exact
     const float2 dqc = __ffma2_rn( q_l, m1, q_r );
     const float2 dqr = __ffma2_rn( q_r, m1, q_rr );
-    const float tiny = FLT_MIN;
-    const bool lx = fminf( dql.x, dqc.x ) > tiny || fmaxf( dql.x, dqc.x ) < -tiny;
-    const bool ly = fminf( dql.y, dqc.y ) > tiny || fmaxf( dql.y, dqc.y ) < -tiny;
-    const bool rx = fminf( dqr.x, dqc.x ) > tiny || fmaxf( dqr.x, dqc.x ) < -tiny;
-    const bool ry = fminf( dqr.y, dqc.y ) > tiny || fmaxf( dqr.y, dqc.y ) < -tiny;
+    // same sign: a positive product (paired multiply, one compare each).  A
+    // positive product needs one difference of normal size, so the sum below
+    // is normal and its SFU reciprocal finite; differences whose product
+    // underflows (both below ~1e-23) give no slope
+    const float2 pl = __fmul2_rn( dql, dqc ), pr = __fmul2_rn( dqr, dqc );
+    const bool lx = pl.x > 0.f, ly = pl.y > 0.f, rx = pr.x > 0.f, ry = pr.y > 0.f;
     const float2 sl = __fadd2_rn( dql, dqc ), sr = __fadd2_rn( dqc, dqr );
     const float2 il = make_float2( rcp( sl.x ), rcp( sl.y ) ), ir = make_float2( rcp( sr.x ), rcp( sr.y ) );
     const float2 tl = __fmul2_rn( dqc, il );
