@@ -43,9 +43,6 @@ FLUX_BYTES_PER_FACE = {4: 8 * 4 + 8 + 7 * 4, 8: 8 * 8 + 8 + 7 * 8}
 # 2.26 M faces (two captured launches, 135.9 MB on average); traffic scales with
 # the faces (same block shape)
 FLUX_DRAM_BYTES_PER_FACE = 60.0
-# the same for the learned mode's list sweep (k_flux_list): 153.5 MB per launch
-# averaged over four captured launches on the 128^3 sample, 2.26 M faces
-FLUX_LIST_DRAM_BYTES_PER_FACE = 67.8
 WORKLOAD = "ot 256^3 periodic MHD, 64 blocks of 64^3, PLM+HLLD+CT, Heun RK2"
 
 
@@ -381,11 +378,9 @@ def flux_roofline(h, head, world, peak, peak_kind):
     k = h["kernels_ms_per_step"]
     launch_ms = (k["flux_x"] + k["flux_y"] + k["flux_z"]) / 6.0      # 3 sweeps x 2 stages
     gbs = faces * FLUX_BYTES_PER_FACE[rsize] / (launch_ms * 1e-3) / 1e9
-    learned = head.startswith("learned")
-    per_face = FLUX_LIST_DRAM_BYTES_PER_FACE if learned else FLUX_DRAM_BYTES_PER_FACE
-    return {"bound": "hbm", "kernel": "%s (one sweep, %s mode)" % ("k_flux_list" if learned else "k_flux", head),
+    return {"bound": "hbm", "kernel": "k_flux (one sweep, %s mode)" % head,
             "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
-            "traffic": per_face * faces if rsize == 4 else None,
+            "traffic": FLUX_DRAM_BYTES_PER_FACE * faces if rsize == 4 else None,
             "algorithmic_bytes_per_launch": faces * FLUX_BYTES_PER_FACE[rsize],
             "launch_ms": launch_ms,
             "basis": "%d B/face x %d faces per launch (%s peak); the sweep is bound by instruction "

@@ -91,10 +91,8 @@ struct args_t
     const float * sel_b;              // b1, b2, b3
     float sel_thr;                    // logit threshold for HLLE
     unsigned long long * sel_cnt;     // [0] faces, [1] faces given HLLE
-    unsigned * sel_list;              // per (axis, block): HLLD faces from the front,
-                                      // HLLE faces from the back (packed positions)
-    unsigned * sel_count;             // per (axis, block): [HLLD, HLLE] list lengths
-    long long sel_cap;                // list capacity per (axis, block)
+    unsigned char * sel_dec;          // per (axis, block, warp of 32 faces): 1 = HLLE
+    long long sel_wcap;               // warps of faces per (axis, block)
     int sel_period;                   // steps between evaluations of the network
     // face sampling for selector training (collect steps only)
     float * smp;                      // [max][17]: 16 features + flux gap
@@ -160,12 +158,9 @@ __device__ __forceinline__ bool sel_eval_step( const scal_t * s, int period )
     return s->sel_force || s->n_steps % period == 0;
 }
 
-__global__ void k_step_begin( scal_t * s, unsigned * sel_count, int n_count, int period )
+__global__ void k_step_begin( scal_t * s )
 {
     s->dt_bits = __double_as_longlong( s->dt_bound );
-    if( sel_count && sel_eval_step( s, period ) )
-        for( int k = 0; k < n_count; ++ k )
-            sel_count[ k ] = 0;
 }
 
 __global__ void k_step_end( scal_t * s, double dt_expand )
@@ -803,6 +798,9 @@ __global__ void __launch_bounds__( 128 ) k_phys_mhd( const args_t< R > a, int si
 // (HLLD step that also logs selector training samples).  Compile-time, so the
 // plain step carries none of the selector's registers.
 constexpr int FLUX_SAMPLE = 3;
+// Learned mode, the sweeps without the network: each warp of faces runs the
+// solver the last evaluation chose for it.
+constexpr int FLUX_APPLY = 4;
 
 // Riemann solve of one face from its reconstructed states and store of the
 // flux (and, for MHD, the two edge EMFs: hlld.h:42-46 -- slot 5 holds
@@ -875,14 +873,14 @@ void solve_store( const args_t< R > & a, int b, int axis, const int * ii, bool v
 // those ghost lines (the tiled kernel below does the rest).
 // Learned mode (no reference counterpart).  The network runs at stage 0 of
 // every sel_period-th step (and the step after new weights): this sweep
-// evaluates it for every face, appends each face to its (axis, block) HLLD or
-// HLLE list, sorts the CTA's 128 faces into one run of HLLD faces and one run
-// of HLLE faces through shared memory (so that each warp executes one solver:
-// a per-face choice inside a warp makes the warp pay for both) and solves
-// them.  Every other sweep runs k_flux_list over the two lists.
+// evaluates it for every face, and a warp's 32 faces go to HLLE together, only
+// when it passes every one of them (a face it flags keeps its warp on HLLD).
+// Each warp thus runs one solver, and the choice is one byte per warp
+// (sel_dec, wid: the warp's number in the sweep's chunk order), which the
+// other sweeps of the period read (FLUX_APPLY) on the same face grid.
 template< bool MHD, class R > __device__ __forceinline__
 void learned_solve( const args_t< R > & a, int b, int axis, const int * ii, bool valid,
-                    R * ql, R * qr )
+                    R * ql, R * qr, unsigned wid )
 {
     constexpr int NF = 7;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -893,67 +891,31 @@ void learned_solve( const args_t< R > & a, int b, int axis, const int * ii, bool
     idx_swap( ql + MOM, axis ); idx_swap( qr + MOM, axis );
     idx_swap( ql + BCC, axis ); idx_swap( qr + BCC, axis );
     __shared__ __nv_bfloat16 xs[ 4 ][ 32 * MLP_IN ];
-    __shared__ R sq[ 128 ][ 17 ];                // rotated left / right states (+1 pad)
-    __shared__ int sid[ 128 ];                   // face position, packed
-    __shared__ int cnt[ 4 ][ 2 ];
     // the network: every lane of the warp takes part in the MMAs
     float f[ MLP_IN ];
     face_features< R >( ql, qr, e.gamma, f );
     const float z = mlp_logit( f, a.sel_w, a.sel_b, xs[ warp ] );
-    const bool cheap = valid && z > a.sel_thr;
-    const unsigned mh = __ballot_sync( 0xffffffffu, valid && ! cheap );
-    const unsigned mc = __ballot_sync( 0xffffffffu, cheap );
-    const unsigned below = ( 1u << lane ) - 1u;
-    // append this warp's faces to the (axis, block) lists the other sweeps use
-    unsigned * cntg = a.sel_count + ( ( size_t ) axis * a.nblk + b ) * 2;
-    unsigned * list = a.sel_list + ( ( size_t ) axis * a.nblk + b ) * a.sel_cap;
-    unsigned bh = 0, bc = 0;
+    const unsigned mv = __ballot_sync( 0xffffffffu, valid );
+    const unsigned mc = __ballot_sync( 0xffffffffu, valid && z > a.sel_thr );
+    const bool cheap = mv != 0u && mc == mv;
     if( lane == 0 )
     {
-        cnt[ warp ][ 0 ] = __popc( mh );
-        cnt[ warp ][ 1 ] = __popc( mc );
-        if( mh ) bh = atomicAdd( cntg, ( unsigned ) __popc( mh ) );
-        if( mc ) bc = atomicAdd( cntg + 1, ( unsigned ) __popc( mc ) );
-        if( mh | mc )
+        a.sel_dec[ ( ( size_t ) axis * a.nblk + b ) * a.sel_wcap + wid ] = cheap ? 1 : 0;
+        if( mv )
         {
-            atomicAdd( a.sel_cnt, ( unsigned long long ) __popc( mh | mc ) );
-            atomicAdd( a.sel_cnt + 1, ( unsigned long long ) __popc( mc ) );
+            atomicAdd( a.sel_cnt, ( unsigned long long ) __popc( mv ) );
+            if( cheap )
+                atomicAdd( a.sel_cnt + 1, ( unsigned long long ) __popc( mv ) );
         }
     }
-    bh = __shfl_sync( 0xffffffffu, bh, 0 );
-    bc = __shfl_sync( 0xffffffffu, bc, 0 );
-    const unsigned packed = unsigned( ( ii[ 0 ] + 2 ) | ( ( ii[ 1 ] + 2 ) << 10 ) | ( ( ii[ 2 ] + 2 ) << 20 ) );
-    if( valid && ! cheap ) list[ bh + __popc( mh & below ) ] = packed;
-    else if( cheap )       list[ a.sel_cap - 1 - ( bc + __popc( mc & below ) ) ] = packed;
-    __syncthreads(  );
-    int nh = 0, nh_before = 0, nc_before = 0, nall = 0;
-    for( int w = 0; w < 4; ++ w )
-    {
-        nh += cnt[ w ][ 0 ];
-        nall += cnt[ w ][ 0 ] + cnt[ w ][ 1 ];
-        if( w < warp ) { nh_before += cnt[ w ][ 0 ]; nc_before += cnt[ w ][ 1 ]; }
-    }
-    int slot = -1;
-    if( valid && ! cheap ) slot = nh_before + __popc( mh & below );
-    else if( cheap )       slot = nh + nc_before + __popc( mc & below );
-    if( slot >= 0 )
-    {
-        for( int k = 0; k < 8; ++ k ) { sq[ slot ][ k ] = ql[ k ]; sq[ slot ][ 8 + k ] = qr[ k ]; }
-        sid[ slot ] = int( packed );
-    }
-    __syncthreads(  );
-    const int j = threadIdx.x;
-    if( j >= nall )
+    if( ! valid )
         return;
-    R l[ 8 ], r[ 8 ], flx[ 8 ];
-    for( int k = 0; k < 8; ++ k ) { l[ k ] = sq[ j ][ k ]; r[ k ] = sq[ j ][ 8 + k ]; }
-    const int pk = sid[ j ];
-    const int f0 = ( pk & 1023 ) - 2, f1 = ( ( pk >> 10 ) & 1023 ) - 2, f2 = ( pk >> 20 ) - 2;
-    if( j < nh ) hlld_fast< R >( flx, l, r, e );
-    else         hlle_fast< R >( flx, l, r, e );
+    R flx[ 8 ];
+    if( cheap ) hlle_fast< R >( flx, ql, qr, e );
+    else        hlld_fast< R >( flx, ql, qr, e );
     idx_swap( flx + MOM, 3 - axis );
     R * F = a.f[ axis ] + ( size_t ) b * NF * a.nfb;
-    const int off = ( f0 + 1 ) + a.sf1 * ( f1 + 1 ) + a.sf2 * ( f2 + 1 );
+    const int off = ( ii[ 0 ] + 1 ) + a.sf1 * ( ii[ 1 ] + 1 ) + a.sf2 * ( ii[ 2 ] + 1 );
     const int nfb = int( a.nfb );
     for( int k = 0; k < 5; ++ k )
         F[ k * nfb + off ] = flx[ k ];
@@ -963,10 +925,13 @@ void learned_solve( const args_t< R > & a, int b, int axis, const int * ii, bool
 
 // Resident CTAs per SM the per-face sweep is compiled for: register budgets
 // that ptxas meets without spilling (FP32 default / HLLE: 64 registers, 8 CTAs;
-// learned: 6; FP64: 4).
+// learned with the network: 6; FP64: 4).  The learned sweep without the network
+// holds both solvers: at 64 registers it spills 12 bytes and still ran 0.5%
+// faster per step than at 72 (7 CTAs).
 template< class R, int MODE > constexpr int flux_min_ctas(  )
 {
-    return sizeof( R ) == 4 ? ( MODE <= KR_RIEMANN_HLLE ? 8 : ( MODE == KR_RIEMANN_LEARNED ? 6 : 4 ) )
+    return sizeof( R ) == 4 ? ( ( MODE <= KR_RIEMANN_HLLE || MODE == FLUX_APPLY ) ? 8
+                                : ( MODE == KR_RIEMANN_LEARNED ? 6 : 4 ) )
                             : ( MODE == KR_RIEMANN_HLLE ? 5 : 4 );
 }
 
@@ -1074,6 +1039,13 @@ void flux_faces( const args_t< R > & a, int axis, int step, int lines, udiv_t dv
     const bool valid = t < total && outside <= 1;
     if( ! valid && ! learned )
         return;
+    // learned mode: the warp's place in the sweep's chunk order (chunks of 128
+    // faces, z plane outer, 4 warps each); without the network its solver
+    // choice is loaded here, in flight with the stencil loads
+    const unsigned wid = ( by * ( ( total + 127u ) >> 7 ) + bx ) * 4u + ( threadIdx.x >> 5 );
+    bool hlle_warp = false;
+    if constexpr( MODE == FLUX_APPLY )
+        hlle_warp = a.sel_dec[ ( ( size_t ) axis * a.nblk + b ) * a.sel_wcap + wid ] != 0;
     const int st = axis == 0 ? 1 : ( axis == 1 ? a.sw1 : a.sw2 );
     R ql[ 8 ], qr[ 8 ];
     if( valid )
@@ -1082,9 +1054,14 @@ void flux_faces( const args_t< R > & a, int axis, int step, int lines, udiv_t dv
                      + ( ( ii[ 0 ] + 2 ) + a.sw1 * ( ii[ 1 ] + 2 ) + a.sw2 * ( ii[ 2 ] + 2 ) );
         plm_stencil< MHD, R >( a, b, axis, step, ii, wb, st, ql, qr );
     }
-    if constexpr( learned )
-    {   // the per-face kernel covers every face of the sweep here (lines == 0)
-        learned_solve< MHD, R >( a, b, axis, ii, valid, ql, qr );
+    if constexpr( learned || MODE == FLUX_APPLY )
+    {   // every face of the sweep here (lines == 0)
+        if constexpr( learned )
+            learned_solve< MHD, R >( a, b, axis, ii, valid, ql, qr, wid );
+        else if( hlle_warp )
+            solve_store< MHD, R, KR_RIEMANN_HLLE >( a, b, axis, ii, true, ql, qr, 0, 0ull );
+        else
+            solve_store< MHD, R, KR_RIEMANN_DEFAULT >( a, b, axis, ii, true, ql, qr, 0, 0ull );
         return;
     }
     const unsigned long long key = ( ( unsigned long long ) b * 3 + axis ) * 0x9E3779B97F4A7C15ull
@@ -1095,13 +1072,15 @@ void flux_faces( const args_t< R > & a, int axis, int step, int lines, udiv_t dv
 template< bool MHD, class R, int MODE >
 __global__ void __launch_bounds__( 128, ( flux_min_ctas< R, MODE >(  ) ) ) k_flux( const args_t< R > a, int axis, int step, int lines, udiv_t dv )
 {
+    if( MODE == FLUX_APPLY && step == 0 && sel_eval_step( a.s, a.sel_period ) )
+        return;                       // the network's sweep (k_flux_eval) solves this one
     flux_faces< MHD, R, MODE >( a, axis, step, lines, dv, blockIdx.x, blockIdx.y );
 }
 
 // Learned mode, the network's sweep: a fixed grid strides over the 128-face
 // chunks (cpp per z plane, nz planes), so on the stages where the network does
-// not run (k_flux_list solves them) only this small grid launches and exits.
-// The chunk loop is uniform over a CTA, as learned_solve's barriers need.
+// not run (k_flux<FLUX_APPLY> solves them) only this small grid launches and
+// exits.
 template< bool MHD, class R >
 __global__ void __launch_bounds__( 128, ( flux_min_ctas< R, KR_RIEMANN_LEARNED >(  ) ) )
 k_flux_eval( const args_t< R > a, int axis, int step, udiv_t dv, unsigned cpp, unsigned nz )
@@ -1110,50 +1089,6 @@ k_flux_eval( const args_t< R > a, int axis, int step, udiv_t dv, unsigned cpp, u
         return;
     for( unsigned ch = blockIdx.x; ch < cpp * nz; ch += gridDim.x )
         flux_faces< MHD, R, KR_RIEMANN_LEARNED >( a, axis, step, 0, dv, ch % cpp, ch / cpp );
-}
-
-// Learned mode, sweeps without the network: one thread per entry of the
-// (axis, block) HLLD and HLLE lists built by the last evaluation.  Warps run
-// one solver; entries of a warp come from one or two producer warps, so loads
-// and stores stay nearly coalesced.
-// (both solvers in one kernel: 72 registers, 7 CTAs / SM, no spills; capped at
-// 64 for 8 CTAs it spilled and ran 1.5% slower)
-template< bool MHD, class R >
-__global__ void __launch_bounds__( 128, 7 )
-k_flux_list( const args_t< R > a, int axis, int step )
-{
-    constexpr int NW = MHD ? 11 : 5;
-    if( step == 0 && sel_eval_step( a.s, a.sel_period ) )
-        return;                       // the network's sweep (k_flux_eval) solves this one
-    const int b = blockIdx.z;
-    const size_t r = ( size_t ) axis * a.nblk + b;
-    const unsigned nh = a.sel_count[ r * 2 ], n = nh + a.sel_count[ r * 2 + 1 ];
-    const unsigned * list = a.sel_list + r * a.sel_cap;
-    // a fixed grid strides over both lists as one index space, the HLLD entries
-    // [0, nh) (front of the list) then the HLLE ones (back); only the warp that
-    // straddles nh mixes the two solvers.  The next entry is fetched before this
-    // face's work.
-    const unsigned stride = gridDim.x * blockDim.x;
-    unsigned j = blockIdx.x * blockDim.x + threadIdx.x;
-    auto entry = [ & ]( unsigned k ) { return k < nh ? list[ k ] : list[ a.sel_cap - 1 - ( k - nh ) ]; };
-    unsigned pk_next = j < n ? entry( j ) : 0u;
-    for( ; j < n; j += stride )
-    {
-    const unsigned pk = pk_next;
-    const bool cheap = j >= nh;
-    if( j + stride < n )
-        pk_next = entry( j + stride );
-    int ii[ 3 ] = { int( pk & 1023u ) - 2, int( ( pk >> 10 ) & 1023u ) - 2, int( pk >> 20 ) - 2 };
-    const int st = axis == 0 ? 1 : ( axis == 1 ? a.sw1 : a.sw2 );
-    R ql[ 8 ], qr[ 8 ];
-    const R * wb = a.w + ( size_t ) b * NW * a.ngw
-                 + ( ( ii[ 0 ] + 2 ) + a.sw1 * ( ii[ 1 ] + 2 ) + a.sw2 * ( ii[ 2 ] + 2 ) );
-    plm_stencil< MHD, R >( a, b, axis, step, ii, wb, st, ql, qr );
-    if( cheap )
-        solve_store< MHD, R, KR_RIEMANN_HLLE >( a, b, axis, ii, true, ql, qr, 0, 0ull );
-    else
-        solve_store< MHD, R, KR_RIEMANN_DEFAULT >( a, b, axis, ii, true, ql, qr, 0, 0ull );
-    }
 }
 
 // Shared-memory tiled sweep over the faces whose transverse position lies in
@@ -1958,9 +1893,8 @@ struct kr_ctx
     unsigned long long * sel_cnt = nullptr;
     float sel_thr = 0.f;
     bool sel_ready = false;
-    unsigned * sel_list = nullptr;     // learned mode: face lists of the last evaluation
-    unsigned * sel_count = nullptr;
-    long long sel_cap = 0;
+    unsigned char * sel_dec = nullptr; // learned mode: solver per warp of faces
+    long long sel_wcap = 0;
     // selector training samples (only during kr_selector_collect)
     float * smp = nullptr;
     unsigned long long * smp_n = nullptr;
@@ -2048,7 +1982,7 @@ static args_t< R > make_args( kr_ctx * c )
         if( c->cfg.bc[ 2 * d + 1 ] == KR_BC_OUT || c->cfg.bc[ 2 * d + 1 ] == KR_BC_FRE )
             a.emf_out |= 1 << d;
     a.sel_w = c->sel_w; a.sel_b = c->sel_b; a.sel_thr = c->sel_thr; a.sel_cnt = c->sel_cnt;
-    a.sel_list = c->sel_list; a.sel_count = c->sel_count; a.sel_cap = c->sel_cap;
+    a.sel_dec = c->sel_dec; a.sel_wcap = c->sel_wcap;
     a.sel_period = c->cfg.sel_period > 1 ? c->cfg.sel_period : 1;
     a.smp = c->smp; a.smp_n = c->smp_n; a.smp_max = c->smp_max;
     a.smp_stride = c->smp_stride; a.smp_seed = c->smp_seed;
@@ -2128,17 +2062,11 @@ static void launch_flux( kr_ctx * c, cudaStream_t st, const args_t< R > & a, int
             k_flux_eval< MHD, R ><<< dim3( ge, 1, c->nblk ), 128, 0, st >>>(
                 a, axis, stage, make_udiv( unsigned( ext[ 0 ] ) ), cpp, unsigned( ext[ 2 ] ) );
         }
-        else
-            k_flux< MHD, R, MODE ><<< dim3( blocks_for( ( long long ) ext[ 0 ] * ext[ 1 ], 128 ), ext[ 2 ], c->nblk ), 128, 0, st >>>(
-                a, axis, stage, 0, make_udiv( unsigned( ext[ 0 ] ) ) );
-        if constexpr( MODE == KR_RIEMANN_LEARNED && MHD )
-        {   // sweeps without the network: the face lists (exits at once on the
-            // network's sweep; CTAs past the lists' length exit); about two
-            // waves of CTAs over all blocks, striding over the lists
-            const unsigned gx = unsigned( std::max< long long >( 1, std::min< long long >(
-                blocks_for( ( long long ) ext[ 0 ] * ext[ 1 ] * ext[ 2 ], 128 ), ( 2LL * c->n_sm * 8 ) / c->nblk ) ) );
-            k_flux_list< MHD, R ><<< dim3( gx, 1, c->nblk ), 128, 0, st >>>( a, axis, stage );
-        }
+        // sweeps without the network: each warp of faces runs the solver
+        // chosen for it (exits at once on the network's sweep)
+        constexpr int M = ( MODE == KR_RIEMANN_LEARNED && MHD ) ? FLUX_APPLY : MODE;
+        k_flux< MHD, R, M ><<< dim3( blocks_for( ( long long ) ext[ 0 ] * ext[ 1 ], 128 ), ext[ 2 ], c->nblk ), 128, 0, st >>>(
+            a, axis, stage, 0, make_udiv( unsigned( ext[ 0 ] ) ) );
         return;
     }
     if( axis == 0 )      launch_tile< MHD, R, MODE, 0 >( c, st, a, stage, t );
@@ -2295,7 +2223,7 @@ template< bool MHD, class R, bool SAMPLE = false >
 static bool enqueue_step( kr_ctx * c, cudaStream_t st )
 {
     const args_t< R > a = make_args< R >( c );
-    k_step_begin<<< 1, 1, 0, st >>>( c->s, c->sel_count, 6 * c->nblk, c->cfg.sel_period > 1 ? c->cfg.sel_period : 1 );
+    k_step_begin<<< 1, 1, 0, st >>>( c->s );
     for( int stage = 0; stage < 2; ++ stage )
     {
         enqueue_front< MHD, R >( c, st, a, stage, untimed_t(  ) );
@@ -2328,7 +2256,7 @@ static bool profile_step( kr_ctx * c, double * ms )
         ms[ kind ] += t;
     };
     bool ok = true;
-    k_step_begin<<< 1, 1, 0, st >>>( c->s, c->sel_count, 6 * c->nblk, c->cfg.sel_period > 1 ? c->cfg.sel_period : 1 );
+    k_step_begin<<< 1, 1, 0, st >>>( c->s );
     for( int stage = 0; stage < 2 && ok; ++ stage )
     {
         enqueue_front< MHD, R >( c, st, a, stage, timed );
@@ -2713,18 +2641,18 @@ static kr_ctx * create_ctx( const kr_cfg * cfg, int n_regions, const kr_region *
                 && ck( c, cudaMalloc( & c->sel_cnt, 2 * sizeof( unsigned long long ) ), "malloc selector" )
                 && ck( c, cudaMemset( c->sel_cnt, 0, 2 * sizeof( unsigned long long ) ), "memset selector" );
     if( cfg->mhd && cfg->riemann == KR_RIEMANN_LEARNED && ok )
-    {   // per (axis, block): a list with room for every face of the sweep
+    {   // per (axis, block): one byte per warp of the per-face sweep's grid
+        // (128-face chunks per z plane x z planes x 4 warps)
         for( int ax = 0; ax < 3; ++ ax )
         {
-            long long f = 1;
+            long long ext[ 3 ];
             for( int d = 0; d < 3; ++ d )
-                f *= d == ax ? n[ d ] + 1 : n[ d ] + 2;
-            c->sel_cap = std::max( c->sel_cap, f );
+                ext[ d ] = d == ax ? n[ d ] + 1 : n[ d ] + 2;
+            c->sel_wcap = std::max( c->sel_wcap, blocks_for( ext[ 0 ] * ext[ 1 ], 128 ) * ext[ 2 ] * 4 );
         }
-        const size_t words = size_t( 3 ) * nb * c->sel_cap;
-        ok = ck( c, cudaMalloc( & c->sel_list, words * sizeof( unsigned ) ), "malloc selector lists" )
-          && ck( c, cudaMalloc( & c->sel_count, 6 * nb * sizeof( unsigned ) ), "malloc selector counts" )
-          && ck( c, cudaMemset( c->sel_count, 0, 6 * nb * sizeof( unsigned ) ), "memset selector counts" );
+        const size_t bytes = size_t( 3 ) * nb * c->sel_wcap;
+        ok = ck( c, cudaMalloc( & c->sel_dec, bytes ), "malloc selector choices" )
+          && ck( c, cudaMemset( c->sel_dec, 0, bytes ), "memset selector choices" );
     }
     c->stage_bytes = nb * ( size_t( c->nc ) * c->nw + ( cfg->mhd ? size_t( c->nbf ) * 3 : 0 ) ) * 8;
     ok = ok && ck( c, cudaMalloc( & c->stage, c->stage_bytes ), "malloc staging" );
@@ -2829,7 +2757,7 @@ void kr_ctx_destroy( kr_ctx * c )
     for( int d = 0; d < 3; ++ d ) cudaFree( c->f[ d ] );
     cudaFree( c->ee ); cudaFree( c->geo ); cudaFree( c->nbr ); cudaFree( c->s );
     cudaFree( c->stage ); cudaFree( c->diag );
-    cudaFree( c->sel_w ); cudaFree( c->sel_b ); cudaFree( c->sel_cnt ); cudaFree( c->sel_list ); cudaFree( c->sel_count );
+    cudaFree( c->sel_w ); cudaFree( c->sel_b ); cudaFree( c->sel_cnt ); cudaFree( c->sel_dec );
     if( c->own_stream && c->stream ) cudaStreamDestroy( c->stream );
     delete c;
 }
@@ -3310,7 +3238,7 @@ int kr_group_step( kr_ctx * const * ctxs, int n, int n_steps )
     const bool mhd = g0.mhd, fp32 = g0.precision == 1;
     for( int step = 0; step < n_steps; ++ step )
     {
-        for( kr_ctx * c : by ) k_step_begin<<< 1, 1, 0, st >>>( c->s, c->sel_count, 6 * c->nblk, c->cfg.sel_period > 1 ? c->cfg.sel_period : 1 );
+        for( kr_ctx * c : by ) k_step_begin<<< 1, 1, 0, st >>>( c->s );
         for( int stage = 0; stage < 2; ++ stage )
         {
             for( kr_ctx * c : by )

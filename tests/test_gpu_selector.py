@@ -8,8 +8,8 @@
   unsafe faces;
 * the learned mixed step stays within 1e-4 relative L1 density of the FP64
   oracle with div B at roundoff, and its gain over the method without it: it
-  sends a share of faces to HLLE while its error stays far below the all-HLLE
-  step's.
+  sends a share of faces to HLLE (whole warps of 32 faces, each passed by the
+  network) while its error stays far below the all-HLLE step's.
 """
 import numpy as np
 import pytest
@@ -93,19 +93,22 @@ def test_learned_step_error_and_gain():
 
     e_hlld, _, _ = run(0)
     e_hlle, _, _ = run(1)
-    e_learn, div, (faces, cheap) = run(2, thr=2.0)
+    # a warp of 32 faces goes to HLLE only when all of them pass the logit
+    # threshold, so the per-face threshold sits below the per-face default
+    thr = -3.0
+    e_learn, div, (faces, cheap) = run(2, thr=thr)
     frac = cheap / faces
     print("rel L1 density: hlld %.2e  hlle %.2e  learned %.2e (HLLE on %.1f%% of faces)"
           % (e_hlld, e_hlle, e_learn, 100 * frac))
     assert e_learn <= 1e-4
     assert div <= 1e-12
-    assert frac > 0.3                      # the network routes faces to HLLE ...
+    assert frac > 0.1                      # the network routes faces to HLLE ...
     assert e_learn < 0.5 * e_hlle          # ... at a fraction of the all-HLLE error
     # choices kept for 4 steps between evaluations of the network
-    e_p4, div4, (faces4, cheap4) = run(2, thr=2.0, sel_period=4)
+    e_p4, div4, (faces4, cheap4) = run(2, thr=thr, sel_period=4)
     print("sel_period 4: rel L1 density %.2e (HLLE on %.1f%% of faces)" % (e_p4, 100 * cheap4 / faces4))
     assert e_p4 <= 1e-4 and div4 <= 1e-12
-    assert cheap4 / faces4 > 0.3
+    assert cheap4 / faces4 > 0.1
 
 
 def test_gradient_and_training_are_reproducible():
