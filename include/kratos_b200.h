@@ -178,14 +178,17 @@ int kr_diagnostics( kr_ctx * ctx, double * max_div_b, double * totals5 );
  * reference always solves HLLD (mhd/riemann/hlld.h).  A 16 -> 32 -> 32 -> 1 MLP
  * (ReLU) predicts per face whether the cheap HLLE flux is within tolerance of
  * HLLD; with riemann = KR_RIEMANN_LEARNED the flux sweep evaluates it with BF16
- * tensor-core MMAs (FP32 accumulate) and uses HLLE where logit > threshold,
- * HLLD elsewhere.  Parameters: 1633 floats, W1[16][32], b1[32], W2[32][32],
+ * tensor-core MMAs (FP32 accumulate) at stage 0 of every sel_period-th step
+ * and uses HLLE for a warp of 32 consecutive faces of the sweep when every one
+ * of them has logit > threshold, HLLD elsewhere; the choice holds until the
+ * next evaluation.  Parameters: 1633 floats, W1[16][32], b1[32], W2[32][32],
  * b2[32], W3[32], b3, row-major [in][out]. */
 
 /* Upload selector parameters and the logit threshold to a context. */
 int kr_set_selector( kr_ctx * ctx, const float * params, float threshold );
 
-/* Faces evaluated and faces given HLLE since the last reset (learned mode). */
+/* Faces evaluated and faces given HLLE (whole warps) since the last reset
+ * (learned mode; counted when the network runs). */
 int kr_selector_stats( kr_ctx * ctx, long long * faces, long long * cheap, int reset );
 
 /* Run n_steps ordinary steps while logging about one face in `stride` (per
