@@ -140,7 +140,7 @@ int         kr_block_info        ( kr_ctx * ctx, int * level, int * reg );
 int kr_set_stream( kr_ctx * ctx, void * stream );
 
 /* Seeded workload initial state into the device state (host-built, uploaded):
- * "shock" (hydro) or "ot" (MHD). */
+ * "shock" (hydro), "ot" or "turb" (MHD; decaying supersonic turbulence). */
 int kr_init_problem( kr_ctx * ctx, const char * name, uint64_t seed );
 
 /* Host <-> device state transfers (layouts above).  bf is ignored for hydro.

@@ -2839,7 +2839,8 @@ int kr_get_state( kr_ctx * c, double * u, double * bf )
 int kr_init_problem( kr_ctx * c, const char * name, uint64_t seed )
 {
     if( ! c || ! name ) return -1;
-    const bool shock = ! std::strcmp( name, "shock" ), ot = ! std::strcmp( name, "ot" );
+    const bool shock = ! std::strcmp( name, "shock" ), turb = ! std::strcmp( name, "turb" );
+    const bool ot = ! std::strcmp( name, "ot" ) || turb;     // the MHD workloads
     if( ( ! shock && ! ot ) || ( ot != bool( c->cfg.mhd ) ) )
     {
         c->err = std::string( "kr_init_problem: unknown workload '" ) + name + "' for this mesh";
@@ -2855,6 +2856,9 @@ int kr_init_problem( kr_ctx * c, const char * name, uint64_t seed )
     const long long sb1 = n[ 0 ] + 5, sb2 = ( long long )( n[ 0 ] + 5 ) * ( n[ 1 ] + 5 );
     auto bidx = [ & ]( int b, int i0, int i1, int i2 )
     {   return ( ( size_t ) b * c->nbf + ( i0 + 2 ) + sb1 * ( i1 + 2 ) + sb2 * ( i2 + 2 ) ) * 3; };
+    kr_turb_t modes;
+    if( turb )
+        kr_turb_modes( & modes, seed );
     auto work = [ & ]( int b )
     {
         const int * reg = & c->reg_h[ 3 * b ];
@@ -2865,9 +2869,9 @@ int kr_init_problem( kr_ctx * c, const char * name, uint64_t seed )
             for( int i0 = 0; i0 <= n[ 0 ]; ++ i0 )
             {
                 double * p = hb.data(  ) + bidx( b, i0, i1, i2 );
-                p[ 0 ] = kr_ot_bx( x_cc( g, reg, lvl, 1, i1 ) );
-                p[ 1 ] = kr_ot_by( x_cc( g, reg, lvl, 0, i0 ) );
-                p[ 2 ] = kr_ot_bz(  );
+                p[ 0 ] = turb ? kr_turb_bx( g.gamma ) : kr_ot_bx( x_cc( g, reg, lvl, 1, i1 ) );
+                p[ 1 ] = turb ? 0.0 : kr_ot_by( x_cc( g, reg, lvl, 0, i0 ) );
+                p[ 2 ] = turb ? 0.0 : kr_ot_bz(  );
             }
         for( int i2 = 0; i2 < n[ 2 ]; ++ i2 )
         for( int i1 = 0; i1 < n[ 1 ]; ++ i1 )
@@ -2891,7 +2895,10 @@ int kr_init_problem( kr_ctx * c, const char * name, uint64_t seed )
                     ++ jj[ a ];
                     bc[ a ] = ( bl + hb[ bidx( b, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) + a ] ) / 2;
                 }
-                kr_ot_cell( u, x, bc, g.gamma, seed, key );
+                if( turb )
+                    kr_turb_cell( u, x, bc, g.gamma, & modes );
+                else
+                    kr_ot_cell( u, x, bc, g.gamma, seed, key );
             }
         }
     };

@@ -15,6 +15,12 @@
  *           B = (-sin 2 pi y, sin 4 pi x, 0) / sqrt(4 pi) sampled at face
  *           centres (exactly divergence free: B_x has no x dependence, B_y no
  *           y dependence)
+ *   turb  : decaying supersonic MHD turbulence (the initial field of a driven
+ *           run; no forcing): rho = 1, sound speed 1 (p = 1 / gamma), a
+ *           random-phase solenoidal velocity on the 128 integer wavevectors
+ *           with 1 <= |k| <= 4 (one of each +-k pair), mode amplitude |k|^-2
+ *           (shell spectrum E(k) ~ k^-2), scaled to rms Mach 5, and a uniform
+ *           B_x giving plasma beta 2 p / B^2 = 0.1
  */
 #ifndef KR_PROBLEMS_H
 #define KR_PROBLEMS_H
@@ -77,6 +83,97 @@ static inline void kr_ot_cell( double * u, const double x_cc[ 3 ], const double 
     v[ 0 ] = -sin( 2 * KR_PI * x_cc[ 1 ] ) + 1e-3 * kr_uniform_pm1( seed, 0, key );
     v[ 1 ] =  sin( 2 * KR_PI * x_cc[ 0 ] ) + 1e-3 * kr_uniform_pm1( seed, 1, key );
     v[ 2 ] =                                 1e-3 * kr_uniform_pm1( seed, 2, key );
+    for( int a = 0; a < 3; ++ a )
+    {
+        ek += v[ a ] * v[ a ];
+        em += b_cc[ a ] * b_cc[ a ];
+    }
+    u[ 0 ] = rho;
+    u[ 1 ] = pre / ( gamma - 1.0 ) + 0.5 * rho * ek + 0.5 * em;
+    for( int a = 0; a < 3; ++ a )
+    {
+        u[ 2 + a ] = rho * v[ a ];
+        u[ 5 + a ] = b_cc[ a ];
+    }
+}
+
+/* turb: the mode table (built once per seed) and the state of one cell. */
+#define KR_TURB_MODES 128
+
+typedef struct
+{
+    double k[ KR_TURB_MODES ][ 3 ];      /* integer wavevector */
+    double a[ KR_TURB_MODES ][ 3 ];      /* amplitude vector, perpendicular to k */
+    double phase[ KR_TURB_MODES ];
+} kr_turb_t;
+
+static inline void kr_turb_modes( kr_turb_t * t, uint64_t seed )
+{
+    int m = 0;
+    double sum_a2 = 0;
+    for( int kz = -4; kz <= 4; ++ kz )
+    for( int ky = -4; ky <= 4; ++ ky )
+    for( int kx = -4; kx <= 4; ++ kx )
+    {
+        const int k2 = kx * kx + ky * ky + kz * kz;
+        if( k2 < 1 || k2 > 16 || ! ( kx > 0 || ( kx == 0 && ( ky > 0 || ( ky == 0 && kz > 0 ) ) ) ) )
+            continue;
+        const double k[ 3 ] = { ( double ) kx, ( double ) ky, ( double ) kz };
+        double r[ 3 ], e[ 3 ], rk = 0, e2 = 0;
+        for( int d = 0; d < 3; ++ d )
+        {
+            r[ d ] = kr_uniform_pm1( seed, 16 + d, ( uint64_t ) m );
+            rk += r[ d ] * k[ d ];
+        }
+        for( int d = 0; d < 3; ++ d )    /* r minus its component along k */
+        {
+            e[ d ] = r[ d ] - rk / k2 * k[ d ];
+            e2 += e[ d ] * e[ d ];
+        }
+        if( e2 < 1e-6 )
+        {   /* r (nearly) parallel to k: use k x (0, 0, 1), or k x (1, 0, 0) */
+            const int z = kx == 0 && ky == 0;
+            e[ 0 ] = z ? 0.0 : k[ 1 ];
+            e[ 1 ] = z ? k[ 2 ] : -k[ 0 ];
+            e[ 2 ] = z ? -k[ 1 ] : 0.0;
+            e2 = e[ 0 ] * e[ 0 ] + e[ 1 ] * e[ 1 ] + e[ 2 ] * e[ 2 ];
+        }
+        const double amp = 1.0 / k2;     /* |k|^-2 */
+        const double s = amp / sqrt( e2 );
+        for( int d = 0; d < 3; ++ d )
+        {
+            t->k[ m ][ d ] = k[ d ];
+            t->a[ m ][ d ] = s * e[ d ];
+        }
+        t->phase[ m ] = KR_PI * ( kr_uniform_pm1( seed, 19, ( uint64_t ) m ) + 1.0 );
+        sum_a2 += amp * amp;
+        ++ m;
+    }
+    /* <|v|^2> over the periodic cell = sum a^2 / 2 (distinct modes are
+     * orthogonal, also on a uniform grid of more than 8 points per axis):
+     * scale to rms Mach 5 at sound speed 1 */
+    const double scale = 5.0 / sqrt( sum_a2 / 2 );
+    for( m = 0; m < KR_TURB_MODES; ++ m )
+        for( int d = 0; d < 3; ++ d )
+            t->a[ m ][ d ] *= scale;
+}
+
+static inline double kr_turb_bx( double gamma ) { return sqrt( 2.0 / gamma / 0.1 ); }
+
+/* u[0] rho, u[1] E (incl. magnetic energy of the face-averaged field),
+ * u[2..4] momentum, u[5..7] cell-centred B.  b_cc: face-averaged B of the cell. */
+static inline void kr_turb_cell( double * u, const double x_cc[ 3 ], const double b_cc[ 3 ],
+                                 double gamma, const kr_turb_t * t )
+{
+    const double rho = 1.0, pre = 1.0 / gamma;
+    double v[ 3 ] = { 0, 0, 0 }, ek = 0, em = 0;
+    for( int m = 0; m < KR_TURB_MODES; ++ m )
+    {
+        const double c = cos( 2 * KR_PI * ( t->k[ m ][ 0 ] * x_cc[ 0 ] + t->k[ m ][ 1 ] * x_cc[ 1 ]
+                                          + t->k[ m ][ 2 ] * x_cc[ 2 ] ) + t->phase[ m ] );
+        for( int d = 0; d < 3; ++ d )
+            v[ d ] += t->a[ m ][ d ] * c;
+    }
     for( int a = 0; a < 3; ++ a )
     {
         ek += v[ a ] * v[ a ];

@@ -97,6 +97,44 @@ struct ot_mhd_t : dynamics::mhd_t
     }
 };
 
+// Decaying supersonic turbulence: uniform B_x, random-phase solenoidal velocity.
+struct turb_mhd_t : dynamics::mhd_t
+{
+    void init_cond( mesh::block::dual_t & d ) override
+    {
+        auto & b_h = dynamic_cast< dynamics::mhd::block_data_t & >( d.h(  ) );
+        const auto & blk = d.b_w.get(  );
+        const auto & geo = blk.geo;
+        kr_turb_t modes;
+        kr_turb_modes( & modes, ( uint64_t ) g_seed );
+        auto n_face = geo.n_ceff;
+        for( auto & n_s : n_face.x )
+            n_s += ( n_s > 1 );
+        for( auto i : utils::loop( n_face ) )
+        {
+            auto * bf = b_h.fld.bf.at( i );
+            bf[ 0 ] = kr_turb_bx( p_eos->gamma );
+            bf[ 1 ] = bf[ 2 ] = 0;
+        }
+        for( auto i : utils::loop( geo.n_ceff ) )
+        {
+            double x[ 3 ], bc[ 3 ];
+            for( int a = 0; a < 3; ++ a )
+            {
+                x[ a ] = geo.x_cc( a, i[ a ] );
+                auto j = i;
+                ++ j[ a ];
+                bc[ a ] = ( b_h.fld.bf.at( i )[ a ] + b_h.fld.bf.at( j )[ a ] ) / 2;
+            }
+            double uu[ 8 ];
+            kr_turb_cell( uu, x, bc, p_eos->gamma, & modes );
+            auto * u = b_h.hyd.u.at( i );
+            for( int n = 0; n < 8; ++ n )
+                u[ n ] = uu[ n ];
+        }
+    }
+};
+
 namespace prob
 {
 void run( int argc, char * argv[  ] )
@@ -117,6 +155,8 @@ void run( int argc, char * argv[  ] )
         mesh.enroll_module< shock_hydro_t >(  );
     else if( name == "ot" )
         mesh.enroll_module< ot_mhd_t >(  );
+    else if( name == "turb" )
+        mesh.enroll_module< turb_mhd_t >(  );
     else
         throw std::runtime_error( "unknown [problem] name " + name );
     mesh.init( args );

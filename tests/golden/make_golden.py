@@ -66,6 +66,10 @@ CASES = [
     ("ot_bc_fix", "ot", (2, 1, 2), (8, 8, 8), 4, 9, 1.6666666666666667,
      {"kinds": "per per per per fixd fixd", "bnd_thread_limit": "4",
       "init": {"rho0": "0.2", "pre0": "0.15", "vel0": "0 0 0", "b0": "0.1 0.05 0.2"}}, "final"),
+    # decaying supersonic MHD turbulence (the initial field of the 512^3
+    # turbulence workload, at small size): rms Mach 5, beta 0.1
+    ("turb_16", "turb", (2, 2, 2), (8, 8, 8), 5, 4, 1.6666666666666667, {}, "final"),
+    ("turb_32", "turb", (2, 2, 2), (16, 16, 16), 6, 4, 1.6666666666666667, {}, "sums"),
     # static mesh refinement, hydro ([refine_region*] sections: level, x_min,
     # x_max); blocks are stored in tree order (level, then z, y, x) with their
     # levels and logical positions

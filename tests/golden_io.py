@@ -7,7 +7,9 @@ import numpy as np
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 CASES = ["shock_16", "ot_16", "ot_ragged", "shock_floor", "shock_c1", "ot_64",
          "shock_bc", "shock_fixd", "ot_bc_out", "ot_bc_ref", "ot_bc_fre",
-         "smr_shock", "smr_bc", "smr_3lvl"]
+         "smr_shock", "smr_bc", "smr_3lvl", "turb_16", "turb_32"]
+# MHD workloads
+MHD_WORKLOADS = ("ot", "turb")
 # statically refined fixtures (blocks in tree order, with level / reg arrays)
 SMR_CASES = ["smr_shock", "smr_bc", "smr_3lvl"]
 # fixtures compared within a tolerance, not bit for bit: name -> relative L1

@@ -25,7 +25,7 @@ def _dyn(meta, precision=2, riemann=0):
     from kratos_b200 import Dynamics
     extra = meta.get("dynamics", {})
     kinds, w_fix, b_fix = G.boundary(meta)
-    return Dynamics(meta["workload"] == "ot", meta["nb"], meta["n"], gamma=meta["gamma"],
+    return Dynamics(meta["workload"] in G.MHD_WORKLOADS, meta["nb"], meta["n"], gamma=meta["gamma"],
                     cfl=meta["cfl"], tmp_floor=float(extra.get("tmp_floor", 1e-9)),
                     precision=precision, riemann=riemann, kinds=kinds, w_fix=w_fix, b_fix=b_fix)
 
@@ -51,7 +51,7 @@ def test_initial_state_bit_exact(name):
 
 
 @pytest.mark.parametrize("name", ["shock_16", "ot_16", "ot_ragged", "shock_floor",
-                                  "shock_bc", "shock_fixd", "ot_bc_out", "ot_bc_fre"])
+                                  "shock_bc", "shock_fixd", "ot_bc_out", "ot_bc_fre", "turb_16"])
 def test_fp64_step_matches_reference(name):
     meta, g = G.load(name)
     d = _dyn(meta)
@@ -134,9 +134,10 @@ def test_mhd_fixed_sides_against_oracle_and_reference():
     assert err(own, g["bf1"] * mask, (0, 1, 2)) <= G.SPREAD_CASES["ot_bc_fix"]
 
 
-@pytest.mark.parametrize("name", ["shock_c1", "ot_64"])
+@pytest.mark.parametrize("name", ["shock_c1", "ot_64", "turb_32"])
 def test_fp64_full_size_checksums(name):
-    """Configs at full block size: checksum-of-fields against the reference."""
+    """Configs at full block size (turb_32: the turbulence workload on 16^3
+    blocks): checksum-of-fields against the reference."""
     meta, g = G.load(name)
     d = _dyn(meta)
     d.init_problem(meta["workload"], meta["seed"])

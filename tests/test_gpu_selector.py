@@ -125,3 +125,46 @@ def test_gradient_and_training_are_reproducible():
     wb, _ = S.train(X, y, w=w0, epochs=3, batch=4096)
     assert np.array_equal(wa, wb)
     assert not np.array_equal(wa, w0)
+
+
+def test_learned_step_on_turbulence():
+    """The learned step on the decaying-turbulence workload (rms Mach 5,
+    beta 0.1; 2^3 blocks of 16^3), with a network trained on the method's own
+    turbulence steps: within 1e-4 relative L1 density of the FP64 oracle, div B
+    at roundoff, and no less accurate than the all-HLLE step."""
+    from kratos_b200 import Dynamics
+    from kratos_b200 import selector as S
+    from oracle.kr_oracle import OracleMesh
+
+    def mk(**kw):
+        d = Dynamics(True, (2, 2, 2), (16, 16, 16), gamma=5 / 3, **kw)
+        d.init_problem("turb", 4)
+        return d
+
+    w, info = S.build_selector([lambda: mk(precision=1)], steps=4, stride=2, tol=3e-4, epochs=25)
+    assert info["samples"] > 10000
+    steps = 6
+    o = OracleMesh(True, (2, 2, 2), (16, 16, 16), 5 / 3)
+    o.init_problem("turb", 4)
+    o.step(steps)
+    ref, _ = o.get_state()
+
+    def run(riemann, thr=None):
+        d = mk(precision=1, riemann=riemann)
+        if thr is not None:
+            d.set_selector(w, thr)
+        d.step(steps)
+        u, _ = d.get_state()
+        div, _ = d.diagnostics()
+        assert d.status() == 0
+        stats = d.selector_stats() if thr is not None else None
+        return np.abs(u[..., 0] - ref[..., 0]).sum() / np.abs(ref[..., 0]).sum(), div, stats
+
+    e_hlld, _, _ = run(0)
+    e_hlle, _, _ = run(1)
+    e_learn, div, (faces, cheap) = run(2, thr=S.DEFAULT_THRESHOLD)
+    print("turbulence rel L1 density: hlld %.2e  hlle %.2e  learned %.2e (HLLE on %.1f%% of faces)"
+          % (e_hlld, e_hlle, e_learn, 100 * cheap / faces))
+    assert e_hlld <= 1e-4 and e_learn <= 1e-4
+    assert div <= 1e-12
+    assert e_learn <= e_hlle

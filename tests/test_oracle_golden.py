@@ -16,7 +16,7 @@ import golden_io as G
 def _mesh(meta):
     extra = meta.get("dynamics", {})
     kinds, w_fix, b_fix = G.boundary(meta)
-    return OracleMesh(meta["workload"] == "ot", meta["nb"], meta["n"], meta["gamma"],
+    return OracleMesh(meta["workload"] in G.MHD_WORKLOADS, meta["nb"], meta["n"], meta["gamma"],
                       cfl=meta["cfl"], t_floor=float(extra.get("tmp_floor", 1e-9)),
                       kinds=kinds, w_fix=w_fix, b_fix=b_fix, regions=G.regions(meta))
 
