@@ -100,6 +100,10 @@ typedef struct
 #define KR_FLAG_HALO_ALL 2     /* route every neighbour copy, same-rank ones     */
                                /* included, through the halo exchange            */
                                /* (verification of the pack / exchange / unpack) */
+#define KR_FLAG_BOXES    4     /* MHD, one rank, periodic: the nb[0] blocks are  */
+                               /* independent periodic boxes, each the unit cube */
+                               /* of n cells with its own CFL dt and time        */
+                               /* (kr_init_boxes, kr_box_times); nb[1] = nb[2] = 1 */
 
 typedef struct kr_ctx kr_ctx;
 
@@ -142,6 +146,18 @@ int kr_set_stream( kr_ctx * ctx, void * stream );
 /* Seeded workload initial state into the device state (host-built, uploaded):
  * "shock" (hydro), "ot" or "turb" (MHD; decaying supersonic turbulence). */
 int kr_init_problem( kr_ctx * ctx, const char * name, uint64_t seed );
+
+/* Batched independent boxes (no reference counterpart as one launch: the
+ * reference runs each box as its own mesh).  kr_box_params: the parameters
+ * of box `box` of a seeded batch (problems.h kr_box_params): out[0] edge
+ * length in cells, out[1..7] rho, p, velocity amplitude, beta, B_x, B_y, B_z.
+ * kr_init_boxes: block b of a KR_FLAG_BOXES context (or the one block of a
+ * periodic one-block MHD context) becomes box box_ids[b]; every box must have
+ * the context's edge length.  kr_box_times: each block's time, last dt and
+ * steps (arrays of kr_block_info's count; null entries skipped). */
+int kr_box_params( uint64_t seed, int box, double gamma, double * out8 );
+int kr_init_boxes( kr_ctx * ctx, uint64_t seed, const int * box_ids );
+int kr_box_times( kr_ctx * ctx, double * t, double * dt_last, long long * n_steps );
 
 /* Host <-> device state transfers (layouts above).  bf is ignored for hydro.
  * kr_get_state writes the cell-centred face-averaged B into u's slots 5..7. */

@@ -6,7 +6,7 @@ _PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_PKG, "libkrb200.so")
 
 KR_ABI_VERSION = 5
-KR_FLAG_TILED, KR_FLAG_HALO_ALL = 1, 2
+KR_FLAG_TILED, KR_FLAG_HALO_ALL, KR_FLAG_BOXES = 1, 2, 4
 BC_KINDS = {"per": 0, "out": 1, "ref": 2, "fre": 3, "fixd": 4}
 KR_RIEMANN_DEFAULT, KR_RIEMANN_HLLE, KR_RIEMANN_LEARNED = 0, 1, 2
 
@@ -59,6 +59,9 @@ SIGNATURES = {
     "kr_last_error": (ctypes.c_char_p, [_vp]),
     "kr_set_stream": (ctypes.c_int, [_vp, _vp]),
     "kr_init_problem": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_uint64]),
+    "kr_box_params": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_int, ctypes.c_double, _dp]),
+    "kr_init_boxes": (ctypes.c_int, [_vp, ctypes.c_uint64, _vp]),
+    "kr_box_times": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "kr_set_state": (ctypes.c_int, [_vp, _vp, _vp]),
     "kr_get_state": (ctypes.c_int, [_vp, _vp, _vp]),
     "kr_step": (ctypes.c_int, [_vp, ctypes.c_int]),

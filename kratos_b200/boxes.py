@@ -1,0 +1,98 @@
+"""Batched independent periodic MHD boxes: a seeded batch of boxes with edge
+lengths from {16, 24, 32, 48, 64} cells, random density, pressure, velocity
+amplitude, field orientation and plasma beta (kratos_b200/csrc/problems.h
+kr_box_params), each advancing on its own CFL dt.
+
+The original Kratos solver runs each box as its own one-block periodic mesh
+(one process per box).  Here the boxes of one edge length are the blocks of one
+context made with KR_FLAG_BOXES: every block is periodic onto itself and keeps
+its own dt and time, so one captured graph steps all boxes of that size, and
+the contexts of the five sizes run on their own streams.  A box advanced here
+matches the same box run alone (tests/test_gpu_boxes.py).
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib as L
+from .engine import Dynamics, KratosError
+
+
+def box_params(seed, box, gamma=5 / 3):
+    """Parameters of box `box` of the batch `seed`."""
+    out = (ctypes.c_double * 8)()
+    if L.lib().kr_box_params(int(seed), int(box), float(gamma), out) != 0:
+        raise KratosError("kr_box_params: bad box index %r" % (box,))
+    return {"n": int(out[0]), "rho": out[1], "pre": out[2], "amp": out[3], "beta": out[4],
+            "b": (out[5], out[6], out[7])}
+
+
+class BoxBatch:
+    """Boxes 0..n_boxes-1 of the batch `seed`, grouped by edge length.
+
+    Keyword arguments go to each group's Dynamics (precision, riemann, cfl,
+    device, ...).  `groups` maps an edge length to (Dynamics, box indices in
+    block order)."""
+
+    def __init__(self, seed, n_boxes, gamma=5 / 3, **kw):
+        if n_boxes < 1:
+            raise ValueError("need at least one box")
+        self.seed, self.n_boxes, self.gamma = int(seed), int(n_boxes), float(gamma)
+        sizes = np.array([box_params(seed, b, gamma)["n"] for b in range(n_boxes)])
+        self.sizes = sizes
+        self.groups = {}
+        self.where = {}
+        try:
+            for n in sorted(set(sizes.tolist())):
+                ids = np.flatnonzero(sizes == n).astype(np.int32)
+                d = Dynamics(True, (len(ids), 1, 1), (n, n, n), gamma=gamma,
+                             flags=kw.pop("flags", 0) | L.KR_FLAG_BOXES, **kw)
+                self.groups[n] = (d, ids)
+                for k, b in enumerate(ids):
+                    self.where[int(b)] = (n, k)
+                d.init_boxes(seed, ids)
+        except Exception:
+            self.close()
+            raise
+
+    @property
+    def n_cells(self):
+        return int(sum(int(n) ** 3 for n in self.sizes))
+
+    def step(self, n_steps=1):
+        """Advance every box n_steps of its own dt (enqueued on each group's
+        stream; get_state / times wait for them)."""
+        for d, _ in self.groups.values():
+            d.step(n_steps)
+
+    def status(self):
+        return max(d.status() for d, _ in self.groups.values())
+
+    def times(self):
+        """Per box (index order): time, last dt."""
+        t, dl = np.empty(self.n_boxes), np.empty(self.n_boxes)
+        for d, ids in self.groups.values():
+            tg, dg, _ = d.box_times()
+            t[ids], dl[ids] = tg, dg
+        return t, dl
+
+    def get_state(self, box):
+        """(u, bf) of one box, in the layout of a one-block mesh."""
+        n, k = self.where[int(box)]
+        d = self.groups[n][0]
+        u, bf = d.get_state()
+        return u[k:k + 1], bf[k:k + 1]
+
+    def states(self):
+        """{box: (u, bf)} of every box (one download per group)."""
+        out = {}
+        for d, ids in self.groups.values():
+            u, bf = d.get_state()
+            for k, b in enumerate(ids):
+                out[int(b)] = (u[k:k + 1], bf[k:k + 1])
+        return out
+
+    def close(self):
+        for d, _ in self.groups.values():
+            d.close()
+        self.groups = {}

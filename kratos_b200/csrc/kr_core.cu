@@ -86,6 +86,7 @@ struct args_t
     R * f[ 3 ];
     R * ee;
     const geo_t * geo;
+    int boxes;                        // 1: every block an independent box, scalars s[ block ]
     // learned face selector (riemann == KR_RIEMANN_LEARNED)
     const unsigned * sel_w;           // [32 lanes][MLP_BFRAG] bf16 pairs
     const float * sel_b;              // b1, b2, b3
@@ -158,21 +159,28 @@ __device__ __forceinline__ bool sel_eval_step( const scal_t * s, int period )
     return s->sel_force || s->n_steps % period == 0;
 }
 
-__global__ void k_step_begin( scal_t * s )
+// ns: 1, or one scalar set per block (independent boxes, KR_FLAG_BOXES); the
+// status word of set 0 collects every set's.
+__global__ void k_step_begin( scal_t * s, int ns )
 {
-    s->dt_bits = __double_as_longlong( s->dt_bound );
+    for( int k = 0; k < ns; ++ k )
+        s[ k ].dt_bits = __double_as_longlong( s[ k ].dt_bound );
 }
 
-__global__ void k_step_end( scal_t * s, double dt_expand )
+__global__ void k_step_end( scal_t * s, double dt_expand, int ns )
 {
-    const double dt = __longlong_as_double( s->dt_bits );
-    if( ! ( dt > 0 ) || ! isfinite( dt ) )
-        s->status |= 1;
-    s->dt_last  = dt;
-    s->t       += dt;
-    s->dt_bound = dt * dt_expand;
-    s->n_steps += 1;
-    s->sel_force = 0;
+    for( int k = 0; k < ns; ++ k )
+    {
+        scal_t & r = s[ k ];
+        const double dt = __longlong_as_double( r.dt_bits );
+        if( ! ( dt > 0 ) || ! isfinite( dt ) )
+            s[ 0 ].status |= 1;
+        r.dt_last  = dt;
+        r.t       += dt;
+        r.dt_bound = dt * dt_expand;
+        r.n_steps += 1;
+        r.sel_force = 0;
+    }
 }
 
 ////////////////////////////////////////////////////////////
@@ -311,7 +319,7 @@ __global__ void __launch_bounds__( 256, ( MHD && DT ) ? 3 : 4 ) k_c2p( const arg
             dt = threadIdx.x < ( blockDim.x >> 5 ) ? red[ threadIdx.x ] : FLT_MAX;
             dt = warp_min( dt );
             if( threadIdx.x == 0 )
-                atomicMin( & a.s->dt_bits, ( unsigned long long ) __double_as_longlong( dt ) );
+                atomicMin( & a.s[ a.boxes ? b : 0 ].dt_bits, ( unsigned long long ) __double_as_longlong( dt ) );
         }
     }
 }
@@ -1360,7 +1368,7 @@ __global__ void __launch_bounds__( 256, ( SMR && sizeof( R ) == 4 ) ? 3 : ( PART
     const unsigned q = udiv_q( t, dv );
     int i[ 3 ] = { int( t - q * unsigned( e0 ) ), int( q ), int( blockIdx.y ) };
     const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
-    const double dt = __longlong_as_double( a.s->dt_bits ) * ( step == 0 ? 1.0 : double( 0.5f ) );
+    const double dt = __longlong_as_double( a.s[ a.boxes ? b : 0 ].dt_bits ) * ( step == 0 ? 1.0 : double( 0.5f ) );
     const geo_t & g = a.geo[ b ];
     // The arrays never overlap: restrict lets the loads of later components
     // issue ahead of the stores of earlier ones.
@@ -1923,6 +1931,8 @@ struct kr_ctx
     // static refinement (hydro, one rank): blocks are the tree's leaves
     bool smr = false;
     int max_level = 0;
+    bool boxes = false;                // KR_FLAG_BOXES: independent periodic boxes
+    int nscal = 1;                     // scalar sets (one per box in that mode)
     std::vector< int > lvl_h, reg_h;   // per block: level, logical position (3)
     smr_item_t * smr_items = nullptr;  // [restriction / flux-average items | prolongation items by level]
     double * favg = nullptr;           // averaged fine fluxes of the flux-average items
@@ -1971,7 +1981,7 @@ static args_t< R > make_args( kr_ctx * c )
     a.w = ( R * ) c->w;
     for( int d = 0; d < 3; ++ d ) a.f[ d ] = ( R * ) c->f[ d ];
     a.ee = ( R * ) c->ee;
-    a.geo = c->geo; a.nbr = c->nbr; a.gid = c->gid; a.s = c->s;
+    a.geo = c->geo; a.nbr = c->nbr; a.gid = c->gid; a.s = c->s; a.boxes = c->boxes;
     a.favg = c->favg; a.favg_n = int( smr_half_sites( c ) );
     for( int d = 0; d < 3; ++ d ) a.nbk[ d ] = c->cfg.nb[ d ];
     for( int k = 0; k < 6; ++ k ) a.bc[ k ] = c->cfg.bc[ k ];
@@ -2223,7 +2233,7 @@ template< bool MHD, class R, bool SAMPLE = false >
 static bool enqueue_step( kr_ctx * c, cudaStream_t st )
 {
     const args_t< R > a = make_args< R >( c );
-    k_step_begin<<< 1, 1, 0, st >>>( c->s );
+    k_step_begin<<< 1, 1, 0, st >>>( c->s, c->nscal );
     for( int stage = 0; stage < 2; ++ stage )
     {
         enqueue_front< MHD, R >( c, st, a, stage, untimed_t(  ) );
@@ -2231,7 +2241,7 @@ static bool enqueue_step( kr_ctx * c, cudaStream_t st )
             return false;
         enqueue_back< MHD, R >( c, st, a, stage, SAMPLE ? FLUX_SAMPLE : c->cfg.riemann, untimed_t(  ) );
     }
-    k_step_end<<< 1, 1, 0, st >>>( c->s, c->cfg.dt_expand );
+    k_step_end<<< 1, 1, 0, st >>>( c->s, c->cfg.dt_expand, c->nscal );
     return true;
 }
 
@@ -2256,7 +2266,7 @@ static bool profile_step( kr_ctx * c, double * ms )
         ms[ kind ] += t;
     };
     bool ok = true;
-    k_step_begin<<< 1, 1, 0, st >>>( c->s );
+    k_step_begin<<< 1, 1, 0, st >>>( c->s, c->nscal );
     for( int stage = 0; stage < 2 && ok; ++ stage )
     {
         enqueue_front< MHD, R >( c, st, a, stage, timed );
@@ -2264,7 +2274,7 @@ static bool profile_step( kr_ctx * c, double * ms )
         if( ok )
             enqueue_back< MHD, R >( c, st, a, stage, c->cfg.riemann, timed );
     }
-    k_step_end<<< 1, 1, 0, st >>>( c->s, c->cfg.dt_expand );
+    k_step_end<<< 1, 1, 0, st >>>( c->s, c->cfg.dt_expand, c->nscal );
     cudaEventDestroy( ev[ 0 ] );
     cudaEventDestroy( ev[ 1 ] );
     return ck( c, cudaStreamSynchronize( st ), "profile" ) && ok;
@@ -2306,10 +2316,20 @@ static bool build_graph( kr_ctx * c )
     return true;
 }
 
+// The configuration the block geometry follows: independent boxes are each
+// the whole domain (one block per axis).
+static kr_cfg geo_cfg( const kr_ctx * c )
+{
+    kr_cfg g = c->cfg;
+    if( c->boxes )
+        g.nb[ 0 ] = g.nb[ 1 ] = g.nb[ 2 ] = 1;
+    return g;
+}
+
 // Geometry exactly as meshgen computes it (meshgen.cpp:252-363).
 static void set_geometry( kr_ctx * c )
 {
-    const kr_cfg & g = c->cfg;
+    const kr_cfg g = geo_cfg( c );
     c->geo_h.resize( c->nblk );
     for( int b = 0; b < c->nblk; ++ b )
     {
@@ -2500,6 +2520,19 @@ static kr_ctx * create_ctx( const kr_cfg * cfg, int n_regions, const kr_region *
         g_create_error = "kr_ctx_create_refined: bad region list";
         return nullptr;
     }
+    if( cfg->flags & KR_FLAG_BOXES )
+    {
+        bool ok = cfg->mhd && ranks_of( * cfg ) <= 1 && n_regions == 0 && ! ( cfg->flags & KR_FLAG_HALO_ALL )
+               && cfg->nb[ 1 ] == 1 && cfg->nb[ 2 ] == 1;
+        for( int k = 0; k < 6; ++ k )
+            ok = ok && cfg->bc[ k ] == KR_BC_PER;
+        if( ! ok )
+        {
+            g_create_error = "kr_ctx_create: KR_FLAG_BOXES needs MHD, one rank, periodic sides, "
+                             "no refinement and nb = (boxes, 1, 1)";
+            return nullptr;
+        }
+    }
     kr_tree tree;
     std::memset( & tree, 0, sizeof( tree ) );
     if( n_regions > 0 && ! build_tree( cfg, n_regions, regions, tree ) )
@@ -2525,6 +2558,7 @@ static kr_ctx * create_ctx( const kr_cfg * cfg, int n_regions, const kr_region *
     kr_ctx * c = new kr_ctx;
     c->cfg = * cfg;
     c->n_sm = n_sm;
+    c->boxes = ( cfg->flags & KR_FLAG_BOXES ) != 0;
     // The shared-memory tiled sweep is opt-in: on the 256^3 OT step it measured
     // slower than the per-face kernel (more registers per thread, long per-thread
     // face loops, a tail of partial CTAs), so the per-face kernel is the default.
@@ -2568,11 +2602,11 @@ static kr_ctx * create_ctx( const kr_cfg * cfg, int n_regions, const kr_region *
     else
     {
         for( int gb : c->gid_h )
-        {
+        {   // an independent box sits at the origin of its own domain
             c->lvl_h.push_back( 0 );
-            c->reg_h.push_back( gb % cfg->nb[ 0 ] );
-            c->reg_h.push_back( ( gb / cfg->nb[ 0 ] ) % cfg->nb[ 1 ] );
-            c->reg_h.push_back( gb / ( cfg->nb[ 0 ] * cfg->nb[ 1 ] ) );
+            c->reg_h.push_back( c->boxes ? 0 : gb % cfg->nb[ 0 ] );
+            c->reg_h.push_back( c->boxes ? 0 : ( gb / cfg->nb[ 0 ] ) % cfg->nb[ 1 ] );
+            c->reg_h.push_back( c->boxes ? 0 : gb / ( cfg->nb[ 0 ] * cfg->nb[ 1 ] ) );
         }
         halo_plan( * cfg, owner, local, halo_all, c->hsend, c->hrecv );
     }
@@ -2633,7 +2667,8 @@ static kr_ctx * create_ctx( const kr_cfg * cfg, int n_regions, const kr_region *
             mx = std::max( mx, 2LL * n[ ( a + 1 ) % 3 ] * n[ ( a + 2 ) % 3 ] );
         c->halo_grid = int( std::min< long long >( 64, blocks_for( mx, 256 ) ) );
     }
-    ok = ok && ck( c, cudaMalloc( & c->s, sizeof( scal_t ) ), "malloc scalars" );
+    c->nscal = c->boxes ? c->nblk : 1;
+    ok = ok && ck( c, cudaMalloc( & c->s, c->nscal * sizeof( scal_t ) ), "malloc scalars" );
     ok = ok && ck( c, cudaMalloc( & c->diag, 8 * sizeof( double ) ), "malloc diag" );
     if( cfg->mhd )
         ok = ok && ck( c, cudaMalloc( & c->sel_w, 32 * MLP_BFRAG * sizeof( unsigned ) ), "malloc selector" )
@@ -2703,15 +2738,21 @@ static kr_ctx * create_ctx( const kr_cfg * cfg, int n_regions, const kr_region *
                 nbr[ b * 27 + k ] = v;
                 continue;
             }
+            if( c->boxes )
+            {   // periodic onto itself in every direction
+                nbr[ b * 27 + k ] = b;
+                continue;
+            }
             const int src = nbr_global( * cfg, c->gid_h[ b ], k );
             nbr[ b * 27 + k ] = src < 0 ? -1 : ( owner[ src ] == c->rank && ! ( halo_all && k != 13 ) ? local[ src ] : -2 );
         }
-    scal_t s0{};
-    s0.dt_bound = cfg->dt_init >= FLT_MIN ? cfg->dt_init : FLT_MAX / 10;   // cycle.cpp:163-166
+    std::vector< scal_t > s0( c->nscal, scal_t{} );
+    for( scal_t & r : s0 )
+        r.dt_bound = cfg->dt_init >= FLT_MIN ? cfg->dt_init : FLT_MAX / 10;   // cycle.cpp:163-166
     ok = ck( c, cudaMemcpyAsync( c->geo, c->geo_h.data(  ), nb * sizeof( geo_t ), cudaMemcpyHostToDevice, c->stream ), "upload geo" )
       && ck( c, cudaMemcpyAsync( c->nbr, nbr.data(  ), nbr.size(  ) * sizeof( int ), cudaMemcpyHostToDevice, c->stream ), "upload nbr" )
       && ck( c, cudaMemcpyAsync( c->gid, c->gid_h.data(  ), nb * sizeof( int ), cudaMemcpyHostToDevice, c->stream ), "upload gid" )
-      && ck( c, cudaMemcpyAsync( c->s, & s0, sizeof( s0 ), cudaMemcpyHostToDevice, c->stream ), "upload scalars" )
+      && ck( c, cudaMemcpyAsync( c->s, s0.data(  ), s0.size(  ) * sizeof( scal_t ), cudaMemcpyHostToDevice, c->stream ), "upload scalars" )
       && ck( c, cudaStreamSynchronize( c->stream ), "sync" );
     if( ! ok )
     {
@@ -2841,7 +2882,7 @@ int kr_init_problem( kr_ctx * c, const char * name, uint64_t seed )
     if( ! c || ! name ) return -1;
     const bool shock = ! std::strcmp( name, "shock" ), turb = ! std::strcmp( name, "turb" );
     const bool ot = ! std::strcmp( name, "ot" ) || turb;     // the MHD workloads
-    if( ( ! shock && ! ot ) || ( ot != bool( c->cfg.mhd ) ) )
+    if( ( ! shock && ! ot ) || ( ot != bool( c->cfg.mhd ) ) || c->boxes )
     {
         c->err = std::string( "kr_init_problem: unknown workload '" ) + name + "' for this mesh";
         return -1;
@@ -2910,6 +2951,87 @@ int kr_init_problem( kr_ctx * c, const char * name, uint64_t seed )
     return kr_set_state( c, hu.data(  ), ot ? hb.data(  ) : nullptr );
 }
 
+int kr_box_params( uint64_t seed, int box, double gamma, double * out )
+{
+    if( ! out || box < 0 ) return -1;
+    kr_box_t p;
+    kr_box_params( & p, seed, box, gamma );
+    const double v[ 8 ] = { double( p.n ), p.rho, p.pre, p.amp, p.beta, p.b[ 0 ], p.b[ 1 ], p.b[ 2 ] };
+    std::copy( v, v + 8, out );
+    return 0;
+}
+
+int kr_init_boxes( kr_ctx * c, uint64_t seed, const int * ids )
+{
+    if( ! c || ! ids ) return -1;
+    bool periodic = true;
+    for( int k = 0; k < 6; ++ k )
+        periodic = periodic && c->cfg.bc[ k ] == KR_BC_PER;
+    if( ! c->cfg.mhd || c->smr || ( ! c->boxes && ! ( c->nblk == 1 && c->nranks == 1 && periodic ) ) )
+    {
+        c->err = "kr_init_boxes: needs a KR_FLAG_BOXES context or a periodic one-block MHD mesh";
+        return -1;
+    }
+    const kr_cfg g = geo_cfg( c );
+    const int * n = g.n;
+    std::vector< kr_box_t > box( c->nblk );
+    for( int b = 0; b < c->nblk; ++ b )
+    {
+        if( ids[ b ] < 0 )
+        {
+            c->err = "kr_init_boxes: negative box index";
+            return -1;
+        }
+        kr_box_params( & box[ b ], seed, ids[ b ], g.gamma );
+        if( box[ b ].n != n[ 0 ] || box[ b ].n != n[ 1 ] || box[ b ].n != n[ 2 ] )
+        {
+            c->err = "kr_init_boxes: box " + std::to_string( ids[ b ] ) + " has " + std::to_string( box[ b ].n )
+                   + " cells per axis, the context's blocks " + std::to_string( n[ 0 ] ) + "x"
+                   + std::to_string( n[ 1 ] ) + "x" + std::to_string( n[ 2 ] );
+            return -1;
+        }
+    }
+    const int nw = c->nw;
+    std::vector< double > hu( size_t( c->nblk ) * c->nc * nw, 0.0 );
+    std::vector< double > hb( size_t( c->nblk ) * c->nbf * 3, 0.0 );
+    const long long sb1 = n[ 0 ] + 5, sb2 = ( long long )( n[ 0 ] + 5 ) * ( n[ 1 ] + 5 );
+    auto bidx = [ & ]( int b, int i0, int i1, int i2 )
+    {   return ( ( size_t ) b * c->nbf + ( i0 + 2 ) + sb1 * ( i1 + 2 ) + sb2 * ( i2 + 2 ) ) * 3; };
+    const int reg0[ 3 ] = { 0, 0, 0 };
+    auto work = [ & ]( int b )
+    {   // the box is its own domain: cell keys and centres of a one-block mesh
+        const kr_box_t & p = box[ b ];
+        for( int i2 = 0; i2 <= n[ 2 ]; ++ i2 )
+        for( int i1 = 0; i1 <= n[ 1 ]; ++ i1 )
+        for( int i0 = 0; i0 <= n[ 0 ]; ++ i0 )
+            for( int a = 0; a < 3; ++ a )
+                hb[ bidx( b, i0, i1, i2 ) + a ] = p.b[ a ];
+        for( int i2 = 0; i2 < n[ 2 ]; ++ i2 )
+        for( int i1 = 0; i1 < n[ 1 ]; ++ i1 )
+        for( int i0 = 0; i0 < n[ 0 ]; ++ i0 )
+        {
+            const int ii[ 3 ] = { i0, i1, i2 };
+            double x[ 3 ], bc[ 3 ];
+            for( int a = 0; a < 3; ++ a )
+            {
+                int jj[ 3 ] = { i0, i1, i2 };
+                x[ a ] = x_cc( g, reg0, 0, a, ii[ a ] );
+                const double bl = hb[ bidx( b, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) + a ];
+                ++ jj[ a ];
+                bc[ a ] = ( bl + hb[ bidx( b, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) + a ] ) / 2;
+            }
+            double * u = hu.data(  ) + ( ( size_t ) b * c->nc + i0 + ( size_t ) n[ 0 ] * ( i1 + ( size_t ) n[ 1 ] * i2 ) ) * nw;
+            kr_box_cell( u, x, bc, g.gamma, & p, kr_cell_key( 0, ii, n ) );
+        }
+    };
+    const int nt = std::max( 1, std::min( c->nblk, int( std::thread::hardware_concurrency(  ) ) ) );
+    std::vector< std::thread > th;
+    for( int t = 0; t < nt; ++ t )
+        th.emplace_back( [ & , t ] (  ) { for( int b = t; b < c->nblk; b += nt ) work( b ); } );
+    for( auto & x : th ) x.join(  );
+    return kr_set_state( c, hu.data(  ), hb.data(  ) );
+}
+
 int kr_step( kr_ctx * c, int n_steps )
 {
     if( ! c || n_steps < 0 ) return -1;
@@ -2948,16 +3070,36 @@ int kr_get_time( kr_ctx * c, double * t, double * dt_last, double * dt_bound, lo
 }
 
 int kr_set_time( kr_ctx * c, double t, double dt_bound )
-{
+{   // independent boxes: every box
     if( ! c ) return -1;
-    scal_t s;
-    if( ! ck( c, cudaMemcpyAsync( & s, c->s, sizeof( s ), cudaMemcpyDeviceToHost, c->stream ), "read scalars" )
+    std::vector< scal_t > s( c->nscal );
+    if( ! ck( c, cudaMemcpyAsync( s.data(  ), c->s, s.size(  ) * sizeof( scal_t ), cudaMemcpyDeviceToHost, c->stream ), "read scalars" )
         || ! ck( c, cudaStreamSynchronize( c->stream ), "sync" ) )
         return -1;
-    s.t = t;
-    s.dt_bound = dt_bound;
-    return ck( c, cudaMemcpyAsync( c->s, & s, sizeof( s ), cudaMemcpyHostToDevice, c->stream ), "write scalars" )
+    for( scal_t & r : s )
+    {
+        r.t = t;
+        r.dt_bound = dt_bound;
+    }
+    return ck( c, cudaMemcpyAsync( c->s, s.data(  ), s.size(  ) * sizeof( scal_t ), cudaMemcpyHostToDevice, c->stream ), "write scalars" )
         && ck( c, cudaStreamSynchronize( c->stream ), "sync" ) ? 0 : -1;
+}
+
+int kr_box_times( kr_ctx * c, double * t, double * dt_last, long long * n_steps )
+{
+    if( ! c ) return -1;
+    std::vector< scal_t > s( c->nscal );
+    if( ! ck( c, cudaMemcpyAsync( s.data(  ), c->s, s.size(  ) * sizeof( scal_t ), cudaMemcpyDeviceToHost, c->stream ), "read scalars" )
+        || ! ck( c, cudaStreamSynchronize( c->stream ), "sync" ) )
+        return -1;
+    for( int b = 0; b < c->nblk; ++ b )
+    {   // one shared set unless the blocks are independent boxes
+        const scal_t & r = s[ c->boxes ? b : 0 ];
+        if( t ) t[ b ] = r.t;
+        if( dt_last ) dt_last[ b ] = r.dt_last;
+        if( n_steps ) n_steps[ b ] = r.n_steps;
+    }
+    return 0;
 }
 
 int kr_status( kr_ctx * c )
@@ -3218,7 +3360,7 @@ int kr_group_step( kr_ctx * const * ctxs, int n, int n_steps )
     for( int k = 0; k < n; ++ k )
     {
         kr_ctx * c = ctxs[ k ];
-        if( ! c || c->nranks != n || by[ c->rank ] || c->cfg.device != g0.device || c->cfg.mhd != g0.mhd
+        if( ! c || c->boxes || c->nranks != n || by[ c->rank ] || c->cfg.device != g0.device || c->cfg.mhd != g0.mhd
             || c->cfg.precision != g0.precision || ( c->cfg.riemann == KR_RIEMANN_LEARNED && ! c->sel_ready ) )
         {
             g_create_error = "kr_group_step: need the n_ranks contexts of one mesh, one per rank, on one device";
@@ -3245,7 +3387,7 @@ int kr_group_step( kr_ctx * const * ctxs, int n, int n_steps )
     const bool mhd = g0.mhd, fp32 = g0.precision == 1;
     for( int step = 0; step < n_steps; ++ step )
     {
-        for( kr_ctx * c : by ) k_step_begin<<< 1, 1, 0, st >>>( c->s );
+        for( kr_ctx * c : by ) k_step_begin<<< 1, 1, 0, st >>>( c->s, c->nscal );
         for( int stage = 0; stage < 2; ++ stage )
         {
             for( kr_ctx * c : by )
@@ -3272,7 +3414,7 @@ int kr_group_step( kr_ctx * const * ctxs, int n, int n_steps )
                 else      fp32 ? group_back< false, float >( c, st, stage ) : group_back< false, double >( c, st, stage );
             }
         }
-        for( kr_ctx * c : by ) k_step_end<<< 1, 1, 0, st >>>( c->s, c->cfg.dt_expand );
+        for( kr_ctx * c : by ) k_step_end<<< 1, 1, 0, st >>>( c->s, c->cfg.dt_expand, c->nscal );
     }
     const cudaError_t e = cudaStreamSynchronize( st );
     const cudaError_t l = cudaGetLastError(  );

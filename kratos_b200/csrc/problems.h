@@ -21,6 +21,12 @@
  *           with 1 <= |k| <= 4 (one of each +-k pair), mode amplitude |k|^-2
  *           (shell spectrum E(k) ~ k^-2), scaled to rms Mach 5, and a uniform
  *           B_x giving plasma beta 2 p / B^2 = 0.1
+ *   box   : one of a batch of independent periodic MHD boxes (box = 0, 1, ...):
+ *           edge length from {16, 24, 32, 48, 64} cells, rho in [0.5, 2),
+ *           p in [0.1, 10), v = A (sin 2 pi y, sin 2 pi z, sin 2 pi x) with
+ *           A / c_s in [0.1, 2) plus 1e-3 A U(-1,1) per component, uniform B of
+ *           random orientation with beta in [0.05, 10), all drawn uniformly
+ *           from (seed, box)
  */
 #ifndef KR_PROBLEMS_H
 #define KR_PROBLEMS_H
@@ -184,6 +190,59 @@ static inline void kr_turb_cell( double * u, const double x_cc[ 3 ], const doubl
     for( int a = 0; a < 3; ++ a )
     {
         u[ 2 + a ] = rho * v[ a ];
+        u[ 5 + a ] = b_cc[ a ];
+    }
+}
+
+/* box: the parameters of box `box` of a batch, and the state of one of its
+ * cells (cell key: the box's own lexicographic cell index at level 0). */
+typedef struct
+{
+    int    n;                            /* cells per axis */
+    double rho, pre, amp, beta, b[ 3 ];
+    uint64_t seed;                       /* the box's noise seed */
+} kr_box_t;
+
+static inline void kr_box_params( kr_box_t * p, uint64_t seed, int box, double gamma )
+{
+    const uint64_t k = ( uint64_t ) box;
+    int s = ( int )( ( kr_uniform_pm1( seed, 32, k ) + 1.0 ) * 2.5 );
+    if( s > 4 )
+        s = 4;
+    p->n    = s == 0 ? 16 : ( s == 1 ? 24 : ( s == 2 ? 32 : ( s == 3 ? 48 : 64 ) ) );
+    p->rho  = 0.5  + 0.75  * ( kr_uniform_pm1( seed, 33, k ) + 1.0 );
+    p->pre  = 0.1  + 4.95  * ( kr_uniform_pm1( seed, 34, k ) + 1.0 );
+    p->beta = 0.05 + 4.975 * ( kr_uniform_pm1( seed, 35, k ) + 1.0 );
+    p->amp  = sqrt( gamma * p->pre / p->rho ) * ( 0.1 + 0.95 * ( kr_uniform_pm1( seed, 36, k ) + 1.0 ) );
+    const double ct = kr_uniform_pm1( seed, 37, k );              /* cos theta */
+    const double st = sqrt( 1.0 - ct * ct );
+    const double ph = KR_PI * ( kr_uniform_pm1( seed, 38, k ) + 1.0 );
+    const double bm = sqrt( 2.0 * p->pre / p->beta );
+    p->b[ 0 ] = bm * st * cos( ph );
+    p->b[ 1 ] = bm * st * sin( ph );
+    p->b[ 2 ] = bm * ct;
+    p->seed = kr_splitmix64( seed ^ ( 0xD1B54A32D192ED03ull * ( k + 1 ) ) );
+}
+
+/* u[0] rho, u[1] E (incl. magnetic energy of the face-averaged field),
+ * u[2..4] momentum, u[5..7] cell-centred B.  b_cc: face-averaged B of the cell. */
+static inline void kr_box_cell( double * u, const double x_cc[ 3 ], const double b_cc[ 3 ],
+                                double gamma, const kr_box_t * p, uint64_t key )
+{
+    double v[ 3 ], ek = 0, em = 0;
+    v[ 0 ] = p->amp * ( sin( 2 * KR_PI * x_cc[ 1 ] ) + 1e-3 * kr_uniform_pm1( p->seed, 40, key ) );
+    v[ 1 ] = p->amp * ( sin( 2 * KR_PI * x_cc[ 2 ] ) + 1e-3 * kr_uniform_pm1( p->seed, 41, key ) );
+    v[ 2 ] = p->amp * ( sin( 2 * KR_PI * x_cc[ 0 ] ) + 1e-3 * kr_uniform_pm1( p->seed, 42, key ) );
+    for( int a = 0; a < 3; ++ a )
+    {
+        ek += v[ a ] * v[ a ];
+        em += b_cc[ a ] * b_cc[ a ];
+    }
+    u[ 0 ] = p->rho;
+    u[ 1 ] = p->pre / ( gamma - 1.0 ) + 0.5 * p->rho * ek + 0.5 * em;
+    for( int a = 0; a < 3; ++ a )
+    {
+        u[ 2 + a ] = p->rho * v[ a ];
         u[ 5 + a ] = b_cc[ a ];
     }
 }

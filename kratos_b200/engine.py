@@ -37,7 +37,7 @@ def make_cfg(mhd, nb, n, gamma=1.66667, cfl=0.3, precision=2, riemann=0,
     c.gamma, c.cfl = float(gamma), float(cfl)
     c.rho_floor, c.tmp_floor = float(rho_floor), float(tmp_floor)
     c.dt_init, c.dt_expand, c.device = float(dt_init), float(dt_expand), int(device)
-    c.flags = int(flags)              # KR_FLAG_TILED, KR_FLAG_HALO_ALL
+    c.flags = int(flags)              # KR_FLAG_TILED, KR_FLAG_HALO_ALL, KR_FLAG_BOXES
     c.n_ranks, c.rank = int(n_ranks), int(rank)
     c.sel_period = int(sel_period)
     for k in range(6):
@@ -177,6 +177,23 @@ class Dynamics:
 
     def init_problem(self, name, seed):
         self._check(L.lib().kr_init_problem(self._h, name.encode(), int(seed)), "kr_init_problem")
+
+    def init_boxes(self, seed, box_ids):
+        """Block b becomes box box_ids[b] of the seeded batch (a context made
+        with flags=KR_FLAG_BOXES, or a periodic one-block MHD mesh)."""
+        ids = np.ascontiguousarray(box_ids, dtype=np.int32).reshape(self.nblk)
+        self._check(L.lib().kr_init_boxes(self._h, int(seed), _ptr(ids)), "kr_init_boxes")
+
+    def init_box(self, seed, box):
+        """One box on a periodic one-block MHD mesh."""
+        self.init_boxes(seed, [box])
+
+    def box_times(self):
+        """Per block: time, last dt and steps (independent boxes: each its own)."""
+        t, dl = np.empty(self.nblk), np.empty(self.nblk)
+        ns = np.empty(self.nblk, np.int64)
+        self._check(L.lib().kr_box_times(self._h, _ptr(t), _ptr(dl), _ptr(ns)), "kr_box_times")
+        return t, dl, ns
 
     def set_state(self, u, bf=None):
         u = np.ascontiguousarray(u, dtype=np.float64).reshape(self.u_shape)

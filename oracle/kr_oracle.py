@@ -80,6 +80,10 @@ def lib():
         L.kro_plm.argtypes = [dp, dp, dp]
         L.kro_init_problem.restype = ctypes.c_int
         L.kro_init_problem.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_ulonglong]
+        L.kro_init_box.restype = ctypes.c_int
+        L.kro_init_box.argtypes = [ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_int]
+        L.kro_box_n.restype = ctypes.c_int
+        L.kro_box_n.argtypes = [ctypes.c_ulonglong, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -181,6 +185,11 @@ class OracleMesh:
         if lib().kro_init_problem(self._h, name.encode(), int(seed)) != 0:
             raise ValueError("unknown problem %r for this mesh" % name)
 
+    def init_box(self, seed, box):
+        """Box `box` of a batch of independent periodic MHD boxes."""
+        if lib().kro_init_box(self._h, int(seed), int(box)) != 0:
+            raise ValueError("box workloads need an MHD mesh")
+
     def x_cc(self, block, axis, i):
         return lib().kro_x_cc(self._h, block, axis, i)
 
@@ -202,3 +211,8 @@ def hlld(ql, qr, axis, gamma):
     f = np.empty(8)
     lib().kro_hlld(_p(ql), _p(qr), int(axis), float(gamma), _p(f))
     return f
+
+
+def box_n(seed, box):
+    """Edge length in cells of box `box` of a batch (problems.h kr_box_params)."""
+    return lib().kro_box_n(int(seed), int(box))

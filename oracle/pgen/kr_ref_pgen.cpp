@@ -135,6 +135,47 @@ struct turb_mhd_t : dynamics::mhd_t
     }
 };
 
+// One box of a batch of independent periodic boxes ([problem] box = index); the
+// mesh is the box: n_cell_global = n_cell_block = its edge length.
+static int g_box = 0;
+
+struct box_mhd_t : dynamics::mhd_t
+{
+    void init_cond( mesh::block::dual_t & d ) override
+    {
+        auto & b_h = dynamic_cast< dynamics::mhd::block_data_t & >( d.h(  ) );
+        const auto & blk = d.b_w.get(  );
+        const auto & geo = blk.geo;
+        kr_box_t p;
+        kr_box_params( & p, ( uint64_t ) g_seed, g_box, p_eos->gamma );
+        auto n_face = geo.n_ceff;
+        for( auto & n_s : n_face.x )
+            n_s += ( n_s > 1 );
+        for( auto i : utils::loop( n_face ) )
+        {
+            auto * bf = b_h.fld.bf.at( i );
+            for( int a = 0; a < 3; ++ a )
+                bf[ a ] = p.b[ a ];
+        }
+        for( auto i : utils::loop( geo.n_ceff ) )
+        {
+            double x[ 3 ], bc[ 3 ];
+            for( int a = 0; a < 3; ++ a )
+            {
+                x[ a ] = geo.x_cc( a, i[ a ] );
+                auto j = i;
+                ++ j[ a ];
+                bc[ a ] = ( b_h.fld.bf.at( i )[ a ] + b_h.fld.bf.at( j )[ a ] ) / 2;
+            }
+            double uu[ 8 ];
+            kr_box_cell( uu, x, bc, p_eos->gamma, & p, cell_key( blk, i ) );
+            auto * u = b_h.hyd.u.at( i );
+            for( int n = 0; n < 8; ++ n )
+                u[ n ] = uu[ n ];
+        }
+    }
+};
+
 namespace prob
 {
 void run( int argc, char * argv[  ] )
@@ -157,6 +198,11 @@ void run( int argc, char * argv[  ] )
         mesh.enroll_module< ot_mhd_t >(  );
     else if( name == "turb" )
         mesh.enroll_module< turb_mhd_t >(  );
+    else if( name == "box" )
+    {
+        g_box = args.get< int >( "problem", "box", 0 );
+        mesh.enroll_module< box_mhd_t >(  );
+    }
     else
         throw std::runtime_error( "unknown [problem] name " + name );
     mesh.init( args );

@@ -1696,3 +1696,57 @@ int kro_init_problem( kro_mesh * m, const char * name, unsigned long long seed )
     }
     return 0;
 }
+
+/* One box of a batch of independent periodic boxes (problems.h kr_box_*): the
+ * mesh is the box (the reference runs each box as its own single-block mesh;
+ * oracle/pgen/kr_ref_pgen.cpp box_mhd_t). */
+int kro_init_box( kro_mesh * m, unsigned long long seed, int box )
+{
+    const int * n = m->c.n;
+    if( ! m->c.mhd || box < 0 )
+        return -1;
+    int nglob[ 3 ];
+    for( int a = 0; a < 3; ++ a )
+        nglob[ a ] = n[ a ] * m->c.nb[ a ];
+    kr_box_t p;
+    kr_box_params( & p, seed, box, m->c.gamma );
+    for( int b = 0; b < m->nblk; ++ b )
+    {
+        const int * reg = blk_reg( m, b );
+        double * u  = m->u[ 0 ] + ( size_t ) b * m->ncell * m->nw;
+        double * bf = m->bf[ 0 ] + ( size_t ) b * m->nbf;
+        for( int i2 = 0; i2 <= n[ 2 ]; ++ i2 )
+        for( int i1 = 0; i1 <= n[ 1 ]; ++ i1 )
+        for( int i0 = 0; i0 <= n[ 0 ]; ++ i0 )
+            for( int a = 0; a < 3; ++ a )
+                bf[ ib( m, i0, i1, i2 ) + a ] = p.b[ a ];
+        for( int i2 = 0; i2 < n[ 2 ]; ++ i2 )
+        for( int i1 = 0; i1 < n[ 1 ]; ++ i1 )
+        for( int i0 = 0; i0 < n[ 0 ]; ++ i0 )
+        {
+            const int ii[ 3 ] = { i0, i1, i2 };
+            int ig[ 3 ];
+            double x[ 3 ], bc[ 3 ];
+            for( int a = 0; a < 3; ++ a )
+            {
+                int jj[ 3 ] = { i0, i1, i2 };
+                ig[ a ] = reg[ a ] * n[ a ] + ii[ a ];
+                x[ a ] = kro_x_cc( m, b, a, ii[ a ] );
+                const double bl = bf[ ib( m, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) + a ];
+                ++ jj[ a ];
+                bc[ a ] = ( bl + bf[ ib( m, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) + a ] ) / 2;
+            }
+            kr_box_cell( u + iu( m, i0, i1, i2 ), x, bc, m->c.gamma, & p,
+                         kr_cell_key( m->tree.level[ b ], ig, nglob ) );
+        }
+    }
+    return 0;
+}
+
+/* edge length (cells) of box `box` of a batch */
+int kro_box_n( unsigned long long seed, int box )
+{
+    kr_box_t p;
+    kr_box_params( & p, seed, box, 5.0 / 3.0 );
+    return p.n;
+}

@@ -95,6 +95,9 @@ double kro_dx  ( const kro_mesh * m, int block, int axis );
  * shared initial-condition header (kratos_b200/csrc/problems.h) with this
  * mesh's geometry, into slot 0.  Returns 0, or -1 for an unknown name. */
 int kro_init_problem( kro_mesh * m, const char * name, unsigned long long seed );
+/* box `box` of a batch of independent periodic MHD boxes (problems.h kr_box_*) */
+int kro_init_box( kro_mesh * m, unsigned long long seed, int box );
+int kro_box_n( unsigned long long seed, int box );
 
 /* Single-face kernels, for unit tests of the restatement.  Inputs are primitive
  * left / right states (rho, p, v0, v1, v2 [, b0, b1, b2]) in the unrotated

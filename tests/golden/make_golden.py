@@ -70,6 +70,11 @@ CASES = [
     # turbulence workload, at small size): rms Mach 5, beta 0.1
     ("turb_16", "turb", (2, 2, 2), (8, 8, 8), 5, 4, 1.6666666666666667, {}, "final"),
     ("turb_32", "turb", (2, 2, 2), (16, 16, 16), 6, 4, 1.6666666666666667, {}, "sums"),
+    # single boxes of the batched independent-box workload (seed 5; box 5 is
+    # 16^3, box 1 24^3, box 3 32^3): each box is its own periodic one-block mesh
+    ("box_5", "box", (1, 1, 1), (16, 16, 16), 5, 5, 1.6666666666666667, {"box": 5}, "final"),
+    ("box_1", "box", (1, 1, 1), (24, 24, 24), 5, 5, 1.6666666666666667, {"box": 1}, "sums"),
+    ("box_3", "box", (1, 1, 1), (32, 32, 32), 5, 5, 1.6666666666666667, {"box": 3}, "sums"),
     # static mesh refinement, hydro ([refine_region*] sections: level, x_min,
     # x_max); blocks are stored in tree order (level, then z, y, x) with their
     # levels and logical positions
@@ -93,9 +98,12 @@ def par_text(problem, nb, n, steps, seed, gamma, extra, prefix):
     kinds = extra.pop("kinds", "per per per per per per")
     init = extra.pop("init", {})
     regions = extra.pop("regions", [])
+    box = extra.pop("box", None)
     dyn.update(extra)
     lines = [
-        "[problem]", "name = %s" % problem, "seed = %d" % seed, "",
+        "[problem]", "name = %s" % problem, "seed = %d" % seed] + \
+        (["box = %d" % box] if box is not None else []) + [
+        "",
         "[mesh]", "x_min = 0 0 0", "x_max = 1 1 1",
         "n_cell_global = %d %d %d" % tuple(ng), "n_cell_block = %d %d %d" % tuple(n), "",
         "[cycle]", "prefix_output = %s" % prefix, "n_cycle_lim = %d" % (steps - 1),

@@ -7,9 +7,11 @@ import numpy as np
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 CASES = ["shock_16", "ot_16", "ot_ragged", "shock_floor", "shock_c1", "ot_64",
          "shock_bc", "shock_fixd", "ot_bc_out", "ot_bc_ref", "ot_bc_fre",
-         "smr_shock", "smr_bc", "smr_3lvl", "turb_16", "turb_32"]
+         "smr_shock", "smr_bc", "smr_3lvl", "turb_16", "turb_32", "box_5", "box_1", "box_3"]
 # MHD workloads
-MHD_WORKLOADS = ("ot", "turb")
+MHD_WORKLOADS = ("ot", "turb", "box")
+# single boxes of the batched-box workload (seed 5): the box index of each
+BOX_CASES = {"box_5": 5, "box_1": 1, "box_3": 3}
 # statically refined fixtures (blocks in tree order, with level / reg arrays)
 SMR_CASES = ["smr_shock", "smr_bc", "smr_3lvl"]
 # fixtures compared within a tolerance, not bit for bit: name -> relative L1
@@ -46,6 +48,14 @@ def field_errors(u, ref):
         den = mom if k >= 2 else np.abs(ref[..., k]).sum()
         out.append(np.abs(u[..., k] - ref[..., k]).sum() / den)
     return out
+
+
+def init(mesh, meta):
+    """Initial state of a fixture's workload on a mesh (oracle or device)."""
+    if meta["workload"] == "box":
+        mesh.init_box(meta["seed"], meta["dynamics"]["box"])
+    else:
+        mesh.init_problem(meta["workload"], meta["seed"])
 
 
 def load(name):

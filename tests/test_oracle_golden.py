@@ -38,7 +38,7 @@ def test_initial_state_bit_exact(name):
 def test_step_bit_exact(name):
     meta, g = G.load(name)
     m = _mesh(meta)
-    m.init_problem(meta["workload"], meta["seed"])
+    G.init(m, meta)
     u_init, bf_init = m.get_state()
     assert np.array_equal(G.checksums(u_init), g["u0_sum"])
     m.step(meta["steps"])
