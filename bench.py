@@ -56,6 +56,8 @@ def parse():
     p.add_argument("--mesh", type=int, default=256, choices=[128, 256],
                    help="global cells per axis (128: profiling-sized sample, 8 blocks of 64^3)")
     p.add_argument("--cpu-baseline", type=int, default=1, help="0: skip the CPU baseline leg")
+    p.add_argument("--boxes", type=int, default=1024,
+                   help="batched-box leg: boxes of the seeded batch (0: skip)")
     p.add_argument("--smr", type=int, default=1,
                    help="1: also time the statically refined hydro mesh (1 GPU only)")
     args = p.parse_args()
@@ -369,6 +371,50 @@ def time_smr(args, local_rank):
     return out
 
 
+def time_boxes(args, local_rank):
+    """Zone-cycles/s of a batch of independent periodic MHD boxes (seed 5,
+    edge lengths 16..64), each on its own CFL dt: one KR_FLAG_BOXES context per
+    edge length, each on its own stream; CUDA events from a start event that
+    every stream waits on to an end event after all of them."""
+    import torch
+    from kratos_b200.boxes import BoxBatch
+    out = {"workload": "%d independent periodic MHD boxes (seed 5), edge lengths from {16, 24, 32, 48, 64}, "
+                       "random rho, p, velocity amplitude, B orientation and beta, PLM + HLLD + CT, "
+                       "Heun RK2, per-box dt" % args.boxes}
+    for mode, prec in (("fp64", 2), ("mixed", 1)):
+        bb = BoxBatch(5, args.boxes, precision=prec, device=local_rank)
+        streams = {}
+        for n, (d, _) in bb.groups.items():
+            streams[n] = torch.cuda.Stream(device=local_rank)
+            d.set_stream(streams[n].cuda_stream)
+        bb.step(args.warmup)
+        torch.cuda.synchronize()
+        main_s = torch.cuda.Stream(device=local_rank)
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(main_s)
+        for st in streams.values():
+            st.wait_event(t0)
+        bb.step(args.steps)
+        for st in streams.values():
+            e = torch.cuda.Event()
+            e.record(st)
+            main_s.wait_event(e)
+        t1.record(main_s)
+        torch.cuda.synchronize()
+        ms = t0.elapsed_time(t1)
+        if bb.status() != 0:
+            raise RuntimeError("device status %d in the %s box batch" % (bb.status(), mode))
+        t, _ = bb.times()
+        out[mode] = {"value": bb.n_cells * args.steps / (ms * 1e-3), "unit": UNIT,
+                     "ms_per_step": ms / args.steps,
+                     "box_time_range": [float(t.min()), float(t.max())]}
+        out["cells"] = bb.n_cells
+        out["boxes_per_size"] = {str(n): int(len(ids)) for n, (_, ids) in bb.groups.items()}
+        bb.close()
+    return out
+
+
 def flux_roofline(h, head, world, peak, peak_kind):
     """Roofline line of the flux sweep: algorithmic bytes per launch over the
     mean launch duration (CUDA events around each launch, kr_profile_step)."""
@@ -455,6 +501,8 @@ def main():
             "64 blocks", "%d blocks" % (NB[0] * NB[1] * NB[2]))
     if rank == 0 and world == 1 and args.smr:
         line["smr"] = time_smr(args, local_rank)
+    if rank == 0 and world == 1 and args.boxes:
+        line["boxes"] = time_boxes(args, local_rank)
     if rank == 0:
         if args.cpu_baseline:
             try:
