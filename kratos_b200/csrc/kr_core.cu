@@ -816,7 +816,7 @@ constexpr int FLUX_APPLY = 4;
 // learned_solve below.)
 template< bool MHD, class R, int MODE > __device__ __forceinline__
 void solve_store( const args_t< R > & a, int b, int axis, const int * ii, bool valid,
-                  R * ql, R * qr, int warp, unsigned long long key )
+                  R * ql, R * qr, int warp, unsigned long long key, bool cheap = false )
 {
     constexpr bool SAMPLE = MODE == FLUX_SAMPLE;
     constexpr int rsel = MODE == FLUX_SAMPLE ? KR_RIEMANN_DEFAULT : MODE;
@@ -840,6 +840,8 @@ void solve_store( const args_t< R > & a, int b, int axis, const int * ii, bool v
         if( ! valid ) return;
         if( rsel == KR_RIEMANN_HLLE )
             hlle_fast< R >( flx, ql, qr, e );
+        else if( MODE == FLUX_APPLY )      // learned mode: this warp's choice
+            hll_pick_fast< R >( flx, ql, qr, e, cheap );
         else
             hlld_fast< R >( flx, ql, qr, e );
         if constexpr( SAMPLE )
@@ -919,8 +921,7 @@ void learned_solve( const args_t< R > & a, int b, int axis, const int * ii, bool
     if( ! valid )
         return;
     R flx[ 8 ];
-    if( cheap ) hlle_fast< R >( flx, ql, qr, e );
-    else        hlld_fast< R >( flx, ql, qr, e );
+    hll_pick_fast< R >( flx, ql, qr, e, cheap );
     idx_swap( flx + MOM, 3 - axis );
     R * F = a.f[ axis ] + ( size_t ) b * NF * a.nfb;
     const int off = ( ii[ 0 ] + 1 ) + a.sf1 * ( ii[ 1 ] + 1 ) + a.sf2 * ( ii[ 2 ] + 1 );
@@ -990,7 +991,8 @@ void plm_stencil( const args_t< R > & a, int b, int axis, int step, const int * 
 // plane (lines: along all line faces), by = z plane, blockIdx.z = block; dv
 // divides by the row length.
 template< bool MHD, class R, int MODE > __device__ __forceinline__
-void flux_faces( const args_t< R > & a, int axis, int step, int lines, udiv_t dv, unsigned bx, unsigned by )
+void flux_faces( const args_t< R > & a, int axis, int step, int lines, udiv_t dv, unsigned bx, unsigned by,
+                 bool hlle_warp = false )
 {
     constexpr int NW = MHD ? 11 : 5;   // stored W words: prim (8) + cell E (3)
     constexpr bool learned = MHD && MODE == KR_RIEMANN_LEARNED;
@@ -1048,12 +1050,8 @@ void flux_faces( const args_t< R > & a, int axis, int step, int lines, udiv_t dv
     if( ! valid && ! learned )
         return;
     // learned mode: the warp's place in the sweep's chunk order (chunks of 128
-    // faces, z plane outer, 4 warps each); without the network its solver
-    // choice is loaded here, in flight with the stencil loads
+    // faces, z plane outer, 4 warps each)
     const unsigned wid = ( by * ( ( total + 127u ) >> 7 ) + bx ) * 4u + ( threadIdx.x >> 5 );
-    bool hlle_warp = false;
-    if constexpr( MODE == FLUX_APPLY )
-        hlle_warp = a.sel_dec[ ( ( size_t ) axis * a.nblk + b ) * a.sel_wcap + wid ] != 0;
     const int st = axis == 0 ? 1 : ( axis == 1 ? a.sw1 : a.sw2 );
     R ql[ 8 ], qr[ 8 ];
     if( valid )
@@ -1066,10 +1064,8 @@ void flux_faces( const args_t< R > & a, int axis, int step, int lines, udiv_t dv
     {   // every face of the sweep here (lines == 0)
         if constexpr( learned )
             learned_solve< MHD, R >( a, b, axis, ii, valid, ql, qr, wid );
-        else if( hlle_warp )
-            solve_store< MHD, R, KR_RIEMANN_HLLE >( a, b, axis, ii, true, ql, qr, 0, 0ull );
         else
-            solve_store< MHD, R, KR_RIEMANN_DEFAULT >( a, b, axis, ii, true, ql, qr, 0, 0ull );
+            solve_store< MHD, R, FLUX_APPLY >( a, b, axis, ii, true, ql, qr, 0, 0ull, hlle_warp );
         return;
     }
     const unsigned long long key = ( ( unsigned long long ) b * 3 + axis ) * 0x9E3779B97F4A7C15ull
@@ -1080,9 +1076,16 @@ void flux_faces( const args_t< R > & a, int axis, int step, int lines, udiv_t dv
 template< bool MHD, class R, int MODE >
 __global__ void __launch_bounds__( 128, ( flux_min_ctas< R, MODE >(  ) ) ) k_flux( const args_t< R > a, int axis, int step, int lines, udiv_t dv )
 {
-    if( MODE == FLUX_APPLY && step == 0 && sel_eval_step( a.s, a.sel_period ) )
-        return;                       // the network's sweep (k_flux_eval) solves this one
-    flux_faces< MHD, R, MODE >( a, axis, step, lines, dv, blockIdx.x, blockIdx.y );
+    bool hlle_warp = false;
+    if constexpr( MODE == FLUX_APPLY )
+    {   // learned mode, sweeps without the network: this warp's solver choice,
+        // loaded first (gridDim.x: 128-face chunks per z plane)
+        if( step == 0 && sel_eval_step( a.s, a.sel_period ) )
+            return;                   // the network's sweep (k_flux_eval) solves this one
+        hlle_warp = a.sel_dec[ ( ( size_t ) axis * a.nblk + blockIdx.z ) * a.sel_wcap
+                               + ( blockIdx.y * gridDim.x + blockIdx.x ) * 4u + ( threadIdx.x >> 5 ) ] != 0;
+    }
+    flux_faces< MHD, R, MODE >( a, axis, step, lines, dv, blockIdx.x, blockIdx.y, hlle_warp );
 }
 
 // Learned mode, the network's sweep: a fixed grid strides over the 128-face

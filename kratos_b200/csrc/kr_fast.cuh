@@ -224,21 +224,37 @@ R hlld_star_fast( R * us, const R * u, const R * w, R rhos, R inv_rhos, R sd, R 
     return u_dot_b;
 }
 
-template< class R > __device__ __forceinline__
-void hlld_fast( R * flx, const R * wl, const R * wr, const eos_c< R > & e )
+// What HLLD and HLLE (the learned mode's cheap flux) both start from: the
+// conserved states, total pressures and the outer wave speeds.
+template< class R > struct hll_prefix
 {
     R u_l[ 8 ], u_r[ 8 ];
-    const R b_x = wl[ BCC ], bx_2 = b_x * b_x;
-    const R pm_l = hlld_cons_fast( u_l, wl, bx_2, b_x, e );
-    const R pm_r = hlld_cons_fast( u_r, wr, bx_2, b_x, e );
-    const R ptot_l = wl[ ENE ] + pm_l, ptot_r = wr[ ENE ] + pm_r;
+    R b_x, bx_2, pm_l, pm_r, spd_m2, spd_p2;
+};
+
+template< class R > __device__ __forceinline__
+void hll_prefix_fast( hll_prefix< R > & h, const R * wl, const R * wr, const eos_c< R > & e )
+{
+    h.b_x = wl[ BCC ];
+    h.bx_2 = h.b_x * h.b_x;
+    h.pm_l = hlld_cons_fast( h.u_l, wl, h.bx_2, h.b_x, e );
+    h.pm_r = hlld_cons_fast( h.u_r, wr, h.bx_2, h.b_x, e );
     const R irl = rcp( wl[ RHO ] ), irr = rcp( wr[ RHO ] );
-    const R cfm_l = c_fms_fast( wl[ ENE ], irl, bx_2,
+    const R cfm_l = c_fms_fast( wl[ ENE ], irl, h.bx_2,
                                 wl[ BCC + 1 ] * wl[ BCC + 1 ] + wl[ BCC + 2 ] * wl[ BCC + 2 ], e.gamma );
-    const R cfm_r = c_fms_fast( wr[ ENE ], irr, bx_2,
+    const R cfm_r = c_fms_fast( wr[ ENE ], irr, h.bx_2,
                                 wr[ BCC + 1 ] * wr[ BCC + 1 ] + wr[ BCC + 2 ] * wr[ BCC + 2 ], e.gamma );
-    const R spd_m2 = rmin( wl[ MOM ] - cfm_l, wr[ MOM ] - cfm_r );
-    const R spd_p2 = rmax( wl[ MOM ] + cfm_l, wr[ MOM ] + cfm_r );
+    h.spd_m2 = rmin( wl[ MOM ] - cfm_l, wr[ MOM ] - cfm_r );
+    h.spd_p2 = rmax( wl[ MOM ] + cfm_l, wr[ MOM ] + cfm_r );
+}
+
+// HLLD from the prefix (mhd/riemann/hlld.h:31-298).
+template< class R > __device__ __forceinline__
+void hlld_tail( R * flx, const R * wl, const R * wr, const hll_prefix< R > & h )
+{
+    const R * u_l = h.u_l, * u_r = h.u_r;
+    const R b_x = h.b_x, bx_2 = h.bx_2, spd_m2 = h.spd_m2, spd_p2 = h.spd_p2;
+    const R ptot_l = wl[ ENE ] + h.pm_l, ptot_r = wr[ ENE ] + h.pm_r;
     flx[ BCC ] = 0;
     if( spd_m2 >= 0 || spd_p2 <= 0 )
     {
@@ -328,28 +344,48 @@ void hlld_fast( R * flx, const R * wl, const R * wr, const eos_c< R > & e )
     flx[ BCC ] = 0;
 }
 
+// HLLE with the HLLD outer speeds, from the prefix.
+template< class R > __device__ __forceinline__
+void hlle_tail( R * flx, const R * wl, const R * wr, const hll_prefix< R > & h )
+{
+    R f_l[ 8 ], f_r[ 8 ];
+    const R s_l = rmin( h.spd_m2, R( 0 ) );
+    const R s_r = rmax( h.spd_p2, R( 0 ) );
+    hlld_f_flux( f_l, h.u_l, wl, wl[ ENE ] + h.pm_l, h.b_x );
+    hlld_f_flux( f_r, h.u_r, wr, wr[ ENE ] + h.pm_r, h.b_x );
+    f_l[ BCC ] = f_r[ BCC ] = 0;
+    const R inv = rcp( s_r - s_l );
+    for( int n = 0; n < 8; ++ n )
+        flx[ n ] = ( s_r * f_l[ n ] - s_l * f_r[ n ] + s_r * s_l * ( h.u_r[ n ] - h.u_l[ n ] ) ) * inv;
+    flx[ BCC ] = 0;
+}
+
+template< class R > __device__ __forceinline__
+void hlld_fast( R * flx, const R * wl, const R * wr, const eos_c< R > & e )
+{
+    hll_prefix< R > h;
+    hll_prefix_fast( h, wl, wr, e );
+    hlld_tail( flx, wl, wr, h );
+}
+
 // HLLE with the HLLD outer speeds (cheap flux of the learned selector).
 template< class R > __device__ __forceinline__
 void hlle_fast( R * flx, const R * wl, const R * wr, const eos_c< R > & e )
 {
-    R u_l[ 8 ], u_r[ 8 ], f_l[ 8 ], f_r[ 8 ];
-    const R b_x = wl[ BCC ], bx_2 = b_x * b_x;
-    const R pm_l = hlld_cons_fast( u_l, wl, bx_2, b_x, e );
-    const R pm_r = hlld_cons_fast( u_r, wr, bx_2, b_x, e );
-    const R irl = rcp( wl[ RHO ] ), irr = rcp( wr[ RHO ] );
-    const R cfm_l = c_fms_fast( wl[ ENE ], irl, bx_2,
-                                wl[ BCC + 1 ] * wl[ BCC + 1 ] + wl[ BCC + 2 ] * wl[ BCC + 2 ], e.gamma );
-    const R cfm_r = c_fms_fast( wr[ ENE ], irr, bx_2,
-                                wr[ BCC + 1 ] * wr[ BCC + 1 ] + wr[ BCC + 2 ] * wr[ BCC + 2 ], e.gamma );
-    const R s_l = rmin( rmin( wl[ MOM ] - cfm_l, wr[ MOM ] - cfm_r ), R( 0 ) );
-    const R s_r = rmax( rmax( wl[ MOM ] + cfm_l, wr[ MOM ] + cfm_r ), R( 0 ) );
-    hlld_f_flux( f_l, u_l, wl, wl[ ENE ] + pm_l, b_x );
-    hlld_f_flux( f_r, u_r, wr, wr[ ENE ] + pm_r, b_x );
-    f_l[ BCC ] = f_r[ BCC ] = 0;
-    const R inv = rcp( s_r - s_l );
-    for( int n = 0; n < 8; ++ n )
-        flx[ n ] = ( s_r * f_l[ n ] - s_l * f_r[ n ] + s_r * s_l * ( u_r[ n ] - u_l[ n ] ) ) * inv;
-    flx[ BCC ] = 0;
+    hll_prefix< R > h;
+    hll_prefix_fast( h, wl, wr, e );
+    hlle_tail( flx, wl, wr, h );
+}
+
+// The learned mode's solver of one face, HLLE where `cheap`, else HLLD, from
+// one shared prefix (one copy of it in the kernel).
+template< class R > __device__ __forceinline__
+void hll_pick_fast( R * flx, const R * wl, const R * wr, const eos_c< R > & e, bool cheap )
+{
+    hll_prefix< R > h;
+    hll_prefix_fast( h, wl, wr, e );
+    if( cheap ) hlle_tail( flx, wl, wr, h );
+    else        hlld_tail( flx, wl, wr, h );
 }
 
 }   // namespace kr
