@@ -43,6 +43,9 @@ FLUX_BYTES_PER_FACE = {4: 8 * 4 + 8 + 7 * 4, 8: 8 * 8 + 8 + 7 * 8}
 # 2.26 M faces (two captured launches, 135.9 MB on average); traffic scales with
 # the faces (same block shape)
 FLUX_DRAM_BYTES_PER_FACE = 60.0
+# DRAM bytes per zone-cycle of one whole mixed step (all 16 launches), ncu on the
+# 128^3 sample (8 blocks of 64^3): 2354 MB over 2,097,152 cells
+STEP_DRAM_BYTES_PER_ZONE_CYCLE_MIXED = 1122.6
 WORKLOAD = "ot 256^3 periodic MHD, 64 blocks of 64^3, PLM+HLLD+CT, Heun RK2"
 
 
@@ -484,7 +487,10 @@ def main():
         "roofline": flux_roofline(h, head, world, peak, peak_kind),
         "step_roofline": {"bound": "hbm", "achieved": step_gbs, "peak": peak, "unit": "GB/s",
                           "frac": step_gbs / peak,
-                          "basis": "whole step: %d B/zone-cycle algorithmic (%s peak); longest kernel kind %s"
+                          "dram_bytes_per_zone_cycle": STEP_DRAM_BYTES_PER_ZONE_CYCLE_MIXED if head != "fp64" else None,
+                          "basis": "whole step: %d B/zone-cycle algorithmic (%s peak); longest kernel kind %s; "
+                                   "DRAM bytes per zone-cycle of the mixed step from one ncu capture "
+                                   "(128^3 sample, same block shape)"
                                    % (BYTES_PER_ZONE_CYCLE, peak_kind, top)},
         "clocks": h["clocks"],
         "e2e": h["e2e"],
