@@ -200,7 +200,7 @@ kro_mesh * kro_create_tree( const kro_cfg * cfg, int n_regions, const kro_region
         const int r = kr_tree_build( & m->tree, cfg->nb, per, cfg->x_min, cfg->x_max,
                                      n_regions, rg, NULL, 0 );
         free( rg );
-        if( r != 0 || ( m->tree.max_level > 0 && cfg->mhd ) )
+        if( r != 0 )
         {
             kr_tree_free( & m->tree );
             free( m );
@@ -1574,6 +1574,8 @@ static void ct_block( kro_mesh * m, int b, void * aux )
 
 int kro_step( kro_mesh * m, int n_steps, double * t, double * dt_bound, double * dt_last )
 {
+    if( m->c.mhd && m->smr )
+        return -2;        /* MHD level jumps (mhd/boundary/comm_functions.h) not restated */
     for( int s = 0; s < n_steps; ++ s )
     {
         double dt_use = 0;

@@ -85,6 +85,10 @@ CASES = [
      {"kinds": "ref out fre out per per",
       "regions": [(1, (0.05, 0.05, 0.2), (0.2, 0.3, 0.6)), (1, (0.7, 0.8, 0.1), (0.9, 0.95, 0.2))]},
      "final"),
+    # static refinement, MHD (Orszag-Tang): the reference's face-B restriction /
+    # Toth-Roe prolongation and EMF correction across the level jump
+    ("smr_ot", "ot", (2, 2, 2), (8, 8, 8), 4, 2, 1.6666666666666667,
+     {"regions": [(1, (0.3, 0.1, 0.1), (0.45, 0.4, 0.4))], "bnd_thread_limit": "4"}, "final"),
     # three levels (a level-2 region inside a level-1 one)
     ("smr_3lvl", "shock", (1, 1, 1), (8, 8, 8), 4, 12, 1.4,
      {"regions": [(2, (0.3, 0.3, 0.3), (0.3, 0.3, 0.3))]}, "final"),

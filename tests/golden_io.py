@@ -12,6 +12,9 @@ CASES = ["shock_16", "ot_16", "ot_ragged", "shock_floor", "shock_c1", "ot_64",
 MHD_WORKLOADS = ("ot", "turb", "box")
 # single boxes of the batched-box workload (seed 5): the box index of each
 BOX_CASES = {"box_5": 5, "box_1": 1, "box_3": 3}
+# statically refined MHD fixtures: tree and initial state pinned; the level-jump
+# step is not restated yet
+MHD_SMR_CASES = ["smr_ot"]
 # statically refined fixtures (blocks in tree order, with level / reg arrays)
 SMR_CASES = ["smr_shock", "smr_bc", "smr_3lvl"]
 # fixtures compared within a tolerance, not bit for bit: name -> relative L1

@@ -155,3 +155,20 @@ def test_refined_fixtures_exercise_every_level_jump():
                         if d[a] in (-1, 2) and all(0 <= d[x] <= 1 for x in range(3) if x != a):
                             seen.add(("fine", a))
     assert {("fine", 0), ("fine", 1), ("fine", 2), ("levels", 2)} <= seen
+
+
+@pytest.mark.parametrize("name", G.MHD_SMR_CASES)
+def test_refined_mhd_tree_and_initial_state(name):
+    """A statically refined MHD mesh: the shared tree gives the reference's
+    leaves (levels and positions, tree order) and the initial conserved state
+    and face field match its checksums bit for bit.  The step across the level
+    jump is not restated yet, and the oracle refuses it."""
+    meta, g = G.load(name)
+    m = _mesh(meta)
+    assert np.array_equal(m.level, g["level"]) and np.array_equal(m.reg, g["reg"])
+    G.init(m, meta)
+    u, bf = m.get_state()
+    assert np.array_equal(G.checksums(u), g["u0_sum"])
+    assert np.array_equal(G.checksums(G.owned_bf(bf, meta["n"])), g["bf0_sum"])
+    with pytest.raises(NotImplementedError):
+        m.step(1)
