@@ -905,8 +905,19 @@ void learned_solve( const args_t< R > & a, int b, int axis, const int * ii, bool
     float f[ MLP_IN ];
     face_features< R >( ql, qr, e.gamma, f );
     const float z = mlp_logit( f, a.sel_w, a.sel_b, xs[ warp ] );
+    // A face that more than one block computes -- on a block side along the
+    // sweep, or within one cell of a transverse side, where the neighbours'
+    // ghost lines (the edge EMFs' inputs) hold it too -- must get the same
+    // flux in every block, or the update stops telescoping: those faces stay
+    // on HLLD (and so does their warp), so the choice never depends on which
+    // block's warp holds them.
+    const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
+    const int a1 = mod3( axis + 1 ), a2 = mod3( axis + 2 );
+    const bool shared = ii[ axis ] == 0 || ii[ axis ] == nn[ axis ]
+                     || ii[ a1 ] <= 0 || ii[ a1 ] >= nn[ a1 ] - 1
+                     || ii[ a2 ] <= 0 || ii[ a2 ] >= nn[ a2 ] - 1;
     const unsigned mv = __ballot_sync( 0xffffffffu, valid );
-    const unsigned mc = __ballot_sync( 0xffffffffu, valid && z > a.sel_thr );
+    const unsigned mc = __ballot_sync( 0xffffffffu, valid && ! shared && z > a.sel_thr );
     const bool cheap = mv != 0u && mc == mv;
     if( lane == 0 )
     {
