@@ -196,8 +196,9 @@ int kr_diagnostics( kr_ctx * ctx, double * max_div_b, double * totals5 );
  * HLLD; with riemann = KR_RIEMANN_LEARNED the flux sweep evaluates it with BF16
  * tensor-core MMAs (FP32 accumulate) at stage 0 of every sel_period-th step
  * and uses HLLE for a warp of 32 consecutive faces of the sweep when every one
- * of them has logit > threshold, HLLD elsewhere; the choice holds until the
- * next evaluation.  Parameters: 1633 floats, W1[16][32], b1[32], W2[32][32],
+ * of them has logit > threshold and none is a face that a neighbouring block
+ * computes too (block sides, the edge EMFs' ghost lines), HLLD elsewhere, so
+ * every face gets one flux; the choice holds until the next evaluation.  Parameters: 1633 floats, W1[16][32], b1[32], W2[32][32],
  * b2[32], W3[32], b3, row-major [in][out]. */
 
 /* Upload selector parameters and the logit threshold to a context. */
