@@ -3144,7 +3144,7 @@ int kr_set_selector( kr_ctx * c, const float * w, float threshold )
         drop_graph( c );                 // the threshold is a kernel argument
     c->sel_thr = threshold;
     c->sel_ready = true;
-    const int one = 1;                   // face lists are rebuilt at the next step
+    const int one = 1;                   // the network runs at the next step
     if( ! ck( c, cudaMemcpyAsync( ( char * ) c->s + offsetof( scal_t, sel_force ), & one, sizeof( one ),
                                   cudaMemcpyHostToDevice, c->stream ), "selector force" )
         || ! ck( c, cudaStreamSynchronize( c->stream ), "sync" ) )
