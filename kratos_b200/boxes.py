@@ -42,11 +42,11 @@ class BoxBatch:
         self.sizes = sizes
         self.groups = {}
         self.where = {}
+        flags = kw.pop("flags", 0) | L.KR_FLAG_BOXES
         try:
             for n in sorted(set(sizes.tolist())):
                 ids = np.flatnonzero(sizes == n).astype(np.int32)
-                d = Dynamics(True, (len(ids), 1, 1), (n, n, n), gamma=gamma,
-                             flags=kw.pop("flags", 0) | L.KR_FLAG_BOXES, **kw)
+                d = Dynamics(True, (len(ids), 1, 1), (n, n, n), gamma=gamma, flags=flags, **kw)
                 self.groups[n] = (d, ids)
                 for k, b in enumerate(ids):
                     self.where[int(b)] = (n, k)
