@@ -444,6 +444,28 @@ static void c2p_block( kro_mesh * m, int b, void * aux )
     m->dtc[ b ] = dt_min;
 }
 
+/* cons -> prim (with floors) and the CFL dt of the state in slot 0, without
+ * stepping: w_out [nblk][n2][n1][n0][nw] interior primitives (MHD: rho, p,
+ * v0..2, B_cc0..2), dt_out [nblk] each block's cfl * min dx / signal speed.
+ * Floor corrections heal slot 0's conserved state as the step's c2p does. */
+void kro_c2p_dt( kro_mesh * m, double * w_out, double * dt_out )
+{
+    c2p_arg ca = { 0 };
+    for( int b = 0; b < m->nblk; ++ b )
+    {
+        c2p_block( m, b, & ca );
+        dt_out[ b ] = m->dtc[ b ];
+        const int * n = m->c.n;
+        const double * w = m->w + ( size_t ) b * m->nw_cells * m->nw;
+        double * o = w_out + ( size_t ) b * m->ncell * m->nw;
+        for( int i2 = 0; i2 < n[ 2 ]; ++ i2 )
+        for( int i1 = 0; i1 < n[ 1 ]; ++ i1 )
+        for( int i0 = 0; i0 < n[ 0 ]; ++ i0 )
+            for( int k = 0; k < m->nw; ++ k )
+                o[ iu( m, i0, i1, i2 ) + k ] = w[ iw( m, i0, i1, i2 ) + k ];
+    }
+}
+
 /* ------------------------------------------------------------------ */
 /* ghost fill (same level, periodic): every ghost cell of w and every  */
 /* non-owned face slot of bf takes the value of the block that owns it */

@@ -82,6 +82,8 @@ void kro_get_state( const kro_mesh * m, double * u, double * bf );
  * from (cycle.cpp:77-115: the CFL minimum is taken against it; afterwards it is
  * dt_use * dt_expand).  Returns the dt of the last step through *dt_last and
  * advances *t.  Returns 0, or -1 on a non-finite dt. */
+/* cons -> prim (floors heal slot 0) and each block's CFL dt of slot 0. */
+void kro_c2p_dt( kro_mesh * m, double * w_out, double * dt_out );
 int  kro_step( kro_mesh * m, int n_steps, double * t, double * dt_bound,
                double * dt_last );
 

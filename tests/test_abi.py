@@ -74,3 +74,21 @@ def test_create_rejects_bad_config_without_touching_a_gpu():
     c.abi_version = 99
     assert not lib.kr_ctx_create(ctypes.byref(c))
     assert b"ABI" in lib.kr_last_error(None)
+
+
+def test_noalloc_rejects_bad_config_without_touching_a_gpu():
+    """kr_c2p_dt_noalloc checks the ABI version and the block size (each axis
+    >= 4 cells, as kr_ctx_create) before any CUDA call."""
+    lib = L.lib()
+    c = L.kr_cfg()
+    lib.kr_cfg_default(ctypes.byref(c))
+    c.mhd = 1
+    c.n[0], c.n[1], c.n[2] = 8, 8, 1                  # a one-cell axis
+    dummy = ctypes.c_void_p(16)
+    rc = lib.kr_c2p_dt_noalloc(ctypes.byref(c), dummy, dummy, dummy, dummy, None)
+    assert rc == -1 and b"n >= 4" in lib.kr_last_error(None)
+    lib.kr_cfg_default(ctypes.byref(c))
+    c.n[0] = c.n[1] = c.n[2] = 8
+    c.abi_version = L.KR_ABI_VERSION - 1
+    rc = lib.kr_c2p_dt_noalloc(ctypes.byref(c), dummy, dummy, dummy, dummy, None)
+    assert rc == -1 and b"ABI" in lib.kr_last_error(None)

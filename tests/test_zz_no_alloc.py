@@ -3,12 +3,15 @@
 Some callers cannot allocate device memory (their host framework owns the memory
 pool, or allocation is not allowed where they run).  kr_c2p_dt_noalloc serves
 them: it converts one block's conserved state to primitives and reduces the CFL
-dt using only a fixed scratch array inside the library.  This test checks, on two
+dt using only a fixed scratch array inside the library.  The tests check, on two
 calls in a row, that its dt equals the dt the regular engine (kr_ctx_create +
-kr_step) computes for the same state, and that its primitives match the
-engine's own cons->prim of that state (read back through kr_get_state) to 1e-13.
-The test allocates its buffers with torch; the entry point allocates nothing.
-This file is collected last so a failure here cannot hide other tests.
+kr_step) computes for the same state and that its primitives match a plain
+formula of that state; that with the pressure floor active (a state that the
+floor heals in about half the cells) its primitives and dt match the oracle's
+cons->prim; and that a warmed-up call changes neither torch's allocated bytes
+nor the device's free memory.  The tests allocate their buffers with torch; the
+entry point allocates nothing.  This file is collected last so a failure here
+cannot hide other tests.
 """
 import ctypes
 
@@ -80,3 +83,78 @@ def test_noalloc_rejects_oversized_block():
                                ctypes.c_void_p(8), ctypes.c_void_p(8), None)
     assert rc == -2
     assert b"exceeds the scratch limit" in lib.kr_last_error(None)
+
+
+def _noalloc(lib, cfg, u_soa, bf_soa, w, dt, stream):
+    return lib.kr_c2p_dt_noalloc(ctypes.byref(cfg), ctypes.c_void_p(u_soa.data_ptr()),
+                                 ctypes.c_void_p(bf_soa.data_ptr() if bf_soa is not None else 0),
+                                 ctypes.c_void_p(w.data_ptr()), ctypes.c_void_p(dt.data_ptr()),
+                                 ctypes.c_void_p(stream.cuda_stream))
+
+
+@pytest.mark.parametrize("mhd", [True, False])
+def test_noalloc_floors_match_oracle(mhd):
+    """Density and pressure floors: the primitives and dt agree with the
+    oracle's cons->prim (floors applied to w) to rounding; u is left as given."""
+    import torch
+    from kratos_b200 import _lib as L
+    from kratos_b200.engine import make_cfg
+    from oracle.kr_oracle import OracleMesh
+    n = (16, 8, 8)
+    gamma = 5.0 / 3.0 if mhd else 1.4
+    name = "ot" if mhd else "shock"
+    # tmp_floor = 1 (as the shock_floor fixture): p < rho on part of the mesh
+    o = OracleMesh(mhd, (1, 1, 1), n, gamma, d_floor=1e-9, t_floor=1.0)
+    o.init_problem(name, 4)
+    u0, bf0 = o.get_state()
+    rng = np.random.default_rng(7)
+    u0[0, ..., 0][rng.random(u0.shape[1:4]) < 0.05] = 1e-12       # density below the floor too
+    o.set_state(u0, bf0)
+    w_ref, dt_ref = o.c2p_dt()
+    cfg = make_cfg(mhd, (1, 1, 1), n, gamma=gamma, rho_floor=1e-9, tmp_floor=1.0)
+    dev = torch.device("cuda:0")
+    u_soa = torch.from_numpy(np.ascontiguousarray(np.moveaxis(u0[0, ..., :5], -1, 0))).to(dev)
+    bf_soa = torch.from_numpy(np.ascontiguousarray(np.moveaxis(bf0[0], -1, 0))).to(dev) if mhd else None
+    u_before = u_soa.clone()
+    nw = 8 if mhd else 5
+    w = torch.zeros((nw, n[2] + 4, n[1] + 4, n[0] + 4), dtype=torch.float64, device=dev)
+    dt = torch.zeros(1, dtype=torch.float64, device=dev)
+    lib = L.lib()
+    stream = torch.cuda.current_stream(dev)
+    for call in range(2):
+        w.zero_()
+        assert _noalloc(lib, cfg, u_soa, bf_soa, w, dt, stream) == 0, lib.kr_last_error(None)
+        torch.cuda.synchronize()
+        wi = np.moveaxis(w[:, 2:-2, 2:-2, 2:-2].cpu().numpy(), 0, -1)
+        healed = w_ref[0, ..., 1] <= 1.0 * w_ref[0, ..., 0] * (1 + 1e-15)
+        assert healed.mean() > 0.2, "the floor must be active in this case"
+        np.testing.assert_allclose(wi, w_ref[0], rtol=1e-12, atol=1e-14)
+        assert float(dt.item()) == pytest.approx(float(dt_ref[0]), rel=1e-13, abs=0), call
+    assert torch.equal(u_soa, u_before), "u is read only"
+
+
+def test_noalloc_allocates_nothing():
+    """After a first (set-up) call, further calls leave torch's allocated bytes
+    and the device's free memory unchanged."""
+    import torch
+    from kratos_b200 import Dynamics
+    from kratos_b200 import _lib as L
+    n = (32, 32, 32)
+    d = Dynamics(True, (1, 1, 1), n, gamma=5.0 / 3.0)
+    d.init_problem("ot", 3)
+    u_aos, bf_aos = d.get_state()
+    dev = torch.device("cuda:0")
+    u_soa = torch.from_numpy(np.ascontiguousarray(np.moveaxis(u_aos[0, ..., :5], -1, 0))).to(dev)
+    bf_soa = torch.from_numpy(np.ascontiguousarray(np.moveaxis(bf_aos[0], -1, 0))).to(dev)
+    w = torch.zeros((8, n[2] + 4, n[1] + 4, n[0] + 4), dtype=torch.float64, device=dev)
+    dt = torch.zeros(1, dtype=torch.float64, device=dev)
+    lib = L.lib()
+    stream = torch.cuda.current_stream(dev)
+    assert _noalloc(lib, d.cfg, u_soa, bf_soa, w, dt, stream) == 0
+    torch.cuda.synchronize()
+    alloc0, free0 = torch.cuda.memory_allocated(dev), torch.cuda.mem_get_info(dev)[0]
+    for _ in range(5):
+        assert _noalloc(lib, d.cfg, u_soa, bf_soa, w, dt, stream) == 0
+    torch.cuda.synchronize()
+    assert torch.cuda.memory_allocated(dev) == alloc0
+    assert torch.cuda.mem_get_info(dev)[0] == free0
