@@ -63,6 +63,8 @@ def parse():
                    help="batched-box leg: boxes of the seeded batch (0: skip)")
     p.add_argument("--smr", type=int, default=1,
                    help="1: also time the statically refined hydro mesh (1 GPU only)")
+    p.add_argument("--turb", type=int, default=512, choices=[0, 128, 256, 512],
+                   help="turbulence leg: global cells per axis (64^3 blocks; 0: skip)")
     args = p.parse_args()
     global NB
     NB = (args.mesh // 64,) * 3
@@ -135,13 +137,14 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------------------- CPU
-def run_reference_cpu(steps, nb=(2, 2, 2), n=(64, 64, 64), threads=None):
+def run_reference_cpu(steps, nb=None, n=N, threads=None):
     """Time the original Kratos solver (its CPU path, built from source into
     oracle/_ref/kratos_ref) on an OT mesh; returns (zone-cycles/s, cores) from
     its own `Speed = ... cell/s` line (cycle.cpp:184-190)."""
     exe = os.path.join(ROOT, "oracle", "_ref", "kratos_ref")
     if not os.path.exists(exe):
         return None
+    nb = nb or NB
     threads = threads or os.cpu_count()
     with tempfile.TemporaryDirectory() as tmp:
         par = os.path.join(tmp, "b.par")
@@ -155,15 +158,47 @@ def run_reference_cpu(steps, nb=(2, 2, 2), n=(64, 64, 64), threads=None):
                 "[dynamics]", "gamma = %r" % GAMMA, "thread_limit = 1", "bnd_thread_limit = 1",
                 "[boundary]", "kinds = per per per per per per", ""]))
         env = dict(os.environ, KR_REF_THREADS=str(threads))
-        out = subprocess.run([exe, par], cwd=tmp, env=env, capture_output=True, text=True, timeout=1200)
+        out = subprocess.run([exe, par], cwd=tmp, env=env, capture_output=True, text=True, timeout=1800)
     m = re.search(r"Speed = ([0-9.eE+-]+) cell/s", out.stdout)
     if not m:
         return None
     return float(m.group(1)), threads
 
 
-def run_oracle_cpu(steps, nb=(2, 2, 2), n=(64, 64, 64)):
+def run_reference_cuda(steps, precision, nb=None, n=N, timeout=900):
+    """Time the original Kratos solver's own CUDA path (baseline/Makefile.cuda:
+    its sources built with nvcc for sm_100a) on the benchmark's OT mesh, on
+    the current GPU; returns its own `Speed = ... cell/s` (zone-cycles/s over
+    its n_cycle_lim + 1 steps, cycle.cpp:184-190), or None if not built."""
+    exe = os.path.join(ROOT, "baseline", "_ref", "kratos_cuda_p%d" % precision)
+    if not os.path.exists(exe):
+        return None
+    nb = nb or NB
+    with tempfile.TemporaryDirectory() as tmp:
+        par = os.path.join(tmp, "b.par")
+        ng = [nb[a] * n[a] for a in range(3)]
+        with open(par, "w") as f:
+            f.write("\n".join([
+                "[problem]", "name = ot", "seed = %d" % SEED, "[mesh]", "x_min = 0 0 0", "x_max = 1 1 1",
+                "n_cell_global = %d %d %d" % tuple(ng), "n_cell_block = %d %d %d" % tuple(n),
+                "[cycle]", "prefix_output = %s/s" % tmp, "n_cycle_lim = %d" % (steps - 1),
+                "final_output = 0", "t_output_next = 1e99", "n_display_freq = 1000000",
+                "[dynamics]", "gamma = %r" % GAMMA,
+                "[boundary]", "kinds = per per per per per per", ""]))
+        env = dict(os.environ, CUDA_VISIBLE_DEVICES=os.environ.get("CUDA_VISIBLE_DEVICES", "0"))
+        out = subprocess.run([exe, par], cwd=tmp, env=env, capture_output=True, text=True, timeout=timeout)
+    m = re.search(r"Speed = ([0-9.eE+-]+) cell/s", out.stdout)
+    if out.returncode != 0 or not m:
+        return {"value": None, "error": (out.stderr or out.stdout)[-400:]}
+    return {"value": float(m.group(1)), "unit": UNIT, "steps": steps,
+            "sample": "the benchmark's %d^3 OT mesh (%d blocks of 64^3), %d steps, the reference's "
+                      "default [dynamics] thread_limit / bnd_thread_limit (64), PRECISION=%d"
+                      % (ng[0], nb[0] * nb[1] * nb[2], steps, precision)}
+
+
+def run_oracle_cpu(steps, nb=None, n=N):
     from oracle.kr_oracle import OracleMesh
+    nb = nb or NB
     o = OracleMesh(True, nb, n, GAMMA)
     o.init_problem("ot", SEED)
     t0 = time.perf_counter()
@@ -172,34 +207,67 @@ def run_oracle_cpu(steps, nb=(2, 2, 2), n=(64, 64, 64)):
     return nb[0] * nb[1] * nb[2] * n[0] * n[1] * n[2] * steps / dt, os.cpu_count()
 
 
+REF_SAMPLE_NOTE = ("original Kratos CPU path (its ARCH=HIPCPU code, PRECISION=2) built from source "
+                   "with the project's HIP-CPU-compatible header, one thread per CTA "
+                   "(thread_limit = bnd_thread_limit = 1), CTAs on all host threads")
+
+
 def cpu_baseline(steps=2):
     r = run_reference_cpu(steps)
-    sample = "%d Heun steps of a 128^3 OT mesh (8 blocks of 64^3), PRECISION=2" % steps
+    sample = "%d Heun steps of the same %d^3 OT mesh (%d blocks of 64^3), PRECISION=2" % (
+        steps, NB[0] * N[0], NB[0] * NB[1] * NB[2])
     if r is not None:
         return {"value": r[0], "unit": UNIT, "cores": r[1], "kind": "reference",
-                "sample": sample + ", original Kratos CPU path (HIP-CPU mode) built from source"}
+                "sample": sample + ", " + REF_SAMPLE_NOTE}
     v, cores = run_oracle_cpu(steps)
     return {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": sample + ", CPU restatement (oracle/)"}
 
 
+# The reference arm runs the benchmark's own mesh (same workload, same
+# config) on the host cores; at ~1.4e6 zone-cycles/s on 16 cores one 256^3
+# step takes ~12 s, so it times at most this many steps (one run: the
+# reference's own `Speed` line over its steps).
+REF_ARM_MAX_STEPS = 8
+
+
+def bench_config(world, mode, n_cells):
+    """The `config` object both arms print (same workload, same keys)."""
+    workload = WORKLOAD
+    if world > 1:
+        nb_g, _ = weak_mesh(world)
+        workload = WORKLOAD.replace(
+            "256^3 periodic MHD, 64 blocks", "%dx%dx%d periodic MHD (256^3 per GPU), %d blocks"
+            % (nb_g[0] * N[0], nb_g[1] * N[1], nb_g[2] * N[2], nb_g[0] * nb_g[1] * nb_g[2]))
+    elif NB[0] * N[0] != 256:
+        workload = WORKLOAD.replace("256^3", "%d^3" % (NB[0] * N[0])).replace(
+            "64 blocks", "%d blocks" % (NB[0] * NB[1] * NB[2]))
+    return {"workload": workload, "mode": mode, "global_cells": n_cells,
+            "parallelism": ("%d GPUs: mesh sharded by blocks (%d blocks of 64^3 per GPU), "
+                            "NCCL halo exchange + dt all-reduce in the step graph" % (world, NB[0] * NB[1] * NB[2]))
+                           if world > 1 else "1 GPU",
+            "l2": "state 1.6 GB > 126 MB L2; no flush needed"}
+
+
 def reference_arm(args, rank, world):
     if rank != 0:
         return
-    steps = max(1, args.steps + args.warmup)
+    steps = max(2, min(args.steps + args.warmup, REF_ARM_MAX_STEPS))
     r = run_reference_cpu(steps)
     if r is not None:
-        kind, v, cores = "reference", r[0], r[1]
+        kind, v, cores, note = "reference", r[0], r[1], REF_SAMPLE_NOTE
     else:
         kind = "port"
         v, cores = run_oracle_cpu(steps)
+        note = "CPU restatement (oracle/)"
+    n_cells = NB[0] * NB[1] * NB[2] * N[0] * N[1] * N[2] * world
+    sample = "%d Heun steps of the benchmark's %d^3 OT mesh (%d blocks of 64^3), %s" % (
+        steps, NB[0] * N[0], NB[0] * NB[1] * NB[2], note)
     line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD,
-                       "mesh_sample": "128^3 = 8 blocks of 64^3 (same block shape)"},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
-                             "sample": "%d Heun steps of a 128^3 OT mesh (8 blocks of 64^3)" % steps},
+            "config": bench_config(world, "learned", n_cells),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -291,6 +359,11 @@ def time_mode(mode, args, local_rank, world, dist):
         ms = float(x.item())
     if d.status() != 0:
         raise RuntimeError("device status %d in mode %s" % (d.status(), mode))
+    div_b, _ = d.diagnostics()
+    if dist is not None:
+        x = torch.tensor([div_b], device="cuda:%d" % local_rank)
+        dist.all_reduce(x, op=dist.ReduceOp.MAX)
+        div_b = float(x.item())
     n_all = d.n_cells
     if dist is not None:
         x = torch.tensor([float(d.n_cells)], device="cuda:%d" % local_rank)
@@ -323,12 +396,18 @@ def time_mode(mode, args, local_rank, world, dist):
     out["rho"] = np.array(hu[..., 0])
     out["e2e"] = {"value": n_all * e2e_steps / wall, "unit": UNIT,
                   "h2d_bytes_per_step": d.state_bytes() // e2e_steps,
-                  "d2h_bytes_per_step": d.state_bytes() // e2e_steps}
+                  "d2h_bytes_per_step": d.state_bytes() // e2e_steps,
+                  "steps_per_transfer": e2e_steps,
+                  "basis": "kr_set_state from pinned host memory, kr_step(%d), kr_get_state to pinned host "
+                           "memory, all inside the wall-clock region; the state crosses PCIe once each way "
+                           "per %d steps" % (e2e_steps, e2e_steps)}
     out["n_cells"] = n_all
+    out["div_b_max"] = div_b
     if sel_info is not None:
         faces, cheap = d.selector_stats()
-        sel_info["hlle_fraction"] = cheap / max(faces, 1)
+        sel_info = dict(sel_info, hlle_fraction=cheap / max(faces, 1))
         out["selector"] = sel_info
+        out["selector_weights"] = w
     del np
     d.close()
     return out
@@ -374,7 +453,7 @@ def time_smr(args, local_rank):
     return out
 
 
-def time_boxes(args, local_rank):
+def time_boxes(args, local_rank, sel=None):
     """Zone-cycles/s of a batch of independent periodic MHD boxes (seed 5,
     edge lengths 16..64), each on its own CFL dt: one KR_FLAG_BOXES context per
     edge length, each on its own stream; CUDA events from a start event that
@@ -384,8 +463,13 @@ def time_boxes(args, local_rank):
     out = {"workload": "%d independent periodic MHD boxes (seed 5), edge lengths from {16, 24, 32, 48, 64}, "
                        "random rho, p, velocity amplitude, B orientation and beta, PLM + HLLD + CT, "
                        "Heun RK2, per-box dt" % args.boxes}
-    for mode, prec in (("fp64", 2), ("mixed", 1)):
-        bb = BoxBatch(5, args.boxes, precision=prec, device=local_rank)
+    box_modes = [("fp64", MODES["fp64"]), ("mixed", MODES["mixed"])]
+    if sel is not None:
+        box_modes.append(("learned", MODES["learned"]))
+    for mode, kw in box_modes:
+        bb = BoxBatch(5, args.boxes, device=local_rank, **kw)
+        if mode == "learned":
+            bb.set_selector(sel[0], sel[1]["threshold"])
         streams = {}
         for n, (d, _) in bb.groups.items():
             streams[n] = torch.cuda.Stream(device=local_rank)
@@ -412,9 +496,75 @@ def time_boxes(args, local_rank):
         out[mode] = {"value": bb.n_cells * args.steps / (ms * 1e-3), "unit": UNIT,
                      "ms_per_step": ms / args.steps,
                      "box_time_range": [float(t.min()), float(t.max())]}
+        if mode == "learned":
+            faces, cheap = bb.selector_stats()
+            out[mode]["hlle_fraction"] = cheap / max(faces, 1)
         out["cells"] = bb.n_cells
         out["boxes_per_size"] = {str(n): int(len(ids)) for n, (_, ids) in bb.groups.items()}
         bb.close()
+    return out
+
+
+TURB_SEED = 4
+
+
+def time_turb(args, local_rank, sel):
+    """The learned step on decaying supersonic MHD turbulence at the stated
+    size (512^3, 512 blocks of 64^3), next to the plain FP64 and the mixed
+    step from the same initial state: zone-cycles/s, HLLE share, relative L1
+    density error against the FP64 step after the same steps, |div B|."""
+    import numpy as np
+    import torch
+    from kratos_b200 import Dynamics
+    ng = args.turb
+    nb = (ng // N[0],) * 3
+    out = {"workload": "turb %d^3 periodic MHD (%d blocks of 64^3): rho 1, rms Mach 5 random-phase solenoidal "
+                       "velocity with a k^-2 spectrum at 1 <= |k| <= 4 (seed %d), uniform B_x at beta 0.1, "
+                       "decaying; PLM + HLLD + CT, Heun RK2; the learned mode's network is the one trained "
+                       "on the OT mesh's faces" % (ng, nb[0] * nb[1] * nb[2], TURB_SEED)}
+    d = Dynamics(True, nb, N, gamma=GAMMA, precision=1, device=local_rank)
+    t0 = time.perf_counter()
+    d.init_problem("turb", TURB_SEED)
+    u0, bf0 = d.get_state()
+    out["init_s"] = time.perf_counter() - t0
+    out["cells"] = d.n_cells
+    d.close()
+    rho = {}
+    for mode in ("fp64", "mixed", "learned"):
+        d = Dynamics(True, nb, N, gamma=GAMMA, device=local_rank, **MODES[mode])
+        if mode == "learned":
+            d.set_selector(sel[0], sel[1]["threshold"])
+        stream = torch.cuda.Stream(device=local_rank)
+        d.set_stream(stream.cuda_stream)
+        d.set_state(u0, bf0)
+        d.step(args.warmup)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        d.step(args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if d.status() != 0:
+            raise RuntimeError("device status %d in the turbulence %s step" % (d.status(), mode))
+        div_b, _ = d.diagnostics()
+        r = {"value": d.n_cells * args.steps / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / args.steps,
+             "div_b_max": div_b}
+        if mode == "learned":
+            faces, cheap = d.selector_stats()
+            r["hlle_fraction"] = cheap / max(faces, 1)
+        u, _ = d.get_state()
+        rho[mode] = np.array(u[..., 0])
+        del u
+        out[mode] = r
+        d.close()
+    den = np.abs(rho["fp64"]).sum()
+    for mode in ("mixed", "learned"):
+        out[mode]["l1_density_vs_fp64"] = float(np.abs(rho[mode] - rho["fp64"]).sum() / den)
+    out["learned_over_fp64"] = out["learned"]["value"] / out["fp64"]["value"]
+    out["learned_over_mixed"] = out["learned"]["value"] / out["mixed"]["value"]
+    out["steps_compared"] = args.warmup + args.steps
     return out
 
 
@@ -451,8 +601,11 @@ def main():
         dist = tdist
     torch.cuda.set_device(local_rank)
     results = {}
+    sel = None
     for mode in [m for m in args.modes.split(",") if m]:
         results[mode] = time_mode(mode, args, local_rank, world, dist)
+        if "selector_weights" in results[mode]:
+            sel = (results[mode].pop("selector_weights"), results[mode]["selector"])
     if "fp64" in results:
         import numpy as np
         ref = results["fp64"]["rho"]
@@ -467,19 +620,31 @@ def main():
     kernels = h["kernels_ms_per_step"]
     top = max(kernels, key=kernels.get)
     step_gbs = h["value"] / world * BYTES_PER_ZONE_CYCLE / 1e9
+    summary = {}
+    for m in ("fp64", "mixed", "learned", "hlle_mixed"):
+        if m in results:
+            summary[m + "_value"] = results[m]["value"]
+    if "fp64" in results:
+        for m in ("mixed", "learned", "hlle_mixed"):
+            if m in results:
+                summary[m + "_over_fp64"] = results[m]["value"] / results["fp64"]["value"]
+                summary[m + "_l1_density_vs_fp64"] = results[m]["l1_density_vs_fp64"]
+    if "learned" in results and "mixed" in results:
+        summary["learned_over_mixed"] = results["learned"]["value"] / results["mixed"]["value"]
+    if "learned" in results:
+        summary["learned_hlle_fraction"] = results["learned"]["selector"]["hlle_fraction"]
+    summary["div_b_max"] = max(r["div_b_max"] for r in results.values())
     line = {
         "metric": METRIC, "value": h["value"], "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": h["ms_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32/f64" if head != "fp64" else "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "mode": head, "global_cells": h["n_cells"],
-                   "parallelism": ("%d GPUs: mesh sharded by blocks (%d blocks of 64^3 per GPU), "
-                                   "NCCL halo exchange + dt all-reduce in the step graph" % (world, NB[0] * NB[1] * NB[2]))
-                                  if world > 1 else "1 GPU",
-                   "l2": "state 1.6 GB > 126 MB L2; no flush needed"},
+        **summary,
+        "config": bench_config(world, head, h["n_cells"]),
         "modes": {m: dict({"value": r["value"], "ms_per_step": r["ms_per_step"],
                            "kernels_ms_per_step": r["kernels_ms_per_step"]},
                           **({"selector": r["selector"]} if "selector" in r else {}),
+                  **{"div_b_max": r["div_b_max"]},
                           **({"l1_density_vs_fp64": r["l1_density_vs_fp64"],
                               "steps_compared": args.warmup + 2 * args.steps}
                              if "l1_density_vs_fp64" in r else {}))
@@ -497,18 +662,12 @@ def main():
         "gpu_launches": h["launches_per_step"] * args.steps,
     }
     line["flux_ms_per_step"] = flux_ms
-    if world > 1:
-        nb_g, _ = weak_mesh(world)
-        line["config"]["workload"] = WORKLOAD.replace(
-            "256^3 periodic MHD, 64 blocks", "%dx%dx%d periodic MHD (256^3 per GPU), %d blocks"
-            % (nb_g[0] * N[0], nb_g[1] * N[1], nb_g[2] * N[2], nb_g[0] * nb_g[1] * nb_g[2]))
-    if args.mesh != 256:
-        line["config"]["workload"] = WORKLOAD.replace("256^3", "%d^3" % args.mesh).replace(
-            "64 blocks", "%d blocks" % (NB[0] * NB[1] * NB[2]))
     if rank == 0 and world == 1 and args.smr:
         line["smr"] = time_smr(args, local_rank)
     if rank == 0 and world == 1 and args.boxes:
-        line["boxes"] = time_boxes(args, local_rank)
+        line["boxes"] = time_boxes(args, local_rank, sel)
+    if rank == 0 and world == 1 and args.turb and sel is not None:
+        line["turb"] = time_turb(args, local_rank, sel)
     if rank == 0:
         if args.cpu_baseline:
             try:

@@ -2,19 +2,20 @@
  *
  * The library replaces the device side of Kratos's dynamics module: the
  * per-stage `integrate` driver that dynamics::base_t::enroll builds
- * (src/modules/dynamics/dynamics.h:65-117), run once per RK stage by
- * dynamics::base_t::step (src/modules/dynamics/dynamics.cpp:156-161), together
+ * (src/modules/dynamics/dynamics.h:51-103), run once per RK stage by
+ * dynamics::base_t::step (src/modules/dynamics/dynamics.cpp:37-42), together
  * with the policy kernels it launches:
  *   cons2prim + CFL dt       hydro/eos/adiabatic.h:211-258, mhd/eos/adiabatic.h:127-234
  *   ghost fill (same level)  hydro/boundary/comm_functions.h:306-483,
  *                            mhd/boundary/comm_functions.h:433-815
  *   level jumps (hydro SMR)  hydro/boundary/comm_functions.h:329-505,
  *                            hydro/integrator/integrator.h:343-382
- *   PLM + HLLC / HLLD flux   prototypes/integrator.h:107-125 flux_kernel,
+ *   PLM + HLLC / HLLD flux   prototypes/integrator.h:14-32 flux_kernel,
  *                            hydro/reconstruct/plm.h, hydro/riemann/hllc.h,
  *                            mhd/riemann/hlld.h
- *   RK2 conserved update     hydro/integrator/integrator.h:241-265, rk2.h:404-425
- *   CT edge EMF + face B     mhd/integrator/integrator.h:189-462, mhd/integrator/rk2.h
+ *   RK2 conserved update     hydro/integrator/integrator.h:241-265,
+ *                            hydro/integrator/rk2.h:20-41
+ *   CT edge EMF + face B     mhd/integrator/integrator.h:191-462, mhd/integrator/rk2.h:20-63
  *   dt reduction             mesh/cycle/cycle.cpp:77-115
  * The host side (mesh, parameter files, snapshots, problem generators) calls
  * it with plain pointers; no torch or CUDA types cross this boundary.
@@ -94,9 +95,7 @@ typedef struct
     int    reserved[ 3 ];
 } kr_cfg;
 
-/* kr_cfg.flags */
-#define KR_FLAG_TILED    1     /* shared-memory tiled flux sweeps (opt-in; the   */
-                               /* per-face kernel is the default)                */
+/* kr_cfg.flags (bit 0, value 1, is reserved and ignored) */
 #define KR_FLAG_HALO_ALL 2     /* route every neighbour copy, same-rank ones     */
                                /* included, through the halo exchange            */
                                /* (verification of the pack / exchange / unpack) */
@@ -174,7 +173,9 @@ int kr_get_time( kr_ctx * ctx, double * t, double * dt_last, double * dt_bound,
 /* Set time and the dt bound the next step starts from (restart). */
 int kr_set_time( kr_ctx * ctx, double t, double dt_bound );
 
-/* Sticky device status word: 0 ok; bit 0 non-finite or non-positive dt. */
+/* Sticky device status word: 0 ok; bit 0 non-finite or non-positive dt; bit 1
+ * a NaN velocity in the state (stage 0's cons -> prim; the density and
+ * pressure floors heal NaN density and pressure, as the reference's do). */
 int kr_status( kr_ctx * ctx );
 
 /* Number of kernel launches kr_step enqueues per step (instrumentation). */
@@ -194,17 +195,19 @@ int kr_diagnostics( kr_ctx * ctx, double * max_div_b, double * totals5 );
  * reference always solves HLLD (mhd/riemann/hlld.h).  A 16 -> 32 -> 32 -> 1 MLP
  * (ReLU) predicts per face whether the cheap HLLE flux is within tolerance of
  * HLLD; with riemann = KR_RIEMANN_LEARNED the flux sweep evaluates it with BF16
- * tensor-core MMAs (FP32 accumulate) at stage 0 of every sel_period-th step
- * and uses HLLE for a warp of 32 consecutive faces of the sweep when every one
- * of them has logit > threshold and none is a face that a neighbouring block
- * computes too (block sides, the edge EMFs' ghost lines), HLLD elsewhere, so
- * every face gets one flux; the choice holds until the next evaluation.  Parameters: 1633 floats, W1[16][32], b1[32], W2[32][32],
- * b2[32], W3[32], b3, row-major [in][out]. */
+ * tensor-core MMAs (FP32 accumulate) at stage 0 of every sel_period-th step.
+ * A face that only its own block computes uses HLLE when every such face of its
+ * warp (32 consecutive faces of the sweep) has logit > threshold; a face that a
+ * neighbouring block computes too (block sides, the edge EMFs' ghost lines)
+ * uses HLLE when its own logit is > threshold, which every block holding it
+ * evaluates identically, so every face gets one flux.  HLLD elsewhere; the
+ * choice holds until the next evaluation.  Parameters: 1633 floats, W1[16][32],
+ * b1[32], W2[32][32], b2[32], W3[32], b3, row-major [in][out]. */
 
 /* Upload selector parameters and the logit threshold to a context. */
 int kr_set_selector( kr_ctx * ctx, const float * params, float threshold );
 
-/* Faces evaluated and faces given HLLE (whole warps) since the last reset
+/* Faces evaluated and faces given HLLE since the last reset
  * (learned mode; counted when the network runs). */
 int kr_selector_stats( kr_ctx * ctx, long long * faces, long long * cheap, int reset );
 
@@ -244,9 +247,12 @@ const char* kr_learn_last_error( void );
  * the array's device address (cudaGetSymbolAddress) -- make that first call
  * before any stream capture.  All calls share the array: calls that overlap on
  * the GPU race and must be serialised by the caller.
- *   cfg   : mhd, n[3], x_min/x_max (one block covering the box), gamma, cfl,
+ *   cfg   : abi_version (KR_ABI_VERSION, else -1), mhd, n[3] (each >= 4,
+ *           else -1), x_min/x_max (one block covering the box), gamma, cfl,
  *           rho_floor, tmp_floor; nb and precision are ignored
- *   u     : device, conserved state [5][n2][n1][n0] (rho, E, m0..2)
+ *   u     : device, conserved state [5][n2][n1][n0] (rho, E, m0..2); read
+ *           only: the density and pressure floors apply to w alone, u is not
+ *           healed (the engine's step writes healed rho / E back into U)
  *   bf    : device, face B [3][n2+5][n1+5][n0+5] (MHD only, else may be NULL)
  *   w     : device output, primitives [nw][n2+4][n1+4][n0+4], interior written
  *           (nw = 8 MHD: rho, p, v0..2, B_cc0..2; 5 hydro)

@@ -3,10 +3,13 @@ import ctypes
 import os
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_PKG, "libkrb200.so")
+# KRATOS_B200_VARIANT=nofma selects the parity build (no fused multiply-add,
+# the reference's own CPU arithmetic), used by tests only
+_VARIANT = os.environ.get("KRATOS_B200_VARIANT", "")
+LIB_PATH = os.path.join(_PKG, "libkrb200%s.so" % ("_" + _VARIANT if _VARIANT else ""))
 
 KR_ABI_VERSION = 5
-KR_FLAG_TILED, KR_FLAG_HALO_ALL, KR_FLAG_BOXES = 1, 2, 4
+KR_FLAG_HALO_ALL, KR_FLAG_BOXES = 2, 4
 BC_KINDS = {"per": 0, "out": 1, "ref": 2, "fre": 3, "fixd": 4}
 KR_RIEMANN_DEFAULT, KR_RIEMANN_HLLE, KR_RIEMANN_LEARNED = 0, 1, 2
 

@@ -65,6 +65,20 @@ class BoxBatch:
         for d, _ in self.groups.values():
             d.step(n_steps)
 
+    def set_selector(self, params, threshold):
+        """Learned mode (riemann = KR_RIEMANN_LEARNED): the same network and
+        threshold for every size group."""
+        for d, _ in self.groups.values():
+            d.set_selector(params, threshold)
+
+    def selector_stats(self, reset=False):
+        """Faces evaluated and faces given HLLE, summed over the groups."""
+        f = c = 0
+        for d, _ in self.groups.values():
+            a, b = d.selector_stats(reset)
+            f, c = f + a, c + b
+        return f, c
+
     def status(self):
         return max(d.status() for d, _ in self.groups.values())
 

@@ -35,20 +35,28 @@ def nvcc():
     raise RuntimeError("nvcc not found")
 
 
-def up_to_date():
-    if not os.path.exists(LIB):
+# Parity variant: the same sources without fused multiply-add (every product
+# rounded before the add, as the reference's CPU build computes), so FP64 steps
+# can be compared with the reference where rounding decides a solver branch.
+# Test infrastructure; the product is LIB.
+LIB_NOFMA = os.path.join(PKG, "libkrb200_nofma.so")
+
+
+def up_to_date(lib=LIB):
+    if not os.path.exists(lib):
         return False
-    t = os.path.getmtime(LIB)
+    t = os.path.getmtime(lib)
     return all(os.path.getmtime(d) <= t for d in DEPS if os.path.exists(d))
 
 
 def build(force=False, verbose=False):
-    if not force and up_to_date():
-        return LIB
-    cmd = [nvcc()] + NVCC_FLAGS + ["-I", os.path.join(ROOT, "include"), "-o", LIB] + SOURCES
-    if verbose:
-        print(" ".join(cmd))
-    subprocess.check_call(cmd)
+    for lib, extra in ((LIB, []), (LIB_NOFMA, ["--fmad=false"])):
+        if not force and up_to_date(lib):
+            continue
+        cmd = [nvcc()] + NVCC_FLAGS + extra + ["-I", os.path.join(ROOT, "include"), "-o", lib] + SOURCES
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.check_call(cmd)
     return LIB
 
 

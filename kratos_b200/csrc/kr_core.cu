@@ -92,7 +92,7 @@ struct args_t
     const float * sel_b;              // b1, b2, b3
     float sel_thr;                    // logit threshold for HLLE
     unsigned long long * sel_cnt;     // [0] faces, [1] faces given HLLE
-    unsigned char * sel_dec;          // per (axis, block, warp of 32 faces): 1 = HLLE
+    unsigned * sel_dec;               // per (axis, block, warp of 32 faces): bit l = lane l on HLLE
     long long sel_wcap;               // warps of faces per (axis, block)
     int sel_period;                   // steps between evaluations of the network
     // face sampling for selector training (collect steps only)
@@ -305,11 +305,21 @@ __global__ void __launch_bounds__( 256, ( MHD && DT ) ? 3 : 4 ) k_c2p( const arg
                 }
             }
             dt = smax > 0 ? a.cfl / smax : FLT_MAX;
+            // fmax drops a NaN speed, so a NaN velocity would leave dt finite:
+            // flag it in the status word (bit 1) instead
+            if( isnan( prim[ MOM ] + prim[ MOM + 1 ] + prim[ MOM + 2 ] ) )
+                dt = -1;
         }
     }
     if( DT )
     {
         __shared__ double red[ 8 ];
+        if( __any_sync( 0xffffffffu, dt < 0 ) )
+        {
+            if( ( threadIdx.x & 31 ) == 0 )
+                atomicOr( & a.s[ 0 ].status, 2 );
+            dt = dt < 0 ? FLT_MAX : dt;
+        }
         dt = warp_min( dt );
         if( ( threadIdx.x & 31 ) == 0 )
             red[ threadIdx.x >> 5 ] = dt;
@@ -878,16 +888,22 @@ void solve_store( const args_t< R > & a, int b, int axis, const int * ii, bool v
     }
 }
 
-// One thread per face.  lines == 0: every face of the sweep (the MHD transverse
-// ghost lines included, mhd/integrator/integrator.h:138-168); lines != 0: only
-// those ghost lines (the tiled kernel below does the rest).
+// One thread per face: every face of the sweep, the MHD transverse ghost lines
+// included (mhd/integrator/integrator.h:138-168).
 // Learned mode (no reference counterpart).  The network runs at stage 0 of
 // every sel_period-th step (and the step after new weights): this sweep
-// evaluates it for every face, and a warp's 32 faces go to HLLE together, only
-// when it passes every one of them (a face it flags keeps its warp on HLLD).
-// Each warp thus runs one solver, and the choice is one byte per warp
-// (sel_dec, wid: the warp's number in the sweep's chunk order), which the
-// other sweeps of the period read (FLUX_APPLY) on the same face grid.
+// evaluates it for every face.  A face that only this block computes follows
+// its warp: the warp's such faces go to HLLE together, only when the network
+// passes every one of them (a face it flags keeps them all on HLLD), so most
+// warps run one solver.  A face that more than one block computes -- on a
+// block side along the sweep, or within one cell of a transverse side, where
+// the neighbours' ghost lines (the edge EMFs' inputs) hold it too -- follows
+// its own logit instead: every block that computes it reconstructs the same
+// states from the same (ghost-copied) primitives and so takes the same
+// decision, and the face gets one flux, so the update keeps telescoping.
+// The choice is kept as one 32-bit mask per warp (sel_dec, wid: the warp's
+// number in the sweep's chunk order), which the other sweeps of the period
+// read (FLUX_APPLY) on the same face grid.
 template< bool MHD, class R > __device__ __forceinline__
 void learned_solve( const args_t< R > & a, int b, int axis, const int * ii, bool valid,
                     R * ql, R * qr, unsigned wid )
@@ -905,28 +921,26 @@ void learned_solve( const args_t< R > & a, int b, int axis, const int * ii, bool
     float f[ MLP_IN ];
     face_features< R >( ql, qr, e.gamma, f );
     const float z = mlp_logit( f, a.sel_w, a.sel_b, xs[ warp ] );
-    // A face that more than one block computes -- on a block side along the
-    // sweep, or within one cell of a transverse side, where the neighbours'
-    // ghost lines (the edge EMFs' inputs) hold it too -- must get the same
-    // flux in every block, or the update stops telescoping: those faces stay
-    // on HLLD (and so does their warp), so the choice never depends on which
-    // block's warp holds them.
+    // faces that a neighbouring block computes too (see above)
     const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
     const int a1 = mod3( axis + 1 ), a2 = mod3( axis + 2 );
     const bool shared = ii[ axis ] == 0 || ii[ axis ] == nn[ axis ]
                      || ii[ a1 ] <= 0 || ii[ a1 ] >= nn[ a1 ] - 1
                      || ii[ a2 ] <= 0 || ii[ a2 ] >= nn[ a2 ] - 1;
-    const unsigned mv = __ballot_sync( 0xffffffffu, valid );
-    const unsigned mc = __ballot_sync( 0xffffffffu, valid && ! shared && z > a.sel_thr );
-    const bool cheap = mv != 0u && mc == mv;
+    const bool pass = z > a.sel_thr;
+    const unsigned mv = __ballot_sync( 0xffffffffu, valid && ! shared );
+    const unsigned mc = __ballot_sync( 0xffffffffu, valid && ! shared && pass );
+    const bool cheap = shared ? pass : ( mv != 0u && mc == mv );
+    const unsigned mask = __ballot_sync( 0xffffffffu, valid && cheap );
+    const unsigned mvalid = __ballot_sync( 0xffffffffu, valid );
     if( lane == 0 )
     {
-        a.sel_dec[ ( ( size_t ) axis * a.nblk + b ) * a.sel_wcap + wid ] = cheap ? 1 : 0;
-        if( mv )
+        a.sel_dec[ ( ( size_t ) axis * a.nblk + b ) * a.sel_wcap + wid ] = mask;
+        if( mvalid )
         {
-            atomicAdd( a.sel_cnt, ( unsigned long long ) __popc( mv ) );
-            if( cheap )
-                atomicAdd( a.sel_cnt + 1, ( unsigned long long ) __popc( mv ) );
+            atomicAdd( a.sel_cnt, ( unsigned long long ) __popc( mvalid ) );
+            if( mask )
+                atomicAdd( a.sel_cnt + 1, ( unsigned long long ) __popc( mask ) );
         }
     }
     if( ! valid )
@@ -999,10 +1013,10 @@ void plm_stencil( const args_t< R > & a, int b, int axis, int step, const int * 
 }
 
 // One CTA's 128 faces of a sweep: bx = CTA along the faces of one (x, y)
-// plane (lines: along all line faces), by = z plane, blockIdx.z = block; dv
+// plane, by = z plane, blockIdx.z = block; dv
 // divides by the row length.
 template< bool MHD, class R, int MODE > __device__ __forceinline__
-void flux_faces( const args_t< R > & a, int axis, int step, int lines, udiv_t dv, unsigned bx, unsigned by,
+void flux_faces( const args_t< R > & a, int axis, int step, udiv_t dv, unsigned bx, unsigned by,
                  bool hlle_warp = false )
 {
     constexpr int NW = MHD ? 11 : 5;   // stored W words: prim (8) + cell E (3)
@@ -1014,47 +1028,22 @@ void flux_faces( const args_t< R > & a, int axis, int step, int lines, udiv_t dv
     int outside = 0;
     unsigned total;
     long long t_lin;                  // face number within the sweep (sampling keys)
-    if( ! lines )
-    {
-        const int lo = MHD ? -1 : 0;
-        int ext[ 3 ];
-        for( int d = 0; d < 3; ++ d )
-            ext[ d ] = d == axis ? nn[ d ] + 1 : nn[ d ] - 2 * lo;
-        total = unsigned( ext[ 0 ] * ext[ 1 ] );
-        const unsigned q = udiv_q( t, dv );
-        ii[ 0 ] = int( t - q * unsigned( ext[ 0 ] ) );
-        ii[ 1 ] = int( q );
-        ii[ 2 ] = int( by );
-        t_lin = ( long long ) t + ( long long ) total * by;
-        for( int d = 0; d < 3; ++ d )
-            if( d != axis )
-            {
-                ii[ d ] += lo;
-                outside += ( ii[ d ] < 0 || ii[ d ] >= nn[ d ] );
-            }
-    }
-    else
-    {
-        const int a1 = mod3( axis + 1 ), a2 = mod3( axis + 2 );
-        const int nf = nn[ axis ] + 1;
-        total = unsigned( nf * ( 2 * nn[ a2 ] + 2 * nn[ a1 ] ) );
-        const unsigned q = udiv_q( t, dv );
-        ii[ axis ] = int( t - q * unsigned( nf ) );
-        long long l = q;
-        t_lin = t;
-        if( l < 2LL * nn[ a2 ] )
+    const int lo = MHD ? -1 : 0;
+    int ext[ 3 ];
+    for( int d = 0; d < 3; ++ d )
+        ext[ d ] = d == axis ? nn[ d ] + 1 : nn[ d ] - 2 * lo;
+    total = unsigned( ext[ 0 ] * ext[ 1 ] );
+    const unsigned q = udiv_q( t, dv );
+    ii[ 0 ] = int( t - q * unsigned( ext[ 0 ] ) );
+    ii[ 1 ] = int( q );
+    ii[ 2 ] = int( by );
+    t_lin = ( long long ) t + ( long long ) total * by;
+    for( int d = 0; d < 3; ++ d )
+        if( d != axis )
         {
-            ii[ a1 ] = ( l & 1 ) ? nn[ a1 ] : -1;
-            ii[ a2 ] = int( l >> 1 );
+            ii[ d ] += lo;
+            outside += ( ii[ d ] < 0 || ii[ d ] >= nn[ d ] );
         }
-        else
-        {
-            l -= 2LL * nn[ a2 ];
-            ii[ a2 ] = ( l & 1 ) ? nn[ a2 ] : -1;
-            ii[ a1 ] = int( l >> 1 );
-        }
-        outside = 1;
-    }
     // corner lines are never read; lanes past the end idle.  Lanes stay alive
     // until the (warp-collective) selector has run.
     const bool valid = t < total && outside <= 1;
@@ -1072,7 +1061,7 @@ void flux_faces( const args_t< R > & a, int axis, int step, int lines, udiv_t dv
         plm_stencil< MHD, R >( a, b, axis, step, ii, wb, st, ql, qr );
     }
     if constexpr( learned || MODE == FLUX_APPLY )
-    {   // every face of the sweep here (lines == 0)
+    {
         if constexpr( learned )
             learned_solve< MHD, R >( a, b, axis, ii, valid, ql, qr, wid );
         else
@@ -1080,12 +1069,12 @@ void flux_faces( const args_t< R > & a, int axis, int step, int lines, udiv_t dv
         return;
     }
     const unsigned long long key = ( ( unsigned long long ) b * 3 + axis ) * 0x9E3779B97F4A7C15ull
-                                 + ( unsigned long long ) ( lines ? t_lin + ( 1ll << 40 ) : t_lin );
+                                 + ( unsigned long long ) t_lin;
     solve_store< MHD, R, MODE >( a, b, axis, ii, valid, ql, qr, threadIdx.x >> 5, key );
 }
 
 template< bool MHD, class R, int MODE >
-__global__ void __launch_bounds__( 128, ( flux_min_ctas< R, MODE >(  ) ) ) k_flux( const args_t< R > a, int axis, int step, int lines, udiv_t dv )
+__global__ void __launch_bounds__( 128, ( flux_min_ctas< R, MODE >(  ) ) ) k_flux( const args_t< R > a, int axis, int step, udiv_t dv )
 {
     bool hlle_warp = false;
     if constexpr( MODE == FLUX_APPLY )
@@ -1093,10 +1082,11 @@ __global__ void __launch_bounds__( 128, ( flux_min_ctas< R, MODE >(  ) ) ) k_flu
         // loaded first (gridDim.x: 128-face chunks per z plane)
         if( step == 0 && sel_eval_step( a.s, a.sel_period ) )
             return;                   // the network's sweep (k_flux_eval) solves this one
-        hlle_warp = a.sel_dec[ ( ( size_t ) axis * a.nblk + blockIdx.z ) * a.sel_wcap
-                               + ( blockIdx.y * gridDim.x + blockIdx.x ) * 4u + ( threadIdx.x >> 5 ) ] != 0;
+        hlle_warp = ( a.sel_dec[ ( ( size_t ) axis * a.nblk + blockIdx.z ) * a.sel_wcap
+                                 + ( blockIdx.y * gridDim.x + blockIdx.x ) * 4u + ( threadIdx.x >> 5 ) ]
+                      >> ( threadIdx.x & 31 ) ) & 1u;
     }
-    flux_faces< MHD, R, MODE >( a, axis, step, lines, dv, blockIdx.x, blockIdx.y, hlle_warp );
+    flux_faces< MHD, R, MODE >( a, axis, step, dv, blockIdx.x, blockIdx.y, hlle_warp );
 }
 
 // Learned mode, the network's sweep: a fixed grid strides over the 128-face
@@ -1110,109 +1100,7 @@ k_flux_eval( const args_t< R > a, int axis, int step, udiv_t dv, unsigned cpp, u
     if( step != 0 || ! sel_eval_step( a.s, a.sel_period ) )
         return;
     for( unsigned ch = blockIdx.x; ch < cpp * nz; ch += gridDim.x )
-        flux_faces< MHD, R, KR_RIEMANN_LEARNED >( a, axis, step, 0, dv, ch % cpp, ch / cpp );
-}
-
-// Shared-memory tiled sweep over the faces whose transverse position lies in
-// the block interior.  A CTA of 32 x 4 threads loads the primitives of its tile
-// once (coalesced, halo of 2 + 1 cells along the sweep) and reconstructs from
-// shared memory.  AX = 1, 2: 32 lanes along x, TS faces along the sweep, one
-// position along the third axis.  AX = 0: TS faces along x, 4 rows along y.
-// Tile t of T covers faces [t*nf/T, (t+1)*nf/T) of the nf = n+1 along the sweep.
-template< bool MHD, class R, int MODE, int AX >
-__global__ void __launch_bounds__( 128, 4 ) k_flux_tile( const args_t< R > a, int step, int T, int TSmax )
-{
-    constexpr int NW = MHD ? 11 : 5;
-    constexpr int NP = MHD ? 8 : 5;
-    extern __shared__ __align__( 16 ) unsigned char smem_raw[  ];
-    R * q = reinterpret_cast< R * >( smem_raw );
-    const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
-    const int b = blockIdx.z;
-    const int nf = nn[ AX ] + 1;
-    const int tid = threadIdx.x + 32 * threadIdx.y;
-    const int warp = threadIdx.y;
-    int tile, f0, f1, base[ 3 ];
-    if( AX != 0 )
-    {   // blockIdx.x = x-tile * T + face tile; blockIdx.y = third-axis position
-        const int A2 = AX == 1 ? 2 : 1;
-        tile = blockIdx.x % T;
-        base[ 0 ] = 32 * ( blockIdx.x / T );
-        base[ A2 ] = blockIdx.y;
-        base[ AX ] = 0;
-    }
-    else
-    {   // blockIdx.x = row group * T + face tile; rows along y; blockIdx.y = z
-        tile = blockIdx.x % T;
-        base[ 1 ] = 4 * ( blockIdx.x / T );
-        base[ 2 ] = blockIdx.y;
-        base[ 0 ] = 0;
-    }
-    f0 = int( ( long long ) tile * nf / T );
-    f1 = int( ( long long )( tile + 1 ) * nf / T );
-    const int ts = f1 - f0;                        // faces in this tile
-    const int ncell = ts + 3;                      // cells f0-2 .. f1
-    // load: q[k][r][c] with (r, c) = (sweep cell, lane) for AX != 0 and
-    // (row, sweep cell) for AX == 0; cells f0-2+s
-    if( AX != 0 )
-    {
-        const int NR = TSmax + 3;
-        for( int idx = tid; idx < NP * ncell * 32; idx += 128 )
-        {
-            const int c = idx & 31, r = ( idx >> 5 ) % ncell, k = ( idx >> 5 ) / ncell;
-            if( MHD && k == BCC + AX )
-                continue;
-            int jj[ 3 ] = { base[ 0 ] + c, base[ 1 ], base[ 2 ] };
-            jj[ AX ] = f0 - 2 + r;
-            q[ ( k * NR + r ) * 32 + c ] = a.w[ iw( a, b, k, NW, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) ];
-        }
-    }
-    else
-    {
-        const int NC = TSmax + 3;
-        for( int idx = tid; idx < NP * 4 * ncell; idx += 128 )
-        {
-            const int c = idx % ncell, r = ( idx / ncell ) % 4, k = idx / ( ncell * 4 );
-            if( MHD && k == BCC )
-                continue;
-            q[ ( k * 4 + r ) * NC + c ] = a.w[ iw( a, b, k, NW, f0 - 2 + c, base[ 1 ] + r, base[ 2 ] ) ];
-        }
-    }
-    __syncthreads(  );
-    // compute: AX != 0 -> face j = threadIdx.y + 4 m, lane c = threadIdx.x;
-    //          AX == 0 -> face j = threadIdx.x + 32 m, row = threadIdx.y
-    const int nloop = AX != 0 ? ( TSmax + 3 ) / 4 : ( TSmax + 31 ) / 32;
-    for( int m = 0; m < nloop; ++ m )
-    {
-        const int j = AX != 0 ? int( threadIdx.y ) + 4 * m : int( threadIdx.x ) + 32 * m;
-        if( AX != 0 && j >= TSmax )
-            break;                                 // j is uniform per warp here
-        const bool valid = j < ts;
-        int ii[ 3 ] = { base[ 0 ], base[ 1 ], base[ 2 ] };
-        if( AX != 0 ) { ii[ 0 ] += threadIdx.x; ii[ AX ] = f0 + j; }
-        else          { ii[ 0 ] = f0 + j; ii[ 1 ] += threadIdx.y; }
-        R ql[ 8 ], qr[ 8 ];
-        if( valid )
-            for( int k = 0; k < NP; ++ k )
-            {
-                if( MHD && k == BCC + AX )
-                {
-                    const R bn = R( a.bf[ step ][ ibf( a, b, AX, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] );
-                    ql[ k ] = qr[ k ] = bn;
-                    continue;
-                }
-                R v[ 4 ];
-                if( AX != 0 )
-                    for( int s = 0; s < 4; ++ s )
-                        v[ s ] = q[ ( k * ( TSmax + 3 ) + j + s ) * 32 + threadIdx.x ];
-                else
-                    for( int s = 0; s < 4; ++ s )
-                        v[ s ] = q[ ( k * 4 + threadIdx.y ) * ( TSmax + 3 ) + j + s ];
-                plm_face_fast< R >( v[ 0 ], v[ 1 ], v[ 2 ], v[ 3 ], ql[ k ], qr[ k ] );
-            }
-        const unsigned long long key = ( ( unsigned long long ) b * 3 + AX ) * 0x9E3779B97F4A7C15ull
-            + ( unsigned long long )( ii[ 0 ] + 1 + ( nn[ 0 ] + 3 ) * ( ( long long )( ii[ 1 ] + 1 ) + ( nn[ 1 ] + 3 ) * ( long long )( ii[ 2 ] + 1 ) ) );
-        solve_store< MHD, R, MODE >( a, b, AX, ii, valid, ql, qr, warp, key );
-    }
+        flux_faces< MHD, R, KR_RIEMANN_LEARNED >( a, axis, step, dv, ch % cpp, ch / cpp );
 }
 
 ////////////////////////////////////////////////////////////
@@ -1315,8 +1203,9 @@ __global__ void __launch_bounds__( 256 ) k_emf( const args_t< R > a, udiv_t dv )
 
 ////////////////////////////////////////////////////////////
 // Conserved update (hydro/integrator/integrator.h:241-265 add_flux with
-// rk2.h:404-425 load) and CT face update (mhd/integrator/integrator.h:385-462,
-// mhd/integrator/rk2.h:244-258 set_field).  One thread per lattice site.
+// hydro/integrator/rk2.h:20-34 load) and CT face update
+// (mhd/integrator/integrator.h:387-462, mhd/integrator/rk2.h:49-63 set_field).
+// One thread per lattice site.
 
 // Static refinement (SMR): the face of a refined side is left out of the
 // update (load_flux_sfc, f_a = -1), and afterwards the cell takes the
@@ -1915,7 +1804,7 @@ struct kr_ctx
     unsigned long long * sel_cnt = nullptr;
     float sel_thr = 0.f;
     bool sel_ready = false;
-    unsigned char * sel_dec = nullptr; // learned mode: solver per warp of faces
+    unsigned * sel_dec = nullptr;     // learned mode: solver per face, a mask per warp
     long long sel_wcap = 0;
     // selector training samples (only during kr_selector_collect)
     float * smp = nullptr;
@@ -1927,7 +1816,6 @@ struct kr_ctx
     cudaGraphExec_t graph_exec = nullptr;
     cudaStream_t graph_stream = nullptr;
     std::vector< geo_t > geo_h;
-    bool no_tiles = false;             // force the per-face flux kernel (testing)
     int n_sm = 148;                    // multiprocessors of the device
     // sharding: this rank's blocks and the halo exchange with the others
     int nranks = 1, rank = 0;
@@ -2029,80 +1917,27 @@ static long long phys_sites( const kr_ctx * c )
     return std::max( { ( long long ) n[ 1 ] * n[ 2 ], ( long long ) n[ 0 ] * n[ 2 ], ( long long ) n[ 0 ] * n[ 1 ] } );
 }
 
-// Flux sweep along `axis`: the shared-memory tiled kernel over the interior
-// transverse positions plus, for MHD, the per-face kernel over the transverse
-// ghost lines; the per-face kernel alone where the tile shape does not fit.
-struct flux_tiling { int T, TSmax; size_t smem; bool ok; };
-
-template< class R >
-static flux_tiling tiling_for( const kr_ctx * c, int axis, int np )
-{
-    const int * n = c->cfg.n;
-    flux_tiling t;
-    const int nf = n[ axis ] + 1;
-    // about 32 faces per tile in FP32, 16 in FP64 (shared memory per CTA)
-    t.T = std::max( 1, nf / ( sizeof( R ) == 4 ? 32 : 16 ) );
-    t.TSmax = ( nf + t.T - 1 ) / t.T;
-    t.smem = axis != 0 ? size_t( np ) * ( t.TSmax + 3 ) * 32 * sizeof( R )
-                       : size_t( np ) * 4 * ( t.TSmax + 3 ) * sizeof( R );
-    t.ok = n[ 0 ] % 32 == 0 && n[ 1 ] % 4 == 0 && t.smem <= 96 * 1024;
-    return t;
-}
-
-template< bool MHD, class R, int MODE, int AX >
-static void launch_tile( kr_ctx * c, cudaStream_t st, const args_t< R > & a, int stage,
-                         const flux_tiling & t )
-{
-    const int * n = c->cfg.n;
-    dim3 grid;
-    if( AX == 0 ) grid = dim3( t.T * ( n[ 1 ] / 4 ), n[ 2 ], c->nblk );
-    else          grid = dim3( t.T * ( n[ 0 ] / 32 ), AX == 1 ? n[ 2 ] : n[ 1 ], c->nblk );
-    static bool attr_set = false;
-    if( ! attr_set && t.smem > 48 * 1024 )
-    {
-        cudaFuncSetAttribute( k_flux_tile< MHD, R, MODE, AX >,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024 );
-        attr_set = true;
-    }
-    k_flux_tile< MHD, R, MODE, AX ><<< grid, dim3( 32, 4 ), t.smem, st >>>( a, stage, t.T, t.TSmax );
-}
-
 template< bool MHD, class R, int MODE >
 static void launch_flux( kr_ctx * c, cudaStream_t st, const args_t< R > & a, int axis, int stage )
 {
+    // one thread per face of the sweep, the MHD transverse ghost lines included
     const int * n = c->cfg.n;
-    constexpr int NP = MHD ? 8 : 5;
-    const flux_tiling t = tiling_for< R >( c, axis, NP );
-    if( ! t.ok || c->no_tiles || MODE == KR_RIEMANN_LEARNED )
+    int ext[ 3 ];
+    for( int d = 0; d < 3; ++ d )
+        ext[ d ] = ( d == axis ) ? n[ d ] + 1 : n[ d ] + ( MHD ? 2 : 0 );
+    if constexpr( MODE == KR_RIEMANN_LEARNED && MHD )
     {
-        int ext[ 3 ];
-        for( int d = 0; d < 3; ++ d )
-            ext[ d ] = ( d == axis ) ? n[ d ] + 1 : n[ d ] + ( MHD ? 2 : 0 );
-        if constexpr( MODE == KR_RIEMANN_LEARNED && MHD )
-        {
-            const unsigned cpp = blocks_for( ( long long ) ext[ 0 ] * ext[ 1 ], 128 );
-            const unsigned ge = unsigned( std::max< long long >( 1, std::min< long long >(
-                ( long long ) cpp * ext[ 2 ], ( 2LL * c->n_sm * flux_min_ctas< R, KR_RIEMANN_LEARNED >(  ) ) / c->nblk ) ) );
-            k_flux_eval< MHD, R ><<< dim3( ge, 1, c->nblk ), 128, 0, st >>>(
-                a, axis, stage, make_udiv( unsigned( ext[ 0 ] ) ), cpp, unsigned( ext[ 2 ] ) );
-        }
-        // sweeps without the network: each warp of faces runs the solver
-        // chosen for it (exits at once on the network's sweep)
-        constexpr int M = ( MODE == KR_RIEMANN_LEARNED && MHD ) ? FLUX_APPLY : MODE;
-        k_flux< MHD, R, M ><<< dim3( blocks_for( ( long long ) ext[ 0 ] * ext[ 1 ], 128 ), ext[ 2 ], c->nblk ), 128, 0, st >>>(
-            a, axis, stage, 0, make_udiv( unsigned( ext[ 0 ] ) ) );
-        return;
+        const unsigned cpp = blocks_for( ( long long ) ext[ 0 ] * ext[ 1 ], 128 );
+        const unsigned ge = unsigned( std::max< long long >( 1, std::min< long long >(
+            ( long long ) cpp * ext[ 2 ], ( 2LL * c->n_sm * flux_min_ctas< R, KR_RIEMANN_LEARNED >(  ) ) / c->nblk ) ) );
+        k_flux_eval< MHD, R ><<< dim3( ge, 1, c->nblk ), 128, 0, st >>>(
+            a, axis, stage, make_udiv( unsigned( ext[ 0 ] ) ), cpp, unsigned( ext[ 2 ] ) );
     }
-    if( axis == 0 )      launch_tile< MHD, R, MODE, 0 >( c, st, a, stage, t );
-    else if( axis == 1 ) launch_tile< MHD, R, MODE, 1 >( c, st, a, stage, t );
-    else                 launch_tile< MHD, R, MODE, 2 >( c, st, a, stage, t );
-    if( MHD )
-    {
-        const int a1 = ( axis + 1 ) % 3, a2 = ( axis + 2 ) % 3;
-        const long long nline = ( long long )( n[ axis ] + 1 ) * ( 2LL * n[ a1 ] + 2LL * n[ a2 ] );
-        k_flux< MHD, R, MODE ><<< dim3( blocks_for( nline, 128 ), 1, c->nblk ), 128, 0, st >>>(
-            a, axis, stage, 1, make_udiv( unsigned( n[ axis ] + 1 ) ) );
-    }
+    // sweeps without the network: each warp of faces runs the solver chosen
+    // for it (exits at once on the network's sweep)
+    constexpr int M = ( MODE == KR_RIEMANN_LEARNED && MHD ) ? FLUX_APPLY : MODE;
+    k_flux< MHD, R, M ><<< dim3( blocks_for( ( long long ) ext[ 0 ] * ext[ 1 ], 128 ), ext[ 2 ], c->nblk ), 128, 0, st >>>(
+        a, axis, stage, make_udiv( unsigned( ext[ 0 ] ) ) );
 }
 
 template< bool MHD, class R >
@@ -2576,7 +2411,6 @@ static kr_ctx * create_ctx( const kr_cfg * cfg, int n_regions, const kr_region *
     // The shared-memory tiled sweep is opt-in: on the 256^3 OT step it measured
     // slower than the per-face kernel (more registers per thread, long per-thread
     // face loops, a tail of partial CTAs), so the per-face kernel is the default.
-    c->no_tiles = ( cfg->flags & KR_FLAG_TILED ) == 0;
     const int * n = cfg->n;
     c->nranks = ranks_of( * cfg );
     c->rank = c->nranks > 1 ? cfg->rank : 0;
@@ -2699,7 +2533,7 @@ static kr_ctx * create_ctx( const kr_cfg * cfg, int n_regions, const kr_region *
                 ext[ d ] = d == ax ? n[ d ] + 1 : n[ d ] + 2;
             c->sel_wcap = std::max( c->sel_wcap, blocks_for( ext[ 0 ] * ext[ 1 ], 128 ) * ext[ 2 ] * 4 );
         }
-        const size_t bytes = size_t( 3 ) * nb * c->sel_wcap;
+        const size_t bytes = size_t( 3 ) * nb * c->sel_wcap * sizeof( unsigned );
         ok = ck( c, cudaMalloc( & c->sel_dec, bytes ), "malloc selector choices" )
           && ck( c, cudaMemset( c->sel_dec, 0, bytes ), "memset selector choices" );
     }
@@ -3215,13 +3049,7 @@ int kr_profile_step( kr_ctx * c, int n_kinds, double * ms )
 int kr_launches_per_step( kr_ctx * c )
 {
     if( ! c ) return -1;
-    int flux = 0;
-    for( int axis = 0; axis < 3; ++ axis )
-    {
-        const flux_tiling t = c->cfg.precision == 1 ? tiling_for< float >( c, axis, c->cfg.mhd ? 8 : 5 )
-                                                    : tiling_for< double >( c, axis, c->cfg.mhd ? 8 : 5 );
-        flux += ( t.ok && ! c->no_tiles && c->cfg.mhd ) ? 2 : 1;
-    }
+    int flux = 3;                     // one per-face sweep per axis
     if( c->cfg.mhd && c->cfg.riemann == KR_RIEMANN_LEARNED )
         flux = 6;                     // per sweep: the network's kernel and the list kernel
     const int halo = ( c->hsend.items.empty(  ) ? 0 : 1 ) + ( c->hrecv.items.empty(  ) ? 0 : 1 );
@@ -3584,15 +3412,22 @@ extern "C" int kr_c2p_dt_noalloc( const kr_cfg * cfg, const double * u, const do
 {
     using namespace kr;
     g_create_error.clear(  );
-    if( ! cfg || ! u || ! w || ! dt_out || ( cfg->mhd && ! bf ) )
+    if( ! cfg || cfg->abi_version != KR_ABI_VERSION )
+    {
+        g_create_error = "kr_c2p_dt_noalloc: missing configuration or ABI version mismatch";
+        return -1;
+    }
+    if( ! u || ! w || ! dt_out || ( cfg->mhd && ! bf ) )
     {
         g_create_error = "kr_c2p_dt_noalloc: null argument";
         return -1;
     }
+    // the same lower bound as kr_ctx_create: every axis holds a PLM stencil, so
+    // each cell's face B has both faces inside the block
     for( int a = 0; a < 3; ++ a )
-        if( cfg->n[ a ] < 1 )
+        if( cfg->n[ a ] < 4 )
         {
-            g_create_error = "kr_c2p_dt_noalloc: block size must be positive";
+            g_create_error = "kr_c2p_dt_noalloc: need n >= 4 cells per axis";
             return -1;
         }
     const long long nc = ( long long ) cfg->n[ 0 ] * cfg->n[ 1 ] * cfg->n[ 2 ];

@@ -37,7 +37,7 @@ def make_cfg(mhd, nb, n, gamma=1.66667, cfl=0.3, precision=2, riemann=0,
     c.gamma, c.cfl = float(gamma), float(cfl)
     c.rho_floor, c.tmp_floor = float(rho_floor), float(tmp_floor)
     c.dt_init, c.dt_expand, c.device = float(dt_init), float(dt_expand), int(device)
-    c.flags = int(flags)              # KR_FLAG_TILED, KR_FLAG_HALO_ALL, KR_FLAG_BOXES
+    c.flags = int(flags)              # KR_FLAG_HALO_ALL, KR_FLAG_BOXES
     c.n_ranks, c.rank = int(n_ranks), int(rank)
     c.sel_period = int(sel_period)
     for k in range(6):

@@ -605,6 +605,12 @@ void mesh_t::evolve(  )
     // needs t after every step; otherwise the steps up to the next displayed
     // cycle run as one batch of graph launches with a single host sync.
     const bool per_step = dt_output_ < 1e30 || t_lim_ < 3e38;
+    // cycle.cpp:168-180: an error inside the loop (here: the device status
+    // word, checked after every batch of steps) ends it; with final_output the
+    // state reached is written and evolve returns.
+    bool to_stop = false;
+    try
+    {
     for( ;; )
     {
         if( update_tout(  ) )
@@ -622,6 +628,10 @@ void mesh_t::evolve(  )
         i_cycle_ = stop;
         double dt = 0;
         kr_get_time( ctx_, & t_, & dt, nullptr, nullptr );
+        if( const int st = kr_status( ctx_ ) )
+            throw std::runtime_error( std::string( "kratos_b200: device status " ) + std::to_string( st )
+                                      + ( st & 2 ? " (NaN velocity in the state)" : " (non-finite or non-positive dt)" )
+                                      + " at cycle " + std::to_string( i_cycle_ ) + "\n" );
         if( i_cycle_ % n_display_ == 0 )
             std::cout << "cycle = " << std::setw( 5 ) << i_cycle_ << std::scientific
                       << std::setprecision( 6 ) << ", t = " << t_ << ", dt = " << dt
@@ -630,9 +640,18 @@ void mesh_t::evolve(  )
             break;
         ++ i_cycle_;
     }
+    }
+    catch( const std::exception & exc )
+    {
+        std::cerr << exc.what(  );
+        to_stop = true;
+    }
+    if( to_stop && final_output_ )
+    {
+        save( file_name(  ) );
+        return;
+    }
     kr_get_time( ctx_, & t_, nullptr, nullptr, nullptr );
-    if( kr_status( ctx_ ) != 0 )
-        throw std::runtime_error( "kratos_b200: device status error (non-finite dt)" );
     const double dwt = std::chrono::duration< double >( std::chrono::steady_clock::now(  ) - start ).count(  );
     const double speed = n_cell_tot / dwt * ( i_cycle_ - i_cycle_0 + 1 );
     std::cout << "Duration = " << dwt << " s, Speed = " << speed << " cell/s,\n"

@@ -10,7 +10,11 @@ import subprocess
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-_LIB_PATH = os.path.join(_HERE, "ref_cpu", "libkr_oracle.so")
+# "" : the restatement as the reference's CPU build computes it (no fused
+#      multiply-add); "fma": the same source with fused multiply-add, to
+#      measure how far rounding alone moves a case
+_LIB_PATHS = {"": os.path.join(_HERE, "ref_cpu", "libkr_oracle.so"),
+              "fma": os.path.join(_HERE, "ref_cpu", "libkr_oracle_fma.so")}
 
 
 class _Cfg(ctypes.Structure):
@@ -43,19 +47,19 @@ class _Region(ctypes.Structure):
 BC_KINDS = {"per": 0, "out": 1, "ref": 2, "fre": 3, "fixd": 4}
 
 
-_lib = None
+_libs = {}
 
 
 def build():
     subprocess.check_call(["make", "-s", "-f", os.path.join(_HERE, "Makefile")])
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(_LIB_PATH):
+def lib(variant=""):
+    if variant not in _libs:
+        path = _LIB_PATHS[variant]
+        if not os.path.exists(path):
             build()
-        L = ctypes.CDLL(_LIB_PATH)
+        L = ctypes.CDLL(path)
         dp = ctypes.POINTER(ctypes.c_double)
         L.kro_create.restype = ctypes.c_void_p
         L.kro_create.argtypes = [ctypes.POINTER(_Cfg)]
@@ -68,6 +72,7 @@ def lib():
         L.kro_destroy.argtypes = [ctypes.c_void_p]
         L.kro_set_state.argtypes = [ctypes.c_void_p, dp, dp]
         L.kro_get_state.argtypes = [ctypes.c_void_p, dp, dp]
+        L.kro_c2p_dt.argtypes = [ctypes.c_void_p, dp, dp]
         L.kro_step.restype = ctypes.c_int
         L.kro_step.argtypes = [ctypes.c_void_p, ctypes.c_int, dp, dp, dp]
         for f in ("kro_x_cc", "kro_x_fc"):
@@ -84,8 +89,8 @@ def lib():
         L.kro_init_box.argtypes = [ctypes.c_void_p, ctypes.c_ulonglong, ctypes.c_int]
         L.kro_box_n.restype = ctypes.c_int
         L.kro_box_n.argtypes = [ctypes.c_ulonglong, ctypes.c_int]
-        _lib = L
-    return _lib
+        _libs[variant] = L
+    return _libs[variant]
 
 
 def _p(a):
@@ -104,7 +109,7 @@ class OracleMesh:
 
     def __init__(self, mhd, nb, n, gamma, cfl=0.3, x_min=(0, 0, 0), x_max=(1, 1, 1),
                  d_floor=1e-9, t_floor=1e-9, dt_expand=2.0, dt_init=0.0, n_threads=0,
-                 kinds=("per",) * 6, w_fix=(0, 0, 0, 0, 0), b_fix=(0, 0, 0), regions=()):
+                 kinds=("per",) * 6, w_fix=(0, 0, 0, 0, 0), b_fix=(0, 0, 0), regions=(), variant=""):
         c = _Cfg()
         c.mhd = int(mhd)
         for a in range(3):
@@ -127,14 +132,15 @@ class OracleMesh:
             rg[k].level = int(lvl)
             for a in range(3):
                 rg[k].x_min[a], rg[k].x_max[a] = float(lo[a]), float(hi[a])
-        self._h = lib().kro_create_tree(ctypes.byref(c), len(regions), rg)
+        self._L = lib(variant)
+        self._h = self._L.kro_create_tree(ctypes.byref(c), len(regions), rg)
         if not self._h:
             raise ValueError("oracle: kro_create_tree failed")
-        self.nblk = lib().kro_nblk(self._h)
+        self.nblk = self._L.kro_nblk(self._h)
         self.level = np.zeros(self.nblk, dtype=np.int32)
         self.reg = np.zeros((self.nblk, 3), dtype=np.int32)
         ip = ctypes.POINTER(ctypes.c_int)
-        lib().kro_block_info(self._h, self.level.ctypes.data_as(ip), self.reg.ctypes.data_as(ip))
+        self._L.kro_block_info(self._h, self.level.ctypes.data_as(ip), self.reg.ctypes.data_as(ip))
         self.t = 0.0
         # cycle.cpp:163-166: an unset dt_init starts the device dt at FLT_MAX / 10
         self.dt_bound = dt_init if dt_init >= np.finfo(np.float32).tiny else FLT_MAX / 10
@@ -142,7 +148,7 @@ class OracleMesh:
 
     def __del__(self):
         if getattr(self, "_h", None):
-            lib().kro_destroy(self._h)
+            self._L.kro_destroy(self._h)
             self._h = None
 
     @property
@@ -159,24 +165,24 @@ class OracleMesh:
         u = np.ascontiguousarray(u, dtype=np.float64).reshape(self.u_shape)
         if self.mhd:
             bf = np.ascontiguousarray(bf, dtype=np.float64).reshape(self.bf_shape)
-            lib().kro_set_state(self._h, _p(u), _p(bf))
+            self._L.kro_set_state(self._h, _p(u), _p(bf))
         else:
-            lib().kro_set_state(self._h, _p(u), None)
+            self._L.kro_set_state(self._h, _p(u), None)
 
     def get_state(self):
         u = np.empty(self.u_shape)
         if self.mhd:
             bf = np.empty(self.bf_shape)
-            lib().kro_get_state(self._h, _p(u), _p(bf))
+            self._L.kro_get_state(self._h, _p(u), _p(bf))
             return u, bf
-        lib().kro_get_state(self._h, _p(u), None)
+        self._L.kro_get_state(self._h, _p(u), None)
         return u, None
 
     def step(self, n_steps=1):
         t = ctypes.c_double(self.t)
         db = ctypes.c_double(self.dt_bound)
         dl = ctypes.c_double(0.0)
-        rc = lib().kro_step(self._h, int(n_steps), ctypes.byref(t), ctypes.byref(db), ctypes.byref(dl))
+        rc = self._L.kro_step(self._h, int(n_steps), ctypes.byref(t), ctypes.byref(db), ctypes.byref(dl))
         if rc == -2:
             raise NotImplementedError("oracle: MHD level jumps are not restated (a refined MHD mesh "
                                       "can be built and initialised, not stepped)")
@@ -184,20 +190,30 @@ class OracleMesh:
             raise FloatingPointError("oracle step produced a non-finite dt")
         self.t, self.dt_bound, self.dt_last = t.value, db.value, dl.value
 
+    def c2p_dt(self):
+        """cons -> prim (floors applied, healing the conserved state) and each
+        block's CFL dt of the current state, without stepping
+        (hydro/eos/adiabatic.h:159-258, mhd/eos/adiabatic.h:84-234).
+        Returns (w [nblk, n2, n1, n0, nw], dt [nblk])."""
+        w = np.empty(self.u_shape)
+        dt = np.empty(self.nblk)
+        self._L.kro_c2p_dt(self._h, _p(w), _p(dt))
+        return w, dt
+
     def init_problem(self, name, seed):
-        if lib().kro_init_problem(self._h, name.encode(), int(seed)) != 0:
+        if self._L.kro_init_problem(self._h, name.encode(), int(seed)) != 0:
             raise ValueError("unknown problem %r for this mesh" % name)
 
     def init_box(self, seed, box):
         """Box `box` of a batch of independent periodic MHD boxes."""
-        if lib().kro_init_box(self._h, int(seed), int(box)) != 0:
+        if self._L.kro_init_box(self._h, int(seed), int(box)) != 0:
             raise ValueError("box workloads need an MHD mesh")
 
     def x_cc(self, block, axis, i):
-        return lib().kro_x_cc(self._h, block, axis, i)
+        return self._L.kro_x_cc(self._h, block, axis, i)
 
     def dx(self, block, axis):
-        return lib().kro_dx(self._h, block, axis)
+        return self._L.kro_dx(self._h, block, axis)
 
 
 def hllc(ql, qr, axis, gamma):

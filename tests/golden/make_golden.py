@@ -31,17 +31,21 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 from kratos_b200.snapshot import Snapshot, to_lex_arrays, to_tree_arrays  # noqa: E402
 
-REF_BIN = os.path.join(ROOT, "oracle", "_ref", "kratos_ref")
+REF_BIN = os.environ.get("KR_REF_BIN", os.path.join(ROOT, "oracle", "_ref", "kratos_ref"))
 
 CASES = [
     # name, problem, nb, n, steps, seed, gamma, extra dynamics keys, keep fields
-    # keep: "full" (initial and final fields), "final" (final fields) or "sums"
+    # keep: "full" (initial and final fields), "final" (final fields), "sums",
+    # or "planes" (sums plus two sampled planes of the final state, below)
     ("shock_16", "shock", (2, 2, 2), (8, 8, 8), 5, 1, 1.4, {}, "full"),
     ("ot_16", "ot", (2, 2, 2), (8, 8, 8), 5, 2, 1.6666666666666667, {}, "full"),
     ("ot_ragged", "ot", (3, 2, 1), (8, 8, 8), 4, 3, 1.6666666666666667, {}, "final"),
     ("shock_floor", "shock", (2, 2, 2), (8, 8, 8), 3, 4, 1.4, {"tmp_floor": "1.0"}, "final"),
     ("shock_c1", "shock", (2, 2, 2), (32, 32, 32), 20, 1, 1.4, {}, "sums"),
     ("ot_64", "ot", (2, 2, 2), (32, 32, 32), 10, 2, 1.6666666666666667, {}, "sums"),
+    # the headline MHD mesh at its full size: 256^3, 64 blocks of 64^3, seed 2,
+    # 50 steps (about 20 minutes of the reference's CPU path on 8 cores)
+    ("ot_256", "ot", (4, 4, 4), (64, 64, 64), 50, 2, 1.6666666666666667, {}, "planes"),
     # physical boundaries (hydro/boundary/phys_functors.h): reflect, outflow, free,
     # fixed (Dirichlet inflow from [init]); "kinds" lists x-, x+, y-, y+, z-, z+
     ("shock_bc", "shock", (2, 2, 2), (8, 8, 8), 5, 5, 1.4,
@@ -131,6 +135,19 @@ def owned_bf(bf, n):
     return bf[:, 2:3 + n[2], 2:3 + n[1], 2:3 + n[0], :].copy()
 
 
+PLANE_STRIDE = 8
+
+
+def sampled_planes(u, nb, n):
+    """Two z-planes of the global cell grid (global z = 0 and the middle one),
+    every PLANE_STRIDE-th cell along x and y: [2, ny, nx, nw]."""
+    nblk, n2, n1, n0, nw = u.shape
+    g = u.reshape(nb[2], nb[1], nb[0], n2, n1, n0, nw).transpose(0, 3, 1, 4, 2, 5, 6)
+    g = g.reshape(nb[2] * n2, nb[1] * n1, nb[0] * n0, nw)
+    zs = [0, g.shape[0] // 2]
+    return np.stack([g[z, ::PLANE_STRIDE, ::PLANE_STRIDE, :] for z in zs])
+
+
 def run_case(name, problem, nb, n, steps, seed, gamma, extra, keep):
     with tempfile.TemporaryDirectory() as tmp:
         prefix = os.path.join(tmp, "snap")
@@ -166,6 +183,8 @@ def run_case(name, problem, nb, n, steps, seed, gamma, extra, keep):
         out["u1"] = u1
         if bf1 is not None:
             out["bf1"] = owned_bf(bf1, n)
+    if keep == "planes":
+        out["u1_planes"] = sampled_planes(u1, nb, n)
     out["u0_sum"], out["u1_sum"] = checksums(u0), checksums(u1)
     if bf0 is not None:
         out["bf0_sum"] = checksums(owned_bf(bf0, n))

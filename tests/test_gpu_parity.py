@@ -74,17 +74,40 @@ def test_fp64_step_matches_reference(name):
             assert e <= TOL_FP64, "bf %d rel L1 %.3e" % (c, e)
 
 
-# Reflecting MHD sides put mirror-image states on the two sides of the wall
-# face, where HLLD's branch choices (contact speed sign, the f_tiny switches)
-# sit at their thresholds; rounding decides them.  Two builds of the oracle
-# that differ only in fused multiply-add already differ by up to 6e-2 relative
-# L1 (face B_z, 4 steps) on this fixture, so the device step -- which fuses --
-# is held to that spread, and to the invariants exactly.
-TOL_ILL_POSED = 1e-1
+def _bf_errors(bf, ref_own, n):
+    """Relative L1 per face-B component over the owned faces, against the L1
+    norm of the whole field (B_z starts at zero in the OT workload)."""
+    own, mask = G.owned_bf(bf, n), G.face_mask(n)
+    den = sum(np.abs(ref_own[..., c][:, mask[..., c]]).sum() for c in range(3))
+    return [np.abs(own[..., c][:, mask[..., c]] - ref_own[..., c][:, mask[..., c]]).sum() / den
+            for c in range(3)]
 
 
 def test_mhd_reflecting_sides():
+    """Reflecting MHD walls put mirror-image states on the two sides of the
+    wall face, where HLLD's branches (the contact-speed sign, the f_tiny
+    switches) sit at their thresholds, so rounding alone moves the result.
+    Measured: the oracle built with fused multiply-add differs from the one
+    without it (the reference's own arithmetic, bit-exact with the fixture) by
+    3.6e-6 relative L1 in density after one step and 2.7e-5 after four, and
+    the device's no-FMA build lands as far away as its fused build (its
+    arithmetic is restructured, so its roundings differ either way).  The
+    device step (FP64) is therefore held, field by field, to 3x the FMA
+    oracle's own distance from the fixture, with mass conserved exactly and
+    div B at roundoff; the same bound with the FMA oracle replaced by the
+    fixture itself is 0, so a kernel error of that size would fail."""
+    from oracle.kr_oracle import OracleMesh
     meta, g = G.load("ot_bc_ref")
+    kinds, w_fix, b_fix = G.boundary(meta)
+    n = meta["n"]
+    o = OracleMesh(True, meta["nb"], n, meta["gamma"], kinds=kinds, w_fix=w_fix, b_fix=b_fix,
+                   variant="fma")
+    o.init_problem("ot", meta["seed"])
+    o.step(meta["steps"])
+    uf, bff = o.get_state()
+    spread_u = G.field_errors(uf, g["u1"])
+    spread_b = _bf_errors(bff, g["bf1"], n)
+    assert max(spread_u) > 1e-8, "rounding must move this case (else hold it to 1e-11)"
     d = _dyn(meta)
     d.init_problem("ot", meta["seed"])
     div0, tot0 = d.diagnostics()
@@ -92,13 +115,10 @@ def test_mhd_reflecting_sides():
     u, bf = d.get_state()
     div1, tot1 = d.diagnostics()
     assert abs(d.time()["t"] - meta["t"]) <= 1e-5 * meta["t"]
-    for k in range(5):
-        assert rel_l1(u[..., k], g["u1"][..., k]) <= TOL_ILL_POSED
-    n, mask = meta["n"], G.face_mask(meta["n"])
-    own = G.owned_bf(bf, n)
-    for c in range(3):
-        m = mask[..., c]
-        assert rel_l1(own[..., c][:, m], g["bf1"][..., c][:, m]) <= TOL_ILL_POSED
+    for k, (e, sp) in enumerate(zip(G.field_errors(u, g["u1"]), spread_u)):
+        assert e <= max(TOL_FP64, 3 * sp), "field %d: %.2e vs FMA spread %.2e" % (k, e, sp)
+    for c, (e, sp) in enumerate(zip(_bf_errors(bf, g["bf1"], n), spread_b)):
+        assert e <= max(TOL_FP64, 3 * sp), "bf %d: %.2e vs FMA spread %.2e" % (c, e, sp)
     assert div1 <= 1e-12
     assert abs(tot1[0] - tot0[0]) <= 1e-12 * abs(tot0[0])    # walls pass no mass
 
