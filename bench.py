@@ -462,18 +462,26 @@ def time_boxes(args, local_rank, sel=None):
     from kratos_b200.boxes import BoxBatch
     out = {"workload": "%d independent periodic MHD boxes (seed 5), edge lengths from {16, 24, 32, 48, 64}, "
                        "random rho, p, velocity amplitude, B orientation and beta, PLM + HLLD + CT, "
-                       "Heun RK2, per-box dt" % args.boxes}
+                       "Heun RK2, per-box dt" % args.boxes,
+           "how": "<mode>: one context and one graph per edge length, each on its own stream; "
+                  "<mode>_batched: one persistent launch per kernel kind over a work list of every box's "
+                  "CTA tiles (kr_batch), one graph per step, CTA counts autotuned first"}
     box_modes = [("fp64", MODES["fp64"]), ("mixed", MODES["mixed"])]
     if sel is not None:
         box_modes.append(("learned", MODES["learned"]))
-    for mode, kw in box_modes:
-        bb = BoxBatch(5, args.boxes, device=local_rank, **kw)
-        if mode == "learned":
+    runs = [(m, kw, False) for m, kw in box_modes] + [(m + "_batched", kw, True) for m, kw in box_modes]
+    for mode, kw, batched in runs:
+        bb = BoxBatch(5, args.boxes, device=local_rank, batched=batched, **kw)
+        if mode.startswith("learned"):
             bb.set_selector(sel[0], sel[1]["threshold"])
         streams = {}
         for n, (d, _) in bb.groups.items():
             streams[n] = torch.cuda.Stream(device=local_rank)
             d.set_stream(streams[n].cuda_stream)
+        tuned = None
+        if batched:
+            with tempfile.TemporaryDirectory() as tmp:
+                tuned, _ = bb.autotune(os.path.join(tmp, "tune.txt"))
         bb.step(args.warmup)
         torch.cuda.synchronize()
         main_s = torch.cuda.Stream(device=local_rank)
@@ -494,9 +502,11 @@ def time_boxes(args, local_rank, sel=None):
             raise RuntimeError("device status %d in the %s box batch" % (bb.status(), mode))
         t, _ = bb.times()
         out[mode] = {"value": bb.n_cells * args.steps / (ms * 1e-3), "unit": UNIT,
-                     "ms_per_step": ms / args.steps,
+                     "ms_per_step": ms / args.steps, "launches_per_step": bb.launches_per_step(),
                      "box_time_range": [float(t.min()), float(t.max())]}
-        if mode == "learned":
+        if tuned is not None:
+            out[mode]["grid"] = tuned
+        if mode.startswith("learned"):
             faces, cheap = bb.selector_stats()
             out[mode]["hlle_fraction"] = cheap / max(faces, 1)
         out["cells"] = bb.n_cells

@@ -262,6 +262,41 @@ const char* kr_learn_last_error( void );
 int kr_c2p_dt_noalloc( const kr_cfg * cfg, const double * u, const double * bf,
                        double * w, double * dt_out, void * stream );
 
+/* ---- Batched launch over blocks of uneven sizes (no reference counterpart as
+ * one launch: the reference runs each box as its own mesh and launches per
+ * block, src/modules/dynamics/dynamics.h:51-103).  A batch joins up to 6
+ * KR_FLAG_BOXES contexts (one per box edge length; same device, precision,
+ * solver, dt_expand and sel_period) so that every kernel kind of the step runs
+ * as one persistent launch over all their blocks: its CTAs walk a work list of
+ * the CTA tiles of every block (bigger blocks first), with the per-group
+ * arguments in the kernel's parameter space, and give the per-context steps'
+ * results bit for bit.  One CUDA graph per step (16 launches; 22 with the
+ * learned selector), on the first context's stream.  The contexts stay owned
+ * by the caller and must outlive the batch; their state, times and selector
+ * calls work as before.
+ *   kr_batch_step       : n_steps Heun steps of every box (enqueued)
+ *   kr_batch_set_grid / kr_batch_get_grid : CTAs of each launch kind (7 kinds:
+ *                         c2p stage 0, c2p stage 1, flux sweeps, the network's
+ *                         sweep, edge EMF, conserved update, face update; 0 =
+ *                         one CTA per work item); returns the kind count
+ *   kr_batch_autotune   : times 1, 2, 4 and 8 waves of resident CTAs and one
+ *                         CTA per item for every kind (two eager steps each,
+ *                         on a copy of the state, restored), keeps each kind's
+ *                         fastest and appends "<key> | c2p0=.. .." to
+ *                         cache_path (the [b200] tune_cache file; NULL: no
+ *                         cache); a line of the same key (device, SM count,
+ *                         precision, solver, sizes and counts) is reused
+ *                         instead.  Returns 1 when cached, 0 when tuned. */
+typedef struct kr_batch kr_batch;
+kr_batch *  kr_batch_create           ( kr_ctx * const * ctxs, int n );
+void        kr_batch_destroy          ( kr_batch * batch );
+const char* kr_batch_last_error       ( const kr_batch * batch );
+int         kr_batch_step             ( kr_batch * batch, int n_steps );
+int         kr_batch_launches_per_step( kr_batch * batch );
+int         kr_batch_get_grid         ( kr_batch * batch, int * grid );
+int         kr_batch_set_grid         ( kr_batch * batch, const int * grid );
+int         kr_batch_autotune         ( kr_batch * batch, const char * cache_path, int * grid_out );
+
 /* ---- Sharding over ranks: one context per GPU.
  * The reference distributes blocks over MPI ranks (mesh/meshgen/meshgen.cpp:
  * 166-247), fills ghosts from other ranks' blocks through MPI messages

@@ -95,6 +95,14 @@ SIGNATURES = {
     "kr_comm_unique_id": (ctypes.c_int, [_vp]),
     "kr_comm_init": (ctypes.c_int, [_vp, _vp]),
     "kr_group_step": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
+    "kr_batch_create": (_vp, [_vp, ctypes.c_int]),
+    "kr_batch_destroy": (None, [_vp]),
+    "kr_batch_last_error": (ctypes.c_char_p, [_vp]),
+    "kr_batch_step": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "kr_batch_launches_per_step": (ctypes.c_int, [_vp]),
+    "kr_batch_get_grid": (ctypes.c_int, [_vp, _vp]),
+    "kr_batch_set_grid": (ctypes.c_int, [_vp, _vp]),
+    "kr_batch_autotune": (ctypes.c_int, [_vp, ctypes.c_char_p, _vp]),
 }
 
 _lib = None

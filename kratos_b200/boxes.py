@@ -18,6 +18,10 @@ from . import _lib as L
 from .engine import Dynamics, KratosError
 
 
+# launch kinds of the batched step, in kr_batch_get_grid's order
+BATCH_KINDS = ("c2p0", "c2p1", "flux", "eval", "emf", "upd1", "upd2")
+
+
 def box_params(seed, box, gamma=5 / 3):
     """Parameters of box `box` of the batch `seed`."""
     out = (ctypes.c_double * 8)()
@@ -32,9 +36,11 @@ class BoxBatch:
 
     Keyword arguments go to each group's Dynamics (precision, riemann, cfl,
     device, ...).  `groups` maps an edge length to (Dynamics, box indices in
-    block order)."""
+    block order).  batched=True steps all groups through one kr_batch: one
+    launch per kernel kind over every box (a work list of the groups' CTA
+    tiles), one CUDA graph per step on the first group's stream."""
 
-    def __init__(self, seed, n_boxes, gamma=5 / 3, **kw):
+    def __init__(self, seed, n_boxes, gamma=5 / 3, batched=False, **kw):
         if n_boxes < 1:
             raise ValueError("need at least one box")
         self.seed, self.n_boxes, self.gamma = int(seed), int(n_boxes), float(gamma)
@@ -51,6 +57,12 @@ class BoxBatch:
                 for k, b in enumerate(ids):
                     self.where[int(b)] = (n, k)
                 d.init_boxes(seed, ids)
+            self._batch = None
+            if batched:
+                hs = (ctypes.c_void_p * len(self.groups))(*[d._h for d, _ in self.groups.values()])
+                self._batch = L.lib().kr_batch_create(hs, len(self.groups))
+                if not self._batch:
+                    raise KratosError(L.lib().kr_batch_last_error(None).decode())
         except Exception:
             self.close()
             raise
@@ -59,11 +71,51 @@ class BoxBatch:
     def n_cells(self):
         return int(sum(int(n) ** 3 for n in self.sizes))
 
+    def _bcheck(self, rc, what):
+        if rc < 0:
+            raise KratosError("%s: %s" % (what, L.lib().kr_batch_last_error(self._batch).decode()))
+        return rc
+
     def step(self, n_steps=1):
         """Advance every box n_steps of its own dt (enqueued on each group's
-        stream; get_state / times wait for them)."""
+        stream, or on the first group's with batched=True; get_state / times
+        wait for them)."""
+        if self._batch:
+            self._bcheck(L.lib().kr_batch_step(self._batch, int(n_steps)), "kr_batch_step")
+            return
         for d, _ in self.groups.values():
             d.step(n_steps)
+
+    @property
+    def stream_groups(self):
+        """The groups whose streams carry the work: all of them, or the first
+        with batched=True."""
+        g = list(self.groups.values())
+        return g[:1] if self._batch else g
+
+    def launches_per_step(self):
+        if self._batch:
+            return L.lib().kr_batch_launches_per_step(self._batch)
+        return sum(d.launches_per_step() for d, _ in self.groups.values())
+
+    def grid(self):
+        """CTAs of each launch kind of the batched step (0: one per work item)."""
+        g = (ctypes.c_int * 7)()
+        self._bcheck(L.lib().kr_batch_get_grid(self._batch, g), "kr_batch_get_grid")
+        return dict(zip(BATCH_KINDS, list(g)))
+
+    def set_grid(self, grid):
+        g = (ctypes.c_int * 7)(*[int(grid[k]) for k in BATCH_KINDS])
+        self._bcheck(L.lib().kr_batch_set_grid(self._batch, g), "kr_batch_set_grid")
+
+    def autotune(self, cache_path=None):
+        """Pick each launch kind's CTA count by timing (kr_batch_autotune), or
+        reuse the choice cached in `cache_path` for this device and batch.
+        Returns (grid, cached)."""
+        g = (ctypes.c_int * 7)()
+        rc = self._bcheck(L.lib().kr_batch_autotune(self._batch, cache_path.encode() if cache_path else None, g),
+                          "kr_batch_autotune")
+        return dict(zip(BATCH_KINDS, list(g))), rc == 1
 
     def set_selector(self, params, threshold):
         """Learned mode (riemann = KR_RIEMANN_LEARNED): the same network and
@@ -107,6 +159,9 @@ class BoxBatch:
         return out
 
     def close(self):
+        if getattr(self, "_batch", None):
+            L.lib().kr_batch_destroy(self._batch)
+            self._batch = None
         for d, _ in self.groups.values():
             d.close()
         self.groups = {}

@@ -17,7 +17,8 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 LIB = os.path.join(PKG, "libkrb200.so")
 SOURCES = [os.path.join(PKG, "csrc", f) for f in ("kr_core.cu", "kr_learn.cu")]
-DEPS = SOURCES + [os.path.join(PKG, "csrc", f) for f in ("kr_math.cuh", "kr_fast.cuh", "kr_mlp.cuh", "problems.h")] + [
+DEPS = SOURCES + [os.path.join(PKG, "csrc", f) for f in ("kr_math.cuh", "kr_fast.cuh", "kr_mlp.cuh", "problems.h",
+                                                         "smr_tree.h", "kr_batch.cuh")] + [
     os.path.join(ROOT, "include", "kratos_b200.h")]
 
 HOST = os.path.join(PKG, "host")

@@ -189,20 +189,18 @@ __global__ void k_step_end( scal_t * s, double dt_expand, int ns )
 
 // DT: stage 0's launch, which also reduces the CFL dt; stage 1's launch has none
 // of that code (fewer registers).
-template< bool MHD, class R, bool DT >
-__global__ void __launch_bounds__( 256, ( MHD && DT ) ? 3 : 4 ) k_c2p( const args_t< R > a, int step, udiv_t dv )
+// One CTA's cells: block b, z plane i2, cell c of the (x, y) plane (every
+// thread of the CTA calls it: the dt reduction is CTA-wide).
+template< bool MHD, class R, bool DT > __device__ __forceinline__
+void c2p_cells( const args_t< R > & a, int step, udiv_t dv, int b, int i2, unsigned c )
 {
-    // grid: x over the cells of one (x, y) plane, y over z, z over blocks
     constexpr int NW = MHD ? 11 : 5;   // stored W words: prim (8) + cell E (3)
-    const int b = blockIdx.z;
-    const unsigned c = blockIdx.x * blockDim.x + threadIdx.x;
     double dt = FLT_MAX;
     if( c < unsigned( a.n0 * a.n1 ) )
     {
         const unsigned q = udiv_q( c, dv );
         const int i0 = int( c - q * unsigned( a.n0 ) );
         const int i1 = int( q );
-        const int i2 = int( blockIdx.y );
         double * U = a.u[ step ];
         double cons[ 5 ], cout[ 5 ], prim[ 5 ];
         for( int k = 0; k < 5; ++ k )
@@ -332,6 +330,13 @@ __global__ void __launch_bounds__( 256, ( MHD && DT ) ? 3 : 4 ) k_c2p( const arg
                 atomicMin( & a.s[ a.boxes ? b : 0 ].dt_bits, ( unsigned long long ) __double_as_longlong( dt ) );
         }
     }
+}
+
+template< bool MHD, class R, bool DT >
+__global__ void __launch_bounds__( 256, ( MHD && DT ) ? 3 : 4 ) k_c2p( const args_t< R > a, int step, udiv_t dv )
+{
+    // grid: x over the cells of one (x, y) plane, y over z, z over blocks
+    c2p_cells< MHD, R, DT >( a, step, dv, blockIdx.z, blockIdx.y, blockIdx.x * blockDim.x + threadIdx.x );
 }
 
 ////////////////////////////////////////////////////////////
@@ -1016,12 +1021,11 @@ void plm_stencil( const args_t< R > & a, int b, int axis, int step, const int * 
 // plane, by = z plane, blockIdx.z = block; dv
 // divides by the row length.
 template< bool MHD, class R, int MODE > __device__ __forceinline__
-void flux_faces( const args_t< R > & a, int axis, int step, udiv_t dv, unsigned bx, unsigned by,
+void flux_faces( const args_t< R > & a, int axis, int step, udiv_t dv, int b, unsigned bx, unsigned by,
                  bool hlle_warp = false )
 {
     constexpr int NW = MHD ? 11 : 5;   // stored W words: prim (8) + cell E (3)
     constexpr bool learned = MHD && MODE == KR_RIEMANN_LEARNED;
-    const int b = blockIdx.z;
     const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
     const unsigned t = bx * blockDim.x + threadIdx.x;
     int ii[ 3 ];
@@ -1086,7 +1090,7 @@ __global__ void __launch_bounds__( 128, ( flux_min_ctas< R, MODE >(  ) ) ) k_flu
                                  + ( blockIdx.y * gridDim.x + blockIdx.x ) * 4u + ( threadIdx.x >> 5 ) ]
                       >> ( threadIdx.x & 31 ) ) & 1u;
     }
-    flux_faces< MHD, R, MODE >( a, axis, step, dv, blockIdx.x, blockIdx.y, hlle_warp );
+    flux_faces< MHD, R, MODE >( a, axis, step, dv, blockIdx.z, blockIdx.x, blockIdx.y, hlle_warp );
 }
 
 // Learned mode, the network's sweep: a fixed grid strides over the 128-face
@@ -1100,7 +1104,7 @@ k_flux_eval( const args_t< R > a, int axis, int step, udiv_t dv, unsigned cpp, u
     if( step != 0 || ! sel_eval_step( a.s, a.sel_period ) )
         return;
     for( unsigned ch = blockIdx.x; ch < cpp * nz; ch += gridDim.x )
-        flux_faces< MHD, R, KR_RIEMANN_LEARNED >( a, axis, step, dv, ch % cpp, ch / cpp );
+        flux_faces< MHD, R, KR_RIEMANN_LEARNED >( a, axis, step, dv, blockIdx.z, ch % cpp, ch / cpp );
 }
 
 ////////////////////////////////////////////////////////////
@@ -1120,17 +1124,15 @@ R face_emf( const args_t< R > & a, int b, int fa, int ax, const int * i )
     return a.f[ fa ][ ifx( a, b, slot, 7, i[ 0 ], i[ 1 ], i[ 2 ] ) ];
 }
 
-template< class R >
-__global__ void __launch_bounds__( 256 ) k_emf( const args_t< R > a, udiv_t dv )
+// Edge site t of the (x, y) plane i2 of block b.
+template< class R > __device__ __forceinline__
+void emf_site( const args_t< R > & a, udiv_t dv, int b, int i2, unsigned t )
 {
-    // grid: x over the edges of one (x, y) plane, y over z, z over blocks
-    const int b = blockIdx.z;
     const int e0 = a.n0 + 1, e1 = a.n1 + 1;
-    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
     if( t >= unsigned( e0 * e1 ) )
         return;
     const unsigned q = udiv_q( t, dv );
-    int i[ 3 ] = { int( t - q * unsigned( e0 ) ), int( q ), int( blockIdx.y ) };
+    int i[ 3 ] = { int( t - q * unsigned( e0 ) ), int( q ), i2 };
     const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
     const R w_e = R( 0.25f );
     // one base offset per site (cell E in W, the fluxes, the edge EMF); the
@@ -1201,6 +1203,13 @@ __global__ void __launch_bounds__( 256 ) k_emf( const args_t< R > a, udiv_t dv )
     }
 }
 
+template< class R >
+__global__ void __launch_bounds__( 256 ) k_emf( const args_t< R > a, udiv_t dv )
+{
+    // grid: x over the edges of one (x, y) plane, y over z, z over blocks
+    emf_site< R >( a, dv, blockIdx.z, blockIdx.y, blockIdx.x * blockDim.x + threadIdx.x );
+}
+
 ////////////////////////////////////////////////////////////
 // Conserved update (hydro/integrator/integrator.h:241-265 add_flux with
 // hydro/integrator/rk2.h:20-34 load) and CT face update
@@ -1258,18 +1267,16 @@ void smr_correct5( const args_t< R > & a, const geo_t & g, int b, const int * i,
 
 // PART 0: cells and faces in one launch; 1: the conserved update only; 2: the
 // CT face update only (MHD: two launches, each with fewer registers).
-template< bool MHD, class R, bool SMR = false, int PART = 0 >
-__global__ void __launch_bounds__( 256, ( SMR && sizeof( R ) == 4 ) ? 3 : ( PART == 2 ? 6 : 4 ) ) k_update( const args_t< R > a, int step, udiv_t dv )
+// Lattice site t of the (x, y) plane i2 of block b.
+template< bool MHD, class R, bool SMR, int PART > __device__ __forceinline__
+void update_site( const args_t< R > & a, int step, udiv_t dv, int b, int i2, unsigned t )
 {
-    // grid: x over the lattice sites of one (x, y) plane, y over z, z over blocks
     constexpr int NF = MHD ? 7 : 5;
-    const int b = blockIdx.z;
     const int e0 = a.n0 + 1, e1 = a.n1 + 1;
-    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
     if( t >= unsigned( e0 * e1 ) )
         return;
     const unsigned q = udiv_q( t, dv );
-    int i[ 3 ] = { int( t - q * unsigned( e0 ) ), int( q ), int( blockIdx.y ) };
+    int i[ 3 ] = { int( t - q * unsigned( e0 ) ), int( q ), i2 };
     const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
     const double dt = __longlong_as_double( a.s[ a.boxes ? b : 0 ].dt_bits ) * ( step == 0 ? 1.0 : double( 0.5f ) );
     const geo_t & g = a.geo[ b ];
@@ -1402,8 +1409,12 @@ __global__ void __launch_bounds__( 256, ( SMR && sizeof( R ) == 4 ) ? 3 : ( PART
     }
 }
 
-////////////////////////////////////////////////////////////
-// Host layout <-> device layout (per-block AoS as in the snapshot).
+template< bool MHD, class R, bool SMR = false, int PART = 0 >
+__global__ void __launch_bounds__( 256, ( SMR && sizeof( R ) == 4 ) ? 3 : ( PART == 2 ? 6 : 4 ) ) k_update( const args_t< R > a, int step, udiv_t dv )
+{
+    // grid: x over the lattice sites of one (x, y) plane, y over z, z over blocks
+    update_site< MHD, R, SMR, PART >( a, step, dv, blockIdx.z, blockIdx.y, blockIdx.x * blockDim.x + threadIdx.x );
+}
 
 template< bool MHD, class R >
 __global__ void k_scatter( const args_t< R > a, const double * hu, const double * hbf )
@@ -3480,3 +3491,4 @@ extern "C" int kr_c2p_dt_noalloc( const kr_cfg * cfg, const double * u, const do
             dx[ 0 ], dx[ 1 ], dx[ 2 ] );
     return ck( nullptr, cudaGetLastError(  ), "kr_c2p_dt_noalloc launch" ) ? 0 : -1;
 }
+#include "kr_batch.cuh"

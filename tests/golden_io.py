@@ -6,7 +6,7 @@ import numpy as np
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 CASES = ["shock_16", "ot_16", "ot_ragged", "shock_floor", "shock_c1", "ot_64",
-         "shock_bc", "shock_fixd", "ot_bc_out", "ot_bc_ref", "ot_bc_fre",
+         "shock_bc", "shock_fixd", "ot_bc_out", "ot_bc_ref", "ot_bc_fre", "ot_bc_fix", "ot_bc_fix0",
          "smr_shock", "smr_bc", "smr_3lvl", "turb_16", "turb_32", "box_5", "box_1", "box_3"]
 # MHD workloads
 MHD_WORKLOADS = ("ot", "turb", "box")
@@ -17,10 +17,6 @@ BOX_CASES = {"box_5": 5, "box_1": 1, "box_3": 3}
 MHD_SMR_CASES = ["smr_ot"]
 # statically refined fixtures (blocks in tree order, with level / reg arrays)
 SMR_CASES = ["smr_shock", "smr_bc", "smr_3lvl"]
-# fixtures compared within a tolerance, not bit for bit: name -> relative L1
-# bound per conserved field.  ot_bc_fix: the reference's MHD fixed sides give
-# results that vary between identical runs (relative L1 ~1.1e-3 after 4 steps)
-SPREAD_CASES = {"ot_bc_fix": 1e-2}
 
 
 def boundary(meta):

@@ -90,3 +90,68 @@ def test_mixed_batch_error_bound(fp64_batch):
         div, _ = d.diagnostics()
         assert div <= 1e-12
     mb.close()
+
+
+@pytest.mark.parametrize("kw", [dict(precision=2), dict(precision=1),
+                                dict(precision=1, riemann=2, sel_period=2)])
+def test_batched_launch_matches_per_group_launches(kw):
+    """One launch per kernel kind over the work list of every group's CTA
+    tiles (kr_batch) runs the per-group launches' tiles with the same code:
+    the boxes' states, times and dt are identical bit for bit, in FP64, mixed
+    and the learned mode (network every 2nd step), with the default grid, one
+    CTA per item, and a grid of one wave."""
+    from kratos_b200.boxes import BoxBatch
+    from kratos_b200 import selector as S
+    w = S.init_params(5) if kw.get("riemann") == 2 else None
+    ref = BoxBatch(5, 24, **kw)
+    if w is not None:
+        ref.set_selector(w, -1.0)
+    ref.step(4)
+    st_ref = ref.states()
+    t_ref, dl_ref = ref.times()
+    for grid in (None, 0, 1):
+        bb = BoxBatch(5, 24, batched=True, **kw)
+        assert bb.launches_per_step() == (22 if w is not None else 16)
+        if grid is not None:
+            g = bb.grid()
+            bb.set_grid({k: (0 if grid == 0 else 148) for k in g})
+        if w is not None:
+            bb.set_selector(w, -1.0)
+        bb.step(4)
+        assert bb.status() == 0
+        st = bb.states()
+        t, dl = bb.times()
+        assert np.array_equal(t, t_ref) and np.array_equal(dl, dl_ref)
+        for b in st_ref:
+            assert np.array_equal(st[b][0], st_ref[b][0]), b
+            assert np.array_equal(st[b][1], st_ref[b][1]), b
+        if w is not None:
+            assert bb.selector_stats() == ref.selector_stats()
+        bb.close()
+    ref.close()
+
+
+def test_batch_autotune_caches_and_keeps_state(tmp_path):
+    """Autotuning times candidate grids on a copy of the state: the boxes'
+    state and times are unchanged by it; the choice is appended to the cache
+    file under the batch's key and read back by the next call."""
+    from kratos_b200.boxes import BATCH_KINDS, BoxBatch
+    cache = str(tmp_path / "tune.txt")
+    bb = BoxBatch(5, 16, batched=True, precision=1)
+    bb.step(2)
+    before = bb.states()
+    t0, _ = bb.times()
+    grid, cached = bb.autotune(cache)
+    assert not cached and set(grid) == set(BATCH_KINDS)
+    after = bb.states()
+    t1, _ = bb.times()
+    assert np.array_equal(t0, t1)
+    for b in before:
+        assert np.array_equal(before[b][0], after[b][0])
+    text = open(cache).read()
+    assert text.count("kr_batch v1") == 1 and "prec1" in text
+    grid2, cached2 = bb.autotune(cache)
+    assert cached2 and grid2 == grid
+    bb.step(2)
+    assert bb.status() == 0
+    bb.close()

@@ -51,7 +51,8 @@ def test_initial_state_bit_exact(name):
 
 
 @pytest.mark.parametrize("name", ["shock_16", "ot_16", "ot_ragged", "shock_floor",
-                                  "shock_bc", "shock_fixd", "ot_bc_out", "ot_bc_fre", "turb_16"])
+                                  "shock_bc", "shock_fixd", "ot_bc_out", "ot_bc_fre", "ot_bc_fix",
+                                  "turb_16"])
 def test_fp64_step_matches_reference(name):
     meta, g = G.load(name)
     d = _dyn(meta)
@@ -123,35 +124,30 @@ def test_mhd_reflecting_sides():
     assert abs(tot1[0] - tot0[0]) <= 1e-12 * abs(tot0[0])    # walls pass no mass
 
 
-def test_mhd_fixed_sides_against_oracle_and_reference():
-    """Fixed MHD sides: the reference's own result varies run to run, so the
-    device step is held to the oracle and to the reference fixture within that
-    spread.  Against the oracle the step stays at rounding level except where
-    an HLLD switch (f_tiny) at the wall face flips under the device's
-    rounding (seen from the first step on this fixture).  Vector fields are
-    measured against the scale of the whole vector (m_z and B_z start near
-    zero in this workload)."""
-    from oracle.kr_oracle import OracleMesh
-    meta, g = G.load("ot_bc_fix")
+def test_mhd_static_fixed_sides():
+    """Fixed MHD sides holding a static medium (vel0 = 0, ot_bc_fix0): the
+    fluxes on the ghost lines between identical static ghost states carry a
+    mass flux that is rounding residue, and the edge EMF's upwind switch
+    (mhd/integrator/integrator.h:268-300) takes its branch from that residue's
+    sign; the reference's residues are -1.4e-17, 2.1e-17 and 0 along x, y, z on
+    this state (tests/test_oracle_golden.py), the device's restructured HLLD
+    leaves others.  With an inflowing medium the same sides match the
+    reference to 1e-11 (ot_bc_fix, above); here the device step is held to
+    1e-4 relative L1 per conserved field and 1e-3 on face B (measured 1e-5
+    and 4e-4 after the 4 steps), with mass conservation and div B exact."""
+    meta, g = G.load("ot_bc_fix0")
     d = _dyn(meta)
     d.init_problem("ot", meta["seed"])
+    div0, _ = d.diagnostics()
     d.step(meta["steps"])
     u, bf = d.get_state()
-    kinds, w_fix, b_fix = G.boundary(meta)
-    o = OracleMesh(True, meta["nb"], meta["n"], meta["gamma"], kinds=kinds, w_fix=w_fix, b_fix=b_fix)
-    o.init_problem("ot", meta["seed"])
-    o.step(meta["steps"])
-    uo, bfo = o.get_state()
-    n, mask = meta["n"], G.face_mask(meta["n"])
-
-    def err(a, b, ks):
-        return max(np.abs(a[..., k] - b[..., k]).sum() for k in ks) / max(np.abs(b[..., k]).sum() for k in ks)
-    for ks in ((0,), (1,), (2, 3, 4)):
-        assert err(u, uo, ks) <= 1e-4, ks
-        assert err(u, g["u1"], ks) <= G.SPREAD_CASES["ot_bc_fix"], ks
-    own, owo = G.owned_bf(bf, n) * mask, G.owned_bf(bfo, n) * mask
-    assert err(own, owo, (0, 1, 2)) <= 1e-3         # measured 3.7e-4: the flip sits at the wall
-    assert err(own, g["bf1"] * mask, (0, 1, 2)) <= G.SPREAD_CASES["ot_bc_fix"]
+    div1, _ = d.diagnostics()
+    assert d.status() == 0
+    for k, e in enumerate(G.field_errors(u, g["u1"])):
+        assert e <= 1e-4, "field %d: %.2e" % (k, e)
+    for c, e in enumerate(_bf_errors(bf, g["bf1"], meta["n"])):
+        assert e <= 1e-3, "bf %d: %.2e" % (c, e)
+    assert div1 <= 1e-12
 
 
 @pytest.mark.parametrize("name", ["shock_c1", "ot_64", "turb_32"])
@@ -172,6 +168,38 @@ def test_fp64_full_size_checksums(name):
     scale = ref[1]
     assert np.all(np.abs(s[0] - ref[0]) <= TOL_FP64 * scale)
     assert abs(d.time()["t"] - meta["t"]) <= 1e-12 * meta["t"]
+
+
+def test_fp64_headline_mesh_against_reference():
+    """The headline MHD configuration at its full size -- 256^3 Orszag-Tang,
+    64 blocks of 64^3, seed 2, 50 steps -- against the reference's own CPU run
+    of the same mesh (ot_256: per-field checksums and two sampled z-planes of
+    the final state).  FP64 step, 1e-10 relative (50 steps of fused rounding
+    through HLLD's branch switches), time to 1e-12."""
+    import sys
+    import os
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    from make_golden import sampled_planes
+    meta, g = G.load("ot_256")
+    d = _dyn(meta)
+    d.init_problem(meta["workload"], meta["seed"])
+    u0, _ = d.get_state()
+    assert np.array_equal(G.checksums(u0[..., :5]), g["u0_sum"][:, :5])
+    d.step(meta["steps"])
+    u, bf = d.get_state()
+    assert d.status() == 0
+    s = G.checksums(u[..., :5])
+    ref = g["u1_sum"][:, :5]
+    np.testing.assert_allclose(s[1:], ref[1:], rtol=TOL_FP64_LONG, atol=0)
+    assert np.all(np.abs(s[0] - ref[0]) <= TOL_FP64_LONG * ref[1])
+    planes = sampled_planes(u, meta["nb"], meta["n"])
+    for k, e in enumerate(G.field_errors(planes[..., :5], g["u1_planes"][..., :5])):
+        assert e <= TOL_FP64_LONG, "plane field %d rel L1 %.2e" % (k, e)
+    n = meta["n"]
+    sb = G.checksums(G.owned_bf(bf, n))
+    np.testing.assert_allclose(sb[1:], g["bf1_sum"][1:], rtol=TOL_FP64_LONG, atol=0)
+    assert abs(d.time()["t"] - meta["t"]) <= 1e-12 * meta["t"]
+    assert abs(d.time()["dt_last"] - meta["dt"]) <= 1e-12 * meta["dt"]
 
 
 def test_fp64_against_oracle_c1_shape():

@@ -114,18 +114,19 @@ def test_hlld_consistency():
         np.testing.assert_allclose(f[7], ez, rtol=1e-12, atol=1e-13)
 
 
-@pytest.mark.parametrize("name", sorted(G.SPREAD_CASES))
-def test_step_within_reference_spread(name):
-    """Cases where the reference itself is not reproducible run to run."""
-    meta, g = G.load(name)
-    m = _mesh(meta)
-    m.init_problem(meta["workload"], meta["seed"])
-    m.step(meta["steps"])
-    u, _ = m.get_state()
-    assert abs(m.t - meta["t"]) <= 1e-6 * meta["t"]
-    for k in range(u.shape[-1]):
-        e = np.abs(u[..., k] - g["u1"][..., k]).sum() / np.abs(g["u1"][..., k]).sum()
-        assert e <= G.SPREAD_CASES[name], (k, e)
+def test_static_fixed_sides_decide_a_switch_by_rounding():
+    """ot_bc_fix0: between the identical, static (v = 0) ghost states of a
+    fixed MHD side, the HLLD mass flux is rounding residue, of either sign
+    (mhd/riemann/hlld.h:81-298), and the edge EMF's upwind switch reads that
+    sign (mhd/integrator/integrator.h:268-300).  The restatement reproduces the
+    reference's arithmetic and hence its residues (bit-exact above); this pins
+    the residues' signs, which the device step is held against within a
+    tolerance (tests/test_gpu_parity.py)."""
+    from oracle import kr_oracle as K
+    w = np.array([0.2, 0.15, 0, 0, 0, 0.1, 0.05, 0.2])
+    f = [K.hlld(w, w, ax, 5 / 3)[0] for ax in range(3)]
+    assert max(abs(x) for x in f) < 1e-15
+    assert f[0] < 0 < f[1] and f[2] == 0
 
 
 @pytest.mark.parametrize("name", G.SMR_CASES)
