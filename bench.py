@@ -55,7 +55,7 @@ def parse():
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--modes", default="fp64,mixed,learned")
+    p.add_argument("--modes", default="fp64,mixed,learned,vl2")
     p.add_argument("--mesh", type=int, default=256, choices=[128, 256],
                    help="global cells per axis (128: profiling-sized sample, 8 blocks of 64^3)")
     p.add_argument("--cpu-baseline", type=int, default=1, help="0: skip the CPU baseline leg")
@@ -63,6 +63,8 @@ def parse():
                    help="batched-box leg: boxes of the seeded batch (0: skip)")
     p.add_argument("--smr", type=int, default=1,
                    help="1: also time the statically refined hydro mesh (1 GPU only)")
+    p.add_argument("--ref-cuda", type=int, default=1,
+                   help="1: also time the reference's own CUDA build (baseline/_ref) on this GPU")
     p.add_argument("--turb", type=int, default=512, choices=[0, 128, 256, 512],
                    help="turbulence leg: global cells per axis (64^3 blocks; 0: skip)")
     args = p.parse_args()
@@ -276,7 +278,9 @@ def reference_arm(args, rank, world):
 MODES = {"fp64": dict(precision=2, riemann=0), "mixed": dict(precision=1, riemann=0),
          "hlle_mixed": dict(precision=1, riemann=1), "learned": dict(precision=1, riemann=2, sel_period=16),
          "learned_p1": dict(precision=1, riemann=2, sel_period=1),
-         "learned_p4": dict(precision=1, riemann=2, sel_period=4)}
+         "learned_p4": dict(precision=1, riemann=2, sel_period=4),
+         "vl2": dict(precision=1, riemann=0, integrator=1),
+         "vl2_fp64": dict(precision=2, riemann=0, integrator=1)}
 
 
 def train_selector(local_rank):
@@ -631,11 +635,11 @@ def main():
     top = max(kernels, key=kernels.get)
     step_gbs = h["value"] / world * BYTES_PER_ZONE_CYCLE / 1e9
     summary = {}
-    for m in ("fp64", "mixed", "learned", "hlle_mixed"):
+    for m in ("fp64", "mixed", "learned", "hlle_mixed", "vl2"):
         if m in results:
             summary[m + "_value"] = results[m]["value"]
     if "fp64" in results:
-        for m in ("mixed", "learned", "hlle_mixed"):
+        for m in ("mixed", "learned", "hlle_mixed", "vl2"):
             if m in results:
                 summary[m + "_over_fp64"] = results[m]["value"] / results["fp64"]["value"]
                 summary[m + "_l1_density_vs_fp64"] = results[m]["l1_density_vs_fp64"]
@@ -678,6 +682,25 @@ def main():
         line["boxes"] = time_boxes(args, local_rank, sel)
     if rank == 0 and world == 1 and args.turb and sel is not None:
         line["turb"] = time_turb(args, local_rank, sel)
+    if rank == 0 and world == 1 and args.ref_cuda:
+        # the GPU bar: the reference's own CUDA path on this GPU, same mesh
+        rc = {}
+        for prec, name in ((2, "fp64"), (1, "mixed")):
+            r = run_reference_cuda(args.steps, prec)
+            if r is not None:
+                rc[name] = r
+        if rc.get("fp64", {}).get("value"):
+            line["reference_cuda_fp64"] = rc["fp64"]["value"]
+            if "fp64" in results:
+                line["fp64_over_reference_cuda_fp64"] = results["fp64"]["value"] / rc["fp64"]["value"]
+            line["value_over_reference_cuda_fp64"] = h["value"] / rc["fp64"]["value"]
+        if rc.get("mixed", {}).get("value"):
+            line["reference_cuda_mixed"] = rc["mixed"]["value"]
+            if "mixed" in results:
+                line["mixed_over_reference_cuda_mixed"] = results["mixed"]["value"] / rc["mixed"]["value"]
+            line["value_over_reference_cuda_mixed"] = h["value"] / rc["mixed"]["value"]
+        if rc:
+            line["reference_cuda"] = rc
     if rank == 0:
         if args.cpu_baseline:
             try:

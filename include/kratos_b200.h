@@ -45,7 +45,7 @@
 extern "C" {
 #endif
 
-#define KR_ABI_VERSION 5
+#define KR_ABI_VERSION 6
 
 /* [boundary] kinds per side (hydro/boundary/phys_functors.h:11-91): an axis is
  * periodic only when both its sides are KR_BC_PER. */
@@ -65,6 +65,17 @@ enum kr_riemann_t
     KR_RIEMANN_HLLE    = 1,    /* two-wave HLLE everywhere (MHD only)            */
     KR_RIEMANN_LEARNED = 2     /* MLP face selector: HLLE where predicted safe,  */
                                /* HLLD elsewhere (MHD only)                      */
+};
+
+/* Time integrator ([b200] integrator). */
+enum kr_integrator_t
+{
+    KR_INTEGRATOR_RK2 = 0,     /* Heun / SSP-RK2, the reference's rk2_t:          */
+                               /*   U* = U + dt L(U), U' = (U + U*) / 2 + dt/2 L(U*) */
+    KR_INTEGRATOR_VL2 = 1      /* van Leer predictor-corrector with CT (Stone &   */
+                               /*   Gardiner 2009, New Astron. 14, 139; no        */
+                               /*   reference counterpart): U* = U + dt/2 L1(U)    */
+                               /*   with donor-cell states, U' = U + dt L(U*)      */
 };
 
 /* Step configuration.  Physics keys mirror the reference's [dynamics] and
@@ -92,7 +103,8 @@ typedef struct
     int    sel_period;         /* learned mode: the network runs at stage 0 of   */
                                /* every sel_period-th step; the other stages    */
                                /* reuse its per-face choices (0 or 1: every step)*/
-    int    reserved[ 3 ];
+    int    integrator;         /* enum kr_integrator_t                           */
+    int    reserved[ 2 ];
 } kr_cfg;
 
 /* kr_cfg.flags (bit 0, value 1, is reserved and ignored) */
@@ -286,7 +298,11 @@ int kr_c2p_dt_noalloc( const kr_cfg * cfg, const double * u, const double * bf,
  *                         cache_path (the [b200] tune_cache file; NULL: no
  *                         cache); a line of the same key (device, SM count,
  *                         precision, solver, sizes and counts) is reused
- *                         instead.  Returns 1 when cached, 0 when tuned. */
+ *                         instead.  Returns 1 when cached, 0 when tuned.
+ *   kr_batch_profile_step: one step run eagerly with CUDA events around every
+ *                         launch; ms[k] = milliseconds of launch kind k (the
+ *                         grid order above), n_kinds >= 7.  The step advances
+ *                         the state like kr_batch_step. */
 typedef struct kr_batch kr_batch;
 kr_batch *  kr_batch_create           ( kr_ctx * const * ctxs, int n );
 void        kr_batch_destroy          ( kr_batch * batch );
@@ -296,6 +312,7 @@ int         kr_batch_launches_per_step( kr_batch * batch );
 int         kr_batch_get_grid         ( kr_batch * batch, int * grid );
 int         kr_batch_set_grid         ( kr_batch * batch, const int * grid );
 int         kr_batch_autotune         ( kr_batch * batch, const char * cache_path, int * grid_out );
+int         kr_batch_profile_step     ( kr_batch * batch, int n_kinds, double * ms );
 
 /* ---- Sharding over ranks: one context per GPU.
  * The reference distributes blocks over MPI ranks (mesh/meshgen/meshgen.cpp:

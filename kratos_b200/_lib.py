@@ -8,10 +8,11 @@ _PKG = os.path.dirname(os.path.abspath(__file__))
 _VARIANT = os.environ.get("KRATOS_B200_VARIANT", "")
 LIB_PATH = os.path.join(_PKG, "libkrb200%s.so" % ("_" + _VARIANT if _VARIANT else ""))
 
-KR_ABI_VERSION = 5
+KR_ABI_VERSION = 6
 KR_FLAG_HALO_ALL, KR_FLAG_BOXES = 2, 4
 BC_KINDS = {"per": 0, "out": 1, "ref": 2, "fre": 3, "fixd": 4}
 KR_RIEMANN_DEFAULT, KR_RIEMANN_HLLE, KR_RIEMANN_LEARNED = 0, 1, 2
+KR_INTEGRATOR_RK2, KR_INTEGRATOR_VL2 = 0, 1
 
 
 class kr_cfg(ctypes.Structure):
@@ -38,7 +39,8 @@ class kr_cfg(ctypes.Structure):
         ("n_ranks", ctypes.c_int),
         ("rank", ctypes.c_int),
         ("sel_period", ctypes.c_int),
-        ("reserved", ctypes.c_int * 3),
+        ("integrator", ctypes.c_int),
+        ("reserved", ctypes.c_int * 2),
     ]
 
 
@@ -103,6 +105,7 @@ SIGNATURES = {
     "kr_batch_get_grid": (ctypes.c_int, [_vp, _vp]),
     "kr_batch_set_grid": (ctypes.c_int, [_vp, _vp]),
     "kr_batch_autotune": (ctypes.c_int, [_vp, ctypes.c_char_p, _vp]),
+    "kr_batch_profile_step": (ctypes.c_int, [_vp, ctypes.c_int, _vp]),
 }
 
 _lib = None

@@ -108,6 +108,15 @@ class BoxBatch:
         g = (ctypes.c_int * 7)(*[int(grid[k]) for k in BATCH_KINDS])
         self._bcheck(L.lib().kr_batch_set_grid(self._batch, g), "kr_batch_set_grid")
 
+    def profile_step(self):
+        """One step eagerly with CUDA events around every launch: milliseconds
+        per launch kind (batched), or per group and kind (kr_profile_step)."""
+        if self._batch:
+            ms = (ctypes.c_double * 7)()
+            self._bcheck(L.lib().kr_batch_profile_step(self._batch, 7, ms), "kr_batch_profile_step")
+            return dict(zip(BATCH_KINDS, list(ms)))
+        return {n: d.profile_step() for n, (d, _) in self.groups.items()}
+
     def autotune(self, cache_path=None):
         """Pick each launch kind's CTA count by timing (kr_batch_autotune), or
         reuse the choice cached in `cache_path` for this device and batch.

@@ -516,6 +516,21 @@ int kr_batch_launches_per_step( kr_batch * bt )
     return 2 + 2 * ( 1 + flux + 3 );
 }
 
+int kr_batch_profile_step( kr_batch * bt, int n_kinds, double * ms )
+{
+    using namespace kr;
+    if( ! bt || ! ms || n_kinds < BK_N ) return -1;
+    for( kr_ctx * c : bt->ctx )
+        if( bt->riemann == KR_RIEMANN_LEARNED && ! c->sel_ready )
+        {
+            bt->err = "kr_batch_profile_step: learned face selector configured but no weights set";
+            return -1;
+        }
+    cudaSetDevice( bt->ctx[ 0 ]->cfg.device );
+    for( int k = 0; k < BK_N; ++ k ) ms[ k ] = 0;
+    return batch_profile_step( bt, ms ) ? 0 : -1;
+}
+
 int kr_batch_get_grid( kr_batch * bt, int * grid )
 {
     if( ! bt || ! grid ) return -1;

@@ -108,6 +108,7 @@ struct args_t
     double w_fix[ 5 ];
     double b_fix[ 3 ];
     int emf_out;                      // bit a: high side of axis a is out / fre (MHD)
+    int vl2;                          // 1: VL2 integrator (donor-cell predictor)
     double * favg;                    // refined mesh: averaged fine face fluxes,
     int favg_n;                       //   [item][5][favg_n] (FP64 in both precisions)
     scal_t * s;
@@ -984,6 +985,18 @@ void plm_stencil( const args_t< R > & a, int b, int axis, int step, const int * 
 {
     constexpr int NP = MHD ? 8 : 5;
     const int ngw = int( a.ngw );
+    if( a.vl2 && step == 0 )
+    {   // VL2 predictor: piecewise-constant (donor-cell) states
+        for( int k = 0; k < NP; ++ k )
+        {
+            const R * p = wb + k * ngw;
+            ql[ k ] = p[ -st ];
+            qr[ k ] = p[ 0 ];
+        }
+        if constexpr( MHD )
+            ql[ BCC + axis ] = qr[ BCC + axis ] = R( a.bf[ step ][ ibf( a, b, axis, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] );
+        return;
+    }
     if constexpr( sizeof( R ) == 4 )
     {
         constexpr int H = NP / 2;
@@ -1278,7 +1291,10 @@ void update_site( const args_t< R > & a, int step, udiv_t dv, int b, int i2, uns
     const unsigned q = udiv_q( t, dv );
     int i[ 3 ] = { int( t - q * unsigned( e0 ) ), int( q ), i2 };
     const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
-    const double dt = __longlong_as_double( a.s[ a.boxes ? b : 0 ].dt_bits ) * ( step == 0 ? 1.0 : double( 0.5f ) );
+    // Heun: U* = U + dt L(U), U' = (U + U*) / 2 + dt / 2 L(U*); VL2:
+    // U* = U + dt / 2 L1(U), U' = U + dt L(U*)
+    const double dt = __longlong_as_double( a.s[ a.boxes ? b : 0 ].dt_bits )
+                    * ( ( step == 0 ) != bool( a.vl2 ) ? 1.0 : double( 0.5f ) );
     const geo_t & g = a.geo[ b ];
     // The arrays never overlap: restrict lets the loads of later components
     // issue ahead of the stores of earlier ones.
@@ -1303,7 +1319,8 @@ void update_site( const args_t< R > & a, int step, udiv_t dv, int b, int i2, uns
                 }
             double v[ 5 ];
             for( int k = 0; k < 5; ++ k )
-                v[ k ] = step == 0 ? us[ c0 + k * a.nc ] : ( us[ c0 + k * a.nc ] + ut[ c0 + k * a.nc ] ) * 0.5f;
+                v[ k ] = step == 0 ? us[ c0 + k * a.nc ]
+                       : ( a.vl2 ? ut[ c0 + k * a.nc ] : ( us[ c0 + k * a.nc ] + ut[ c0 + k * a.nc ] ) * 0.5f );
             if constexpr( ! SMR )
                 for( int k = 0; k < 5; ++ k )
                 {
@@ -1349,7 +1366,7 @@ void update_site( const args_t< R > & a, int step, udiv_t dv, int b, int i2, uns
             for( int k = 0; k < 5; ++ k )
             {   // FP64 fluxes: one component at a time keeps the registers low
                 const long long c = c0 + k * a.nc;
-                double v = step == 0 ? us[ c ] : ( us[ c ] + ut[ c ] ) * 0.5f;
+                double v = step == 0 ? us[ c ] : ( a.vl2 ? ut[ c ] : ( us[ c ] + ut[ c ] ) * 0.5f );
                 for( int d = 0; d < 3; ++ d )
                 {
                     const double f_a = g.sfc[ d ] * dt_dv;
@@ -1389,7 +1406,7 @@ void update_site( const args_t< R > & a, int step, udiv_t dv, int b, int i2, uns
         // the reference scales by -dt / sfc; -dt * (1 / sfc) differs in rounding only
         db *= -dt * g.isfc[ c ];
         const long long k = ob + ( long long ) c * a.nbf;
-        const double nb = db + ( step == 0 ? bs[ k ] : ( bs[ k ] + bt[ k ] ) / 2 );
+        const double nb = db + ( step == 0 ? bs[ k ] : ( a.vl2 ? bt[ k ] : ( bs[ k ] + bt[ k ] ) / 2 ) );
         bt[ k ] = nb;
         // Same-level face-B ghost strips by push, for the next stage: a face
         // next to a transverse side is a ghost face of the block across it
@@ -1900,6 +1917,7 @@ static args_t< R > make_args( kr_ctx * c )
     for( int k = 0; k < 6; ++ k ) a.bc[ k ] = c->cfg.bc[ k ];
     for( int k = 0; k < 5; ++ k ) a.w_fix[ k ] = c->cfg.w_fix[ k ];
     for( int k = 0; k < 3; ++ k ) a.b_fix[ k ] = c->cfg.b_fix[ k ];
+    a.vl2 = c->cfg.integrator == KR_INTEGRATOR_VL2;
     a.emf_out = 0;
     for( int d = 0; d < 3; ++ d )
         if( c->cfg.bc[ 2 * d + 1 ] == KR_BC_OUT || c->cfg.bc[ 2 * d + 1 ] == KR_BC_FRE )
@@ -2368,6 +2386,11 @@ static kr_ctx * create_ctx( const kr_cfg * cfg, int n_regions, const kr_region *
     if( cfg->riemann != KR_RIEMANN_DEFAULT && ! cfg->mhd )
     {
         g_create_error = "kr_ctx_create: HLLE / learned selection is MHD only";
+        return nullptr;
+    }
+    if( cfg->integrator != KR_INTEGRATOR_RK2 && cfg->integrator != KR_INTEGRATOR_VL2 )
+    {
+        g_create_error = "kr_ctx_create: integrator must be KR_INTEGRATOR_RK2 or KR_INTEGRATOR_VL2";
         return nullptr;
     }
     if( cfg->n_ranks < 0 || cfg->n_ranks > 65536 || ( cfg->n_ranks > 1 && ( cfg->rank < 0 || cfg->rank >= cfg->n_ranks ) ) )

@@ -25,7 +25,7 @@ def make_cfg(mhd, nb, n, gamma=1.66667, cfl=0.3, precision=2, riemann=0,
              x_min=(0, 0, 0), x_max=(1, 1, 1), rho_floor=1e-9, tmp_floor=1e-9,
              dt_init=0.0, dt_expand=2.0, device=0, flags=0,
              kinds=("per",) * 6, w_fix=(0, 0, 0, 0, 0), b_fix=(0, 0, 0), n_ranks=1, rank=0,
-             sel_period=1):
+             sel_period=1, integrator=0):
     """A kr_cfg (include/kratos_b200.h) from keyword arguments."""
     lib = L.lib()
     c = L.kr_cfg()
@@ -40,6 +40,7 @@ def make_cfg(mhd, nb, n, gamma=1.66667, cfl=0.3, precision=2, riemann=0,
     c.flags = int(flags)              # KR_FLAG_HALO_ALL, KR_FLAG_BOXES
     c.n_ranks, c.rank = int(n_ranks), int(rank)
     c.sel_period = int(sel_period)
+    c.integrator = int(integrator)    # KR_INTEGRATOR_RK2 (the reference's), KR_INTEGRATOR_VL2
     for k in range(6):
         c.bc[k] = L.BC_KINDS[kinds[k]]
     for k in range(5):

@@ -279,6 +279,12 @@ void mesh_t::init( const input & args )
     c.mhd = mhd_;
     c.precision = args.get< int >( "b200", "precision", 2 );
     c.riemann = args.get< int >( "b200", "riemann", 0 );
+    {   // [b200] integrator = rk2 (the reference's Heun step) | vl2
+        const std::string itg = args.get< std::string >( "b200", "integrator", "rk2" );
+        if( itg != "rk2" && itg != "vl2" )
+            throw std::runtime_error( "[b200] integrator must be rk2 or vl2, not " + itg );
+        c.integrator = itg == "vl2" ? KR_INTEGRATOR_VL2 : KR_INTEGRATOR_RK2;
+    }
     for( int a = 0; a < 3; ++ a )
     {
         c.nb[ a ] = nb_[ a ];

@@ -33,6 +33,7 @@ class _Cfg(ctypes.Structure):
         ("bc", ctypes.c_int * 6),
         ("w_fix", ctypes.c_double * 5),
         ("b_fix", ctypes.c_double * 3),
+        ("integrator", ctypes.c_int),
     ]
 
 
@@ -109,7 +110,8 @@ class OracleMesh:
 
     def __init__(self, mhd, nb, n, gamma, cfl=0.3, x_min=(0, 0, 0), x_max=(1, 1, 1),
                  d_floor=1e-9, t_floor=1e-9, dt_expand=2.0, dt_init=0.0, n_threads=0,
-                 kinds=("per",) * 6, w_fix=(0, 0, 0, 0, 0), b_fix=(0, 0, 0), regions=(), variant=""):
+                 kinds=("per",) * 6, w_fix=(0, 0, 0, 0, 0), b_fix=(0, 0, 0), regions=(), variant="",
+                 integrator=0):
         c = _Cfg()
         c.mhd = int(mhd)
         for a in range(3):
@@ -117,6 +119,7 @@ class OracleMesh:
             c.x_min[a], c.x_max[a] = float(x_min[a]), float(x_max[a])
         c.gamma, c.cfl, c.d_floor, c.t_floor = float(gamma), float(cfl), float(d_floor), float(t_floor)
         c.dt_expand, c.n_threads = float(dt_expand), int(n_threads)
+        c.integrator = int(integrator)            # 0 Heun RK2, 1 VL2
         for k in range(6):
             c.bc[k] = BC_KINDS[kinds[k]]
         for k in range(5):

@@ -19,6 +19,18 @@
 
 #include "../../kratos_b200/csrc/problems.h"
 
+// Built with -DKR_B200_MODULE (oracle/Makefile.ref, kratos_ref_b200), the same
+// problem generator runs the reference's mesh, cycle and outputs with the
+// dynamics step of the B200 engine (kratos_b200/reference_binding).
+#ifdef KR_B200_MODULE
+#include "../../kratos_b200/reference_binding/b200_dynamics.h"
+using hydro_base_t = kratos_b200::b200_t< dynamics::hydro_t >;
+using mhd_base_t   = kratos_b200::b200_t< dynamics::mhd_t >;
+#else
+using hydro_base_t = dynamics::hydro_t;
+using mhd_base_t   = dynamics::mhd_t;
+#endif
+
 namespace
 {
 int          g_seed = 1;
@@ -33,7 +45,7 @@ uint64_t cell_key( const mesh::block_t & b, const type::idx_t & i )
 }
 }   // namespace
 
-struct shock_hydro_t : dynamics::hydro_t
+struct shock_hydro_t : hydro_base_t
 {
     // hydro_t::enroll_default enrols the block data and boundary keeper only;
     // the default policy set (PLM + HLLC + RK2) is enrolled here, as a hydro
@@ -61,7 +73,7 @@ struct shock_hydro_t : dynamics::hydro_t
     }
 };
 
-struct ot_mhd_t : dynamics::mhd_t
+struct ot_mhd_t : mhd_base_t
 {
     void init_cond( mesh::block::dual_t & d ) override
     {
@@ -98,7 +110,7 @@ struct ot_mhd_t : dynamics::mhd_t
 };
 
 // Decaying supersonic turbulence: uniform B_x, random-phase solenoidal velocity.
-struct turb_mhd_t : dynamics::mhd_t
+struct turb_mhd_t : mhd_base_t
 {
     void init_cond( mesh::block::dual_t & d ) override
     {
@@ -139,7 +151,7 @@ struct turb_mhd_t : dynamics::mhd_t
 // mesh is the box: n_cell_global = n_cell_block = its edge length.
 static int g_box = 0;
 
-struct box_mhd_t : dynamics::mhd_t
+struct box_mhd_t : mhd_base_t
 {
     void init_cond( mesh::block::dual_t & d ) override
     {

@@ -1344,7 +1344,13 @@ static void flux_pencil( kro_mesh * m, int b, int axis, int step, int t1, int t2
                 ii[ axis ] = fc - 2 + s;
                 q4[ s ] = w[ iw( m, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) + k ];
             }
-            plm_face( q4[ 0 ], q4[ 1 ], q4[ 2 ], q4[ 3 ], & ql[ k ], & qr[ k ] );
+            if( m->c.integrator == 1 && step == 0 )
+            {   /* VL2 predictor: piecewise-constant (donor-cell) states */
+                ql[ k ] = q4[ 1 ];
+                qr[ k ] = q4[ 2 ];
+            }
+            else
+                plm_face( q4[ 0 ], q4[ 1 ], q4[ 2 ], q4[ 3 ], & ql[ k ], & qr[ k ] );
         }
         if( m->c.mhd )
             hlld_calc( flx, ql, qr, axis, m->c.gamma );
@@ -1406,7 +1412,8 @@ static void update_block( kro_mesh * m, int b, void * aux )
         const long c = iu( m, i0, i1, i2 );
         double v[ 8 ];
         for( int k = 0; k < nw; ++ k )
-            v[ k ] = step == 0 ? us[ c + k ] : ( us[ c + k ] + ut[ c + k ] ) * 0.5f;
+            v[ k ] = step == 0 ? us[ c + k ]
+                   : ( m->c.integrator == 1 ? ut[ c + k ] : ( us[ c + k ] + ut[ c + k ] ) * 0.5f );
         for( int a = 0; a < 3; ++ a )
         {
             int ii[ 3 ] = { i0, i1, i2 };
@@ -1585,7 +1592,8 @@ static void ct_block( kro_mesh * m, int b, void * aux )
             const double sfc = m->sfc0[ b * 3 + a ];
             db *= ( sfc > 0 ? ( -ca->dt / sfc ) : 0. );
             const long k = ib( m, i[ 0 ], i[ 1 ], i[ 2 ] ) + a;
-            bt[ k ] = db + ( step == 0 ? bs[ k ] : ( bs[ k ] + bt[ k ] ) / 2 );
+            bt[ k ] = db + ( step == 0 ? bs[ k ]
+                           : ( m->c.integrator == 1 ? bt[ k ] : ( bs[ k ] + bt[ k ] ) / 2 ) );
         }
     }
 }
@@ -1631,7 +1639,13 @@ int kro_step( kro_mesh * m, int n_steps, double * t, double * dt_bound, double *
                 par_blocks( m, ghost_block, & ga );
                 par_blocks( m, m->c.mhd ? bc_block_mhd : bc_block, & ga );
             }
-            const double dt = dt_use * ( stage == 0 ? 1.0 : ( double ) 0.5f );
+            /* Heun: U* = U + dt L(U), U' = (U + U*) / 2 + dt / 2 L(U*).
+             * VL2 (van Leer predictor-corrector with CT; Stone & Gardiner 2009,
+             * New Astronomy 14, 139): U* = U + dt / 2 L1(U) with donor-cell
+             * states, U' = U + dt L(U*) with PLM states.  No counterpart in
+             * the reference. */
+            const double dt = m->c.integrator == 1 ? dt_use * ( stage == 0 ? ( double ) 0.5f : 1.0 )
+                                                   : dt_use * ( stage == 0 ? 1.0 : ( double ) 0.5f );
             for( int axis = 2; axis >= 0; -- axis )
             {
                 flux_arg fa = { stage, axis };

@@ -47,6 +47,7 @@ typedef struct
     int    bc[ 6 ];
     double w_fix[ 5 ];       /* [init] rho0, pre0, vel0 for KRO_FIXD            */
     double b_fix[ 3 ];       /* [init] b0 for KRO_FIXD (MHD)                    */
+    int    integrator;       /* 0: Heun RK2 (the reference's rk2_t); 1: VL2     */
 } kro_cfg;
 
 typedef struct kro_mesh kro_mesh;

@@ -140,6 +140,20 @@ def owned_bf(bf, n):
     return bf[:, 2:3 + n[2], 2:3 + n[1], 2:3 + n[0], :].copy()
 
 
+def face_checksums(bf, n):
+    """Checksums [4, 3] of the faces each block owns (component c at 0..n
+    along c and 0..n-1 along the other axes; the rest of the owned box holds
+    ghost slots whose fill is a convention of each code)."""
+    own = owned_bf(bf, n)
+    out = np.zeros((4, 3))
+    for c in range(3):
+        sl = [slice(None), slice(0, n[2]), slice(0, n[1]), slice(0, n[0])]
+        sl[3 - c] = slice(0, n[c] + 1)
+        v = own[tuple(sl) + (c,)].ravel()
+        out[:, c] = [v.sum(), np.abs(v).sum(), v.min(), v.max()]
+    return out
+
+
 PLANE_STRIDE = 8
 
 
@@ -153,15 +167,20 @@ def sampled_planes(u, nb, n):
     return np.stack([g[z, ::PLANE_STRIDE, ::PLANE_STRIDE, :] for z in zs])
 
 
-def run_case(name, problem, nb, n, steps, seed, gamma, extra, keep):
+def run_snapshots(exe, problem, nb, n, steps, seed, gamma, extra, env=None):
+    """Run a Kratos executable on a case; its initial and final snapshots."""
     with tempfile.TemporaryDirectory() as tmp:
         prefix = os.path.join(tmp, "snap")
         par = os.path.join(tmp, "case.par")
         with open(par, "w") as f:
             f.write(par_text(problem, nb, n, steps, seed, gamma, extra, prefix))
-        subprocess.check_call([REF_BIN, par], cwd=tmp, stdout=subprocess.DEVNULL)
-        s0 = Snapshot.read(prefix + "_00000.bin")
-        s1 = Snapshot.read(prefix + "_00001.bin")
+        subprocess.check_call([exe, par], cwd=tmp, stdout=subprocess.DEVNULL,
+                              env=dict(os.environ, **(env or {})))
+        return Snapshot.read(prefix + "_00000.bin"), Snapshot.read(prefix + "_00001.bin")
+
+
+def run_case(name, problem, nb, n, steps, seed, gamma, extra, keep):
+    s0, s1 = run_snapshots(REF_BIN, problem, nb, n, steps, seed, gamma, extra)
     if extra.get("regions"):
         level, reg, u0, bf0 = to_tree_arrays(s0)
         level1, reg1, u1, bf1 = to_tree_arrays(s1)
@@ -192,8 +211,8 @@ def run_case(name, problem, nb, n, steps, seed, gamma, extra, keep):
         out["u1_planes"] = sampled_planes(u1, nb, n)
     out["u0_sum"], out["u1_sum"] = checksums(u0), checksums(u1)
     if bf0 is not None:
-        out["bf0_sum"] = checksums(owned_bf(bf0, n))
-        out["bf1_sum"] = checksums(owned_bf(bf1, n))
+        out["bf0_sum"] = face_checksums(bf0, n)
+        out["bf1_sum"] = face_checksums(bf1, n)
     path = os.path.join(HERE, name + ".npz")
     np.savez_compressed(path, **out)
     print("%-12s t=%.6e  %7.1f kB" % (name, meta["t"], os.path.getsize(path) / 1e3))

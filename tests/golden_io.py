@@ -83,3 +83,16 @@ def face_mask(n):
         sl[2 - c] = slice(0, n[c] + 1)
         m[tuple(sl) + (c,)] = True
     return m
+
+
+def face_checksums(bf, n):
+    """Checksums [4, 3] (sum, sum of |.|, min, max per component) of the faces
+    each block owns, as tests/golden/make_golden.py stores them."""
+    own = owned_bf(bf, n)
+    out = np.zeros((4, 3))
+    for c in range(3):
+        sl = [slice(None), slice(0, n[2]), slice(0, n[1]), slice(0, n[0])]
+        sl[3 - c] = slice(0, n[c] + 1)
+        v = own[tuple(sl) + (c,)].ravel()
+        out[:, c] = [v.sum(), np.abs(v).sum(), v.min(), v.max()]
+    return out

@@ -196,7 +196,7 @@ def test_fp64_headline_mesh_against_reference():
     for k, e in enumerate(G.field_errors(planes[..., :5], g["u1_planes"][..., :5])):
         assert e <= TOL_FP64_LONG, "plane field %d rel L1 %.2e" % (k, e)
     n = meta["n"]
-    sb = G.checksums(G.owned_bf(bf, n))
+    sb = G.face_checksums(bf, n)
     np.testing.assert_allclose(sb[1:], g["bf1_sum"][1:], rtol=TOL_FP64_LONG, atol=0)
     assert abs(d.time()["t"] - meta["t"]) <= 1e-12 * meta["t"]
     assert abs(d.time()["dt_last"] - meta["dt"]) <= 1e-12 * meta["dt"]

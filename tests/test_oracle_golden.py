@@ -170,6 +170,6 @@ def test_refined_mhd_tree_and_initial_state(name):
     G.init(m, meta)
     u, bf = m.get_state()
     assert np.array_equal(G.checksums(u), g["u0_sum"])
-    assert np.array_equal(G.checksums(G.owned_bf(bf, meta["n"])), g["bf0_sum"])
+    assert np.array_equal(G.face_checksums(bf, meta["n"]), g["bf0_sum"])
     with pytest.raises(NotImplementedError):
         m.step(1)
