@@ -295,8 +295,8 @@ int kr_c2p_dt_noalloc( const kr_cfg * cfg, const double * u, const double * bf,
  *                         CTA per item for every kind (two eager steps each,
  *                         on a copy of the state, restored), keeps each kind's
  *                         fastest and appends "<key> | c2p0=.. .." to
- *                         cache_path (the [b200] tune_cache file; NULL: no
- *                         cache); a line of the same key (device, SM count,
+ *                         cache_path (NULL: no cache); a line of the same
+ *                         key (device, SM count,
  *                         precision, solver, sizes and counts) is reused
  *                         instead.  Returns 1 when cached, 0 when tuned.
  *   kr_batch_profile_step: one step run eagerly with CUDA events around every

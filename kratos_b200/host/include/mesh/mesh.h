@@ -59,6 +59,7 @@ private:
     const input * args_ = nullptr;
     bool mhd_ = false;
     int nb_[ 3 ] = { 1, 1, 1 }, n_[ 3 ] = { 1, 1, 1 };
+    bool periodic_[ 3 ] = { true, true, true };
     // cycle
     double t_ = 0, t_lim_ = 3.4e38, dt_output_ = 1e32, t_output_ = 0;
     int n_cycle_lim_ = 0, i_cycle_ = 0, i_output_ = 0, n_display_ = 1;

@@ -10,6 +10,7 @@
 #include <iomanip>
 #include <iostream>
 #include <map>
+#include <set>
 #include <stdexcept>
 
 #include "../../../include/kratos_b200.h"
@@ -67,6 +68,170 @@ void put_str( std::vector< char > & o, const std::string & s )
 {
     put_size( o, s.size(  ) );
     o.insert( o.end(  ), s.begin(  ), s.end(  ) );
+}
+
+// Global block ids in the reference's order: blocks along a Hilbert curve
+// (meshgen.cpp:188-243 dist_fractal) drawn by an L-system turtle
+// (utilities/l_system/l_system.cpp): the 3-D rule below, 'F' one unit step
+// along the turtle's x axis, the other symbols quarter turns composed on the
+// right (+ - about z, & ^ about y, > < about x), kept here as integer rotation
+// matrices; a refined node is replaced by its children in the order of the same
+// curve one level down, placed where that curve's bounding box meets the
+// node's children.  lvl[b], reg[3b..3b+2]: each block's level and position.
+struct hilbert_walk
+{
+    const char * rule = "^<XF^<XFX-F^>>XFX&F+>>XFX-F>X->";
+    std::map< std::array< int, 4 >, int > leaf;      // (level, x) -> block
+    std::set< std::array< int, 4 > > refined;
+    std::vector< int > ids;
+    std::vector< std::array< int, 3 > > nodes;
+    int l_base = 1, lim = 1, next = 0;
+    bool dry = false;
+    struct turtle { int l; int x[ 3 ]; int m[ 3 ][ 3 ]; };
+
+    static void turn( int m[ 3 ][ 3 ], char c )
+    {   // m = m * R, R the quarter turn of c
+        const int axis = ( c == '+' || c == '-' ) ? 2 : ( ( c == '&' || c == '^' ) ? 1 : 0 );
+        const int sgn = ( c == '+' || c == '&' || c == '>' ) ? 1 : -1;
+        const int a1 = ( axis + 1 ) % 3, a2 = ( axis + 2 ) % 3;
+        int r[ 3 ][ 3 ] = { { 0, 0, 0 }, { 0, 0, 0 }, { 0, 0, 0 } };
+        r[ axis ][ axis ] = 1;
+        r[ a2 ][ a1 ] = sgn;
+        r[ a1 ][ a2 ] = -sgn;
+        int o[ 3 ][ 3 ];
+        for( int i = 0; i < 3; ++ i )
+            for( int j = 0; j < 3; ++ j )
+            {
+                o[ i ][ j ] = 0;
+                for( int k = 0; k < 3; ++ k )
+                    o[ i ][ j ] += m[ i ][ k ] * r[ k ][ j ];
+            }
+        std::memcpy( m, o, sizeof( o ) );
+    }
+    bool visit( const turtle & t )
+    {   // true: a refined node, walked one level down instead
+        const std::array< int, 4 > key = { t.l - l_base, t.x[ 0 ], t.x[ 1 ], t.x[ 2 ] };
+        if( refined.count( key ) )
+            return true;
+        const auto it = leaf.find( key );
+        if( it != leaf.end(  ) )
+            ids[ it->second ] = next ++;
+        return false;
+    }
+    void step( turtle & t )
+    {
+        if( t.l >= lim )
+            return node( t );
+        for( const char * c = rule; * c; ++ c )
+            if( * c == 'X' )
+            {
+                ++ t.l;
+                step( t );
+                -- t.l;
+            }
+            else if( * c == 'F' )
+                for( int a = 0; a < 3; ++ a )
+                    t.x[ a ] += t.m[ a ][ 0 ];
+            else
+                turn( t.m, * c );
+    }
+    void node( const turtle & t )
+    {
+        if( dry || ! visit( t ) )
+        {
+            nodes.push_back( { t.x[ 0 ], t.x[ 1 ], t.x[ 2 ] } );
+            return;
+        }
+        const size_t start = nodes.size(  );
+        dry = true;
+        ++ lim;
+        turtle m = t;
+        m.x[ 0 ] = m.x[ 1 ] = m.x[ 2 ] = 0;
+        step( m );
+        int dx[ 3 ] = { 0, 0, 0 };
+        for( size_t k = start; k < nodes.size(  ); ++ k )
+            for( int a = 0; a < 3; ++ a )
+                dx[ a ] = std::min( dx[ a ], nodes[ k ][ a ] );
+        nodes.resize( start );
+        m = t;
+        for( int a = 0; a < 3; ++ a )
+            m.x[ a ] = 2 * t.x[ a ] - dx[ a ];
+        dry = false;
+        step( m );
+        -- lim;
+    }
+};
+
+std::vector< int > hilbert_ids( const std::vector< int > & lvl, const std::vector< int > & reg, const int * nb )
+{
+    hilbert_walk h;
+    const size_t nblk = lvl.size(  );
+    h.ids.assign( nblk, -1 );
+    for( size_t b = 0; b < nblk; ++ b )
+    {
+        int x[ 3 ] = { reg[ 3 * b ], reg[ 3 * b + 1 ], reg[ 3 * b + 2 ] };
+        h.leaf[ { lvl[ b ], x[ 0 ], x[ 1 ], x[ 2 ] } ] = int( b );
+        for( int l = lvl[ b ]; l > 0; -- l )
+        {   // every ancestor is a refined node (region.h:60-66 coarsen)
+            for( int a = 0; a < 3; ++ a )
+                x[ a ] = ( x[ a ] > 0 ? x[ a ] : x[ a ] - 1 ) / 2;
+            h.refined.insert( { l - 1, x[ 0 ], x[ 1 ], x[ 2 ] } );
+        }
+    }
+    int n_base = std::max( nb[ 0 ], std::max( nb[ 1 ], nb[ 2 ] ) ) - 1, l_base = 0;
+    while( n_base >>= 1 )
+        ++ l_base;
+    h.l_base = h.lim = l_base + 1;
+    hilbert_walk::turtle t = { 0, { 0, 0, 0 }, { { 1, 0, 0 }, { 0, 1, 0 }, { 0, 0, 1 } } };
+    h.step( t );
+    for( int id : h.ids )
+        if( id < 0 )
+            throw std::runtime_error( "block numbering: a block off the Hilbert walk" );
+    return h.ids;
+}
+
+// The serialized block tree (mesh/tree/tree.cpp:11-20 write, through
+// utilities/data_transfer/serialize.h): the map of nodes -- refined ones
+// (mask) and leaves with their ids -- in key order (level, then x0, x1, x2),
+// as size_t count and raw (region_logic_t: 3 x int + level; tree_node_t: id_l,
+// id_g, rank, mask + padding) pairs, then n_dim, reg_max and the periodic
+// flags.  A reference restart reads it (meshgen.cpp:96-104).
+snap_entry mesh_tree_blob( const std::vector< mesh::block_t > & blocks, const int * nb,
+                           const bool * periodic )
+{
+    std::map< std::array< int, 4 >, std::array< int, 4 > > nodes;   // key -> id_l, id_g, rank, mask
+    for( const auto & b : blocks )
+    {
+        int x[ 3 ] = { b.reg[ 0 ], b.reg[ 1 ], b.reg[ 2 ] };
+        nodes[ { b.reg.level, x[ 0 ], x[ 1 ], x[ 2 ] } ] = { b.id_g, b.id_g, 0, 0 };
+        for( int l = b.reg.level; l > 0; -- l )
+        {
+            for( int a = 0; a < 3; ++ a )
+                x[ a ] = ( x[ a ] > 0 ? x[ a ] : x[ a ] - 1 ) / 2;
+            nodes[ { l - 1, x[ 0 ], x[ 1 ], x[ 2 ] } ] = { -1, -1, -1, 1 };
+        }
+    }
+    snap_entry e;
+    e.u_size = 1;
+    put_size( e.bytes, nodes.size(  ) );
+    auto put_i = [ & ]( int v )
+    {
+        const char * p = reinterpret_cast< const char * >( & v );
+        e.bytes.insert( e.bytes.end(  ), p, p + 4 );
+    };
+    for( const auto & kv : nodes )
+    {
+        put_i( kv.first[ 1 ] ); put_i( kv.first[ 2 ] ); put_i( kv.first[ 3 ] ); put_i( kv.first[ 0 ] );
+        put_i( kv.second[ 0 ] ); put_i( kv.second[ 1 ] ); put_i( kv.second[ 2 ] );
+        const char tail[ 4 ] = { char( kv.second[ 3 ] ), 0, 0, 0 };
+        e.bytes.insert( e.bytes.end(  ), tail, tail + 4 );
+    }
+    put_i( 3 );
+    for( int a = 0; a < 3; ++ a )
+        put_i( nb[ a ] );
+    for( int a = 0; a < 3; ++ a )
+        e.bytes.push_back( char( periodic[ a ] ? 1 : 0 ) );
+    return e;
 }
 
 // Whole-file snapshot reader: tag -> bytes of its blob.
@@ -303,6 +468,8 @@ void mesh_t::init( const input & args )
     args( "boundary", "kinds", kinds );
     for( int s = 0; s < 6; ++ s )
         c.bc[ s ] = s < int( kinds.size(  ) ) ? bc_kind( kinds[ s ] ) : KR_BC_PER;
+    for( int a = 0; a < 3; ++ a )
+        periodic_[ a ] = c.bc[ 2 * a ] == KR_BC_PER && c.bc[ 2 * a + 1 ] == KR_BC_PER;
     c.w_fix[ 0 ] = args.get< double >( "init", "rho0", 0 );
     c.w_fix[ 1 ] = args.get< double >( "init", "pre0", 0 );
     const auto v0 = args.get< type::coord2_t >( "init", "vel0", 0 );
@@ -338,7 +505,7 @@ void mesh_t::init( const input & args )
     for( int b = 0; b < nblk; ++ b )
     {
         block_t & blk = blocks_[ b ];
-        blk.id_g = blk.id_l = b;
+        blk.id_l = b;
         blk.reg.level = lvl[ b ];
         double vol = 1.;
         for( int a = 0; a < 3; ++ a )
@@ -370,6 +537,13 @@ void mesh_t::init( const input & args )
         if( ! snap->load( args.get< std::string >( "file", "binary" ) ) )
             throw std::runtime_error( "restart: unreadable snapshot" );
     }
+    // Global ids as the reference assigns them (its Hilbert-curve order), so
+    // that snapshots name their blocks as a reference restart looks them up
+    {
+        const std::vector< int > ids = hilbert_ids( lvl, regs, nb_ );
+        for( int b = 0; b < nblk; ++ b )
+            blocks_[ b ].id_g = ids[ b ];
+    }
     // Stored blocks are matched by level and logical position (i_logic): the
     // reference numbers blocks along a Hilbert curve (meshgen.cpp:188-243),
     // this layer level by level, lexicographically.
@@ -400,8 +574,9 @@ void mesh_t::init( const input & args )
                 throw std::runtime_error( "restart: snapshot lacks a block of this mesh" );
     }
     data_.clear(  );
-    for( auto & blk : blocks_ )
+    for( size_t ib = 0; ib < blocks_.size(  ); ++ ib )
     {
+        block_t & blk = blocks_[ ib ];
         std::shared_ptr< block::base_data_t > p;
         if( mhd_ )
         {
@@ -421,7 +596,7 @@ void mesh_t::init( const input & args )
         p->geo = blk.geo;
         if( snap )
         {   // restart: slot 0 of the stored fields (hyd_data.cpp:49-57, fld_data.cpp:87-95)
-            const std::string pre = snap_block[ blk.id_g ];
+            const std::string pre = snap_block[ ib ];
             auto & h = dynamic_cast< dynamics::hydro::block_data_t & >( * p );
             snap->get( pre + "hydro_cons_field", h.hyd.u.dat, h.hyd.u.n_ctot );
             if( mhd_ )
@@ -544,6 +719,7 @@ void mesh_t::save( const std::string & file )
     put( "cycle", & i_cycle_, 1, 4 );
     put( "i_out", & i_output_, 1, 4 );
     put( "t_out", & t_output_, 1, 8 );
+    e[ "mesh_tree" ] = mesh_tree_blob( blocks_, nb_, periodic_ );
     for( size_t b = 0; b < blocks_.size(  ); ++ b )
     {
         const block_t & blk = blocks_[ b ];

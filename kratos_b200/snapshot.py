@@ -134,3 +134,95 @@ def to_tree_arrays(snap: Snapshot):
     if rows and ("block_%d|field_bf_field" % rows[0][1]) in snap.data:
         bf = np.stack([snap.field(bid, "field_bf_")[0] for _, bid in rows])
     return level, reg, u, bf
+
+
+# ---------------------------------------------------------------- block ids
+# The reference numbers blocks along a Hilbert curve (meshgen.cpp:188-243
+# dist_fractal), drawn by an L-system turtle (utilities/l_system/l_system.cpp):
+# the 3-D rule below, 'F' a unit step along the turtle's x axis, the other
+# symbols quarter turns (+ - about z, & ^ about y, > < about x) composed on the
+# right.  A refined node is replaced by its children in the order of the same
+# curve one level down, placed where the curve's bounding box meets the node's
+# children.  Restated here (turns as integer rotation matrices) so that a
+# snapshot names its blocks block_<id> as the reference would on restart.
+_HILBERT_3D = "^<XF^<XFX-F^>>XFX&F+>>XFX-F>X->"
+
+
+def _turn(axis, sgn):
+    m = np.eye(3, dtype=np.int64)
+    a1, a2 = (axis + 1) % 3, (axis + 2) % 3
+    m[a1, a1] = m[a2, a2] = 0
+    m[a2, a1] = sgn
+    m[a1, a2] = -sgn
+    return m
+
+
+_TURNS = {"+": _turn(2, 1), "-": _turn(2, -1), "&": _turn(1, 1), "^": _turn(1, -1),
+          ">": _turn(0, 1), "<": _turn(0, -1)}
+
+
+def hilbert_ids(levels, regs, nb):
+    """Global block ids (the reference's id_g) of the blocks of a 3-D mesh:
+    levels[b], regs[b] (logical position at that level), nb root blocks per
+    axis.  Returns (ids [nblk], tree) with tree the refined (masked) nodes as
+    a set of (level, x0, x1, x2)."""
+    leaves = {(int(l), *map(int, r)): b for b, (l, r) in enumerate(zip(levels, regs))}
+    masked = set()
+    for (l, x0, x1, x2) in leaves:
+        x = [x0, x1, x2]
+        for up in range(l, 0, -1):
+            x = [(v if v > 0 else v - 1) // 2 if v < 0 else v // 2 for v in x]
+            masked.add((up - 1, *x))
+    n_base = max(nb) - 1
+    l_base = 0
+    while n_base > 1:
+        n_base >>= 1
+        l_base += 1
+    l_base += 1 if max(nb) > 1 else 1
+    ids = np.full(len(levels), -1, np.int64)
+    state = {"lim": l_base, "reg": False, "next": 0}
+    nodes = []
+
+    def rule_ref(x, l):
+        key = (l - l_base, *x)
+        if key in masked:
+            return True
+        if key in leaves:
+            ids[leaves[key]] = state["next"]
+            state["next"] += 1
+        return False
+
+    def step(t):
+        if t["l"] >= state["lim"]:
+            refine(t)
+            return
+        for ch in _HILBERT_3D:
+            if ch == "X":
+                t["l"] += 1
+                step(t)
+                t["l"] -= 1
+            elif ch == "F":
+                t["x"] = [t["x"][a] + int(t["m"][a, 0]) for a in range(3)]
+            else:
+                t["m"] = t["m"] @ _TURNS[ch]
+
+    def refine(t):
+        if state["reg"] or not rule_ref(t["x"], t["l"]):
+            nodes.append(list(t["x"]))
+            return
+        start = len(nodes)
+        state["reg"] = True
+        state["lim"] += 1
+        dry = {"l": t["l"], "x": [0, 0, 0], "m": t["m"].copy()}
+        step(dry)
+        dx = [0, 0, 0]
+        for p in nodes[start:]:
+            dx = [min(dx[a], p[a]) for a in range(3)]
+        del nodes[start:]
+        sub = {"l": t["l"], "x": [2 * t["x"][a] - dx[a] for a in range(3)], "m": t["m"].copy()}
+        state["reg"] = False
+        step(sub)
+        state["lim"] -= 1
+
+    step({"l": 0, "x": [0, 0, 0], "m": np.eye(3, dtype=np.int64)})
+    return ids, masked

@@ -29,7 +29,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
-from kratos_b200.snapshot import Snapshot, to_lex_arrays, to_tree_arrays  # noqa: E402
+from kratos_b200.snapshot import Snapshot, block_ids, to_lex_arrays, to_tree_arrays  # noqa: E402
 
 REF_BIN = os.environ.get("KR_REF_BIN", os.path.join(ROOT, "oracle", "_ref", "kratos_ref"))
 
@@ -167,6 +167,20 @@ def sampled_planes(u, nb, n):
     return np.stack([g[z, ::PLANE_STRIDE, ::PLANE_STRIDE, :] for z in zs])
 
 
+def block_ids_in_order(snap, nb, refined):
+    """The reference's global id of each block, in the fixture's block order
+    (lexicographic, or tree order for a refined mesh)."""
+    rows = []
+    for bid in block_ids(snap):
+        lv = int(snap.array("block_%d|level" % bid, "i")[0])
+        il = snap.array("block_%d|i_logic" % bid, "i").astype(int)
+        key = (lv, int(il[2]), int(il[1]), int(il[0])) if refined else \
+            (0, int(il[2]), int(il[1]), int(il[0]))
+        rows.append((key, bid))
+    rows.sort()
+    return np.array([bid for _, bid in rows], np.int64)
+
+
 def run_snapshots(exe, problem, nb, n, steps, seed, gamma, extra, env=None):
     """Run a Kratos executable on a case; its initial and final snapshots."""
     with tempfile.TemporaryDirectory() as tmp:
@@ -199,6 +213,7 @@ def run_case(name, problem, nb, n, steps, seed, gamma, extra, keep):
     out = {"meta": np.array(json.dumps(meta))}
     if extra.get("regions"):
         out["level"], out["reg"] = level, reg
+    out["ids"] = block_ids_in_order(s0, nb, bool(extra.get("regions")))
     if keep == "full":
         out["u0"] = u0
         if bf0 is not None:

@@ -221,3 +221,61 @@ def test_refined_restart_from_reference_snapshot(host_exe, tmp_path):
     d.step(3)
     u, _ = d.get_state()
     assert np.array_equal(u3, u)
+
+
+def test_hilbert_numbering_matches_reference_snapshots():
+    """The block ids the host layer writes follow the reference's Hilbert-curve
+    order (meshgen.cpp:188-243): the Python restatement (kratos_b200.snapshot,
+    the same walk as host.cpp's) against the ids in the reference's own
+    snapshots -- uniform, ragged and refined meshes up to three levels."""
+    from kratos_b200.snapshot import hilbert_ids
+    for name in ["ot_16", "ot_ragged", "smr_shock", "smr_bc", "smr_3lvl", "smr_ot"]:
+        meta, g = G.load(name)
+        if "level" in g:
+            lvl, reg = g["level"], g["reg"]
+        else:
+            nb = meta["nb"]
+            idx = np.arange(nb[0] * nb[1] * nb[2])
+            lvl = np.zeros(len(idx), int)
+            reg = np.stack([idx % nb[0], (idx // nb[0]) % nb[1], idx // (nb[0] * nb[1])], 1)
+        ids, _ = hilbert_ids(lvl, reg, meta["nb"])
+        assert sorted(ids) == list(range(len(ids)))
+        if "ids" in g:
+            assert np.array_equal(ids, g["ids"]), name
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["ot_16", "smr_shock"])
+def test_reference_restarts_from_host_layer_snapshot(host_exe, tmp_path, name):
+    """The snapshot format is a two-way boundary: the host layer writes the
+    serialized block tree (mesh_tree, mesh/tree/tree.cpp:11-20) and names its
+    blocks by the reference's Hilbert ids, so the ORIGINAL Kratos code
+    (oracle/_ref/kratos_ref) restarts from it.  3 steps on the GPU, then the
+    reference continues to the fixture's 5 (its loop repeats the stored cycle,
+    so n_cycle_lim = 3) and matches the reference's own 5-step run to the FP64
+    parity bound; the mesh_tree bytes equal the reference's own."""
+    import make_golden as M
+    from kratos_b200.snapshot import Snapshot, to_lex_arrays, to_tree_arrays
+    ref = os.path.join(ROOT, "oracle", "_ref", "kratos_ref")
+    if not os.path.exists(ref):
+        pytest.fail("%s is not built (make -f oracle/Makefile.ref REF=<kratos tree>)" % ref)
+    c = [x for x in M.CASES if x[0] == name][0]
+    _, problem, nb, n, steps, seed, gamma, extra, _ = c
+    prefix = str(tmp_path / "h")
+    par = tmp_path / "h.par"
+    par.write_text(M.par_text(problem, nb, n, 3, seed, gamma, extra, prefix))
+    subprocess.check_call([host_exe, str(par)], cwd=str(tmp_path), stdout=subprocess.DEVNULL)
+    # the reference's own snapshot of the same mesh, for the tree bytes
+    s_ref, _ = M.run_snapshots(ref, problem, nb, n, 1, seed, gamma, extra)
+    s_host = Snapshot.read(prefix + "_00000.bin")
+    assert s_host.data["mesh_tree"] == s_ref.data["mesh_tree"]
+    over = tmp_path / "more.par"
+    over.write_text("[cycle]\nn_cycle_lim = 3\nprefix_output = %s\n" % str(tmp_path / "r"))
+    subprocess.check_call([ref, prefix + "_00001.bin", str(over)], cwd=str(tmp_path), stdout=subprocess.DEVNULL)
+    s = Snapshot.read(str(tmp_path / "r_00002.bin"))
+    meta, g = G.load(name)
+    assert int(s.array("cycle", "i")[0]) == 3
+    assert abs(float(s.array("time")[0]) - meta["t"]) <= 1e-12 * meta["t"]
+    u = to_tree_arrays(s)[2] if extra.get("regions") else to_lex_arrays(s, nb)[0]
+    for k, e in enumerate(G.field_errors(u[..., :5], g["u1"][..., :5])):
+        assert e <= TOL_FP64, "field %d rel L1 %.3e" % (k, e)
