@@ -1480,30 +1480,58 @@ __global__ void k_gather( const args_t< R > a, double * hu, double * hbf )
 // Diagnostics: max |div B| (owned cells) and domain totals.
 
 template< bool MHD, class R >
-__global__ void k_diag( const args_t< R > a, double * out )
+__global__ void __launch_bounds__( 256 ) k_diag( const args_t< R > a, double * out )
 {
+    // per thread: one cell's contributions; then a CTA reduction and one
+    // atomic per CTA and quantity (not one per cell: the per-cell atomics on
+    // six addresses serialised the whole grid)
     const int b = blockIdx.y;
     const long long t = ( long long ) blockIdx.x * blockDim.x + threadIdx.x;
-    if( t >= a.nc )
-        return;
-    const int i0 = int( t % a.n0 ), i1 = int( ( t / a.n0 ) % a.n1 ), i2 = int( t / ( ( long long ) a.n0 * a.n1 ) );
-    const geo_t & g = a.geo[ b ];
-    for( int k = 0; k < 5; ++ k )
-        atomicAdd( out + 1 + k, a.u[ 0 ][ iuc( a, b, k, i0, i1, i2 ) ] * g.vol );
-    if( MHD )
+    double v[ 5 ] = { 0, 0, 0, 0, 0 }, div = 0;
+    if( t < a.nc )
     {
-        const int ii[ 3 ] = { i0, i1, i2 };
-        double div = 0;
-        for( int d = 0; d < 3; ++ d )
+        const int i0 = int( t % a.n0 ), i1 = int( ( t / a.n0 ) % a.n1 ), i2 = int( t / ( ( long long ) a.n0 * a.n1 ) );
+        const geo_t & g = a.geo[ b ];
+        for( int k = 0; k < 5; ++ k )
+            v[ k ] = a.u[ 0 ][ iuc( a, b, k, i0, i1, i2 ) ] * g.vol;
+        if( MHD )
         {
-            int jj[ 3 ] = { ii[ 0 ], ii[ 1 ], ii[ 2 ] };
-            const double bl = a.bf[ 0 ][ ibf( a, b, d, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) ];
-            ++ jj[ d ];
-            const double br = a.bf[ 0 ][ ibf( a, b, d, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) ];
-            div += ( br - bl ) * g.sfc[ d ];
+            const int ii[ 3 ] = { i0, i1, i2 };
+            for( int d = 0; d < 3; ++ d )
+            {
+                int jj[ 3 ] = { ii[ 0 ], ii[ 1 ], ii[ 2 ] };
+                const double bl = a.bf[ 0 ][ ibf( a, b, d, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) ];
+                ++ jj[ d ];
+                const double br = a.bf[ 0 ][ ibf( a, b, d, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) ];
+                div += ( br - bl ) * g.sfc[ d ];
+            }
+            div = fabs( div ) / g.vol;
         }
-        div = fabs( div ) / g.vol;
-        atomicMax( ( unsigned long long * ) out, ( unsigned long long ) __double_as_longlong( div ) );
+    }
+    __shared__ double red[ 6 ][ 8 ];
+    for( int o = 16; o > 0; o >>= 1 )
+    {
+        for( int k = 0; k < 5; ++ k )
+            v[ k ] += __shfl_xor_sync( 0xffffffffu, v[ k ], o );
+        div = fmax( div, __shfl_xor_sync( 0xffffffffu, div, o ) );
+    }
+    const int w = threadIdx.x >> 5;
+    if( ( threadIdx.x & 31 ) == 0 )
+    {
+        for( int k = 0; k < 5; ++ k )
+            red[ k ][ w ] = v[ k ];
+        red[ 5 ][ w ] = div;
+    }
+    __syncthreads(  );
+    if( threadIdx.x < 6 )
+    {
+        double r = red[ threadIdx.x ][ 0 ];
+        for( int k = 1; k < int( blockDim.x >> 5 ); ++ k )
+            r = threadIdx.x < 5 ? r + red[ threadIdx.x ][ k ] : fmax( r, red[ threadIdx.x ][ k ] );
+        if( threadIdx.x < 5 )
+            atomicAdd( out + 1 + threadIdx.x, r );
+        else if( MHD )
+            atomicMax( ( unsigned long long * ) out, ( unsigned long long ) __double_as_longlong( r ) );
     }
 }
 
