@@ -187,8 +187,7 @@ class OracleMesh:
         dl = ctypes.c_double(0.0)
         rc = self._L.kro_step(self._h, int(n_steps), ctypes.byref(t), ctypes.byref(db), ctypes.byref(dl))
         if rc == -2:
-            raise NotImplementedError("oracle: MHD level jumps are not restated (a refined MHD mesh "
-                                      "can be built and initialised, not stepped)")
+            raise NotImplementedError("oracle: a refined MHD mesh steps on periodic domains only")
         if rc != 0:
             raise FloatingPointError("oracle step produced a non-finite dt")
         self.t, self.dt_bound, self.dt_last = t.value, db.value, dl.value

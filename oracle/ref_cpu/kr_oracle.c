@@ -1,6 +1,7 @@
 /* CPU restatement (FP64) of the Kratos hydro / ideal-MHD step.  TEST
  * INFRASTRUCTURE ONLY -- see kr_oracle.h for scope, layout and conventions.
  * Build: oracle/Makefile (gcc, no fused multiply-add). */
+#define _GNU_SOURCE                      /* qsort_r */
 #include "kr_oracle.h"
 #include "../../kratos_b200/csrc/problems.h"
 #include "../../kratos_b200/csrc/smr_tree.h"
@@ -33,7 +34,11 @@ struct kro_mesh
     double *dtc;                         /* per block CFL minimum           */
     kr_tree tree;                        /* blocks: levels, positions, faces */
     int     smr;                         /* more than one level             */
+    struct mh_holder * hold;             /* MHD refined meshes: the exchange */
+    int     n_hold;                      /* holders, in the reference's order */
 };
+
+static void build_holders( kro_mesh * m );   /* refined MHD meshes, below */
 
 /* logical position and per-axis block count of block b's level */
 static inline const int * blk_reg( const kro_mesh * m, int b ) { return m->tree.reg + 3 * b; }
@@ -244,6 +249,8 @@ kro_mesh * kro_create_tree( const kro_cfg * cfg, int n_regions, const kro_region
         m->f[ a ] = ( double * ) calloc( ( size_t ) m->nblk * m->nf[ a ], sizeof( double ) );
     m->ee = ( double * ) calloc( ( size_t ) m->nblk * m->nee, sizeof( double ) );
     set_geometry( m );
+    if( m->smr && cfg->mhd )
+        build_holders( m );
     return m;
 }
 
@@ -269,6 +276,7 @@ void kro_destroy( kro_mesh * m )
     free( m->w );
     for( int a = 0; a < 3; ++ a ) free( m->f[ a ] );
     free( m->ee );
+    free( m->hold );
     free( m );
 }
 
@@ -835,6 +843,686 @@ static void smr_flux_block( kro_mesh * m, int b, void * aux )
 }
 
 /* ------------------------------------------------------------------ */
+/* Static refinement, MHD: the reference's exchange holders, one per     */
+/* (host block, neighbour) pair with faces, edges and vertices enrolled   */
+/* (mhd/boundary/keeper.h:280-285 desired_mode).  Each holder pushes from */
+/* its host into its guest: same-level copies (to_same), restrictions     */
+/* (finer host, to_coarser) and prolongations (coarser host, to_finer) of */
+/* the primitives, with the tangential face B of face holders; after the  */
+/* flux sweeps the finer hosts' face holders average the fluxes and edge  */
+/* E of a refined face into the coarser guest and edge holders the edge E */
+/* of a refined edge, both writing the average back onto their own edges. */
+/* Every holder's index space is restated as the reference launches it   */
+/* (grids of resource_pack / resource_flux / resource_edge, the dispatch  */
+/* of a CTA row, BND_TH threads per CTA and the last CTA's second pass),  */
+/* and the holders run in the reference's order: hosts by level, then     */
+/* logical position (x most significant; region.h lex_ord_t), each       */
+/* host's neighbours by their direction flags in the same order.          */
+
+enum { BND_TH = 4, ORD = 2, NGH = 2 };   /* [dynamics] bnd_thread_limit; PLM order; ghosts */
+
+typedef struct mh_holder
+{
+    int host, guest;
+    int x[ 3 ], xr[ 3 ];         /* direction flags, seen from host and from guest */
+    int mode, d_lvl, rhs, ax[ 3 ];
+    int os[ 3 ], oc[ 3 ];        /* offset_s, offset_c: primitives            */
+    int obs[ 3 ], obc[ 3 ], obr[ 3 ];   /* offset_bs / bc / br: face B        */
+    int oes[ 3 ], oec[ 3 ];      /* offset_es / ec: edge E                    */
+} mh_holder;
+
+/* region.h:110-145 neighbor_t: flags of g (level lg) seen from h (level lh) */
+static void nb_flags( const int * h, int lh, const int * g, int lg, int * x )
+{
+    const int d = lg - lh;
+    for( int a = 0; a < 3; ++ a )
+    {
+        const int base = d >= 0 ? h[ a ] * ( 1 << d ) : ( h[ a ] >> -d );
+        x[ a ] = g[ a ] - base;
+        if( x[ a ] > 0 && d <= 0 )
+            x[ a ] *= 2;
+    }
+}
+
+static int leaf_at( const kro_mesh * m, int l, const int * r )
+{   /* the block index of the leaf at (l, r), or -1 */
+    const unsigned char * nd = m->tree.node[ l ];
+    if( ! nd || nd[ kr_tree_idx( & m->tree, l, r ) ] != 1 )
+        return -1;
+    for( int b = 0; b < m->nblk; ++ b )
+        if( m->tree.level[ b ] == l && ! memcmp( m->tree.reg + 3 * b, r, sizeof( int ) * 3 ) )
+            return b;
+    return -1;
+}
+
+static int cmp_host( const void * pa, const void * pb, void * pm )
+{   /* region.h:17-34 lex_ord_t: level, then x[0], x[1], x[2] */
+    const kro_mesh * m = ( const kro_mesh * ) pm;
+    const int a = * ( const int * ) pa, b = * ( const int * ) pb;
+    if( m->tree.level[ a ] != m->tree.level[ b ] )
+        return m->tree.level[ a ] - m->tree.level[ b ];
+    for( int k = 0; k < 3; ++ k )
+        if( m->tree.reg[ 3 * a + k ] != m->tree.reg[ 3 * b + k ] )
+            return m->tree.reg[ 3 * a + k ] - m->tree.reg[ 3 * b + k ];
+    return 0;
+}
+
+static int cmp_flags( const void * pa, const void * pb )
+{
+    const mh_holder * a = ( const mh_holder * ) pa, * b = ( const mh_holder * ) pb;
+    for( int k = 0; k < 3; ++ k )
+        if( a->x[ k ] != b->x[ k ] )
+            return a->x[ k ] - b->x[ k ];
+    return 0;
+}
+
+/* boundary.cpp:33-60 comm_base_t::set_geo (axis, rhs) and
+ * mhd/boundary/comm_functions.h:58-122 set_geo (offsets; one rank) */
+static void holder_geo( const kro_mesh * m, mh_holder * h )
+{
+    const int * n = m->c.n;
+    h->rhs = 0;
+    for( int a = 0; a < 3; ++ a )
+    {
+        h->ax[ a ] = 0;
+        const int out = h->x[ a ] < 0 || h->x[ a ] > 1;
+        if( ( h->mode != 0 ) ^ out )
+        {
+            h->rhs = h->x[ a ] > 0;
+            for( int k = 0; k < 3; ++ k )
+                h->ax[ ( h->mode + k ) % 3 ] = ( a + k ) % 3;
+            break;
+        }
+        else if( h->mode == 2 )
+            h->ax[ a ] = a;
+    }
+    const int ax = h->ax[ 0 ];
+    const int sh = h->d_lvl == 0 ? ORD : ( h->d_lvl > 0 ? ORD >> 1 : ORD << 1 );   /* shift(ord, -d_lvl) */
+    for( int a = 0; a < 3; ++ a )
+    {
+        const int n2 = n[ a ] / 2;
+        const int xp = h->x[ a ] > 0 ? h->x[ a ] : 0, rp = h->xr[ a ] > 0 ? h->xr[ a ] : 0;
+        h->oes[ a ] = xp * n2;
+        h->oec[ a ] = rp * n2;
+        h->obs[ a ] = xp * n2;
+        h->obc[ a ] = rp * n2;
+        h->obr[ a ] = xp * n2;
+        h->os[ a ] = xp * n2 - sh * ( h->x[ a ] > 0 );
+        h->oc[ a ] = rp * n2 - ORD * ( h->x[ a ] > 0 );
+    }
+    h->obs[ ax ] -= h->x [ ax ] > 1;
+    h->obr[ ax ] -= h->xr[ ax ] > 1;
+    h->obc[ ax ] -= h->x [ ax ] > 1;
+    if( h->mode == 1 )
+    {
+        const int a1 = h->ax[ 1 ];
+        h->os[ a1 ] = h->x [ a1 ] * ( n[ a1 ] / 2 );
+        h->oc[ a1 ] = h->xr[ a1 ] * ( n[ a1 ] / 2 );
+    }
+}
+
+/* tree.cpp:176-197 neighbors: for every level-(l+1) site around the block
+ * (offsets -1..2 per axis, the block's own 2 x 2 x 2 excluded), wrapped on
+ * periodic axes, the first leaf on the way down to level l - 1 */
+static void build_holders( kro_mesh * m )
+{
+    int * order = ( int * ) malloc( sizeof( int ) * m->nblk );
+    for( int b = 0; b < m->nblk; ++ b )
+        order[ b ] = b;
+    qsort_r( order, m->nblk, sizeof( int ), cmp_host, m );
+    mh_holder * hs = ( mh_holder * ) calloc( ( size_t ) m->nblk * 64, sizeof( mh_holder ) );
+    int nh = 0;
+    for( int k = 0; k < m->nblk; ++ k )
+    {
+        const int b = order[ k ], l = m->tree.level[ b ];
+        const int * r = m->tree.reg + 3 * b;
+        const int first = nh;
+        int di[ 3 ];
+        for( di[ 0 ] = -1; di[ 0 ] < 3; ++ di[ 0 ] )
+        for( di[ 1 ] = -1; di[ 1 ] < 3; ++ di[ 1 ] )
+        for( di[ 2 ] = -1; di[ 2 ] < 3; ++ di[ 2 ] )
+        {
+            if( di[ 0 ] >= 0 && di[ 0 ] <= 1 && di[ 1 ] >= 0 && di[ 1 ] <= 1 && di[ 2 ] >= 0 && di[ 2 ] <= 1 )
+                continue;
+            int t[ 3 ], t0[ 3 ];
+            for( int a = 0; a < 3; ++ a )
+                t[ a ] = t0[ a ] = 2 * r[ a ] + di[ a ];
+            if( ! kr_tree_regularize( & m->tree, l + 1, t ) )
+                continue;
+            for( int lt = l + 1; lt >= ( l > 0 ? l - 1 : 0 ); -- lt )
+            {
+                const int g = leaf_at( m, lt, t );
+                if( g >= 0 )
+                {
+                    mh_holder h;
+                    memset( & h, 0, sizeof( h ) );
+                    h.host = b;
+                    h.guest = g;
+                    h.d_lvl = lt - l;
+                    nb_flags( r, l, t0, lt, h.x );
+                    nb_flags( t0, lt, r, l, h.xr );
+                    int dup = 0;
+                    for( int q = first; q < nh; ++ q )
+                        dup |= ! memcmp( hs[ q ].x, h.x, sizeof( h.x ) );
+                    if( ! dup )
+                    {
+                        h.mode = -1;
+                        for( int a = 0; a < 3; ++ a )
+                            h.mode += h.x[ a ] != 0 && h.x[ a ] != 1;
+                        holder_geo( m, & h );
+                        hs[ nh ++ ] = h;
+                    }
+                    break;
+                }
+                for( int a = 0; a < 3; ++ a )   /* region.h:61-69 coarsen */
+                {
+                    t [ a ] = ( t [ a ] > 0 ? t [ a ] : t [ a ] - 1 ) / 2;
+                    t0[ a ] = ( t0[ a ] > 0 ? t0[ a ] : t0[ a ] - 1 ) / 2;
+                }
+            }
+        }
+        qsort( hs + first, nh - first, sizeof( mh_holder ), cmp_flags );
+    }
+    free( order );
+    m->hold = hs;
+    m->n_hold = nh;
+}
+
+static inline double * w_at( const kro_mesh * m, int b, const int * i )
+{
+    return m->w + ( size_t ) b * m->nw_cells * m->nw + iw( m, i[ 0 ], i[ 1 ], i[ 2 ] );
+}
+static inline double * bf_at( const kro_mesh * m, int step, int b, const int * i )
+{
+    return m->bf[ step ] + ( size_t ) b * m->nbf + ib( m, i[ 0 ], i[ 1 ], i[ 2 ] );
+}
+static inline double * ee_at( const kro_mesh * m, int b, const int * i )
+{
+    return m->ee + ( size_t ) b * m->nee + ie( m, i[ 0 ], i[ 1 ], i[ 2 ] );
+}
+static inline double * f_at( const kro_mesh * m, int a, int b, const int * i )
+{
+    return m->f[ a ] + ( size_t ) b * m->nf[ a ] + ifl( m, a, i[ 0 ], i[ 1 ], i[ 2 ] );
+}
+
+/* a launch of one holder: grid (nbx, nby), nth threads per CTA */
+typedef struct { int nbx, nby, nth; } mh_grid;
+
+static mh_grid grid_of( int n1, int nby )
+{   /* boundary.cpp:10-16 resource_thbl, along axis[ 1 ] */
+    mh_grid g;
+    g.nth = n1 < BND_TH ? n1 : BND_TH;
+    g.nbx = ( g.nth - 1 + n1 ) / g.nth;
+    g.nby = nby;
+    return g;
+}
+
+/* mhd/boundary/comm_functions.h:323-368 resource_pack */
+static mh_grid grid_pack( const kro_mesh * m, const mh_holder * h )
+{
+    int nc[ 3 ] = { m->c.n[ 0 ], m->c.n[ 1 ], m->c.n[ 2 ] };
+    const int a1 = h->ax[ 1 ], a2 = h->ax[ 2 ];
+    if( h->d_lvl >= 0 )
+    {
+        if( h->mode > 0 ) nc[ a2 ] = ORD;
+        if( h->mode > 1 ) nc[ a1 ] = ORD;
+    }
+    for( int a = 0; a < 3; ++ a )
+        nc[ a ] /= 1 + ( h->d_lvl != 0 );
+    if( h->d_lvl < 0 && h->mode > 0 )
+    {
+        nc[ a2 ] = NGH;
+        if( h->mode > 1 ) nc[ a1 ] = NGH;
+    }
+    int nby = nc[ a2 ];
+    if( h->mode == 0 )
+        nby += h->d_lvl > 0 ? NGH / 2 : ( h->d_lvl < 0 ? h->xr[ a2 ] > 0 : 1 );
+    return grid_of( nc[ a1 ], nby );
+}
+
+/* comm_functions.h:160-174 dispatch: axis[0] 0, axis[1] along the CTA row */
+static inline void dispatch( const mh_holder * h, const mh_grid * g, int bx, int by, int tx, int * i )
+{
+    i[ h->ax[ 0 ] ] = 0;
+    i[ h->ax[ 1 ] ] = bx * g->nth + tx;
+    i[ h->ax[ 2 ] ] = by;
+}
+
+/* hydro/boundary/comm_functions.h:306-327 to_same and
+ * mhd/boundary/comm_functions.h:422-465 to_same (face B of face holders) */
+static void mh_to_same( kro_mesh * m, const mh_holder * h, int step )
+{
+    const int * n = m->c.n, nw = m->nw;
+    const int ax = h->ax[ 0 ], a1 = h->ax[ 1 ], a2 = h->ax[ 2 ];
+    const mh_grid g = grid_pack( m, h );
+    for( int by = 0; by < g.nby; ++ by )
+    for( int bx = 0; bx < g.nbx; ++ bx )
+    for( int tx = 0; tx < g.nth; ++ tx )
+    {
+        int i0[ 3 ], im[ 3 ], ibb[ 3 ];
+        dispatch( h, & g, bx, by, tx, i0 );
+        if( i0[ a2 ] < n[ a2 ] )
+        {
+            for( int a = 0; a < 3; ++ a )
+            {
+                im[ a ] = h->os[ a ] + i0[ a ];
+                ibb[ a ] = h->oc[ a ] + i0[ a ];
+            }
+            for( int k = 0; k < ORD; ++ k )
+            {
+                im[ ax ] = k + h->os[ ax ];
+                ibb[ ax ] = k + h->oc[ ax ];
+                memcpy( w_at( m, h->guest, ibb ), w_at( m, h->host, im ), sizeof( double ) * nw );
+            }
+        }
+        if( h->mode != 0 )
+            continue;
+        for( int a = 0; a < 3; ++ a )
+        {
+            im[ a ] = h->obs[ a ] + i0[ a ];
+            ibb[ a ] = h->obc[ a ] + i0[ a ];
+        }
+        const int jmax = ( bx == g.nbx - 1 ) + 1;
+        for( int j = 0; j < jmax && ibb[ a1 ] < n[ a1 ] + 1; ++ j )
+        {
+            double * bt = bf_at( m, step, h->guest, ibb );
+            const double * bs = bf_at( m, step, h->host, im );
+            bt[ a1 ] = bs[ a1 ];
+            bt[ a2 ] = bs[ a2 ];
+            ibb[ a1 ] += g.nth;
+            im[ a1 ] += g.nth;
+        }
+    }
+}
+
+/* mhd/boundary/comm_functions.h:446-452 in_band_axis */
+static inline int in_band( int i, int off )
+{
+    return off == 0 || ( i - off >= 0 && i - off < ORD );
+}
+
+/* mhd/boundary/comm_functions.h:467-691 to_finer: the primitives of the
+ * coarser host's cells next to the face, limited-slope prolongation into
+ * the finer guest's ghosts (face holders: the whole receiver slab with its
+ * tangential ghost extensions; edge / vertex holders: ORD-wide bands), and
+ * for face holders the tangential face B of the guest's first ghost layer
+ * by Toth & Roe's divergence-preserving prolongation. */
+static void mh_to_finer( kro_mesh * m, const mh_holder * h, int step )
+{
+    const int * n = m->c.n, nw = m->nw;
+    const int ax = h->ax[ 0 ], a1 = h->ax[ 1 ], a2 = h->ax[ 2 ];
+    const mh_grid g = grid_pack( m, h );
+    for( int by = 0; by < g.nby; ++ by )
+    for( int bx = 0; bx < g.nbx; ++ bx )
+    for( int tx = 0; tx < g.nth; ++ tx )
+    {
+        int i0[ 3 ], im[ 3 ], ibb[ 3 ];
+        dispatch( h, & g, bx, by, tx, i0 );
+        for( int a = 0; a < 3; ++ a )
+        {
+            ibb[ a ] = h->oc[ a ] + 2 * i0[ a ];
+            im[ a ] = h->os[ a ] + i0[ a ];
+        }
+        const int im_max = ( h->mode > 0 && h->oc[ a1 ] != 0 ) ? 1 : ( n[ a1 ] + ORD ) / 2;
+        const int jmax = ( bx == g.nbx - 1 ) + 1;
+        for( int j = 0; j < jmax && i0[ a1 ] < im_max; ++ j )
+        {
+            double qc[ 8 ], dq[ 3 ][ 8 ];
+            for( int k = 0; k < ORD; ++ k )
+            {
+                im[ ax ] = h->os[ ax ] + k / 2;
+                ibb[ ax ] = h->oc[ ax ] + k;
+                if( ( k & 1 ) == 0 )
+                {
+                    memcpy( qc, w_at( m, h->host, im ), sizeof( double ) * nw );
+                    for( int q = 0; q < 3; ++ q )
+                    {
+                        const int aq = h->ax[ q ];
+                        ++ im[ aq ];
+                        const double * qr = w_at( m, h->host, im );
+                        im[ aq ] -= 2;
+                        const double * ql = w_at( m, h->host, im );
+                        ++ im[ aq ];
+                        for( int c = 0; c < nw; ++ c )
+                            dq[ aq ][ c ] = minmod( qr[ c ] - qc[ c ], qc[ c ] - ql[ c ] ) * 0.25f;
+                    }
+                }
+                for( int d1 = 0; d1 < 2; ++ d1 )
+                for( int d2 = 0; d2 < 2; ++ d2 )
+                {
+                    ibb[ a1 ] += d1;
+                    ibb[ a2 ] += d2;
+                    if( h->mode == 0 || ( in_band( ibb[ a1 ], h->oc[ a1 ] ) && in_band( ibb[ a2 ], h->oc[ a2 ] ) ) )
+                    {
+                        double * q = w_at( m, h->guest, ibb );
+                        for( int c = 0; c < nw; ++ c )
+                            q[ c ] = qc[ c ] + dq[ ax ][ c ] * ( 2 * ( k & 1 ) - 1 )
+                                   + dq[ a1 ][ c ] * ( 2 * d1 - 1 )
+                                   + dq[ a2 ][ c ] * ( 2 * d2 - 1 );
+                    }
+                    ibb[ a1 ] -= d1;
+                    ibb[ a2 ] -= d2;
+                }
+            }
+            ibb[ a1 ] += 2 * g.nth;
+            im[ a1 ] += g.nth;
+            i0[ a1 ] += g.nth;
+        }
+        if( h->mode != 0 )
+            continue;
+        /* face B (comm_functions.h:588-690) */
+        dispatch( h, & g, bx, by, tx, i0 );
+        for( int a = 0; a < 3; ++ a )
+        {
+            ibb[ a ] = 2 * i0[ a ] + h->obc[ a ];
+            im[ a ] = i0[ a ] + h->obr[ a ];
+        }
+        if( ibb[ a2 ] > n[ a2 ] - 2 || ibb[ a1 ] > n[ a1 ] - 2 )
+            continue;
+        ibb[ ax ] = h->rhs ? -1 : n[ ax ];
+        im[ ax ] = h->rhs ? n[ ax ] - 1 : 0;
+        double bb[ 3 ][ 3 ][ 2 ][ 2 ], db1[ 2 ], db2[ 3 ], db3[ 3 ];
+        for( int a = 0; a < 3; ++ a )
+        {
+            const int ap[ 2 ] = { mod3( a + 1 ), mod3( a + 2 ) };
+            for( int d = 0; d < 2; ++ d )
+            {
+                im[ a ] += d;
+                const double bc = bf_at( m, step, h->host, im )[ a ];
+                for( int q = 0; q < 2; ++ q )
+                {
+                    im[ ap[ q ] ] -= 1;
+                    const double bl = bf_at( m, step, h->host, im )[ a ];
+                    im[ ap[ q ] ] += 2;
+                    const double br = bf_at( m, step, h->host, im )[ a ];
+                    im[ ap[ q ] ] -= 1;
+                    db1[ q ] = minmod( br - bc, bc - bl ) / 4;
+                }
+                bb[ a ][ 2 * d ][ 0 ][ 0 ] = bc - db1[ 0 ] - db1[ 1 ];
+                bb[ a ][ 2 * d ][ 0 ][ 1 ] = bc - db1[ 0 ] + db1[ 1 ];
+                bb[ a ][ 2 * d ][ 1 ][ 0 ] = bc + db1[ 0 ] - db1[ 1 ];
+                bb[ a ][ 2 * d ][ 1 ][ 1 ] = bc + db1[ 0 ] + db1[ 1 ];
+                im[ a ] -= d;
+            }
+        }
+        for( int a = 0; a < 3; ++ a )
+        {
+            const int b1 = mod3( a + 1 ), b2 = mod3( a + 2 );
+            db2[ a ] = 0;
+            for( int l = 0; l < 2; ++ l )
+                for( int q = 0; q < 2; ++ q )   /* the reference divides only the second term by 8 */
+                    db2[ a ] += ( 2 * q - 1 ) * ( bb[ b1 ][ 2 ][ l ][ q ] - bb[ b1 ][ 0 ][ l ][ q ] )
+                              + ( 2 * l - 1 ) * ( bb[ b2 ][ 2 ][ l ][ q ] - bb[ b2 ][ 0 ][ l ][ q ] ) / 8;
+            db3[ a ] = 0;
+            for( int k = 0; k < 2; ++ k )
+                for( int l = 0; l < 2; ++ l )
+                    for( int q = 0; q < 2; ++ q )
+                        db3[ a ] += ( 2 * k - 1 ) / 16.f * ( 2 * l - 1 ) * ( 2 * q - 1 ) * bb[ a ][ 2 * k ][ l ][ q ];
+        }
+        for( int a = 0; a < 3; ++ a )
+        {
+            const int b1 = mod3( a + 1 ), b2 = mod3( a + 2 );
+            for( int l = 0; l < 2; ++ l )
+                for( int q = 0; q < 2; ++ q )
+                    bb[ a ][ 1 ][ l ][ q ] = db2[ a ] + ( bb[ a ][ 2 ][ l ][ q ] + bb[ a ][ 0 ][ l ][ q ] ) / 2
+                                           + db3[ b1 ] * ( 2 * l - 1 ) + db3[ b2 ] * ( 2 * q - 1 );
+        }
+        const int l_max = ( ibb[ a1 ] == n[ a1 ] - 2 ) + 2;
+        const int q_max = ( ibb[ a2 ] == n[ a2 ] - 2 ) + 2;
+        for( int l = 0; l < l_max; ++ l )
+            for( int q = 0; q < q_max; ++ q )
+            {
+                ibb[ a1 ] += l;
+                ibb[ a2 ] += q;
+                double * bt = bf_at( m, step, h->guest, ibb );
+                if( q < 2 )
+                    bt[ a1 ] = bb[ a1 ][ l ][ q ][ h->rhs ];
+                if( l < 2 )
+                    bt[ a2 ] = bb[ a2 ][ q ][ h->rhs ][ l ];
+                ibb[ a1 ] -= l;
+                ibb[ a2 ] -= q;
+            }
+    }
+}
+
+/* hydro/boundary/comm_functions.h:329-380 to_coarser (volume averages of
+ * the finer host's cells) inside mhd/boundary/comm_functions.h:693-780
+ * to_coarser, which limits edge / vertex holders to the NGH-wide band and
+ * adds, for face holders, the area average of the tangential face B over
+ * the two finer cell rows next to the face. */
+static void mh_to_coarser( kro_mesh * m, const mh_holder * h, int step )
+{
+    const int * n = m->c.n, nw = m->nw;
+    const int ax = h->ax[ 0 ], a1 = h->ax[ 1 ], a2 = h->ax[ 2 ];
+    const mh_grid g = grid_pack( m, h );
+    const double dv = m->vol0[ h->host ];
+    for( int by = 0; by < g.nby; ++ by )
+    for( int bx = 0; bx < g.nbx; ++ bx )
+    for( int tx = 0; tx < g.nth; ++ tx )
+    {
+        int i0[ 3 ], im[ 3 ], ibb[ 3 ];
+        dispatch( h, & g, bx, by, tx, i0 );
+        const int lim2 = h->mode > 0 ? NGH : n[ a2 ] / 2;
+        const int lim1 = h->mode > 1 ? NGH : n[ a1 ] / 2;
+        if( i0[ a2 ] < lim2 && i0[ a1 ] < lim1 )
+        {
+            for( int a = 0; a < 3; ++ a )
+            {
+                im[ a ] = h->os[ a ] + 2 * i0[ a ];
+                ibb[ a ] = i0[ a ] + h->oc[ a ];
+            }
+            double p[ 8 ], norm = 0;
+            for( int k = 0; k < 2 * ORD; ++ k )
+            {
+                im[ ax ] = k + h->os[ ax ];
+                if( ( k & 1 ) == 0 )
+                {
+                    ibb[ ax ] = k / 2 + h->oc[ ax ];
+                    norm = 0;
+                    for( int c = 0; c < nw; ++ c )
+                        p[ c ] = 0;
+                }
+                const int s1 = im[ a1 ], s2 = im[ a2 ];
+                for( int d1 = 0; d1 < 2; ++ d1 )
+                for( int d2 = 0; d2 < 2; ++ d2 )
+                {
+                    im[ a1 ] = s1 + d1;
+                    im[ a2 ] = s2 + d2;
+                    const double * q = w_at( m, h->host, im );
+                    for( int c = 0; c < nw; ++ c )
+                        p[ c ] += q[ c ] * dv;
+                    norm += dv;
+                }
+                im[ a1 ] = s1;
+                im[ a2 ] = s2;
+                if( k & 1 )
+                {
+                    double * o = w_at( m, h->guest, ibb );
+                    for( int c = 0; c < nw; ++ c )
+                        o[ c ] = p[ c ] / norm;
+                }
+            }
+        }
+        if( h->mode != 0 )
+            continue;
+        for( int a = 0; a < 3; ++ a )
+        {
+            im[ a ] = 2 * i0[ a ] + h->obs[ a ];
+            ibb[ a ] = i0[ a ] + h->obc[ a ];
+        }
+        if( h->obs[ ax ] > 0 )
+            -- im[ ax ];
+        const int jmax = ( bx == g.nbx - 1 ) + 1;
+        const int ib_max = n[ a1 ] / 2 + ( h->obc[ a1 ] > 1 );
+        for( int j = 0; j < jmax && i0[ a1 ] < ib_max; ++ j )
+        {
+            im[ a1 ] = 2 * i0[ a1 ] + h->obs[ a1 ];
+            double * bt = bf_at( m, step, h->guest, ibb );
+            for( int l = 0; l < 2; ++ l )
+            {
+                const int a = h->ax[ 1 + l ], ap = h->ax[ 2 - l ];
+                if( im[ ap ] >= n[ ap ] )
+                    continue;
+                double bsum = 0, s = 0;
+                const double ds = m->sfc0[ h->host * 3 + a ];
+                for( int k = 0; k < 2; ++ k )
+                {
+                    bsum += ds * bf_at( m, step, h->host, im )[ a ];
+                    s += ds;
+                    ++ im[ ap ];
+                    bsum += ds * bf_at( m, step, h->host, im )[ a ];
+                    s += ds;
+                    -- im[ ap ];
+                    ++ im[ ax ];
+                }
+                im[ ax ] -= 2;
+                bt[ a ] = s > 0 ? bsum / s : 0;
+            }
+            i0[ a1 ] += g.nth;
+            ibb[ a1 ] += g.nth;
+        }
+    }
+}
+
+/* act_flx, a finer host's face holder (mhd/boundary/comm_functions.h:818-884
+ * flux_to_buf over hydro/boundary/comm_functions.h:469-505): the coarser
+ * guest's flux on the refined face is the area average of the 4 finer
+ * fluxes; its tangential edge E the length average of the 2 finer edges,
+ * written back onto both. */
+static void mh_flux_to_buf( kro_mesh * m, const mh_holder * h )
+{
+    const int * n = m->c.n, nw = m->nw;
+    const int ax = h->ax[ 0 ], a1 = h->ax[ 1 ], a2 = h->ax[ 2 ];
+    /* resource_flux (comm_functions.h:384-399) */
+    const mh_grid g = grid_of( n[ a1 ] / 2, n[ a2 ] / 2 + ( h->xr[ a2 ] > 0 ) );
+    const double ds = m->sfc0[ h->host * 3 + ax ];
+    for( int by = 0; by < g.nby; ++ by )
+    for( int bx = 0; bx < g.nbx; ++ bx )
+    for( int tx = 0; tx < g.nth; ++ tx )
+    {
+        int i0[ 3 ], im[ 3 ], ibb[ 3 ];
+        dispatch( h, & g, bx, by, tx, i0 );
+        if( i0[ a2 ] < n[ a2 ] / 2 )
+        {
+            for( int a = 0; a < 3; ++ a )
+                ibb[ a ] = i0[ a ] + h->oc[ a ];
+            ibb[ ax ] = h->rhs ? 0 : n[ ax ];
+            im[ ax ] = h->rhs ? n[ ax ] : 0;
+            double * fb = f_at( m, ax, h->guest, ibb );
+            for( int c = 0; c < nw; ++ c )
+                fb[ c ] = 0;
+            double norm = 0;
+            for( int d1 = 0; d1 < 2; ++ d1 )
+            for( int d2 = 0; d2 < 2; ++ d2 )
+            {
+                im[ a1 ] = 2 * i0[ a1 ] + d1;
+                im[ a2 ] = 2 * i0[ a2 ] + d2;
+                const double * fm = f_at( m, ax, h->host, im );
+                for( int c = 0; c < nw; ++ c )
+                    fb[ c ] += fm[ c ] * ds;
+                norm += ds;
+            }
+            for( int c = 0; c < nw; ++ c )
+                fb[ c ] /= norm;
+        }
+        for( int a = 0; a < 3; ++ a )
+        {
+            im[ a ] = 2 * i0[ a ] + h->oes[ a ];
+            ibb[ a ] = i0[ a ] + h->oec[ a ];
+        }
+        const int jmax = ( bx == g.nbx - 1 ) + 1;
+        const int ib_max = n[ a1 ] / 2 + ( h->oec[ a1 ] > 1 );
+        for( int j = 0; j < jmax && i0[ a1 ] < ib_max; ++ j )
+        {
+            im[ a1 ] = 2 * i0[ a1 ] + h->oes[ a1 ];
+            double * eb = ee_at( m, h->guest, ibb );
+            double * em = ee_at( m, h->host, im );
+            for( int q = 0; q < 3; ++ q )
+            {
+                const int am = h->ax[ mod3( ax + q ) ];
+                if( am == ax )
+                    continue;
+                const double dl_l = m->dx0[ h->host * 3 + am ];
+                const double e_l = em[ am ] * dl_l;
+                ++ im[ am ];
+                double * ep = ee_at( m, h->host, im );
+                const double dl_r = m->dx0[ h->host * 3 + am ];
+                const double e_r = ep[ am ] * dl_r;
+                -- im[ am ];
+                eb[ am ] = ( e_l + e_r ) / ( dl_l + dl_r );
+                em[ am ] = eb[ am ];
+                ep[ am ] = eb[ am ];
+            }
+            ibb[ a1 ] += g.nth;
+            i0[ a1 ] += g.nth;
+        }
+    }
+}
+
+/* act_flx, a finer host's edge holder (mhd/boundary/comm_functions.h:918-954
+ * edge_efield): the coarser guest's E along the refined edge is the length
+ * average of the 2 finer edges, written back onto both. */
+static void mh_edge_efield( kro_mesh * m, const mh_holder * h )
+{
+    const int a1 = h->ax[ 1 ];
+    const int ne = m->c.n[ a1 ] / 2;                  /* resource_edge */
+    const mh_grid g = grid_of( ne, 1 );
+    for( int bx = 0; bx < g.nbx; ++ bx )
+    for( int tx = 0; tx < g.nth; ++ tx )
+    {
+        int i0[ 3 ], im[ 3 ], ibb[ 3 ];
+        dispatch( h, & g, bx, 0, tx, i0 );
+        for( int a = 0; a < 3; ++ a )
+        {
+            im[ a ] = h->oes[ a ] + 2 * i0[ a ];
+            ibb[ a ] = h->oec[ a ] + i0[ a ];
+        }
+        double * el = ee_at( m, h->host, im );
+        const double dl_l = m->dx0[ h->host * 3 + a1 ];
+        double et = el[ a1 ] * dl_l;
+        ++ im[ a1 ];
+        double * er = ee_at( m, h->host, im );
+        const double dl_r = m->dx0[ h->host * 3 + a1 ];
+        et += er[ a1 ] * dl_r;
+        const double ea = et / ( dl_l + dl_r );
+        ee_at( m, h->guest, ibb )[ a1 ] = ea;
+        el[ a1 ] = ea;
+        er[ a1 ] = ea;
+    }
+}
+
+/* keeper.cpp:148-160 act_bnd with mhd/boundary/keeper.h:304-326: the
+ * restrictions, the same-level copies, the prolongations (which read the
+ * coarser hosts' ghosts filled before), the restrictions again (their
+ * second pass, keeper.cpp:121-127 q_plgt.unpk), each in holder order. */
+static void mh_act_bnd( kro_mesh * m, int step )
+{
+    for( int k = 0; k < m->n_hold; ++ k )
+        if( m->hold[ k ].d_lvl < 0 ) mh_to_coarser( m, m->hold + k, step );
+    for( int k = 0; k < m->n_hold; ++ k )
+        if( m->hold[ k ].d_lvl == 0 ) mh_to_same( m, m->hold + k, step );
+    for( int k = 0; k < m->n_hold; ++ k )
+        if( m->hold[ k ].d_lvl > 0 ) mh_to_finer( m, m->hold + k, step );
+    for( int k = 0; k < m->n_hold; ++ k )
+        if( m->hold[ k ].d_lvl < 0 ) mh_to_coarser( m, m->hold + k, step );
+}
+
+/* keeper.cpp:162-166 act_flx: the finer hosts' face and edge holders */
+static void mh_act_flx( kro_mesh * m )
+{
+    for( int k = 0; k < m->n_hold; ++ k )
+    {
+        const mh_holder * h = m->hold + k;
+        if( h->d_lvl >= 0 )
+            continue;
+        if( h->mode == 0 )
+            mh_flux_to_buf( m, h );
+        else if( h->mode == 1 )
+            mh_edge_efield( m, h );
+    }
+}
+
+/* ------------------------------------------------------------------ */
 /* MHD physical boundaries (mhd/boundary/phys.h:118-250 operator(),      */
 /* phys_functors.h:9-132 free / fixed / outflow / reflect).  Per side on  */
 /* the domain edge, every transverse row of the ghost shell (ghost rows   */
@@ -1324,6 +2012,21 @@ static void flux_pencil( kro_mesh * m, int b, int axis, int step, int t1, int t2
     const double * w  = m->w + ( size_t ) b * m->nw_cells * nw;
     const double * bf = m->c.mhd ? m->bf[ step ] + ( size_t ) b * m->nbf : NULL;
     double * f = m->f[ axis ] + ( size_t ) b * m->nf[ axis ];
+    /* mhd/integrator/data.h:98-130 load_primative: on a transverse ghost
+     * line next to a side whose neighbour is on another level, the normal
+     * B of a face is the cell-centred B of the cell above it */
+    int cross = 0;
+    if( m->c.mhd && m->smr )
+        for( int q = 0; q < 2; ++ q )
+        {
+            const int a = q ? a2 : a1, t = q ? t2 : t1;
+            const int side = t < 0 ? 0 : ( t >= m->c.n[ a ] ? 1 : -1 );
+            if( side >= 0 )
+            {
+                const int fk = m->tree.face[ 6 * b + 2 * a + side ];
+                cross |= fk == KR_FACE_FINE || fk == KR_FACE_COARSE;
+            }
+        }
     for( int fc = 0; fc <= nax; ++ fc )
     {
         double ql[ 8 ], qr[ 8 ], flx[ 8 ];
@@ -1335,7 +2038,8 @@ static void flux_pencil( kro_mesh * m, int b, int axis, int step, int t1, int t2
             if( m->c.mhd && k == BCC + axis )
             {
                 ii[ axis ] = fc;
-                ql[ k ] = qr[ k ] = bf[ ib( m, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) + axis ];
+                ql[ k ] = qr[ k ] = cross ? w[ iw( m, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) + k ]
+                                          : bf[ ib( m, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) + axis ];
                 continue;
             }
             double q4[ 4 ];
@@ -1605,7 +2309,9 @@ static void ct_block( kro_mesh * m, int b, void * aux )
 int kro_step( kro_mesh * m, int n_steps, double * t, double * dt_bound, double * dt_last )
 {
     if( m->c.mhd && m->smr )
-        return -2;        /* MHD level jumps (mhd/boundary/comm_functions.h) not restated */
+        for( int a = 0; a < 3; ++ a )
+            if( ! periodic_axis( m, a ) )
+                return -2;        /* refined MHD meshes: periodic domains only */
     for( int s = 0; s < n_steps; ++ s )
     {
         double dt_use = 0;
@@ -1623,7 +2329,9 @@ int kro_step( kro_mesh * m, int n_steps, double * t, double * dt_bound, double *
                     return -1;
             }
             ghost_arg ga = { stage };
-            if( m->smr )
+            if( m->smr && m->c.mhd )
+                mh_act_bnd( m, stage );
+            else if( m->smr )
             {   /* keeper.cpp:148-160 act_bnd */
                 par_blocks( m, smr_restrict_block, NULL );
                 par_blocks( m, bc_block, & ga );
@@ -1651,13 +2359,19 @@ int kro_step( kro_mesh * m, int n_steps, double * t, double * dt_bound, double *
                 flux_arg fa = { stage, axis };
                 par_blocks( m, flux_block, & fa );
             }
-            if( m->smr )                 /* keeper.cpp:162-166 act_flx */
+            if( m->smr && m->c.mhd )
+            {   /* dynamics.h:80-99: calc_flx (sweeps, then the edge E), act_flx, intg_flx */
+                par_blocks( m, emf_block, NULL );
+                mh_act_flx( m );
+            }
+            else if( m->smr )            /* keeper.cpp:162-166 act_flx */
                 par_blocks( m, smr_flux_block, NULL );
             upd_arg ua = { stage, dt };
             par_blocks( m, update_block, & ua );
             if( m->c.mhd )
             {
-                par_blocks( m, emf_block, NULL );
+                if( ! m->smr )
+                    par_blocks( m, emf_block, NULL );
                 ct_arg cta = { stage, dt };
                 par_blocks( m, ct_block, & cta );
             }

@@ -4,9 +4,10 @@
  * the package is checked against; nothing in the product links or calls it.
  *
  * Scope: a Cartesian mesh of nb[0] x nb[1] x nb[2] root blocks, optionally
- * statically refined (hydro: restriction / prolongation of the ghost cells
- * across a level jump and the flux correction of the coarse side), two ghost
- * layers (PLM), Heun RK2 (two stages per step).
+ * statically refined (restriction / prolongation of the ghost cells across a
+ * level jump and the flux correction of the coarse side; MHD also the face-B
+ * restriction, Toth-Roe face-B prolongation and the edge-E correction, on
+ * periodic domains), two ghost layers (PLM), Heun RK2 (two stages per step).
  *   hydro : adiabatic EOS, PLM (van Leer harmonic limiter), HLLC.
  *   mhd   : adiabatic EOS with face-centred B, PLM, HLLD, Gardiner-Stone
  *           upwinded edge EMF (constrained transport), CT face update.
@@ -60,11 +61,12 @@ typedef struct
 } kro_region;
 
 kro_mesh * kro_create ( const kro_cfg * cfg );
-/* A mesh with static refinement (hydro only): the leaves of the block tree
+/* A mesh with static refinement: the leaves of the block tree
  * that the regions build (meshgen.cpp:111-160, tree.cpp:139-232), numbered
  * level by level, lexicographically inside a level.  With no region (or only
- * level-0 regions) this is kro_create's uniform mesh.  NULL for an MHD mesh
- * with refinement or a region outside the domain. */
+ * level-0 regions) this is kro_create's uniform mesh.  NULL for a region
+ * outside the domain.  kro_step returns -2 on a refined MHD mesh with a
+ * non-periodic axis (physical sides across a level jump are not restated). */
 kro_mesh * kro_create_tree( const kro_cfg * cfg, int n_regions, const kro_region * regions );
 int        kro_nblk   ( const kro_mesh * m );
 /* Level and logical position (at that level) of every block: level[nblk],

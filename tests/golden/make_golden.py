@@ -98,6 +98,13 @@ CASES = [
     # Toth-Roe prolongation and EMF correction across the level jump
     ("smr_ot", "ot", (2, 2, 2), (8, 8, 8), 4, 2, 1.6666666666666667,
      {"regions": [(1, (0.3, 0.1, 0.1), (0.45, 0.4, 0.4))], "bnd_thread_limit": "4"}, "final"),
+    # MHD on three levels (a level-2 point region inside a level-1 one)
+    ("smr_ot3", "ot", (1, 1, 1), (8, 8, 8), 4, 13, 1.6666666666666667,
+     {"regions": [(2, (0.3, 0.3, 0.3), (0.3, 0.3, 0.3))], "bnd_thread_limit": "4"}, "final"),
+    # MHD, a level-1 slab across four root blocks: coarse blocks that meet
+    # the refined region only along an edge or at a vertex
+    ("smr_ot_slab", "ot", (2, 2, 2), (8, 8, 8), 4, 14, 1.6666666666666667,
+     {"regions": [(1, (0.3, 0.3, 0.2), (0.7, 0.45, 0.6))], "bnd_thread_limit": "4"}, "sums"),
     # three levels (a level-2 region inside a level-1 one)
     ("smr_3lvl", "shock", (1, 1, 1), (8, 8, 8), 4, 12, 1.4,
      {"regions": [(2, (0.3, 0.3, 0.3), (0.3, 0.3, 0.3))]}, "final"),

@@ -162,8 +162,8 @@ def test_refined_fixtures_exercise_every_level_jump():
 def test_refined_mhd_tree_and_initial_state(name):
     """A statically refined MHD mesh: the shared tree gives the reference's
     leaves (levels and positions, tree order) and the initial conserved state
-    and face field match its checksums bit for bit.  The step across the level
-    jump is not restated yet, and the oracle refuses it."""
+    and face field match its checksums bit for bit (the step itself is in
+    test_step_bit_exact)."""
     meta, g = G.load(name)
     m = _mesh(meta)
     assert np.array_equal(m.level, g["level"]) and np.array_equal(m.reg, g["reg"])
@@ -171,5 +171,32 @@ def test_refined_mhd_tree_and_initial_state(name):
     u, bf = m.get_state()
     assert np.array_equal(G.checksums(u), g["u0_sum"])
     assert np.array_equal(G.face_checksums(bf, meta["n"]), g["bf0_sum"])
-    with pytest.raises(NotImplementedError):
-        m.step(1)
+
+
+def test_refined_mhd_fixtures_exercise_every_holder_kind():
+    """Between them the refined MHD fixtures hold every exchange the level
+    jump needs: same-level, restriction and prolongation across faces, edges
+    and vertices, and three levels."""
+    from oracle.kr_oracle import OracleMesh
+    seen = set()
+    for name in G.MHD_SMR_CASES:
+        meta, g = G.load(name)
+        lv, reg = g["level"], g["reg"]
+        seen.add(("levels", int(lv.max()) + 1))
+        nb = np.array(meta["nb"])
+        for b in range(len(lv)):
+            for c in range(len(lv)):
+                if b == c or abs(int(lv[c]) - int(lv[b])) > 1:
+                    continue
+                d = int(lv[c]) - int(lv[b])
+                lim = nb << lv[c]
+                base = reg[b] * 2 if d > 0 else (reg[b] >> 1 if d < 0 else reg[b])
+                for wrap in np.ndindex(3, 3, 3):
+                    x = reg[c] + (np.array(wrap) - 1) * lim - base
+                    if d <= 0:
+                        x = np.where(x > 0, 2 * x, x)
+                    if np.all((x >= -1) & (x <= 2)) and not np.all((x >= 0) & (x <= 1)):
+                        mode = int(np.sum((x != 0) & (x != 1))) - 1
+                        seen.add((d, mode))
+    want = {(d, mode) for d in (-1, 0, 1) for mode in (0, 1, 2)} | {("levels", 3)}
+    assert want <= seen, want - seen
