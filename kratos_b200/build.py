@@ -18,7 +18,7 @@ ROOT = os.path.dirname(PKG)
 LIB = os.path.join(PKG, "libkrb200.so")
 SOURCES = [os.path.join(PKG, "csrc", f) for f in ("kr_core.cu", "kr_learn.cu")]
 DEPS = SOURCES + [os.path.join(PKG, "csrc", f) for f in ("kr_math.cuh", "kr_fast.cuh", "kr_mlp.cuh", "problems.h",
-                                                         "smr_tree.h", "kr_batch.cuh")] + [
+                                                         "smr_tree.h", "kr_batch.cuh", "kr_smr_mhd.cuh")] + [
     os.path.join(ROOT, "include", "kratos_b200.h")]
 
 HOST = os.path.join(PKG, "host")

@@ -60,6 +60,7 @@ struct geo_t
     int phys;                     // bit 2a+s: side (a, s) is a non-periodic domain side
     int fine;                     // bit 2a+s: the neighbours across side (a, s) are finer
     int fitem[ 6 ];               // refined side: first of its 4 flux-average items
+    int xlev;                     // bit 2a+s: the neighbours across side (a, s) are on another level
 };
 
 // Static refinement: one (block, face) pair across a level jump.  dst / src:
@@ -111,6 +112,7 @@ struct args_t
     int vl2;                          // 1: VL2 integrator (donor-cell predictor)
     double * favg;                    // refined mesh: averaged fine face fluxes,
     int favg_n;                       //   [item][5][favg_n] (FP64 in both precisions)
+    int mh_smr;                       // 1: refined MHD mesh (ghost-line normal B rule)
     scal_t * s;
 };
 
@@ -979,7 +981,34 @@ template< class R, int MODE > constexpr int flux_min_ctas(  )
 // (wb: the right cell's first word, st: stride along the sweep, ngw: word
 // stride); the normal B of an MHD face comes from the face lattice instead.
 // FP32: words k and k + NP / 2 in pairs (plm_face_fast2).
-template< bool MHD, class R > __device__ __forceinline__
+// The normal B of a face for the reconstruction: the face lattice's value;
+// on a refined MHD mesh, along a transverse ghost line next to a side whose
+// neighbours are on another level, the cell-centred B of the cell above the
+// face instead (mhd/integrator/data.h:98-130 load_primative; no holder
+// carries face B onto those lines).  wb: that cell's first W word.
+template< class R, bool XL > __device__ __forceinline__
+R normal_b( const args_t< R > & a, int b, int axis, int step, const int * ii, const R * wb )
+{
+    if constexpr( XL )
+    {
+        const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
+        const int x = a.geo[ b ].xlev;
+        bool cross = false;
+        for( int q = 1; q <= 2; ++ q )
+        {
+            const int t = mod3( axis + q );
+            if( ii[ t ] < 0 )
+                cross |= ( x >> ( 2 * t ) ) & 1;
+            else if( ii[ t ] >= nn[ t ] )
+                cross |= ( x >> ( 2 * t + 1 ) ) & 1;
+        }
+        if( cross )
+            return wb[ ( BCC + axis ) * a.ngw ];
+    }
+    return R( a.bf[ step ][ ibf( a, b, axis, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] );
+}
+
+template< bool MHD, class R, bool XL = false > __device__ __forceinline__
 void plm_stencil( const args_t< R > & a, int b, int axis, int step, const int * ii, const R * wb,
                   int st, R * ql, R * qr )
 {
@@ -994,7 +1023,7 @@ void plm_stencil( const args_t< R > & a, int b, int axis, int step, const int * 
             qr[ k ] = p[ 0 ];
         }
         if constexpr( MHD )
-            ql[ BCC + axis ] = qr[ BCC + axis ] = R( a.bf[ step ][ ibf( a, b, axis, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] );
+            ql[ BCC + axis ] = qr[ BCC + axis ] = normal_b< R, XL >( a, b, axis, step, ii, wb );
         return;
     }
     if constexpr( sizeof( R ) == 4 )
@@ -1015,14 +1044,14 @@ void plm_stencil( const args_t< R > & a, int b, int axis, int step, const int * 
             plm_face_fast< R >( p[ -2 * st ], p[ -st ], p[ 0 ], p[ st ], ql[ NP - 1 ], qr[ NP - 1 ] );
         }
         if constexpr( MHD )
-            ql[ BCC + axis ] = qr[ BCC + axis ] = R( a.bf[ step ][ ibf( a, b, axis, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] );
+            ql[ BCC + axis ] = qr[ BCC + axis ] = normal_b< R, XL >( a, b, axis, step, ii, wb );
     }
     else
         for( int k = 0; k < NP; ++ k )
         {
             if( MHD && k == BCC + axis )
             {
-                ql[ k ] = qr[ k ] = R( a.bf[ step ][ ibf( a, b, axis, ii[ 0 ], ii[ 1 ], ii[ 2 ] ) ] );
+                ql[ k ] = qr[ k ] = normal_b< R, XL >( a, b, axis, step, ii, wb );
                 continue;
             }
             const R * p = wb + k * ngw;
@@ -1033,7 +1062,7 @@ void plm_stencil( const args_t< R > & a, int b, int axis, int step, const int * 
 // One CTA's 128 faces of a sweep: bx = CTA along the faces of one (x, y)
 // plane, by = z plane, blockIdx.z = block; dv
 // divides by the row length.
-template< bool MHD, class R, int MODE > __device__ __forceinline__
+template< bool MHD, class R, int MODE, bool XL = false > __device__ __forceinline__
 void flux_faces( const args_t< R > & a, int axis, int step, udiv_t dv, int b, unsigned bx, unsigned by,
                  bool hlle_warp = false )
 {
@@ -1075,7 +1104,7 @@ void flux_faces( const args_t< R > & a, int axis, int step, udiv_t dv, int b, un
     {
         const R * wb = a.w + ( size_t ) b * NW * a.ngw
                      + ( ( ii[ 0 ] + 2 ) + a.sw1 * ( ii[ 1 ] + 2 ) + a.sw2 * ( ii[ 2 ] + 2 ) );
-        plm_stencil< MHD, R >( a, b, axis, step, ii, wb, st, ql, qr );
+        plm_stencil< MHD, R, XL >( a, b, axis, step, ii, wb, st, ql, qr );
     }
     if constexpr( learned || MODE == FLUX_APPLY )
     {
@@ -1090,7 +1119,8 @@ void flux_faces( const args_t< R > & a, int axis, int step, udiv_t dv, int b, un
     solve_store< MHD, R, MODE >( a, b, axis, ii, valid, ql, qr, threadIdx.x >> 5, key );
 }
 
-template< bool MHD, class R, int MODE >
+// XL: a refined MHD mesh (the ghost-line normal-B rule, normal_b).
+template< bool MHD, class R, int MODE, bool XL = false >
 __global__ void __launch_bounds__( 128, ( flux_min_ctas< R, MODE >(  ) ) ) k_flux( const args_t< R > a, int axis, int step, udiv_t dv )
 {
     bool hlle_warp = false;
@@ -1103,7 +1133,7 @@ __global__ void __launch_bounds__( 128, ( flux_min_ctas< R, MODE >(  ) ) ) k_flu
                                  + ( blockIdx.y * gridDim.x + blockIdx.x ) * 4u + ( threadIdx.x >> 5 ) ]
                       >> ( threadIdx.x & 31 ) ) & 1u;
     }
-    flux_faces< MHD, R, MODE >( a, axis, step, dv, blockIdx.z, blockIdx.x, blockIdx.y, hlle_warp );
+    flux_faces< MHD, R, MODE, XL >( a, axis, step, dv, blockIdx.z, blockIdx.x, blockIdx.y, hlle_warp );
 }
 
 // Learned mode, the network's sweep: a fixed grid strides over the 128-face
@@ -1833,6 +1863,8 @@ static nccl_api_t & nccl(  )
     return api;
 }
 
+#include "kr_smr_mhd.cuh"
+
 struct kr_ctx
 {
     kr_cfg cfg;
@@ -1896,6 +1928,11 @@ struct kr_ctx
     double * favg = nullptr;           // averaged fine fluxes of the flux-average items
     int n_restrict = 0;
     std::vector< int > prolong_off;    // prolongation items of level l: [prolong_off[l - 1], prolong_off[l])
+    // refined MHD: the exchange holders (kr_smr_mhd.cuh)
+    mh_t * mh_list = nullptr;
+    int mh_same[ 2 ] = { 0, 0 }, mh_restrict[ 2 ] = { 0, 0 };
+    std::vector< int > mh_prolong, mh_waves;
+    int mh_items = 1;                  // largest item count of a holder (grid x of its launch)
 };
 
 static thread_local std::string g_create_error;
@@ -1941,6 +1978,7 @@ static args_t< R > make_args( kr_ctx * c )
     a.ee = ( R * ) c->ee;
     a.geo = c->geo; a.nbr = c->nbr; a.gid = c->gid; a.s = c->s; a.boxes = c->boxes;
     a.favg = c->favg; a.favg_n = int( smr_half_sites( c ) );
+    a.mh_smr = c->smr && c->cfg.mhd;
     for( int d = 0; d < 3; ++ d ) a.nbk[ d ] = c->cfg.nb[ d ];
     for( int k = 0; k < 6; ++ k ) a.bc[ k ] = c->cfg.bc[ k ];
     for( int k = 0; k < 5; ++ k ) a.w_fix[ k ] = c->cfg.w_fix[ k ];
@@ -1993,8 +2031,14 @@ static void launch_flux( kr_ctx * c, cudaStream_t st, const args_t< R > & a, int
     // sweeps without the network: each warp of faces runs the solver chosen
     // for it (exits at once on the network's sweep)
     constexpr int M = ( MODE == KR_RIEMANN_LEARNED && MHD ) ? FLUX_APPLY : MODE;
-    k_flux< MHD, R, M ><<< dim3( blocks_for( ( long long ) ext[ 0 ] * ext[ 1 ], 128 ), ext[ 2 ], c->nblk ), 128, 0, st >>>(
-        a, axis, stage, make_udiv( unsigned( ext[ 0 ] ) ) );
+    const dim3 grid( blocks_for( ( long long ) ext[ 0 ] * ext[ 1 ], 128 ), ext[ 2 ], c->nblk );
+    if constexpr( MHD && ( MODE == KR_RIEMANN_DEFAULT || MODE == KR_RIEMANN_HLLE ) )
+        if( c->smr )
+        {
+            k_flux< MHD, R, M, true ><<< grid, 128, 0, st >>>( a, axis, stage, make_udiv( unsigned( ext[ 0 ] ) ) );
+            return;
+        }
+    k_flux< MHD, R, M ><<< grid, 128, 0, st >>>( a, axis, stage, make_udiv( unsigned( ext[ 0 ] ) ) );
 }
 
 template< bool MHD, class R >
@@ -2013,6 +2057,15 @@ static void launch_flux_mode( kr_ctx * c, cudaStream_t st, const args_t< R > & a
 // EMF, update).  `timed( kind, launch )` wraps each piece (profiling: kinds
 // 0 c2p, 1 ghost and halo, 2..4 flux z, y, x, 5 emf, 6 update).
 struct untimed_t { template< class F > void operator(  )( int, F && f ) const { f(  ); } };
+
+// One phase of the refined-MHD exchange: holders [i0, i1) of the plan.
+template< class R, int KIND >
+static void launch_mh( kr_ctx * c, cudaStream_t st, const args_t< R > & a, int i0, int i1, int stage )
+{
+    for( int j = i0; j < i1; j += 65535 )      // one CTA row per holder
+        k_mh< R, KIND ><<< dim3( blocks_for( c->mh_items, 128 ), unsigned( std::min( i1 - j, 65535 ) ) ), 128, 0, st >>>(
+            a, c->mh_list + j, stage );
+}
 
 template< bool MHD, class R, class T >
 static void enqueue_front( kr_ctx * c, cudaStream_t st, const args_t< R > & a, int stage, T && timed )
@@ -2037,6 +2090,17 @@ static void enqueue_back( kr_ctx * c, cudaStream_t st, const args_t< R > & a, in
             k_halo< MHD, R, false ><<< dim3( c->halo_grid, unsigned( c->hrecv.items.size(  ) ) ), 256, 0, st >>>(
                 a, c->recv_items, ( R * ) c->recv_w, c->recv_b, stage );
         // (the same-level ghost fill happens in k_c2p and k_update: push)
+        if( MHD && c->mh_list )
+        {   // refined MHD: every ghost by the exchange holders (keeper.cpp:148-160
+            // act_bnd: restrictions, same-level copies, prolongations by the
+            // coarser host's level, the restrictions' second pass)
+            launch_mh< R, MH_RESTRICT >( c, st, a, c->mh_restrict[ 0 ], c->mh_restrict[ 1 ], stage );
+            launch_mh< R, MH_SAME >( c, st, a, c->mh_same[ 0 ], c->mh_same[ 1 ], stage );
+            for( size_t l = 0; l + 1 < c->mh_prolong.size(  ); ++ l )
+                launch_mh< R, MH_PROLONG >( c, st, a, c->mh_prolong[ l ], c->mh_prolong[ l + 1 ], stage );
+            launch_mh< R, MH_RESTRICT >( c, st, a, c->mh_restrict[ 0 ], c->mh_restrict[ 1 ], stage );
+            return;
+        }
         if( c->n_restrict )            // finer -> coarser ghosts
             k_restrict< R ><<< dim3( blocks_for( 2 * smr_half_sites( c ), 128 ), c->n_restrict ), 128, 0, st >>>( a, c->smr_items );
         if( ! MHD && has_phys( c ) )
@@ -2061,6 +2125,19 @@ static void enqueue_back( kr_ctx * c, cudaStream_t st, const args_t< R > & a, in
         timed( 5, [ & ] { k_emf< R ><<< dim3( blocks_for( ( long long )( n[ 0 ] + 1 ) * ( n[ 1 ] + 1 ), 256 ), n[ 2 ] + 1, nb ), 256, 0, st >>>(
             a, make_udiv( unsigned( n[ 0 ] + 1 ) ) ); } );
     const dim3 ug( blocks_for( ( long long )( n[ 0 ] + 1 ) * ( n[ 1 ] + 1 ), 256 ), n[ 2 ] + 1, nb );
+    if constexpr( MHD )
+        if( c->smr )
+        {   // refined MHD (dynamics.h:80-99): the coarse face flux over a
+            // refined side, the edge-E correction in waves, then the update
+            timed( 6, [ & ] {
+                if( c->n_restrict )
+                    k_flux_avg< R ><<< dim3( blocks_for( smr_half_sites( c ), 128 ), c->n_restrict ), 128, 0, st >>>( a, c->smr_items );
+                for( size_t w = 0; w + 1 < c->mh_waves.size(  ); ++ w )
+                    launch_mh< R, MH_FLUX >( c, st, a, c->mh_waves[ w ], c->mh_waves[ w + 1 ], stage );
+                k_update< MHD, R, true, 1 ><<< ug, 256, 0, st >>>( a, stage, make_udiv( unsigned( n[ 0 ] + 1 ) ) );
+                k_update< MHD, R, false, 2 ><<< ug, 256, 0, st >>>( a, stage, make_udiv( unsigned( n[ 0 ] + 1 ) ) ); } );
+            return;
+        }
     if constexpr( ! MHD )
         if( c->smr )
         {
@@ -2242,7 +2319,7 @@ static void set_geometry( kr_ctx * c )
         const int * reg = & c->reg_h[ 3 * b ];
         const int lvl = c->lvl_h[ b ];
         geo_t & o = c->geo_h[ b ];
-        o.phys = o.fine = 0;
+        o.phys = o.fine = o.xlev = 0;
         for( int f = 0; f < 6; ++ f ) o.fitem[ f ] = -1;
         for( int side = 0; side < 6; ++ side )
             if( g.bc[ side ] != KR_BC_PER && reg[ side / 2 ] == ( side & 1 ? ( g.nb[ side / 2 ] << lvl ) - 1 : 0 ) )
@@ -2330,8 +2407,10 @@ static bool build_tree( const kr_cfg * cfg, int n_regions, const kr_region * reg
     if( tree.max_level == 0 )
         return true;
     const char * why = nullptr;
-    if( cfg->mhd )
-        why = "static refinement is hydro only";
+    if( cfg->mhd && ! ( per[ 0 ] && per[ 1 ] && per[ 2 ] ) )
+        why = "static refinement of an MHD mesh needs periodic sides";
+    else if( cfg->mhd && cfg->riemann == KR_RIEMANN_LEARNED )
+        why = "the learned face selector runs on uniform meshes";
     else if( ranks_of( * cfg ) > 1 || ( cfg->flags & KR_FLAG_HALO_ALL ) )
         why = "static refinement runs on one rank, without KR_FLAG_HALO_ALL";
     else if( cfg->n[ 0 ] % 2 || cfg->n[ 1 ] % 2 || cfg->n[ 2 ] % 2 )
@@ -2485,6 +2564,7 @@ static kr_ctx * create_ctx( const kr_cfg * cfg, int n_regions, const kr_region *
         }
     const bool halo_all = ( cfg->flags & KR_FLAG_HALO_ALL ) != 0;
     std::vector< smr_item_t > smr_items;
+    std::vector< mh_t > mh_plan_h;
     if( smr )
     {   // the tree's leaves, one rank, no halo exchange
         c->smr = true;
@@ -2502,6 +2582,17 @@ static kr_ctx * create_ctx( const kr_cfg * cfg, int n_regions, const kr_region *
             h->b_off.assign( 1, 0 ); h->b_cnt.assign( 1, 0 );
         }
         smr_plan( tree, cfg->n, smr_items, c->n_restrict, c->prolong_off );
+        if( cfg->mhd )
+        {
+            mh_plan_t mp = mh_plan( tree, cfg->n );
+            c->mh_same[ 0 ] = mp.same[ 0 ]; c->mh_same[ 1 ] = mp.same[ 1 ];
+            c->mh_restrict[ 0 ] = mp.restrict_[ 0 ]; c->mh_restrict[ 1 ] = mp.restrict_[ 1 ];
+            c->mh_prolong = mp.prolong;
+            c->mh_waves = mp.waves;
+            mh_plan_h.swap( mp.list );
+            for( const mh_t & h : mh_plan_h )
+                c->mh_items = std::max( { c->mh_items, h.nbx * h.nby * h.nth, h.fbx * h.fby * h.fth } );
+        }
         if( smr_items.size(  ) > 65535 )
         {   // one grid row per item
             g_create_error = "kr_ctx_create_refined: more than 65535 level-jump items";
@@ -2557,6 +2648,10 @@ static kr_ctx * create_ctx( const kr_cfg * cfg, int n_regions, const kr_region *
           && ck( c, cudaMalloc( & c->smr_items, smr_items.size(  ) * sizeof( smr_item_t ) ), "malloc refinement items" )
           && ck( c, cudaMemcpyAsync( c->smr_items, smr_items.data(  ), smr_items.size(  ) * sizeof( smr_item_t ),
                                      cudaMemcpyHostToDevice, c->stream ), "upload refinement items" );
+    if( ok && ! mh_plan_h.empty(  ) )
+        ok = ck( c, cudaMalloc( & c->mh_list, mh_plan_h.size(  ) * sizeof( mh_t ) ), "malloc exchange holders" )
+          && ck( c, cudaMemcpyAsync( c->mh_list, mh_plan_h.data(  ), mh_plan_h.size(  ) * sizeof( mh_t ),
+                                     cudaMemcpyHostToDevice, c->stream ), "upload exchange holders" );
     // halo exchange: item lists and buffers (1-word minimum keeps pointers valid)
     {
         const halo_side_t * hs[ 2 ] = { & c->hsend, & c->hrecv };
@@ -2628,7 +2723,7 @@ static kr_ctx * create_ctx( const kr_cfg * cfg, int n_regions, const kr_region *
         for( int k = 0; k < 27; ++ k )
         {
             if( smr )
-            {
+            {   // refined MHD: the exchange holders fill every ghost, no push
                 const int sh[ 3 ] = { k % 3 - 1, ( k / 3 ) % 3 - 1, k / 9 - 1 };
                 const int nz = ( sh[ 0 ] != 0 ) + ( sh[ 1 ] != 0 ) + ( sh[ 2 ] != 0 );
                 int v = k == 13 ? b : -3;
@@ -2638,6 +2733,10 @@ static kr_ctx * create_ctx( const kr_cfg * cfg, int n_regions, const kr_region *
                     const int f = 2 * a + ( sh[ a ] > 0 );
                     const int kind = tree.face[ 6 * b + f ];
                     v = kind == KR_FACE_SAME ? tree.fnb[ ( 6 * b + f ) * 4 ] : ( kind == KR_FACE_PHYS ? -1 : -3 );
+                    if( cfg->mhd && kind == KR_FACE_SAME )
+                        v = -3;
+                    if( kind == KR_FACE_FINE || kind == KR_FACE_COARSE )
+                        c->geo_h[ b ].xlev |= 1 << f;
                     if( kind == KR_FACE_FINE )
                         c->geo_h[ b ].fine |= 1 << f;
                     if( kind == KR_FACE_FINE )
@@ -2700,7 +2799,7 @@ void kr_ctx_destroy( kr_ctx * c )
     if( c->stream ) cudaStreamSynchronize( c->stream );
     drop_graph( c );                   // before the communicator its graph uses
     if( c->comm ) nccl(  ).CommDestroy( c->comm );
-    cudaFree( c->gid ); cudaFree( c->smr_items ); cudaFree( c->favg );
+    cudaFree( c->gid ); cudaFree( c->smr_items ); cudaFree( c->favg ); cudaFree( c->mh_list );
     cudaFree( c->send_items ); cudaFree( c->recv_items );
     cudaFree( c->send_w ); cudaFree( c->recv_w ); cudaFree( c->send_b ); cudaFree( c->recv_b );
     for( int s = 0; s < 2; ++ s ) { cudaFree( c->u[ s ] ); cudaFree( c->bf[ s ] ); }
@@ -2791,7 +2890,8 @@ int kr_init_problem( kr_ctx * c, const char * name, uint64_t seed )
 {
     if( ! c || ! name ) return -1;
     const bool shock = ! std::strcmp( name, "shock" ), turb = ! std::strcmp( name, "turb" );
-    const bool ot = ! std::strcmp( name, "ot" ) || turb;     // the MHD workloads
+    const bool blast = ! std::strcmp( name, "blast" );
+    const bool ot = ! std::strcmp( name, "ot" ) || turb || blast;     // the MHD workloads
     if( ( ! shock && ! ot ) || ( ot != bool( c->cfg.mhd ) ) || c->boxes )
     {
         c->err = std::string( "kr_init_problem: unknown workload '" ) + name + "' for this mesh";
@@ -2810,6 +2910,9 @@ int kr_init_problem( kr_ctx * c, const char * name, uint64_t seed )
     kr_turb_t modes;
     if( turb )
         kr_turb_modes( & modes, seed );
+    double centre[ 3 ];
+    for( int a = 0; a < 3; ++ a )
+        centre[ a ] = ( g.x_min[ a ] + g.x_max[ a ] ) / 2;
     auto work = [ & ]( int b )
     {
         const int * reg = & c->reg_h[ 3 * b ];
@@ -2820,9 +2923,15 @@ int kr_init_problem( kr_ctx * c, const char * name, uint64_t seed )
             for( int i0 = 0; i0 <= n[ 0 ]; ++ i0 )
             {
                 double * p = hb.data(  ) + bidx( b, i0, i1, i2 );
-                p[ 0 ] = turb ? kr_turb_bx( g.gamma ) : kr_ot_bx( x_cc( g, reg, lvl, 1, i1 ) );
-                p[ 1 ] = turb ? 0.0 : kr_ot_by( x_cc( g, reg, lvl, 0, i0 ) );
-                p[ 2 ] = turb ? 0.0 : kr_ot_bz(  );
+                if( blast )
+                    for( int a = 0; a < 3; ++ a )
+                        p[ a ] = kr_blast_b( a );
+                else
+                {
+                    p[ 0 ] = turb ? kr_turb_bx( g.gamma ) : kr_ot_bx( x_cc( g, reg, lvl, 1, i1 ) );
+                    p[ 1 ] = turb ? 0.0 : kr_ot_by( x_cc( g, reg, lvl, 0, i0 ) );
+                    p[ 2 ] = turb ? 0.0 : kr_ot_bz(  );
+                }
             }
         for( int i2 = 0; i2 < n[ 2 ]; ++ i2 )
         for( int i1 = 0; i1 < n[ 1 ]; ++ i1 )
@@ -2848,6 +2957,8 @@ int kr_init_problem( kr_ctx * c, const char * name, uint64_t seed )
                 }
                 if( turb )
                     kr_turb_cell( u, x, bc, g.gamma, & modes );
+                else if( blast )
+                    kr_blast_cell( u, x, bc, centre, g.gamma );
                 else
                     kr_ot_cell( u, x, bc, g.gamma, seed, key );
             }
@@ -3067,6 +3178,7 @@ int kr_selector_collect( kr_ctx * c, int n_steps, unsigned stride, uint64_t seed
 {
     if( ! c || ! out || max_samples <= 0 || stride == 0 || n_steps < 0 ) return -1;
     if( ! c->cfg.mhd ) { c->err = "kr_selector_collect: MHD only"; return -1; }
+    if( c->smr ) { c->err = "kr_selector_collect: the learned face selector runs on uniform meshes"; return -1; }
     cudaSetDevice( c->cfg.device );
     const size_t bytes = size_t( max_samples ) * ( MLP_IN + 1 ) * sizeof( float );
     if( ! ck( c, cudaMalloc( & c->smp, bytes ), "malloc samples" )
@@ -3120,7 +3232,15 @@ int kr_launches_per_step( kr_ctx * c )
         for( int s = 0; s < 6; ++ s )
             phys += c->cfg.bc[ s ] != KR_BC_PER;
     int smr = 0;
-    if( c->smr )
+    if( c->smr && c->mh_list )
+    {   // refined MHD: restrictions (two passes), copies, prolongations by
+        // level, the flux average and the edge-E waves
+        smr = 2 * ( c->mh_restrict[ 1 ] > c->mh_restrict[ 0 ] ) + ( c->mh_same[ 1 ] > c->mh_same[ 0 ] )
+            + ( c->n_restrict ? 1 : 0 ) + int( c->mh_waves.size(  ) ) - 1;
+        for( size_t l = 0; l + 1 < c->mh_prolong.size(  ); ++ l )
+            smr += c->mh_prolong[ l + 1 ] > c->mh_prolong[ l ];
+    }
+    else if( c->smr )
     {
         smr = c->n_restrict ? 2 : 0;     // restriction, flux average
         for( int l = 1; l <= c->max_level; ++ l )

@@ -27,6 +27,9 @@
  *           A / c_s in [0.1, 2) plus 1e-3 A U(-1,1) per component, uniform B of
  *           random orientation with beta in [0.05, 10), all drawn uniformly
  *           from (seed, box)
+ *   blast : magnetized blast wave, rho = 1, v = 0, p = 100 in the cells whose
+ *           centre lies within r < 0.1 of the domain's centre, 0.1 elsewhere,
+ *           uniform B = (1, 1, 0) / sqrt(2)
  */
 #ifndef KR_PROBLEMS_H
 #define KR_PROBLEMS_H
@@ -243,6 +246,34 @@ static inline void kr_box_cell( double * u, const double x_cc[ 3 ], const double
     for( int a = 0; a < 3; ++ a )
     {
         u[ 2 + a ] = p->rho * v[ a ];
+        u[ 5 + a ] = b_cc[ a ];
+    }
+}
+
+/* blast: face fields and the conserved state of one cell.  c: the domain's
+ * centre.  u[0] rho, u[1] E (incl. magnetic energy of the face-averaged
+ * field), u[2..4] momentum, u[5..7] cell-centred B. */
+static inline double kr_blast_b( int axis ) { return axis < 2 ? sqrt( 0.5 ) : 0.0; }
+
+static inline double kr_blast_pre( const double x_cc[ 3 ], const double c[ 3 ] )
+{
+    double r2 = 0;
+    for( int a = 0; a < 3; ++ a )
+        r2 += ( x_cc[ a ] - c[ a ] ) * ( x_cc[ a ] - c[ a ] );
+    return r2 < 0.01 ? 100.0 : 0.1;
+}
+
+static inline void kr_blast_cell( double * u, const double x_cc[ 3 ], const double b_cc[ 3 ],
+                                  const double c[ 3 ], double gamma )
+{
+    double em = 0;
+    for( int a = 0; a < 3; ++ a )
+        em += b_cc[ a ] * b_cc[ a ];
+    u[ 0 ] = 1.0;
+    u[ 1 ] = kr_blast_pre( x_cc, c ) / ( gamma - 1.0 ) + 0.5 * em;
+    for( int a = 0; a < 3; ++ a )
+    {
+        u[ 2 + a ] = 0.0;
         u[ 5 + a ] = b_cc[ a ];
     }
 }

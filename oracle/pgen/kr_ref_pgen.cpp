@@ -7,7 +7,7 @@
 // reference) and overrides only init_cond, so that the reference integrates the
 // same seeded initial states as this package (kratos_b200/csrc/problems.h).
 //
-// [problem] name = shock | ot ; [problem] seed = <int>
+// [problem] name = shock | ot | turb | box | blast ; [problem] seed = <int>
 #include <iostream>
 
 #include "device/general.h"
@@ -147,6 +147,44 @@ struct turb_mhd_t : mhd_base_t
     }
 };
 
+// Magnetized blast wave: over-pressured sphere at the domain's centre, uniform B.
+static double g_centre[ 3 ] = { 0.5, 0.5, 0.5 };
+
+struct blast_mhd_t : mhd_base_t
+{
+    void init_cond( mesh::block::dual_t & d ) override
+    {
+        auto & b_h = dynamic_cast< dynamics::mhd::block_data_t & >( d.h(  ) );
+        const auto & blk = d.b_w.get(  );
+        const auto & geo = blk.geo;
+        auto n_face = geo.n_ceff;
+        for( auto & n_s : n_face.x )
+            n_s += ( n_s > 1 );
+        for( auto i : utils::loop( n_face ) )
+        {
+            auto * bf = b_h.fld.bf.at( i );
+            for( int a = 0; a < 3; ++ a )
+                bf[ a ] = kr_blast_b( a );
+        }
+        for( auto i : utils::loop( geo.n_ceff ) )
+        {
+            double x[ 3 ], bc[ 3 ];
+            for( int a = 0; a < 3; ++ a )
+            {
+                x[ a ] = geo.x_cc( a, i[ a ] );
+                auto j = i;
+                ++ j[ a ];
+                bc[ a ] = ( b_h.fld.bf.at( i )[ a ] + b_h.fld.bf.at( j )[ a ] ) / 2;
+            }
+            double uu[ 8 ];
+            kr_blast_cell( uu, x, bc, g_centre, p_eos->gamma );
+            auto * u = b_h.hyd.u.at( i );
+            for( int n = 0; n < 8; ++ n )
+                u[ n ] = uu[ n ];
+        }
+    }
+};
+
 // One box of a batch of independent periodic boxes ([problem] box = index); the
 // mesh is the box: n_cell_global = n_cell_block = its edge length.
 static int g_box = 0;
@@ -210,6 +248,14 @@ void run( int argc, char * argv[  ] )
         mesh.enroll_module< ot_mhd_t >(  );
     else if( name == "turb" )
         mesh.enroll_module< turb_mhd_t >(  );
+    else if( name == "blast" )
+    {
+        const auto x0 = args.get< type::coord2_t >( "mesh", "x_min" );
+        const auto x1 = args.get< type::coord2_t >( "mesh", "x_max" );
+        for( int a = 0; a < 3; ++ a )
+            g_centre[ a ] = ( x0[ a ] + x1[ a ] ) / 2;
+        mesh.enroll_module< blast_mhd_t >(  );
+    }
     else if( name == "box" )
     {
         g_box = args.get< int >( "problem", "box", 0 );

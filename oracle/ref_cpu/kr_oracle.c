@@ -2393,7 +2393,11 @@ int kro_init_problem( kro_mesh * m, const char * name, unsigned long long seed )
     for( int a = 0; a < 3; ++ a )
         nglob[ a ] = n[ a ] * m->c.nb[ a ];
     const int is_shock = ! strcmp( name, "shock" ), is_turb = ! strcmp( name, "turb" );
-    const int is_ot = ! strcmp( name, "ot" ) || is_turb;      /* the MHD workloads */
+    const int is_blast = ! strcmp( name, "blast" );
+    const int is_ot = ! strcmp( name, "ot" ) || is_turb || is_blast;   /* the MHD workloads */
+    double centre[ 3 ];
+    for( int a = 0; a < 3; ++ a )
+        centre[ a ] = ( m->c.x_min[ a ] + m->c.x_max[ a ] ) / 2;
     if( ! is_shock && ! is_ot )
         return -1;
     if( is_ot != m->c.mhd )
@@ -2412,9 +2416,9 @@ int kro_init_problem( kro_mesh * m, const char * name, unsigned long long seed )
             for( int i0 = 0; i0 <= n[ 0 ]; ++ i0 )
             {
                 double * p = bf + ib( m, i0, i1, i2 );
-                p[ 0 ] = is_turb ? kr_turb_bx( m->c.gamma ) : kr_ot_bx( kro_x_cc( m, b, 1, i1 ) );
-                p[ 1 ] = is_turb ? 0.0 : kr_ot_by( kro_x_cc( m, b, 0, i0 ) );
-                p[ 2 ] = is_turb ? 0.0 : kr_ot_bz(  );
+                p[ 0 ] = is_blast ? kr_blast_b( 0 ) : ( is_turb ? kr_turb_bx( m->c.gamma ) : kr_ot_bx( kro_x_cc( m, b, 1, i1 ) ) );
+                p[ 1 ] = is_blast ? kr_blast_b( 1 ) : ( is_turb ? 0.0 : kr_ot_by( kro_x_cc( m, b, 0, i0 ) ) );
+                p[ 2 ] = is_blast ? kr_blast_b( 2 ) : ( is_turb ? 0.0 : kr_ot_bz(  ) );
             }
         for( int i2 = 0; i2 < n[ 2 ]; ++ i2 )
         for( int i1 = 0; i1 < n[ 1 ]; ++ i1 )
@@ -2439,7 +2443,9 @@ int kro_init_problem( kro_mesh * m, const char * name, unsigned long long seed )
                     ++ jj[ a ];
                     bc[ a ] = ( bl + bf[ ib( m, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) + a ] ) / 2;
                 }
-                if( is_turb )
+                if( is_blast )
+                    kr_blast_cell( c, x, bc, centre, m->c.gamma );
+                else if( is_turb )
                     kr_turb_cell( c, x, bc, m->c.gamma, & modes );
                 else
                     kr_ot_cell( c, x, bc, m->c.gamma, seed, key );

@@ -30,6 +30,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 from kratos_b200.snapshot import Snapshot, block_ids, to_lex_arrays, to_tree_arrays  # noqa: E402
+from kratos_b200.amr import gradient_regions  # noqa: E402
 
 REF_BIN = os.environ.get("KR_REF_BIN", os.path.join(ROOT, "oracle", "_ref", "kratos_ref"))
 
@@ -105,6 +106,10 @@ CASES = [
     # the refined region only along an edge or at a vertex
     ("smr_ot_slab", "ot", (2, 2, 2), (8, 8, 8), 4, 14, 1.6666666666666667,
      {"regions": [(1, (0.3, 0.3, 0.2), (0.7, 0.45, 0.6))], "bnd_thread_limit": "4"}, "sums"),
+    # the magnetized blast on a mesh that the gradient criterion refines at
+    # t = 0 (kratos_b200/amr.py; 2^3 roots of 8^3, two levels, 120 blocks)
+    ("smr_blast", "blast", (2, 2, 2), (8, 8, 8), 4, 15, 1.6666666666666667,
+     {"regions": gradient_regions((2, 2, 2), (8, 8, 8), 2), "bnd_thread_limit": "4"}, "sums"),
     # three levels (a level-2 region inside a level-1 one)
     ("smr_3lvl", "shock", (1, 1, 1), (8, 8, 8), 4, 12, 1.4,
      {"regions": [(2, (0.3, 0.3, 0.3), (0.3, 0.3, 0.3))]}, "final"),
@@ -133,7 +138,7 @@ def par_text(problem, nb, n, steps, seed, gamma, extra, prefix):
     if init:
         lines += ["[init]"] + ["%s = %s" % kv for kv in init.items()] + [""]
     for k, (level, lo, hi) in enumerate(regions):
-        lines += ["[refine_region_%c]" % "abcdefghij"[k], "level = %d" % level,
+        lines += ["[refine_region_%04d]" % k, "level = %d" % level,
                   "x_min = %r %r %r" % tuple(lo), "x_max = %r %r %r" % tuple(hi), ""]
     return "\n".join(lines)
 

@@ -1,0 +1,151 @@
+"""Statically refined MHD meshes on the GPU, through the C ABI
+(kr_ctx_create_refined with mhd = 1), against the original Kratos solver's
+refined MHD runs (golden fixtures smr_ot, smr_ot3, smr_ot_slab, and smr_blast on
+the mesh that the gradient criterion of kratos_b200/amr.py refines) and the CPU
+restatement.
+
+Tolerances as for the uniform FP64 MHD step: relative L1 per conserved field
+(momentum against the momentum vector's L1 norm) and per owned face-B
+component (against the whole field's L1 norm) <= 1e-11 after the fixtures' 4
+steps (fused multiply-adds on the device), <= 1e-10 for the longer oracle run;
+checksum-only fixtures to 1e-11 relative.  Size-independent: |div B| <= 1e-12
+on every block of every level, and the totals of a periodic refined mesh kept
+to rounding (the flux average and the edge-E correction make the level jump
+conservative for mass, energy and momentum).
+"""
+import numpy as np
+import pytest
+
+import golden_io as G
+
+pytestmark = pytest.mark.gpu
+
+TOL_FP64 = 1e-11
+TOL_FP64_LONG = 1e-10
+TOL_MIXED = 1e-4
+
+
+def rel_l1(a, b):
+    den = np.abs(b).sum()
+    return np.abs(a - b).sum() / (den if den > 0 else 1.0)
+
+
+def _dyn(meta, precision=2, **kw):
+    from kratos_b200 import Dynamics
+    return Dynamics(True, meta["nb"], meta["n"], gamma=meta["gamma"], cfl=meta["cfl"],
+                    precision=precision, regions=G.regions(meta), **kw)
+
+
+def _bf_errors(bf, ref_own, n):
+    own, mask = G.owned_bf(bf, n), G.face_mask(n)
+    den = sum(np.abs(ref_own[..., c][:, mask[..., c]]).sum() for c in range(3))
+    return [np.abs(own[..., c][:, mask[..., c]] - ref_own[..., c][:, mask[..., c]]).sum() / den
+            for c in range(3)]
+
+
+@pytest.mark.parametrize("name", G.MHD_SMR_CASES)
+def test_refined_mhd_step_matches_reference(name):
+    meta, g = G.load(name)
+    d = _dyn(meta)
+    assert np.array_equal(d.level, g["level"]) and np.array_equal(d.reg, g["reg"])
+    d.init_problem(meta["workload"], meta["seed"])
+    u0, _ = d.get_state()
+    np.testing.assert_array_equal(G.checksums(u0)[:, :5], g["u0_sum"][:, :5])
+    d.step(meta["steps"])
+    u, bf = d.get_state()
+    tm = d.time()
+    assert d.status() == 0
+    assert abs(tm["t"] - meta["t"]) <= 1e-12 * meta["t"]
+    assert abs(tm["dt_last"] - meta["dt"]) <= 1e-12 * meta["dt"]
+    if "u1" in g:
+        for k, e in enumerate(G.field_errors(u, g["u1"])):
+            assert e <= TOL_FP64, "field %d rel L1 %.3e" % (k, e)
+        for c, e in enumerate(_bf_errors(bf, g["bf1"], meta["n"])):
+            assert e <= TOL_FP64, "bf %d rel L1 %.3e" % (c, e)
+    else:
+        s = G.checksums(u)
+        for k in range(5):
+            np.testing.assert_allclose(s[:2, k], g["u1_sum"][:2, k], rtol=TOL_FP64, atol=1e-13)
+        np.testing.assert_allclose(G.face_checksums(bf, meta["n"])[:2], g["bf1_sum"][:2],
+                                   rtol=TOL_FP64, atol=1e-13)
+
+
+@pytest.mark.parametrize("name", G.MHD_SMR_CASES)
+def test_refined_mhd_keeps_div_b_and_totals(name):
+    """div B stays at rounding on every block of every level, and the totals
+    of the periodic refined mesh stay constant over 20 steps."""
+    meta, g = G.load(name)
+    d = _dyn(meta)
+    d.init_problem(meta["workload"], meta["seed"])
+    div0, tot0 = d.diagnostics()
+    assert div0 <= 1e-12
+    d.step(20)
+    assert d.status() == 0
+    div, tot = d.diagnostics()
+    assert div <= 1e-12, "max |div B| %.3e" % div
+    assert abs(tot[0] - tot0[0]) <= 1e-12 * abs(tot0[0])
+    assert abs(tot[1] - tot0[1]) <= 1e-12 * abs(tot0[1])
+    assert np.all(np.abs(tot[2:] - tot0[2:]) <= 1e-12 * abs(tot0[1]))
+
+
+def test_refined_mhd_matches_oracle_longer():
+    """Two level jumps on a mesh of ragged boxes, 12 steps, device FP64 against
+    the restatement."""
+    from kratos_b200 import Dynamics
+    from oracle.kr_oracle import OracleMesh
+    nb, n = (2, 2, 2), (8, 8, 12)
+    regions = [(1, (0.1, 0.55, 0.2), (0.45, 0.9, 0.35)), (2, (0.3, 0.7, 0.25), (0.35, 0.75, 0.3))]
+    m = OracleMesh(True, nb, n, 5 / 3, regions=regions)
+    d = Dynamics(True, nb, n, gamma=5 / 3, regions=regions)
+    assert np.array_equal(d.level, m.level) and np.array_equal(d.reg, m.reg)
+    assert d.level.max() == 2
+    m.init_problem("ot", 23)
+    d.init_problem("ot", 23)
+    m.step(12)
+    d.step(12)
+    u_ref, bf_ref = m.get_state()
+    u, bf = d.get_state()
+    assert d.time()["t"] == pytest.approx(m.t, rel=1e-12)
+    for k, e in enumerate(G.field_errors(u, u_ref)):
+        assert e <= TOL_FP64_LONG, "field %d rel L1 %.3e" % (k, e)
+    for c, e in enumerate(_bf_errors(bf, G.owned_bf(bf_ref, n), n)):
+        assert e <= TOL_FP64_LONG, "bf %d rel L1 %.3e" % (c, e)
+
+
+def test_blast_on_criterion_mesh_matches_oracle():
+    """The magnetized blast on the criterion-refined mesh (three levels), 8
+    steps, the whole state against the restatement."""
+    from kratos_b200 import Dynamics
+    from kratos_b200.amr import gradient_regions
+    from oracle.kr_oracle import OracleMesh
+    nb, n = (2, 2, 2), (8, 8, 8)
+    regions = gradient_regions(nb, n, 2)
+    m = OracleMesh(True, nb, n, 5 / 3, regions=regions)
+    d = Dynamics(True, nb, n, gamma=5 / 3, regions=regions)
+    assert np.array_equal(d.level, m.level) and d.level.max() == 2
+    m.init_problem("blast", 0)
+    d.init_problem("blast", 0)
+    m.step(8)
+    d.step(8)
+    u_ref, bf_ref = m.get_state()
+    u, bf = d.get_state()
+    for k, e in enumerate(G.field_errors(u, u_ref)):
+        assert e <= TOL_FP64_LONG, "field %d rel L1 %.3e" % (k, e)
+    for c, e in enumerate(_bf_errors(bf, G.owned_bf(bf_ref, n), n)):
+        assert e <= TOL_FP64_LONG, "bf %d rel L1 %.3e" % (c, e)
+
+
+def test_refined_mhd_mixed_within_bound_of_fp64():
+    meta, g = G.load("smr_ot3")
+    rho = {}
+    for prec in (2, 1):
+        d = _dyn(meta, precision=prec)
+        d.init_problem(meta["workload"], meta["seed"])
+        d.step(10)
+        assert d.status() == 0
+        div, _ = d.diagnostics()
+        assert div <= 1e-12
+        rho[prec] = d.get_state()[0][..., 0]
+    e = rel_l1(rho[1], rho[2])
+    print("refined MHD mixed vs FP64: rel L1 density %.2e" % e)
+    assert e <= TOL_MIXED

@@ -179,7 +179,7 @@ def test_refined_mhd_fixtures_exercise_every_holder_kind():
     and vertices, and three levels."""
     from oracle.kr_oracle import OracleMesh
     seen = set()
-    for name in G.MHD_SMR_CASES:
+    for name in ["smr_ot", "smr_ot3", "smr_ot_slab"]:
         meta, g = G.load(name)
         lv, reg = g["level"], g["reg"]
         seen.add(("levels", int(lv.max()) + 1))
