@@ -63,6 +63,8 @@ def parse():
                    help="batched-box leg: boxes of the seeded batch (0: skip)")
     p.add_argument("--smr", type=int, default=1,
                    help="1: also time the statically refined hydro mesh (1 GPU only)")
+    p.add_argument("--blast", type=int, default=1,
+                   help="also time the magnetized blast on the criterion-refined MHD mesh (0: skip)")
     p.add_argument("--ref-cuda", type=int, default=1,
                    help="1: also time the reference's own CUDA build (baseline/_ref) on this GPU")
     p.add_argument("--turb", type=int, default=512, choices=[0, 128, 256, 512],
@@ -457,6 +459,46 @@ def time_smr(args, local_rank):
     return out
 
 
+def time_blast(args, local_rank):
+    """Zone-cycles/s of the magnetized blast on a mesh that the gradient
+    criterion refines at t = 0 (kratos_b200/amr.py): root 128^3 in 16^3 blocks,
+    three refinement levels, PLM + HLLD + CT, every block of every level in one
+    captured graph per step; mixed and FP64."""
+    import torch
+    from kratos_b200 import Dynamics
+    from kratos_b200.amr import gradient_regions
+    nb, n = (8, 8, 8), (16, 16, 16)
+    regions = gradient_regions(nb, n, 3)
+    out = {"workload": "magnetized blast (p = 100 inside r < 0.1 of the centre, 0.1 outside, rho = 1, "
+                       "B = (1, 1, 0) / sqrt 2), root 128^3 in 512 blocks of 16^3, three levels refined at "
+                       "t = 0 where max_axes(|d rho| / 2 rho + |d p| / 2 p) > 0.5 (%d refine_region points), "
+                       "periodic, PLM + HLLD + CT, Heun RK2" % len(regions)}
+    for mode, prec in (("mixed", 1), ("fp64", 2)):
+        d = Dynamics(True, nb, n, gamma=5 / 3, precision=prec, device=local_rank, regions=regions)
+        stream = torch.cuda.Stream(device=local_rank)
+        d.set_stream(stream.cuda_stream)
+        d.init_problem("blast", SEED)
+        d.step(args.warmup)
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        d.step(args.steps)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        ms = t0.elapsed_time(t1)
+        if d.status() != 0:
+            raise RuntimeError("device status %d in the blast %s step" % (d.status(), mode))
+        div, _ = d.diagnostics()
+        out[mode] = {"value": d.n_cells * args.steps / (ms * 1e-3), "unit": UNIT,
+                     "ms_per_step": ms / args.steps, "kernels_ms_per_step": d.profile_step(),
+                     "launches_per_step": d.launches_per_step(), "div_b_max": div}
+        out["blocks_per_level"] = [int((d.level == l).sum()) for l in range(int(d.level.max()) + 1)]
+        out["cells"] = d.n_cells
+        d.close()
+    return out
+
+
 def time_boxes(args, local_rank, sel=None):
     """Zone-cycles/s of a batch of independent periodic MHD boxes (seed 5,
     edge lengths 16..64), each on its own CFL dt: one KR_FLAG_BOXES context per
@@ -678,6 +720,8 @@ def main():
     line["flux_ms_per_step"] = flux_ms
     if rank == 0 and world == 1 and args.smr:
         line["smr"] = time_smr(args, local_rank)
+    if rank == 0 and world == 1 and args.blast:
+        line["blast"] = time_blast(args, local_rank)
     if rank == 0 and world == 1 and args.boxes:
         line["boxes"] = time_boxes(args, local_rank, sel)
     if rank == 0 and world == 1 and args.turb and sel is not None:

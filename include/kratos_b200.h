@@ -187,7 +187,9 @@ int kr_set_time( kr_ctx * ctx, double t, double dt_bound );
 
 /* Sticky device status word: 0 ok; bit 0 non-finite or non-positive dt; bit 1
  * a NaN velocity in the state (stage 0's cons -> prim; the density and
- * pressure floors heal NaN density and pressure, as the reference's do). */
+ * pressure floors heal NaN density and pressure, as the reference's do); bit 2
+ * an exchange index outside its block's arrays on a refined MHD mesh (the
+ * access was skipped). */
 int kr_status( kr_ctx * ctx );
 
 /* Number of kernel launches kr_step enqueues per step (instrumentation). */

@@ -31,7 +31,7 @@
 // that way); same-level copies copy the E of the host's cell, which c2p
 // computed from the same B and v.
 
-enum { MH_TH = 4, MH_ORD = 2, MH_NGH = 2 };      // [dynamics] bnd_thread_limit; PLM order; ghosts
+enum { MH_TH = 64, MH_ORD = 2, MH_NGH = 2 };     // [dynamics] bnd_thread_limit (its default); PLM order; ghosts
 enum { MH_SAME = 0, MH_RESTRICT = 1, MH_PROLONG = 2, MH_FLUX = 3 };
 
 struct mh_t
@@ -43,6 +43,7 @@ struct mh_t
     int oes[ 3 ], oec[ 3 ];              // edge E
     int nbx, nby, nth;                   // launch grid of the holder's exchange kernel
     int fbx, fby, fth;                   // and of its edge-E correction
+    int n1;                              // the exchange grid's extent along ax[ 1 ]
 };
 
 __device__ __forceinline__ void mh_dispatch( const mh_t & h, int nth, int bx, int by, int tx, int * i )
@@ -52,20 +53,36 @@ __device__ __forceinline__ void mh_dispatch( const mh_t & h, int nth, int bx, in
     i[ h.ax[ 2 ] ] = by;
 }
 
+// Accessors with their own bounds check: an index outside the array's box
+// (W: ghosts -2..n+1; face B: -2..n+2; edge E: -1..n+1) sets status bit 2 and
+// the access goes to a scratch word instead.
+__device__ double mh_sink[ 4 ];
+
+template< class R > __device__ __forceinline__
+bool mh_in( const args_t< R > & a, int b, const int * i, int lo, int hi_extra )
+{
+    const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
+    bool ok = b >= 0 && b < a.nblk;
+    for( int d = 0; d < 3; ++ d )
+        ok &= i[ d ] >= lo && i[ d ] <= nn[ d ] + hi_extra;
+    if( ! ok )
+        atomicOr( & a.s[ 0 ].status, 4 );
+    return ok;
+}
 template< class R > __device__ __forceinline__
 R * mh_w( const args_t< R > & a, int b, int c, const int * i )
 {
-    return a.w + iw( a, b, c, 11, i[ 0 ], i[ 1 ], i[ 2 ] );
+    return mh_in( a, b, i, -2, 1 ) ? a.w + iw( a, b, c, 11, i[ 0 ], i[ 1 ], i[ 2 ] ) : ( R * ) mh_sink;
 }
 template< class R > __device__ __forceinline__
 double * mh_bf( const args_t< R > & a, int step, int b, int c, const int * i )
 {
-    return a.bf[ step ] + ibf( a, b, c, i[ 0 ], i[ 1 ], i[ 2 ] );
+    return mh_in( a, b, i, -2, 2 ) ? a.bf[ step ] + ibf( a, b, c, i[ 0 ], i[ 1 ], i[ 2 ] ) : mh_sink;
 }
 template< class R > __device__ __forceinline__
 R * mh_ee( const args_t< R > & a, int b, int c, const int * i )
 {
-    return a.ee + ifx( a, b, c, 3, i[ 0 ], i[ 1 ], i[ 2 ] );
+    return mh_in( a, b, i, -1, 1 ) ? a.ee + ifx( a, b, c, 3, i[ 0 ], i[ 1 ], i[ 2 ] ) : ( R * ) mh_sink;
 }
 
 __device__ __forceinline__ double mh_minmod( double x, double y )
@@ -102,7 +119,9 @@ void mh_same( const args_t< R > & a, const mh_t & h, int step, int bx, int by, i
     const int ax = h.ax[ 0 ], a1 = h.ax[ 1 ], a2 = h.ax[ 2 ];
     int i0[ 3 ], im[ 3 ], ib[ 3 ];
     mh_dispatch( h, h.nth, bx, by, tx, i0 );
-    if( i0[ a2 ] < n[ a2 ] )
+    // a CTA row covers its extent along ax[ 1 ] exactly while that is at most
+    // MH_TH; the guard keeps larger extents in bounds
+    if( i0[ a2 ] < n[ a2 ] && i0[ a1 ] < h.n1 )
     {
         for( int d = 0; d < 3; ++ d )
         {
@@ -363,6 +382,8 @@ void mh_edge_e( const args_t< R > & a, const mh_t & h, int bx, int by, int tx, c
     mh_dispatch( h, h.fth, bx, by, tx, i0 );
     if( h.mode == 1 )
     {
+        if( i0[ a1 ] >= n[ a1 ] / 2 )
+            return;
         for( int d = 0; d < 3; ++ d )
         {
             im[ d ] = h.oes[ d ] + 2 * i0[ d ];
@@ -507,6 +528,7 @@ static mh_t mh_make( int host, int guest, int d_lvl, const int * x, const int * 
         nc[ a2 ] = MH_NGH;
         if( h.mode > 1 ) nc[ a1 ] = MH_NGH;
     }
+    h.n1 = nc[ a1 ];
     h.nth = mh_grid_th( nc[ a1 ] );
     h.nbx = ( h.nth - 1 + nc[ a1 ] ) / h.nth;
     h.nby = nc[ a2 ];

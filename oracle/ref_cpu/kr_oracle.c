@@ -859,7 +859,7 @@ static void smr_flux_block( kro_mesh * m, int b, void * aux )
 /* logical position (x most significant; region.h lex_ord_t), each       */
 /* host's neighbours by their direction flags in the same order.          */
 
-enum { BND_TH = 4, ORD = 2, NGH = 2 };   /* [dynamics] bnd_thread_limit; PLM order; ghosts */
+enum { BND_TH = 64, ORD = 2, NGH = 2 };  /* [dynamics] bnd_thread_limit (its default); PLM order; ghosts */
 
 typedef struct mh_holder
 {
@@ -869,6 +869,7 @@ typedef struct mh_holder
     int os[ 3 ], oc[ 3 ];        /* offset_s, offset_c: primitives            */
     int obs[ 3 ], obc[ 3 ], obr[ 3 ];   /* offset_bs / bc / br: face B        */
     int oes[ 3 ], oec[ 3 ];      /* offset_es / ec: edge E                    */
+    int n1;                      /* the exchange grid's extent along axis[ 1 ] */
 } mh_holder;
 
 /* region.h:110-145 neighbor_t: flags of g (level lg) seen from h (level lh) */
@@ -961,6 +962,8 @@ static void holder_geo( const kro_mesh * m, mh_holder * h )
     }
 }
 
+static void holder_extent( const kro_mesh * m, mh_holder * h );
+
 /* tree.cpp:176-197 neighbors: for every level-(l+1) site around the block
  * (offsets -1..2 per axis, the block's own 2 x 2 x 2 excluded), wrapped on
  * periodic axes, the first leaf on the way down to level l - 1 */
@@ -1010,6 +1013,7 @@ static void build_holders( kro_mesh * m )
                         for( int a = 0; a < 3; ++ a )
                             h.mode += h.x[ a ] != 0 && h.x[ a ] != 1;
                         holder_geo( m, & h );
+                        holder_extent( m, & h );
                         hs[ nh ++ ] = h;
                     }
                     break;
@@ -1080,6 +1084,16 @@ static mh_grid grid_pack( const kro_mesh * m, const mh_holder * h )
     return grid_of( nc[ a1 ], nby );
 }
 
+static void holder_extent( const kro_mesh * m, mh_holder * h )
+{   /* grid_pack's n_cell along axis[ 1 ] */
+    const int a1 = h->ax[ 1 ];
+    int e = m->c.n[ a1 ];
+    if( h->d_lvl >= 0 && h->mode > 1 ) e = ORD;
+    e /= 1 + ( h->d_lvl != 0 );
+    if( h->d_lvl < 0 && h->mode > 1 ) e = NGH;
+    h->n1 = e;
+}
+
 /* comm_functions.h:160-174 dispatch: axis[0] 0, axis[1] along the CTA row */
 static inline void dispatch( const mh_holder * h, const mh_grid * g, int bx, int by, int tx, int * i )
 {
@@ -1101,7 +1115,10 @@ static void mh_to_same( kro_mesh * m, const mh_holder * h, int step )
     {
         int i0[ 3 ], im[ 3 ], ibb[ 3 ];
         dispatch( h, & g, bx, by, tx, i0 );
-        if( i0[ a2 ] < n[ a2 ] )
+        /* the CTA row covers exactly its extent along axis[ 1 ] while that is
+         * at most BND_TH (the reference's threads past it would step out of
+         * the arrays); the guard keeps larger extents in bounds */
+        if( i0[ a2 ] < n[ a2 ] && i0[ a1 ] < h->n1 )
         {
             for( int a = 0; a < 3; ++ a )
             {
@@ -1402,7 +1419,7 @@ static void mh_flux_to_buf( kro_mesh * m, const mh_holder * h )
     {
         int i0[ 3 ], im[ 3 ], ibb[ 3 ];
         dispatch( h, & g, bx, by, tx, i0 );
-        if( i0[ a2 ] < n[ a2 ] / 2 )
+        if( i0[ a2 ] < n[ a2 ] / 2 && i0[ a1 ] < n[ a1 ] / 2 )
         {
             for( int a = 0; a < 3; ++ a )
                 ibb[ a ] = i0[ a ] + h->oc[ a ];
@@ -1472,6 +1489,8 @@ static void mh_edge_efield( kro_mesh * m, const mh_holder * h )
     {
         int i0[ 3 ], im[ 3 ], ibb[ 3 ];
         dispatch( h, & g, bx, 0, tx, i0 );
+        if( i0[ a1 ] >= ne )
+            continue;
         for( int a = 0; a < 3; ++ a )
         {
             im[ a ] = h->oes[ a ] + 2 * i0[ a ];
