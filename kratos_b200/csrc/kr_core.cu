@@ -664,7 +664,7 @@ __global__ void __launch_bounds__( 128 ) k_prolong( const args_t< R > a, const s
 // area average of the 4 fine face fluxes it covers ((d1, d2), d1 outer).  Kept
 // in FP64 (a.favg) in both precisions, so the coarse correction carries the
 // fine fluxes without a rounding to the flux word type.
-template< class R >
+template< class R, int NF = 5 >        // NF: flux words per face (5 hydro, 7 MHD)
 __global__ void __launch_bounds__( 128 ) k_flux_avg( const args_t< R > a, const smr_item_t * items )
 {
     const smr_item_t it = items[ blockIdx.y ];
@@ -686,7 +686,7 @@ __global__ void __launch_bounds__( 128 ) k_flux_avg( const args_t< R > a, const 
             jj[ a1 ] = 2 * t1 + e1;
             jj[ a2 ] = 2 * t2 + e2;
             for( int c = 0; c < 5; ++ c )
-                acc[ c ] += double( a.f[ ax ][ ifx( a, it.src, c, 5, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) ] ) * ds;
+                acc[ c ] += double( a.f[ ax ][ ifx( a, it.src, c, NF, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) ] ) * ds;
             norm += ds;
         }
     for( int c = 0; c < 5; ++ c )
@@ -2131,7 +2131,7 @@ static void enqueue_back( kr_ctx * c, cudaStream_t st, const args_t< R > & a, in
             // refined side, the edge-E correction in waves, then the update
             timed( 6, [ & ] {
                 if( c->n_restrict )
-                    k_flux_avg< R ><<< dim3( blocks_for( smr_half_sites( c ), 128 ), c->n_restrict ), 128, 0, st >>>( a, c->smr_items );
+                    k_flux_avg< R, 7 ><<< dim3( blocks_for( smr_half_sites( c ), 128 ), c->n_restrict ), 128, 0, st >>>( a, c->smr_items );
                 for( size_t w = 0; w + 1 < c->mh_waves.size(  ); ++ w )
                     launch_mh< R, MH_FLUX >( c, st, a, c->mh_waves[ w ], c->mh_waves[ w + 1 ], stage );
                 k_update< MHD, R, true, 1 ><<< ug, 256, 0, st >>>( a, stage, make_udiv( unsigned( n[ 0 ] + 1 ) ) );

@@ -72,20 +72,30 @@ def test_refined_mhd_step_matches_reference(name):
 
 @pytest.mark.parametrize("name", G.MHD_SMR_CASES)
 def test_refined_mhd_keeps_div_b_and_totals(name):
-    """div B stays at rounding on every block of every level, and the totals
-    of the periodic refined mesh stay constant over 20 steps."""
+    """div B stays at rounding on every block of every level over 20 steps, and
+    the totals move as the restatement's do.  (The reference's refined MHD step
+    is not exactly conservative: across 20 steps the restatement, which is the
+    reference bit for bit, drifts by up to ~1e-10 in mass and ~1e-7 in energy
+    and momentum; the device must follow that drift.)"""
+    from oracle.kr_oracle import OracleMesh
     meta, g = G.load(name)
     d = _dyn(meta)
-    d.init_problem(meta["workload"], meta["seed"])
+    G.init(d, meta)
     div0, tot0 = d.diagnostics()
     assert div0 <= 1e-12
     d.step(20)
     assert d.status() == 0
     div, tot = d.diagnostics()
     assert div <= 1e-12, "max |div B| %.3e" % div
-    assert abs(tot[0] - tot0[0]) <= 1e-12 * abs(tot0[0])
-    assert abs(tot[1] - tot0[1]) <= 1e-12 * abs(tot0[1])
-    assert np.all(np.abs(tot[2:] - tot0[2:]) <= 1e-12 * abs(tot0[1]))
+    m = OracleMesh(True, meta["nb"], meta["n"], meta["gamma"], cfl=meta["cfl"], regions=G.regions(meta))
+    G.init(m, meta)
+    m.step(20)
+    u_ref, _ = m.get_state()
+    vol = np.array([np.prod([m.dx(b, a) for a in range(3)]) for b in range(m.nblk)])
+    ref = np.einsum("b,bzyxk->k", vol, u_ref[..., :5])
+    scale = [abs(tot0[0]), abs(tot0[1])] + [abs(tot0[1])] * 3
+    for k in range(5):
+        assert abs(tot[k] - ref[k]) <= 1e-10 * scale[k], "total %d: %.3e vs %.3e" % (k, tot[k], ref[k])
 
 
 def test_refined_mhd_matches_oracle_longer():
