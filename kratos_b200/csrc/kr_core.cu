@@ -33,6 +33,7 @@
 #include <string>
 #include <thread>
 #include <type_traits>
+#include <unordered_map>
 #include <vector>
 
 namespace kr
@@ -707,15 +708,16 @@ __global__ void __launch_bounds__( 128 ) k_flux_avg( const args_t< R > a, const 
 // face B, but those values from not-yet-filled rows land only in ghost-shell
 // corner slots that no stencil reads.
 
+// field: 1 writes the face B of the ghost layers too, 0 the primitives only
+// (the second pass of a refined mesh's exchange, phys.h:199-249 step < 0).
 template< class R >
-__global__ void __launch_bounds__( 128 ) k_phys_mhd( const args_t< R > a, int side, int step )
+__global__ void __launch_bounds__( 128 ) k_phys_mhd( const args_t< R > a, int side, int step, int field = 1 )
 {
     const int b = blockIdx.y;
     const int axis = side >> 1, right = side & 1;
     const int kind = a.bc[ side ];
-    const int g = a.gid[ b ];
-    const int reg[ 3 ] = { g % a.nbk[ 0 ], ( g / a.nbk[ 0 ] ) % a.nbk[ 1 ], g / ( a.nbk[ 0 ] * a.nbk[ 1 ] ) };
-    if( reg[ axis ] != ( right ? a.nbk[ axis ] - 1 : 0 ) )
+    const int ph = a.geo[ b ].phys;          // bit 2d+s: side (d, s) is a domain side here
+    if( ! ( ( ph >> side ) & 1 ) )
         return;
     const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
     const int a1 = mod3( axis + 1 ), a2 = mod3( axis + 2 );
@@ -730,9 +732,9 @@ __global__ void __launch_bounds__( 128 ) k_phys_mhd( const args_t< R > a, int si
     {
         const int d = h ? a2 : a1;
         int r = i_tgt[ d ], f = i_tgt[ d ];
-        if( a.bc[ 2 * d ] != KR_BC_PER && reg[ d ] == 0 )
+        if( ( ph >> ( 2 * d ) ) & 1 )
         {   r = max( r, 0 ); f = max( f, 0 ); }
-        if( a.bc[ 2 * d + 1 ] != KR_BC_PER && reg[ d ] == a.nbk[ d ] - 1 )
+        if( ( ph >> ( 2 * d + 1 ) ) & 1 )
         {   r = min( r, nn[ d ] - 1 ); f = min( f, nn[ d ] ); }
         i_src[ d ] = r;
         i_sfc[ d ] = f;
@@ -804,7 +806,7 @@ __global__ void __launch_bounds__( 128 ) k_phys_mhd( const args_t< R > a, int si
             a.w[ iw( a, b, 8 + d, 11, i_tgt[ 0 ], i_tgt[ 1 ], i_tgt[ 2 ] ) ] =
                 p[ BCC + d1 ] * p[ MOM + d2 ] - p[ BCC + d2 ] * p[ MOM + d1 ];
         }
-        for( int q = 0; q < 3; ++ q )
+        for( int q = 0; q < 3 && field; ++ q )
         {
             if( q == axis )
                 BFw[ ibf( a, b, q, i_fbc[ 0 ], i_fbc[ 1 ], i_fbc[ 2 ] ) ] = bfb[ 2 + i ][ q ];
@@ -1225,11 +1227,10 @@ void emf_site( const args_t< R > & a, udiv_t dv, int b, int i2, unsigned t )
     // boundary-plane edges of a high out / fre side: the interior cell's
     // advective E, with the reference's velocity scaling (w holds v, which it
     // multiplies by 1 / rho once more) -- integrator.h:329-382
-    const int g = a.gid[ b ];
-    const int reg[ 3 ] = { g % a.nbk[ 0 ], ( g / a.nbk[ 0 ] ) % a.nbk[ 1 ], g / ( a.nbk[ 0 ] * a.nbk[ 1 ] ) };
+    const int ph = a.geo[ b ].phys;
     for( int d = 0; d < 3; ++ d )
     {
-        if( ! ( a.emf_out >> d & 1 ) || i[ d ] != nn[ d ] || nn[ d ] < 2 || reg[ d ] != a.nbk[ d ] - 1 )
+        if( ! ( a.emf_out >> d & 1 ) || i[ d ] != nn[ d ] || nn[ d ] < 2 || ! ( ( ph >> ( 2 * d + 1 ) ) & 1 ) )
             continue;
         int jc[ 3 ] = { i[ 0 ], i[ 1 ], i[ 2 ] };
         -- jc[ d ];
@@ -1930,9 +1931,9 @@ struct kr_ctx
     std::vector< int > prolong_off;    // prolongation items of level l: [prolong_off[l - 1], prolong_off[l])
     // refined MHD: the exchange holders (kr_smr_mhd.cuh)
     mh_t * mh_list = nullptr;
-    int mh_same[ 2 ] = { 0, 0 }, mh_restrict[ 2 ] = { 0, 0 };
+    uint2 * mh_work = nullptr;         // (holder, item) per thread, phase by phase
+    int mh_same[ 2 ] = { 0, 0 }, mh_restrict[ 2 ] = { 0, 0 };   // work-item ranges
     std::vector< int > mh_prolong, mh_waves;
-    int mh_items = 1;                  // largest item count of a holder (grid x of its launch)
 };
 
 static thread_local std::string g_create_error;
@@ -2058,13 +2059,12 @@ static void launch_flux_mode( kr_ctx * c, cudaStream_t st, const args_t< R > & a
 // 0 c2p, 1 ghost and halo, 2..4 flux z, y, x, 5 emf, 6 update).
 struct untimed_t { template< class F > void operator(  )( int, F && f ) const { f(  ); } };
 
-// One phase of the refined-MHD exchange: holders [i0, i1) of the plan.
+// One phase of the refined-MHD exchange: work items [i0, i1) of the plan.
 template< class R, int KIND >
 static void launch_mh( kr_ctx * c, cudaStream_t st, const args_t< R > & a, int i0, int i1, int stage )
 {
-    for( int j = i0; j < i1; j += 65535 )      // one CTA row per holder
-        k_mh< R, KIND ><<< dim3( blocks_for( c->mh_items, 128 ), unsigned( std::min( i1 - j, 65535 ) ) ), 128, 0, st >>>(
-            a, c->mh_list + j, stage );
+    if( i1 > i0 )
+        k_mh< R, KIND ><<< blocks_for( i1 - i0, 256 ), 256, 0, st >>>( a, c->mh_list, c->mh_work + i0, i1 - i0, stage );
 }
 
 template< bool MHD, class R, class T >
@@ -2094,11 +2094,23 @@ static void enqueue_back( kr_ctx * c, cudaStream_t st, const args_t< R > & a, in
         {   // refined MHD: every ghost by the exchange holders (keeper.cpp:148-160
             // act_bnd: restrictions, same-level copies, prolongations by the
             // coarser host's level, the restrictions' second pass)
+            auto sides = [ & ]( int field )
+            {   // keeper.cpp:148-157 and mhd/boundary/keeper.h:304-309
+                for( int side = 0; side < 6; ++ side )
+                    if( c->cfg.bc[ side ] != KR_BC_PER )
+                    {
+                        const int ax = side / 2;
+                        const long long rows = ( long long )( n[ ( ax + 1 ) % 3 ] + 4 ) * ( n[ ( ax + 2 ) % 3 ] + 4 );
+                        k_phys_mhd< R ><<< dim3( blocks_for( rows, 128 ), nb ), 128, 0, st >>>( a, side, stage, field );
+                    }
+            };
             launch_mh< R, MH_RESTRICT >( c, st, a, c->mh_restrict[ 0 ], c->mh_restrict[ 1 ], stage );
+            sides( 1 );
             launch_mh< R, MH_SAME >( c, st, a, c->mh_same[ 0 ], c->mh_same[ 1 ], stage );
             for( size_t l = 0; l + 1 < c->mh_prolong.size(  ); ++ l )
                 launch_mh< R, MH_PROLONG >( c, st, a, c->mh_prolong[ l ], c->mh_prolong[ l + 1 ], stage );
             launch_mh< R, MH_RESTRICT >( c, st, a, c->mh_restrict[ 0 ], c->mh_restrict[ 1 ], stage );
+            sides( 0 );
             return;
         }
         if( c->n_restrict )            // finer -> coarser ghosts
@@ -2407,9 +2419,7 @@ static bool build_tree( const kr_cfg * cfg, int n_regions, const kr_region * reg
     if( tree.max_level == 0 )
         return true;
     const char * why = nullptr;
-    if( cfg->mhd && ! ( per[ 0 ] && per[ 1 ] && per[ 2 ] ) )
-        why = "static refinement of an MHD mesh needs periodic sides";
-    else if( cfg->mhd && cfg->riemann == KR_RIEMANN_LEARNED )
+    if( cfg->mhd && cfg->riemann == KR_RIEMANN_LEARNED )
         why = "the learned face selector runs on uniform meshes";
     else if( ranks_of( * cfg ) > 1 || ( cfg->flags & KR_FLAG_HALO_ALL ) )
         why = "static refinement runs on one rank, without KR_FLAG_HALO_ALL";
@@ -2565,6 +2575,7 @@ static kr_ctx * create_ctx( const kr_cfg * cfg, int n_regions, const kr_region *
     const bool halo_all = ( cfg->flags & KR_FLAG_HALO_ALL ) != 0;
     std::vector< smr_item_t > smr_items;
     std::vector< mh_t > mh_plan_h;
+    std::vector< uint2 > mh_work_h;
     if( smr )
     {   // the tree's leaves, one rank, no halo exchange
         c->smr = true;
@@ -2590,8 +2601,7 @@ static kr_ctx * create_ctx( const kr_cfg * cfg, int n_regions, const kr_region *
             c->mh_prolong = mp.prolong;
             c->mh_waves = mp.waves;
             mh_plan_h.swap( mp.list );
-            for( const mh_t & h : mh_plan_h )
-                c->mh_items = std::max( { c->mh_items, h.nbx * h.nby * h.nth, h.fbx * h.fby * h.fth } );
+            mh_work_h.swap( mp.work );
         }
         if( smr_items.size(  ) > 65535 )
         {   // one grid row per item
@@ -2651,7 +2661,10 @@ static kr_ctx * create_ctx( const kr_cfg * cfg, int n_regions, const kr_region *
     if( ok && ! mh_plan_h.empty(  ) )
         ok = ck( c, cudaMalloc( & c->mh_list, mh_plan_h.size(  ) * sizeof( mh_t ) ), "malloc exchange holders" )
           && ck( c, cudaMemcpyAsync( c->mh_list, mh_plan_h.data(  ), mh_plan_h.size(  ) * sizeof( mh_t ),
-                                     cudaMemcpyHostToDevice, c->stream ), "upload exchange holders" );
+                                     cudaMemcpyHostToDevice, c->stream ), "upload exchange holders" )
+          && ck( c, cudaMalloc( & c->mh_work, mh_work_h.size(  ) * sizeof( uint2 ) ), "malloc exchange items" )
+          && ck( c, cudaMemcpyAsync( c->mh_work, mh_work_h.data(  ), mh_work_h.size(  ) * sizeof( uint2 ),
+                                     cudaMemcpyHostToDevice, c->stream ), "upload exchange items" );
     // halo exchange: item lists and buffers (1-word minimum keeps pointers valid)
     {
         const halo_side_t * hs[ 2 ] = { & c->hsend, & c->hrecv };
@@ -2799,7 +2812,7 @@ void kr_ctx_destroy( kr_ctx * c )
     if( c->stream ) cudaStreamSynchronize( c->stream );
     drop_graph( c );                   // before the communicator its graph uses
     if( c->comm ) nccl(  ).CommDestroy( c->comm );
-    cudaFree( c->gid ); cudaFree( c->smr_items ); cudaFree( c->favg ); cudaFree( c->mh_list );
+    cudaFree( c->gid ); cudaFree( c->smr_items ); cudaFree( c->favg ); cudaFree( c->mh_list ); cudaFree( c->mh_work );
     cudaFree( c->send_items ); cudaFree( c->recv_items );
     cudaFree( c->send_w ); cudaFree( c->recv_w ); cudaFree( c->send_b ); cudaFree( c->recv_b );
     for( int s = 0; s < 2; ++ s ) { cudaFree( c->u[ s ] ); cudaFree( c->bf[ s ] ); }
@@ -3230,7 +3243,7 @@ int kr_launches_per_step( kr_ctx * c )
     int phys = ! c->cfg.mhd && has_phys( c ) ? 1 : 0;
     if( c->cfg.mhd )
         for( int s = 0; s < 6; ++ s )
-            phys += c->cfg.bc[ s ] != KR_BC_PER;
+            phys += ( c->cfg.bc[ s ] != KR_BC_PER ) * ( c->mh_list ? 2 : 1 );   // refined MHD: two passes
     int smr = 0;
     if( c->smr && c->mh_list )
     {   // refined MHD: restrictions (two passes), copies, prolongations by

@@ -20,11 +20,11 @@
 // launch grid of each (resource_pack / resource_flux / resource_edge, at most
 // MH_TH threads per CTA row, the last CTA's second pass).  A phase of the
 // exchange (copies, restrictions, prolongations by the coarser host's level)
-// is one launch whose CTA rows are the phase's holders; inside a phase no two
-// holders write the same slot (each writes its own guest's band), so the
-// launch order of their items does not matter.  The edge-E correction reads
-// what earlier holders of the same blocks wrote back, so its holders run in
-// waves: a holder waits for every earlier holder that shares a block with it.
+// is one launch of one thread per work item (holder, item); inside a phase no
+// two holders write the same slot (each writes its own guest's band), so the
+// order of the items does not matter.  The edge-E correction reads what
+// earlier holders wrote back, so its holders run in waves: a holder waits for
+// every earlier holder that reads or writes one of its edges.
 //
 // Every written ghost cell also gets its cell E, B x v from the written
 // primitives (mhd/integrator/integrator.h:201-213 computes a ghost cell's E
@@ -433,24 +433,26 @@ void mh_edge_e( const args_t< R > & a, const mh_t & h, int bx, int by, int tx, c
     }
 }
 
-// One phase: CTA row blockIdx.y is holder list[ blockIdx.y ]; its items are
-// the (CTA row, CTA, thread) triples of the reference's launch of it.
+// One phase: one thread per work item (holder, item), the items of a holder
+// being the (CTA row, CTA, thread) triples of the reference's launch of it.
 template< class R, int KIND >
-__global__ void __launch_bounds__( 128 ) k_mh( const args_t< R > a, const mh_t * list, int step )
+__global__ void __launch_bounds__( 256 ) k_mh( const args_t< R > a, const mh_t * list, const uint2 * work, int n_work,
+                                              int step )
 {
-    const mh_t h = list[ blockIdx.y ];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if( t >= n_work )
+        return;
+    const uint2 wk = work[ t ];
+    const mh_t & h = list[ wk.x ];
     const int n[ 3 ] = { a.n0, a.n1, a.n2 };
-    const int bx_n = KIND == MH_FLUX ? h.fbx : h.nbx, by_n = KIND == MH_FLUX ? h.fby : h.nby;
+    const int bx_n = KIND == MH_FLUX ? h.fbx : h.nbx;
     const int th_n = KIND == MH_FLUX ? h.fth : h.nth;
-    const int items = bx_n * by_n * th_n;
-    for( int t = blockIdx.x * blockDim.x + threadIdx.x; t < items; t += gridDim.x * blockDim.x )
-    {
-        const int tx = t % th_n, bx = ( t / th_n ) % bx_n, by = t / ( th_n * bx_n );
-        if constexpr( KIND == MH_SAME )     mh_same( a, h, step, bx, by, tx, n );
-        if constexpr( KIND == MH_RESTRICT ) mh_restrict( a, h, step, bx, by, tx, n );
-        if constexpr( KIND == MH_PROLONG )  mh_prolong( a, h, step, bx, by, tx, n );
-        if constexpr( KIND == MH_FLUX )     mh_edge_e( a, h, bx, by, tx, n );
-    }
+    const int it = int( wk.y );
+    const int tx = it % th_n, bx = ( it / th_n ) % bx_n, by = it / ( th_n * bx_n );
+    if constexpr( KIND == MH_SAME )     mh_same( a, h, step, bx, by, tx, n );
+    if constexpr( KIND == MH_RESTRICT ) mh_restrict( a, h, step, bx, by, tx, n );
+    if constexpr( KIND == MH_PROLONG )  mh_prolong( a, h, step, bx, by, tx, n );
+    if constexpr( KIND == MH_FLUX )     mh_edge_e( a, h, bx, by, tx, n );
 }
 
 ////////////////////////////////////////////////////////////
@@ -631,53 +633,128 @@ static std::vector< mh_t > mh_holders( const kr_tree & t, const int * n )
     return out;
 }
 
+// The edges (block, component, index) that a finer host's edge-E correction
+// reads or writes, as 64-bit keys (the index arithmetic of mh_edge_e).
+static void mh_edge_keys( const mh_t & h, const int * n, std::vector< unsigned long long > & keys )
+{
+    auto key = [ & ]( int b, int c, const int * i )
+    {
+        return ( ( ( unsigned long long ) b * 3 + c ) << 33 )
+             | ( ( unsigned long long )( i[ 0 ] + 1 ) << 22 ) | ( ( unsigned long long )( i[ 1 ] + 1 ) << 11 )
+             | ( unsigned long long )( i[ 2 ] + 1 );
+    };
+    keys.clear(  );
+    const int ax = h.ax[ 0 ], a1 = h.ax[ 1 ];
+    for( int by = 0; by < h.fby; ++ by )
+    for( int bx = 0; bx < h.fbx; ++ bx )
+    for( int tx = 0; tx < h.fth; ++ tx )
+    {
+        int i0[ 3 ], im[ 3 ], ib[ 3 ];
+        i0[ ax ] = 0; i0[ a1 ] = bx * h.fth + tx; i0[ h.ax[ 2 ] ] = by;
+        if( h.mode == 1 )
+        {
+            if( i0[ a1 ] >= n[ a1 ] / 2 )
+                continue;
+            for( int d = 0; d < 3; ++ d ) { im[ d ] = h.oes[ d ] + 2 * i0[ d ]; ib[ d ] = h.oec[ d ] + i0[ d ]; }
+            keys.push_back( key( h.guest, a1, ib ) );
+            keys.push_back( key( h.host, a1, im ) );
+            ++ im[ a1 ];
+            keys.push_back( key( h.host, a1, im ) );
+            continue;
+        }
+        for( int d = 0; d < 3; ++ d ) { im[ d ] = 2 * i0[ d ] + h.oes[ d ]; ib[ d ] = i0[ d ] + h.oec[ d ]; }
+        const int jmax = ( bx == h.fbx - 1 ) + 1;
+        const int ib_max = n[ a1 ] / 2 + ( h.oec[ a1 ] > 1 );
+        for( int j = 0; j < jmax && i0[ a1 ] < ib_max; ++ j )
+        {
+            im[ a1 ] = 2 * i0[ a1 ] + h.oes[ a1 ];
+            for( int q = 0; q < 3; ++ q )
+            {
+                const int am = h.ax[ ( ax + q ) % 3 ];
+                if( am == ax )
+                    continue;
+                keys.push_back( key( h.guest, am, ib ) );
+                keys.push_back( key( h.host, am, im ) );
+                ++ im[ am ];
+                keys.push_back( key( h.host, am, im ) );
+                -- im[ am ];
+            }
+            ib[ a1 ] += h.fth;
+            i0[ a1 ] += h.fth;
+        }
+    }
+}
+
 // The launch lists of a refined MHD mesh: copies, restrictions, the
 // prolongations grouped by the coarser host's level, and the edge-E
-// correction's waves; offsets into one device array.
+// correction's waves (a holder runs after every earlier holder that touches
+// one of its edges).  Every segment of holders is also flattened into work
+// items (holder, item) for one thread each.
 struct mh_plan_t
 {
     std::vector< mh_t > list;
-    int same[ 2 ] = { 0, 0 }, restrict_[ 2 ] = { 0, 0 };
-    std::vector< int > prolong;          // [levels + 1] offsets
-    std::vector< int > waves;            // [waves + 1] offsets
+    std::vector< uint2 > work;
+    int same[ 2 ] = { 0, 0 }, restrict_[ 2 ] = { 0, 0 };     // work-item ranges
+    std::vector< int > prolong;          // [levels + 1] work offsets
+    std::vector< int > waves;            // [waves + 1] work offsets
 };
 
 static mh_plan_t mh_plan( const kr_tree & t, const int * n )
 {
     const std::vector< mh_t > hs = mh_holders( t, n );
     mh_plan_t p;
-    auto add = [ & ]( auto pred ) { for( const mh_t & h : hs ) if( pred( h ) ) p.list.push_back( h ); };
-    p.same[ 0 ] = int( p.list.size(  ) );
-    add( []( const mh_t & h ) { return h.d_lvl == 0; } );
-    p.same[ 1 ] = p.restrict_[ 0 ] = int( p.list.size(  ) );
-    add( []( const mh_t & h ) { return h.d_lvl < 0; } );
-    p.restrict_[ 1 ] = int( p.list.size(  ) );
-    p.prolong.push_back( int( p.list.size(  ) ) );
-    for( int l = 0; l < t.max_level; ++ l )
+    auto add = [ & ]( const mh_t & h, bool flux )
     {
-        add( [ & ]( const mh_t & h ) { return h.d_lvl > 0 && t.level[ h.host ] == l; } );
-        p.prolong.push_back( int( p.list.size(  ) ) );
-    }
+        const unsigned idx = unsigned( p.list.size(  ) );
+        p.list.push_back( h );
+        const int items = flux ? h.fbx * h.fby * h.fth : h.nbx * h.nby * h.nth;
+        for( int k = 0; k < items; ++ k )
+            p.work.push_back( make_uint2( idx, unsigned( k ) ) );
+    };
+    auto phase = [ & ]( auto pred, bool flux )
+    {
+        for( const mh_t & h : hs )
+            if( pred( h ) )
+                add( h, flux );
+        return int( p.work.size(  ) );
+    };
+    p.same[ 0 ] = 0;
+    p.same[ 1 ] = p.restrict_[ 0 ] = phase( []( const mh_t & h ) { return h.d_lvl == 0; }, false );
+    p.restrict_[ 1 ] = phase( []( const mh_t & h ) { return h.d_lvl < 0; }, false );
+    p.prolong.push_back( p.restrict_[ 1 ] );
+    for( int l = 0; l < t.max_level; ++ l )
+        p.prolong.push_back( phase( [ & ]( const mh_t & h ) { return h.d_lvl > 0 && t.level[ h.host ] == l; }, false ) );
     // edge-E waves, in holder order
-    std::vector< mh_t > fx;
+    std::vector< const mh_t * > fx;
     for( const mh_t & h : hs )
         if( h.d_lvl < 0 && h.mode < 2 )
-            fx.push_back( h );
-    std::vector< int > wave( fx.size(  ), 0 ), last( t.nblk, -1 );   // last: a block's latest wave
+            fx.push_back( & h );
+    std::vector< int > wave( fx.size(  ), 0 );
+    std::unordered_map< unsigned long long, int > last;
+    std::vector< unsigned long long > keys;
     int n_wave = 0;
     for( size_t q = 0; q < fx.size(  ); ++ q )
     {
-        wave[ q ] = std::max( last[ fx[ q ].host ], last[ fx[ q ].guest ] ) + 1;
-        last[ fx[ q ].host ] = last[ fx[ q ].guest ] = wave[ q ];
-        n_wave = std::max( n_wave, wave[ q ] + 1 );
+        mh_edge_keys( * fx[ q ], n, keys );
+        int w = 0;
+        for( unsigned long long k : keys )
+        {
+            auto it = last.find( k );
+            if( it != last.end(  ) )
+                w = std::max( w, it->second + 1 );
+        }
+        wave[ q ] = w;
+        for( unsigned long long k : keys )
+            last[ k ] = w;
+        n_wave = std::max( n_wave, w + 1 );
     }
-    p.waves.push_back( int( p.list.size(  ) ) );
+    p.waves.push_back( int( p.work.size(  ) ) );
     for( int w = 0; w < n_wave; ++ w )
     {
         for( size_t q = 0; q < fx.size(  ); ++ q )
             if( wave[ q ] == w )
-                p.list.push_back( fx[ q ] );
-        p.waves.push_back( int( p.list.size(  ) ) );
+                add( * fx[ q ], true );
+        p.waves.push_back( int( p.work.size(  ) ) );
     }
     return p;
 }

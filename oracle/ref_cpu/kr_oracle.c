@@ -511,7 +511,7 @@ static inline int nbr_block( const kro_mesh * m, int b, const int sh[ 3 ] )
     return reg[ 0 ] + m->c.nb[ 0 ] * ( reg[ 1 ] + m->c.nb[ 1 ] * reg[ 2 ] );
 }
 
-typedef struct { int step; } ghost_arg;
+typedef struct { int step; int no_field; } ghost_arg;   /* no_field: MHD sides, primitives only */
 
 static void ghost_block( kro_mesh * m, int b, void * aux )
 {
@@ -1514,16 +1514,21 @@ static void mh_edge_efield( kro_mesh * m, const mh_holder * h )
  * restrictions, the same-level copies, the prolongations (which read the
  * coarser hosts' ghosts filled before), the restrictions again (their
  * second pass, keeper.cpp:121-127 q_plgt.unpk), each in holder order. */
+static void bc_block_mhd( kro_mesh * m, int b, void * aux );
+
 static void mh_act_bnd( kro_mesh * m, int step )
 {
+    ghost_arg pass1 = { step, 0 }, pass2 = { step, 1 };
     for( int k = 0; k < m->n_hold; ++ k )
         if( m->hold[ k ].d_lvl < 0 ) mh_to_coarser( m, m->hold + k, step );
+    par_blocks( m, bc_block_mhd, & pass1 );      /* keeper.cpp:148-157: the sides, then the copies */
     for( int k = 0; k < m->n_hold; ++ k )
         if( m->hold[ k ].d_lvl == 0 ) mh_to_same( m, m->hold + k, step );
     for( int k = 0; k < m->n_hold; ++ k )
         if( m->hold[ k ].d_lvl > 0 ) mh_to_finer( m, m->hold + k, step );
     for( int k = 0; k < m->n_hold; ++ k )
         if( m->hold[ k ].d_lvl < 0 ) mh_to_coarser( m, m->hold + k, step );
+    par_blocks( m, bc_block_mhd, & pass2 );      /* mhd/boundary/keeper.h:304-309: primitives again */
 }
 
 /* keeper.cpp:162-166 act_flx: the finer hosts' face and edge holders */
@@ -1559,17 +1564,17 @@ static void mh_act_flx( kro_mesh * m )
 static void bc_block_mhd( kro_mesh * m, int b, void * aux )
 {
     const int step = ( ( ghost_arg * ) aux )->step;
+    const int field = ! ( ( ghost_arg * ) aux )->no_field;  /* phys.h:199-249: step >= 0 */
     const int * n = m->c.n;
     const int nw = m->nw;
-    const int reg[ 3 ] = { b % m->c.nb[ 0 ], ( b / m->c.nb[ 0 ] ) % m->c.nb[ 1 ],
-                           b / ( m->c.nb[ 0 ] * m->c.nb[ 1 ] ) };
+    const int * reg = blk_reg( m, b );
     double * w = m->w + ( size_t ) b * m->nw_cells * nw;
     double * bf = m->bf[ step ] + ( size_t ) b * m->nbf;
     int phy[ 3 ][ 2 ];                       /* geo.phybnd_flag */
     for( int a = 0; a < 3; ++ a )
     {
         phy[ a ][ 0 ] = m->c.bc[ 2 * a ] != KRO_PER && reg[ a ] == 0;
-        phy[ a ][ 1 ] = m->c.bc[ 2 * a + 1 ] != KRO_PER && reg[ a ] == m->c.nb[ a ] - 1;
+        phy[ a ][ 1 ] = m->c.bc[ 2 * a + 1 ] != KRO_PER && reg[ a ] == blk_lim( m, b, a ) - 1;
     }
     for( int side = 0; side < 6; ++ side )
     {
@@ -1654,6 +1659,8 @@ static void bc_block_mhd( kro_mesh * m, int b, void * aux )
                 for( int q = 0; q < 3; ++ q )
                 {
                     ht[ BCC + q ] = bc[ 2 + i ][ q ];
+                    if( ! field )
+                        continue;
                     if( q == axis )
                         bf[ ib( m, i_fbc[ 0 ], i_fbc[ 1 ], i_fbc[ 2 ] ) + q ] = bfb[ 2 + i ][ q ];
                     else
@@ -2261,9 +2268,8 @@ static void emf_block( kro_mesh * m, int b, void * aux )
             if( i[ a ] != n[ a ] || n[ a ] < 2 )
                 continue;
             const int kind = m->c.bc[ 2 * a + 1 ];
-            const int reg_a = a == 0 ? b % m->c.nb[ 0 ]
-                            : a == 1 ? ( b / m->c.nb[ 0 ] ) % m->c.nb[ 1 ] : b / ( m->c.nb[ 0 ] * m->c.nb[ 1 ] );
-            if( kind == KRO_PER || reg_a != m->c.nb[ a ] - 1 || ( kind != KRO_OUT && kind != KRO_FRE ) )
+            const int reg_a = blk_reg( m, b )[ a ];
+            if( kind == KRO_PER || reg_a != blk_lim( m, b, a ) - 1 || ( kind != KRO_OUT && kind != KRO_FRE ) )
                 continue;
             int jc[ 3 ] = { i[ 0 ], i[ 1 ], i[ 2 ] };
             -- jc[ a ];
@@ -2327,10 +2333,6 @@ static void ct_block( kro_mesh * m, int b, void * aux )
 
 int kro_step( kro_mesh * m, int n_steps, double * t, double * dt_bound, double * dt_last )
 {
-    if( m->c.mhd && m->smr )
-        for( int a = 0; a < 3; ++ a )
-            if( ! periodic_axis( m, a ) )
-                return -2;        /* refined MHD meshes: periodic domains only */
     for( int s = 0; s < n_steps; ++ s )
     {
         double dt_use = 0;

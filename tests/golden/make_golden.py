@@ -110,6 +110,16 @@ CASES = [
     # t = 0 (kratos_b200/amr.py; 2^3 roots of 8^3, two levels, 120 blocks)
     ("smr_blast", "blast", (2, 2, 2), (8, 8, 8), 4, 15, 1.6666666666666667,
      {"regions": gradient_regions((2, 2, 2), (8, 8, 8), 2), "bnd_thread_limit": "4"}, "sums"),
+    # refined MHD with physical sides: outflow / free along x, reflecting along
+    # y, the level-1 region touching the x- and y- sides
+    ("smr_ot_bc", "ot", (2, 2, 2), (8, 8, 8), 4, 16, 1.6666666666666667,
+     {"kinds": "out fre ref ref per per", "bnd_thread_limit": "4",
+      "regions": [(1, (0.05, 0.05, 0.3), (0.2, 0.2, 0.6))]}, "final"),
+    # refined MHD with fixed (inflowing) z sides, the region touching both
+    ("smr_ot_fix", "ot", (2, 1, 2), (8, 8, 8), 4, 17, 1.6666666666666667,
+     {"kinds": "per per per per fixd fixd", "bnd_thread_limit": "4",
+      "init": {"rho0": "0.2", "pre0": "0.15", "vel0": "0.3 -0.2 0.1", "b0": "0.1 0.05 0.2"},
+      "regions": [(1, (0.55, 0.3, 0.05), (0.7, 0.6, 0.95))]}, "final"),
     # three levels (a level-2 region inside a level-1 one)
     ("smr_3lvl", "shock", (1, 1, 1), (8, 8, 8), 4, 12, 1.4,
      {"regions": [(2, (0.3, 0.3, 0.3), (0.3, 0.3, 0.3))]}, "final"),

@@ -7,7 +7,7 @@ import numpy as np
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 CASES = ["shock_16", "ot_16", "ot_ragged", "shock_floor", "shock_c1", "ot_64",
          "shock_bc", "shock_fixd", "ot_bc_out", "ot_bc_ref", "ot_bc_fre", "ot_bc_fix", "ot_bc_fix0",
-         "smr_shock", "smr_bc", "smr_3lvl", "smr_ot", "smr_ot3", "smr_ot_slab", "smr_blast",
+         "smr_shock", "smr_bc", "smr_3lvl", "smr_ot", "smr_ot3", "smr_ot_slab", "smr_blast", "smr_ot_bc", "smr_ot_fix",
          "turb_16", "turb_32", "box_5", "box_1", "box_3"]
 # MHD workloads
 MHD_WORKLOADS = ("ot", "turb", "box", "blast")
@@ -15,7 +15,7 @@ MHD_WORKLOADS = ("ot", "turb", "box", "blast")
 BOX_CASES = {"box_5": 5, "box_1": 1, "box_3": 3}
 # statically refined MHD fixtures (two and three levels; the blast's mesh from
 # the gradient criterion, kratos_b200/amr.py)
-MHD_SMR_CASES = ["smr_ot", "smr_ot3", "smr_ot_slab", "smr_blast"]
+MHD_SMR_CASES = ["smr_ot", "smr_ot3", "smr_ot_slab", "smr_blast", "smr_ot_bc", "smr_ot_fix"]
 # statically refined fixtures (blocks in tree order, with level / reg arrays)
 SMR_CASES = ["smr_shock", "smr_bc", "smr_3lvl"]
 

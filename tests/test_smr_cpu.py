@@ -15,7 +15,6 @@ def _refined(mhd=False, nb=(2, 2, 2), n=(8, 8, 8), regions=REG, **kw):
 
 
 @pytest.mark.parametrize("kw,msg", [
-    (dict(mhd=True, kinds=("out", "out", "per", "per", "per", "per")), "needs periodic sides"),
     (dict(mhd=True, riemann=2), "uniform meshes"),
     (dict(n_ranks=2, rank=0), "one rank"),
     (dict(flags=2), "one rank"),
