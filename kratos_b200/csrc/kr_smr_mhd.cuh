@@ -44,6 +44,7 @@ struct mh_t
     int nbx, nby, nth;                   // launch grid of the holder's exchange kernel
     int fbx, fby, fth;                   // and of its edge-E correction
     int n1;                              // the exchange grid's extent along ax[ 1 ]
+    int wx[ 3 ], bx[ 3 ];                // same level: the boxes of W and face-B copies (x, y, z)
 };
 
 __device__ __forceinline__ void mh_dispatch( const mh_t & h, int nth, int bx, int by, int tx, int * i )
@@ -112,7 +113,42 @@ __device__ __forceinline__ bool mh_in_band( int i, int off )
     return off == 0 || ( i - off >= 0 && i - off < MH_ORD );
 }
 
-// same level (hydro comm_functions.h:306-327 to_same; MHD 422-465)
+// same level (hydro comm_functions.h:306-327 to_same; MHD 422-465), over the
+// copies' own boxes with x fastest: the reference's rows run across y or z
+// for x-side holders, which would leave every thread of a warp on its own
+// cache line; a same-level holder's copies are disjoint, so their order is
+// free.  Item `it` < the W box's size: one cell of W (11 words, E included);
+// then, for face holders, one face of the tangential face B.
+template< class R > __device__ __forceinline__
+void mh_same_box( const args_t< R > & a, const mh_t & h, int step, int it )
+{
+    const int a1 = h.ax[ 1 ], a2 = h.ax[ 2 ];
+    const int nw = h.wx[ 0 ] * h.wx[ 1 ] * h.wx[ 2 ];
+    int c[ 3 ], im[ 3 ], ib[ 3 ];
+    if( it < nw )
+    {
+        c[ 0 ] = it % h.wx[ 0 ]; c[ 1 ] = ( it / h.wx[ 0 ] ) % h.wx[ 1 ]; c[ 2 ] = it / ( h.wx[ 0 ] * h.wx[ 1 ] );
+        for( int d = 0; d < 3; ++ d )
+        {
+            im[ d ] = h.os[ d ] + c[ d ];
+            ib[ d ] = h.oc[ d ] + c[ d ];
+        }
+        for( int k = 0; k < 11; ++ k )
+            * mh_w( a, h.guest, k, ib ) = * mh_w( a, h.host, k, im );
+        return;
+    }
+    it -= nw;
+    c[ 0 ] = it % h.bx[ 0 ]; c[ 1 ] = ( it / h.bx[ 0 ] ) % h.bx[ 1 ]; c[ 2 ] = it / ( h.bx[ 0 ] * h.bx[ 1 ] );
+    for( int d = 0; d < 3; ++ d )
+    {
+        im[ d ] = h.obs[ d ] + c[ d ];
+        ib[ d ] = h.obc[ d ] + c[ d ];
+    }
+    * mh_bf( a, step, h.guest, a1, ib ) = * mh_bf( a, step, h.host, a1, im );
+    * mh_bf( a, step, h.guest, a2, ib ) = * mh_bf( a, step, h.host, a2, im );
+}
+
+// the same copies in the reference's row order (kept for reading against it)
 template< class R > __device__ __forceinline__
 void mh_same( const args_t< R > & a, const mh_t & h, int step, int bx, int by, int tx, const int * n )
 {
@@ -448,8 +484,12 @@ __global__ void __launch_bounds__( 256 ) k_mh( const args_t< R > a, const mh_t *
     const int bx_n = KIND == MH_FLUX ? h.fbx : h.nbx;
     const int th_n = KIND == MH_FLUX ? h.fth : h.nth;
     const int it = int( wk.y );
+    if constexpr( KIND == MH_SAME )
+    {
+        mh_same_box( a, h, step, it );
+        return;
+    }
     const int tx = it % th_n, bx = ( it / th_n ) % bx_n, by = it / ( th_n * bx_n );
-    if constexpr( KIND == MH_SAME )     mh_same( a, h, step, bx, by, tx, n );
     if constexpr( KIND == MH_RESTRICT ) mh_restrict( a, h, step, bx, by, tx, n );
     if constexpr( KIND == MH_PROLONG )  mh_prolong( a, h, step, bx, by, tx, n );
     if constexpr( KIND == MH_FLUX )     mh_edge_e( a, h, bx, by, tx, n );
@@ -529,6 +569,21 @@ static mh_t mh_make( int host, int guest, int d_lvl, const int * x, const int * 
     {
         nc[ a2 ] = MH_NGH;
         if( h.mode > 1 ) nc[ a1 ] = MH_NGH;
+    }
+    // same level: the boxes the reference's rows cover (to_same's W rows: ORD
+    // along ax[ 0 ], the row extent along ax[ 1 ], n or ORD rows along ax[ 2 ];
+    // face B of face holders: 1 x (n + 1) x (n + 1))
+    if( d_lvl == 0 )
+    {
+        h.wx[ ax ] = MH_ORD;
+        h.wx[ a1 ] = nc[ a1 ];
+        h.wx[ a2 ] = h.mode == 0 ? n[ a2 ] : MH_ORD;
+        if( h.mode == 0 )
+        {
+            h.bx[ ax ] = 1;
+            h.bx[ a1 ] = n[ a1 ] + 1;
+            h.bx[ a2 ] = n[ a2 ] + 1;
+        }
     }
     h.n1 = nc[ a1 ];
     h.nth = mh_grid_th( nc[ a1 ] );
@@ -707,7 +762,9 @@ static mh_plan_t mh_plan( const kr_tree & t, const int * n )
     {
         const unsigned idx = unsigned( p.list.size(  ) );
         p.list.push_back( h );
-        const int items = flux ? h.fbx * h.fby * h.fth : h.nbx * h.nby * h.nth;
+        const int items = flux ? h.fbx * h.fby * h.fth
+                        : h.d_lvl == 0 ? h.wx[ 0 ] * h.wx[ 1 ] * h.wx[ 2 ] + h.bx[ 0 ] * h.bx[ 1 ] * h.bx[ 2 ]
+                                       : h.nbx * h.nby * h.nth;
         for( int k = 0; k < items; ++ k )
             p.work.push_back( make_uint2( idx, unsigned( k ) ) );
     };
