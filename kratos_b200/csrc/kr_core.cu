@@ -1932,7 +1932,7 @@ struct kr_ctx
     // refined MHD: the exchange holders (kr_smr_mhd.cuh)
     mh_t * mh_list = nullptr;
     uint2 * mh_work = nullptr;         // (holder, item) per thread, phase by phase
-    int mh_same[ 2 ] = { 0, 0 }, mh_restrict[ 2 ] = { 0, 0 };   // work-item ranges
+    int mh_restrict[ 2 ] = { 0, 0 };   // work-item range
     std::vector< int > mh_prolong, mh_waves;
 };
 
@@ -2104,9 +2104,9 @@ static void enqueue_back( kr_ctx * c, cudaStream_t st, const args_t< R > & a, in
                         k_phys_mhd< R ><<< dim3( blocks_for( rows, 128 ), nb ), 128, 0, st >>>( a, side, stage, field );
                     }
             };
+            // (the same-level copies were pushed by k_c2p and the CT update)
             launch_mh< R, MH_RESTRICT >( c, st, a, c->mh_restrict[ 0 ], c->mh_restrict[ 1 ], stage );
             sides( 1 );
-            launch_mh< R, MH_SAME >( c, st, a, c->mh_same[ 0 ], c->mh_same[ 1 ], stage );
             for( size_t l = 0; l + 1 < c->mh_prolong.size(  ); ++ l )
                 launch_mh< R, MH_PROLONG >( c, st, a, c->mh_prolong[ l ], c->mh_prolong[ l + 1 ], stage );
             launch_mh< R, MH_RESTRICT >( c, st, a, c->mh_restrict[ 0 ], c->mh_restrict[ 1 ], stage );
@@ -2576,6 +2576,7 @@ static kr_ctx * create_ctx( const kr_cfg * cfg, int n_regions, const kr_region *
     std::vector< smr_item_t > smr_items;
     std::vector< mh_t > mh_plan_h;
     std::vector< uint2 > mh_work_h;
+    std::vector< int > mh_same_h;      // (block, direction, neighbour) of same-level pairs
     if( smr )
     {   // the tree's leaves, one rank, no halo exchange
         c->smr = true;
@@ -2596,12 +2597,12 @@ static kr_ctx * create_ctx( const kr_cfg * cfg, int n_regions, const kr_region *
         if( cfg->mhd )
         {
             mh_plan_t mp = mh_plan( tree, cfg->n );
-            c->mh_same[ 0 ] = mp.same[ 0 ]; c->mh_same[ 1 ] = mp.same[ 1 ];
             c->mh_restrict[ 0 ] = mp.restrict_[ 0 ]; c->mh_restrict[ 1 ] = mp.restrict_[ 1 ];
             c->mh_prolong = mp.prolong;
             c->mh_waves = mp.waves;
             mh_plan_h.swap( mp.list );
             mh_work_h.swap( mp.work );
+            mh_same_h.swap( mp.same_nbr );
         }
         if( smr_items.size(  ) > 65535 )
         {   // one grid row per item
@@ -2736,7 +2737,8 @@ static kr_ctx * create_ctx( const kr_cfg * cfg, int n_regions, const kr_region *
         for( int k = 0; k < 27; ++ k )
         {
             if( smr )
-            {   // refined MHD: the exchange holders fill every ghost, no push
+            {   // refined MHD: same-level neighbours in all 26 directions by push
+                // (below, from the holders), the level jumps by the exchange
                 const int sh[ 3 ] = { k % 3 - 1, ( k / 3 ) % 3 - 1, k / 9 - 1 };
                 const int nz = ( sh[ 0 ] != 0 ) + ( sh[ 1 ] != 0 ) + ( sh[ 2 ] != 0 );
                 int v = k == 13 ? b : -3;
@@ -2768,6 +2770,8 @@ static kr_ctx * create_ctx( const kr_cfg * cfg, int n_regions, const kr_region *
             const int src = nbr_global( * cfg, c->gid_h[ b ], k );
             nbr[ b * 27 + k ] = src < 0 ? -1 : ( owner[ src ] == c->rank && ! ( halo_all && k != 13 ) ? local[ src ] : -2 );
         }
+    for( const int * h = mh_same_h.data(  ); h < mh_same_h.data(  ) + mh_same_h.size(  ); h += 3 )
+        nbr[ h[ 0 ] * 27 + h[ 1 ] ] = h[ 2 ];
     std::vector< scal_t > s0( c->nscal, scal_t{} );
     for( scal_t & r : s0 )
         r.dt_bound = cfg->dt_init >= FLT_MIN ? cfg->dt_init : FLT_MAX / 10;   // cycle.cpp:163-166
@@ -3248,7 +3252,7 @@ int kr_launches_per_step( kr_ctx * c )
     if( c->smr && c->mh_list )
     {   // refined MHD: restrictions (two passes), copies, prolongations by
         // level, the flux average and the edge-E waves
-        smr = 2 * ( c->mh_restrict[ 1 ] > c->mh_restrict[ 0 ] ) + ( c->mh_same[ 1 ] > c->mh_same[ 0 ] )
+        smr = 2 * ( c->mh_restrict[ 1 ] > c->mh_restrict[ 0 ] )
             + ( c->n_restrict ? 1 : 0 ) + int( c->mh_waves.size(  ) ) - 1;
         for( size_t l = 0; l + 1 < c->mh_prolong.size(  ); ++ l )
             smr += c->mh_prolong[ l + 1 ] > c->mh_prolong[ l ];

@@ -19,10 +19,13 @@
 // each host's neighbours by their direction flags), with the reference's
 // launch grid of each (resource_pack / resource_flux / resource_edge, at most
 // MH_TH threads per CTA row, the last CTA's second pass).  A phase of the
-// exchange (copies, restrictions, prolongations by the coarser host's level)
-// is one launch of one thread per work item (holder, item); inside a phase no
-// two holders write the same slot (each writes its own guest's band), so the
-// order of the items does not matter.  The edge-E correction reads what
+// exchange (restrictions, prolongations by the coarser host's level) is one
+// launch of one thread per work item (holder, item); inside a phase no two
+// holders write the same slot (each writes its own guest's band), so the
+// order of the items does not matter.  Same-level copies use the push of the
+// uniform step instead (k_c2p writes each cell into the neighbours whose ghost
+// shell holds it, the CT update the face-B strips): the same copies, written
+// while the data is in registers.  The edge-E correction reads what
 // earlier holders wrote back, so its holders run in waves: a holder waits for
 // every earlier holder that reads or writes one of its edges.
 //
@@ -32,7 +35,7 @@
 // computed from the same B and v.
 
 enum { MH_TH = 64, MH_ORD = 2, MH_NGH = 2 };     // [dynamics] bnd_thread_limit (its default); PLM order; ghosts
-enum { MH_SAME = 0, MH_RESTRICT = 1, MH_PROLONG = 2, MH_FLUX = 3 };
+enum { MH_RESTRICT = 1, MH_PROLONG = 2, MH_FLUX = 3 };
 
 struct mh_t
 {
@@ -44,7 +47,7 @@ struct mh_t
     int nbx, nby, nth;                   // launch grid of the holder's exchange kernel
     int fbx, fby, fth;                   // and of its edge-E correction
     int n1;                              // the exchange grid's extent along ax[ 1 ]
-    int wx[ 3 ], bx[ 3 ];                // same level: the boxes of W and face-B copies (x, y, z)
+    int dir;                             // the guest's direction ( x + 1 ) + 3 ( y + 1 ) + 9 ( z + 1 )
 };
 
 __device__ __forceinline__ void mh_dispatch( const mh_t & h, int nth, int bx, int by, int tx, int * i )
@@ -111,82 +114,6 @@ void mh_cell_e( const args_t< R > & a, int b, const int * i )
 __device__ __forceinline__ bool mh_in_band( int i, int off )
 {   // mhd/boundary/comm_functions.h:446-452 in_band_axis
     return off == 0 || ( i - off >= 0 && i - off < MH_ORD );
-}
-
-// same level (hydro comm_functions.h:306-327 to_same; MHD 422-465), over the
-// copies' own boxes with x fastest: the reference's rows run across y or z
-// for x-side holders, which would leave every thread of a warp on its own
-// cache line; a same-level holder's copies are disjoint, so their order is
-// free.  Item `it` < the W box's size: one cell of W (11 words, E included);
-// then, for face holders, one face of the tangential face B.
-template< class R > __device__ __forceinline__
-void mh_same_box( const args_t< R > & a, const mh_t & h, int step, int it )
-{
-    const int a1 = h.ax[ 1 ], a2 = h.ax[ 2 ];
-    const int nw = h.wx[ 0 ] * h.wx[ 1 ] * h.wx[ 2 ];
-    int c[ 3 ], im[ 3 ], ib[ 3 ];
-    if( it < nw )
-    {
-        c[ 0 ] = it % h.wx[ 0 ]; c[ 1 ] = ( it / h.wx[ 0 ] ) % h.wx[ 1 ]; c[ 2 ] = it / ( h.wx[ 0 ] * h.wx[ 1 ] );
-        for( int d = 0; d < 3; ++ d )
-        {
-            im[ d ] = h.os[ d ] + c[ d ];
-            ib[ d ] = h.oc[ d ] + c[ d ];
-        }
-        for( int k = 0; k < 11; ++ k )
-            * mh_w( a, h.guest, k, ib ) = * mh_w( a, h.host, k, im );
-        return;
-    }
-    it -= nw;
-    c[ 0 ] = it % h.bx[ 0 ]; c[ 1 ] = ( it / h.bx[ 0 ] ) % h.bx[ 1 ]; c[ 2 ] = it / ( h.bx[ 0 ] * h.bx[ 1 ] );
-    for( int d = 0; d < 3; ++ d )
-    {
-        im[ d ] = h.obs[ d ] + c[ d ];
-        ib[ d ] = h.obc[ d ] + c[ d ];
-    }
-    * mh_bf( a, step, h.guest, a1, ib ) = * mh_bf( a, step, h.host, a1, im );
-    * mh_bf( a, step, h.guest, a2, ib ) = * mh_bf( a, step, h.host, a2, im );
-}
-
-// the same copies in the reference's row order (kept for reading against it)
-template< class R > __device__ __forceinline__
-void mh_same( const args_t< R > & a, const mh_t & h, int step, int bx, int by, int tx, const int * n )
-{
-    const int ax = h.ax[ 0 ], a1 = h.ax[ 1 ], a2 = h.ax[ 2 ];
-    int i0[ 3 ], im[ 3 ], ib[ 3 ];
-    mh_dispatch( h, h.nth, bx, by, tx, i0 );
-    // a CTA row covers its extent along ax[ 1 ] exactly while that is at most
-    // MH_TH; the guard keeps larger extents in bounds
-    if( i0[ a2 ] < n[ a2 ] && i0[ a1 ] < h.n1 )
-    {
-        for( int d = 0; d < 3; ++ d )
-        {
-            im[ d ] = h.os[ d ] + i0[ d ];
-            ib[ d ] = h.oc[ d ] + i0[ d ];
-        }
-        for( int k = 0; k < MH_ORD; ++ k )
-        {
-            im[ ax ] = k + h.os[ ax ];
-            ib[ ax ] = k + h.oc[ ax ];
-            for( int c = 0; c < 11; ++ c )
-                * mh_w( a, h.guest, c, ib ) = * mh_w( a, h.host, c, im );
-        }
-    }
-    if( h.mode != 0 )
-        return;
-    for( int d = 0; d < 3; ++ d )
-    {
-        im[ d ] = h.obs[ d ] + i0[ d ];
-        ib[ d ] = h.obc[ d ] + i0[ d ];
-    }
-    const int jmax = ( bx == h.nbx - 1 ) + 1;
-    for( int j = 0; j < jmax && ib[ a1 ] < n[ a1 ] + 1; ++ j )
-    {
-        * mh_bf( a, step, h.guest, a1, ib ) = * mh_bf( a, step, h.host, a1, im );
-        * mh_bf( a, step, h.guest, a2, ib ) = * mh_bf( a, step, h.host, a2, im );
-        ib[ a1 ] += h.nth;
-        im[ a1 ] += h.nth;
-    }
 }
 
 // finer host -> coarser guest (hydro comm_functions.h:329-380 to_coarser
@@ -484,11 +411,6 @@ __global__ void __launch_bounds__( 256 ) k_mh( const args_t< R > a, const mh_t *
     const int bx_n = KIND == MH_FLUX ? h.fbx : h.nbx;
     const int th_n = KIND == MH_FLUX ? h.fth : h.nth;
     const int it = int( wk.y );
-    if constexpr( KIND == MH_SAME )
-    {
-        mh_same_box( a, h, step, it );
-        return;
-    }
     const int tx = it % th_n, bx = ( it / th_n ) % bx_n, by = it / ( th_n * bx_n );
     if constexpr( KIND == MH_RESTRICT ) mh_restrict( a, h, step, bx, by, tx, n );
     if constexpr( KIND == MH_PROLONG )  mh_prolong( a, h, step, bx, by, tx, n );
@@ -521,6 +443,9 @@ static mh_t mh_make( int host, int guest, int d_lvl, const int * x, const int * 
     mh_t h;
     std::memset( & h, 0, sizeof( h ) );
     h.host = host; h.guest = guest; h.d_lvl = d_lvl;
+    h.dir = 0;
+    for( int k = 2; k >= 0; -- k )           // flags -1 | 0, 1 | 2: below, beside, above
+        h.dir = 3 * h.dir + ( x[ k ] < 0 ? 0 : ( x[ k ] > 1 ? 2 : 1 ) );
     h.mode = -1;
     for( int k = 0; k < 3; ++ k )
         h.mode += x[ k ] != 0 && x[ k ] != 1;
@@ -569,21 +494,6 @@ static mh_t mh_make( int host, int guest, int d_lvl, const int * x, const int * 
     {
         nc[ a2 ] = MH_NGH;
         if( h.mode > 1 ) nc[ a1 ] = MH_NGH;
-    }
-    // same level: the boxes the reference's rows cover (to_same's W rows: ORD
-    // along ax[ 0 ], the row extent along ax[ 1 ], n or ORD rows along ax[ 2 ];
-    // face B of face holders: 1 x (n + 1) x (n + 1))
-    if( d_lvl == 0 )
-    {
-        h.wx[ ax ] = MH_ORD;
-        h.wx[ a1 ] = nc[ a1 ];
-        h.wx[ a2 ] = h.mode == 0 ? n[ a2 ] : MH_ORD;
-        if( h.mode == 0 )
-        {
-            h.bx[ ax ] = 1;
-            h.bx[ a1 ] = n[ a1 ] + 1;
-            h.bx[ a2 ] = n[ a2 ] + 1;
-        }
     }
     h.n1 = nc[ a1 ];
     h.nth = mh_grid_th( nc[ a1 ] );
@@ -749,7 +659,8 @@ struct mh_plan_t
 {
     std::vector< mh_t > list;
     std::vector< uint2 > work;
-    int same[ 2 ] = { 0, 0 }, restrict_[ 2 ] = { 0, 0 };     // work-item ranges
+    std::vector< int > same_nbr;         // (block, direction 0..26, neighbour) of same-level holders
+    int restrict_[ 2 ] = { 0, 0 };       // work-item range
     std::vector< int > prolong;          // [levels + 1] work offsets
     std::vector< int > waves;            // [waves + 1] work offsets
 };
@@ -762,9 +673,7 @@ static mh_plan_t mh_plan( const kr_tree & t, const int * n )
     {
         const unsigned idx = unsigned( p.list.size(  ) );
         p.list.push_back( h );
-        const int items = flux ? h.fbx * h.fby * h.fth
-                        : h.d_lvl == 0 ? h.wx[ 0 ] * h.wx[ 1 ] * h.wx[ 2 ] + h.bx[ 0 ] * h.bx[ 1 ] * h.bx[ 2 ]
-                                       : h.nbx * h.nby * h.nth;
+        const int items = flux ? h.fbx * h.fby * h.fth : h.nbx * h.nby * h.nth;
         for( int k = 0; k < items; ++ k )
             p.work.push_back( make_uint2( idx, unsigned( k ) ) );
     };
@@ -775,8 +684,13 @@ static mh_plan_t mh_plan( const kr_tree & t, const int * n )
                 add( h, flux );
         return int( p.work.size(  ) );
     };
-    p.same[ 0 ] = 0;
-    p.same[ 1 ] = p.restrict_[ 0 ] = phase( []( const mh_t & h ) { return h.d_lvl == 0; }, false );
+    // same level: the push of the uniform step (k_c2p, the CT update) through
+    // the neighbour table, direction ( x + 1 ) + 3 ( y + 1 ) + 9 ( z + 1 ) with
+    // flags 2 taken as +1; its copies are the ones to_same makes
+    for( const mh_t & h : hs )
+        if( h.d_lvl == 0 )
+            p.same_nbr.insert( p.same_nbr.end(  ), { h.host, h.dir, h.guest } );
+    p.restrict_[ 0 ] = 0;
     p.restrict_[ 1 ] = phase( []( const mh_t & h ) { return h.d_lvl < 0; }, false );
     p.prolong.push_back( p.restrict_[ 1 ] );
     for( int l = 0; l < t.max_level; ++ l )
