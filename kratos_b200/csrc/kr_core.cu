@@ -2109,7 +2109,9 @@ static void enqueue_back( kr_ctx * c, cudaStream_t st, const args_t< R > & a, in
             sides( 1 );
             for( size_t l = 0; l + 1 < c->mh_prolong.size(  ); ++ l )
                 launch_mh< R, MH_PROLONG >( c, st, a, c->mh_prolong[ l ], c->mh_prolong[ l + 1 ], stage );
-            launch_mh< R, MH_RESTRICT >( c, st, a, c->mh_restrict[ 0 ], c->mh_restrict[ 1 ], stage );
+            // (the reference's second restriction pass, keeper.cpp:121-127,
+            // rewrites the same values: its inputs are finer interiors, which
+            // nothing in between changes, with blocks of >= 4 cells per axis)
             sides( 0 );
             return;
         }
@@ -3252,7 +3254,7 @@ int kr_launches_per_step( kr_ctx * c )
     if( c->smr && c->mh_list )
     {   // refined MHD: restrictions (two passes), copies, prolongations by
         // level, the flux average and the edge-E waves
-        smr = 2 * ( c->mh_restrict[ 1 ] > c->mh_restrict[ 0 ] )
+        smr = ( c->mh_restrict[ 1 ] > c->mh_restrict[ 0 ] )
             + ( c->n_restrict ? 1 : 0 ) + int( c->mh_waves.size(  ) ) - 1;
         for( size_t l = 0; l + 1 < c->mh_prolong.size(  ); ++ l )
             smr += c->mh_prolong[ l + 1 ] > c->mh_prolong[ l ];

@@ -48,6 +48,8 @@ struct mh_t
     int fbx, fby, fth;                   // and of its edge-E correction
     int n1;                              // the exchange grid's extent along ax[ 1 ]
     int dir;                             // the guest's direction ( x + 1 ) + 3 ( y + 1 ) + 9 ( z + 1 )
+    int rw[ 2 ], rb[ 2 ];                // restriction / prolongation: the (ax[ 1 ], ax[ 2 ]) extents
+                                         // of the primitives' and the face B's rows
 };
 
 __device__ __forceinline__ void mh_dispatch( const mh_t & h, int nth, int bx, int by, int tx, int * i )
@@ -118,53 +120,56 @@ __device__ __forceinline__ bool mh_in_band( int i, int off )
 
 // finer host -> coarser guest (hydro comm_functions.h:329-380 to_coarser
 // inside MHD 693-780: NGH-wide bands for edge / vertex holders, the area
-// average of the tangential face B for face holders)
+// average of the tangential face B for face holders).  One row (c1, c2) of
+// the reference's dispatch (ax[ 1 ], ax[ 2 ]) per call; the face-B rows include
+// the last CTA's second pass.
 template< class R > __device__ __forceinline__
-void mh_restrict( const args_t< R > & a, const mh_t & h, int step, int bx, int by, int tx, const int * n )
+void mh_restrict_w( const args_t< R > & a, const mh_t & h, int c1, int c2 )
+{
+    const int ax = h.ax[ 0 ], a1 = h.ax[ 1 ], a2 = h.ax[ 2 ];
+    int i0[ 3 ], im[ 3 ], ib[ 3 ];
+    i0[ ax ] = 0; i0[ a1 ] = c1; i0[ a2 ] = c2;
+    for( int d = 0; d < 3; ++ d )
+    {
+        im[ d ] = h.os[ d ] + 2 * i0[ d ];
+        ib[ d ] = i0[ d ] + h.oc[ d ];
+    }
+    const double dv = a.geo[ h.host ].vol;
+    for( int k2 = 0; k2 < MH_ORD; ++ k2 )
+    {
+        double p[ 8 ], norm = 0;
+        for( int c = 0; c < 8; ++ c )
+            p[ c ] = 0;
+        for( int kk = 0; kk < 2; ++ kk )
+        {
+            im[ ax ] = 2 * k2 + kk + h.os[ ax ];
+            const int s1 = im[ a1 ], s2 = im[ a2 ];
+            for( int d1 = 0; d1 < 2; ++ d1 )
+            for( int d2 = 0; d2 < 2; ++ d2 )
+            {
+                im[ a1 ] = s1 + d1;
+                im[ a2 ] = s2 + d2;
+                for( int c = 0; c < 8; ++ c )
+                    p[ c ] += double( * mh_w( a, h.host, c, im ) ) * dv;
+                norm += dv;
+            }
+            im[ a1 ] = s1;
+            im[ a2 ] = s2;
+        }
+        ib[ ax ] = k2 + h.oc[ ax ];
+        for( int c = 0; c < 8; ++ c )
+            * mh_w( a, h.guest, c, ib ) = R( p[ c ] / norm );
+        mh_cell_e( a, h.guest, ib );
+    }
+}
+
+template< class R > __device__ __forceinline__
+void mh_restrict_b( const args_t< R > & a, const mh_t & h, int step, int c1, int c2, const int * n )
 {
     const int ax = h.ax[ 0 ], a1 = h.ax[ 1 ], a2 = h.ax[ 2 ];
     const geo_t & g = a.geo[ h.host ];
     int i0[ 3 ], im[ 3 ], ib[ 3 ];
-    mh_dispatch( h, h.nth, bx, by, tx, i0 );
-    const int lim2 = h.mode > 0 ? MH_NGH : n[ a2 ] / 2;
-    const int lim1 = h.mode > 1 ? MH_NGH : n[ a1 ] / 2;
-    if( i0[ a2 ] < lim2 && i0[ a1 ] < lim1 )
-    {
-        for( int d = 0; d < 3; ++ d )
-        {
-            im[ d ] = h.os[ d ] + 2 * i0[ d ];
-            ib[ d ] = i0[ d ] + h.oc[ d ];
-        }
-        const double dv = g.vol;
-        for( int k2 = 0; k2 < MH_ORD; ++ k2 )
-        {
-            double p[ 8 ], norm = 0;
-            for( int c = 0; c < 8; ++ c )
-                p[ c ] = 0;
-            for( int kk = 0; kk < 2; ++ kk )
-            {
-                im[ ax ] = 2 * k2 + kk + h.os[ ax ];
-                const int s1 = im[ a1 ], s2 = im[ a2 ];
-                for( int d1 = 0; d1 < 2; ++ d1 )
-                for( int d2 = 0; d2 < 2; ++ d2 )
-                {
-                    im[ a1 ] = s1 + d1;
-                    im[ a2 ] = s2 + d2;
-                    for( int c = 0; c < 8; ++ c )
-                        p[ c ] += double( * mh_w( a, h.host, c, im ) ) * dv;
-                    norm += dv;
-                }
-                im[ a1 ] = s1;
-                im[ a2 ] = s2;
-            }
-            ib[ ax ] = k2 + h.oc[ ax ];
-            for( int c = 0; c < 8; ++ c )
-                * mh_w( a, h.guest, c, ib ) = R( p[ c ] / norm );
-            mh_cell_e( a, h.guest, ib );
-        }
-    }
-    if( h.mode != 0 )
-        return;
+    i0[ ax ] = 0; i0[ a1 ] = c1; i0[ a2 ] = c2;
     for( int d = 0; d < 3; ++ d )
     {
         im[ d ] = 2 * i0[ d ] + h.obs[ d ];
@@ -172,96 +177,87 @@ void mh_restrict( const args_t< R > & a, const mh_t & h, int step, int bx, int b
     }
     if( h.obs[ ax ] > 0 )
         -- im[ ax ];
-    const int jmax = ( bx == h.nbx - 1 ) + 1;
-    const int ib_max = n[ a1 ] / 2 + ( h.obc[ a1 ] > 1 );
-    for( int j = 0; j < jmax && i0[ a1 ] < ib_max; ++ j )
+    for( int l = 0; l < 2; ++ l )
     {
-        im[ a1 ] = 2 * i0[ a1 ] + h.obs[ a1 ];
-        for( int l = 0; l < 2; ++ l )
+        const int c = h.ax[ 1 + l ], cp = h.ax[ 2 - l ];
+        if( im[ cp ] >= n[ cp ] )
+            continue;
+        const double ds = g.sfc[ c ];
+        double bsum = 0, s = 0;
+        for( int k = 0; k < 2; ++ k )
         {
-            const int c = h.ax[ 1 + l ], cp = h.ax[ 2 - l ];
-            if( im[ cp ] >= n[ cp ] )
-                continue;
-            const double ds = g.sfc[ c ];
-            double bsum = 0, s = 0;
-            for( int k = 0; k < 2; ++ k )
-            {
-                bsum += ds * * mh_bf( a, step, h.host, c, im );
-                s += ds;
-                ++ im[ cp ];
-                bsum += ds * * mh_bf( a, step, h.host, c, im );
-                s += ds;
-                -- im[ cp ];
-                ++ im[ ax ];
-            }
-            im[ ax ] -= 2;
-            * mh_bf( a, step, h.guest, c, ib ) = s > 0 ? bsum / s : 0.;
+            bsum += ds * * mh_bf( a, step, h.host, c, im );
+            s += ds;
+            ++ im[ cp ];
+            bsum += ds * * mh_bf( a, step, h.host, c, im );
+            s += ds;
+            -- im[ cp ];
+            ++ im[ ax ];
         }
-        i0[ a1 ] += h.nth;
-        ib[ a1 ] += h.nth;
+        im[ ax ] -= 2;
+        * mh_bf( a, step, h.guest, c, ib ) = s > 0 ? bsum / s : 0.;
     }
 }
 
-// coarser host -> finer guest (MHD comm_functions.h:467-691 to_finer)
+// coarser host -> finer guest (MHD comm_functions.h:467-691 to_finer), one
+// row (c1, c2) of the reference's dispatch per call: the primitives of one
+// coarser cell (rows include the last CTA's second pass), or the face B of
+// one coarser cell's fine ghost faces.
 template< class R > __device__ __forceinline__
-void mh_prolong( const args_t< R > & a, const mh_t & h, int step, int bx, int by, int tx, const int * n )
+void mh_prolong_w( const args_t< R > & a, const mh_t & h, int c1, int c2 )
 {
     const int ax = h.ax[ 0 ], a1 = h.ax[ 1 ], a2 = h.ax[ 2 ];
     int i0[ 3 ], im[ 3 ], ib[ 3 ];
-    mh_dispatch( h, h.nth, bx, by, tx, i0 );
+    i0[ ax ] = 0; i0[ a1 ] = c1; i0[ a2 ] = c2;
     for( int d = 0; d < 3; ++ d )
     {
         ib[ d ] = h.oc[ d ] + 2 * i0[ d ];
         im[ d ] = h.os[ d ] + i0[ d ];
     }
-    const int im_max = ( h.mode > 0 && h.oc[ a1 ] != 0 ) ? 1 : ( n[ a1 ] + MH_ORD ) / 2;
-    const int jmax = ( bx == h.nbx - 1 ) + 1;
-    for( int j = 0; j < jmax && i0[ a1 ] < im_max; ++ j )
+    double qc[ 8 ], dq[ 3 ][ 8 ];
+    im[ ax ] = h.os[ ax ];
+    for( int c = 0; c < 8; ++ c )
+        qc[ c ] = double( * mh_w( a, h.host, c, im ) );
+    for( int q = 0; q < 3; ++ q )
     {
-        double qc[ 8 ], dq[ 3 ][ 8 ];
-        im[ ax ] = h.os[ ax ];
+        const int aq = h.ax[ q ];
+        ++ im[ aq ];
+        double qr[ 8 ];
         for( int c = 0; c < 8; ++ c )
-            qc[ c ] = double( * mh_w( a, h.host, c, im ) );
-        for( int q = 0; q < 3; ++ q )
-        {
-            const int aq = h.ax[ q ];
-            ++ im[ aq ];
-            double qr[ 8 ];
-            for( int c = 0; c < 8; ++ c )
-                qr[ c ] = double( * mh_w( a, h.host, c, im ) );
-            im[ aq ] -= 2;
-            for( int c = 0; c < 8; ++ c )
-                dq[ aq ][ c ] = mh_minmod( qr[ c ] - qc[ c ], qc[ c ] - double( * mh_w( a, h.host, c, im ) ) ) * 0.25f;
-            ++ im[ aq ];
-        }
-        for( int k = 0; k < MH_ORD; ++ k )
-        {
-            ib[ ax ] = h.oc[ ax ] + k;
-            for( int d1 = 0; d1 < 2; ++ d1 )
-            for( int d2 = 0; d2 < 2; ++ d2 )
-            {
-                ib[ a1 ] += d1;
-                ib[ a2 ] += d2;
-                if( h.mode == 0 || ( mh_in_band( ib[ a1 ], h.oc[ a1 ] ) && mh_in_band( ib[ a2 ], h.oc[ a2 ] ) ) )
-                {
-                    for( int c = 0; c < 8; ++ c )
-                        * mh_w( a, h.guest, c, ib ) = R( qc[ c ] + dq[ ax ][ c ] * ( 2 * ( k & 1 ) - 1 )
-                                                        + dq[ a1 ][ c ] * ( 2 * d1 - 1 )
-                                                        + dq[ a2 ][ c ] * ( 2 * d2 - 1 ) );
-                    mh_cell_e( a, h.guest, ib );
-                }
-                ib[ a1 ] -= d1;
-                ib[ a2 ] -= d2;
-            }
-        }
-        ib[ a1 ] += 2 * h.nth;
-        im[ a1 ] += h.nth;
-        i0[ a1 ] += h.nth;
+            qr[ c ] = double( * mh_w( a, h.host, c, im ) );
+        im[ aq ] -= 2;
+        for( int c = 0; c < 8; ++ c )
+            dq[ aq ][ c ] = mh_minmod( qr[ c ] - qc[ c ], qc[ c ] - double( * mh_w( a, h.host, c, im ) ) ) * 0.25f;
+        ++ im[ aq ];
     }
-    if( h.mode != 0 )
-        return;
-    // face B, Toth & Roe (comm_functions.h:588-690)
-    mh_dispatch( h, h.nth, bx, by, tx, i0 );
+    for( int k = 0; k < MH_ORD; ++ k )
+    {
+        ib[ ax ] = h.oc[ ax ] + k;
+        for( int d1 = 0; d1 < 2; ++ d1 )
+        for( int d2 = 0; d2 < 2; ++ d2 )
+        {
+            ib[ a1 ] += d1;
+            ib[ a2 ] += d2;
+            if( h.mode == 0 || ( mh_in_band( ib[ a1 ], h.oc[ a1 ] ) && mh_in_band( ib[ a2 ], h.oc[ a2 ] ) ) )
+            {
+                for( int c = 0; c < 8; ++ c )
+                    * mh_w( a, h.guest, c, ib ) = R( qc[ c ] + dq[ ax ][ c ] * ( 2 * ( k & 1 ) - 1 )
+                                                    + dq[ a1 ][ c ] * ( 2 * d1 - 1 )
+                                                    + dq[ a2 ][ c ] * ( 2 * d2 - 1 ) );
+                mh_cell_e( a, h.guest, ib );
+            }
+            ib[ a1 ] -= d1;
+            ib[ a2 ] -= d2;
+        }
+    }
+}
+
+template< class R > __device__ __forceinline__
+void mh_prolong_b( const args_t< R > & a, const mh_t & h, int step, int c1, int c2, const int * n )
+{
+    const int ax = h.ax[ 0 ], a1 = h.ax[ 1 ], a2 = h.ax[ 2 ];
+    int i0[ 3 ], im[ 3 ], ib[ 3 ];
+    i0[ ax ] = 0; i0[ a1 ] = c1; i0[ a2 ] = c2;
     for( int d = 0; d < 3; ++ d )
     {
         ib[ d ] = 2 * i0[ d ] + h.obc[ d ];
@@ -396,8 +392,10 @@ void mh_edge_e( const args_t< R > & a, const mh_t & h, int bx, int by, int tx, c
     }
 }
 
-// One phase: one thread per work item (holder, item), the items of a holder
-// being the (CTA row, CTA, thread) triples of the reference's launch of it.
+// One phase: one thread per work item (holder, item).  For restrictions and
+// prolongations an item is one row (ax[ 1 ], ax[ 2 ]) of the reference's
+// dispatch, the rows of its CTAs' second passes included; for the edge-E
+// correction one (CTA row, CTA, thread) triple of its launch.
 template< class R, int KIND >
 __global__ void __launch_bounds__( 256 ) k_mh( const args_t< R > a, const mh_t * list, const uint2 * work, int n_work,
                                               int step )
@@ -408,13 +406,31 @@ __global__ void __launch_bounds__( 256 ) k_mh( const args_t< R > a, const mh_t *
     const uint2 wk = work[ t ];
     const mh_t & h = list[ wk.x ];
     const int n[ 3 ] = { a.n0, a.n1, a.n2 };
-    const int bx_n = KIND == MH_FLUX ? h.fbx : h.nbx;
-    const int th_n = KIND == MH_FLUX ? h.fth : h.nth;
-    const int it = int( wk.y );
-    const int tx = it % th_n, bx = ( it / th_n ) % bx_n, by = it / ( th_n * bx_n );
-    if constexpr( KIND == MH_RESTRICT ) mh_restrict( a, h, step, bx, by, tx, n );
-    if constexpr( KIND == MH_PROLONG )  mh_prolong( a, h, step, bx, by, tx, n );
-    if constexpr( KIND == MH_FLUX )     mh_edge_e( a, h, bx, by, tx, n );
+    int it = int( wk.y );
+    if constexpr( KIND == MH_FLUX )
+    {
+        const int tx = it % h.fth, bx = ( it / h.fth ) % h.fbx, by = it / ( h.fth * h.fbx );
+        mh_edge_e( a, h, bx, by, tx, n );
+        return;
+    }
+    // a row (c1, c2): the primitives' rows first, then the face B's, each
+    // with x fastest where x is one of the two dispatch axes
+    const bool w = it < h.rw[ 0 ] * h.rw[ 1 ];
+    if( ! w )
+        it -= h.rw[ 0 ] * h.rw[ 1 ];
+    const int * e = w ? h.rw : h.rb;
+    const bool x2 = h.ax[ 2 ] == 0;
+    const int c1 = x2 ? it / e[ 1 ] : it % e[ 0 ], c2 = x2 ? it % e[ 1 ] : it / e[ 0 ];
+    if constexpr( KIND == MH_RESTRICT )
+    {
+        if( w ) mh_restrict_w( a, h, c1, c2 );
+        else    mh_restrict_b( a, h, step, c1, c2, n );
+    }
+    if constexpr( KIND == MH_PROLONG )
+    {
+        if( w ) mh_prolong_w( a, h, c1, c2 );
+        else    mh_prolong_b( a, h, step, c1, c2, n );
+    }
 }
 
 ////////////////////////////////////////////////////////////
@@ -501,6 +517,33 @@ static mh_t mh_make( int host, int guest, int d_lvl, const int * x, const int * 
     h.nby = nc[ a2 ];
     if( h.mode == 0 )
         h.nby += d_lvl > 0 ? MH_NGH / 2 : ( d_lvl < 0 ? xr[ a2 ] > 0 : 1 );
+    // restriction / prolongation rows (ax[ 1 ], ax[ 2 ]) that the reference's
+    // guards admit: first passes [ 0, nbx nth ), the last CTA's second pass
+    // up to ( nbx + 1 ) nth
+    const int first = h.nbx * h.nth, second = ( h.nbx + 1 ) * h.nth;
+    if( d_lvl < 0 )
+    {
+        const int lim2 = h.mode > 0 ? MH_NGH : n[ a2 ] / 2;
+        const int lim1 = h.mode > 1 ? MH_NGH : n[ a1 ] / 2;
+        h.rw[ 0 ] = std::min( lim1, first );
+        h.rw[ 1 ] = std::min( lim2, h.nby );
+        if( h.mode == 0 )
+        {
+            h.rb[ 0 ] = std::min( n[ a1 ] / 2 + ( h.obc[ a1 ] > 1 ), second );
+            h.rb[ 1 ] = h.nby;
+        }
+    }
+    else if( d_lvl > 0 )
+    {
+        const int im_max = ( h.mode > 0 && h.oc[ a1 ] != 0 ) ? 1 : ( n[ a1 ] + MH_ORD ) / 2;
+        h.rw[ 0 ] = std::min( im_max, second );
+        h.rw[ 1 ] = h.nby;
+        if( h.mode == 0 )
+        {
+            h.rb[ 0 ] = first;
+            h.rb[ 1 ] = h.nby;
+        }
+    }
     // edge-E grid: resource_flux (face holders), resource_edge (edge holders)
     if( h.mode == 0 )
     {
@@ -673,7 +716,7 @@ static mh_plan_t mh_plan( const kr_tree & t, const int * n )
     {
         const unsigned idx = unsigned( p.list.size(  ) );
         p.list.push_back( h );
-        const int items = flux ? h.fbx * h.fby * h.fth : h.nbx * h.nby * h.nth;
+        const int items = flux ? h.fbx * h.fby * h.fth : h.rw[ 0 ] * h.rw[ 1 ] + h.rb[ 0 ] * h.rb[ 1 ];
         for( int k = 0; k < items; ++ k )
             p.work.push_back( make_uint2( idx, unsigned( k ) ) );
     };
