@@ -1071,7 +1071,7 @@ void flux_faces( const args_t< R > & a, int axis, int step, udiv_t dv, int b, un
     constexpr int NW = MHD ? 11 : 5;   // stored W words: prim (8) + cell E (3)
     constexpr bool learned = MHD && MODE == KR_RIEMANN_LEARNED;
     const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
-    const unsigned t = bx * blockDim.x + threadIdx.x;
+    unsigned t = bx * blockDim.x + threadIdx.x;
     int ii[ 3 ];
     int outside = 0;
     unsigned total;
@@ -1081,6 +1081,14 @@ void flux_faces( const args_t< R > & a, int axis, int step, udiv_t dv, int b, un
     for( int d = 0; d < 3; ++ d )
         ext[ d ] = d == axis ? nn[ d ] + 1 : nn[ d ] - 2 * lo;
     total = unsigned( ext[ 0 ] * ext[ 1 ] );
+    if constexpr( XL )
+    {   // refined MHD: one index over the whole block's faces (its blocks are
+        // small, and per-plane rows of 128 faces left a fifth of the lanes idle)
+        by = t / total;
+        t -= by * total;
+        if( by >= unsigned( ext[ 2 ] ) )
+            return;
+    }
     const unsigned q = udiv_q( t, dv );
     ii[ 0 ] = int( t - q * unsigned( ext[ 0 ] ) );
     ii[ 1 ] = int( q );
@@ -2035,8 +2043,9 @@ static void launch_flux( kr_ctx * c, cudaStream_t st, const args_t< R > & a, int
     const dim3 grid( blocks_for( ( long long ) ext[ 0 ] * ext[ 1 ], 128 ), ext[ 2 ], c->nblk );
     if constexpr( MHD && ( MODE == KR_RIEMANN_DEFAULT || MODE == KR_RIEMANN_HLLE ) )
         if( c->smr )
-        {
-            k_flux< MHD, R, M, true ><<< grid, 128, 0, st >>>( a, axis, stage, make_udiv( unsigned( ext[ 0 ] ) ) );
+        {   // one flat index over each block's faces (flux_faces, XL)
+            const dim3 flat( blocks_for( ( long long ) ext[ 0 ] * ext[ 1 ] * ext[ 2 ], 128 ), 1, c->nblk );
+            k_flux< MHD, R, M, true ><<< flat, 128, 0, st >>>( a, axis, stage, make_udiv( unsigned( ext[ 0 ] ) ) );
             return;
         }
     k_flux< MHD, R, M ><<< grid, 128, 0, st >>>( a, axis, stage, make_udiv( unsigned( ext[ 0 ] ) ) );
