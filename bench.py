@@ -465,16 +465,14 @@ def time_blast(args, local_rank):
     three refinement levels, PLM + HLLD + CT, every block of every level in one
     captured graph per step; mixed and FP64."""
     import torch
-    from kratos_b200 import Dynamics
-    from kratos_b200.amr import gradient_regions
-    nb, n = (8, 8, 8), (16, 16, 16)
-    regions = gradient_regions(nb, n, 3)
+    from kratos_b200.blast import blast_mesh
     out = {"workload": "magnetized blast (p = 100 inside r < 0.1 of the centre, 0.1 outside, rho = 1, "
                        "B = (1, 1, 0) / sqrt 2), root 128^3 in 512 blocks of 16^3, three levels refined at "
-                       "t = 0 where max_axes(|d rho| / 2 rho + |d p| / 2 p) > 0.5 (%d refine_region points), "
-                       "periodic, PLM + HLLD + CT, Heun RK2" % len(regions)}
+                       "t = 0 where max_axes(|d rho| / 2 rho + |d p| / 2 p) > 0.5 (kratos_b200/amr.py), "
+                       "periodic, PLM + HLLD + CT, Heun RK2"}
     for mode, prec in (("mixed", 1), ("fp64", 2)):
-        d = Dynamics(True, nb, n, gamma=5 / 3, precision=prec, device=local_rank, regions=regions)
+        d, regions = blast_mesh(prec, local_rank)
+        out["refine_regions"] = len(regions)
         stream = torch.cuda.Stream(device=local_rank)
         d.set_stream(stream.cuda_stream)
         d.init_problem("blast", SEED)

@@ -8,10 +8,14 @@ Tolerances as for the uniform FP64 MHD step: relative L1 per conserved field
 (momentum against the momentum vector's L1 norm) and per owned face-B
 component (against the whole field's L1 norm) <= 1e-11 after the fixtures' 4
 steps (fused multiply-adds on the device), <= 1e-10 for the longer oracle run;
-checksum-only fixtures to 1e-11 relative.  Size-independent: |div B| <= 1e-12
-on every block of every level, and the totals of a periodic refined mesh kept
-to rounding (the flux average and the edge-E correction make the level jump
-conservative for mass, energy and momentum).
+checksum-only fixtures to 1e-11 relative.  Rounding-sensitive workloads (the
+blast's pressure jump of 1000, reflecting walls) are held to the larger of
+those bounds and 10x the restatement's own spread between builds with and
+without fused multiply-add.  Size-independent: |div B| <= 1e-12 on every block
+of every level, and the totals of a periodic refined mesh follow the
+restatement's (the reference's refined MHD step lets them drift at ~1e-10 in
+mass and ~1e-7 in energy and momentum over 20 steps, through the stage-1
+edge-E write-back between sibling fine blocks).
 """
 import numpy as np
 import pytest
