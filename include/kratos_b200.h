@@ -45,7 +45,7 @@
 extern "C" {
 #endif
 
-#define KR_ABI_VERSION 6
+#define KR_ABI_VERSION 7
 
 /* [boundary] kinds per side (hydro/boundary/phys_functors.h:11-91): an axis is
  * periodic only when both its sides are KR_BC_PER. */
@@ -115,6 +115,10 @@ typedef struct
                                /* independent periodic boxes, each the unit cube */
                                /* of n cells with its own CFL dt and time        */
                                /* (kr_init_boxes, kr_box_times); nb[1] = nb[2] = 1 */
+#define KR_FLAG_UNFUSED  8     /* MHD, uniform mesh: run stage 0's cell and CT   */
+                               /* updates and stage 1's cons -> prim as three    */
+                               /* launches instead of one fused launch (the same */
+                               /* arithmetic; a check)                           */
 
 typedef struct kr_ctx kr_ctx;
 
@@ -197,7 +201,9 @@ int kr_launches_per_step( kr_ctx * ctx );
 
 /* Run one step eagerly (outside the captured graph) with CUDA events around
  * every kernel and return the step's milliseconds per kernel kind in ms[0..6]:
- * c2p, ghost, flux z, flux y, flux x, emf, update (both stages summed).
+ * c2p, ghost, flux z, flux y, flux x, emf, update (both stages summed; on a
+ * uniform MHD mesh without KR_FLAG_UNFUSED stage 0's fused update + c2p
+ * counts as update).
  * The step advances the state like kr_step.  n_kinds must be >= 7. */
 int kr_profile_step( kr_ctx * ctx, int n_kinds, double * ms );
 
@@ -284,15 +290,17 @@ int kr_c2p_dt_noalloc( const kr_cfg * cfg, const double * u, const double * bf,
  * as one persistent launch over all their blocks: its CTAs walk a work list of
  * the CTA tiles of every block (bigger blocks first), with the per-group
  * arguments in the kernel's parameter space, and give the per-context steps'
- * results bit for bit.  One CUDA graph per step (16 launches; 22 with the
- * learned selector), on the first context's stream.  The contexts stay owned
+ * results bit for bit.  One CUDA graph per step (14 launches, 20 with the
+ * learned selector; 16 and 22 for contexts made with KR_FLAG_UNFUSED), on the
+ * first context's stream.  The contexts stay owned
  * by the caller and must outlive the batch; their state, times and selector
  * calls work as before.
  *   kr_batch_step       : n_steps Heun steps of every box (enqueued)
- *   kr_batch_set_grid / kr_batch_get_grid : CTAs of each launch kind (7 kinds:
+ *   kr_batch_set_grid / kr_batch_get_grid : CTAs of each launch kind (8 kinds:
  *                         c2p stage 0, c2p stage 1, flux sweeps, the network's
- *                         sweep, edge EMF, conserved update, face update; 0 =
- *                         one CTA per work item); returns the kind count
+ *                         sweep, edge EMF, conserved update, face update, and
+ *                         stage 0's fused update + c2p; 0 = one CTA per work
+ *                         item); returns the kind count
  *   kr_batch_autotune   : times 1, 2, 4 and 8 waves of resident CTAs and one
  *                         CTA per item for every kind (two eager steps each,
  *                         on a copy of the state, restored), keeps each kind's
@@ -303,7 +311,7 @@ int kr_c2p_dt_noalloc( const kr_cfg * cfg, const double * u, const double * bf,
  *                         instead.  Returns 1 when cached, 0 when tuned.
  *   kr_batch_profile_step: one step run eagerly with CUDA events around every
  *                         launch; ms[k] = milliseconds of launch kind k (the
- *                         grid order above), n_kinds >= 7.  The step advances
+ *                         grid order above), n_kinds >= 8.  The step advances
  *                         the state like kr_batch_step. */
 typedef struct kr_batch kr_batch;
 kr_batch *  kr_batch_create           ( kr_ctx * const * ctxs, int n );

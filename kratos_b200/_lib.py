@@ -8,8 +8,8 @@ _PKG = os.path.dirname(os.path.abspath(__file__))
 _VARIANT = os.environ.get("KRATOS_B200_VARIANT", "")
 LIB_PATH = os.path.join(_PKG, "libkrb200%s.so" % ("_" + _VARIANT if _VARIANT else ""))
 
-KR_ABI_VERSION = 6
-KR_FLAG_HALO_ALL, KR_FLAG_BOXES = 2, 4
+KR_ABI_VERSION = 7
+KR_FLAG_HALO_ALL, KR_FLAG_BOXES, KR_FLAG_UNFUSED = 2, 4, 8
 BC_KINDS = {"per": 0, "out": 1, "ref": 2, "fre": 3, "fixd": 4}
 KR_RIEMANN_DEFAULT, KR_RIEMANN_HLLE, KR_RIEMANN_LEARNED = 0, 1, 2
 KR_INTEGRATOR_RK2, KR_INTEGRATOR_VL2 = 0, 1

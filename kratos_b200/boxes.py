@@ -19,7 +19,7 @@ from .engine import Dynamics, KratosError
 
 
 # launch kinds of the batched step, in kr_batch_get_grid's order
-BATCH_KINDS = ("c2p0", "c2p1", "flux", "eval", "emf", "upd1", "upd2")
+BATCH_KINDS = ("c2p0", "c2p1", "flux", "eval", "emf", "upd1", "upd2", "updc2p")
 
 
 def box_params(seed, box, gamma=5 / 3):
@@ -100,20 +100,20 @@ class BoxBatch:
 
     def grid(self):
         """CTAs of each launch kind of the batched step (0: one per work item)."""
-        g = (ctypes.c_int * 7)()
+        g = (ctypes.c_int * len(BATCH_KINDS))()
         self._bcheck(L.lib().kr_batch_get_grid(self._batch, g), "kr_batch_get_grid")
         return dict(zip(BATCH_KINDS, list(g)))
 
     def set_grid(self, grid):
-        g = (ctypes.c_int * 7)(*[int(grid[k]) for k in BATCH_KINDS])
+        g = (ctypes.c_int * len(BATCH_KINDS))(*[int(grid[k]) for k in BATCH_KINDS])
         self._bcheck(L.lib().kr_batch_set_grid(self._batch, g), "kr_batch_set_grid")
 
     def profile_step(self):
         """One step eagerly with CUDA events around every launch: milliseconds
         per launch kind (batched), or per group and kind (kr_profile_step)."""
         if self._batch:
-            ms = (ctypes.c_double * 7)()
-            self._bcheck(L.lib().kr_batch_profile_step(self._batch, 7, ms), "kr_batch_profile_step")
+            ms = (ctypes.c_double * len(BATCH_KINDS))()
+            self._bcheck(L.lib().kr_batch_profile_step(self._batch, len(BATCH_KINDS), ms), "kr_batch_profile_step")
             return dict(zip(BATCH_KINDS, list(ms)))
         return {n: d.profile_step() for n, (d, _) in self.groups.items()}
 
@@ -121,7 +121,7 @@ class BoxBatch:
         """Pick each launch kind's CTA count by timing (kr_batch_autotune), or
         reuse the choice cached in `cache_path` for this device and batch.
         Returns (grid, cached)."""
-        g = (ctypes.c_int * 7)()
+        g = (ctypes.c_int * len(BATCH_KINDS))()
         rc = self._bcheck(L.lib().kr_batch_autotune(self._batch, cache_path.encode() if cache_path else None, g),
                           "kr_batch_autotune")
         return dict(zip(BATCH_KINDS, list(g))), rc == 1

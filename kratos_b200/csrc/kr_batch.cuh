@@ -123,9 +123,27 @@ k_update_list( const __grid_constant__ multi_t< R > m, int step, const int4 * __
     }
 }
 
+// Stage 0's update, CT and stage 1's c2p in one launch (update_c2p_cell), over
+// the c2p work list (item: x group, y block, z plane, w tile of 256 cells).
+template< class R >
+__global__ void __launch_bounds__( 256, 3 )
+k_update_c2p_list( const __grid_constant__ multi_t< R > m, const int4 * __restrict__ items, int n_items )
+{
+    for( int it = blockIdx.x; it < n_items; it += gridDim.x )
+    {
+        const int4 t = items[ it ];
+        const args_t< R > & a = m.a[ t.x ];
+        const unsigned c = unsigned( t.w ) * 256u + threadIdx.x;
+        if( c >= unsigned( a.n0 * a.n1 ) )
+            continue;
+        const unsigned q = udiv_q( c, m.dv_c[ t.x ] );
+        update_c2p_cell< R >( a, t.y, int( c - q * unsigned( a.n0 ) ), int( q ), t.z );
+    }
+}
+
 // Launch kinds with a tunable grid, in this order in kr_batch::grid.
-enum { BK_C2P0, BK_C2P1, BK_FLUX, BK_EVAL, BK_EMF, BK_UPD1, BK_UPD2, BK_N };
-static const char * const BK_NAME[ BK_N ] = { "c2p0", "c2p1", "flux", "eval", "emf", "upd1", "upd2" };
+enum { BK_C2P0, BK_C2P1, BK_FLUX, BK_EVAL, BK_EMF, BK_UPD1, BK_UPD2, BK_UPDC2P, BK_N };
+static const char * const BK_NAME[ BK_N ] = { "c2p0", "c2p1", "flux", "eval", "emf", "upd1", "upd2", "updc2p" };
 // resident CTAs per SM each kind is compiled for (its __launch_bounds__)
 template< class R > static int bk_min_ctas( int k )
 {
@@ -137,6 +155,7 @@ template< class R > static int bk_min_ctas( int k )
     case BK_EVAL: return flux_min_ctas< R, KR_RIEMANN_LEARNED >(  );
     case BK_EMF:  return 4;
     case BK_UPD1: return 4;
+    case BK_UPDC2P: return 3;
     default:      return 6;
     }
 }
@@ -151,6 +170,7 @@ struct kr_batch
     // bigger blocks first
     int4 * items = nullptr;
     long long off[ 5 ] = { 0 }, cnt[ 5 ] = { 0 };
+    bool fuse = false;                   // every context fuses stage 0's update with stage 1's c2p
     int grid[ kr::BK_N ] = { 0 };        // CTAs per launch kind (0: one per item)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -223,9 +243,10 @@ static void batch_enqueue( kr_batch * bt, cudaStream_t st, T && timed )
     const bool learned = bt->riemann == KR_RIEMANN_LEARNED;
     for( int stage = 0; stage < 2; ++ stage )
     {
-        timed( stage ? BK_C2P1 : BK_C2P0, [ & ] {
-            ( stage == 0 ? k_c2p_list< true, R, true > : k_c2p_list< true, R, false > )
-                <<< bgrid( bt, stage ? BK_C2P1 : BK_C2P0, 0 ), 256, 0, st >>>( m, stage, it + bt->off[ 0 ], int( bt->cnt[ 0 ] ) ); } );
+        if( ! ( bt->fuse && stage == 1 ) )        // (fused: stage 0's update did stage 1's c2p)
+            timed( stage ? BK_C2P1 : BK_C2P0, [ & ] {
+                ( stage == 0 ? k_c2p_list< true, R, true > : k_c2p_list< true, R, false > )
+                    <<< bgrid( bt, stage ? BK_C2P1 : BK_C2P0, 0 ), 256, 0, st >>>( m, stage, it + bt->off[ 0 ], int( bt->cnt[ 0 ] ) ); } );
         for( int axis = 2; axis >= 0; -- axis )
         {
             const int list = 1 + ( 2 - axis );
@@ -248,6 +269,12 @@ static void batch_enqueue( kr_batch * bt, cudaStream_t st, T && timed )
         const int4 * le = it + bt->off[ 4 ];
         const int ne = int( bt->cnt[ 4 ] );
         timed( BK_EMF, [ & ] { k_emf_list< R ><<< bgrid( bt, BK_EMF, 4 ), 256, 0, st >>>( m, le, ne ); } );
+        if( bt->fuse && stage == 0 )
+        {
+            timed( BK_UPDC2P, [ & ] {
+                k_update_c2p_list< R ><<< bgrid( bt, BK_UPDC2P, 0 ), 256, 0, st >>>( m, it + bt->off[ 0 ], int( bt->cnt[ 0 ] ) ); } );
+            continue;
+        }
         timed( BK_UPD1, [ & ] { k_update_list< true, R, 1 ><<< bgrid( bt, BK_UPD1, 4 ), 256, 0, st >>>( m, stage, le, ne ); } );
         timed( BK_UPD2, [ & ] { k_update_list< true, R, 2 ><<< bgrid( bt, BK_UPD2, 4 ), 256, 0, st >>>( m, stage, le, ne ); } );
     }
@@ -370,7 +397,7 @@ static std::string batch_key( const kr_batch * bt )
 {
     cudaDeviceProp prop;
     cudaGetDeviceProperties( & prop, bt->ctx[ 0 ]->cfg.device );
-    std::string k = "kr_batch v1 ";
+    std::string k = "kr_batch v2 ";
     for( const char * p = prop.name; * p; ++ p )
         k += ( * p == ' ' ) ? '_' : * p;
     k += " sm" + std::to_string( prop.multiProcessorCount ) + " prec" + std::to_string( bt->precision )
@@ -418,6 +445,9 @@ kr_batch * kr_batch_create( kr_ctx * const * ctxs, int n )
     std::vector< int > order( n );
     for( int g = 0; g < n; ++ g ) order[ g ] = g;
     std::stable_sort( order.begin(  ), order.end(  ), [ & ]( int x, int y ) { return ctxs[ x ]->cfg.n[ 0 ] > ctxs[ y ]->cfg.n[ 0 ]; } );
+    bt->fuse = true;
+    for( int g = 0; g < n; ++ g )
+        bt->fuse = bt->fuse && ctxs[ g ]->fuse;
     std::vector< int4 > items;
     for( int list = 0; list < 5; ++ list )
     {
@@ -513,7 +543,8 @@ int kr_batch_launches_per_step( kr_batch * bt )
 {
     if( ! bt ) return -1;
     const int flux = bt->riemann == KR_RIEMANN_LEARNED ? 6 : 3;
-    return 2 + 2 * ( 1 + flux + 3 );
+    // fused: stage 0's two updates and stage 1's c2p are one launch
+    return 2 + 2 * ( 1 + flux + 3 ) - ( bt->fuse ? 2 : 0 );
 }
 
 int kr_batch_profile_step( kr_batch * bt, int n_kinds, double * ms )

@@ -12,7 +12,8 @@
 //   EE[block][3][n2+3][n1+3][n0+3]           edge EMF (R)
 // R is double for the FP64 step and float for the mixed step.  One Heun step
 // is 2 x (c2p, ghost, flux z, flux y, flux x, [emf], update) plus two scalar
-// kernels, captured once into a CUDA graph and replayed.
+// kernels, captured once into a CUDA graph and replayed.  On a uniform MHD mesh
+// stage 0's two updates and stage 1's c2p are one launch (k_update_c2p).
 #include "../../include/kratos_b200.h"
 #include "kr_fast.cuh"
 #include "kr_mlp.cuh"
@@ -191,6 +192,85 @@ __global__ void k_step_end( scal_t * s, double dt_expand, int ns )
 // cons -> prim over the interior of every block, CFL dt at stage 0
 // (hydro/eos/adiabatic.h:211-258; mhd/eos/adiabatic.h:127-234).
 
+// cons -> prim of interior cell (i0, i1, i2) of block b from its conserved
+// words (cons, changed) and, MHD, the face B on its low and high side per axis
+// (b_l, b_r): stores the W words into W (the primitives and the cell E),
+// pushes them into the ghost shells of the same-level neighbours, and writes
+// floored words back to U.  prim, bc_2, b_max, cs2 return what the CFL dt needs.
+template< bool MHD, class R > __device__ __forceinline__
+void c2p_point( const args_t< R > & a, R * W, double * U, int b, int i0, int i1, int i2,
+                double * cons, const double * b_l, const double * b_r,
+                double * prim, double * bc_2, double * b_max, double & cs2 )
+{
+    constexpr int NW = MHD ? 11 : 5;   // stored W words: prim (8) + cell E (3)
+    double cout[ 5 ];
+    double bc[ 3 ], e_m = 0;
+    if( MHD )
+    {
+        for( int d = 0; d < 3; ++ d )
+        {
+            const double bc_m = ( b_l[ d ] + b_r[ d ] ) / 2;
+            bc[ d ] = bc_m;
+            bc_2[ d ] = bc_m * bc_m;
+            e_m += bc_2[ d ];
+            b_max[ d ] = fmax( fabs( b_l[ d ] ), fabs( b_r[ d ] ) );
+        }
+        e_m /= 2;
+        cons[ ENE ] -= e_m;
+    }
+    const int healed = c2p( cons, prim, cout, a.gamma, a.d_floor, a.t_floor, cs2 );
+    if( healed )
+    {
+        U[ iuc( a, b, RHO, i0, i1, i2 ) ] = cout[ RHO ];
+        U[ iuc( a, b, ENE, i0, i1, i2 ) ] = MHD ? cout[ ENE ] + e_m : cout[ ENE ];
+        atomicAdd( & a.s->heal_count, 1 );
+    }
+    R wv[ NW ];
+    for( int k = 0; k < 5; ++ k )
+        wv[ k ] = R( prim[ k ] );
+    if( MHD )
+        for( int d = 0; d < 3; ++ d )
+        {   // cell-centred E = B x v (mhd/eos/adiabatic.h:216-220), from the
+            // stored (R-rounded) primitives so ghost copies agree bit for bit
+            const int d1 = mod3( d + 1 ), d2 = mod3( d + 2 );
+            wv[ BCC + d ] = R( bc[ d ] );
+            wv[ 8 + d ] = R( bc[ d1 ] ) * R( prim[ MOM + d2 ] ) - R( bc[ d2 ] ) * R( prim[ MOM + d1 ] );
+        }
+    const int ngw = int( a.ngw );
+    {
+        R * o = W + iw( a, b, 0, NW, i0, i1, i2 );
+#pragma unroll
+        for( int k = 0; k < NW; ++ k )
+            o[ k * ngw ] = wv[ k ];
+    }
+    // Same-level ghost fill by push: a cell within two cells of a side is a
+    // ghost cell of the block across it (faces, edges, corners).  The block
+    // that holds this cell's position at i + sh n in its ghost shell is the
+    // neighbour in direction -sh, the one whose k_ghost pull in direction sh
+    // reads this cell; past a physical side (-1), on another rank (-2, the
+    // halo exchange) or across a level jump (-3) nothing is written here.
+    // Per axis the shift is +1 within two cells of the low side, -1 of the
+    // high side (n >= 4: never both); the targets are the nonempty subsets.
+    const int sx = i0 < 2 ? 1 : ( i0 >= a.n0 - 2 ? -1 : 0 );
+    const int sy = i1 < 2 ? 1 : ( i1 >= a.n1 - 2 ? -1 : 0 );
+    const int sz = i2 < 2 ? 1 : ( i2 >= a.n2 - 2 ? -1 : 0 );
+    const int mask = ( sx != 0 ) | ( sy != 0 ) << 1 | ( sz != 0 ) << 2;
+    if( mask )
+        for( int m = 1; m < 8; ++ m )
+        {
+            if( m & ~mask )
+                continue;
+            const int dx = m & 1 ? sx : 0, dy = m & 2 ? sy : 0, dz = m & 4 ? sz : 0;
+            const int dst = a.nbr[ b * 27 + ( 1 - dx ) + 3 * ( 1 - dy ) + 9 * ( 1 - dz ) ];
+            if( dst < 0 )
+                continue;
+            R * o = W + iw( a, dst, 0, NW, i0 + dx * a.n0, i1 + dy * a.n1, i2 + dz * a.n2 );
+#pragma unroll
+            for( int k = 0; k < NW; ++ k )
+                o[ k * ngw ] = wv[ k ];
+        }
+}
+
 // DT: stage 0's launch, which also reduces the CFL dt; stage 1's launch has none
 // of that code (fewer registers).
 // One CTA's cells: block b, z plane i2, cell c of the (x, y) plane (every
@@ -198,7 +278,6 @@ __global__ void k_step_end( scal_t * s, double dt_expand, int ns )
 template< bool MHD, class R, bool DT > __device__ __forceinline__
 void c2p_cells( const args_t< R > & a, int step, udiv_t dv, int b, int i2, unsigned c )
 {
-    constexpr int NW = MHD ? 11 : 5;   // stored W words: prim (8) + cell E (3)
     double dt = FLT_MAX;
     if( c < unsigned( a.n0 * a.n1 ) )
     {
@@ -206,10 +285,10 @@ void c2p_cells( const args_t< R > & a, int step, udiv_t dv, int b, int i2, unsig
         const int i0 = int( c - q * unsigned( a.n0 ) );
         const int i1 = int( q );
         double * U = a.u[ step ];
-        double cons[ 5 ], cout[ 5 ], prim[ 5 ];
+        double cons[ 5 ], prim[ 5 ];
         for( int k = 0; k < 5; ++ k )
             cons[ k ] = U[ iuc( a, b, k, i0, i1, i2 ) ];
-        double bc[ 3 ], bc_2[ 3 ], b_max[ 3 ], e_m = 0;
+        double b_l[ 3 ], b_r[ 3 ], bc_2[ 3 ], b_max[ 3 ], cs2;
         if( MHD )
         {
             const double * BF = a.bf[ step ];
@@ -217,71 +296,12 @@ void c2p_cells( const args_t< R > & a, int step, udiv_t dv, int b, int i2, unsig
             for( int d = 0; d < 3; ++ d )
             {
                 int jj[ 3 ] = { ii[ 0 ], ii[ 1 ], ii[ 2 ] };
-                const double b_l = BF[ ibf( a, b, d, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) ];
+                b_l[ d ] = BF[ ibf( a, b, d, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) ];
                 ++ jj[ d ];
-                const double b_r = BF[ ibf( a, b, d, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) ];
-                const double bc_m = ( b_l + b_r ) / 2;
-                bc[ d ] = bc_m;
-                bc_2[ d ] = bc_m * bc_m;
-                e_m += bc_2[ d ];
-                b_max[ d ] = fmax( fabs( b_l ), fabs( b_r ) );
+                b_r[ d ] = BF[ ibf( a, b, d, jj[ 0 ], jj[ 1 ], jj[ 2 ] ) ];
             }
-            e_m /= 2;
-            cons[ ENE ] -= e_m;
         }
-        double cs2;
-        const int healed = c2p( cons, prim, cout, a.gamma, a.d_floor, a.t_floor, cs2 );
-        if( healed )
-        {
-            U[ iuc( a, b, RHO, i0, i1, i2 ) ] = cout[ RHO ];
-            U[ iuc( a, b, ENE, i0, i1, i2 ) ] = MHD ? cout[ ENE ] + e_m : cout[ ENE ];
-            atomicAdd( & a.s->heal_count, 1 );
-        }
-        R wv[ NW ];
-        for( int k = 0; k < 5; ++ k )
-            wv[ k ] = R( prim[ k ] );
-        if( MHD )
-            for( int d = 0; d < 3; ++ d )
-            {   // cell-centred E = B x v (mhd/eos/adiabatic.h:216-220), from the
-                // stored (R-rounded) primitives so ghost copies agree bit for bit
-                const int d1 = mod3( d + 1 ), d2 = mod3( d + 2 );
-                wv[ BCC + d ] = R( bc[ d ] );
-                wv[ 8 + d ] = R( bc[ d1 ] ) * R( prim[ MOM + d2 ] ) - R( bc[ d2 ] ) * R( prim[ MOM + d1 ] );
-            }
-        {
-            R * o = a.w + iw( a, b, 0, NW, i0, i1, i2 );
-            const int ngw = int( a.ngw );
-#pragma unroll
-            for( int k = 0; k < NW; ++ k )
-                o[ k * ngw ] = wv[ k ];
-        }
-        // Same-level ghost fill by push: a cell within two cells of a side is a
-        // ghost cell of the block across it (faces, edges, corners).  The block
-        // that holds this cell's position at i + sh n in its ghost shell is the
-        // neighbour in direction -sh, the one whose k_ghost pull in direction sh
-        // reads this cell; past a physical side (-1), on another rank (-2, the
-        // halo exchange) or across a level jump (-3) nothing is written here.
-        // Per axis the shift is +1 within two cells of the low side, -1 of the
-        // high side (n >= 4: never both); the targets are the nonempty subsets.
-        const int sx = i0 < 2 ? 1 : ( i0 >= a.n0 - 2 ? -1 : 0 );
-        const int sy = i1 < 2 ? 1 : ( i1 >= a.n1 - 2 ? -1 : 0 );
-        const int sz = i2 < 2 ? 1 : ( i2 >= a.n2 - 2 ? -1 : 0 );
-        const int mask = ( sx != 0 ) | ( sy != 0 ) << 1 | ( sz != 0 ) << 2;
-        if( mask )
-            for( int m = 1; m < 8; ++ m )
-            {
-                if( m & ~mask )
-                    continue;
-                const int dx = m & 1 ? sx : 0, dy = m & 2 ? sy : 0, dz = m & 4 ? sz : 0;
-                const int dst = a.nbr[ b * 27 + ( 1 - dx ) + 3 * ( 1 - dy ) + 9 * ( 1 - dz ) ];
-                if( dst < 0 )
-                    continue;
-                R * o = a.w + iw( a, dst, 0, NW, i0 + dx * a.n0, i1 + dy * a.n1, i2 + dz * a.n2 );
-                const int ngw = int( a.ngw );
-#pragma unroll
-                for( int k = 0; k < NW; ++ k )
-                    o[ k * ngw ] = wv[ k ];
-            }
+        c2p_point< MHD, R >( a, a.w, U, b, i0, i1, i2, cons, b_l, b_r, prim, bc_2, b_max, cs2 );
         if( DT )
         {   // cfl * min_a dx_a / s_a as cfl / max_a ( s_a / dx_a ): one division
             // (the reference divides per axis; rounding differs only); like
@@ -1177,68 +1197,62 @@ R face_emf( const args_t< R > & a, int b, int fa, int ax, const int * i )
     return a.f[ fa ][ ifx( a, b, slot, 7, i[ 0 ], i[ 1 ], i[ 2 ] ) ];
 }
 
-// Edge site t of the (x, y) plane i2 of block b.
-template< class R > __device__ __forceinline__
-void emf_site( const args_t< R > & a, udiv_t dv, int b, int i2, unsigned t )
+// Edge EMF E_ax at lattice site i of block b (i[ ax ] < n[ ax ], the other two
+// indices face positions 0..n): the average of the four face EMFs around the
+// edge plus the corner terms upwinded by the sign of the mass flux.
+template< class R, int ax > __device__ __forceinline__
+R emf_edge( const args_t< R > & a, int b, const int * i )
 {
-    const int e0 = a.n0 + 1, e1 = a.n1 + 1;
-    if( t >= unsigned( e0 * e1 ) )
-        return;
-    const unsigned q = udiv_q( t, dv );
-    int i[ 3 ] = { int( t - q * unsigned( e0 ) ), int( q ), i2 };
-    const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
     const R w_e = R( 0.25f );
-    // one base offset per site (cell E in W, the fluxes, the edge EMF); the
-    // neighbours by constant strides
-    const long long oW = iw( a, b, 8, 11, i[ 0 ], i[ 1 ], i[ 2 ] );
-    const long long oF = ifx( a, b, 0, 7, i[ 0 ], i[ 1 ], i[ 2 ] );
-    const long long oE = ifx( a, b, 0, 3, i[ 0 ], i[ 1 ], i[ 2 ] );
     const int sw[ 3 ] = { 1, a.sw1, a.sw2 }, sf[ 3 ] = { 1, a.sf1, a.sf2 };
-    for( int ax = 0; ax < 3; ++ ax )
+    const long long oF = ifx( a, b, 0, 7, i[ 0 ], i[ 1 ], i[ 2 ] );
+    const int ax1 = mod3( 1 + ax ), ax2 = mod3( 2 + ax );
+    const R * we = a.w + iw( a, b, 8 + ax, 11, i[ 0 ], i[ 1 ], i[ 2 ] );   // cell E_ax, stored by k_c2p
+    R ec[ 2 ][ 2 ];
+    ec[ 1 ][ 1 ] = we[ 0 ];
+    ec[ 1 ][ 0 ] = we[ -sw[ ax1 ] ];
+    ec[ 0 ][ 0 ] = we[ -sw[ ax1 ] - sw[ ax2 ] ];
+    ec[ 0 ][ 1 ] = we[ -sw[ ax2 ] ];
+    R e = 0;
+    for( int it = 0; it < 2; ++ it )
     {
-        if( i[ ax ] >= nn[ ax ] )
-            continue;
-        const int ax1 = mod3( 1 + ax ), ax2 = mod3( 2 + ax );
-        const R * we = a.w + oW + ( long long ) ax * a.ngw;   // cell E_ax, stored by k_c2p
-        R ec[ 2 ][ 2 ];
-        ec[ 1 ][ 1 ] = we[ 0 ];
-        ec[ 1 ][ 0 ] = we[ -sw[ ax1 ] ];
-        ec[ 0 ][ 0 ] = we[ -sw[ ax1 ] - sw[ ax2 ] ];
-        ec[ 0 ][ 1 ] = we[ -sw[ ax2 ] ];
-        R e = 0;
-        for( int it = 0; it < 2; ++ it )
+        const int a_para = it == 0 ? ax1 : ax2;
+        const int a_perp = it == 0 ? ax2 : ax1;
+        // E_ax held by the flux of axis a_para (face_emf's slot)
+        const R * fe = a.f[ a_para ] + oF + ( long long )( ( ax == mod3( a_para + 1 ) ) ? 5 : 6 ) * a.nfb;
+        const R ef_m = fe[ -sf[ a_perp ] ];
+        const R ef_p = fe[ 0 ];
+        e += w_e * ( ef_m + ef_p );
+        const R * fr = a.f[ a_perp ] + oF;                   // mass flux (RHO = 0)
+        const R frho_p = fr[ 0 ];
+        const R frho_m = fr[ -sf[ a_para ] ];
+        const R de_p = frho_p > 0 ?  ( ec[ 0 ][ 1 ] - ef_m ) :  ( ec[ 1 ][ 1 ] - ef_p );
+        const R de_m = frho_m > 0 ? -( ec[ 0 ][ 0 ] - ef_m ) : -( ec[ 1 ][ 0 ] - ef_p );
+        e += w_e * ( de_m - de_p );
+        if( it == 0 )
         {
-            const int a_para = it == 0 ? ax1 : ax2;
-            const int a_perp = it == 0 ? ax2 : ax1;
-            // E_ax held by the flux of axis a_para (face_emf's slot)
-            const R * fe = a.f[ a_para ] + oF + ( long long )( ( ax == mod3( a_para + 1 ) ) ? 5 : 6 ) * a.nfb;
-            const R ef_m = fe[ -sf[ a_perp ] ];
-            const R ef_p = fe[ 0 ];
-            e += w_e * ( ef_m + ef_p );
-            const R * fr = a.f[ a_perp ] + oF;                   // mass flux (RHO = 0)
-            const R frho_p = fr[ 0 ];
-            const R frho_m = fr[ -sf[ a_para ] ];
-            const R de_p = frho_p > 0 ?  ( ec[ 0 ][ 1 ] - ef_m ) :  ( ec[ 1 ][ 1 ] - ef_p );
-            const R de_m = frho_m > 0 ? -( ec[ 0 ][ 0 ] - ef_m ) : -( ec[ 1 ][ 0 ] - ef_p );
-            e += w_e * ( de_m - de_p );
-            if( it == 0 )
-            {
-                const R swp = ec[ 0 ][ 1 ];
-                ec[ 0 ][ 1 ] = ec[ 1 ][ 0 ];
-                ec[ 1 ][ 0 ] = swp;
-            }
+            const R swp = ec[ 0 ][ 1 ];
+            ec[ 0 ][ 1 ] = ec[ 1 ][ 0 ];
+            ec[ 1 ][ 0 ] = swp;
         }
-        a.ee[ oE + ( long long ) ax * a.nfb ] = e;
     }
+    return e;
+}
+
+// An edge in the boundary plane of a high out / fre side takes the interior
+// cell's advective E instead, with the reference's velocity scaling (w holds
+// v, which it multiplies by 1 / rho once more) -- integrator.h:329-382.  On an
+// edge of two such planes the later axis wins, as in the reference's loop.
+template< class R, int ax > __device__ __forceinline__
+void emf_edge_side( const args_t< R > & a, int b, const int * i, R & e )
+{
     if( ! a.emf_out )
         return;
-    // boundary-plane edges of a high out / fre side: the interior cell's
-    // advective E, with the reference's velocity scaling (w holds v, which it
-    // multiplies by 1 / rho once more) -- integrator.h:329-382
+    const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
     const int ph = a.geo[ b ].phys;
     for( int d = 0; d < 3; ++ d )
     {
-        if( ! ( a.emf_out >> d & 1 ) || i[ d ] != nn[ d ] || nn[ d ] < 2 || ! ( ( ph >> ( 2 * d + 1 ) ) & 1 ) )
+        if( d == ax || ! ( a.emf_out >> d & 1 ) || i[ d ] != nn[ d ] || nn[ d ] < 2 || ! ( ( ph >> ( 2 * d + 1 ) ) & 1 ) )
             continue;
         int jc[ 3 ] = { i[ 0 ], i[ 1 ], i[ 2 ] };
         -- jc[ d ];
@@ -1250,9 +1264,33 @@ void emf_site( const args_t< R > & a, udiv_t dv, int b, int i2, unsigned t )
             b_c[ q ] = a.w[ iw( a, b, BCC + q, 11, jc[ 0 ], jc[ 1 ], jc[ 2 ] ) ];
         }
         const int d1 = mod3( d + 1 ), d2 = mod3( d + 2 );
-        a.ee[ ifx( a, b, d1, 3, i[ 0 ], i[ 1 ], i[ 2 ] ) ] = v_c[ d ] * b_c[ d2 ] - v_c[ d2 ] * b_c[ d ];
-        a.ee[ ifx( a, b, d2, 3, i[ 0 ], i[ 1 ], i[ 2 ] ) ] = v_c[ d1 ] * b_c[ d ] - v_c[ d ] * b_c[ d1 ];
+        e = ax == d1 ? v_c[ d ] * b_c[ d2 ] - v_c[ d2 ] * b_c[ d ]
+                     : v_c[ d1 ] * b_c[ d ] - v_c[ d ] * b_c[ d1 ];
     }
+}
+
+template< class R, int ax > __device__ __forceinline__
+R emf_edge_full( const args_t< R > & a, int b, const int * i )
+{
+    R e = emf_edge< R, ax >( a, b, i );
+    emf_edge_side< R, ax >( a, b, i, e );
+    return e;
+}
+
+// Edge site t of the (x, y) plane i2 of block b.
+template< class R > __device__ __forceinline__
+void emf_site( const args_t< R > & a, udiv_t dv, int b, int i2, unsigned t )
+{
+    const int e0 = a.n0 + 1, e1 = a.n1 + 1;
+    if( t >= unsigned( e0 * e1 ) )
+        return;
+    const unsigned q = udiv_q( t, dv );
+    const int i[ 3 ] = { int( t - q * unsigned( e0 ) ), int( q ), i2 };
+    const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
+    const long long oE = ifx( a, b, 0, 3, i[ 0 ], i[ 1 ], i[ 2 ] );
+    if( i[ 0 ] < nn[ 0 ] ) a.ee[ oE ] = emf_edge_full< R, 0 >( a, b, i );
+    if( i[ 1 ] < nn[ 1 ] ) a.ee[ oE + a.nfb ] = emf_edge_full< R, 1 >( a, b, i );
+    if( i[ 2 ] < nn[ 2 ] ) a.ee[ oE + 2 * a.nfb ] = emf_edge_full< R, 2 >( a, b, i );
 }
 
 template< class R >
@@ -1317,139 +1355,133 @@ void smr_correct5( const args_t< R > & a, const geo_t & g, int b, const int * i,
             }
 }
 
-// PART 0: cells and faces in one launch; 1: the conserved update only; 2: the
-// CT face update only (MHD: two launches, each with fewer registers).
-// Lattice site t of the (x, y) plane i2 of block b.
-template< bool MHD, class R, bool SMR, int PART > __device__ __forceinline__
-void update_site( const args_t< R > & a, int step, udiv_t dv, int b, int i2, unsigned t )
+// dt of the stage's update: Heun U* = U + dt L(U), U' = (U + U*) / 2 + dt / 2
+// L(U*); VL2 U* = U + dt / 2 L1(U), U' = U + dt L(U*).
+template< class R > __device__ __forceinline__
+double stage_dt( const args_t< R > & a, int step, int b )
+{
+    return __longlong_as_double( a.s[ a.boxes ? b : 0 ].dt_bits )
+         * ( ( step == 0 ) != bool( a.vl2 ) ? 1.0 : double( 0.5f ) );
+}
+
+// Conserved update of interior cell i of block b from its six face fluxes,
+// written to the target slot; v returns the five new words.
+template< bool MHD, class R, bool SMR > __device__ __forceinline__
+void update_cell( const args_t< R > & a, int step, int b, const int * i, double dt, double * v )
 {
     constexpr int NF = MHD ? 7 : 5;
-    const int e0 = a.n0 + 1, e1 = a.n1 + 1;
-    if( t >= unsigned( e0 * e1 ) )
-        return;
-    const unsigned q = udiv_q( t, dv );
-    int i[ 3 ] = { int( t - q * unsigned( e0 ) ), int( q ), i2 };
     const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
-    // Heun: U* = U + dt L(U), U' = (U + U*) / 2 + dt / 2 L(U*); VL2:
-    // U* = U + dt / 2 L1(U), U' = U + dt L(U*)
-    const double dt = __longlong_as_double( a.s[ a.boxes ? b : 0 ].dt_bits )
-                    * ( ( step == 0 ) != bool( a.vl2 ) ? 1.0 : double( 0.5f ) );
     const geo_t & g = a.geo[ b ];
     // The arrays never overlap: restrict lets the loads of later components
     // issue ahead of the stores of earlier ones.
     const R * __restrict__ F[ 3 ] = { a.f[ 0 ], a.f[ 1 ], a.f[ 2 ] };
-    const R * __restrict__ EE = a.ee;
-    if( PART != 2 && i[ 0 ] < nn[ 0 ] && i[ 1 ] < nn[ 1 ] && i[ 2 ] < nn[ 2 ] )
-    {
-        const double * __restrict__ us = a.u[ step ];
-        double * __restrict__ ut = a.u[ 1 - step ];
-        const double dt_dv = dt / g.vol;
-        const long long o = ifx( a, b, 0, NF, i[ 0 ], i[ 1 ], i[ 2 ] );
-        const long long c0 = iuc( a, b, 0, i[ 0 ], i[ 1 ], i[ 2 ] );
-        const long long s1[ 3 ] = { 1, a.sf1, a.sf2 };
-        if constexpr( sizeof( R ) == 4 )
-        {   // all loads first (30 flux words, 5 or 10 state words), then the sums
-            R fl[ 3 ][ 5 ], fr[ 3 ][ 5 ];
-            for( int d = 0; d < 3; ++ d )
-                for( int k = 0; k < 5; ++ k )
-                {
-                    fl[ d ][ k ] = F[ d ][ o + k * a.nfb ];
-                    fr[ d ][ k ] = F[ d ][ o + k * a.nfb + s1[ d ] ];
-                }
-            double v[ 5 ];
+    const double * __restrict__ us = a.u[ step ];
+    double * __restrict__ ut = a.u[ 1 - step ];
+    const double dt_dv = dt / g.vol;
+    const long long o = ifx( a, b, 0, NF, i[ 0 ], i[ 1 ], i[ 2 ] );
+    const long long c0 = iuc( a, b, 0, i[ 0 ], i[ 1 ], i[ 2 ] );
+    const long long s1[ 3 ] = { 1, a.sf1, a.sf2 };
+    if constexpr( sizeof( R ) == 4 )
+    {   // all loads first (30 flux words, 5 or 10 state words), then the sums
+        R fl[ 3 ][ 5 ], fr[ 3 ][ 5 ];
+        for( int d = 0; d < 3; ++ d )
             for( int k = 0; k < 5; ++ k )
-                v[ k ] = step == 0 ? us[ c0 + k * a.nc ]
-                       : ( a.vl2 ? ut[ c0 + k * a.nc ] : ( us[ c0 + k * a.nc ] + ut[ c0 + k * a.nc ] ) * 0.5f );
-            if constexpr( ! SMR )
-                for( int k = 0; k < 5; ++ k )
-                {
-                    for( int d = 0; d < 3; ++ d )
-                    {
-                        const double f_a = g.sfc[ d ] * dt_dv;
-                        double res = 0;
-                        res += f_a * double( fl[ d ][ k ] );
-                        res -= f_a * double( fr[ d ][ k ] );
-                        v[ k ] += res;
-                    }
-                    ut[ c0 + k * a.nc ] = v[ k ];
-                }
-            else
             {
-                bool nl[ 3 ], nr[ 3 ];
-                for( int d = 0; d < 3; ++ d )
-                {
-                    nl[ d ] = ( ( g.fine >> ( 2 * d ) ) & 1 ) && i[ d ] == 0;
-                    nr[ d ] = ( ( g.fine >> ( 2 * d + 1 ) ) & 1 ) && i[ d ] == nn[ d ] - 1;
-                }
-#pragma unroll
-                for( int k = 0; k < 5; ++ k )
-#pragma unroll
-                    for( int d = 0; d < 3; ++ d )
-                    {
-                        const double f_a = g.sfc[ d ] * dt_dv;
-                        double res = 0;
-                        if( ! nl[ d ] )
-                            res += f_a * double( fl[ d ][ k ] );
-                        if( ! nr[ d ] )
-                            res -= f_a * double( fr[ d ][ k ] );
-                        v[ k ] += res;
-                    }
-                if( g.fine )
-                    smr_correct5( a, g, b, i, nn, dt, v );
-#pragma unroll
-                for( int k = 0; k < 5; ++ k )
-                    ut[ c0 + k * a.nc ] = v[ k ];
+                fl[ d ][ k ] = F[ d ][ o + k * a.nfb ];
+                fr[ d ][ k ] = F[ d ][ o + k * a.nfb + s1[ d ] ];
             }
-        }
-        else
+        for( int k = 0; k < 5; ++ k )
+            v[ k ] = step == 0 ? us[ c0 + k * a.nc ]
+                   : ( a.vl2 ? ut[ c0 + k * a.nc ] : ( us[ c0 + k * a.nc ] + ut[ c0 + k * a.nc ] ) * 0.5f );
+        if constexpr( ! SMR )
             for( int k = 0; k < 5; ++ k )
-            {   // FP64 fluxes: one component at a time keeps the registers low
-                const long long c = c0 + k * a.nc;
-                double v = step == 0 ? us[ c ] : ( a.vl2 ? ut[ c ] : ( us[ c ] + ut[ c ] ) * 0.5f );
+            {
                 for( int d = 0; d < 3; ++ d )
                 {
                     const double f_a = g.sfc[ d ] * dt_dv;
                     double res = 0;
-                    if( ! SMR || ! ( ( ( g.fine >> ( 2 * d ) ) & 1 ) && i[ d ] == 0 ) )
-                        res += f_a * double( F[ d ][ o + k * a.nfb ] );
-                    if( ! SMR || ! ( ( ( g.fine >> ( 2 * d + 1 ) ) & 1 ) && i[ d ] == nn[ d ] - 1 ) )
-                        res -= f_a * double( F[ d ][ o + k * a.nfb + s1[ d ] ] );
-                    v += res;
+                    res += f_a * double( fl[ d ][ k ] );
+                    res -= f_a * double( fr[ d ][ k ] );
+                    v[ k ] += res;
                 }
-                if constexpr( SMR )
-                    v = smr_correct( a, g, b, i, nn, k, dt, v );
-                ut[ c ] = v;
+                ut[ c0 + k * a.nc ] = v[ k ];
             }
+        else
+        {
+            bool nl[ 3 ], nr[ 3 ];
+            for( int d = 0; d < 3; ++ d )
+            {
+                nl[ d ] = ( ( g.fine >> ( 2 * d ) ) & 1 ) && i[ d ] == 0;
+                nr[ d ] = ( ( g.fine >> ( 2 * d + 1 ) ) & 1 ) && i[ d ] == nn[ d ] - 1;
+            }
+#pragma unroll
+            for( int k = 0; k < 5; ++ k )
+#pragma unroll
+                for( int d = 0; d < 3; ++ d )
+                {
+                    const double f_a = g.sfc[ d ] * dt_dv;
+                    double res = 0;
+                    if( ! nl[ d ] )
+                        res += f_a * double( fl[ d ][ k ] );
+                    if( ! nr[ d ] )
+                        res -= f_a * double( fr[ d ][ k ] );
+                    v[ k ] += res;
+                }
+            if( g.fine )
+                smr_correct5( a, g, b, i, nn, dt, v );
+#pragma unroll
+            for( int k = 0; k < 5; ++ k )
+                ut[ c0 + k * a.nc ] = v[ k ];
+        }
     }
-    if( ! MHD || PART == 1 )
-        return;
+    else
+        for( int k = 0; k < 5; ++ k )
+        {   // FP64 fluxes: one component at a time keeps the registers low
+            const long long c = c0 + k * a.nc;
+            double w = step == 0 ? us[ c ] : ( a.vl2 ? ut[ c ] : ( us[ c ] + ut[ c ] ) * 0.5f );
+            for( int d = 0; d < 3; ++ d )
+            {
+                const double f_a = g.sfc[ d ] * dt_dv;
+                double res = 0;
+                if( ! SMR || ! ( ( ( g.fine >> ( 2 * d ) ) & 1 ) && i[ d ] == 0 ) )
+                    res += f_a * double( F[ d ][ o + k * a.nfb ] );
+                if( ! SMR || ! ( ( ( g.fine >> ( 2 * d + 1 ) ) & 1 ) && i[ d ] == nn[ d ] - 1 ) )
+                    res -= f_a * double( F[ d ][ o + k * a.nfb + s1[ d ] ] );
+                w += res;
+            }
+            if constexpr( SMR )
+                w = smr_correct( a, g, b, i, nn, k, dt, w );
+            ut[ c ] = w;
+            v[ k ] = w;
+        }
+}
+
+// CT update of face B component c at lattice site i of block b from its four
+// edge EMFs: e1 = E_ax1 at i, e1p at i + e_ax2, e2 = E_ax2 at i, e2p at i + e_ax1
+// (ax1, ax2 = c + 1, c + 2).  WRITE: store it, and push it into the ghost strip
+// of the same-level block across a transverse side it lies next to (for the
+// next stage: that block's sweeps read it); -1 / -2 neighbours as for W.
+template< class R, bool WRITE > __device__ __forceinline__
+double ct_face( const args_t< R > & a, const geo_t & g, int b, int c, const int * i, int step, double dt,
+                R e1, R e1p, R e2, R e2p )
+{
+    const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
+    const int sb[ 3 ] = { 1, a.sb1, a.sb2 };
     const double * __restrict__ bs = a.bf[ step ];
     double * __restrict__ bt = a.bf[ 1 - step ];
-    // one base offset per site; components and neighbours by constant strides
-    const long long oe = ifx( a, b, 0, 3, i[ 0 ], i[ 1 ], i[ 2 ] );
-    const long long ob = ibf( a, b, 0, i[ 0 ], i[ 1 ], i[ 2 ] );
-    const int se[ 3 ] = { 1, a.sf1, a.sf2 };
-    const int sb[ 3 ] = { 1, a.sb1, a.sb2 };
-    for( int c = 0; c < 3; ++ c )
+    const int ax1 = mod3( c + 1 ), ax2 = mod3( c + 2 );
+    double db;
+    db  = double( e1 ) * g.dx[ ax1 ];
+    db -= double( e2 ) * g.dx[ ax2 ];
+    db += double( e2p ) * g.dx[ ax2 ];
+    db -= double( e1p ) * g.dx[ ax1 ];
+    // the reference scales by -dt / sfc; -dt * (1 / sfc) differs in rounding only
+    db *= -dt * g.isfc[ c ];
+    const long long k = ibf( a, b, c, i[ 0 ], i[ 1 ], i[ 2 ] );
+    const double nb = db + ( step == 0 ? bs[ k ] : ( a.vl2 ? bt[ k ] : ( bs[ k ] + bt[ k ] ) / 2 ) );
+    if constexpr( WRITE )
     {
-        const int ax1 = mod3( c + 1 ), ax2 = mod3( c + 2 );
-        if( i[ ax1 ] >= nn[ ax1 ] || i[ ax2 ] >= nn[ ax2 ] )
-            continue;
-        const R * e1 = EE + oe + ( long long ) ax1 * a.nfb;
-        const R * e2 = EE + oe + ( long long ) ax2 * a.nfb;
-        double db;
-        db  = double( e1[ 0 ] ) * g.dx[ ax1 ];
-        db -= double( e2[ 0 ] ) * g.dx[ ax2 ];
-        db += double( e2[ se[ ax1 ] ] ) * g.dx[ ax2 ];
-        db -= double( e1[ se[ ax2 ] ] ) * g.dx[ ax1 ];
-        // the reference scales by -dt / sfc; -dt * (1 / sfc) differs in rounding only
-        db *= -dt * g.isfc[ c ];
-        const long long k = ob + ( long long ) c * a.nbf;
-        const double nb = db + ( step == 0 ? bs[ k ] : ( a.vl2 ? bt[ k ] : ( bs[ k ] + bt[ k ] ) / 2 ) );
         bt[ k ] = nb;
-        // Same-level face-B ghost strips by push, for the next stage: a face
-        // next to a transverse side is a ghost face of the block across it
-        // (the one whose pull along that axis reads it); -1 / -2 as for W.
         for( int l = 0; l < 2; ++ l )
         {
             const int t = l ? ax2 : ax1;
@@ -1463,6 +1495,43 @@ void update_site( const args_t< R > & a, int step, udiv_t dv, int b, int i2, uns
             bt[ k + ( long long )( dst - b ) * 3 * a.nbf + ( long long ) dj * sb[ t ] ] = nb;
         }
     }
+    return nb;
+}
+
+// PART 0: cells and faces in one launch; 1: the conserved update only; 2: the
+// CT face update only (MHD: two launches, each with fewer registers).
+// Lattice site t of the (x, y) plane i2 of block b.
+template< bool MHD, class R, bool SMR, int PART > __device__ __forceinline__
+void update_site( const args_t< R > & a, int step, udiv_t dv, int b, int i2, unsigned t )
+{
+    const int e0 = a.n0 + 1, e1 = a.n1 + 1;
+    if( t >= unsigned( e0 * e1 ) )
+        return;
+    const unsigned q = udiv_q( t, dv );
+    int i[ 3 ] = { int( t - q * unsigned( e0 ) ), int( q ), i2 };
+    const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
+    const double dt = stage_dt( a, step, b );
+    const geo_t & g = a.geo[ b ];
+    if( PART != 2 && i[ 0 ] < nn[ 0 ] && i[ 1 ] < nn[ 1 ] && i[ 2 ] < nn[ 2 ] )
+    {
+        double v[ 5 ];
+        update_cell< MHD, R, SMR >( a, step, b, i, dt, v );
+    }
+    if( ! MHD || PART == 1 )
+        return;
+    const R * __restrict__ EE = a.ee;
+    // one base offset per site; components and neighbours by constant strides
+    const long long oe = ifx( a, b, 0, 3, i[ 0 ], i[ 1 ], i[ 2 ] );
+    const int se[ 3 ] = { 1, a.sf1, a.sf2 };
+    for( int c = 0; c < 3; ++ c )
+    {
+        const int ax1 = mod3( c + 1 ), ax2 = mod3( c + 2 );
+        if( i[ ax1 ] >= nn[ ax1 ] || i[ ax2 ] >= nn[ ax2 ] )
+            continue;
+        const R * e1 = EE + oe + ( long long ) ax1 * a.nfb;
+        const R * e2 = EE + oe + ( long long ) ax2 * a.nfb;
+        ct_face< R, true >( a, g, b, c, i, step, dt, e1[ 0 ], e1[ se[ ax2 ] ], e2[ 0 ], e2[ se[ ax1 ] ] );
+    }
 }
 
 template< bool MHD, class R, bool SMR = false, int PART = 0 >
@@ -1470,6 +1539,63 @@ __global__ void __launch_bounds__( 256, ( SMR && sizeof( R ) == 4 ) ? 3 : ( PART
 {
     // grid: x over the lattice sites of one (x, y) plane, y over z, z over blocks
     update_site< MHD, R, SMR, PART >( a, step, dv, blockIdx.z, blockIdx.y, blockIdx.x * blockDim.x + threadIdx.x );
+}
+
+////////////////////////////////////////////////////////////
+// Stage 0 of a uniform MHD step after the edge EMF, in one launch: the cell
+// update, the CT update of the cell's six faces and cons -> prim of (U*, B*)
+// for stage 1 -- what k_update's two parts and stage 1's k_c2p do, through the
+// same functions, one thread per cell with no shared memory.  A face is written
+// by the cell above it (its low face) and, at the block's high end, by the last
+// cell; the cell below computes it again for its own cell-centred B.  At stage
+// 0 both computations read only slot 0 of B and the edge EMFs and the writes go
+// to slot 1, so they agree bit for bit.  (Stage 1 updates B in place, so there
+// the faces keep one writer each and c2p stays at the start of the next step.)
+// Nothing here reads W, so the new primitives go straight to it.
+template< class R > __device__ __forceinline__
+void update_c2p_cell( const args_t< R > & a, int b, int i0, int i1, int i2 )
+{
+    const int i[ 3 ] = { i0, i1, i2 };
+    const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
+    const geo_t & g = a.geo[ b ];
+    const double dt = stage_dt( a, 0, b );
+    double v[ 5 ];
+    update_cell< true, R, false >( a, 0, b, i, dt, v );
+    const R * __restrict__ EE = a.ee;
+    const int se[ 3 ] = { 1, a.sf1, a.sf2 };
+    double b_l[ 3 ], b_r[ 3 ];
+#pragma unroll
+    for( int c = 0; c < 3; ++ c )
+    {
+        const int ax1 = mod3( c + 1 ), ax2 = mod3( c + 2 );
+#pragma unroll
+        for( int side = 0; side < 2; ++ side )
+        {
+            int j[ 3 ] = { i0, i1, i2 };
+            j[ c ] += side;
+            const long long oe = ifx( a, b, 0, 3, j[ 0 ], j[ 1 ], j[ 2 ] );
+            const R * e1 = EE + oe + ( long long ) ax1 * a.nfb;
+            const R * e2 = EE + oe + ( long long ) ax2 * a.nfb;
+            const R e1a = e1[ 0 ], e1b = e1[ se[ ax2 ] ], e2a = e2[ 0 ], e2b = e2[ se[ ax1 ] ];
+            const bool own = side == 0 || i[ c ] == nn[ c ] - 1;
+            const double nb = own ? ct_face< R, true >( a, g, b, c, j, 0, dt, e1a, e1b, e2a, e2b )
+                                  : ct_face< R, false >( a, g, b, c, j, 0, dt, e1a, e1b, e2a, e2b );
+            ( side ? b_r : b_l )[ c ] = nb;
+        }
+    }
+    double prim[ 5 ], bc_2[ 3 ], b_max[ 3 ], cs2;
+    c2p_point< true, R >( a, a.w, a.u[ 1 ], b, i0, i1, i2, v, b_l, b_r, prim, bc_2, b_max, cs2 );
+}
+
+template< class R >
+__global__ void __launch_bounds__( 256, 4 ) k_update_c2p( const args_t< R > a, udiv_t dv )
+{
+    // grid: x over the cells of one (x, y) plane, y over z, z over blocks
+    const unsigned c = blockIdx.x * blockDim.x + threadIdx.x;
+    if( c >= unsigned( a.n0 * a.n1 ) )
+        return;
+    const unsigned q = udiv_q( c, dv );
+    update_c2p_cell< R >( a, blockIdx.z, int( c - q * unsigned( a.n0 ) ), int( q ), blockIdx.y );
 }
 
 template< bool MHD, class R >
@@ -1887,6 +2013,7 @@ struct kr_ctx
     double * u[ 2 ] = { nullptr, nullptr };
     double * bf[ 2 ] = { nullptr, nullptr };
     void * w = nullptr;
+    bool fuse = false;                 // uniform MHD: stage 0's update and stage 1's c2p in one launch
     void * f[ 3 ] = { nullptr, nullptr, nullptr };
     void * ee = nullptr;
     geo_t * geo = nullptr;
@@ -2081,8 +2208,9 @@ static void enqueue_front( kr_ctx * c, cudaStream_t st, const args_t< R > & a, i
 {
     const unsigned nb = unsigned( c->nblk );
     const int * n = c->cfg.n;
-    timed( 0, [ & ] { ( stage == 0 ? k_c2p< MHD, R, true > : k_c2p< MHD, R, false > )<<< dim3( blocks_for( ( long long ) n[ 0 ] * n[ 1 ], 256 ), n[ 2 ], nb ), 256, 0, st >>>(
-        a, stage, make_udiv( unsigned( n[ 0 ] ) ) ); } );
+    if( ! ( c->fuse && stage == 1 ) )        // (fused: stage 0's update did stage 1's c2p)
+        timed( 0, [ & ] { ( stage == 0 ? k_c2p< MHD, R, true > : k_c2p< MHD, R, false > )<<< dim3( blocks_for( ( long long ) n[ 0 ] * n[ 1 ], 256 ), n[ 2 ], nb ), 256, 0, st >>>(
+            a, stage, make_udiv( unsigned( n[ 0 ] ) ) ); } );
     if( ! c->hsend.items.empty(  ) )
         timed( 1, [ & ] {
             k_halo< MHD, R, true ><<< dim3( c->halo_grid, unsigned( c->hsend.items.size(  ) ) ), 256, 0, st >>>(
@@ -2171,7 +2299,10 @@ static void enqueue_back( kr_ctx * c, cudaStream_t st, const args_t< R > & a, in
             return;
         }
     timed( 6, [ & ] {
-        if( MHD )
+        if( MHD && c->fuse && stage == 0 )      // update, CT and stage 1's c2p
+            k_update_c2p< R ><<< dim3( blocks_for( ( long long ) n[ 0 ] * n[ 1 ], 256 ), n[ 2 ], nb ), 256, 0, st >>>(
+                a, make_udiv( unsigned( n[ 0 ] ) ) );
+        else if( MHD )
         {
             k_update< MHD, R, false, 1 ><<< ug, 256, 0, st >>>( a, stage, make_udiv( unsigned( n[ 0 ] + 1 ) ) );
             k_update< MHD, R, false, 2 ><<< ug, 256, 0, st >>>( a, stage, make_udiv( unsigned( n[ 0 ] + 1 ) ) );
@@ -2658,6 +2789,7 @@ static kr_ctx * create_ctx( const kr_cfg * cfg, int n_regions, const kr_region *
             ok = ok && ck( c, cudaMalloc( & c->bf[ s ], nb * 3 * c->nbf * 8 ), "malloc bf" );
     }
     ok = ok && ck( c, cudaMalloc( & c->w, nb * c->nws * c->ngw * c->rsize ), "malloc w" );
+    c->fuse = cfg->mhd && ! c->smr && ! ( cfg->flags & KR_FLAG_UNFUSED );
     for( int d = 0; d < 3 && ok; ++ d )
         ok = ck( c, cudaMalloc( & c->f[ d ], nb * c->nf * c->nfb * c->rsize ), "malloc f" );
     if( cfg->mhd && ok )
@@ -3274,7 +3406,8 @@ int kr_launches_per_step( kr_ctx * c )
         for( int l = 1; l <= c->max_level; ++ l )
             smr += c->prolong_off[ l ] > c->prolong_off[ l - 1 ];
     }
-    return 2 + 2 * ( ( c->cfg.mhd ? 4 : 2 ) + flux + phys + halo + smr );
+    // fused: stage 0's two updates and stage 1's c2p are one launch
+    return 2 + 2 * ( ( c->cfg.mhd ? 4 : 2 ) + flux + phys + halo + smr ) - ( c->fuse ? 2 : 0 );
 }
 
 int kr_diagnostics( kr_ctx * c, double * max_div_b, double * totals5 )

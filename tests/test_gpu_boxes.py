@@ -115,7 +115,7 @@ def test_batched_launch_matches_per_group_launches(kw):
     t_ref, dl_ref = ref.times()
     for grid in (None, 0, 1):
         bb = BoxBatch(5, 24, batched=True, **kw)
-        assert bb.launches_per_step() == (22 if w is not None else 16)
+        assert bb.launches_per_step() == (20 if w is not None else 14)   # stage 0's update fused with c2p
         if grid is not None:
             g = bb.grid()
             bb.set_grid({k: (0 if grid == 0 else 148) for k in g})
@@ -161,7 +161,7 @@ def test_batch_autotune_caches_and_keeps_state(tmp_path):
     for b in before:
         assert np.array_equal(before[b][0], after[b][0])
     text = open(cache).read()
-    assert text.count("kr_batch v1") == 1 and "prec1" in text
+    assert text.count("kr_batch v2") == 1 and "prec1" in text
     grid2, cached2 = bb.autotune(cache)
     assert cached2 and grid2 == grid
     bb.step(2)
