@@ -39,13 +39,12 @@ BYTES_PER_ZONE_CYCLE = 320
 # the transverse ghost lines the edge EMF reads: (n+1) ((n+2)^2 - 4) per block.
 FLUX_BYTES_PER_FACE = {4: 8 * 4 + 8 + 7 * 4, 8: 8 * 8 + 8 + 7 * 8}
 # DRAM bytes per face of one FP32 flux launch, ncu dram__bytes_read.sum +
-# dram__bytes_write.sum on the 128^3 sample (8 blocks of 64^3) divided by its
-# 2.26 M faces (two captured launches, 135.9 MB on average); traffic scales with
-# the faces (same block shape)
-FLUX_DRAM_BYTES_PER_FACE = 60.0
-# DRAM bytes per zone-cycle of one whole mixed step (all 16 launches), ncu on the
-# 128^3 sample (8 blocks of 64^3): 2354 MB over 2,097,152 cells
-STEP_DRAM_BYTES_PER_ZONE_CYCLE_MIXED = 1122.6
+# dram__bytes_write.sum on this workload (three launches of the first timed
+# step, 1319.3 MB on average) divided by its 18.1 M faces
+FLUX_DRAM_BYTES_PER_FACE = 72.9
+# DRAM bytes per zone-cycle of one whole mixed step, ncu on this workload, one
+# kernel kind per capture (profiles/step_dram_mixed_ot256.md)
+STEP_DRAM_BYTES_PER_ZONE_CYCLE_MIXED = 1290.8
 WORKLOAD = "ot 256^3 periodic MHD, 64 blocks of 64^3, PLM+HLLD+CT, Heun RK2"
 
 
@@ -708,8 +707,8 @@ def main():
                           "frac": step_gbs / peak,
                           "dram_bytes_per_zone_cycle": STEP_DRAM_BYTES_PER_ZONE_CYCLE_MIXED if head != "fp64" else None,
                           "basis": "whole step: %d B/zone-cycle algorithmic (%s peak); longest kernel kind %s; "
-                                   "DRAM bytes per zone-cycle of the mixed step from one ncu capture "
-                                   "(128^3 sample, same block shape)"
+                                   "DRAM bytes per zone-cycle of the mixed step from ncu captures "
+                                   "of each kernel kind on this workload"
                                    % (BYTES_PER_ZONE_CYCLE, peak_kind, top)},
         "clocks": h["clocks"],
         "e2e": h["e2e"],
