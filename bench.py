@@ -44,7 +44,7 @@ FLUX_BYTES_PER_FACE = {4: 8 * 4 + 8 + 7 * 4, 8: 8 * 8 + 8 + 7 * 8}
 FLUX_DRAM_BYTES_PER_FACE = 72.9
 # DRAM bytes per zone-cycle of one whole mixed step, ncu on this workload, one
 # kernel kind per capture (profiles/step_dram_mixed_ot256.md)
-STEP_DRAM_BYTES_PER_ZONE_CYCLE_MIXED = 1290.8
+STEP_DRAM_BYTES_PER_ZONE_CYCLE_MIXED = 1343.2
 WORKLOAD = "ot 256^3 periodic MHD, 64 blocks of 64^3, PLM+HLLD+CT, Heun RK2"
 
 

@@ -118,7 +118,9 @@ typedef struct
 #define KR_FLAG_UNFUSED  8     /* MHD, uniform mesh: run stage 0's cell and CT   */
                                /* updates and stage 1's cons -> prim as three    */
                                /* launches instead of one fused launch (the same */
-                               /* arithmetic; a check)                           */
+                               /* arithmetic; a check).  Fused by default in the */
+                               /* FP64 step and in kr_batch launches; the FP32   */
+                               /* step always runs the three launches            */
 
 typedef struct kr_ctx kr_ctx;
 
@@ -201,9 +203,8 @@ int kr_launches_per_step( kr_ctx * ctx );
 
 /* Run one step eagerly (outside the captured graph) with CUDA events around
  * every kernel and return the step's milliseconds per kernel kind in ms[0..6]:
- * c2p, ghost, flux z, flux y, flux x, emf, update (both stages summed; on a
- * uniform MHD mesh without KR_FLAG_UNFUSED stage 0's fused update + c2p
- * counts as update).
+ * c2p, ghost, flux z, flux y, flux x, emf, update (both stages summed; where
+ * stage 0's update and stage 1's c2p are fused, they count as update).
  * The step advances the state like kr_step.  n_kinds must be >= 7. */
 int kr_profile_step( kr_ctx * ctx, int n_kinds, double * ms );
 
@@ -291,8 +292,8 @@ int kr_c2p_dt_noalloc( const kr_cfg * cfg, const double * u, const double * bf,
  * the CTA tiles of every block (bigger blocks first), with the per-group
  * arguments in the kernel's parameter space, and give the per-context steps'
  * results bit for bit.  One CUDA graph per step (14 launches, 20 with the
- * learned selector; 16 and 22 for contexts made with KR_FLAG_UNFUSED), on the
- * first context's stream.  The contexts stay owned
+ * learned selector: stage 0's update and stage 1's c2p fused; 16 and 22 for
+ * contexts made with KR_FLAG_UNFUSED), on the first context's stream.  The contexts stay owned
  * by the caller and must outlive the batch; their state, times and selector
  * calls work as before.
  *   kr_batch_step       : n_steps Heun steps of every box (enqueued)

@@ -447,7 +447,7 @@ kr_batch * kr_batch_create( kr_ctx * const * ctxs, int n )
     std::stable_sort( order.begin(  ), order.end(  ), [ & ]( int x, int y ) { return ctxs[ x ]->cfg.n[ 0 ] > ctxs[ y ]->cfg.n[ 0 ]; } );
     bt->fuse = true;
     for( int g = 0; g < n; ++ g )
-        bt->fuse = bt->fuse && ctxs[ g ]->fuse;
+        bt->fuse = bt->fuse && ctxs[ g ]->fuse_batch;
     std::vector< int4 > items;
     for( int list = 0; list < 5; ++ list )
     {

@@ -251,24 +251,6 @@ def test_mixed_precision_error_bound():
     assert div <= 1e-12
 
 
-@pytest.mark.parametrize("precision", [2, 1])
-@pytest.mark.parametrize("mhd", [True, False])
-def test_tiled_sweep_equals_per_face_sweep(mhd, precision):
-    """The shared-memory tiled flux sweep reconstructs from the same values as
-    the per-face kernel, so the two give bit-identical states."""
-    from kratos_b200 import Dynamics
-    out = []
-    for flags in (0, 1):
-        d = Dynamics(mhd, (2, 1, 1), (64, 32, 16), gamma=5 / 3 if mhd else 1.4,
-                     precision=precision, flags=flags)
-        d.init_problem("ot" if mhd else "shock", 3)
-        d.step(3)
-        out.append(d.get_state())
-    assert np.array_equal(out[0][0], out[1][0])
-    if mhd:
-        assert np.array_equal(G.owned_bf(out[0][1], (64, 32, 16)), G.owned_bf(out[1][1], (64, 32, 16)))
-
-
 def test_status_word_starts_clean_and_steps_counted():
     from kratos_b200 import Dynamics
     d = Dynamics(False, (1, 1, 1), (8, 8, 8), gamma=1.4)
