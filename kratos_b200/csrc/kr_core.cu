@@ -1197,62 +1197,68 @@ R face_emf( const args_t< R > & a, int b, int fa, int ax, const int * i )
     return a.f[ fa ][ ifx( a, b, slot, 7, i[ 0 ], i[ 1 ], i[ 2 ] ) ];
 }
 
-// Edge EMF E_ax at lattice site i of block b (i[ ax ] < n[ ax ], the other two
-// indices face positions 0..n): the average of the four face EMFs around the
-// edge plus the corner terms upwinded by the sign of the mass flux.
-template< class R, int ax > __device__ __forceinline__
-R emf_edge( const args_t< R > & a, int b, const int * i )
+// Edge site t of the (x, y) plane i2 of block b.
+template< class R > __device__ __forceinline__
+void emf_site( const args_t< R > & a, udiv_t dv, int b, int i2, unsigned t )
 {
+    const int e0 = a.n0 + 1, e1 = a.n1 + 1;
+    if( t >= unsigned( e0 * e1 ) )
+        return;
+    const unsigned q = udiv_q( t, dv );
+    int i[ 3 ] = { int( t - q * unsigned( e0 ) ), int( q ), i2 };
+    const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
     const R w_e = R( 0.25f );
-    const int sw[ 3 ] = { 1, a.sw1, a.sw2 }, sf[ 3 ] = { 1, a.sf1, a.sf2 };
+    // one base offset per site (cell E in W, the fluxes, the edge EMF); the
+    // neighbours by constant strides
+    const long long oW = iw( a, b, 8, 11, i[ 0 ], i[ 1 ], i[ 2 ] );
     const long long oF = ifx( a, b, 0, 7, i[ 0 ], i[ 1 ], i[ 2 ] );
-    const int ax1 = mod3( 1 + ax ), ax2 = mod3( 2 + ax );
-    const R * we = a.w + iw( a, b, 8 + ax, 11, i[ 0 ], i[ 1 ], i[ 2 ] );   // cell E_ax, stored by k_c2p
-    R ec[ 2 ][ 2 ];
-    ec[ 1 ][ 1 ] = we[ 0 ];
-    ec[ 1 ][ 0 ] = we[ -sw[ ax1 ] ];
-    ec[ 0 ][ 0 ] = we[ -sw[ ax1 ] - sw[ ax2 ] ];
-    ec[ 0 ][ 1 ] = we[ -sw[ ax2 ] ];
-    R e = 0;
-    for( int it = 0; it < 2; ++ it )
+    const long long oE = ifx( a, b, 0, 3, i[ 0 ], i[ 1 ], i[ 2 ] );
+    const int sw[ 3 ] = { 1, a.sw1, a.sw2 }, sf[ 3 ] = { 1, a.sf1, a.sf2 };
+    for( int ax = 0; ax < 3; ++ ax )
     {
-        const int a_para = it == 0 ? ax1 : ax2;
-        const int a_perp = it == 0 ? ax2 : ax1;
-        // E_ax held by the flux of axis a_para (face_emf's slot)
-        const R * fe = a.f[ a_para ] + oF + ( long long )( ( ax == mod3( a_para + 1 ) ) ? 5 : 6 ) * a.nfb;
-        const R ef_m = fe[ -sf[ a_perp ] ];
-        const R ef_p = fe[ 0 ];
-        e += w_e * ( ef_m + ef_p );
-        const R * fr = a.f[ a_perp ] + oF;                   // mass flux (RHO = 0)
-        const R frho_p = fr[ 0 ];
-        const R frho_m = fr[ -sf[ a_para ] ];
-        const R de_p = frho_p > 0 ?  ( ec[ 0 ][ 1 ] - ef_m ) :  ( ec[ 1 ][ 1 ] - ef_p );
-        const R de_m = frho_m > 0 ? -( ec[ 0 ][ 0 ] - ef_m ) : -( ec[ 1 ][ 0 ] - ef_p );
-        e += w_e * ( de_m - de_p );
-        if( it == 0 )
+        if( i[ ax ] >= nn[ ax ] )
+            continue;
+        const int ax1 = mod3( 1 + ax ), ax2 = mod3( 2 + ax );
+        const R * we = a.w + oW + ( long long ) ax * a.ngw;   // cell E_ax, stored by k_c2p
+        R ec[ 2 ][ 2 ];
+        ec[ 1 ][ 1 ] = we[ 0 ];
+        ec[ 1 ][ 0 ] = we[ -sw[ ax1 ] ];
+        ec[ 0 ][ 0 ] = we[ -sw[ ax1 ] - sw[ ax2 ] ];
+        ec[ 0 ][ 1 ] = we[ -sw[ ax2 ] ];
+        R e = 0;
+        for( int it = 0; it < 2; ++ it )
         {
-            const R swp = ec[ 0 ][ 1 ];
-            ec[ 0 ][ 1 ] = ec[ 1 ][ 0 ];
-            ec[ 1 ][ 0 ] = swp;
+            const int a_para = it == 0 ? ax1 : ax2;
+            const int a_perp = it == 0 ? ax2 : ax1;
+            // E_ax held by the flux of axis a_para (face_emf's slot)
+            const R * fe = a.f[ a_para ] + oF + ( long long )( ( ax == mod3( a_para + 1 ) ) ? 5 : 6 ) * a.nfb;
+            const R ef_m = fe[ -sf[ a_perp ] ];
+            const R ef_p = fe[ 0 ];
+            e += w_e * ( ef_m + ef_p );
+            const R * fr = a.f[ a_perp ] + oF;                   // mass flux (RHO = 0)
+            const R frho_p = fr[ 0 ];
+            const R frho_m = fr[ -sf[ a_para ] ];
+            const R de_p = frho_p > 0 ?  ( ec[ 0 ][ 1 ] - ef_m ) :  ( ec[ 1 ][ 1 ] - ef_p );
+            const R de_m = frho_m > 0 ? -( ec[ 0 ][ 0 ] - ef_m ) : -( ec[ 1 ][ 0 ] - ef_p );
+            e += w_e * ( de_m - de_p );
+            if( it == 0 )
+            {
+                const R swp = ec[ 0 ][ 1 ];
+                ec[ 0 ][ 1 ] = ec[ 1 ][ 0 ];
+                ec[ 1 ][ 0 ] = swp;
+            }
         }
+        a.ee[ oE + ( long long ) ax * a.nfb ] = e;
     }
-    return e;
-}
-
-// An edge in the boundary plane of a high out / fre side takes the interior
-// cell's advective E instead, with the reference's velocity scaling (w holds
-// v, which it multiplies by 1 / rho once more) -- integrator.h:329-382.  On an
-// edge of two such planes the later axis wins, as in the reference's loop.
-template< class R, int ax > __device__ __forceinline__
-void emf_edge_side( const args_t< R > & a, int b, const int * i, R & e )
-{
     if( ! a.emf_out )
         return;
-    const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
+    // boundary-plane edges of a high out / fre side: the interior cell's
+    // advective E, with the reference's velocity scaling (w holds v, which it
+    // multiplies by 1 / rho once more) -- integrator.h:329-382
     const int ph = a.geo[ b ].phys;
     for( int d = 0; d < 3; ++ d )
     {
-        if( d == ax || ! ( a.emf_out >> d & 1 ) || i[ d ] != nn[ d ] || nn[ d ] < 2 || ! ( ( ph >> ( 2 * d + 1 ) ) & 1 ) )
+        if( ! ( a.emf_out >> d & 1 ) || i[ d ] != nn[ d ] || nn[ d ] < 2 || ! ( ( ph >> ( 2 * d + 1 ) ) & 1 ) )
             continue;
         int jc[ 3 ] = { i[ 0 ], i[ 1 ], i[ 2 ] };
         -- jc[ d ];
@@ -1264,33 +1270,9 @@ void emf_edge_side( const args_t< R > & a, int b, const int * i, R & e )
             b_c[ q ] = a.w[ iw( a, b, BCC + q, 11, jc[ 0 ], jc[ 1 ], jc[ 2 ] ) ];
         }
         const int d1 = mod3( d + 1 ), d2 = mod3( d + 2 );
-        e = ax == d1 ? v_c[ d ] * b_c[ d2 ] - v_c[ d2 ] * b_c[ d ]
-                     : v_c[ d1 ] * b_c[ d ] - v_c[ d ] * b_c[ d1 ];
+        a.ee[ ifx( a, b, d1, 3, i[ 0 ], i[ 1 ], i[ 2 ] ) ] = v_c[ d ] * b_c[ d2 ] - v_c[ d2 ] * b_c[ d ];
+        a.ee[ ifx( a, b, d2, 3, i[ 0 ], i[ 1 ], i[ 2 ] ) ] = v_c[ d1 ] * b_c[ d ] - v_c[ d ] * b_c[ d1 ];
     }
-}
-
-template< class R, int ax > __device__ __forceinline__
-R emf_edge_full( const args_t< R > & a, int b, const int * i )
-{
-    R e = emf_edge< R, ax >( a, b, i );
-    emf_edge_side< R, ax >( a, b, i, e );
-    return e;
-}
-
-// Edge site t of the (x, y) plane i2 of block b.
-template< class R > __device__ __forceinline__
-void emf_site( const args_t< R > & a, udiv_t dv, int b, int i2, unsigned t )
-{
-    const int e0 = a.n0 + 1, e1 = a.n1 + 1;
-    if( t >= unsigned( e0 * e1 ) )
-        return;
-    const unsigned q = udiv_q( t, dv );
-    const int i[ 3 ] = { int( t - q * unsigned( e0 ) ), int( q ), i2 };
-    const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
-    const long long oE = ifx( a, b, 0, 3, i[ 0 ], i[ 1 ], i[ 2 ] );
-    if( i[ 0 ] < nn[ 0 ] ) a.ee[ oE ] = emf_edge_full< R, 0 >( a, b, i );
-    if( i[ 1 ] < nn[ 1 ] ) a.ee[ oE + a.nfb ] = emf_edge_full< R, 1 >( a, b, i );
-    if( i[ 2 ] < nn[ 2 ] ) a.ee[ oE + 2 * a.nfb ] = emf_edge_full< R, 2 >( a, b, i );
 }
 
 template< class R >
@@ -1364,25 +1346,23 @@ double stage_dt( const args_t< R > & a, int step, int b )
          * ( ( step == 0 ) != bool( a.vl2 ) ? 1.0 : double( 0.5f ) );
 }
 
-// Conserved update of interior cell i of block b from its six face fluxes,
-// written to the target slot; v returns the five new words.
-template< bool MHD, class R, bool SMR > __device__ __forceinline__
-void update_cell( const args_t< R > & a, int step, int b, const int * i, double dt, double * v )
+// Stage 0's conserved update of interior cell i of a uniform MHD block from its
+// six face fluxes (update_site's PART 1 arithmetic, term for term), written to
+// slot 1; v returns the five new words.
+template< class R > __device__ __forceinline__
+void update_cell( const args_t< R > & a, int b, const int * i, double dt, double * v )
 {
-    constexpr int NF = MHD ? 7 : 5;
-    const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
+    constexpr int NF = 7;
     const geo_t & g = a.geo[ b ];
-    // The arrays never overlap: restrict lets the loads of later components
-    // issue ahead of the stores of earlier ones.
     const R * __restrict__ F[ 3 ] = { a.f[ 0 ], a.f[ 1 ], a.f[ 2 ] };
-    const double * __restrict__ us = a.u[ step ];
-    double * __restrict__ ut = a.u[ 1 - step ];
+    const double * __restrict__ us = a.u[ 0 ];
+    double * __restrict__ ut = a.u[ 1 ];
     const double dt_dv = dt / g.vol;
     const long long o = ifx( a, b, 0, NF, i[ 0 ], i[ 1 ], i[ 2 ] );
     const long long c0 = iuc( a, b, 0, i[ 0 ], i[ 1 ], i[ 2 ] );
     const long long s1[ 3 ] = { 1, a.sf1, a.sf2 };
     if constexpr( sizeof( R ) == 4 )
-    {   // all loads first (30 flux words, 5 or 10 state words), then the sums
+    {   // all loads first (30 flux words, 5 state words), then the sums
         R fl[ 3 ][ 5 ], fr[ 3 ][ 5 ];
         for( int d = 0; d < 3; ++ d )
             for( int k = 0; k < 5; ++ k )
@@ -1391,79 +1371,48 @@ void update_cell( const args_t< R > & a, int step, int b, const int * i, double 
                 fr[ d ][ k ] = F[ d ][ o + k * a.nfb + s1[ d ] ];
             }
         for( int k = 0; k < 5; ++ k )
-            v[ k ] = step == 0 ? us[ c0 + k * a.nc ]
-                   : ( a.vl2 ? ut[ c0 + k * a.nc ] : ( us[ c0 + k * a.nc ] + ut[ c0 + k * a.nc ] ) * 0.5f );
-        if constexpr( ! SMR )
-            for( int k = 0; k < 5; ++ k )
-            {
-                for( int d = 0; d < 3; ++ d )
-                {
-                    const double f_a = g.sfc[ d ] * dt_dv;
-                    double res = 0;
-                    res += f_a * double( fl[ d ][ k ] );
-                    res -= f_a * double( fr[ d ][ k ] );
-                    v[ k ] += res;
-                }
-                ut[ c0 + k * a.nc ] = v[ k ];
-            }
-        else
+            v[ k ] = us[ c0 + k * a.nc ];
+        for( int k = 0; k < 5; ++ k )
         {
-            bool nl[ 3 ], nr[ 3 ];
             for( int d = 0; d < 3; ++ d )
             {
-                nl[ d ] = ( ( g.fine >> ( 2 * d ) ) & 1 ) && i[ d ] == 0;
-                nr[ d ] = ( ( g.fine >> ( 2 * d + 1 ) ) & 1 ) && i[ d ] == nn[ d ] - 1;
+                const double f_a = g.sfc[ d ] * dt_dv;
+                double res = 0;
+                res += f_a * double( fl[ d ][ k ] );
+                res -= f_a * double( fr[ d ][ k ] );
+                v[ k ] += res;
             }
-#pragma unroll
-            for( int k = 0; k < 5; ++ k )
-#pragma unroll
-                for( int d = 0; d < 3; ++ d )
-                {
-                    const double f_a = g.sfc[ d ] * dt_dv;
-                    double res = 0;
-                    if( ! nl[ d ] )
-                        res += f_a * double( fl[ d ][ k ] );
-                    if( ! nr[ d ] )
-                        res -= f_a * double( fr[ d ][ k ] );
-                    v[ k ] += res;
-                }
-            if( g.fine )
-                smr_correct5( a, g, b, i, nn, dt, v );
-#pragma unroll
-            for( int k = 0; k < 5; ++ k )
-                ut[ c0 + k * a.nc ] = v[ k ];
+            ut[ c0 + k * a.nc ] = v[ k ];
         }
     }
     else
         for( int k = 0; k < 5; ++ k )
         {   // FP64 fluxes: one component at a time keeps the registers low
             const long long c = c0 + k * a.nc;
-            double w = step == 0 ? us[ c ] : ( a.vl2 ? ut[ c ] : ( us[ c ] + ut[ c ] ) * 0.5f );
+            double w = us[ c ];
             for( int d = 0; d < 3; ++ d )
             {
                 const double f_a = g.sfc[ d ] * dt_dv;
                 double res = 0;
-                if( ! SMR || ! ( ( ( g.fine >> ( 2 * d ) ) & 1 ) && i[ d ] == 0 ) )
-                    res += f_a * double( F[ d ][ o + k * a.nfb ] );
-                if( ! SMR || ! ( ( ( g.fine >> ( 2 * d + 1 ) ) & 1 ) && i[ d ] == nn[ d ] - 1 ) )
-                    res -= f_a * double( F[ d ][ o + k * a.nfb + s1[ d ] ] );
+                res += f_a * double( F[ d ][ o + k * a.nfb ] );
+                res -= f_a * double( F[ d ][ o + k * a.nfb + s1[ d ] ] );
                 w += res;
             }
-            if constexpr( SMR )
-                w = smr_correct( a, g, b, i, nn, k, dt, w );
             ut[ c ] = w;
             v[ k ] = w;
         }
 }
 
 // CT update of face B component c at lattice site i of block b from its four
-// edge EMFs: e1 = E_ax1 at i, e1p at i + e_ax2, e2 = E_ax2 at i, e2p at i + e_ax1
-// (ax1, ax2 = c + 1, c + 2).  WRITE: store it, and push it into the ghost strip
-// of the same-level block across a transverse side it lies next to (for the
-// next stage: that block's sweeps read it); -1 / -2 neighbours as for W.
+// edge EMFs (update_site's PART 2 arithmetic, term for term): e1 = E_ax1 at i,
+// e1p at i + e_ax2, e2 = E_ax2 at i, e2p at i + e_ax1 (ax1, ax2 = c + 1, c + 2).
+// WRITE: store it, and push it into the ghost strip of the same-level block
+// across a transverse side it lies next to (for the next stage: that block's
+// sweeps read it); -1 / -2 neighbours as for W.
+// k: the face's index in BF (ibf( a, b, c, i )).
 template< class R, bool WRITE > __device__ __forceinline__
-double ct_face( const args_t< R > & a, const geo_t & g, int b, int c, const int * i, int step, double dt,
-                R e1, R e1p, R e2, R e2p )
+double ct_face( const args_t< R > & a, const geo_t & g, int b, int c, const int * i, long long k, int step,
+                double dt, R e1, R e1p, R e2, R e2p )
 {
     const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
     const int sb[ 3 ] = { 1, a.sb1, a.sb2 };
@@ -1477,7 +1426,6 @@ double ct_face( const args_t< R > & a, const geo_t & g, int b, int c, const int 
     db -= double( e1p ) * g.dx[ ax1 ];
     // the reference scales by -dt / sfc; -dt * (1 / sfc) differs in rounding only
     db *= -dt * g.isfc[ c ];
-    const long long k = ibf( a, b, c, i[ 0 ], i[ 1 ], i[ 2 ] );
     const double nb = db + ( step == 0 ? bs[ k ] : ( a.vl2 ? bt[ k ] : ( bs[ k ] + bt[ k ] ) / 2 ) );
     if constexpr( WRITE )
     {
@@ -1504,25 +1452,113 @@ double ct_face( const args_t< R > & a, const geo_t & g, int b, int c, const int 
 template< bool MHD, class R, bool SMR, int PART > __device__ __forceinline__
 void update_site( const args_t< R > & a, int step, udiv_t dv, int b, int i2, unsigned t )
 {
+    constexpr int NF = MHD ? 7 : 5;
     const int e0 = a.n0 + 1, e1 = a.n1 + 1;
     if( t >= unsigned( e0 * e1 ) )
         return;
     const unsigned q = udiv_q( t, dv );
     int i[ 3 ] = { int( t - q * unsigned( e0 ) ), int( q ), i2 };
     const int nn[ 3 ] = { a.n0, a.n1, a.n2 };
-    const double dt = stage_dt( a, step, b );
+    // Heun: U* = U + dt L(U), U' = (U + U*) / 2 + dt / 2 L(U*); VL2:
+    // U* = U + dt / 2 L1(U), U' = U + dt L(U*)
+    const double dt = __longlong_as_double( a.s[ a.boxes ? b : 0 ].dt_bits )
+                    * ( ( step == 0 ) != bool( a.vl2 ) ? 1.0 : double( 0.5f ) );
     const geo_t & g = a.geo[ b ];
+    // The arrays never overlap: restrict lets the loads of later components
+    // issue ahead of the stores of earlier ones.
+    const R * __restrict__ F[ 3 ] = { a.f[ 0 ], a.f[ 1 ], a.f[ 2 ] };
+    const R * __restrict__ EE = a.ee;
     if( PART != 2 && i[ 0 ] < nn[ 0 ] && i[ 1 ] < nn[ 1 ] && i[ 2 ] < nn[ 2 ] )
     {
-        double v[ 5 ];
-        update_cell< MHD, R, SMR >( a, step, b, i, dt, v );
+        const double * __restrict__ us = a.u[ step ];
+        double * __restrict__ ut = a.u[ 1 - step ];
+        const double dt_dv = dt / g.vol;
+        const long long o = ifx( a, b, 0, NF, i[ 0 ], i[ 1 ], i[ 2 ] );
+        const long long c0 = iuc( a, b, 0, i[ 0 ], i[ 1 ], i[ 2 ] );
+        const long long s1[ 3 ] = { 1, a.sf1, a.sf2 };
+        if constexpr( sizeof( R ) == 4 )
+        {   // all loads first (30 flux words, 5 or 10 state words), then the sums
+            R fl[ 3 ][ 5 ], fr[ 3 ][ 5 ];
+            for( int d = 0; d < 3; ++ d )
+                for( int k = 0; k < 5; ++ k )
+                {
+                    fl[ d ][ k ] = F[ d ][ o + k * a.nfb ];
+                    fr[ d ][ k ] = F[ d ][ o + k * a.nfb + s1[ d ] ];
+                }
+            double v[ 5 ];
+            for( int k = 0; k < 5; ++ k )
+                v[ k ] = step == 0 ? us[ c0 + k * a.nc ]
+                       : ( a.vl2 ? ut[ c0 + k * a.nc ] : ( us[ c0 + k * a.nc ] + ut[ c0 + k * a.nc ] ) * 0.5f );
+            if constexpr( ! SMR )
+                for( int k = 0; k < 5; ++ k )
+                {
+                    for( int d = 0; d < 3; ++ d )
+                    {
+                        const double f_a = g.sfc[ d ] * dt_dv;
+                        double res = 0;
+                        res += f_a * double( fl[ d ][ k ] );
+                        res -= f_a * double( fr[ d ][ k ] );
+                        v[ k ] += res;
+                    }
+                    ut[ c0 + k * a.nc ] = v[ k ];
+                }
+            else
+            {
+                bool nl[ 3 ], nr[ 3 ];
+                for( int d = 0; d < 3; ++ d )
+                {
+                    nl[ d ] = ( ( g.fine >> ( 2 * d ) ) & 1 ) && i[ d ] == 0;
+                    nr[ d ] = ( ( g.fine >> ( 2 * d + 1 ) ) & 1 ) && i[ d ] == nn[ d ] - 1;
+                }
+#pragma unroll
+                for( int k = 0; k < 5; ++ k )
+#pragma unroll
+                    for( int d = 0; d < 3; ++ d )
+                    {
+                        const double f_a = g.sfc[ d ] * dt_dv;
+                        double res = 0;
+                        if( ! nl[ d ] )
+                            res += f_a * double( fl[ d ][ k ] );
+                        if( ! nr[ d ] )
+                            res -= f_a * double( fr[ d ][ k ] );
+                        v[ k ] += res;
+                    }
+                if( g.fine )
+                    smr_correct5( a, g, b, i, nn, dt, v );
+#pragma unroll
+                for( int k = 0; k < 5; ++ k )
+                    ut[ c0 + k * a.nc ] = v[ k ];
+            }
+        }
+        else
+            for( int k = 0; k < 5; ++ k )
+            {   // FP64 fluxes: one component at a time keeps the registers low
+                const long long c = c0 + k * a.nc;
+                double v = step == 0 ? us[ c ] : ( a.vl2 ? ut[ c ] : ( us[ c ] + ut[ c ] ) * 0.5f );
+                for( int d = 0; d < 3; ++ d )
+                {
+                    const double f_a = g.sfc[ d ] * dt_dv;
+                    double res = 0;
+                    if( ! SMR || ! ( ( ( g.fine >> ( 2 * d ) ) & 1 ) && i[ d ] == 0 ) )
+                        res += f_a * double( F[ d ][ o + k * a.nfb ] );
+                    if( ! SMR || ! ( ( ( g.fine >> ( 2 * d + 1 ) ) & 1 ) && i[ d ] == nn[ d ] - 1 ) )
+                        res -= f_a * double( F[ d ][ o + k * a.nfb + s1[ d ] ] );
+                    v += res;
+                }
+                if constexpr( SMR )
+                    v = smr_correct( a, g, b, i, nn, k, dt, v );
+                ut[ c ] = v;
+            }
     }
     if( ! MHD || PART == 1 )
         return;
-    const R * __restrict__ EE = a.ee;
+    const double * __restrict__ bs = a.bf[ step ];
+    double * __restrict__ bt = a.bf[ 1 - step ];
     // one base offset per site; components and neighbours by constant strides
     const long long oe = ifx( a, b, 0, 3, i[ 0 ], i[ 1 ], i[ 2 ] );
+    const long long ob = ibf( a, b, 0, i[ 0 ], i[ 1 ], i[ 2 ] );
     const int se[ 3 ] = { 1, a.sf1, a.sf2 };
+    const int sb[ 3 ] = { 1, a.sb1, a.sb2 };
     for( int c = 0; c < 3; ++ c )
     {
         const int ax1 = mod3( c + 1 ), ax2 = mod3( c + 2 );
@@ -1530,7 +1566,31 @@ void update_site( const args_t< R > & a, int step, udiv_t dv, int b, int i2, uns
             continue;
         const R * e1 = EE + oe + ( long long ) ax1 * a.nfb;
         const R * e2 = EE + oe + ( long long ) ax2 * a.nfb;
-        ct_face< R, true >( a, g, b, c, i, step, dt, e1[ 0 ], e1[ se[ ax2 ] ], e2[ 0 ], e2[ se[ ax1 ] ] );
+        double db;
+        db  = double( e1[ 0 ] ) * g.dx[ ax1 ];
+        db -= double( e2[ 0 ] ) * g.dx[ ax2 ];
+        db += double( e2[ se[ ax1 ] ] ) * g.dx[ ax2 ];
+        db -= double( e1[ se[ ax2 ] ] ) * g.dx[ ax1 ];
+        // the reference scales by -dt / sfc; -dt * (1 / sfc) differs in rounding only
+        db *= -dt * g.isfc[ c ];
+        const long long k = ob + ( long long ) c * a.nbf;
+        const double nb = db + ( step == 0 ? bs[ k ] : ( a.vl2 ? bt[ k ] : ( bs[ k ] + bt[ k ] ) / 2 ) );
+        bt[ k ] = nb;
+        // Same-level face-B ghost strips by push, for the next stage: a face
+        // next to a transverse side is a ghost face of the block across it
+        // (the one whose pull along that axis reads it); -1 / -2 as for W.
+        for( int l = 0; l < 2; ++ l )
+        {
+            const int t = l ? ax2 : ax1;
+            if( i[ t ] != 0 && i[ t ] != nn[ t ] - 1 )
+                continue;
+            const int s = i[ t ] == 0 ? -1 : 1;
+            const int dst = a.nbr[ b * 27 + 13 + s * ( t == 0 ? 1 : ( t == 1 ? 3 : 9 ) ) ];
+            if( dst < 0 )
+                continue;
+            const int dj = ( s < 0 ? nn[ t ] : -1 ) - i[ t ];
+            bt[ k + ( long long )( dst - b ) * 3 * a.nbf + ( long long ) dj * sb[ t ] ] = nb;
+        }
     }
 }
 
@@ -1544,8 +1604,9 @@ __global__ void __launch_bounds__( 256, ( SMR && sizeof( R ) == 4 ) ? 3 : ( PART
 ////////////////////////////////////////////////////////////
 // Stage 0 of a uniform MHD step after the edge EMF, in one launch: the cell
 // update, the CT update of the cell's six faces and cons -> prim of (U*, B*)
-// for stage 1 -- what k_update's two parts and stage 1's k_c2p do, through the
-// same functions, one thread per cell with no shared memory.  A face is written
+// for stage 1 -- what k_update's two parts and stage 1's k_c2p do, with the
+// same arithmetic term for term (c2p_point is shared with k_c2p), one thread
+// per cell with no shared memory.  A face is written
 // by the cell above it (its low face) and, at the block's high end, by the last
 // cell; the cell below computes it again for its own cell-centred B.  At stage
 // 0 both computations read only slot 0 of B and the edge EMFs and the writes go
@@ -1560,9 +1621,11 @@ void update_c2p_cell( const args_t< R > & a, int b, int i0, int i1, int i2 )
     const geo_t & g = a.geo[ b ];
     const double dt = stage_dt( a, 0, b );
     double v[ 5 ];
-    update_cell< true, R, false >( a, 0, b, i, dt, v );
+    update_cell< R >( a, b, i, dt, v );
     const R * __restrict__ EE = a.ee;
     const int se[ 3 ] = { 1, a.sf1, a.sf2 };
+    const int sb[ 3 ] = { 1, a.sb1, a.sb2 };
+    const long long ob = ibf( a, b, 0, i0, i1, i2 );
     double b_l[ 3 ], b_r[ 3 ];
 #pragma unroll
     for( int c = 0; c < 3; ++ c )
@@ -1577,9 +1640,10 @@ void update_c2p_cell( const args_t< R > & a, int b, int i0, int i1, int i2 )
             const R * e1 = EE + oe + ( long long ) ax1 * a.nfb;
             const R * e2 = EE + oe + ( long long ) ax2 * a.nfb;
             const R e1a = e1[ 0 ], e1b = e1[ se[ ax2 ] ], e2a = e2[ 0 ], e2b = e2[ se[ ax1 ] ];
+            const long long k = ob + ( long long ) c * a.nbf + ( side ? sb[ c ] : 0 );
             const bool own = side == 0 || i[ c ] == nn[ c ] - 1;
-            const double nb = own ? ct_face< R, true >( a, g, b, c, j, 0, dt, e1a, e1b, e2a, e2b )
-                                  : ct_face< R, false >( a, g, b, c, j, 0, dt, e1a, e1b, e2a, e2b );
+            const double nb = own ? ct_face< R, true >( a, g, b, c, j, k, 0, dt, e1a, e1b, e2a, e2b )
+                                  : ct_face< R, false >( a, g, b, c, j, k, 0, dt, e1a, e1b, e2a, e2b );
             ( side ? b_r : b_l )[ c ] = nb;
         }
     }
