@@ -4,8 +4,8 @@ launch) against the same stage run as separate launches (KR_FLAG_UNFUSED:
 k_update x2, then stage 1's k_c2p).  The step graph fuses in FP64 (the FP32
 graph keeps the separate launches, measured faster), the batched work-list
 launch in both precisions, so the single-mesh cases run in FP64 and the boxes
-(per-group graphs and the batched launch) in both.  Both paths call the same per-cell and
-per-face functions: built without fused multiply-add (the parity build,
+(per-group graphs and the batched launch) in both.  Both paths do the same
+arithmetic term for term: built without fused multiply-add (the parity build,
 libkrb200_nofma.so) the state after several steps agrees bit for bit; in the
 product build the compiler may contract a product into an add in one path and
 not the other, so there the bound is rounding: relative L1 per field <= 1e-12
@@ -95,7 +95,7 @@ def _compare_boxes(precision, exact):
         assert bb.status() == 0
         states.append({n: d.get_state() for n, (d, _) in bb.groups.items()})
         bb.close()
-    # the batched launch compiles the same functions into other kernels: in the
+    # the batched launch compiles the same arithmetic into other kernels: in the
     # mixed step a contraction difference can flip an FP32 rounding, so it is
     # held to the batched path's own bound (1e-6, as in test_gpu_boxes)
     tol_batched = {2: TOL[2], 1: 1e-6}[precision]
