@@ -8,8 +8,12 @@
 // per-site code on the item's group arguments (read from the kernel's
 // parameter space by the item's group index), so a batched step gives the
 // per-group steps' results bit for bit while 1024 boxes of five sizes step in
-// 16 launches instead of 5 x 16, captured as one CUDA graph.  The number of
-// resident CTAs of each launch is a tuning parameter (kr_batch_autotune).
+// 14 launches instead of 5 x 14, captured as one CUDA graph.  The list is not
+// stored: an item is decoded from its number with the list's per-group
+// offsets and extents (batch_item), so the group index -- and every argument
+// read through it -- is the same for all threads of the CTA and the compiler
+// can keep it in uniform registers.  The number of resident CTAs of each
+// launch is a tuning parameter (kr_batch_autotune).
 //
 // Included at the end of kr_core.cu (it uses the engine's kernels' device
 // functions and the context internals).
@@ -26,7 +30,32 @@ struct multi_t
     udiv_t dv_e[ KR_BATCH_MAX ];          // edge / lattice rows: n0 + 1
     udiv_t dv_f[ 3 ][ KR_BATCH_MAX ];     // face rows of each sweep
     unsigned cpp_f[ 3 ][ KR_BATCH_MAX ];  // 128-face tiles per z plane of each sweep
+    // the work lists [c2p | flux z | flux y | flux x | lattice sites]: per list,
+    // the first item of each group in list order (l_off[.][ng] = the count),
+    // that group, and its tiles per plane and planes per block
+    int ng;
+    int l_off[ 5 ][ KR_BATCH_MAX + 1 ];
+    int l_grp[ 5 ][ KR_BATCH_MAX ];
+    int l_tiles[ 5 ][ KR_BATCH_MAX ];
+    int l_planes[ 5 ][ KR_BATCH_MAX ];
 };
+
+// Item it of work list `list`: x group, y block, z plane, w tile.  Uniform over
+// the CTA when it is (it comes from blockIdx and the loop counter).
+template< class R > __device__ __forceinline__
+int4 batch_item( const multi_t< R > & m, int list, int it )
+{
+    int p = 0;
+#pragma unroll
+    for( int q = 1; q < KR_BATCH_MAX; ++ q )
+        if( q < m.ng && it >= m.l_off[ list ][ q ] )
+            p = q;
+    int r = it - m.l_off[ list ][ p ];
+    const int tiles = m.l_tiles[ list ][ p ], planes = m.l_planes[ list ][ p ];
+    const int x = r % tiles;
+    r /= tiles;
+    return make_int4( m.l_grp[ list ][ p ], r / planes, r % planes, x );
+}
 
 struct multi_scal_t
 {
@@ -62,11 +91,11 @@ __global__ void k_step_end_multi( const __grid_constant__ multi_scal_t m, double
 // item: x group, y block, z plane, w tile
 template< bool MHD, class R, bool DT >
 __global__ void __launch_bounds__( 256, ( MHD && DT ) ? 3 : 4 )
-k_c2p_list( const __grid_constant__ multi_t< R > m, int step, const int4 * __restrict__ items, int n_items )
+k_c2p_list( const __grid_constant__ multi_t< R > m, int step, int n_items )
 {
     for( int it = blockIdx.x; it < n_items; it += gridDim.x )
     {
-        const int4 t = items[ it ];
+        const int4 t = batch_item( m, 0, it );
         c2p_cells< MHD, R, DT >( m.a[ t.x ], step, m.dv_c[ t.x ], t.y, t.z, unsigned( t.w ) * 256u + threadIdx.x );
         if( DT )
             __syncthreads(  );            // the CTA reduction's shared words are reused
@@ -77,7 +106,7 @@ k_c2p_list( const __grid_constant__ multi_t< R > m, int step, const int4 * __res
 // (stage 0 of an evaluation step only), FLUX_APPLY the other sweeps.
 template< bool MHD, class R, int MODE >
 __global__ void __launch_bounds__( 128, ( flux_min_ctas< R, MODE >(  ) ) )
-k_flux_list( const __grid_constant__ multi_t< R > m, int axis, int step, const int4 * __restrict__ items, int n_items )
+k_flux_list( const __grid_constant__ multi_t< R > m, int axis, int step, int n_items )
 {
     if constexpr( MODE == KR_RIEMANN_LEARNED || MODE == FLUX_APPLY )
     {   // every group steps in lockstep: group 0's scalars decide
@@ -87,7 +116,7 @@ k_flux_list( const __grid_constant__ multi_t< R > m, int axis, int step, const i
     }
     for( int it = blockIdx.x; it < n_items; it += gridDim.x )
     {
-        const int4 t = items[ it ];
+        const int4 t = batch_item( m, 1 + ( 2 - axis ), it );
         const args_t< R > & a = m.a[ t.x ];
         if constexpr( MODE == FLUX_APPLY )
         {
@@ -103,22 +132,22 @@ k_flux_list( const __grid_constant__ multi_t< R > m, int axis, int step, const i
 
 template< class R >
 __global__ void __launch_bounds__( 256 )
-k_emf_list( const __grid_constant__ multi_t< R > m, const int4 * __restrict__ items, int n_items )
+k_emf_list( const __grid_constant__ multi_t< R > m, int n_items )
 {
     for( int it = blockIdx.x; it < n_items; it += gridDim.x )
     {
-        const int4 t = items[ it ];
+        const int4 t = batch_item( m, 4, it );
         emf_site< R >( m.a[ t.x ], m.dv_e[ t.x ], t.y, t.z, unsigned( t.w ) * 256u + threadIdx.x );
     }
 }
 
 template< bool MHD, class R, int PART >
 __global__ void __launch_bounds__( 256, ( PART == 2 ? 6 : 4 ) )
-k_update_list( const __grid_constant__ multi_t< R > m, int step, const int4 * __restrict__ items, int n_items )
+k_update_list( const __grid_constant__ multi_t< R > m, int step, int n_items )
 {
     for( int it = blockIdx.x; it < n_items; it += gridDim.x )
     {
-        const int4 t = items[ it ];
+        const int4 t = batch_item( m, 4, it );
         update_site< MHD, R, false, PART >( m.a[ t.x ], step, m.dv_e[ t.x ], t.y, t.z, unsigned( t.w ) * 256u + threadIdx.x );
     }
 }
@@ -127,11 +156,11 @@ k_update_list( const __grid_constant__ multi_t< R > m, int step, const int4 * __
 // the c2p work list (item: x group, y block, z plane, w tile of 256 cells).
 template< class R >
 __global__ void __launch_bounds__( 256, 3 )
-k_update_c2p_list( const __grid_constant__ multi_t< R > m, const int4 * __restrict__ items, int n_items )
+k_update_c2p_list( const __grid_constant__ multi_t< R > m, int n_items )
 {
     for( int it = blockIdx.x; it < n_items; it += gridDim.x )
     {
-        const int4 t = items[ it ];
+        const int4 t = batch_item( m, 0, it );
         const args_t< R > & a = m.a[ t.x ];
         const unsigned c = unsigned( t.w ) * 256u + threadIdx.x;
         if( c >= unsigned( a.n0 * a.n1 ) )
@@ -167,9 +196,10 @@ struct kr_batch
     std::string err;
     int precision = 2, riemann = 0;
     // work lists: [c2p | flux z | flux y | flux x | lattice sites], ordered
-    // bigger blocks first
-    int4 * items = nullptr;
-    long long off[ 5 ] = { 0 }, cnt[ 5 ] = { 0 };
+    // bigger blocks first (decoded on the device, batch_item)
+    long long cnt[ 5 ] = { 0 };
+    int l_off[ 5 ][ KR_BATCH_MAX + 1 ] = { { 0 } }, l_grp[ 5 ][ KR_BATCH_MAX ] = { { 0 } };
+    int l_tiles[ 5 ][ KR_BATCH_MAX ] = { { 0 } }, l_planes[ 5 ][ KR_BATCH_MAX ] = { { 0 } };
     bool fuse = false;                   // every context fuses stage 0's update with stage 1's c2p
     int grid[ kr::BK_N ] = { 0 };        // CTAs per launch kind (0: one per item)
     cudaGraph_t graph = nullptr;
@@ -209,6 +239,11 @@ static multi_t< R > make_multi( kr_batch * bt )
             m.cpp_f[ axis ][ g ] = unsigned( blocks_for( ( long long ) ext[ 0 ] * ext[ 1 ], 128 ) );
         }
     }
+    m.ng = int( bt->ctx.size(  ) );
+    std::memcpy( m.l_off, bt->l_off, sizeof( m.l_off ) );
+    std::memcpy( m.l_grp, bt->l_grp, sizeof( m.l_grp ) );
+    std::memcpy( m.l_tiles, bt->l_tiles, sizeof( m.l_tiles ) );
+    std::memcpy( m.l_planes, bt->l_planes, sizeof( m.l_planes ) );
     return m;
 }
 
@@ -239,44 +274,41 @@ static void batch_enqueue( kr_batch * bt, cudaStream_t st, T && timed )
     const multi_t< R > m = make_multi< R >( bt );
     const multi_scal_t ms = make_multi_scal( bt );
     k_step_begin_multi<<< 1, 1, 0, st >>>( ms );
-    const int4 * it = bt->items;
     const bool learned = bt->riemann == KR_RIEMANN_LEARNED;
     for( int stage = 0; stage < 2; ++ stage )
     {
         if( ! ( bt->fuse && stage == 1 ) )        // (fused: stage 0's update did stage 1's c2p)
             timed( stage ? BK_C2P1 : BK_C2P0, [ & ] {
                 ( stage == 0 ? k_c2p_list< true, R, true > : k_c2p_list< true, R, false > )
-                    <<< bgrid( bt, stage ? BK_C2P1 : BK_C2P0, 0 ), 256, 0, st >>>( m, stage, it + bt->off[ 0 ], int( bt->cnt[ 0 ] ) ); } );
+                    <<< bgrid( bt, stage ? BK_C2P1 : BK_C2P0, 0 ), 256, 0, st >>>( m, stage, int( bt->cnt[ 0 ] ) ); } );
         for( int axis = 2; axis >= 0; -- axis )
         {
             const int list = 1 + ( 2 - axis );
-            const int4 * li = it + bt->off[ list ];
             const int nl = int( bt->cnt[ list ] );
             if( learned )
             {
                 timed( BK_EVAL, [ & ] {
-                    k_flux_list< true, R, KR_RIEMANN_LEARNED ><<< bgrid( bt, BK_EVAL, list ), 128, 0, st >>>( m, axis, stage, li, nl ); } );
+                    k_flux_list< true, R, KR_RIEMANN_LEARNED ><<< bgrid( bt, BK_EVAL, list ), 128, 0, st >>>( m, axis, stage, nl ); } );
                 timed( BK_FLUX, [ & ] {
-                    k_flux_list< true, R, FLUX_APPLY ><<< bgrid( bt, BK_FLUX, list ), 128, 0, st >>>( m, axis, stage, li, nl ); } );
+                    k_flux_list< true, R, FLUX_APPLY ><<< bgrid( bt, BK_FLUX, list ), 128, 0, st >>>( m, axis, stage, nl ); } );
             }
             else if( bt->riemann == KR_RIEMANN_HLLE )
                 timed( BK_FLUX, [ & ] {
-                    k_flux_list< true, R, KR_RIEMANN_HLLE ><<< bgrid( bt, BK_FLUX, list ), 128, 0, st >>>( m, axis, stage, li, nl ); } );
+                    k_flux_list< true, R, KR_RIEMANN_HLLE ><<< bgrid( bt, BK_FLUX, list ), 128, 0, st >>>( m, axis, stage, nl ); } );
             else
                 timed( BK_FLUX, [ & ] {
-                    k_flux_list< true, R, KR_RIEMANN_DEFAULT ><<< bgrid( bt, BK_FLUX, list ), 128, 0, st >>>( m, axis, stage, li, nl ); } );
+                    k_flux_list< true, R, KR_RIEMANN_DEFAULT ><<< bgrid( bt, BK_FLUX, list ), 128, 0, st >>>( m, axis, stage, nl ); } );
         }
-        const int4 * le = it + bt->off[ 4 ];
         const int ne = int( bt->cnt[ 4 ] );
-        timed( BK_EMF, [ & ] { k_emf_list< R ><<< bgrid( bt, BK_EMF, 4 ), 256, 0, st >>>( m, le, ne ); } );
+        timed( BK_EMF, [ & ] { k_emf_list< R ><<< bgrid( bt, BK_EMF, 4 ), 256, 0, st >>>( m, ne ); } );
         if( bt->fuse && stage == 0 )
         {
             timed( BK_UPDC2P, [ & ] {
-                k_update_c2p_list< R ><<< bgrid( bt, BK_UPDC2P, 0 ), 256, 0, st >>>( m, it + bt->off[ 0 ], int( bt->cnt[ 0 ] ) ); } );
+                k_update_c2p_list< R ><<< bgrid( bt, BK_UPDC2P, 0 ), 256, 0, st >>>( m, int( bt->cnt[ 0 ] ) ); } );
             continue;
         }
-        timed( BK_UPD1, [ & ] { k_update_list< true, R, 1 ><<< bgrid( bt, BK_UPD1, 4 ), 256, 0, st >>>( m, stage, le, ne ); } );
-        timed( BK_UPD2, [ & ] { k_update_list< true, R, 2 ><<< bgrid( bt, BK_UPD2, 4 ), 256, 0, st >>>( m, stage, le, ne ); } );
+        timed( BK_UPD1, [ & ] { k_update_list< true, R, 1 ><<< bgrid( bt, BK_UPD1, 4 ), 256, 0, st >>>( m, stage, ne ); } );
+        timed( BK_UPD2, [ & ] { k_update_list< true, R, 2 ><<< bgrid( bt, BK_UPD2, 4 ), 256, 0, st >>>( m, stage, ne ); } );
     }
     k_step_end_multi<<< 1, 1, 0, st >>>( ms, bt->ctx[ 0 ]->cfg.dt_expand );
 }
@@ -448,12 +480,12 @@ kr_batch * kr_batch_create( kr_ctx * const * ctxs, int n )
     bt->fuse = true;
     for( int g = 0; g < n; ++ g )
         bt->fuse = bt->fuse && ctxs[ g ]->fuse_batch;
-    std::vector< int4 > items;
     for( int list = 0; list < 5; ++ list )
     {
-        bt->off[ list ] = ( long long ) items.size(  );
-        for( int g : order )
+        long long count = 0;
+        for( int p = 0; p < n; ++ p )
         {
+            const int g = order[ p ];
             const int * nn = ctxs[ g ]->cfg.n;
             long long tiles, planes;
             if( list == 0 )      { tiles = blocks_for( ( long long ) nn[ 0 ] * nn[ 1 ], 256 ); planes = nn[ 2 ]; }
@@ -467,24 +499,23 @@ kr_batch * kr_batch_create( kr_ctx * const * ctxs, int n )
                 tiles = blocks_for( ( long long ) ext[ 0 ] * ext[ 1 ], 128 );
                 planes = ext[ 2 ];
             }
-            for( int b = 0; b < ctxs[ g ]->nblk; ++ b )
-                for( long long z = 0; z < planes; ++ z )
-                    for( long long x = 0; x < tiles; ++ x )
-                        items.push_back( make_int4( g, b, int( z ), int( x ) ) );
+            bt->l_off[ list ][ p ] = int( count );
+            bt->l_grp[ list ][ p ] = g;
+            bt->l_tiles[ list ][ p ] = int( tiles );
+            bt->l_planes[ list ][ p ] = int( planes );
+            count += tiles * planes * ctxs[ g ]->nblk;
         }
-        bt->cnt[ list ] = ( long long ) items.size(  ) - bt->off[ list ];
+        if( count >= ( 1LL << 31 ) )
+        {
+            g_create_error = "kr_batch_create: a work list of more than 2^31 items";
+            delete bt;
+            return nullptr;
+        }
+        bt->l_off[ list ][ n ] = int( count );
+        bt->cnt[ list ] = count;
     }
     for( int k = 0; k < BK_N; ++ k )          // default: 4 waves of resident CTAs
         bt->grid[ k ] = 4 * bt->n_sm * ( bt->precision == 1 ? bk_min_ctas< float >( k ) : bk_min_ctas< double >( k ) );
-    if( ! bck( bt, cudaMalloc( & bt->items, items.size(  ) * sizeof( int4 ) ), "malloc work list" )
-        || ! bck( bt, cudaMemcpy( bt->items, items.data(  ), items.size(  ) * sizeof( int4 ), cudaMemcpyHostToDevice ),
-                  "upload work list" ) )
-    {
-        g_create_error = bt->err;
-        cudaFree( bt->items );
-        delete bt;
-        return nullptr;
-    }
     return bt;
 }
 
@@ -494,7 +525,6 @@ void kr_batch_destroy( kr_batch * bt )
     cudaSetDevice( bt->ctx[ 0 ]->cfg.device );
     kr::batch_drop_graph( bt );
     if( bt->ev ) cudaEventDestroy( bt->ev );
-    cudaFree( bt->items );
     delete bt;
 }
 
