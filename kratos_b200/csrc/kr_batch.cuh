@@ -36,9 +36,14 @@ struct multi_t
     int ng;
     int l_off[ 5 ][ KR_BATCH_MAX + 1 ];
     int l_grp[ 5 ][ KR_BATCH_MAX ];
-    int l_tiles[ 5 ][ KR_BATCH_MAX ];
-    int l_planes[ 5 ][ KR_BATCH_MAX ];
+    udiv_t l_tiles[ 5 ][ KR_BATCH_MAX ];   // multiply-high quotients (d = 1: the identity)
+    udiv_t l_planes[ 5 ][ KR_BATCH_MAX ];
 };
+
+__device__ __forceinline__ unsigned udiv_q1( unsigned n, const udiv_t & v )
+{
+    return v.d == 1 ? n : udiv_q( n, v );
+}
 
 // Item it of work list `list`: x group, y block, z plane, w tile.  Uniform over
 // the CTA when it is (it comes from blockIdx and the loop counter).
@@ -50,11 +55,11 @@ int4 batch_item( const multi_t< R > & m, int list, int it )
     for( int q = 1; q < KR_BATCH_MAX; ++ q )
         if( q < m.ng && it >= m.l_off[ list ][ q ] )
             p = q;
-    int r = it - m.l_off[ list ][ p ];
-    const int tiles = m.l_tiles[ list ][ p ], planes = m.l_planes[ list ][ p ];
-    const int x = r % tiles;
-    r /= tiles;
-    return make_int4( m.l_grp[ list ][ p ], r / planes, r % planes, x );
+    const unsigned r = unsigned( it - m.l_off[ list ][ p ] );
+    const udiv_t & dt = m.l_tiles[ list ][ p ], & dp = m.l_planes[ list ][ p ];
+    const unsigned q = udiv_q1( r, dt );              // block * planes + plane
+    const unsigned b = udiv_q1( q, dp );
+    return make_int4( m.l_grp[ list ][ p ], int( b ), int( q - b * dp.d ), int( r - q * dt.d ) );
 }
 
 struct multi_scal_t
@@ -104,10 +109,14 @@ k_c2p_list( const __grid_constant__ multi_t< R > m, int step, int n_items )
 
 // MODE: the step's solver; KR_RIEMANN_LEARNED launches the network's sweep
 // (stage 0 of an evaluation step only), FLUX_APPLY the other sweeps.
-template< bool MHD, class R, int MODE >
+// AXIS is a template argument: with a runtime axis, the per-group arguments
+// read through the item's group index left an 80-byte local array in the
+// kernel (the per-size k_flux has none).
+template< bool MHD, class R, int MODE, int AXIS >
 __global__ void __launch_bounds__( 128, ( flux_min_ctas< R, MODE >(  ) ) )
-k_flux_list( const __grid_constant__ multi_t< R > m, int axis, int step, int n_items )
+k_flux_list( const __grid_constant__ multi_t< R > m, int step, int n_items )
 {
+    constexpr int axis = AXIS;
     if constexpr( MODE == KR_RIEMANN_LEARNED || MODE == FLUX_APPLY )
     {   // every group steps in lockstep: group 0's scalars decide
         const bool eval = step == 0 && sel_eval_step( m.a[ 0 ].s, m.a[ 0 ].sel_period );
@@ -199,7 +208,7 @@ struct kr_batch
     // bigger blocks first (decoded on the device, batch_item)
     long long cnt[ 5 ] = { 0 };
     int l_off[ 5 ][ KR_BATCH_MAX + 1 ] = { { 0 } }, l_grp[ 5 ][ KR_BATCH_MAX ] = { { 0 } };
-    int l_tiles[ 5 ][ KR_BATCH_MAX ] = { { 0 } }, l_planes[ 5 ][ KR_BATCH_MAX ] = { { 0 } };
+    kr::udiv_t l_tiles[ 5 ][ KR_BATCH_MAX ] = { }, l_planes[ 5 ][ KR_BATCH_MAX ] = { };
     bool fuse = false;                   // every context fuses stage 0's update with stage 1's c2p
     int grid[ kr::BK_N ] = { 0 };        // CTAs per launch kind (0: one per item)
     cudaGraph_t graph = nullptr;
@@ -285,19 +294,24 @@ static void batch_enqueue( kr_batch * bt, cudaStream_t st, T && timed )
         {
             const int list = 1 + ( 2 - axis );
             const int nl = int( bt->cnt[ list ] );
+            auto sweep = [ & ]( int kind, auto mode )
+            {
+                constexpr int M = decltype( mode )::value;
+                const unsigned g = bgrid( bt, kind, list );
+                timed( kind, [ & ] {
+                    if( axis == 0 )      k_flux_list< true, R, M, 0 ><<< g, 128, 0, st >>>( m, stage, nl );
+                    else if( axis == 1 ) k_flux_list< true, R, M, 1 ><<< g, 128, 0, st >>>( m, stage, nl );
+                    else                 k_flux_list< true, R, M, 2 ><<< g, 128, 0, st >>>( m, stage, nl ); } );
+            };
             if( learned )
             {
-                timed( BK_EVAL, [ & ] {
-                    k_flux_list< true, R, KR_RIEMANN_LEARNED ><<< bgrid( bt, BK_EVAL, list ), 128, 0, st >>>( m, axis, stage, nl ); } );
-                timed( BK_FLUX, [ & ] {
-                    k_flux_list< true, R, FLUX_APPLY ><<< bgrid( bt, BK_FLUX, list ), 128, 0, st >>>( m, axis, stage, nl ); } );
+                sweep( BK_EVAL, std::integral_constant< int, KR_RIEMANN_LEARNED >(  ) );
+                sweep( BK_FLUX, std::integral_constant< int, FLUX_APPLY >(  ) );
             }
             else if( bt->riemann == KR_RIEMANN_HLLE )
-                timed( BK_FLUX, [ & ] {
-                    k_flux_list< true, R, KR_RIEMANN_HLLE ><<< bgrid( bt, BK_FLUX, list ), 128, 0, st >>>( m, axis, stage, nl ); } );
+                sweep( BK_FLUX, std::integral_constant< int, KR_RIEMANN_HLLE >(  ) );
             else
-                timed( BK_FLUX, [ & ] {
-                    k_flux_list< true, R, KR_RIEMANN_DEFAULT ><<< bgrid( bt, BK_FLUX, list ), 128, 0, st >>>( m, axis, stage, nl ); } );
+                sweep( BK_FLUX, std::integral_constant< int, KR_RIEMANN_DEFAULT >(  ) );
         }
         const int ne = int( bt->cnt[ 4 ] );
         timed( BK_EMF, [ & ] { k_emf_list< R ><<< bgrid( bt, BK_EMF, 4 ), 256, 0, st >>>( m, ne ); } );
@@ -501,9 +515,17 @@ kr_batch * kr_batch_create( kr_ctx * const * ctxs, int n )
             }
             bt->l_off[ list ][ p ] = int( count );
             bt->l_grp[ list ][ p ] = g;
-            bt->l_tiles[ list ][ p ] = int( tiles );
-            bt->l_planes[ list ][ p ] = int( planes );
-            count += tiles * planes * ctxs[ g ]->nblk;
+            bt->l_tiles[ list ][ p ] = make_udiv( unsigned( tiles ) );
+            bt->l_planes[ list ][ p ] = make_udiv( unsigned( planes ) );
+            const long long items = tiles * planes * ctxs[ g ]->nblk;
+            // the multiply-high quotients are exact while item * divisor < 2^32
+            if( items * std::max( tiles, planes ) >= ( 1LL << 32 ) )
+            {
+                g_create_error = "kr_batch_create: a box group's work list is too long for 32-bit item decoding";
+                delete bt;
+                return nullptr;
+            }
+            count += items;
         }
         if( count >= ( 1LL << 31 ) )
         {
