@@ -1149,10 +1149,14 @@ void flux_faces( const args_t< R > & a, int axis, int step, udiv_t dv, int b, un
     solve_store< MHD, R, MODE >( a, b, axis, ii, valid, ql, qr, threadIdx.x >> 5, key );
 }
 
-// XL: a refined MHD mesh (the ghost-line normal-B rule, normal_b).
-template< bool MHD, class R, int MODE, bool XL = false >
-__global__ void __launch_bounds__( 128, ( flux_min_ctas< R, MODE >(  ) ) ) k_flux( const args_t< R > a, int axis, int step, udiv_t dv )
+// XL: a refined MHD mesh (the ghost-line normal-B rule, normal_b).  AXIS: the
+// sweep direction as a compile-time constant, so the stencil stride, the
+// component permutation and the face extents fold into the code (one kernel
+// per axis; the sweep is bound by instruction issue).
+template< bool MHD, class R, int MODE, bool XL, int AXIS >
+__global__ void __launch_bounds__( 128, ( flux_min_ctas< R, MODE >(  ) ) ) k_flux( const args_t< R > a, int step, udiv_t dv )
 {
+    constexpr int axis = AXIS;
     bool hlle_warp = false;
     if constexpr( MODE == FLUX_APPLY )
     {   // learned mode, sweeps without the network: this warp's solver choice,
@@ -1170,10 +1174,11 @@ __global__ void __launch_bounds__( 128, ( flux_min_ctas< R, MODE >(  ) ) ) k_flu
 // chunks (cpp per z plane, nz planes), so on the stages where the network does
 // not run (k_flux<FLUX_APPLY> solves them) only this small grid launches and
 // exits.
-template< bool MHD, class R >
+template< bool MHD, class R, int AXIS >
 __global__ void __launch_bounds__( 128, ( flux_min_ctas< R, KR_RIEMANN_LEARNED >(  ) ) )
-k_flux_eval( const args_t< R > a, int axis, int step, udiv_t dv, unsigned cpp, unsigned nz )
+k_flux_eval( const args_t< R > a, int step, udiv_t dv, unsigned cpp, unsigned nz )
 {
+    constexpr int axis = AXIS;
     if( step != 0 || ! sel_eval_step( a.s, a.sel_period ) )
         return;
     for( unsigned ch = blockIdx.x; ch < cpp * nz; ch += gridDim.x )
@@ -2214,8 +2219,8 @@ static long long phys_sites( const kr_ctx * c )
     return std::max( { ( long long ) n[ 1 ] * n[ 2 ], ( long long ) n[ 0 ] * n[ 2 ], ( long long ) n[ 0 ] * n[ 1 ] } );
 }
 
-template< bool MHD, class R, int MODE >
-static void launch_flux( kr_ctx * c, cudaStream_t st, const args_t< R > & a, int axis, int stage )
+template< bool MHD, class R, int MODE, int axis >
+static void launch_flux_axis( kr_ctx * c, cudaStream_t st, const args_t< R > & a, int stage )
 {
     // one thread per face of the sweep, the MHD transverse ghost lines included
     const int * n = c->cfg.n;
@@ -2227,8 +2232,8 @@ static void launch_flux( kr_ctx * c, cudaStream_t st, const args_t< R > & a, int
         const unsigned cpp = blocks_for( ( long long ) ext[ 0 ] * ext[ 1 ], 128 );
         const unsigned ge = unsigned( std::max< long long >( 1, std::min< long long >(
             ( long long ) cpp * ext[ 2 ], ( 2LL * c->n_sm * flux_min_ctas< R, KR_RIEMANN_LEARNED >(  ) ) / c->nblk ) ) );
-        k_flux_eval< MHD, R ><<< dim3( ge, 1, c->nblk ), 128, 0, st >>>(
-            a, axis, stage, make_udiv( unsigned( ext[ 0 ] ) ), cpp, unsigned( ext[ 2 ] ) );
+        k_flux_eval< MHD, R, axis ><<< dim3( ge, 1, c->nblk ), 128, 0, st >>>(
+            a, stage, make_udiv( unsigned( ext[ 0 ] ) ), cpp, unsigned( ext[ 2 ] ) );
     }
     // sweeps without the network: each warp of faces runs the solver chosen
     // for it (exits at once on the network's sweep)
@@ -2238,10 +2243,18 @@ static void launch_flux( kr_ctx * c, cudaStream_t st, const args_t< R > & a, int
         if( c->smr )
         {   // one flat index over each block's faces (flux_faces, XL)
             const dim3 flat( blocks_for( ( long long ) ext[ 0 ] * ext[ 1 ] * ext[ 2 ], 128 ), 1, c->nblk );
-            k_flux< MHD, R, M, true ><<< flat, 128, 0, st >>>( a, axis, stage, make_udiv( unsigned( ext[ 0 ] ) ) );
+            k_flux< MHD, R, M, true, axis ><<< flat, 128, 0, st >>>( a, stage, make_udiv( unsigned( ext[ 0 ] ) ) );
             return;
         }
-    k_flux< MHD, R, M ><<< grid, 128, 0, st >>>( a, axis, stage, make_udiv( unsigned( ext[ 0 ] ) ) );
+    k_flux< MHD, R, M, false, axis ><<< grid, 128, 0, st >>>( a, stage, make_udiv( unsigned( ext[ 0 ] ) ) );
+}
+
+template< bool MHD, class R, int MODE >
+static void launch_flux( kr_ctx * c, cudaStream_t st, const args_t< R > & a, int axis, int stage )
+{
+    if( axis == 0 )      launch_flux_axis< MHD, R, MODE, 0 >( c, st, a, stage );
+    else if( axis == 1 ) launch_flux_axis< MHD, R, MODE, 1 >( c, st, a, stage );
+    else                 launch_flux_axis< MHD, R, MODE, 2 >( c, st, a, stage );
 }
 
 template< bool MHD, class R >
