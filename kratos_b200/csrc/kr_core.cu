@@ -1600,7 +1600,7 @@ void update_site( const args_t< R > & a, int step, udiv_t dv, int b, int i2, uns
 }
 
 template< bool MHD, class R, bool SMR = false, int PART = 0 >
-__global__ void __launch_bounds__( 256, ( SMR && sizeof( R ) == 4 ) ? 3 : ( PART == 2 ? 6 : 4 ) ) k_update( const args_t< R > a, int step, udiv_t dv )
+__global__ void __launch_bounds__( 256, ( SMR && sizeof( R ) == 4 ) ? 4 : ( PART == 2 ? 6 : 4 ) ) k_update( const args_t< R > a, int step, udiv_t dv )
 {
     // grid: x over the lattice sites of one (x, y) plane, y over z, z over blocks
     update_site< MHD, R, SMR, PART >( a, step, dv, blockIdx.z, blockIdx.y, blockIdx.x * blockDim.x + threadIdx.x );
